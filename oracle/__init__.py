@@ -1,0 +1,298 @@
+"""Python access to the oracles (test infrastructure only).
+
+Two CPU libraries check the CUDA path:
+
+* ``liboracle.so`` - the C restatement of the reference algorithms (``mr_oracle.c``);
+* ``_ref/libmuhrec_ref.so`` - the reference's own modules compiled from source by
+  ``ref/Makefile`` (present wherever the reference tree was available at build time;
+  the built file travels with the repository snapshot).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import
+this package. The product library never loads either file.
+
+Array convention: projections are numpy ``float32`` arrays of shape ``(nproj, nv, nu)``
+(kipl ``TImage<float,3>`` order, u fastest).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_F = ctypes.POINTER(ctypes.c_float)
+_D = ctypes.POINTER(ctypes.c_double)
+_SZ = ctypes.POINTER(ctypes.c_size_t)
+_sz = ctypes.c_size_t
+_f = ctypes.c_float
+
+FILTERS = {"ram-lak": 0, "shepp-logan": 1, "hanning": 2, "hamming": 3, "butterworth": 4}
+AVERAGE = {"ImageSum": 0, "ImageAverage": 1, "ImageMedian": 2, "ImageWeightedAverage": 3, "ImageMin": 4, "ImageMax": 5}
+
+
+def _p(a: np.ndarray, t=_F):
+    return a.ctypes.data_as(t)
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+_orc = None
+_ref = None
+
+
+def orc() -> ctypes.CDLL:
+    """The C restatement library (raises if it was not built)."""
+    global _orc
+    if _orc is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle library missing: {path} (run make -C oracle)")
+        lib = ctypes.CDLL(path)
+        lib.orc_frame_dose.restype = ctypes.c_float
+        lib.orc_projfilter_size.restype = ctypes.c_size_t
+        _orc = lib
+    return _orc
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(_HERE, "_ref", "libmuhrec_ref.so"))
+
+
+def ref() -> ctypes.CDLL:
+    """The reference modules compiled from source (raises if absent)."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(_HERE, "_ref", "libmuhrec_ref.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference oracle missing: {path} (run make -C oracle ref)")
+        lib = ctypes.CDLL(path)
+        lib.ref_last_error.restype = ctypes.c_char_p
+        lib.ref_frame_dose.restype = ctypes.c_float
+        _ref = lib
+    return _ref
+
+
+def _check_ref(rc: int) -> None:
+    if rc != 0:
+        raise RuntimeError("reference module failed: " + ref().ref_last_error().decode())
+
+
+# ----------------------------------------------------------------- averaging / dose
+
+
+def average(stack, method: str = "ImageAverage", use_ref: bool = False) -> np.ndarray:
+    stack = _f32(stack)
+    n, nv, nu = stack.shape
+    out = np.empty((nv, nu), np.float32)
+    if use_ref:
+        _check_ref(ref().ref_average(_p(stack), _sz(nu), _sz(nv), _sz(n), AVERAGE[method], _p(out)))
+    else:
+        if orc().orc_average(_p(stack), _sz(nu), _sz(nv), _sz(n), AVERAGE[method], _p(out)) != 0:
+            raise ValueError(f"average method {method} not restated")
+    return out
+
+
+def frame_dose(frame, roi) -> float:
+    frame = _f32(frame)
+    r = np.ascontiguousarray(roi, dtype=np.uint64).astype(np.uintp)
+    return float(orc().orc_frame_dose(_p(frame), _sz(frame.shape[-1]), _p(r, _SZ)))
+
+
+# ----------------------------------------------------------------------- FullLogNorm
+
+
+@dataclass
+class LogNormRefs:
+    dark: np.ndarray
+    logflat: np.ndarray
+    darkdose: float
+    flatdose: float
+
+
+def lognorm_refs(darks, flats, method="ImageAverage", usenormregion=False, dose_roi=(0, 0, 0, 0)) -> LogNormRefs:
+    """NormBase::ReferenceLoader + FullLogNorm::SetReferenceImages (NormPlugins.cpp:91-341)."""
+    darks, flats = _f32(darks), _f32(flats)
+    nd, nf = darks.shape[0], flats.shape[0]
+    nv, nu = flats.shape[1:]
+    dark = average(darks, method) if nd else np.zeros((nv, nu), np.float32)
+    darkdose = np.float32(0.0)
+    if nd:
+        acc = np.float32(0.0)
+        for i in range(nd):
+            t = np.float32(frame_dose(darks[i], dose_roi)) if usenormregion else np.float32(0.0)
+            acc = t if i == 0 else np.float32(acc + t)
+        darkdose = np.float32(acc / np.float32(nd))
+    flatdose = np.float32(1.0)
+    flat = average(flats, method) if nf else np.zeros((nv, nu), np.float32)
+    if nf:
+        acc = np.float32(0.0)
+        for i in range(nf):
+            t = (np.float32(frame_dose(flats[i], dose_roi)) if usenormregion else np.float32(1.0)) - darkdose
+            t = np.float32(t)
+            acc = t if i == 0 else np.float32(acc + t)
+        flatdose = np.float32(acc / np.float32(nf))
+    logflat = np.empty_like(flat)
+    orc().orc_lognorm_logflat(_p(dark), _p(flat), _sz(flat.size), int(nd > 0), _f(flatdose), _p(logflat))
+    return LogNormRefs(dark, logflat, float(darkdose), float(flatdose))
+
+
+def lognorm_doselog(doses, darkdose: float) -> np.ndarray:
+    doses = _f32(doses)
+    out = np.empty_like(doses)
+    orc().orc_lognorm_doselog(_p(doses), _sz(doses.size), _f(darkdose), _p(out))
+    return out
+
+
+def lognorm_apply(proj, dark, logflat, doselog, ndc=True, nob=True) -> np.ndarray:
+    """FullLogNorm::ProcessCore 3D (NormPlugins.cpp:411-552) on float projections."""
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    dark, logflat, doselog = _f32(dark), _f32(logflat), _f32(doselog)
+    nproj = out.shape[0]
+    npix = out[0].size
+    orc().orc_lognorm_apply(_p(out), _sz(npix), _sz(nproj), _p(dark), _p(logflat), _p(doselog),
+                            _sz(doselog.size), int(ndc), int(nob))
+    return out
+
+
+def ref_fulllognorm(proj, darks, flats, method="ImageAverage", usenormregion=False, dose_roi=(0, 0, 0, 0)):
+    """The reference FullLogNorm module on float projections. Returns (out, dark, logflat, doses, (dd, fd))."""
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    darks, flats = _f32(darks), _f32(flats)
+    nproj, nv, nu = out.shape
+    dark = np.zeros((nv, nu), np.float32)
+    logflat = np.zeros((nv, nu), np.float32)
+    doses = np.zeros(nproj, np.float32)
+    rd = np.zeros(2, np.float32)
+    roi = np.asarray(dose_roi, dtype=np.uintp)
+    _check_ref(ref().ref_fulllognorm(_p(out), _sz(nu), _sz(nv), _sz(nproj), _p(darks), _sz(darks.shape[0]),
+                                     _p(flats), _sz(flats.shape[0]), AVERAGE[method], int(usenormregion),
+                                     _p(roi, _SZ), _p(dark), _p(logflat), _p(doses), _p(rd)))
+    return out, dark, logflat, doses, (float(rd[0]), float(rd[1]))
+
+
+# --------------------------------------------------------------------- ProjectionFilter
+
+
+@dataclass
+class FilterPlan:
+    nu: int
+    nfft: int
+    ninsert: int
+    filter: np.ndarray
+    pad: np.ndarray
+
+
+def projfilter_plan(nu, filtertype="hanning", cutoff=0.5, order=1.0, usebias=True, biasweight=0.1,
+                    paddingdoubler=2) -> FilterPlan:
+    nfft = int(orc().orc_projfilter_size(_sz(nu), int(paddingdoubler)))
+    filt = np.zeros(nfft // 2, np.float32)
+    pad = np.zeros(nfft, np.float32)
+    ins = _sz(0)
+    rc = orc().orc_projfilter_build(_sz(nu), FILTERS[filtertype.lower()], _f(cutoff), _f(order), int(usebias),
+                                    _f(biasweight), int(paddingdoubler), _p(filt), _p(pad), ctypes.byref(ins))
+    if rc != 0:
+        raise ValueError("Cut off frequency is not in valid range")
+    return FilterPlan(nu, nfft, ins.value, filt, pad[: ins.value].copy())
+
+
+def projfilter(proj, plan: FilterPlan) -> np.ndarray:
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    rows = out.size // plan.nu
+    orc().orc_projfilter_apply(_p(out), _sz(plan.nu), _sz(rows), _p(plan.filter), _p(plan.pad),
+                               _sz(plan.nfft), _sz(plan.ninsert))
+    return out
+
+
+def ref_projfilter(proj, filtertype="hanning", cutoff=0.5, order=1.0, usebias=True, biasweight=0.1,
+                   paddingdoubler=2):
+    """The reference ProjectionFilterSingle module. Returns (out, filter, nfft)."""
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    nproj, nv, nu = out.shape
+    nfft = int(orc().orc_projfilter_size(_sz(nu), int(paddingdoubler)))
+    filt = np.zeros(nfft // 2, np.float32)
+    n = _sz(0)
+    _check_ref(ref().ref_projfilter(_p(out), _sz(nu), _sz(nv), _sz(nproj), filtertype.encode(), _f(cutoff),
+                                    _f(order), int(usebias), _f(biasweight), int(paddingdoubler), _p(filt),
+                                    ctypes.byref(n)))
+    return out, filt, n.value
+
+
+# ---------------------------------------------------------------------- parallel BP
+
+
+def bp_parallel(proj, angles, weights, center, direction=0, buffersize=16, correcttilt=False, tiltangle=0.0,
+                tiltpivot=0.0, roi_y0=0, nslices=None, use_ref=False, serial=False) -> np.ndarray:
+    """MultiProjectionBPparallel through StdBackProjectorBase::Process 3D.
+
+    Returns the ZXY volume, shape (nu [y], nu [x], nv [z])."""
+    proj = _f32(proj)
+    nproj, nv, nu = proj.shape
+    angles, weights = _f32(angles), _f32(weights)
+    vol = np.zeros((nu, nu, nv), np.float32)
+    if use_ref:
+        _check_ref(ref().ref_bp_parallel(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights), _f(center),
+                                         int(direction), _sz(buffersize), int(correcttilt), _f(tiltangle),
+                                         _f(tiltpivot), _sz(roi_y0), int(serial), _p(vol)))
+    else:
+        rc = orc().orc_bp_parallel(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights), _f(center),
+                                   int(direction), _sz(buffersize), int(correcttilt), _f(tiltangle), _f(tiltpivot),
+                                   _sz(roi_y0), _sz(nslices if nslices is not None else nv), _p(vol))
+        if rc != 0:
+            raise ValueError("invalid parallel-beam backprojection arguments")
+    return vol
+
+
+# ---------------------------------------------------------------------------- FDK
+
+
+class FdkGeom(ctypes.Structure):
+    _fields_ = [("sod", ctypes.c_float), ("sdd", ctypes.c_float), ("ppoint", ctypes.c_float * 2),
+                ("center", ctypes.c_float), ("resolution", ctypes.c_float * 2), ("voxelsize", ctypes.c_float * 3),
+                ("direction", ctypes.c_int), ("correcttilt", ctypes.c_int), ("tiltangle", ctypes.c_float),
+                ("tiltpivot", ctypes.c_float)]
+
+
+def fdk_geom(sod, sdd, ppoint, center, resolution, voxelsize, direction=0, correcttilt=False, tiltangle=0.0,
+             tiltpivot=0.0) -> FdkGeom:
+    g = FdkGeom()
+    g.sod, g.sdd = sod, sdd
+    g.ppoint[0], g.ppoint[1] = ppoint
+    g.center = center
+    g.resolution[0], g.resolution[1] = resolution
+    g.voxelsize[0], g.voxelsize[1], g.voxelsize[2] = voxelsize
+    g.direction = int(direction)
+    g.correcttilt = int(correcttilt)
+    g.tiltangle = tiltangle
+    g.tiltpivot = tiltpivot
+    return g
+
+
+def fdk(proj, angles, weights, geom: FdkGeom, use_ref=False) -> np.ndarray:
+    """FDKbp_single through FdkReconBase::Process 3D. Returns the XYZ volume (nv, nu, nu)."""
+    proj = _f32(proj)
+    nproj, nv, nu = proj.shape
+    angles, weights = _f32(angles), _f32(weights)
+    vol = np.zeros((nv, nu, nu), np.float32)
+    if use_ref:
+        _check_ref(ref().ref_fdk(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights),
+                                 ctypes.byref(geom), _p(vol), None))
+    else:
+        orc().orc_fdk(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights), ctypes.byref(geom), _p(vol))
+    return vol
+
+
+def fdk_ramp(img) -> np.ndarray:
+    out = np.array(img, dtype=np.float32, copy=True, order="C")
+    h, w = out.shape
+    orc().orc_fdk_ramp(_p(out), _sz(w), _sz(h))
+    return out
+
+
+def fdk_projmatrix(geom: FdkGeom, nu: int, angle: float) -> np.ndarray:
+    pm = np.zeros(12, np.float32)
+    orc().orc_fdk_projmatrix(ctypes.byref(geom), _sz(nu), _f(angle), _p(pm))
+    return pm

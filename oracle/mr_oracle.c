@@ -1,0 +1,589 @@
+/* CPU restatement of the MuhRec reconstruction hot path (test infrastructure only).
+ * See mr_oracle.h for the contract. Reference citations are relative to the reference
+ * project root. Built with -ffp-contract=off: every float operation rounds separately,
+ * in the order the reference writes it.
+ */
+#include "mr_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* kipl math constants (core/kipl/kipl/include/math/mathconstants.h:7-8) */
+static const double kDPi = 3.1415926535897932384626433832795028841971693993751;
+static const float kFPi = 3.1415926535897932384626f;
+
+/* ------------------------------------------------------------------ helpers */
+
+static int cmp_float(const void *a, const void *b)
+{
+    float x = *(const float *)a, y = *(const float *)b;
+    return (x > y) - (x < y);
+}
+
+/* kipl::math::median (core/kipl/kipl/include/math/core/median.hpp:10-22): sorted copy,
+ * middle element, or 0.5*(a+b) in double for even counts. */
+static float median_f(const float *v, size_t n)
+{
+    float *tmp = (float *)malloc(n * sizeof(float));
+    memcpy(tmp, v, n * sizeof(float));
+    qsort(tmp, n, sizeof(float), cmp_float);
+    float med;
+    if (n & 1)
+        med = tmp[n / 2];
+    else
+        med = (float)(0.5 * ((double)tmp[n / 2 - 1] + (double)tmp[n / 2]));
+    free(tmp);
+    return med;
+}
+
+/* iterative radix-2 complex FFT in FP64, sign -1 forward, +1 backward, unnormalised */
+static void fft_c2c(double *re, double *im, size_t n, int sign)
+{
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            double t = re[i]; re[i] = re[j]; re[j] = t;
+            t = im[i]; im[i] = im[j]; im[j] = t;
+        }
+    }
+    for (size_t len = 2; len <= n; len <<= 1) {
+        size_t half = len >> 1;
+        for (size_t k = 0; k < half; ++k) {
+            double ang = sign * 2.0 * M_PI * (double)k / (double)len;
+            double wr = cos(ang), wi = sin(ang);
+            for (size_t i = 0; i < n; i += len) {
+                double ur = re[i + k], ui = im[i + k];
+                double xr = re[i + k + half], xi = im[i + k + half];
+                double vr = xr * wr - xi * wi, vi = xr * wi + xi * wr;
+                re[i + k] = ur + vr; im[i + k] = ui + vi;
+                re[i + k + half] = ur - vr; im[i + k + half] = ui - vi;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------- reference averaging */
+
+/* AverageImage::operator() (core/algorithms/ImagingAlgorithms/src/averageimage.cpp:35-219).
+ * The weighted average (StdDevFilter weights, :123-172) is not restated here. */
+int orc_average(const float *stack, size_t nu, size_t nv, size_t n, int method, float *out)
+{
+    const size_t npix = nu * nv;
+    if (n == 0) return -1;
+    switch (method) {
+    case ORC_AVG_SUM:
+    case ORC_AVG_AVERAGE: {
+        for (size_t j = 0; j < npix; ++j) out[j] = 0.0f;
+        for (size_t i = 0; i < n; ++i)
+            for (size_t j = 0; j < npix; ++j) out[j] += stack[i * npix + j];
+        if (method == ORC_AVG_AVERAGE) {
+            float q = 1.0f / (float)n;
+            for (size_t j = 0; j < npix; ++j) out[j] *= q;
+        }
+        return 0;
+    }
+    case ORC_AVG_MEDIAN: {
+        /* median_STL: partial sort, middle element; even counts average the two middle
+         * values in float (median.hpp:24-41) */
+        float *col = (float *)malloc(n * sizeof(float));
+        for (size_t j = 0; j < npix; ++j) {
+            for (size_t i = 0; i < n; ++i) col[i] = stack[i * npix + j];
+            qsort(col, n, sizeof(float), cmp_float);
+            out[j] = (n & 1) ? col[n / 2] : (col[n / 2 - 1] + col[n / 2]) / 2.0f;
+        }
+        free(col);
+        return 0;
+    }
+    case ORC_AVG_MIN:
+    case ORC_AVG_MAX: {
+        for (size_t j = 0; j < npix; ++j) {
+            float v = stack[j];
+            for (size_t i = 1; i < n; ++i) {
+                float s = stack[i * npix + j];
+                v = method == ORC_AVG_MIN ? (s < v ? s : v) : (s > v ? s : v);
+            }
+            out[j] = v;
+        }
+        return 0;
+    }
+    default:
+        return -1;
+    }
+}
+
+/* ProjectionReader::GetProjectionDose (ReconFramework/src/ProjectionReader.cpp:752-783) */
+float orc_frame_dose(const float *frame, size_t nu, const size_t *roi)
+{
+    if ((roi[0] * roi[1] * roi[2] * roi[3]) == 0) return 1.0f;
+    size_t w = roi[2] - roi[0], h = roi[3] - roi[1];
+    float *means = (float *)calloc(h, sizeof(float));
+    for (size_t y = 0; y < h; ++y) {
+        const float *p = frame + (roi[1] + y) * nu + roi[0];
+        for (size_t x = 0; x < w; ++x) means[y] += p[x];
+        means[y] = means[y] / (float)w;
+    }
+    float d = median_f(means, h);
+    free(means);
+    return d;
+}
+
+/* ------------------------------------------------------------ FullLogNorm */
+
+/* FullLogNorm::SetReferenceImages (NormPlugins.cpp:300-341) */
+void orc_lognorm_logflat(const float *dark, const float *flat, size_t npix, int ndc, float flatdose, float *logflat)
+{
+    float dose = 1.0f / flatdose;
+    for (size_t i = 0; i < npix; ++i) {
+        float p = ndc ? flat[i] - dark[i] : flat[i];
+        logflat[i] = p <= 0 ? 0.0f : logf(p * dose);
+    }
+}
+
+/* FullLogNorm::ProcessCore 3D dose list (NormPlugins.cpp:416-425) */
+void orc_lognorm_doselog(const float *doses, size_t nproj, float darkdose, float *doselog)
+{
+    for (size_t i = 0; i < nproj; ++i) {
+        float d = doses[i] - darkdose;
+        doselog[i] = logf(d < 1 ? 1.0f : d);
+    }
+}
+
+/* FullLogNorm::ProcessCore 3D, non-LUT branches (NormPlugins.cpp:481-549) */
+void orc_lognorm_apply(float *proj, size_t npix, size_t nproj, const float *dark, const float *logflat,
+                       const float *doselog, size_t ndose, int ndc, int nob)
+{
+    for (size_t j = 0; j < nproj; ++j) {
+        float *p = proj + j * npix;
+        float dose = ndose != 1 ? doselog[j] : doselog[0];
+        for (size_t i = 0; i < npix; ++i) {
+            float v = ndc ? p[i] - dark[i] : p[i];
+            if (v <= 0.0f)
+                p[i] = 0.0f;
+            else
+                p[i] = nob ? (logflat[i] - logf(v)) + dose : -logf(v) + dose;
+        }
+    }
+}
+
+/* -------------------------------------------------- ProjectionFilterSingle */
+
+/* ProjectionFilterBase::ComputeFilterSize (ProjectionFilter.cpp:120-125) */
+size_t orc_projfilter_size(size_t nu, int paddingdoubler)
+{
+    double e = log((double)nu) / log(2.0);
+    return (size_t)1 << ((size_t)ceil(e) + (size_t)paddingdoubler);
+}
+
+/* ProjectionFilterSingle::BuildFilter + PreparePadding (ProjectionFilter.cpp:254-299,364-376),
+ * with kipl::math::Sigmoid (core/kipl/kipl/include/math/core/mathfunctions.hpp:60-63). */
+int orc_projfilter_build(size_t nu, int filtertype, float cutoff, float order, int usebias, float biasweight,
+                         int paddingdoubler, float *filter, float *pad, size_t *ninsert)
+{
+    size_t nfft = orc_projfilter_size(nu, paddingdoubler);
+    size_t n2 = nfft / 2;
+    if (!((0 < cutoff) && (cutoff <= 0.5f))) return -1;
+    float forder = filtertype == ORC_FILTER_BUTTERWORTH ? order : 0.0f;
+    size_t cut = (size_t)(2 * cutoff * n2);
+    float rampstep = 1.0f / ((n2 - 1.0f));
+    for (size_t i = 0; i < n2; ++i) filter[i] = i * rampstep;
+    float fstep = 1.0f / ((cut - 1.0f));
+    for (size_t i = 0; i < cut; ++i) {
+        switch (filtertype) {
+        case ORC_FILTER_RAMLAK: break;
+        case ORC_FILTER_SHEPPLOGAN: filter[i] = (float)sin(kDPi * i * fstep * cutoff) / n2; break;
+        case ORC_FILTER_HANNING: filter[i] *= (float)(0.5f + 0.5f * cosf(i * fstep * kFPi * cutoff)); break;
+        case ORC_FILTER_HAMMING: filter[i] *= (float)(0.54 + 0.46 * cos(i * fstep * kDPi * cutoff)); break;
+        case ORC_FILTER_BUTTERWORTH: filter[i] /= (float)(1 + powf(i * fstep * cutoff, forder)); break;
+        default: return -1;
+        }
+    }
+    for (size_t i = cut; i < n2; ++i) filter[i] = 0.0f;
+    if (usebias) filter[0] = biasweight * filter[1];
+
+    size_t ins = n2 - nu / 2;
+    for (size_t i = 0; i < ins; ++i) {
+        float x = (float)i / (float)ins - 0.5f;
+        pad[i] = (float)(1.0 / (1.0 + expf(-(x - 0.0f) / 0.07f)));
+    }
+    *ninsert = ins;
+    return 0;
+}
+
+/* ProjectionFilterSingle::FilterProjection + Pad (ProjectionFilter.cpp:301-362) */
+void orc_projfilter_apply(float *proj, size_t nu, size_t nrows, const float *filter, const float *pad,
+                          size_t nfft, size_t ninsert)
+{
+    const size_t n2 = nfft / 2;
+    const size_t nlen = nfft + 16;
+    const float scale = kFPi / (4.0f * n2);
+#pragma omp parallel
+    {
+        float *line = (float *)malloc(nlen * sizeof(float));
+        double *re = (double *)malloc(nfft * sizeof(double));
+        double *im = (double *)malloc(nfft * sizeof(double));
+#pragma omp for schedule(static)
+        for (long r = 0; r < (long)nrows; ++r) {
+            float *src = proj + (size_t)r * nu;
+            memset(line, 0, nlen * sizeof(float));
+            memcpy(line + ninsert, src, nu * sizeof(float));
+            for (size_t i = 0; i < ninsert; ++i) {
+                line[i] = src[0] * pad[i];
+                line[nlen - 1 - i] = src[nu - 1] * pad[i];
+            }
+            for (size_t i = 0; i < nfft; ++i) { re[i] = line[i]; im[i] = 0.0; }
+            fft_c2c(re, im, nfft, -1);
+            /* bins 0..n2-1 are filtered; bin n2 (Nyquist) keeps its value */
+            for (size_t i = 0; i < n2; ++i) {
+                double f = (double)(float)((float)re[i] * filter[i]);
+                double g = (double)(float)((float)im[i] * filter[i]);
+                re[i] = f; im[i] = g;
+            }
+            /* c2r: Hermitian extension of bins 0..n2, imaginary parts of 0 and n2 ignored */
+            im[0] = 0.0;
+            im[n2] = 0.0;
+            for (size_t k = 1; k < n2; ++k) { re[nfft - k] = re[k]; im[nfft - k] = -im[k]; }
+            fft_c2c(re, im, nfft, +1);
+            for (size_t i = 0; i < nu; ++i) src[i] = (float)re[i + ninsert] * scale;
+        }
+        free(line); free(re); free(im);
+    }
+}
+
+/* ------------------------------------------------------ parallel-beam BP */
+
+/* BackProjectorModuleBase::BuildCircleMask (ReconFramework/src/BackProjectorModuleBase.cpp:153-218),
+ * no matrix ROI. mask[2*i] = first, mask[2*i+1] = second. */
+static void circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, size_t nslices, size_t *mask)
+{
+    const float cx = (float)(nx >> 1);
+    const float cy = (float)(ny >> 1);
+    float R = cx - 1;
+    if (correcttilt) {
+        float slices = (float)nslices;
+        R -= floorf(tanf(fabsf(tiltangle) * kFPi / 180.0f) * slices);
+    }
+    const float R2 = R * R;
+    for (size_t i = 0; i < ny; ++i) {
+        float y = (float)i - cy;
+        float y2 = y * y;
+        if (y2 <= R2) {
+            float x = sqrtf(R2 - y2);
+            mask[2 * i] = (size_t)ceilf(cx - x);
+            size_t s = (size_t)floorf(cx + x);
+            mask[2 * i + 1] = (nx - 1u) < s ? (nx - 1u) : s;
+        } else {
+            mask[2 * i] = 0;
+            mask[2 * i + 1] = 0;
+        }
+    }
+}
+
+/* One buffer flush of MultiProjectionBPparallel::BackProject (MultiProjBPparallel.cpp:39-170).
+ * buf: [count][nu][nvpad] weighted, transposed projections. */
+static void bp_flush(const float *buf, size_t count, size_t nu, size_t nv, size_t nvpad, const float *fsin,
+                     const float *fcos, const float *fstartu, const size_t *mask, int correcttilt,
+                     float tiltangle, float tiltpivot, size_t roi_y0, float *vol)
+{
+    const size_t sizez = nv / 4;
+    const int sizeum2 = (int)(nu - 2);
+    const float centeroffset = ((float)roi_y0 - tiltpivot) * tanf(tiltangle * kFPi / 180);
+    const float centerinc = 4 * tanf(tiltangle * kFPi / 180);
+#pragma omp parallel for schedule(static)
+    for (long y = 1; y <= (long)nu; ++y) {
+        float local[1024 * 4];
+        for (size_t i = 0; i < count; ++i)
+            local[i] = correcttilt ? (fstartu[i] + fcos[i] * (float)y) - centeroffset : fstartu[i] + fcos[i] * (float)y;
+        const size_t x0 = mask[2 * (y - 1)], x1 = mask[2 * (y - 1) + 1];
+        for (size_t x = x0 + 1; x <= x1; ++x) {
+            float *col = vol + ((size_t)(y - 1) * nu + (x - 1)) * nv;
+            for (size_t i = 0; i < count; ++i) {
+                float posu = local[i] - fsin[i] * (float)x;
+                int n = (int)posu;
+                if (n < 0 || sizeum2 < n) continue;
+                const float *a = buf + (i * nu + (size_t)n) * nvpad;
+                const float *b = a + nvpad;
+                if (!correcttilt) {
+                    const float wb = fabsf(posu - (float)n);
+                    const float wa = 1.0f - wb;
+                    for (size_t z = 0; z < 4 * sizez; ++z) col[z] = col[z] + (a[z] * wa + b[z] * wb);
+                } else {
+                    posu -= (float)n;
+                    for (size_t zg = 0; zg < sizez; ++zg) {
+                        const float wb = fabsf(posu - (float)zg * centerinc);
+                        const float wa = 1.0f - wb;
+                        for (size_t q = 0; q < 4; ++q) {
+                            size_t z = 4 * zg + q;
+                            col[z] = col[z] + (a[z] * wa + b[z] * wb);
+                        }
+                        posu -= centerinc;
+                    }
+                }
+            }
+        }
+    }
+}
+
+int orc_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
+                    const float *weights, float center, int direction, size_t buffersize, int correcttilt,
+                    float tiltangle, float tiltpivot, size_t roi_y0, size_t nslices, float *vol)
+{
+    if (buffersize == 0 || buffersize > 1024 || nu < 2) return -1;
+    const size_t rest = (nv & 3) ? 4 - (nv & 3) : 0;
+    const size_t nvpad = nv + rest;
+    size_t *mask = (size_t *)malloc(2 * nu * sizeof(size_t));
+    circle_mask(nu, nu, correcttilt, tiltangle, nslices, mask);
+    float *buf = (float *)calloc(buffersize * nu * nvpad, sizeof(float));
+    float fsin[1024], fcos[1024], fstartu[1024];
+    memset(vol, 0, nu * nu * nv * sizeof(float));
+    const size_t mcx = nu / 2;
+    /* StdBackProjectorBase::Process 2D (StdBackProjectorBase.cpp:64-118) */
+    const float dirweight = 2.0f * ((float)direction - 0.5f);
+    size_t counter = 0;
+    for (size_t k = 0; k < nproj; ++k) {
+        fsin[counter] = sinf(dirweight * angles[k] * kFPi / 180.0f);
+        fcos[counter] = cosf(dirweight * angles[k] * kFPi / 180.0f);
+        fstartu[counter] = mcx * (fsin[counter] - fcos[counter]) + center;
+        const float *p = proj + k * nu * nv;
+        float *dst = buf + counter * nu * nvpad;
+        for (size_t u = 0; u < nu; ++u)
+            for (size_t v = 0; v < nv; ++v) dst[u * nvpad + v] = p[v * nu + u] * weights[k];
+        counter++;
+        const int last = k == nproj - 1;
+        if (last || buffersize <= counter) {
+            if (buffersize <= counter) counter--; /* the buffer-full flush drops its last entry */
+            bp_flush(buf, counter, nu, nv, nvpad, fsin, fcos, fstartu, mask, correcttilt, tiltangle, tiltpivot,
+                     roi_y0, vol);
+            counter = 0;
+        }
+    }
+    free(buf);
+    free(mask);
+    return 0;
+}
+
+/* ----------------------------------------------------------------- FDK */
+
+/* FDKbp_single::getProjMatrix (fdkbp_single.cpp:83-255) */
+void orc_fdk_projmatrix(const orc_fdk_geom *g, size_t nu, float angle, float *pm)
+{
+    (void)nu;
+    float extrinsic[16] = {0};
+    float intrinsic[12] = {0};
+    const float sad = g->sod, sid = g->sdd;
+    const float offcenter = (g->ppoint[0] - (float)0 - g->center) * g->voxelsize[0];
+    float cam[3] = {0.0f, 0.0f, 0.0f};
+    if (g->direction == 0) {
+        cam[0] = sad * cosf(-angle * kFPi / 180.0f);
+        cam[1] = sad * sinf(-angle * kFPi / 180.0f);
+    } else {
+        cam[0] = sad * cosf(angle * kFPi / 180.0f);
+        cam[1] = sad * sinf(angle * kFPi / 180.0f);
+    }
+    float plt[3], pup[3], nrm[3];
+    const float vup[3] = {0.0f, 0.0f, 1.0f};
+    const float tgt[3] = {0.0f, 0.0f, 0.0f};
+    nrm[0] = cam[0] - tgt[0];
+    nrm[1] = cam[1] - tgt[1];
+    nrm[2] = cam[2] - tgt[2];
+    float nn = sqrtf(nrm[0] * nrm[0] + nrm[1] * nrm[1] + nrm[2] * nrm[2]);
+    nrm[0] /= nn; nrm[1] /= nn; nrm[2] /= nn;
+    plt[0] = nrm[1] * vup[2] - nrm[2] * vup[1];
+    plt[1] = nrm[2] * vup[0] - nrm[0] * vup[2];
+    plt[2] = nrm[0] * vup[1] - nrm[1] * vup[0];
+    float np = sqrtf(plt[0] * plt[0] + plt[1] * plt[1] + plt[2] * plt[2]);
+    plt[0] /= np; plt[1] /= np; plt[2] /= np;
+    pup[0] = plt[1] * nrm[2] - plt[2] * nrm[1];
+    pup[1] = plt[2] * nrm[0] - plt[0] * nrm[2];
+    pup[2] = plt[0] * nrm[1] - plt[1] * nrm[0];
+    float nq = sqrtf(pup[0] * pup[0] + pup[1] * pup[1] + pup[2] * pup[2]);
+    pup[0] /= nq; pup[1] /= nq; pup[2] /= nq;
+    extrinsic[0] = -1.0f * plt[0]; extrinsic[1] = -1.0f * plt[1]; extrinsic[2] = -1.0f * plt[2];
+    extrinsic[4] = -1.0f * pup[0]; extrinsic[5] = -1.0f * pup[1]; extrinsic[6] = -1.0f * pup[2];
+    extrinsic[8] = -1.0f * nrm[0]; extrinsic[9] = -1.0f * nrm[1]; extrinsic[10] = -1.0f * nrm[2];
+    extrinsic[15] = 1.0f;
+    extrinsic[3] = plt[0] * tgt[0] + plt[1] * tgt[1] + plt[2] * tgt[2] - offcenter;
+    extrinsic[7] = pup[0] * tgt[0] + pup[1] * tgt[1] + pup[2] * tgt[2];
+    extrinsic[11] = nrm[0] * tgt[0] + nrm[1] * tgt[1] + nrm[2] * tgt[2] + sad;
+    intrinsic[0] = 1.0f / g->resolution[0];
+    intrinsic[5] = 1.0f / g->resolution[1];
+    intrinsic[10] = 1.0f / sid;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) {
+            float acc = 0.0f;
+            for (int k = 0; k < 4; ++k) acc += intrinsic[i * 4 + k] * extrinsic[k * 4 + j];
+            pm[i * 4 + j] = acc;
+        }
+}
+
+/* FDKbp_single::ramp_filter_tuned + prepareFFT (fdkbp_single.cpp:832-982) on one
+ * projection [height][width]; FFTs in FP64. */
+void orc_fdk_ramp(float *img, size_t width, size_t height)
+{
+    const unsigned margin = 5;
+    const unsigned padwidth = (unsigned)(2 * pow(2, ceil(log((double)(unsigned)width) / log(2))));
+    const unsigned padfactor = padwidth - (unsigned)width;
+    float *pad = (float *)calloc((size_t)padwidth * height, sizeof(float));
+    for (size_t r = 0; r < height; ++r) memcpy(pad + r * padwidth + padfactor / 2, img + r * width, width * sizeof(float));
+    for (unsigned r = 0; r < margin; ++r) memcpy(pad + r * padwidth, pad + margin * padwidth, padwidth * sizeof(float));
+    for (unsigned r = (unsigned)height - margin; r < height; ++r)
+        memcpy(pad + (size_t)r * padwidth, pad + (height - margin - 1) * padwidth, padwidth * sizeof(float));
+    for (size_t r = 0; r < height; ++r) {
+        for (unsigned c = 0; c < margin; ++c) pad[r * padwidth + c] = pad[r * padwidth + margin];
+        for (unsigned c = padwidth - margin; c < padwidth; ++c) pad[r * padwidth + c] = pad[r * padwidth + padwidth - margin - 1];
+    }
+    float *ramp = (float *)malloc(padwidth * sizeof(float));
+    for (unsigned i = 0; i < padwidth / 2; ++i) ramp[i] = (float)i;
+    for (unsigned i = padwidth / 2; i < padwidth; ++i) ramp[i] = (float)(padwidth - i);
+    const float degtorad = kFPi / 180.0f;
+    for (unsigned i = 0; i < padwidth; ++i) {
+        ramp[i] = (float)(ramp[i] * (0.54 + 0.46 * (cosf(i * degtorad * 360 / padwidth) + 1)));
+        ramp[i] = (float)(ramp[i] / (padwidth * 0.5));
+    }
+    const float rpad = 1.0f / padwidth;
+#pragma omp parallel
+    {
+        double *re = (double *)malloc(padwidth * sizeof(double));
+        double *im = (double *)malloc(padwidth * sizeof(double));
+#pragma omp for schedule(static)
+        for (long r = 0; r < (long)height; ++r) {
+            float *row = pad + (size_t)r * padwidth;
+            for (unsigned c = 0; c < padwidth; ++c) { re[c] = row[c]; im[c] = 0.0; }
+            fft_c2c(re, im, padwidth, -1);
+            for (unsigned c = 0; c < padwidth; ++c) {
+                re[c] = (double)(float)((float)re[c] * ramp[c]);
+                im[c] = (double)(float)((float)im[c] * ramp[c]);
+            }
+            fft_c2c(re, im, padwidth, +1);
+            for (unsigned c = 0; c < padwidth; ++c) row[c] = (float)re[c] * rpad;
+        }
+        free(re); free(im);
+    }
+    for (size_t r = 0; r < height; ++r) memcpy(img + r * width, pad + r * padwidth + padfactor / 2, width * sizeof(float));
+    free(ramp);
+    free(pad);
+}
+
+/* FdkReconBase::Process 3D + FDKbp_single::reconstruct/project_volume_onto_image_c
+ * (fdkreconbase.cpp:217-277, fdkbp_single.cpp:259-531,641-683). Full detector ROI
+ * (roi = projection_roi = {0,0,nu,nv}), volume nu x nu x nv. */
+int orc_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
+            const orc_fdk_geom *g, float *vol)
+{
+    const size_t sx = nu, sy = nu, sz = nv;
+    const size_t npix = nu * nv;
+    size_t *mask = (size_t *)malloc(2 * sy * sizeof(size_t));
+    circle_mask(sx, sy, g->correcttilt, g->tiltangle, nv, mask);
+    float *cbct = (float *)calloc(sx * sy * sz, sizeof(float));
+    float *img = (float *)malloc(npix * sizeof(float));
+    float *xip = (float *)malloc(3 * sx * sizeof(float));
+    float *yip = (float *)malloc(3 * sy * sizeof(float));
+    float *zip = (float *)malloc(3 * sz * sizeof(float));
+    const size_t roi[4] = {0, 0, nu, nv}, proi3 = nv;
+
+    /* geometry constants of project_volume_onto_image_c (fdkbp_single.cpp:302-386) */
+    const float scale = g->sod / g->sdd;
+    const float *spacing = g->voxelsize;
+    const float U = (float)(roi[2] - roi[0]);
+    const float V = (float)(roi[3] - roi[1]);
+    float origin[3];
+    origin[0] = -(U - g->center) * spacing[0] - spacing[0] / 2;
+    origin[1] = -(U - g->center) * spacing[1] - spacing[1] / 2;
+    origin[2] = -(V - (g->ppoint[1] - (float)roi[1])) * spacing[2] - spacing[2] / 2;
+    const float radius = (float)sy * g->voxelsize[0] / 2;
+    size_t cb[4] = {roi[0], 0, roi[2], 0};
+    const float fp1 = g->ppoint[1], r1 = (float)roi[1], r3 = (float)roi[3];
+    const float vx = g->voxelsize[0], sdd = g->sdd, sod = g->sod, res0 = g->resolution[0];
+    if (fp1 >= r1 && fp1 >= r3) {
+        cb[3] = (size_t)(fp1 - ((fp1 - r3) * vx * sdd / (sod + radius)) / res0);
+        float value = fp1 - ((fp1 - r1) * vx * sdd / (sod - radius)) / res0;
+        cb[1] = value <= 0 ? 0 : (size_t)(fp1 - ((fp1 - r1) * vx * sdd / (sod - radius)) / res0);
+    }
+    if (fp1 < r1 && fp1 < r3) {
+        float value = fp1 + ((r1 - fp1) * vx * sdd / (sod + radius)) / res0;
+        cb[1] = (size_t)value;
+        float value2 = fp1 + ((r3 - fp1) * vx * sdd / (sod - radius)) / res0;
+        cb[3] = value2 >= proi3 ? proi3 : (size_t)(float)value2;
+    }
+    if (fp1 >= r1 && fp1 < r3) {
+        float value = fp1 - ((fp1 - r1) * vx * sdd / (sod - radius)) / res0;
+        cb[1] = value <= 0 ? 0 : (size_t)(fp1 - ((fp1 - r1) * vx * sdd / (sod - radius)) / res0);
+        float value2 = fp1 + ((r3 - fp1) * vx * sdd / (sod - radius)) / res0;
+        cb[3] = value2 >= proi3 ? proi3 : (size_t)(float)value2;
+    }
+    if (cb[1] != 0) cb[1] -= 8;
+    if (cb[3] + 8 <= proi3) cb[3] += 8;
+    const float ic[2] = {g->ppoint[0] - (float)cb[0], g->ppoint[1] - (float)cb[1]};
+    const float sad_sid_2 = (g->sod * g->sod) / (g->sdd * g->sdd);
+
+    for (size_t p = 0; p < nproj; ++p) {
+        const float *src = proj + p * npix;
+        for (size_t i = 0; i < npix; ++i) img[i] = src[i] * weights[p];
+        float pm[12];
+        orc_fdk_projmatrix(g, nu, angles[p], pm);
+        orc_fdk_ramp(img, nu, nv);
+        for (size_t i = 0; i < npix; ++i) {
+            img[i] *= sad_sid_2;
+            img[i] *= scale;
+        }
+        for (size_t i = 0; i < sx; ++i) {
+            float x = (float)(origin[0] + (float)i * spacing[0]);
+            xip[i * 3 + 0] = x * (pm[0] + ic[0] * pm[8]);
+            xip[i * 3 + 1] = x * (pm[4] + ic[1] * pm[8]);
+            xip[i * 3 + 2] = x * pm[8];
+        }
+        for (size_t j = 0; j < sy; ++j) {
+            float y = (float)(origin[1] + (float)j * spacing[1]);
+            yip[j * 3 + 0] = y * (pm[1] + ic[0] * pm[9]);
+            yip[j * 3 + 1] = y * (pm[5] + ic[1] * pm[9]);
+            yip[j * 3 + 2] = y * pm[9];
+        }
+        for (size_t k = 0; k < sz; ++k) {
+            float z = (float)(origin[2] + (float)k * spacing[2]);
+            if (g->correcttilt) {
+                float pos = (float)cb[3] - (float)k - g->tiltpivot;
+                float cor = (float)(tan(-g->tiltangle * kDPi / 180) * pos + g->center);
+                pm[3] = ((cor - (g->ppoint[0] - (float)roi[0])) * g->voxelsize[0]) / g->resolution[0];
+            }
+            zip[k * 3 + 0] = z * (pm[2] + ic[0] * pm[10]) + ic[0] * pm[11] + pm[3];
+            zip[k * 3 + 1] = z * (pm[6] + ic[1] * pm[10]) + ic[1] * pm[11] + pm[7];
+            zip[k * 3 + 2] = z * pm[10] + pm[11];
+        }
+        const float fh = (float)nv, fw = (float)nu;
+#pragma omp parallel for schedule(static)
+        for (long k = 0; k < (long)sz; ++k) {
+            for (size_t j = 0; j < sy; ++j) {
+                const float a0 = zip[3 * k] + yip[3 * j];
+                const float a1 = zip[3 * k + 1] + yip[3 * j + 1];
+                const float a2 = zip[3 * k + 2] + yip[3 * j + 2];
+                float *line = cbct + (size_t)k * sy * sx + j * sx;
+                for (size_t i = mask[2 * j] + 1; i <= mask[2 * j + 1]; ++i) {
+                    const float dw = 1.0f / (a2 + xip[3 * i + 2]);
+                    float r = dw * (a1 + xip[3 * i + 1]);
+                    float c = dw * (a0 + xip[3 * i]);
+                    float val;
+                    r += 0.5f;
+                    c += 0.5f;
+                    if (r < 0 || r >= fh || c < 0 || c >= fw)
+                        val = 0.0f;
+                    else
+                        val = img[(size_t)(int)r * nu + (size_t)(int)c];
+                    line[i] += dw * dw * val;
+                }
+            }
+        }
+    }
+    /* final per-slice horizontal mirror and z reversal (fdkreconbase.cpp:259-270) */
+    for (size_t k = 0; k < sz; ++k)
+        for (size_t j = 0; j < sy; ++j)
+            for (size_t i = 0; i < sx; ++i)
+                vol[(sz - k - 1) * sy * sx + j * sx + i] = cbct[k * sy * sx + j * sx + (sx - 1 - i)];
+    free(mask); free(cbct); free(img); free(xip); free(yip); free(zip);
+    return 0;
+}

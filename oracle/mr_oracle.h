@@ -1,0 +1,80 @@
+/* CPU restatement of the MuhRec reconstruction hot path (test infrastructure only).
+ *
+ * This is the oracle the CUDA path is checked against. It restates, in plain C, the
+ * algorithms of the reference modules named beside each function (paths relative to the
+ * reference project root). Only tests/, __graft_entry__.smoke() and the CPU-baseline leg
+ * of bench.py may load it; the product library never links or calls it.
+ *
+ * Parity pinning: every function here is checked against the reference's own modules
+ * compiled from source (oracle/ref, libmuhrec_ref.so) and against the reference's
+ * golden vectors (tests/golden). Float arithmetic follows the reference's operation
+ * order with no contraction (built with -ffp-contract=off), so results are bit-identical
+ * where the reference is deterministic; FFTs run in FP64 (FFTW is not available).
+ *
+ * Layouts: projections [nproj][nv][nu] (u fastest), the kipl TImage<float,3> order.
+ */
+#ifndef MR_ORACLE_H
+#define MR_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ImagingAlgorithms::AverageImage methods (averageimage.h:16-23) */
+enum { ORC_AVG_SUM = 0, ORC_AVG_AVERAGE, ORC_AVG_MEDIAN, ORC_AVG_WEIGHTED, ORC_AVG_MIN, ORC_AVG_MAX };
+
+int orc_average(const float *stack, size_t nu, size_t nv, size_t n, int method, float *out);
+float orc_frame_dose(const float *frame, size_t nu, const size_t *roi);
+
+/* FullLogNorm (StdPreprocModules/src/NormPlugins.cpp:300-552) */
+void orc_lognorm_logflat(const float *dark, const float *flat, size_t npix, int ndc, float flatdose, float *logflat);
+void orc_lognorm_doselog(const float *doses, size_t nproj, float darkdose, float *doselog);
+void orc_lognorm_apply(float *proj, size_t npix, size_t nproj, const float *dark, const float *logflat,
+                       const float *doselog, size_t ndose, int ndc, int nob);
+
+/* ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:120-376) */
+enum { ORC_FILTER_RAMLAK = 0, ORC_FILTER_SHEPPLOGAN, ORC_FILTER_HANNING, ORC_FILTER_HAMMING, ORC_FILTER_BUTTERWORTH };
+size_t orc_projfilter_size(size_t nu, int paddingdoubler);
+int orc_projfilter_build(size_t nu, int filtertype, float cutoff, float order, int usebias, float biasweight,
+                         int paddingdoubler, float *filter, float *pad, size_t *ninsert);
+void orc_projfilter_apply(float *proj, size_t nu, size_t nrows, const float *filter, const float *pad,
+                          size_t nfft, size_t ninsert);
+
+/* MultiProjectionBPparallel through StdBackProjectorBase (StdBackProjectors/src/
+ * StdBackProjectorBase.cpp:64-201, MultiProjBPparallel.cpp:39-170,
+ * ReconFramework/src/BackProjectorModuleBase.cpp:153-218). vol: ZXY [nu][nu][nv]. */
+int orc_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
+                    const float *weights, float center, int direction, size_t buffersize, int correcttilt,
+                    float tiltangle, float tiltpivot, size_t roi_y0, size_t nslices, float *vol);
+
+/* FDKbp_single via FdkReconBase (FDKBackProjectors/src/fdkbp_single.cpp:83-994,
+ * fdkreconbase.cpp:91-277). vol: XYZ [nv][nu][nu] after the final mirror. */
+typedef struct {
+    float sod, sdd;
+    float ppoint[2];
+    float center;
+    float resolution[2];
+    float voxelsize[3];
+    int direction;
+    int correcttilt;
+    float tiltangle;
+    float tiltpivot;
+} orc_fdk_geom;
+int orc_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
+            const orc_fdk_geom *g, float *vol);
+/* pieces of orc_fdk, exposed for kernel-level checks */
+void orc_fdk_ramp(float *img, size_t width, size_t height);
+void orc_fdk_projmatrix(const orc_fdk_geom *g, size_t nu, float angle, float *pm /*12*/);
+
+/* FP64 backprojection references for the precision form (no reference counterpart):
+ * the same sampling as the FP32 paths with all geometry and accumulation in double. */
+int orc_fdk_f64(const float *filtered, size_t nu, size_t nv, size_t nproj, const double *pm /*12 per proj*/,
+                const double *ic /*2*/, const size_t *mask /*2 per row*/, int bilinear, const size_t *slices,
+                size_t nslices, double *out /*[nslices][nu][nu]*/);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

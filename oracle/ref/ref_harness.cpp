@@ -1,0 +1,462 @@
+// C-ABI harness around the reference's own CPU modules (test infrastructure only).
+//
+// This translation unit is compiled against the reference headers and linked with the
+// reference sources (see oracle/ref/Makefile). It exposes each hot-path module through
+// plain pointers so the tests can run the UNMODIFIED reference code on the same seeded
+// inputs as the CUDA path. Nothing here is on the product path: only tests/ and the
+// CPU-baseline leg of bench.py load the resulting oracle/_ref/libmuhrec_ref.so.
+//
+// The reference modules normally receive their inputs through the engine (file reader,
+// XML config). The harness sets the same fields in code instead:
+//   * ReconConfig fields are assigned directly (frameworks/tomography/Framework/
+//     ReconFramework/include/ReconConfig.h:77-175);
+//   * per-projection doses and the reference-frame doses follow ProjectionReader::
+//     GetProjectionDose (ProjectionReader.cpp:752-783): median of the row means inside
+//     the dose ROI;
+//   * reference frames are averaged with ImagingAlgorithms::AverageImage exactly as
+//     NormBase::ReferenceLoader does (NormPlugins.cpp:91-230), then handed to
+//     FullLogNorm::SetReferenceImages (NormPlugins.cpp:300-341).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <functional>
+#include <iostream>
+#include <iterator>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+
+// Module internals (reference images, doses, protected ProcessCore) are set/called
+// directly, so member access is opened for the reference headers only.
+#define protected public
+#define private public
+#include <base/timage.h>
+#include <ReconConfig.h>
+#include <ParameterHandling.h>
+#include <averageimage.h>
+#include <MorphSpotClean.h>
+#include <StripeFilter.h>
+#include <math/median.h>
+#include "NormPlugins.h"
+#include "ProjectionFilter.h"
+#include "MorphSpotCleanModule.h"
+#include "WaveletRingClean.h"
+#include "MultiProjBPparallel.h"
+#include "MultiProjBP.h"
+#include "fdkbp_single.h"
+#include "linearforwardprojector.h"
+#undef private
+#undef protected
+
+namespace {
+
+std::string g_error;
+
+std::string list_text(const float *v, size_t n)
+{
+    std::ostringstream s;
+    char buf[64];
+    for (size_t i = 0; i < n; ++i) {
+        std::snprintf(buf, sizeof(buf), "%.9g", static_cast<double>(v[i]));
+        if (i) s << ' ';
+        s << buf;
+    }
+    return s.str();
+}
+
+// ProjectionReader::GetProjectionDose restated on an in-memory frame
+// (ProjectionReader.cpp:760-782): median over rows of the row mean inside roi.
+float frame_dose(const float *frame, size_t nu, const size_t *roi)
+{
+    if (!(roi[0] * roi[1] * roi[2] * roi[3])) return 1.0f;
+    const size_t w = roi[2] - roi[0], h = roi[3] - roi[1];
+    std::vector<float> means(h, 0.0f);
+    for (size_t y = 0; y < h; ++y) {
+        const float *p = frame + (roi[1] + y) * nu + roi[0];
+        for (size_t x = 0; x < w; ++x) means[y] += p[x];
+        means[y] = means[y] / static_cast<float>(w);
+    }
+    float dose = 0.0f;
+    kipl::math::median(means.data(), h, &dose);
+    return dose;
+}
+
+template <typename F>
+int guarded(F f)
+{
+    try {
+        f();
+        return 0;
+    } catch (kipl::base::KiplException &e) {
+        g_error = e.what();
+    } catch (std::exception &e) {
+        g_error = e.what();
+    } catch (...) {
+        g_error = "unknown exception";
+    }
+    return -1;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *ref_last_error() { return g_error.c_str(); }
+
+float ref_frame_dose(const float *frame, size_t nu, const size_t *roi) { return frame_dose(frame, nu, roi); }
+
+// ImagingAlgorithms::AverageImage::operator() (averageimage.cpp:35-61)
+int ref_average(const float *stack, size_t nu, size_t nv, size_t n, int method, float *out)
+{
+    return guarded([&] {
+        size_t dims[3] = {nu, nv, n};
+        kipl::base::TImage<float, 3> img(dims);
+        std::memcpy(img.GetDataPtr(), stack, sizeof(float) * nu * nv * n);
+        ImagingAlgorithms::AverageImage avg;
+        kipl::base::TImage<float, 2> r = avg(img, static_cast<ImagingAlgorithms::AverageImage::eAverageMethod>(method));
+        std::memcpy(out, r.GetDataPtr(), sizeof(float) * nu * nv);
+    });
+}
+
+// FullLogNorm: reference preparation (ReferenceLoader + SetReferenceImages) and
+// ProcessCore 3D (NormPlugins.cpp:411-552) on projections [nproj][nv][nu].
+// dose_roi is in projection coordinates (x0,y0,x1,y1); all-zero disables dose ROI use.
+int ref_fulllognorm(float *proj, size_t nu, size_t nv, size_t nproj,
+                    const float *darks, size_t ndark, const float *flats, size_t nflat,
+                    int refavg, int usenormregion, const size_t *dose_roi,
+                    float *dark_out, float *flat_out, float *doses_out, float *refdoses_out)
+{
+    return guarded([&] {
+        FullLogNorm mod;
+        ReconConfig cfg;
+        cfg.ProjectionInfo.nDCCount = ndark;
+        cfg.ProjectionInfo.nOBCount = nflat;
+        std::memcpy(cfg.ProjectionInfo.dose_roi, dose_roi, 4 * sizeof(size_t));
+        std::map<std::string, std::string> par;
+        par["usenormregion"] = usenormregion ? "true" : "false";
+        par["uselut"] = "false";
+        ImagingAlgorithms::AverageImage::eAverageMethod m =
+            static_cast<ImagingAlgorithms::AverageImage::eAverageMethod>(refavg);
+        par["referenceaverage"] = enum2string(m);
+        mod.Configure(cfg, par);
+
+        size_t d2[2] = {nu, nv};
+        ImagingAlgorithms::AverageImage avg;
+        kipl::base::TImage<float, 2> dark(d2), flat(d2);
+        float darkdose = 0.0f, flatdose = 1.0f;
+        if (ndark) {
+            size_t d3[3] = {nu, nv, ndark};
+            kipl::base::TImage<float, 3> st(d3);
+            std::memcpy(st.GetDataPtr(), darks, sizeof(float) * nu * nv * ndark);
+            float dose = 0.0f;
+            for (size_t i = 0; i < ndark; ++i) {
+                float t = usenormregion ? frame_dose(darks + i * nu * nv, nu, dose_roi) : 0.0f;
+                dose = i == 0 ? t : dose + t;
+            }
+            darkdose = dose / static_cast<float>(ndark);
+            dark = avg(st, m);
+        }
+        if (nflat) {
+            size_t d3[3] = {nu, nv, nflat};
+            kipl::base::TImage<float, 3> st(d3);
+            std::memcpy(st.GetDataPtr(), flats, sizeof(float) * nu * nv * nflat);
+            float dose = 0.0f;
+            for (size_t i = 0; i < nflat; ++i) {
+                float t = (usenormregion ? frame_dose(flats + i * nu * nv, nu, dose_roi) : 1.0f) - darkdose;
+                dose = i == 0 ? t : dose + t;
+            }
+            flatdose = dose / static_cast<float>(nflat);
+            flat = avg(st, m);
+        }
+        mod.fDarkDose = darkdose;
+        mod.fFlatDose = flatdose;
+        if (dark_out) std::memcpy(dark_out, dark.GetDataPtr(), sizeof(float) * nu * nv);
+        mod.SetReferenceImages(dark, flat);
+        if (flat_out) std::memcpy(flat_out, mod.mFlatField.GetDataPtr(), sizeof(float) * nu * nv);
+        if (refdoses_out) {
+            refdoses_out[0] = darkdose;
+            refdoses_out[1] = flatdose;
+        }
+
+        std::vector<float> doses(nproj, 1.0f);
+        if (usenormregion)
+            for (size_t i = 0; i < nproj; ++i) doses[i] = frame_dose(proj + i * nu * nv, nu, dose_roi);
+        if (doses_out) std::memcpy(doses_out, doses.data(), sizeof(float) * nproj);
+        std::map<std::string, std::string> coeff;
+        coeff["dose"] = list_text(doses.data(), nproj);
+
+        size_t d3[3] = {nu, nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+        mod.Process(img, coeff);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * nu * nv * nproj);
+    });
+}
+
+// ProjectionFilterSingle (ProjectionFilter.cpp:254-376) on projections [nproj][nv][nu].
+int ref_projfilter(float *proj, size_t nu, size_t nv, size_t nproj, const char *filtertype,
+                   float cutoff, float order, int usebias, float biasweight, int paddingdoubler,
+                   float *filter_out, size_t *nfft_out)
+{
+    return guarded([&] {
+        ProjectionFilterSingle mod(nullptr);
+        ReconConfig cfg;
+        cfg.ProjectionInfo.roi[0] = 0;
+        cfg.ProjectionInfo.roi[1] = 0;
+        cfg.ProjectionInfo.roi[2] = nu;
+        cfg.ProjectionInfo.roi[3] = nv;
+        std::map<std::string, std::string> par;
+        par["filtertype"] = filtertype;
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.9g", cutoff);
+        par["cutoff"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", order);
+        par["order"] = b;
+        par["usebias"] = usebias ? "true" : "false";
+        std::snprintf(b, sizeof(b), "%.9g", biasweight);
+        par["biasweight"] = b;
+        par["paddingdoubler"] = std::to_string(paddingdoubler);
+        mod.Configure(cfg, par);
+        if (nfft_out) *nfft_out = mod.nFFTsize;
+        if (filter_out) std::memcpy(filter_out, mod.mFilter.GetDataPtr(), sizeof(float) * mod.mFilter.Size());
+        if (proj && nproj) {
+            size_t d3[3] = {nu, nv, nproj};
+            kipl::base::TImage<float, 3> img(d3);
+            std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+            std::map<std::string, std::string> coeff;
+            mod.Process(img, coeff);
+            std::memcpy(proj, img.GetDataPtr(), sizeof(float) * nu * nv * nproj);
+        }
+    });
+}
+
+// MultiProjectionBPparallel (MultiProjBPparallel.cpp:39-170) driven through
+// StdBackProjectorBase::Process 3D (StdBackProjectorBase.cpp:120-149).
+// proj: [nproj][nv][nu]; vol out: ZXY [nu (y)][nu (x)][nv (z)].
+// serial != 0 selects the serial MultiProjectionBP (MultiProjBP.cpp:36-146) instead.
+int ref_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj,
+                    const float *angles, const float *weights, float center, int direction,
+                    size_t buffersize, int correcttilt, float tiltangle, float tiltpivot,
+                    size_t roi_y0, int serial, float *vol)
+{
+    return guarded([&] {
+        ReconConfig cfg;
+        cfg.ProjectionInfo.fCenter = center;
+        cfg.ProjectionInfo.eDirection = static_cast<kipl::base::eRotationDirection>(direction);
+        cfg.ProjectionInfo.bCorrectTilt = correcttilt != 0;
+        cfg.ProjectionInfo.fTiltAngle = tiltangle;
+        cfg.ProjectionInfo.fTiltPivotPosition = tiltpivot;
+        cfg.ProjectionInfo.imagetype = ReconConfig::cProjections::ImageType_Projections;
+        cfg.ProjectionInfo.beamgeometry = ReconConfig::cProjections::BeamGeometry_Parallel;
+        cfg.ProjectionInfo.nDims[0] = nu;
+        cfg.ProjectionInfo.nDims[1] = nv;
+        cfg.MatrixInfo.bUseROI = false;
+        std::map<std::string, std::string> par;
+        par["ProjectionBufferSize"] = std::to_string(buffersize);
+        par["SliceBlock"] = "32";
+        par["SubVolume"] = "1 1";
+        StdBackProjectorBase *bp = nullptr;
+        if (serial)
+            bp = new MultiProjectionBP(nullptr);
+        else
+            bp = new MultiProjectionBPparallel(nullptr);
+        std::unique_ptr<StdBackProjectorBase> hold(bp);
+        bp->Configure(cfg, par);
+        size_t roi[4] = {0, roi_y0, nu, roi_y0 + nv};
+        bp->SetROI(roi);
+        size_t d3[3] = {nu, nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+        std::map<std::string, std::string> params;
+        params["angles"] = list_text(angles, nproj);
+        params["weights"] = list_text(weights, nproj);
+        bp->Process(img, params);
+        std::memcpy(vol, bp->volume.GetDataPtr(), sizeof(float) * bp->volume.Size());
+    });
+}
+
+struct ref_fdk_geom {
+    float sod, sdd;
+    float ppoint[2];
+    float center;
+    float resolution[2];
+    float voxelsize[3];
+    int direction;
+    int correcttilt;
+    float tiltangle;
+    float tiltpivot;
+};
+
+// FDKbp_single (fdkbp_single.cpp:83-994) through FdkReconBase::Process 3D
+// (fdkreconbase.cpp:217-277). proj: [nproj][nv][nu]; vol out: XYZ [nv][nu][nu]
+// after the final mirror/z-reversal; cbct_out (optional) before it.
+int ref_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
+            const float *weights, const ref_fdk_geom *g, float *vol, float *cbct_out)
+{
+    return guarded([&] {
+        ReconConfig cfg;
+        cfg.ProjectionInfo.fSOD = g->sod;
+        cfg.ProjectionInfo.fSDD = g->sdd;
+        cfg.ProjectionInfo.fpPoint[0] = g->ppoint[0];
+        cfg.ProjectionInfo.fpPoint[1] = g->ppoint[1];
+        cfg.ProjectionInfo.fCenter = g->center;
+        cfg.ProjectionInfo.fResolution[0] = g->resolution[0];
+        cfg.ProjectionInfo.fResolution[1] = g->resolution[1];
+        cfg.MatrixInfo.fVoxelSize[0] = g->voxelsize[0];
+        cfg.MatrixInfo.fVoxelSize[1] = g->voxelsize[1];
+        cfg.MatrixInfo.fVoxelSize[2] = g->voxelsize[2];
+        cfg.ProjectionInfo.eDirection = static_cast<kipl::base::eRotationDirection>(g->direction);
+        cfg.ProjectionInfo.bCorrectTilt = g->correcttilt != 0;
+        cfg.ProjectionInfo.fTiltAngle = g->tiltangle;
+        cfg.ProjectionInfo.fTiltPivotPosition = g->tiltpivot;
+        cfg.ProjectionInfo.imagetype = ReconConfig::cProjections::ImageType_Projections;
+        cfg.ProjectionInfo.beamgeometry = ReconConfig::cProjections::BeamGeometry_Cone;
+        cfg.ProjectionInfo.nDims[0] = nu;
+        cfg.ProjectionInfo.nDims[1] = nv;
+        cfg.ProjectionInfo.nFirstIndex = 0;
+        cfg.ProjectionInfo.nLastIndex = nproj - 1;
+        cfg.ProjectionInfo.nProjectionStep = 1;
+        size_t roi[4] = {0, 0, nu, nv};
+        std::memcpy(cfg.ProjectionInfo.roi, roi, sizeof(roi));
+        std::memcpy(cfg.ProjectionInfo.projection_roi, roi, sizeof(roi));
+        cfg.MatrixInfo.nDims[0] = nu;
+        cfg.MatrixInfo.nDims[1] = nu;
+        cfg.MatrixInfo.nDims[2] = nv;
+        cfg.MatrixInfo.bUseROI = false;
+        std::map<std::string, std::string> par;
+        par["ProjectionBufferSize"] = "16";
+        par["SliceBlock"] = "32";
+        par["SubVolume"] = "1 1";
+        FDKbp_single fdk(nullptr);
+        fdk.Configure(cfg, par);
+        fdk.SetROI(roi);
+        size_t d3[3] = {nu, nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+        std::map<std::string, std::string> params;
+        params["angles"] = list_text(angles, nproj);
+        params["weights"] = list_text(weights, nproj);
+        fdk.Process(img, params);
+        std::memcpy(vol, fdk.volume.GetDataPtr(), sizeof(float) * fdk.volume.Size());
+        if (cbct_out) std::memcpy(cbct_out, fdk.cbct_volume.GetDataPtr(), sizeof(float) * fdk.cbct_volume.Size());
+        delete[] fdk.proj_matrices;
+    });
+}
+
+// ImagingAlgorithms::MorphSpotClean::process on one image [nv][nu]
+// (MorphSpotClean.cpp:41-83), configured like the python binding tests.
+int ref_morphspotclean(float *img, size_t nu, size_t nv, int detect, int clean, int conn,
+                       const float *th, const float *sigma, int edgesmooth, int maxarea,
+                       int clamp, float minlevel, float maxlevel, int removeinfnan)
+{
+    return guarded([&] {
+        ImagingAlgorithms::MorphSpotClean c;
+        c.setCleanMethod(static_cast<ImagingAlgorithms::eMorphDetectionMethod>(detect),
+                         static_cast<ImagingAlgorithms::eMorphCleanMethod>(clean));
+        c.setConnectivity(static_cast<kipl::morphology::MorphConnect>(conn));
+        c.setLimits(clamp != 0, minlevel, maxlevel, maxarea);
+        c.cleanInfNan(removeinfnan != 0);
+        if (edgesmooth > 0) c.setEdgeConditioning(edgesmooth);
+        size_t d2[2] = {nu, nv};
+        kipl::base::TImage<float, 2> im(d2);
+        std::memcpy(im.GetDataPtr(), img, sizeof(float) * nu * nv);
+        std::vector<float> t(th, th + 2), s(sigma, sigma + 2);
+        c.process(im, t, s);
+        std::memcpy(img, im.GetDataPtr(), sizeof(float) * nu * nv);
+    });
+}
+
+// MorphSpotCleanModule::Configure + ProcessCore 3D (MorphSpotCleanModule.cpp:37-183)
+// on projections [nproj][nv][nu]. Parameters use the module's text names.
+int ref_morphspotclean_module(float *proj, size_t nu, size_t nv, size_t nproj, const char *connectivity,
+                              const char *cleanmethod, const char *detectionmethod, const char *threshold,
+                              const char *sigma, int edgesmooth, int maxarea, int removeinfnan, int clampdata,
+                              float minlevel, float maxlevel)
+{
+    return guarded([&] {
+        MorphSpotCleanModule mod(nullptr);
+        ReconConfig cfg;
+        std::map<std::string, std::string> par;
+        par["connectivity"] = connectivity;
+        par["cleanmethod"] = cleanmethod;
+        par["detectionmethod"] = detectionmethod;
+        par["threshold"] = threshold;
+        par["sigma"] = sigma;
+        par["edgesmooth"] = std::to_string(edgesmooth);
+        par["maxarea"] = std::to_string(maxarea);
+        par["removeinfnan"] = removeinfnan ? "true" : "false";
+        par["clampdata"] = clampdata ? "true" : "false";
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.9g", minlevel);
+        par["minlevel"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", maxlevel);
+        par["maxlevel"] = b;
+        par["threading"] = "false";
+        if (mod.Configure(cfg, par) != 0) throw std::runtime_error("MorphSpotCleanModule::Configure failed");
+        size_t d3[3] = {nu, nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+        std::map<std::string, std::string> coeff;
+        mod.Process(img, coeff);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * nu * nv * nproj);
+    });
+}
+
+// ImagingAlgorithms::StripeFilter::process on one sinogram [ntheta][nu]
+// (StripeFilter.cpp:83-135).
+int ref_stripefilter(float *sino, size_t nu, size_t ntheta, const char *wname, int scale, float sigma, int op)
+{
+    return guarded([&] {
+        size_t d2[2] = {nu, ntheta};
+        ImagingAlgorithms::StripeFilter f(d2, wname, scale, sigma);
+        kipl::base::TImage<float, 2> im(d2);
+        std::memcpy(im.GetDataPtr(), sino, sizeof(float) * nu * ntheta);
+        f.process(im, static_cast<ImagingAlgorithms::eStripeFilterOperation>(op));
+        std::memcpy(sino, im.GetDataPtr(), sizeof(float) * nu * ntheta);
+    });
+}
+
+// StripeFilter damping window for one level (StripeFilter.cpp:183-213).
+int ref_stripefilter_window(size_t nu, size_t ntheta, const char *wname, int scale, float sigma, int level,
+                            float *out, size_t *n_out)
+{
+    return guarded([&] {
+        size_t d2[2] = {nu, ntheta};
+        ImagingAlgorithms::StripeFilter f(d2, wname, scale, sigma);
+        std::vector<float> w = f.filterWindow(level);
+        *n_out = w.size();
+        if (out) std::copy(w.begin(), w.end(), out);
+    });
+}
+
+// WaveletRingClean::Configure + ProcessCore 3D (WaveletRingClean.cpp:29-103) on
+// projections [nproj][nv][nu].
+int ref_waveletringclean(float *proj, size_t nu, size_t nv, size_t nproj, const char *wname, int decnum,
+                         float sigma)
+{
+    return guarded([&] {
+        WaveletRingClean mod(nullptr);
+        ReconConfig cfg;
+        std::map<std::string, std::string> par;
+        par["wname"] = wname;
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.9g", sigma);
+        par["sigma"] = b;
+        par["decnum"] = std::to_string(decnum);
+        par["parallel"] = "false";
+        par["method"] = "verticalfft";
+        mod.Configure(cfg, par);
+        size_t d3[3] = {nu, nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+        std::map<std::string, std::string> coeff;
+        mod.Process(img, coeff);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * nu * nv * nproj);
+    });
+}
+
+} // extern "C"
