@@ -1,0 +1,395 @@
+"""Benchmark: FDK cone-beam reconstruction of a 1024^3 volume from 1024 projections of
+1024 x 1024 pixels (uint16 counts -> FullLogNorm -> FDK ramp filter -> FDK backprojection),
+FP32 and with BF16-stored filtered projections.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mr|reference] [--small]
+
+One step = one full reconstruction of the block with the counts already in HBM. `value`
+is voxel x projection updates per second (GUPS, whole job over all ranks), FP32 path.
+`e2e` is the same metric through the public pipeline with pinned host buffers: the
+uint16 counts go host->device and the float volume comes back every step.
+
+Multi-GPU (torchrun): every rank reconstructs its own z-slab block of the same size
+(independent slabs, no data-path collective); `scaling` is weak; the step time is the
+maximum over ranks.
+
+`--impl reference` times the reference's own CPU FDK (FDKbp_single compiled from the
+reference sources into oracle/_ref) on a bounded sample of the same workload with all
+host threads, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "backprojection GUPS + projections/s, FP32 vs BF16-proj at <=1e-3 rel RMS vs FP64"
+
+
+def workload(small: bool):
+    if small:
+        return dict(name="FDK 256^3 from 256 projections of 256x256 (profiling case)", nu=256, nv=256, nproj=256,
+                    sod=300.0, sdd=600.0, pitch=0.8, voxel=0.4, i0=50000.0)
+    # BASELINE precision form: FDK cone-beam geometry of the 512^3 case scaled x2
+    return dict(name="FDK 1024^3 from 1024 projections of 1024x1024", nu=1024, nv=1024, nproj=1024, sod=300.0,
+                sdd=600.0, pitch=0.2, voxel=0.1, i0=50000.0)
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            p = [x.strip() for x in ln.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax.append(float(p[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_inputs(w, seed, device):
+    import torch
+
+    from imagingsuite_b200 import phantom
+
+    ells = phantom.ellipsoids(1000 + 4)
+    fov = w["nu"] * w["voxel"]
+    integ = phantom.cone_integrals_torch(ells, w["nproj"], w["nu"], w["nv"], w["sod"], w["sdd"], w["pitch"], fov,
+                                         device)
+    counts, flats, darks = phantom.counts_torch(integ, w["i0"], 2000 + 4 + seed, 10, 10)
+    del integ
+    torch.cuda.synchronize()
+    return counts, flats, darks
+
+
+def make_config(w):
+    from imagingsuite_b200 import modules as M
+
+    cfg = M.ReconConfig()
+    pi = cfg.ProjectionInfo
+    pi.fSOD, pi.fSDD = w["sod"], w["sdd"]
+    pi.fpPoint = ((w["nu"] - 1) / 2.0, (w["nv"] - 1) / 2.0)
+    pi.fCenter = (w["nu"] - 1) / 2.0
+    pi.fResolution = (w["pitch"], w["pitch"])
+    pi.roi = pi.projection_roi = (0, 0, w["nu"], w["nv"])
+    pi.nDims = (w["nu"], w["nv"], w["nproj"])
+    cfg.MatrixInfo.fVoxelSize = (w["voxel"],) * 3
+    cfg.MatrixInfo.nDims = (w["nu"], w["nu"], w["nv"])
+    return cfg
+
+
+def time_steps(fn, steps, warmup, stream, dist_ctx, events_kernel=None):
+    """Warm up, then time exactly `steps` calls between barriers + synchronize; returns
+    (max-over-ranks seconds, per-step kernel durations dict)."""
+    import torch
+
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    if dist_ctx:
+        dist_ctx.barrier()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    for _ in range(steps):
+        fn()
+    end.record(stream)
+    torch.cuda.synchronize()
+    if dist_ctx:
+        dist_ctx.barrier()
+    t = start.elapsed_time(end) / 1e3
+    if dist_ctx:
+        t = dist_ctx.max(t)
+    return t
+
+
+class Dist:
+    def __init__(self):
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        self.dist = dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self.dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
+
+    def barrier(self):
+        self.dist.barrier()
+
+    def max(self, v: float) -> float:
+        import torch
+
+        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+
+def kernel_time(fn, stream, reps=2):
+    """Average device duration of one call of fn (CUDA events on `stream`)."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record(stream)
+    for _ in range(reps):
+        fn()
+    e.record(stream)
+    torch.cuda.synchronize()
+    return s.elapsed_time(e) / 1e3 / reps
+
+
+def run_mr(args):
+    import torch
+
+    from imagingsuite_b200 import _lib as L
+    from imagingsuite_b200 import pipeline
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    dctx = Dist() if world > 1 else None
+    rank = dctx.rank if dctx else 0
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    w = workload(args.small)
+    nu, nv, nproj = w["nu"], w["nv"], w["nproj"]
+    updates = float(nu) * nu * nv * nproj
+
+    counts, flats, darks = make_inputs(w, rank, device)
+    cfg = make_config(w)
+    angles = np.arange(nproj, dtype=np.float32) * np.float32(360.0 / nproj)
+    weights = np.full(nproj, np.float32(1.0 / nproj), np.float32)
+    pipe32 = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="fp32")
+    pipe16 = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="bf16")
+    stream = torch.cuda.current_stream()
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    t32 = time_steps(lambda: pipe32.run_device(counts), args.steps, args.warmup, stream, dctx)
+    clocks = sampler.stop()
+    t16 = time_steps(lambda: pipe16.run_device(counts), args.steps, max(3, args.warmup // 2), stream, dctx)
+
+    # dominant kernel (FDK backprojection) alone, on the launching stream
+    fdk = pipe32.fdk
+    filt = torch.empty((nproj, nv, nu), device=device)
+    proj = pipe32._lognorm_into(counts)
+    wgt, X, Y, Z, s2, sc, uni = fdk._geo
+    st = stream.cuda_stream
+    L.check(L.lib().mr_fdk_filter(proj.data_ptr(), nu, nv, nproj, wgt.data_ptr(), s2, sc, L.MR_F32, filt.data_ptr(),
+                                  None, st))
+    vol = torch.empty((nv, nu, nu), device=device)
+
+    def bp32():
+        L.check(L.lib().mr_fdk_backproject(filt.data_ptr(), L.MR_F32, None, nu, nv, nproj, X.data_ptr(), Y.data_ptr(),
+                                           Z.data_ptr(), uni, fdk._mask.data_ptr(), 0, vol.data_ptr(), st))
+
+    tbp = kernel_time(bp32, stream)
+    q16 = torch.empty((nproj, nv, nu), dtype=torch.uint16, device=device)
+    qs = torch.empty(nproj, device=device)
+    L.check(L.lib().mr_quantize(filt.data_ptr(), nu * nv, nproj, L.MR_BF16, q16.data_ptr(), qs.data_ptr(), st))
+    vol16 = torch.empty((nv, nu, nu), device=device)
+
+    def bp16():
+        L.check(L.lib().mr_fdk_backproject(q16.data_ptr(), L.MR_BF16, qs.data_ptr(), nu, nv, nproj, X.data_ptr(),
+                                           Y.data_ptr(), Z.data_ptr(), uni, fdk._mask.data_ptr(), 0, vol16.data_ptr(),
+                                           st))
+
+    tbp16 = kernel_time(bp16, stream)
+    # precision: BF16-stored vs FP32 volumes on 16 seeded slices
+    rng = np.random.default_rng(16)
+    sl = torch.from_numpy(np.sort(rng.choice(nv, 16, replace=False))).to(device)
+    a, b = vol16.index_select(0, sl).double(), vol.index_select(0, sl).double()
+    rel16 = float(torch.sqrt(((a - b) ** 2).mean() / (b ** 2).mean()).item())
+    del filt, q16, vol16, vol
+
+    # end to end through the pipeline with pinned host buffers
+    counts_h = counts.cpu().pin_memory()
+    out_h = torch.empty((nv, nu, nu), dtype=torch.float32).pin_memory()
+    te2e = time_steps(lambda: pipe32.run_host(counts_h, out_h, device), max(1, min(args.steps, 3)), 1, stream, dctx)
+    e2e_steps = max(1, min(args.steps, 3))
+
+    res = None
+    if rank == 0:
+        peaks = {}
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        except OSError:
+            pass
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+        bp_bytes = 4.0 * updates  # gathered FP32 samples, 4 B per voxel x projection update
+        ach = bp_bytes / tbp / 1e9
+        n = world
+        res = {
+            "metric": METRIC,
+            "value": n * updates * args.steps / t32 / 1e9,
+            "unit": "GUPS",
+            "n_gpus": n,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": t32 / args.steps * 1e3,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic (seeded 10-ellipsoid phantom, analytic cone-beam line integrals, Poisson I0=5e4)",
+            "config": {"workload": w["name"], "volume": [nu, nu, nv], "projections": nproj, "detector": [nu, nv],
+                       "chain": "FullLogNorm(u16) -> FDK ramp filter -> FDK NN backprojection",
+                       "l2": "inputs larger than L2 (2.1 GB counts per step)", "parallelism": f"z-slab x{n}"},
+            "projections_per_s": n * nproj * args.steps / t32,
+            "bf16": {"value": n * updates * args.steps / t16 / 1e9,
+                     "unit": "GUPS", "ms_per_step": t16 / args.steps * 1e3,
+                     "backprojection_gups": updates / tbp16 / 1e9, "rel_rms_vs_fp32_16_slices": rel16},
+            "backprojection_gups": updates / tbp / 1e9,
+            "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "traffic": None, "kernel": "k_fdk<f32>",
+                         "note": f"algorithmic bytes = 4 B/update gathered; peak {peak_src}"},
+            "e2e": {"value": n * updates * e2e_steps / te2e / 1e9, "unit": "GUPS",
+                    "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(nu * nu * nv * 4)},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            res["cpu_baseline"] = cpu_baseline(w, counts, flats, darks, angles, weights, budget_s=args.cpu_budget)
+    if dctx:
+        dctx.barrier()
+        dctx.dist.destroy_process_group()
+    return res
+
+
+def cpu_baseline(w, counts, flats, darks, angles, weights, budget_s=20.0, nsample=None):
+    """The reference FDKbp_single (compiled from the reference sources) on a bounded sample:
+    the full volume from the first `nsample` projections, all host threads."""
+    import oracle
+
+    if not oracle.ref_available():
+        return {"value": None, "unit": "GUPS", "cores": 0, "kind": "reference", "sample": "reference library absent"}
+    nu, nv = w["nu"], w["nv"]
+    cores = os.cpu_count() or 1
+    c = counts[:1].cpu().numpy().astype(np.float32)
+    # normalised projections from the CUDA path's reference images (input preparation only)
+    dark = darks.float().mean(0).cpu().numpy()
+    flat = flats.float().mean(0).cpu().numpy()
+    p1 = np.where(c - dark > 0, np.log(np.maximum(flat - dark, 1e-3)) - np.log(np.maximum(c - dark, 1e-3)), 0)
+    g = oracle.fdk_geom(w["sod"], w["sdd"], ((nu - 1) / 2.0, (nv - 1) / 2.0), (nu - 1) / 2.0, (w["pitch"],) * 2,
+                        (w["voxel"],) * 3)
+    t0 = time.perf_counter()
+    oracle.fdk(p1, angles[:1], weights[:1], g, use_ref=True)
+    t1 = time.perf_counter() - t0
+    n = nsample or max(1, min(16, int(budget_s / max(t1, 1e-3))))
+    proj = np.repeat(p1, n, axis=0)
+    t0 = time.perf_counter()
+    oracle.fdk(proj, angles[:n], weights[:n], g, use_ref=True)
+    t = time.perf_counter() - t0
+    return {"value": float(nu) * nu * nv * n / t / 1e9, "unit": "GUPS", "cores": cores, "kind": "reference",
+            "sample": f"reference FDKbp_single, full {nu}x{nu}x{nv} volume from {n} projections "
+                      f"({t:.1f} s, ramp filter + backprojection, OMP_NUM_THREADS={os.environ.get('OMP_NUM_THREADS', cores)})"}
+
+
+def run_reference(args):
+    """--impl reference: the reference CPU implementation on a bounded sample per step."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1 and rank != 0:
+        return None
+    import oracle
+
+    w = workload(args.small)
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "reference library oracle/_ref/libmuhrec_ref.so not built"}
+    nu, nv = w["nu"], w["nv"]
+    rng = np.random.default_rng(0)
+    nsample = 2
+    proj = rng.standard_normal((nsample, nv, nu)).astype(np.float32)
+    angles = np.arange(nsample, dtype=np.float32) * np.float32(360.0 / w["nproj"])
+    weights = np.full(nsample, np.float32(1.0 / w["nproj"]))
+    g = oracle.fdk_geom(w["sod"], w["sdd"], ((nu - 1) / 2.0, (nv - 1) / 2.0), (nu - 1) / 2.0, (w["pitch"],) * 2,
+                        (w["voxel"],) * 3)
+    for _ in range(args.warmup):
+        oracle.fdk(proj[:1], angles[:1], weights[:1], g, use_ref=True)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        oracle.fdk(proj, angles, weights, g, use_ref=True)
+    t = time.perf_counter() - t0
+    updates = float(nu) * nu * nv * nsample
+    v = updates * args.steps / t / 1e9
+    cores = os.cpu_count() or 1
+    return {"impl": "reference", "metric": METRIC, "value": v, "unit": "GUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": w["name"], "sample_projections_per_step": nsample},
+            "cpu_baseline": {"value": v, "unit": "GUPS", "cores": cores, "kind": "reference",
+                             "sample": f"full {nu}x{nu}x{nv} volume from {nsample} projections per step"},
+            "e2e": {"value": v, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mr", choices=["mr", "reference"])
+    ap.add_argument("--small", action="store_true", help="256^3 profiling case")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    res = run_reference(args) if args.impl == "reference" else run_mr(args)
+    if res is not None:
+        print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

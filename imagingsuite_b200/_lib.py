@@ -1,0 +1,94 @@
+"""ctypes binding of the mrcuda C ABI (``include/mrcuda.h``).
+
+The library is built in-tree by ``imagingsuite_b200.build``. Loading fails loudly when it
+is missing: there is no CPU fallback for any entry point.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libmrcuda.so")
+
+c_size = ctypes.c_size_t
+c_int = ctypes.c_int
+c_float = ctypes.c_float
+c_void = ctypes.c_void_p
+P_float = ctypes.POINTER(ctypes.c_float)
+P_size = ctypes.POINTER(ctypes.c_size_t)
+P_int = ctypes.POINTER(ctypes.c_int)
+P_u32 = ctypes.POINTER(ctypes.c_uint32)
+
+MR_OK, MR_ERR_ARGUMENT, MR_ERR_CUDA, MR_ERR_ALLOCATION, MR_ERR_UNSUPPORTED, MR_ERR_DEVICE = range(6)
+MR_F32, MR_BF16, MR_F16, MR_U16 = 0, 1, 2, 3
+
+
+class FdkGeom(ctypes.Structure):
+    """mr_fdk_geom: the ReconConfig fields FDKbp_single reads."""
+
+    _fields_ = [("sod", c_float), ("sdd", c_float), ("ppoint", c_float * 2), ("center", c_float),
+                ("resolution", c_float * 2), ("voxelsize", c_float * 3), ("direction", c_int),
+                ("correcttilt", c_int), ("tiltangle", c_float), ("tiltpivot", c_float)]
+
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "mr_version": (c_int, []),
+    "mr_status_string": (ctypes.c_char_p, [c_int]),
+    "mr_last_error": (ctypes.c_char_p, []),
+    "mr_reference_average": (c_int, [c_void, c_size, c_size, c_size, c_int, c_void, c_void]),
+    "mr_projection_dose": (c_int, [c_void, c_int, c_size, c_size, c_size, P_size, c_void, c_void]),
+    "mr_lognorm_logflat": (c_int, [c_void, c_void, c_size, c_int, c_float, c_void, c_void]),
+    "mr_lognorm_doselog": (c_int, [P_float, c_size, c_float, P_float]),
+    "mr_lognorm_apply": (c_int, [c_void, c_int, c_size, c_size, c_void, c_void, c_void, c_size, c_int, c_int,
+                                 c_void, c_void]),
+    "mr_projfilter_tables": (c_int, [c_size, ctypes.c_char_p, c_float, c_float, c_int, c_float, c_int, P_size, P_size,
+                                     P_float, P_float]),
+    "mr_projfilter_create": (c_int, [c_size, ctypes.c_char_p, c_float, c_float, c_int, c_float, c_int,
+                                     ctypes.POINTER(c_void)]),
+    "mr_projfilter_destroy": (c_int, [c_void]),
+    "mr_projfilter_info": (c_int, [c_void, P_size, P_size, P_float, P_float]),
+    "mr_projfilter_apply": (c_int, [c_void, c_void, c_void, c_size, c_void, c_size, c_void]),
+    "mr_bp_parallel_geometry": (c_int, [P_float, c_size, c_size, c_float, c_int, P_float, P_float, P_float]),
+    "mr_bp_circle_mask": (c_int, [c_size, c_size, c_int, c_float, c_size, P_u32]),
+    "mr_bp_parallel_tilt": (c_int, [c_float, c_float, c_size, P_float, P_float]),
+    "mr_bp_parallel": (c_int, [c_void, c_int, c_void, c_void, c_void, c_void, c_void, c_void, c_size, c_size, c_size,
+                               c_void, c_int, c_float, c_float, c_void, c_void]),
+    "mr_quantize": (c_int, [c_void, c_size, c_size, c_int, c_void, c_void, c_void]),
+    "mr_fdk_partials": (c_int, [ctypes.POINTER(FdkGeom), c_size, c_size, P_float, c_size, P_float, P_float, P_float,
+                                P_float, P_float, P_int]),
+    "mr_fdk_filter": (c_int, [c_void, c_size, c_size, c_size, c_void, c_float, c_float, c_int, c_void, c_void,
+                              c_void]),
+    "mr_fdk_backproject": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_int,
+                                   c_void, c_int, c_void, c_void]),
+}
+
+EXPORTED = tuple(_PROTOS)
+
+_lib = None
+
+
+class MrError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"mrcuda library not built: {LIB_PATH} (python -m imagingsuite_b200.build)")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _PROTOS.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != MR_OK:
+        raise MrError(status, lib().mr_last_error().decode())

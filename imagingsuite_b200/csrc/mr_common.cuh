@@ -1,0 +1,71 @@
+// Shared helpers of the mrcuda library: status/error plumbing, launch checks,
+// 16-bit projection storage. Host and device.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cstdarg>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "mrcuda.h"
+
+namespace mr {
+
+// Per-thread last error message (mr_last_error).
+void set_error(const char *fmt, ...);
+
+inline mr_status fail(mr_status s, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    set_error("%s", buf);
+    return s;
+}
+
+inline mr_status check_launch(const char *what)
+{
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(MR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    return MR_OK;
+}
+
+#define MR_CUDA_TRY(call)                                                                                   \
+    do {                                                                                                   \
+        cudaError_t e_ = (call);                                                                           \
+        if (e_ != cudaSuccess) return ::mr::fail(MR_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));   \
+    } while (0)
+
+inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+inline unsigned div_up(size_t a, size_t b) { return static_cast<unsigned>((a + b - 1) / b); }
+
+// ---- 16-bit projection storage: value = stored * scale (scale per projection, a power of two)
+template <int DT>
+struct Sample;
+template <>
+struct Sample<MR_F32> {
+    using T = float;
+    static __device__ __forceinline__ float load(const float *p, size_t i) { return __ldg(p + i); }
+};
+template <>
+struct Sample<MR_BF16> {
+    using T = __nv_bfloat16;
+    static __device__ __forceinline__ float load(const __nv_bfloat16 *p, size_t i)
+    {
+        return __bfloat162float(__ldg(p + i));
+    }
+};
+template <>
+struct Sample<MR_F16> {
+    using T = __half;
+    static __device__ __forceinline__ float load(const __half *p, size_t i) { return __half2float(__ldg(p + i)); }
+};
+
+} // namespace mr

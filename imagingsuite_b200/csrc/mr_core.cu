@@ -1,0 +1,294 @@
+// Library plumbing (version, status text, per-thread error message), reference-frame
+// averaging, projection dose and the FullLogNorm kernels.
+//
+// Reference: frameworks/tomography/Preprocessing/StdPreprocModules/src/NormPlugins.cpp
+// (FullLogNorm), core/algorithms/ImagingAlgorithms/src/averageimage.cpp (AverageImage),
+// frameworks/tomography/Framework/ReconFramework/src/ProjectionReader.cpp:752-783 (dose).
+#include "mr_common.cuh"
+
+#include <cmath>
+#include <cstring>
+
+namespace mr {
+
+static thread_local std::string g_last_error;
+
+void set_error(const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+// ------------------------------------------------------------------ reference averaging
+
+// One thread per pixel; frames summed in frame order so the float rounding sequence is the
+// reference's (ComputeSum :63-77, ComputeAverage :79-89, ComputeMin/Max :174-219).
+__global__ void k_average(const float *__restrict__ frames, size_t npix, int n, int method, float *__restrict__ out)
+{
+    size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (j >= npix) return;
+    if (method == 0 || method == 1) {
+        float s = 0.0f;
+        for (int i = 0; i < n; ++i) s = __fadd_rn(s, frames[i * npix + j]);
+        if (method == 1) s = __fmul_rn(s, __fdiv_rn(1.0f, static_cast<float>(n)));
+        out[j] = s;
+    } else if (method == 4 || method == 5) {
+        float v = frames[j];
+        for (int i = 1; i < n; ++i) {
+            float s = frames[i * npix + j];
+            v = method == 4 ? (s < v ? s : v) : (s > v ? s : v);
+        }
+        out[j] = v;
+    } else {
+        // ImageMedian (:91-106, median_STL): middle of the sorted column; even counts
+        // average the two middle values in float.
+        float col[64];
+        for (int i = 0; i < n; ++i) col[i] = frames[i * npix + j];
+        for (int i = 1; i < n; ++i) {
+            float key = col[i];
+            int q = i - 1;
+            while (q >= 0 && col[q] > key) {
+                col[q + 1] = col[q];
+                --q;
+            }
+            col[q + 1] = key;
+        }
+        out[j] = (n & 1) ? col[n / 2] : __fdiv_rn(__fadd_rn(col[n / 2 - 1], col[n / 2]), 2.0f);
+    }
+}
+
+// ------------------------------------------------------------------ projection dose
+
+// Row means of the dose ROI: one thread per (frame, row), columns summed in order
+// (ProjectionReader.cpp:768-774).
+template <typename T>
+__global__ void k_row_means(const T *__restrict__ in, size_t nu, size_t nv, size_t nframes, size_t x0, size_t y0,
+                            size_t w, size_t h, float *__restrict__ means)
+{
+    size_t y = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    size_t f = blockIdx.y;
+    if (y >= h || f >= nframes) return;
+    const T *p = in + f * nu * nv + (y0 + y) * nu + x0;
+    float s = 0.0f;
+    for (size_t x = 0; x < w; ++x) s = __fadd_rn(s, static_cast<float>(p[x]));
+    means[f * h + y] = __fdiv_rn(s, static_cast<float>(w));
+}
+
+// Median of h row means per frame: bitonic sort in shared memory, then the middle
+// element, or 0.5*(a+b) in double for even h (kipl median.hpp:10-22).
+__global__ void k_median(const float *__restrict__ means, size_t h, unsigned npow2, float *__restrict__ dose)
+{
+    extern __shared__ float s[];
+    const float *m = means + blockIdx.x * h;
+    for (unsigned i = threadIdx.x; i < npow2; i += blockDim.x) s[i] = i < h ? m[i] : INFINITY;
+    __syncthreads();
+    for (unsigned k = 2; k <= npow2; k <<= 1) {
+        for (unsigned j = k >> 1; j > 0; j >>= 1) {
+            for (unsigned i = threadIdx.x; i < npow2; i += blockDim.x) {
+                unsigned l = i ^ j;
+                if (l > i) {
+                    bool up = (i & k) == 0;
+                    float a = s[i], b = s[l];
+                    if ((a > b) == up) {
+                        s[i] = b;
+                        s[l] = a;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    if (threadIdx.x == 0) {
+        float d = (h & 1) ? s[h / 2] : static_cast<float>(0.5 * (static_cast<double>(s[h / 2 - 1]) + s[h / 2]));
+        dose[blockIdx.x] = d;
+    }
+}
+
+__global__ void k_fill(float *p, size_t n, float v)
+{
+    size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+// ------------------------------------------------------------------ FullLogNorm
+
+__global__ void k_logflat(const float *__restrict__ dark, const float *__restrict__ flat, size_t npix, int ndc,
+                          float dose, float *__restrict__ logflat)
+{
+    size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (i >= npix) return;
+    float p = ndc ? __fsub_rn(flat[i], dark[i]) : flat[i];
+    logflat[i] = p <= 0.0f ? 0.0f : logf(__fmul_rn(p, dose));
+}
+
+template <typename T>
+__device__ __forceinline__ float lognorm_px(T raw, float dark, float logflat, float dose, int ndc, int nob)
+{
+    float v = ndc ? __fsub_rn(static_cast<float>(raw), dark) : static_cast<float>(raw);
+    if (v <= 0.0f) return 0.0f;
+    float lg = logf(v);
+    return nob ? __fadd_rn(__fsub_rn(logflat, lg), dose) : __fadd_rn(-lg, dose);
+}
+
+// Grid-stride over groups of 4 pixels of one projection row block; blockIdx.y = projection.
+// Vector loads when npix % 4 == 0 (the common case), scalar tail otherwise.
+template <typename T>
+__global__ void k_lognorm(const T *__restrict__ in, size_t npix, const float *__restrict__ dark,
+                          const float *__restrict__ logflat, const float *__restrict__ doselog, size_t ndose, int ndc,
+                          int nob, int vec, float *__restrict__ out)
+{
+    const size_t j = blockIdx.y;
+    const float dose = ndose != 1 ? doselog[j] : doselog[0];
+    const T *src = in + j * npix;
+    float *dst = out + j * npix;
+    const size_t n4 = vec ? npix / 4 : 0;
+    for (size_t q = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; q < n4;
+         q += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float4 d = ndc ? reinterpret_cast<const float4 *>(dark)[q] : make_float4(0, 0, 0, 0);
+        const float4 f = nob ? reinterpret_cast<const float4 *>(logflat)[q] : make_float4(0, 0, 0, 0);
+        float4 r;
+        if constexpr (sizeof(T) == 2) {
+            const ushort4 v = reinterpret_cast<const ushort4 *>(src)[q];
+            r.x = lognorm_px(v.x, d.x, f.x, dose, ndc, nob);
+            r.y = lognorm_px(v.y, d.y, f.y, dose, ndc, nob);
+            r.z = lognorm_px(v.z, d.z, f.z, dose, ndc, nob);
+            r.w = lognorm_px(v.w, d.w, f.w, dose, ndc, nob);
+        } else {
+            const float4 v = reinterpret_cast<const float4 *>(src)[q];
+            r.x = lognorm_px(v.x, d.x, f.x, dose, ndc, nob);
+            r.y = lognorm_px(v.y, d.y, f.y, dose, ndc, nob);
+            r.z = lognorm_px(v.z, d.z, f.z, dose, ndc, nob);
+            r.w = lognorm_px(v.w, d.w, f.w, dose, ndc, nob);
+        }
+        reinterpret_cast<float4 *>(dst)[q] = r;
+    }
+    for (size_t i = n4 * 4 + blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < npix;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        dst[i] = lognorm_px(src[i], ndc ? dark[i] : 0.0f, nob ? logflat[i] : 0.0f, dose, ndc, nob);
+    }
+}
+
+} // namespace mr
+
+using namespace mr;
+
+extern "C" {
+
+int mr_version(void) { return 100; }
+
+const char *mr_status_string(mr_status s)
+{
+    switch (s) {
+    case MR_OK: return "ok";
+    case MR_ERR_ARGUMENT: return "invalid argument";
+    case MR_ERR_CUDA: return "CUDA error";
+    case MR_ERR_ALLOCATION: return "allocation failed";
+    case MR_ERR_UNSUPPORTED: return "unsupported";
+    case MR_ERR_DEVICE: return "device-side error status";
+    default: return "unknown status";
+    }
+}
+
+const char *mr_last_error(void) { return g_last_error.c_str(); }
+
+mr_status mr_reference_average(const float *frames_d, size_t nu, size_t nv, size_t n, int method, float *out_d,
+                               void *stream)
+{
+    if (!frames_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_reference_average: null pointer");
+    if (n == 0) return fail(MR_ERR_ARGUMENT, "mr_reference_average: no frames");
+    if (!(method == 0 || method == 1 || method == 2 || method == 4 || method == 5))
+        return fail(MR_ERR_UNSUPPORTED, "mr_reference_average: method %d not supported", method);
+    if (method == 2 && n > 64) return fail(MR_ERR_ARGUMENT, "mr_reference_average: median of more than 64 frames");
+    const size_t npix = nu * nv;
+    if (npix == 0) return MR_OK;
+    k_average<<<div_up(npix, 256), 256, 0, as_stream(stream)>>>(frames_d, npix, static_cast<int>(n), method, out_d);
+    return check_launch("k_average");
+}
+
+mr_status mr_projection_dose(const void *in_d, int dtype, size_t nu, size_t nv, size_t nframes, const size_t *roi_h,
+                             float *dose_d, void *stream)
+{
+    if (!in_d || !dose_d || !roi_h) return fail(MR_ERR_ARGUMENT, "mr_projection_dose: null pointer");
+    if (dtype != MR_F32 && dtype != MR_U16) return fail(MR_ERR_ARGUMENT, "mr_projection_dose: dtype must be f32 or u16");
+    if (nframes == 0) return MR_OK;
+    cudaStream_t s = as_stream(stream);
+    if ((roi_h[0] * roi_h[1] * roi_h[2] * roi_h[3]) == 0) {
+        k_fill<<<div_up(nframes, 256), 256, 0, s>>>(dose_d, nframes, 1.0f);
+        return check_launch("k_fill");
+    }
+    if (roi_h[2] <= roi_h[0] || roi_h[3] <= roi_h[1] || roi_h[2] > nu || roi_h[3] > nv)
+        return fail(MR_ERR_ARGUMENT, "mr_projection_dose: ROI outside the projection");
+    const size_t w = roi_h[2] - roi_h[0], h = roi_h[3] - roi_h[1];
+    if (h > 8192) return fail(MR_ERR_ARGUMENT, "mr_projection_dose: ROI taller than 8192 rows");
+    float *means = nullptr;
+    MR_CUDA_TRY(cudaMallocAsync(&means, nframes * h * sizeof(float), s));
+    dim3 g(div_up(h, 128), static_cast<unsigned>(nframes));
+    if (dtype == MR_F32)
+        k_row_means<float><<<g, 128, 0, s>>>(static_cast<const float *>(in_d), nu, nv, nframes, roi_h[0], roi_h[1], w, h,
+                                             means);
+    else
+        k_row_means<uint16_t><<<g, 128, 0, s>>>(static_cast<const uint16_t *>(in_d), nu, nv, nframes, roi_h[0],
+                                                roi_h[1], w, h, means);
+    mr_status st = check_launch("k_row_means");
+    if (st == MR_OK) {
+        unsigned p2 = 1;
+        while (p2 < h) p2 <<= 1;
+        k_median<<<static_cast<unsigned>(nframes), 256, p2 * sizeof(float), s>>>(means, h, p2, dose_d);
+        st = check_launch("k_median");
+    }
+    cudaFreeAsync(means, s);
+    return st;
+}
+
+mr_status mr_lognorm_logflat(const float *dark_d, const float *flat_d, size_t npix, int ndc, float flatdose,
+                             float *logflat_d, void *stream)
+{
+    if (!flat_d || !logflat_d || (ndc && !dark_d)) return fail(MR_ERR_ARGUMENT, "mr_lognorm_logflat: null pointer");
+    const float dose = 1.0f / flatdose; // host division, as the reference (NormPlugins.cpp:306)
+    if (dose != dose) return fail(MR_ERR_ARGUMENT, "The reference dose is a NaN");
+    if (std::isinf(dose)) return fail(MR_ERR_ARGUMENT, "The reference dose is Inf");
+    if (npix == 0) return MR_OK;
+    k_logflat<<<div_up(npix, 256), 256, 0, as_stream(stream)>>>(dark_d, flat_d, npix, ndc, dose, logflat_d);
+    return check_launch("k_logflat");
+}
+
+mr_status mr_lognorm_doselog(const float *dose_h, size_t n, float darkdose, float *doselog_h)
+{
+    if ((!dose_h || !doselog_h) && n) return fail(MR_ERR_ARGUMENT, "mr_lognorm_doselog: null pointer");
+    for (size_t i = 0; i < n; ++i) {
+        float d = dose_h[i] - darkdose;
+        doselog_h[i] = std::log(d < 1 ? 1.0f : d); // float overload, as the reference
+    }
+    return MR_OK;
+}
+
+mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t nproj, const float *dark_d,
+                           const float *logflat_d, const float *doselog_d, size_t ndose, int ndc, int nob,
+                           float *out_d, void *stream)
+{
+    if (!in_d || !out_d || !doselog_d || (ndc && !dark_d) || (nob && !logflat_d))
+        return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply: null pointer");
+    if (in_dtype != MR_U16 && in_dtype != MR_F32) return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply: input must be u16 or f32");
+    if (ndose != 1 && ndose != nproj) return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply: ndose must be 1 or nproj");
+    if (nproj > 65535) return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply: more than 65535 projections per call");
+    if (npix == 0 || nproj == 0) return MR_OK;
+    const unsigned gx = std::min<unsigned>(div_up(npix / 4 + 1, 256), 64u);
+    // 16-byte vector path when every row start is 16-byte aligned
+    const uintptr_t align = reinterpret_cast<uintptr_t>(in_d) | reinterpret_cast<uintptr_t>(out_d) |
+                            reinterpret_cast<uintptr_t>(dark_d) | reinterpret_cast<uintptr_t>(logflat_d);
+    const int vec = (npix % 4 == 0) && (align % 16 == 0);
+    dim3 g(gx, static_cast<unsigned>(nproj));
+    if (in_dtype == MR_U16)
+        k_lognorm<uint16_t><<<g, 256, 0, as_stream(stream)>>>(static_cast<const uint16_t *>(in_d), npix, dark_d,
+                                                              logflat_d, doselog_d, ndose, ndc, nob, vec, out_d);
+    else
+        k_lognorm<float><<<g, 256, 0, as_stream(stream)>>>(static_cast<const float *>(in_d), npix, dark_d, logflat_d,
+                                                           doselog_d, ndose, ndc, nob, vec, out_d);
+    return check_launch("k_lognorm");
+}
+
+} // extern "C"

@@ -1,0 +1,553 @@
+"""MuhRec preprocessing and backprojector modules on the mrcuda kernels.
+
+Each class mirrors a reference module of the tomography framework: the same class name,
+the same ``Configure(config, parameters)`` parameter names and meanings, the same
+``SetROI``/``Process`` call sequence that ``ReconEngine::Process3D`` / ``BackProject3D``
+drive (frameworks/tomography/Framework/ReconFramework/src/ReconEngine.cpp:1314-1714), and
+the same exceptions for bad input (``ReconException`` here). Data are torch tensors on a
+CUDA device; projections have the kipl ``TImage<float,3>`` layout ``(nproj, nv, nu)``.
+Every computation runs in ``libmrcuda.so``; there is no CPU path.
+
+Modules added beside the reference ones accept two extra parameters:
+``precision`` (``fp32`` | ``bf16`` | ``fp16``: storage of filtered projections in the
+backprojectors) and ``referencecompat`` (``true`` reproduces the reference's buffer rule of
+MultiProjectionBPparallel, which skips the last projection of every full buffer).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._lib import check
+
+
+class ReconException(RuntimeError):
+    """Mirror of ReconException (frameworks/tomography/Framework/ReconFramework/include/ReconException.h)."""
+
+
+# ---------------------------------------------------------------------------- config
+
+
+@dataclass
+class ProjectionInfo:
+    """Subset of ReconConfig::cProjections (ReconConfig.h:77-175) read by the hot path."""
+
+    nDims: tuple = (0, 0, 0)
+    fResolution: tuple = (0.1, 0.1)
+    fCenter: float = 0.0
+    fSOD: float = 100.0
+    fSDD: float = 100.0
+    fpPoint: tuple = (0.0, 0.0)
+    fTiltAngle: float = 0.0
+    fTiltPivotPosition: float = 0.0
+    bCorrectTilt: bool = False
+    nOBCount: int = 0
+    nDCCount: int = 0
+    roi: tuple = (0, 0, 0, 0)
+    projection_roi: tuple = (0, 0, 0, 0)
+    dose_roi: tuple = (0, 0, 0, 0)
+    eDirection: int = 0  # kipl::base::RotationDirCW = 0, RotationDirCCW = 1
+
+
+@dataclass
+class MatrixInfo:
+    """Subset of ReconConfig::cMatrix (ReconConfig.h:177-200)."""
+
+    nDims: tuple = (0, 0, 0)
+    fVoxelSize: tuple = (0.1, 0.1, 0.1)
+    bUseROI: bool = False
+
+
+@dataclass
+class ReconConfig:
+    ProjectionInfo: ProjectionInfo = field(default_factory=ProjectionInfo)
+    MatrixInfo: MatrixInfo = field(default_factory=MatrixInfo)
+
+
+def _string2bool(s: str) -> bool:
+    v = str(s).strip().lower()
+    if v in ("true", "1", "yes", "on"):
+        return True
+    if v in ("false", "0", "no", "off"):
+        return False
+    raise ReconException(f"Could not convert {s!r} to bool")
+
+
+def _get(parameters: dict, name: str) -> str:
+    # ModuleConfig GetStringParameter (core/modules/ModuleConfig/src/ParameterHandling.cpp:25-40)
+    if name not in parameters:
+        raise ReconException(f"The parameter {name} was not found in the parameter list")
+    return str(parameters[name])
+
+
+def _float_vector(text: str, n: int) -> np.ndarray:
+    """GetFloatParameterVector (ParameterHandling.cpp:55-77): n values from a space separated list."""
+    vals = np.array(str(text).split(), dtype=np.float32)
+    if vals.size < n:
+        raise ReconException(f"Parameter list has {vals.size} values, {n} needed")
+    return vals[:n]
+
+
+def _stream() -> int:
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _ptr(t: torch.Tensor | None) -> int | None:
+    return None if t is None else t.data_ptr()
+
+
+def _require_cuda(t: torch.Tensor, what: str) -> None:
+    if not isinstance(t, torch.Tensor) or not t.is_cuda:
+        raise ReconException(f"{what} must be a CUDA tensor")
+    if not t.is_contiguous():
+        raise ReconException(f"{what} must be contiguous")
+
+
+_DT = {torch.float32: L.MR_F32, torch.uint16: L.MR_U16}
+_PRECISION = {"fp32": L.MR_F32, "bf16": L.MR_BF16, "fp16": L.MR_F16}
+_AVERAGE = {"imagesum": 0, "imageaverage": 1, "imagemedian": 2, "imageweightedaverage": 3, "imagemin": 4,
+            "imagemax": 5}
+
+
+# ------------------------------------------------------------------------ FullLogNorm
+
+
+class FullLogNorm:
+    """FullLogNorm (frameworks/tomography/Preprocessing/StdPreprocModules/src/NormPlugins.cpp:243-552).
+
+    Reference frames are given in memory (``SetReferenceImages(darks, flats)``) instead of
+    read from files by ``LoadReferenceImages``; their doses follow ``ReferenceLoader``
+    (NormPlugins.cpp:91-230)."""
+
+    def __init__(self):
+        self.bUseNormROI = True
+        self.bUseLUT = False
+        self.referenceaverage = "ImageWeightedAverage"
+        self.nOBCount = self.nDCCount = 0
+        self.dose_roi = (0, 0, 0, 0)
+        self.fDarkDose = 0.0
+        self.fFlatDose = 1.0
+        self.mDark = None
+        self.mFlatField = None  # log of the flat field after SetReferenceImages
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        pi = config.ProjectionInfo
+        self.nOBCount, self.nDCCount = int(pi.nOBCount), int(pi.nDCCount)
+        self.bUseNormROI = _string2bool(_get(parameters, "usenormregion"))
+        self.bUseLUT = _string2bool(parameters.get("uselut", "false"))
+        if self.bUseLUT:
+            raise ReconException("FullLogNorm: uselut=true is not supported by this module")
+        self.referenceaverage = _get(parameters, "referenceaverage")
+        if self.referenceaverage.lower() not in _AVERAGE:
+            raise ReconException(f"Unknown reference average method {self.referenceaverage}")
+        self.dose_roi = tuple(int(v) for v in pi.dose_roi)
+        return 0
+
+    def GetParameters(self) -> dict:
+        return {"usenormregion": "true" if self.bUseNormROI else "false", "uselut": "false",
+                "referenceaverage": self.referenceaverage}
+
+    def _frame_doses(self, frames: torch.Tensor) -> np.ndarray:
+        n, nv, nu = frames.shape
+        out = torch.empty(n, dtype=torch.float32, device=frames.device)
+        roi = (ctypes.c_size_t * 4)(*self.dose_roi)
+        check(L.lib().mr_projection_dose(frames.data_ptr(), _DT[frames.dtype], nu, nv, n, roi, out.data_ptr(),
+                                         _stream()))
+        return out.cpu().numpy()
+
+    def _average(self, frames: torch.Tensor) -> torch.Tensor:
+        n, nv, nu = frames.shape
+        m = _AVERAGE[self.referenceaverage.lower()]
+        if m == 3:
+            raise ReconException("ImageWeightedAverage is not supported by this module; use ImageAverage")
+        out = torch.empty((nv, nu), dtype=torch.float32, device=frames.device)
+        check(L.lib().mr_reference_average(frames.data_ptr(), nu, nv, n, m, out.data_ptr(), _stream()))
+        return out
+
+    def SetReferenceImages(self, darks: torch.Tensor, flats: torch.Tensor) -> None:
+        """Average the reference frames, compute their doses, store dark and log(flat)."""
+        for t, w in ((darks, "dark frames"), (flats, "flat frames")):
+            _require_cuda(t, w)
+        darks = darks.float() if darks.dtype != torch.float32 else darks
+        flats = flats.float() if flats.dtype != torch.float32 else flats
+        nd, nf = darks.shape[0], flats.shape[0]
+        self.nDCCount, self.nOBCount = nd, nf
+        f32 = np.float32
+        darkdose = f32(0.0)
+        if nd:
+            doses = self._frame_doses(darks) if self.bUseNormROI else np.zeros(nd, np.float32)
+            acc = f32(0.0)
+            for i in range(nd):
+                acc = doses[i] if i == 0 else f32(acc + doses[i])
+            darkdose = f32(acc / f32(nd))
+            self.mDark = self._average(darks)
+        else:
+            self.mDark = torch.zeros(flats.shape[1:], dtype=torch.float32, device=flats.device)
+        flatdose = f32(1.0)
+        if nf:
+            doses = self._frame_doses(flats) if self.bUseNormROI else np.ones(nf, np.float32)
+            acc = f32(0.0)
+            for i in range(nf):
+                t = f32(doses[i] - darkdose)
+                acc = t if i == 0 else f32(acc + t)
+            flatdose = f32(acc / f32(nf))
+            flat = self._average(flats)
+        else:
+            raise ReconException("FullLogNorm needs flat field images")
+        self.fDarkDose, self.fFlatDose = float(darkdose), float(flatdose)
+        self.mFlatField = torch.empty_like(flat)
+        check(L.lib().mr_lognorm_logflat(self.mDark.data_ptr(), flat.data_ptr(), flat.numel(), int(nd > 0),
+                                         float(flatdose), self.mFlatField.data_ptr(), _stream()))
+
+    def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
+        return self.ProcessCore(img, coeff if coeff is not None else {})
+
+    def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
+        """ProcessCore 3D. ``img`` is float32 or uint16 (raw counts); returns float32.
+        Doses come from ``coeff['dose']`` (text, as the engine passes them) or, when absent,
+        are computed on the device over the dose ROI (ProjectionReader::GetProjectionDose)."""
+        _require_cuda(img, "projections")
+        if self.mFlatField is None:
+            raise ReconException("FullLogNorm: reference images are not set")
+        nproj, nv, nu = img.shape
+        if self.mFlatField.numel() != nv * nu:
+            raise ReconException(f"Flat field ({self.mFlatField.shape[1]}, {self.mFlatField.shape[0]}), does not match "
+                                 f"projection ({nu}, {nv})")
+        if self.bUseNormROI:
+            doses = (_float_vector(coeff["dose"], nproj) if "dose" in coeff else self._frame_doses(img))
+            doses = np.ascontiguousarray(doses, np.float32)
+            dl = np.empty_like(doses)
+            check(L.lib().mr_lognorm_doselog(doses.ctypes.data_as(L.P_float), nproj, self.fDarkDose,
+                                             dl.ctypes.data_as(L.P_float)))
+        else:
+            dl = np.zeros(1, np.float32)
+        doselog = torch.from_numpy(dl).to(img.device)
+        out = img if img.dtype == torch.float32 else torch.empty(img.shape, dtype=torch.float32, device=img.device)
+        check(L.lib().mr_lognorm_apply(img.data_ptr(), _DT[img.dtype], nv * nu, nproj, self.mDark.data_ptr(),
+                                       self.mFlatField.data_ptr(), doselog.data_ptr(), doselog.numel(),
+                                       int(self.nDCCount > 0), int(self.nOBCount > 0), out.data_ptr(), _stream()))
+        return out
+
+
+# ------------------------------------------------------------ ProjectionFilterSingle
+
+
+class ProjectionFilterSingle:
+    """ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:230-376)."""
+
+    def __init__(self):
+        self.m_FilterType = "Hamming"
+        self.m_fCutOff = 0.5
+        self.m_fOrder = 1.0
+        self.m_bUseBias = True
+        self.m_fBiasWeight = 0.1
+        self.m_nPaddingDoubler = 2
+        self._plan = None
+        self.nImageSize = 0
+
+    def __del__(self):
+        if getattr(self, "_plan", None):
+            L.lib().mr_projfilter_destroy(self._plan)
+            self._plan = None
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        roi = config.ProjectionInfo.roi
+        n = int(roi[2]) - int(roi[0])
+        self.m_FilterType = _get(parameters, "filtertype")
+        self.m_fCutOff = float(np.float32(_get(parameters, "cutoff")))
+        self.m_fOrder = float(np.float32(_get(parameters, "order")))
+        self.m_bUseBias = _string2bool(_get(parameters, "usebias"))
+        self.m_fBiasWeight = float(np.float32(_get(parameters, "biasweight")))
+        self.m_nPaddingDoubler = int(_get(parameters, "paddingdoubler"))
+        self.nImageSize = n
+        self.BuildFilter(n)
+        return 0
+
+    def BuildFilter(self, n: int) -> None:
+        if self._plan:
+            L.lib().mr_projfilter_destroy(self._plan)
+            self._plan = None
+        plan = ctypes.c_void_p()
+        st = L.lib().mr_projfilter_create(n, self.m_FilterType.encode(), self.m_fCutOff, self.m_fOrder,
+                                          int(self.m_bUseBias), self.m_fBiasWeight, self.m_nPaddingDoubler,
+                                          ctypes.byref(plan))
+        if st != L.MR_OK:
+            raise ReconException(L.lib().mr_last_error().decode())
+        self._plan = plan
+
+    def GetParameters(self) -> dict:
+        return {"filtertype": self.m_FilterType, "cutoff": str(self.m_fCutOff), "order": str(self.m_fOrder),
+                "usebias": "true" if self.m_bUseBias else "false", "biasweight": str(self.m_fBiasWeight),
+                "paddingdoubler": str(self.m_nPaddingDoubler)}
+
+    def filter_tables(self):
+        nfft, ins = ctypes.c_size_t(), ctypes.c_size_t()
+        check(L.lib().mr_projfilter_info(self._plan, ctypes.byref(nfft), ctypes.byref(ins), None, None))
+        f = np.zeros(nfft.value // 2, np.float32)
+        p = np.zeros(max(ins.value, 1), np.float32)
+        check(L.lib().mr_projfilter_info(self._plan, None, None, f.ctypes.data_as(L.P_float),
+                                         p.ctypes.data_as(L.P_float)))
+        return nfft.value, ins.value, f, p[: ins.value]
+
+    def Process(self, img: torch.Tensor, coeff: dict | None = None, weights: torch.Tensor | None = None) -> torch.Tensor:
+        return self.ProcessCore(img, coeff if coeff is not None else {}, weights)
+
+    def ProcessCore(self, img: torch.Tensor, coeff: dict, weights: torch.Tensor | None = None) -> torch.Tensor:
+        """Filters every detector row in place. ``weights`` (optional, one per projection)
+        fuses the backprojector's projection weighting into the output."""
+        if img.numel() == 0:
+            raise ReconException("Empty projection image")
+        _require_cuda(img, "projections")
+        if img.dtype != torch.float32:
+            raise ReconException("ProjectionFilterSingle expects float32 projections")
+        nproj, nv, nu = img.shape
+        if nu != self.nImageSize:
+            raise ReconException(f"Projection width {nu} does not match the configured ROI width {self.nImageSize}")
+        if weights is not None:
+            _require_cuda(weights, "weights")
+        check(L.lib().mr_projfilter_apply(self._plan, img.data_ptr(), img.data_ptr(), nproj * nv, _ptr(weights), nv,
+                                          _stream()))
+        return img
+
+
+# --------------------------------------------------------------- backprojector base
+
+
+class _BackProjectorBase:
+    def __init__(self, name: str):
+        self.m_sModuleName = name
+        self.mConfig = ReconConfig()
+        self.nProjectionBufferSize = 16
+        self.nSliceBlock = 32
+        self.nSubVolume = (1, 1)
+        self.precision = "fp32"
+        self.referencecompat = True
+        self.volume = None
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        self.mConfig = config
+        self.nProjectionBufferSize = int(_get(parameters, "ProjectionBufferSize"))
+        self.nSliceBlock = int(_get(parameters, "SliceBlock"))
+        sv = str(_get(parameters, "SubVolume")).split()
+        self.nSubVolume = tuple(int(v) for v in sv[:2])
+        self.precision = str(parameters.get("precision", "fp32")).lower()
+        if self.precision not in _PRECISION:
+            raise ReconException(f"Unknown precision {self.precision}")
+        self.referencecompat = _string2bool(parameters.get("referencecompat", "true"))
+        return 0
+
+    def Initialize(self) -> int:
+        return 0
+
+    def GetParameters(self) -> dict:
+        return {"ProjectionBufferSize": str(self.nProjectionBufferSize), "SliceBlock": str(self.nSliceBlock),
+                "SubVolume": f"{self.nSubVolume[0]} {self.nSubVolume[1]}", "precision": self.precision,
+                "referencecompat": "true" if self.referencecompat else "false"}
+
+    def GetVolume(self) -> torch.Tensor:
+        return self.volume
+
+
+class MultiProjectionBPparallel(_BackProjectorBase):
+    """MultiProjectionBPparallel (StdBackProjectors/src/MultiProjBPparallel.cpp) with the
+    StdBackProjectorBase driver (StdBackProjectorBase.cpp). Volume is MatrixZXY:
+    tensor (ny, nx, nz) = (nu, nu, nv), z fastest."""
+
+    def __init__(self):
+        super().__init__("Multi projection BP parallel")
+        self.SizeU = self.SizeV = 0
+        self._mask = None
+        self._roi = (0, 0, 0, 0)
+
+    def SetROI(self, roi) -> None:
+        pi = self.mConfig.ProjectionInfo
+        self._roi = tuple(int(v) for v in roi)
+        self.SizeU = self._roi[2] - self._roi[0]
+        self.SizeV = self._roi[3] - self._roi[1]
+        if self.SizeU < 2:
+            raise ReconException("The projection ROI is too narrow")
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.volume = torch.zeros((self.SizeU, self.SizeU, self.SizeV), dtype=torch.float32, device=dev)
+        mask = np.zeros(2 * self.SizeU, np.uint32)
+        nslices = int(pi.nDims[1]) if pi.nDims[1] else self.SizeV
+        check(L.lib().mr_bp_circle_mask(self.SizeU, self.SizeU, int(pi.bCorrectTilt), float(pi.fTiltAngle), nslices,
+                                        mask.ctypes.data_as(L.P_u32)))
+        self.mask_host = mask
+        self._mask = torch.from_numpy(mask.view(np.int32)).to(dev)
+
+    def used_projections(self, nproj: int) -> np.ndarray:
+        """Indices the reference backprojects: StdBackProjectorBase::Process 2D flushes a full
+        buffer without its last entry (StdBackProjectorBase.cpp:104-113)."""
+        k = np.arange(nproj)
+        if not self.referencecompat:
+            return k
+        b = self.nProjectionBufferSize
+        return k[(k % b) != (b - 1)]
+
+    def Process(self, projections: torch.Tensor, parameters: dict, prefiltered_weights: bool = False) -> int:
+        """Backprojects projections (nproj, nv, nu) with ``parameters['angles']`` and
+        ``parameters['weights']`` (space separated text, as ReconEngine passes them).
+        ``prefiltered_weights`` marks projections already multiplied by their weights
+        (the fused filter path); the weights are then not applied again."""
+        if self.volume is None:
+            raise ReconException("The target matrix is not allocated.")
+        _require_cuda(projections, "projections")
+        nproj, nv, nu = projections.shape
+        if nu != self.SizeU or nv != self.SizeV:
+            raise ReconException(f"Projection size ({nu}, {nv}) does not match the ROI ({self.SizeU}, {self.SizeV})")
+        weights = _float_vector(_get(parameters, "weights"), nproj)
+        angles = _float_vector(_get(parameters, "angles"), nproj)
+        pi = self.mConfig.ProjectionInfo
+        sel = self.used_projections(nproj)
+        if sel.size == 0:
+            return 0
+        ang = np.ascontiguousarray(angles[sel])
+        s = np.empty_like(ang)
+        c = np.empty_like(ang)
+        su = np.empty_like(ang)
+        check(L.lib().mr_bp_parallel_geometry(ang.ctypes.data_as(L.P_float), ang.size, self.SizeU, float(pi.fCenter),
+                                              int(pi.eDirection), s.ctypes.data_as(L.P_float),
+                                              c.ctypes.data_as(L.P_float), su.ctypes.data_as(L.P_float)))
+        toff, tinc = ctypes.c_float(0), ctypes.c_float(0)
+        if pi.bCorrectTilt:
+            check(L.lib().mr_bp_parallel_tilt(float(pi.fTiltAngle), float(pi.fTiltPivotPosition), self._roi[1],
+                                              ctypes.byref(toff), ctypes.byref(tinc)))
+        dev = projections.device
+        geo = torch.from_numpy(np.stack([s, c, su, weights[sel]])).to(dev)
+        idx = torch.from_numpy(sel.astype(np.int32)).to(dev)
+        proj = projections
+        dtype = _PRECISION[self.precision]
+        scale = None
+        if dtype != L.MR_F32:
+            proj, scale = quantize(projections, self.precision)
+        check(L.lib().mr_bp_parallel(proj.data_ptr(), dtype, _ptr(scale),
+                                     None if prefiltered_weights else geo[3].data_ptr(), idx.data_ptr(), geo[0].data_ptr(),
+                                     geo[1].data_ptr(), geo[2].data_ptr(), sel.size, self.SizeU, self.SizeV,
+                                     self._mask.data_ptr(), int(pi.bCorrectTilt), toff.value, tinc.value,
+                                     self.volume.data_ptr(), _stream()))
+        return 0
+
+    def GetSlice(self, idx: int) -> torch.Tensor:
+        """BackProjectorModuleBase::GetSlice for MatrixZXY: slice[y][x] = volume[y][x][idx]."""
+        if idx >= self.volume.shape[2]:
+            raise ReconException("Slice index greater than matrix size (ZXY matrix)")
+        return self.volume[:, :, idx]
+
+    def GetNSlices(self) -> int:
+        return self.volume.shape[2]
+
+
+class FDKbp_single(_BackProjectorBase):
+    """FDKbp_single (FDKBackProjectors/src/fdkbp_single.cpp) with the FdkReconBase driver
+    (fdkreconbase.cpp). Volume is MatrixXYZ: tensor (nz, ny, nx) = (nv, nu, nu), x fastest."""
+
+    def __init__(self):
+        super().__init__("FDKbp_single")
+        self._first = True
+
+    def SetROI(self, roi) -> None:
+        self._roi = tuple(int(v) for v in roi)
+        if self._roi[0] != 0 or self._roi[1] != 0:
+            raise ReconException("FDKbp_single: only a full-detector ROI starting at (0, 0) is supported")
+        self.SizeU = self._roi[2] - self._roi[0]
+        self.SizeV = self._roi[3] - self._roi[1]
+        pi = self.mConfig.ProjectionInfo
+        dev = torch.device("cuda", torch.cuda.current_device())
+        self.volume = torch.zeros((self.SizeV, self.SizeU, self.SizeU), dtype=torch.float32, device=dev)
+        mask = np.zeros(2 * self.SizeU, np.uint32)
+        nslices = int(pi.nDims[1]) if pi.nDims[1] else self.SizeV
+        check(L.lib().mr_bp_circle_mask(self.SizeU, self.SizeU, int(pi.bCorrectTilt), float(pi.fTiltAngle), nslices,
+                                        mask.ctypes.data_as(L.P_u32)))
+        self._mask = torch.from_numpy(mask.view(np.int32)).to(dev)
+        self._first = True
+        self._geo_key = None
+
+    def geometry(self) -> L.FdkGeom:
+        pi, mi = self.mConfig.ProjectionInfo, self.mConfig.MatrixInfo
+        g = L.FdkGeom()
+        g.sod, g.sdd = pi.fSOD, pi.fSDD
+        g.ppoint[0], g.ppoint[1] = pi.fpPoint
+        g.center = pi.fCenter
+        g.resolution[0], g.resolution[1] = pi.fResolution
+        g.voxelsize[0], g.voxelsize[1], g.voxelsize[2] = mi.fVoxelSize
+        g.direction = int(pi.eDirection)
+        g.correcttilt = int(pi.bCorrectTilt)
+        g.tiltangle = pi.fTiltAngle
+        g.tiltpivot = pi.fTiltPivotPosition
+        return g
+
+    def partials(self, angles: np.ndarray):
+        nu, nv, n = self.SizeU, self.SizeV, angles.size
+        xip = np.empty((n, nu, 3), np.float32)
+        yip = np.empty((n, nu, 3), np.float32)
+        zip_ = np.empty((n, nv, 3), np.float32)
+        s2, sc, uni = ctypes.c_float(), ctypes.c_float(), ctypes.c_int()
+        g = self.geometry()
+        a = np.ascontiguousarray(angles, np.float32)
+        check(L.lib().mr_fdk_partials(ctypes.byref(g), nu, nv, a.ctypes.data_as(L.P_float), n,
+                                      xip.ctypes.data_as(L.P_float), yip.ctypes.data_as(L.P_float),
+                                      zip_.ctypes.data_as(L.P_float), ctypes.byref(s2), ctypes.byref(sc),
+                                      ctypes.byref(uni)))
+        return xip, yip, zip_, s2.value, sc.value, uni.value
+
+    def Process(self, projections: torch.Tensor, parameters: dict) -> int:
+        if self.volume is None:
+            raise ReconException("The target matrix is not allocated.")
+        _require_cuda(projections, "projections")
+        if projections.dtype != torch.float32:
+            raise ReconException("FDKbp_single expects float32 projections")
+        nproj, nv, nu = projections.shape
+        if nu != self.SizeU or nv != self.SizeV:
+            raise ReconException(f"Projection size ({nu}, {nv}) does not match the ROI ({self.SizeU}, {self.SizeV})")
+        weights = _float_vector(_get(parameters, "weights"), nproj)
+        angles = _float_vector(_get(parameters, "angles"), nproj)
+        dev = projections.device
+        # per-projection geometry depends only on the configuration and the angles: keep the
+        # device copies while they stay the same
+        key = (angles.tobytes(), weights.tobytes(), str(dev))
+        if getattr(self, "_geo_key", None) != key:
+            xip, yip, zip_, s2, sc, uni = self.partials(angles)
+            self._geo = (torch.from_numpy(weights).to(dev), *(torch.from_numpy(a).to(dev) for a in (xip, yip, zip_)),
+                         s2, sc, uni)
+            self._geo_key = key
+        w, X, Y, Z, s2, sc, uni = self._geo
+        dtype = _PRECISION[self.precision]
+        if dtype == L.MR_F32:
+            filt = torch.empty_like(projections)
+            scale = None
+        else:
+            filt = torch.empty(projections.shape, dtype=torch.uint16, device=dev)
+            scale = torch.empty(nproj, dtype=torch.float32, device=dev)
+        st = _stream()
+        check(L.lib().mr_fdk_filter(projections.data_ptr(), nu, nv, nproj, w.data_ptr(), s2, sc, dtype, filt.data_ptr(),
+                                    _ptr(scale), st))
+        check(L.lib().mr_fdk_backproject(filt.data_ptr(), dtype, _ptr(scale), nu, nv, nproj, X.data_ptr(), Y.data_ptr(),
+                                         Z.data_ptr(), uni, self._mask.data_ptr(), int(not self._first),
+                                         self.volume.data_ptr(), st))
+        self._first = False
+        return 0
+
+    def GetSlice(self, idx: int) -> torch.Tensor:
+        if idx >= self.volume.shape[0]:
+            raise ReconException("Slice index greater than matrix size (XYZ matrix)")
+        return self.volume[idx]
+
+    def GetNSlices(self) -> int:
+        return self.volume.shape[0]
+
+
+def quantize(proj: torch.Tensor, precision: str):
+    """Per-projection power-of-two scaled 16-bit copy (mr_quantize) of float projections
+    (nproj, nv, nu). Returns (bits as uint16 tensor, scales)."""
+    _require_cuda(proj, "projections")
+    nproj = proj.shape[0]
+    per = proj[0].numel()
+    out = torch.empty(proj.shape, dtype=torch.uint16, device=proj.device)
+    scale = torch.empty(nproj, dtype=torch.float32, device=proj.device)
+    check(L.lib().mr_quantize(proj.data_ptr(), per, nproj, _PRECISION[precision], out.data_ptr(), scale.data_ptr(),
+                              _stream()))
+    return out, scale

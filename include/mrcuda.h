@@ -1,0 +1,197 @@
+/* mrcuda: B200 (sm_100a) kernels for the MuhRec reconstruction hot path, behind a C ABI.
+ *
+ * Every entry point takes plain pointers and sizes. Pointers named *_d are device
+ * pointers (cudaMalloc'd or otherwise device-accessible); *_h are host pointers.
+ * `stream` is a cudaStream_t passed as void* (NULL = the legacy default stream).
+ * Calls are asynchronous on `stream` unless stated otherwise; argument errors are
+ * reported before anything is launched. Every call returns an mr_status; MR_OK is 0.
+ * On failure, mr_last_error() returns a message for the calling thread.
+ *
+ * Array layouts follow kipl::base::TImage (first index fastest):
+ *   projections  [nproj][nv][nu]   u (detector column) fastest
+ *   parallel-beam volume (MatrixZXY) [ny][nx][nz]  z fastest, nx = ny = nu, nz = nv
+ *   FDK volume (MatrixXYZ)           [nz][ny][nx]  x fastest, nx = ny = nu, nz = nv
+ *
+ * Reference interfaces each group replaces are cited as file:line, relative to the
+ * reference project root (DTasev/imagingsuite).
+ */
+#ifndef MRCUDA_H
+#define MRCUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int mr_status;
+enum {
+    MR_OK = 0,
+    MR_ERR_ARGUMENT = 1,    /* invalid size, pointer or parameter (nothing launched) */
+    MR_ERR_CUDA = 2,        /* a CUDA runtime call failed */
+    MR_ERR_ALLOCATION = 3,  /* device or host allocation failed */
+    MR_ERR_UNSUPPORTED = 4, /* valid request this build does not implement */
+    MR_ERR_DEVICE = 5       /* a kernel reported an error status (bounded wait expired, ...) */
+};
+
+/* Library version (major*10000 + minor*100 + patch) and status text. */
+int mr_version(void);
+const char *mr_status_string(mr_status s);
+const char *mr_last_error(void);
+
+/* Precision of stored projections. MR_F32 is the reference arithmetic; MR_BF16 and
+ * MR_F16 store filtered projections in 16 bits with a per-projection power-of-two
+ * scale and accumulate in FP32. */
+enum { MR_F32 = 0, MR_BF16 = 1, MR_F16 = 2 };
+
+/* ---------------------------------------------------------------------------------
+ * Reference frames and doses (FullLogNorm preparation)
+ * replaces ImagingAlgorithms::AverageImage::operator()
+ *   (core/algorithms/ImagingAlgorithms/src/averageimage.cpp:35-61) and
+ *   ProjectionReader::GetProjectionDose (frameworks/tomography/Framework/ReconFramework/
+ *   src/ProjectionReader.cpp:752-783).
+ * method: 0 ImageSum, 1 ImageAverage, 2 ImageMedian, 4 ImageMin, 5 ImageMax
+ * (averageimage.h:16-23). frames_d: [n][nv][nu] float. */
+mr_status mr_reference_average(const float *frames_d, size_t nu, size_t nv, size_t n, int method, float *out_d,
+                               void *stream);
+/* Dose of each frame: median over the rows of roi (x0,y0,x1,y1) of the row means.
+ * in_d holds nframes frames of nu x nv, as float (dtype MR_F32) or uint16 (dtype 3).
+ * A ROI with any zero coordinate gives 1.0 like the reference. */
+enum { MR_U16 = 3 };
+mr_status mr_projection_dose(const void *in_d, int dtype, size_t nu, size_t nv, size_t nframes, const size_t *roi_h,
+                             float *dose_d, void *stream);
+
+/* ---------------------------------------------------------------------------------
+ * FullLogNorm (frameworks/tomography/Preprocessing/StdPreprocModules/src/NormPlugins.cpp)
+ * mr_lognorm_logflat replaces FullLogNorm::SetReferenceImages (:300-341):
+ *     logflat = (F - D <= 0) ? 0 : log((F - D) / flatdose)     (ndc = 0: F alone)
+ * mr_lognorm_doselog replaces the dose list of ProcessCore 3D (:416-425), on the host:
+ *     doselog[j] = log(max(dose[j] - darkdose, 1))
+ * mr_lognorm_apply replaces ProcessCore 3D (:481-549), non-LUT path:
+ *     p = (I - D <= 0) ? 0 : logflat - log(I - D) + doselog[j]   (nob = 0: -log(I-D)+doselog)
+ * in_d: [nproj][npix] of uint16 (in_dtype MR_U16) or float (MR_F32; may alias out_d).
+ * ndose: 1 (one value for all projections) or nproj. */
+mr_status mr_lognorm_logflat(const float *dark_d, const float *flat_d, size_t npix, int ndc, float flatdose,
+                             float *logflat_d, void *stream);
+mr_status mr_lognorm_doselog(const float *dose_h, size_t n, float darkdose, float *doselog_h);
+mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t nproj, const float *dark_d,
+                           const float *logflat_d, const float *doselog_d, size_t ndose, int ndc, int nob,
+                           float *out_d, void *stream);
+
+/* ---------------------------------------------------------------------------------
+ * ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:78-376)
+ * Plan = ProjectionFilterBase::Configure/BuildFilter/PreparePadding (:78-93,254-299,364-376):
+ *   nfft = 2^(ceil(log2 nu) + paddingdoubler); filter over bins 0..nfft/2-1.
+ *   filtertype: "ram-lak", "shepp-logan", "hanning", "hamming", "butterworth" (any case).
+ * Apply = FilterProjection + Pad (:301-362) on nrows rows of nu floats:
+ *   sigmoid-tapered padding, r2c, bins 0..nfft/2-1 times the filter (Nyquist untouched),
+ *   c2r, times pi/(2 nfft), cropped. in_d may alias out_d.
+ * row_weight_d (optional, may be NULL): one factor per group of rows_per_weight rows,
+ *   multiplied into the output after the reference's scale (the backprojector weighting
+ *   of StdBackProjectorBase::Process, StdBackProjectorBase.cpp:80, fused). */
+typedef struct mr_filter_plan mr_filter_plan;
+/* Host-only: the filter table (nfft/2 floats, filter_h may be NULL to query sizes) and the
+ * padding taper (ninsert floats) exactly as BuildFilter/PreparePadding compute them. */
+mr_status mr_projfilter_tables(size_t nu, const char *filtertype, float cutoff, float order, int usebias,
+                               float biasweight, int paddingdoubler, size_t *nfft, size_t *ninsert, float *filter_h,
+                               float *pad_h);
+mr_status mr_projfilter_create(size_t nu, const char *filtertype, float cutoff, float order, int usebias,
+                               float biasweight, int paddingdoubler, mr_filter_plan **plan);
+mr_status mr_projfilter_destroy(mr_filter_plan *plan);
+/* Copies the filter table (nfft/2 floats) and padding table (ninsert floats) to the host. */
+mr_status mr_projfilter_info(const mr_filter_plan *plan, size_t *nfft, size_t *ninsert, float *filter_h,
+                             float *pad_h);
+mr_status mr_projfilter_apply(const mr_filter_plan *plan, const float *in_d, float *out_d, size_t nrows,
+                              const float *row_weight_d, size_t rows_per_weight, void *stream);
+
+/* Precision form: 16-bit copy of nproj float projections of `per` values each, with a
+ * power-of-two scale per projection (value = stored * scale_d[i]; the largest magnitude
+ * maps into [2^13, 2^14) for MR_F16, into [0.5, 1) for MR_BF16). out_d holds bf16/f16 bits. */
+mr_status mr_quantize(const float *in_d, size_t per, size_t nproj, int dtype, uint16_t *out_d, float *scale_d,
+                      void *stream);
+
+/* ---------------------------------------------------------------------------------
+ * Parallel-beam backprojection: MultiProjectionBPparallel
+ * (frameworks/tomography/Backprojectors/StdBackProjectors/src/MultiProjBPparallel.cpp:39-170)
+ * with the geometry of StdBackProjectorBase::Process/SetROI
+ * (StdBackProjectorBase.cpp:64-201) and BackProjectorModuleBase::BuildCircleMask
+ * (frameworks/tomography/Framework/ReconFramework/src/BackProjectorModuleBase.cpp:153-218).
+ *
+ * mr_bp_parallel_geometry (host) fills, per projection, exactly the reference's floats:
+ *   sin_h = sin(d*angle*pi/180), cos_h likewise, startu_h = (nu/2)*(sin - cos) + center,
+ *   d = +1 for counter-clockwise (direction 1), -1 for clockwise (direction 0).
+ * mr_bp_circle_mask (host) fills mask_h[2*y], mask_h[2*y+1] = first, second of row y.
+ *
+ * mr_bp_parallel accumulates (+=) into vol_d ([nu][nu][nv], z fastest) the linear
+ * interpolation backprojection of nproj projections:
+ *   vol[z][x-1][y-1] += P_i[z][n]*(1-f) + P_i[z][n+1]*f,   u = startu_i + cos_i*y - sin_i*x,
+ *   n = (int)u in [0, nu-2], f = |u - n|, x in (first, second] of mask row y-1,
+ * projections applied in list order i = 0..nproj-1, entry i reading projection slab
+ * index_d[i] of proj_d (index_d NULL: slab i) and multiplied by weight_d[i] first
+ * (weight_d may be NULL for pre-weighted projections); sin/cos/startu are per list entry. Only z < 4*(nv/4) is updated, as in the
+ * reference. proj_d: [slabs][nv][nu] in `dtype`; for MR_BF16/MR_F16, scale_d[slab] is the
+ * per-projection scale (value = stored * scale). Tilt (correcttilt != 0) follows the
+ * reference tilt branch (:47-110) with tiltoffset = (roi_y0 - pivot)*tan(tilt) and
+ * tiltinc = 4*tan(tilt), both computed by the caller (see mr_bp_parallel_tilt).
+ * sin/cos/startu/weight/mask are device arrays (copy the host results over). */
+mr_status mr_bp_parallel_geometry(const float *angles_h, size_t nproj, size_t nu, float center, int direction,
+                                  float *sin_h, float *cos_h, float *startu_h);
+mr_status mr_bp_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, size_t nslices,
+                            uint32_t *mask_h);
+mr_status mr_bp_parallel_tilt(float tiltangle, float tiltpivot, size_t roi_y0, float *tiltoffset,
+                              float *tiltinc);
+mr_status mr_bp_parallel(const void *proj_d, int dtype, const float *scale_d, const float *weight_d,
+                         const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
+                         size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt, float tiltoffset,
+                         float tiltinc, float *vol_d, void *stream);
+
+/* ---------------------------------------------------------------------------------
+ * FDK cone-beam backprojection: FDKbp_single
+ * (frameworks/tomography/Backprojectors/FDKBackProjectors/src/fdkbp_single.cpp:83-994)
+ * driven as FdkReconBase::Process 3D (fdkreconbase.cpp:217-277).
+ *
+ * Geometry as ReconConfig fields (ReconConfig.h): source-object / source-detector
+ * distances, piercing point (detector pixels), centre of rotation, detector pitch,
+ * voxel size; direction 0 = clockwise. The detector ROI is the full projection
+ * (roi = projection_roi = {0, 0, nu, nv}) and the volume is nu x nu x nv. */
+typedef struct {
+    float sod, sdd;
+    float ppoint[2];
+    float center;
+    float resolution[2];
+    float voxelsize[3];
+    int direction;
+    int correcttilt;
+    float tiltangle;
+    float tiltpivot;
+} mr_fdk_geom;
+
+/* Per-projection partial projections (host, exact reference float arithmetic):
+ * xip [nproj][nu][3], yip [nproj][nu][3], zip [nproj][nv][3] of
+ * project_volume_onto_image_c (:293-445), and the image scale factors. *uniform_z is set
+ * to 1 when, for every projection, zip[k][0] and zip[k][2] do not depend on k (always the
+ * case without tilt correction), which lets the backprojector hoist the detector column
+ * and the distance weight out of the slice loop. */
+mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const float *angles_h, size_t nproj,
+                          float *xip_h, float *yip_h, float *zip_h, float *sad_sid_2, float *scale, int *uniform_z);
+/* Ramp filter (ramp_filter_tuned, :832-958) of nproj projections [nproj][nv][nu] with
+ * the input weighting of FdkReconBase::Process (img *= weight, :243) and the image
+ * rescale of project_volume_onto_image_c (cbi *= sad_sid_2; cbi *= scale, :380-384)
+ * fused. out_dtype MR_F32, or MR_BF16/MR_F16 with scale_out_d[nproj] written. */
+mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, const float *weight_d,
+                        float sad_sid_2, float scale, int out_dtype, void *out_d, float *scale_out_d,
+                        void *stream);
+/* Voxel-driven nearest-neighbour backprojection (:450-525) of nproj filtered
+ * projections into the final volume (after FdkReconBase's per-slice mirror and z
+ * reversal, fdkreconbase.cpp:259-270). vol_d [nv][nu][nu] is overwritten when
+ * accumulate == 0, else added to (continuing a previous batch of projections).
+ * xip/yip/zip: device copies of mr_fdk_partials. mask_d: mr_bp_circle_mask(nu, nu, ...). */
+mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
+                             size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
+                             const uint32_t *mask_d, int accumulate, float *vol_d, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MRCUDA_H */

@@ -78,7 +78,7 @@ def ref() -> ctypes.CDLL:
 
 def _check_ref(rc: int) -> None:
     if rc != 0:
-        raise RuntimeError("reference module failed: " + ref().ref_last_error().decode())
+        raise RuntimeError("reference module failed: " + ref().ref_last_error().decode(errors="replace"))
 
 
 # ----------------------------------------------------------------- averaging / dose
@@ -296,3 +296,35 @@ def fdk_projmatrix(geom: FdkGeom, nu: int, angle: float) -> np.ndarray:
     pm = np.zeros(12, np.float32)
     orc().orc_fdk_projmatrix(ctypes.byref(geom), _sz(nu), _f(angle), _p(pm))
     return pm
+
+
+def fdk_prepare(proj, weights, geom: FdkGeom) -> np.ndarray:
+    """img *= weight, ramp filter, rescale - the per-projection preparation before FDK BP."""
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    nproj, nv, nu = out.shape
+    w = _f32(weights)
+    orc().orc_fdk_prepare(_p(out), _sz(nu), _sz(nv), _sz(nproj), _p(w), ctypes.byref(geom))
+    return out
+
+
+def fdk_bp(filtered, angles, geom: FdkGeom) -> np.ndarray:
+    """FDK backprojection + final mirror of prepared projections. Returns (nv, nu, nu)."""
+    filtered = _f32(filtered)
+    nproj, nv, nu = filtered.shape
+    a = _f32(angles)
+    vol = np.zeros((nv, nu, nu), np.float32)
+    orc().orc_fdk_bp(_p(filtered), _sz(nu), _sz(nv), _sz(nproj), _p(a), ctypes.byref(geom), _p(vol))
+    return vol
+
+
+def bp_geometry(angles, nu, center, direction=0):
+    a = _f32(angles)
+    s, c, su = (np.empty_like(a) for _ in range(3))
+    orc().orc_bp_geometry(_p(a), _sz(a.size), _sz(nu), _f(center), int(direction), _p(s), _p(c), _p(su))
+    return s, c, su
+
+
+def circle_mask(nx, ny, correcttilt=False, tiltangle=0.0, nslices=0) -> np.ndarray:
+    m = np.zeros(2 * ny, np.uintp)
+    orc().orc_circle_mask(_sz(nx), _sz(ny), int(correcttilt), _f(tiltangle), _sz(nslices), _p(m, _SZ))
+    return m.astype(np.uint32)

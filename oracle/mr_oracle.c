@@ -473,8 +473,8 @@ void orc_fdk_ramp(float *img, size_t width, size_t height)
 /* FdkReconBase::Process 3D + FDKbp_single::reconstruct/project_volume_onto_image_c
  * (fdkreconbase.cpp:217-277, fdkbp_single.cpp:259-531,641-683). Full detector ROI
  * (roi = projection_roi = {0,0,nu,nv}), volume nu x nu x nv. */
-int orc_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
-            const orc_fdk_geom *g, float *vol)
+static int fdk_core(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
+                    const orc_fdk_geom *g, int prefiltered, float *vol)
 {
     const size_t sx = nu, sy = nu, sz = nv;
     const size_t npix = nu * nv;
@@ -524,13 +524,17 @@ int orc_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *
 
     for (size_t p = 0; p < nproj; ++p) {
         const float *src = proj + p * npix;
-        for (size_t i = 0; i < npix; ++i) img[i] = src[i] * weights[p];
         float pm[12];
         orc_fdk_projmatrix(g, nu, angles[p], pm);
-        orc_fdk_ramp(img, nu, nv);
-        for (size_t i = 0; i < npix; ++i) {
-            img[i] *= sad_sid_2;
-            img[i] *= scale;
+        if (prefiltered) {
+            memcpy(img, src, npix * sizeof(float));
+        } else {
+            for (size_t i = 0; i < npix; ++i) img[i] = src[i] * weights[p];
+            orc_fdk_ramp(img, nu, nv);
+            for (size_t i = 0; i < npix; ++i) {
+                img[i] *= sad_sid_2;
+                img[i] *= scale;
+            }
         }
         for (size_t i = 0; i < sx; ++i) {
             float x = (float)(origin[0] + (float)i * spacing[0]);
@@ -586,4 +590,52 @@ int orc_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *
                 vol[(sz - k - 1) * sy * sx + j * sx + i] = cbct[k * sy * sx + j * sx + (sx - 1 - i)];
     free(mask); free(cbct); free(img); free(xip); free(yip); free(zip);
     return 0;
+}
+
+int orc_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
+            const orc_fdk_geom *g, float *vol)
+{
+    return fdk_core(proj, nu, nv, nproj, angles, weights, g, 0, vol);
+}
+
+/* The per-projection image preparation of FdkReconBase::Process + reconstruct +
+ * project_volume_onto_image_c: img *= weight, ramp_filter_tuned, cbi *= sad_sid_2, cbi *= scale. */
+void orc_fdk_prepare(float *proj, size_t nu, size_t nv, size_t nproj, const float *weights, const orc_fdk_geom *g)
+{
+    const float scale = g->sod / g->sdd;
+    const float sad_sid_2 = (g->sod * g->sod) / (g->sdd * g->sdd);
+    for (size_t p = 0; p < nproj; ++p) {
+        float *img = proj + p * nu * nv;
+        for (size_t i = 0; i < nu * nv; ++i) img[i] = img[i] * weights[p];
+        orc_fdk_ramp(img, nu, nv);
+        for (size_t i = 0; i < nu * nv; ++i) {
+            img[i] *= sad_sid_2;
+            img[i] *= scale;
+        }
+    }
+}
+
+/* Backprojection and final mirror only, of projections already prepared by orc_fdk_prepare. */
+int orc_fdk_bp(const float *filtered, size_t nu, size_t nv, size_t nproj, const float *angles, const orc_fdk_geom *g,
+               float *vol)
+{
+    return fdk_core(filtered, nu, nv, nproj, angles, NULL, g, 1, vol);
+}
+
+/* Host geometry of StdBackProjectorBase::Process 2D (StdBackProjectorBase.cpp:72-79). */
+void orc_bp_geometry(const float *angles, size_t n, size_t nu, float center, int direction, float *fsin, float *fcos,
+                     float *fstartu)
+{
+    const float dirweight = 2.0f * ((float)direction - 0.5f);
+    const size_t mcx = nu / 2;
+    for (size_t k = 0; k < n; ++k) {
+        fsin[k] = sinf(dirweight * angles[k] * kFPi / 180.0f);
+        fcos[k] = cosf(dirweight * angles[k] * kFPi / 180.0f);
+        fstartu[k] = mcx * (fsin[k] - fcos[k]) + center;
+    }
+}
+
+void orc_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, size_t nslices, size_t *mask)
+{
+    circle_mask(nx, ny, correcttilt, tiltangle, nslices, mask);
 }

@@ -49,6 +49,10 @@ int orc_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj, const
                     const float *weights, float center, int direction, size_t buffersize, int correcttilt,
                     float tiltangle, float tiltpivot, size_t roi_y0, size_t nslices, float *vol);
 
+void orc_bp_geometry(const float *angles, size_t n, size_t nu, float center, int direction, float *fsin, float *fcos,
+                     float *fstartu);
+void orc_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, size_t nslices, size_t *mask);
+
 /* FDKbp_single via FdkReconBase (FDKBackProjectors/src/fdkbp_single.cpp:83-994,
  * fdkreconbase.cpp:91-277). vol: XYZ [nv][nu][nu] after the final mirror. */
 typedef struct {
@@ -65,14 +69,12 @@ typedef struct {
 int orc_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
             const orc_fdk_geom *g, float *vol);
 /* pieces of orc_fdk, exposed for kernel-level checks */
+void orc_fdk_prepare(float *proj, size_t nu, size_t nv, size_t nproj, const float *weights, const orc_fdk_geom *g);
+int orc_fdk_bp(const float *filtered, size_t nu, size_t nv, size_t nproj, const float *angles, const orc_fdk_geom *g,
+               float *vol);
 void orc_fdk_ramp(float *img, size_t width, size_t height);
 void orc_fdk_projmatrix(const orc_fdk_geom *g, size_t nu, float angle, float *pm /*12*/);
 
-/* FP64 backprojection references for the precision form (no reference counterpart):
- * the same sampling as the FP32 paths with all geometry and accumulation in double. */
-int orc_fdk_f64(const float *filtered, size_t nu, size_t nv, size_t nproj, const double *pm /*12 per proj*/,
-                const double *ic /*2*/, const size_t *mask /*2 per row*/, int bilinear, const size_t *slices,
-                size_t nslices, double *out /*[nslices][nu][nu]*/);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,288 @@
+"""CUDA path against the oracle, through the C ABI (gpu).
+
+Bars: bit-exact for the integer dark/flat arithmetic, reference averaging, doses and the
+backprojection geometry/accumulation (given identical filtered projections); the log in
+FullLogNorm within 1 ulp (CUDA logf vs glibc logf); FFT-based filters within 1e-5
+relative RMS (float FFT vs the oracle's FP64 FFT); full FP32 volumes within 1e-5
+relative RMS of the oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from imagingsuite_b200 import _lib as L
+from imagingsuite_b200 import modules as M
+
+pytestmark = pytest.mark.gpu
+
+
+def relrms(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.sqrt(np.mean((a - b) ** 2) / max(np.mean(b ** 2), 1e-300)))
+
+
+def ulps(a, b):
+    a = np.asarray(a, np.float32).view(np.int32).astype(np.int64)
+    b = np.asarray(b, np.float32).view(np.int32).astype(np.int64)
+    return np.abs(a - b)
+
+
+def dev(x, cuda):
+    return torch.from_numpy(np.ascontiguousarray(x)).to(cuda)
+
+
+def stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+# ------------------------------------------------------------------ FullLogNorm
+
+
+def _counts(seed, nproj, nv, nu):
+    rng = np.random.default_rng(seed)
+    darks = np.round(rng.normal(100, 3, (5, nv, nu))).astype(np.uint16)
+    flats = (rng.poisson(30000, (5, nv, nu)) + 100).astype(np.uint16)
+    proj = (rng.poisson(15000, (nproj, nv, nu)) + 100).astype(np.uint16)
+    proj[0, 0, :7] = 60  # I - D <= 0
+    return proj, flats, darks
+
+
+@pytest.mark.parametrize("usenorm", [False, True])
+@pytest.mark.parametrize("method", ["ImageAverage", "ImageSum", "ImageMedian", "ImageMax"])
+def test_fulllognorm_module(cuda, usenorm, method):
+    proj, flats, darks = _counts(1, 13, 20, 36)
+    roi = (3, 2, 30, 17)
+    cfg = M.ReconConfig()
+    cfg.ProjectionInfo.dose_roi = roi
+    cfg.ProjectionInfo.nOBCount, cfg.ProjectionInfo.nDCCount = 5, 5
+    mod = M.FullLogNorm()
+    mod.Configure(cfg, {"usenormregion": str(usenorm).lower(), "uselut": "false", "referenceaverage": method})
+    mod.SetReferenceImages(dev(darks, cuda), dev(flats, cuda))
+    out = mod.Process(dev(proj, cuda), {}).cpu().numpy()
+
+    refs = O.lognorm_refs(darks.astype(np.float32), flats.astype(np.float32), method, usenorm, roi)
+    assert np.array_equal(mod.mDark.cpu().numpy(), refs.dark)            # averaging: exact
+    assert (mod.fDarkDose, mod.fFlatDose) == (refs.darkdose, refs.flatdose)  # doses: exact
+    assert ulps(mod.mFlatField.cpu().numpy(), refs.logflat).max() <= 1
+    if usenorm:
+        doses = np.array([O.frame_dose(proj[i].astype(np.float32), roi) for i in range(proj.shape[0])], np.float32)
+        dl = O.lognorm_doselog(doses, refs.darkdose)
+    else:
+        dl = np.zeros(1, np.float32)
+    exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, dl)
+    u = ulps(out, exp)
+    assert u.max() <= 2, u.max()
+    assert np.mean(u == 0) > 0.9
+    assert np.array_equal(out == 0, exp == 0)  # the (I - D <= 0) mask is exact
+
+
+def test_lognorm_f32_inplace_and_unaligned(cuda):
+    proj, flats, darks = _counts(2, 3, 7, 13)  # npix = 91: scalar path
+    refs = O.lognorm_refs(darks.astype(np.float32), flats.astype(np.float32))
+    p = dev(proj.astype(np.float32), cuda)
+    d, lf = dev(refs.dark, cuda), dev(refs.logflat, cuda)
+    dl = torch.zeros(1, device=cuda)
+    L.check(L.lib().mr_lognorm_apply(p.data_ptr(), L.MR_F32, 91, 3, d.data_ptr(), lf.data_ptr(), dl.data_ptr(), 1, 1, 1,
+                                     p.data_ptr(), stream()))
+    exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, np.zeros(1, np.float32))
+    assert ulps(p.cpu().numpy(), exp).max() <= 2
+
+
+def test_lognorm_rejects_bad_arguments(cuda):
+    x = torch.zeros(10, device=cuda)
+    st = L.lib().mr_lognorm_apply(x.data_ptr(), L.MR_F32, 10, 2, x.data_ptr(), x.data_ptr(), x.data_ptr(), 3, 1, 1,
+                                  x.data_ptr(), stream())
+    assert st == L.MR_ERR_ARGUMENT
+    with pytest.raises(M.ReconException):
+        mod = M.FullLogNorm()
+        mod.Configure(M.ReconConfig(), {"usenormregion": "false", "referenceaverage": "ImageAverage"})
+        mod.Process(torch.zeros((1, 4, 4), device=cuda), {})
+
+
+# ------------------------------------------------------------ ProjectionFilterSingle
+
+
+@pytest.mark.parametrize("ftype", ["ram-lak", "shepp-logan", "hanning", "hamming", "butterworth"])
+@pytest.mark.parametrize("nu,pd,cutoff", [(256, 2, 0.5), (100, 1, 0.3), (2048, 2, 0.5), (37, 0, 0.25)])
+def test_projfilter(cuda, ftype, nu, pd, cutoff):
+    rng = np.random.default_rng(nu)
+    proj = rng.standard_normal((3, 5, nu)).astype(np.float32) + 2.0
+    cfg = M.ReconConfig()
+    cfg.ProjectionInfo.roi = (0, 0, nu, 5)
+    mod = M.ProjectionFilterSingle()
+    mod.Configure(cfg, {"filtertype": ftype, "cutoff": str(cutoff), "order": "2", "usebias": "true",
+                        "biasweight": "0.1", "paddingdoubler": str(pd)})
+    out = mod.Process(dev(proj, cuda)).cpu().numpy()
+    exp = O.projfilter(proj, O.projfilter_plan(nu, ftype, cutoff, 2.0, True, 0.1, pd))
+    assert relrms(out, exp) < 1e-5
+
+
+def test_projfilter_fused_weights(cuda):
+    rng = np.random.default_rng(5)
+    proj = rng.standard_normal((4, 6, 128)).astype(np.float32)
+    w = rng.uniform(0.5, 2, 4).astype(np.float32)
+    cfg = M.ReconConfig()
+    cfg.ProjectionInfo.roi = (0, 0, 128, 6)
+    mod = M.ProjectionFilterSingle()
+    mod.Configure(cfg, {"filtertype": "hanning", "cutoff": "0.5", "order": "1", "usebias": "true",
+                        "biasweight": "0.1", "paddingdoubler": "2"})
+    a = mod.Process(dev(proj, cuda), weights=dev(w, cuda)).cpu().numpy()
+    b = mod.Process(dev(proj, cuda)).cpu().numpy() * w[:, None, None]
+    assert relrms(a, b) < 1e-6
+
+
+# ------------------------------------------------------------------- parallel beam
+
+
+def _bp_module(cfg, nu, nv, buffersize=16, compat=True, precision="fp32"):
+    bp = M.MultiProjectionBPparallel()
+    bp.Configure(cfg, {"ProjectionBufferSize": str(buffersize), "SliceBlock": "32", "SubVolume": "1 1",
+                       "referencecompat": str(compat).lower(), "precision": precision})
+    bp.SetROI((0, cfg.ProjectionInfo.roi[1], nu, cfg.ProjectionInfo.roi[1] + nv))
+    return bp
+
+
+def _text(a):
+    return " ".join("%.9g" % v for v in a)
+
+
+@pytest.mark.parametrize("tilt", [False, True])
+@pytest.mark.parametrize("direction", [0, 1])
+def test_bp_parallel_bit_exact(cuda, tilt, direction):
+    rng = np.random.default_rng(7)
+    nproj, nv, nu = 45, 16, 64
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
+    cfg = M.ReconConfig()
+    pi = cfg.ProjectionInfo
+    pi.fCenter, pi.eDirection, pi.bCorrectTilt, pi.fTiltAngle, pi.fTiltPivotPosition = 31.3, direction, tilt, 0.6, 2.0
+    pi.roi = (0, 3, nu, 3 + nv)
+    pi.nDims = (nu, nv, nproj)
+    bp = _bp_module(cfg, nu, nv)
+    bp.Process(dev(proj, cuda), {"angles": _text(ang), "weights": _text(w)})
+    vol = bp.GetVolume().cpu().numpy()
+    exp = O.bp_parallel(proj, ang, w, 31.3, direction=direction, buffersize=16, correcttilt=tilt, tiltangle=0.6,
+                        tiltpivot=2.0, roi_y0=3, nslices=nv)
+    assert np.array_equal(vol, exp)
+
+
+@pytest.mark.parametrize("nproj,nv,nu", [(360, 64, 256), (17, 7, 33), (5, 4, 2), (1, 8, 31)])
+def test_bp_parallel_sizes(cuda, nproj, nv, nu):
+    rng = np.random.default_rng(nu)
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    w = np.full(nproj, np.float32(np.pi / nproj))
+    cfg = M.ReconConfig()
+    cfg.ProjectionInfo.fCenter = (nu - 1) / 2.0
+    cfg.ProjectionInfo.roi = (0, 0, nu, nv)
+    bp = _bp_module(cfg, nu, nv)
+    bp.Process(dev(proj, cuda), {"angles": _text(ang), "weights": _text(w)})
+    exp = O.bp_parallel(proj, ang, w, (nu - 1) / 2.0, buffersize=16)
+    assert np.array_equal(bp.GetVolume().cpu().numpy(), exp)
+
+
+def test_bp_parallel_all_projections_mode(cuda):
+    """referencecompat=false backprojects every projection (no buffer-drop rule)."""
+    rng = np.random.default_rng(8)
+    nproj, nv, nu = 40, 8, 48
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 4.5).astype(np.float32)
+    w = np.ones(nproj, np.float32)
+    cfg = M.ReconConfig()
+    cfg.ProjectionInfo.fCenter = 23.5
+    cfg.ProjectionInfo.roi = (0, 0, nu, nv)
+    bp = _bp_module(cfg, nu, nv, compat=False)
+    bp.Process(dev(proj, cuda), {"angles": _text(ang), "weights": _text(w)})
+    exp = O.bp_parallel(proj, ang, w, 23.5, buffersize=1024)  # one buffer flush: nothing dropped
+    assert np.array_equal(bp.GetVolume().cpu().numpy(), exp)
+
+
+# -------------------------------------------------------------------------- FDK
+
+
+def _fdk_cfg(nu, nv, pp=None, direction=0, tilt=False):
+    cfg = M.ReconConfig()
+    pi = cfg.ProjectionInfo
+    pi.fSOD, pi.fSDD = 300.0, 600.0
+    pi.fpPoint = pp if pp is not None else ((nu - 1) / 2.0, (nv - 1) / 2.0)
+    pi.fCenter = (nu - 1) / 2.0 + 0.3
+    pi.fResolution = (0.2, 0.2)
+    pi.eDirection = direction
+    pi.bCorrectTilt, pi.fTiltAngle, pi.fTiltPivotPosition = tilt, 0.5, nv / 2.0
+    pi.nDims = (nu, nv, 0)
+    cfg.MatrixInfo.fVoxelSize = (0.1, 0.1, 0.1)
+    return cfg
+
+
+def _ogeom(cfg):
+    pi = cfg.ProjectionInfo
+    return O.fdk_geom(pi.fSOD, pi.fSDD, pi.fpPoint, pi.fCenter, pi.fResolution, cfg.MatrixInfo.fVoxelSize,
+                      pi.eDirection, pi.bCorrectTilt, pi.fTiltAngle, pi.fTiltPivotPosition)
+
+
+def test_fdk_filter(cuda):
+    rng = np.random.default_rng(11)
+    nproj, nv, nu = 6, 40, 96
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32) + 1.0
+    w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
+    cfg = _fdk_cfg(nu, nv)
+    g = _ogeom(cfg)
+    exp = O.fdk_prepare(proj, w, g)
+    out = torch.empty((nproj, nv, nu), device=cuda)
+    sc = np.float32(300.0) / np.float32(600.0)
+    s2 = np.float32(np.float32(300.0 * 300.0) / np.float32(600.0 * 600.0))
+    L.check(L.lib().mr_fdk_filter(dev(proj, cuda).data_ptr(), nu, nv, nproj, dev(w, cuda).data_ptr(), float(s2),
+                                  float(sc), L.MR_F32, out.data_ptr(), None, stream()))
+    assert relrms(out.cpu().numpy(), exp) < 1e-5
+
+
+@pytest.mark.parametrize("direction", [0, 1])
+@pytest.mark.parametrize("pp", [None, (40.0, 31.3)])
+@pytest.mark.parametrize("tilt", [False, True])
+def test_fdk_backproject_bit_exact(cuda, direction, pp, tilt):
+    """Given identical prepared projections the GPU FDK volume equals the oracle's bit for bit."""
+    rng = np.random.default_rng(12)
+    nproj, nv, nu = 12, 40, 64
+    cfg = _fdk_cfg(nu, nv, pp, direction, tilt)
+    g = _ogeom(cfg)
+    filt = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 30.0).astype(np.float32)
+    exp = O.fdk_bp(filt, ang, g)
+    mod = M.FDKbp_single()
+    mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
+    mod.SetROI((0, 0, nu, nv))
+    xip, yip, zip_, s2, sc, uni = mod.partials(ang)
+    assert uni == (0 if tilt else 1)
+    vol = torch.empty((nv, nu, nu), device=cuda)
+    X, Y, Z = (dev(a, cuda) for a in (xip, yip, zip_))
+    L.check(L.lib().mr_fdk_backproject(dev(filt, cuda).data_ptr(), L.MR_F32, None, nu, nv, nproj, X.data_ptr(),
+                                       Y.data_ptr(), Z.data_ptr(), uni, mod._mask.data_ptr(), 0, vol.data_ptr(),
+                                       stream()))
+    assert np.array_equal(vol.cpu().numpy(), exp)
+
+
+def test_fdk_module_end_to_end(cuda):
+    rng = np.random.default_rng(13)
+    nproj, nv, nu = 24, 48, 64
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32) + 0.5
+    ang = (np.arange(nproj) * 15.0).astype(np.float32)
+    w = np.full(nproj, np.float32(0.25))
+    cfg = _fdk_cfg(nu, nv)
+    mod = M.FDKbp_single()
+    mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
+    mod.SetROI((0, 0, nu, nv))
+    p = {"angles": _text(ang), "weights": _text(w)}
+    mod.Process(dev(proj[:10], cuda), {"angles": _text(ang[:10]), "weights": _text(w[:10])})
+    mod.Process(dev(proj[10:], cuda), {"angles": _text(ang[10:]), "weights": _text(w[10:])})  # accumulates
+    exp = O.fdk(proj, ang, w, _ogeom(cfg))
+    assert relrms(mod.GetVolume().cpu().numpy(), exp) < 1e-5
+    assert p  # parameters use the engine's text form
+
+
+def test_fdk_rejects_short_detector(cuda):
+    x = torch.zeros((1, 8, 16), device=cuda)
+    st = L.lib().mr_fdk_filter(x.data_ptr(), 16, 8, 1, None, 1.0, 1.0, L.MR_F32, x.data_ptr(), None, stream())
+    assert st == L.MR_ERR_ARGUMENT

@@ -1,0 +1,128 @@
+"""The C restatement (oracle/liboracle.so) against the reference's own modules compiled from
+source (oracle/_ref/libmuhrec_ref.so), on seeded inputs. These pins are what make the
+oracle trustworthy: every GPU parity test compares against the restatement."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+
+def _rng(seed):
+    return np.random.default_rng(seed)
+
+
+@pytest.mark.parametrize("tilt", [False, True])
+@pytest.mark.parametrize("direction", [0, 1])
+@pytest.mark.parametrize("buffersize", [16, 7])
+def test_bp_parallel_bit_exact(ref_lib, tilt, direction, buffersize):
+    rng = _rng(10 + buffersize)
+    nproj, nv, nu = 37, 12, 48
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
+    kw = dict(direction=direction, buffersize=buffersize, correcttilt=tilt, tiltangle=0.6, tiltpivot=2.0, roi_y0=3)
+    a = O.bp_parallel(proj, ang, w, 23.5, **kw)
+    b = O.bp_parallel(proj, ang, w, 23.5, use_ref=True, **kw)
+    assert np.array_equal(a, b)
+
+
+def test_bp_parallel_ragged_sizes(ref_lib):
+    # nv not a multiple of 4 (the reference only updates 4*(nv/4) slices), odd nu
+    rng = _rng(3)
+    nproj, nv, nu = 9, 7, 33
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 20.0).astype(np.float32)
+    w = np.ones(nproj, np.float32)
+    a = O.bp_parallel(proj, ang, w, 16.2, buffersize=16)
+    b = O.bp_parallel(proj, ang, w, 16.2, buffersize=16, use_ref=True)
+    assert np.array_equal(a, b)
+    assert not a[:, :, 4:].any()
+
+
+@pytest.mark.parametrize("direction", [0, 1])
+@pytest.mark.parametrize("pp", [(23.5, 19.5), (20.0, 30.2), (26.0, 4.0)])
+def test_fdk_bit_exact(ref_lib, direction, pp):
+    rng = _rng(20)
+    nproj, nv, nu = 16, 36, 40
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 360.0 / nproj).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
+    g = O.fdk_geom(300.0, 600.0, pp, 19.7, (0.2, 0.2), (0.1, 0.1, 0.1), direction=direction)
+    a = O.fdk(proj, ang, w, g)
+    b = O.fdk(proj, ang, w, g, use_ref=True)
+    assert np.array_equal(a, b)
+
+
+def test_fdk_prepare_then_bp_equals_fdk():
+    rng = _rng(21)
+    nproj, nv, nu = 8, 24, 32
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 45.0).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
+    g = O.fdk_geom(250.0, 500.0, (15.5, 11.5), 15.5, (0.2, 0.2), (0.1, 0.1, 0.1))
+    a = O.fdk(proj, ang, w, g)
+    b = O.fdk_bp(O.fdk_prepare(proj, w, g), ang, g)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("usenorm", [False, True])
+@pytest.mark.parametrize("method", ["ImageAverage", "ImageSum", "ImageMedian", "ImageMin", "ImageMax"])
+def test_fulllognorm_bit_exact(ref_lib, usenorm, method):
+    rng = _rng(30)
+    nproj, nv, nu = 11, 10, 24
+    darks = np.round(rng.normal(100, 3, (4, nv, nu))).astype(np.float32)
+    flats = (rng.poisson(30000, (5, nv, nu)) + darks[0]).astype(np.float32)
+    proj = (rng.poisson(20000, (nproj, nv, nu)) + 100).astype(np.float32)
+    proj[0, 0, :5] = 50  # I - D <= 0 branch
+    roi = (2, 2, 20, 9)
+    out_r, dark_r, lf_r, doses_r, (dd, fd) = O.ref_fulllognorm(proj, darks, flats, method, usenorm, roi)
+    refs = O.lognorm_refs(darks, flats, method, usenorm, roi)
+    assert np.array_equal(refs.dark, dark_r)
+    assert np.array_equal(refs.logflat, lf_r)
+    assert refs.darkdose == dd and refs.flatdose == fd
+    if usenorm:
+        doses = np.array([O.frame_dose(proj[i], roi) for i in range(nproj)], np.float32)
+        assert np.array_equal(doses, doses_r)
+        dl = O.lognorm_doselog(doses, refs.darkdose)
+    else:
+        dl = np.zeros(1, np.float32)
+    out = O.lognorm_apply(proj, refs.dark, refs.logflat, dl)
+    assert np.array_equal(out, out_r)
+
+
+@pytest.mark.parametrize("ftype", ["ram-lak", "shepp-logan", "hanning", "hamming", "butterworth"])
+@pytest.mark.parametrize("nu,pd,cutoff", [(64, 2, 0.5), (50, 1, 0.35), (33, 0, 0.2)])
+def test_projfilter(ref_lib, ftype, nu, pd, cutoff):
+    rng = _rng(40)
+    proj = rng.standard_normal((3, 5, nu)).astype(np.float32)
+    plan = O.projfilter_plan(nu, ftype, cutoff, 2.0, True, 0.1, pd)
+    out_r, filt_r, nfft = O.ref_projfilter(proj, ftype, cutoff, 2.0, True, 0.1, pd)
+    assert nfft == plan.nfft
+    assert np.array_equal(plan.filter, filt_r)
+    out = O.projfilter(proj, plan)
+    rel = np.sqrt(np.mean((out - out_r) ** 2) / np.mean(out_r ** 2))
+    assert rel < 1e-6
+
+
+def test_projfilter_bad_cutoff(ref_lib):
+    with pytest.raises(ValueError):
+        O.projfilter_plan(64, "hanning", 0.7)
+    with pytest.raises(RuntimeError):
+        O.ref_projfilter(np.zeros((1, 2, 64), np.float32), "hanning", 0.7)
+
+
+@pytest.mark.parametrize("method", ["ImageSum", "ImageAverage", "ImageMedian", "ImageMin", "ImageMax"])
+@pytest.mark.parametrize("n", [1, 4, 5])
+def test_average(ref_lib, method, n):
+    rng = _rng(50 + n)
+    stack = np.round(rng.normal(1000, 30, (n, 6, 9))).astype(np.float32)
+    assert np.array_equal(O.average(stack, method), O.average(stack, method, use_ref=True))
+
+
+def test_frame_dose(ref_lib):
+    rng = _rng(60)
+    frame = rng.uniform(0, 100, (20, 30)).astype(np.float32)
+    for roi in [(3, 2, 25, 18), (1, 1, 30, 20), (5, 5, 6, 7), (0, 3, 10, 9)]:
+        r = np.asarray(roi, np.uintp)
+        ref = O.ref().ref_frame_dose(O._p(frame), O._sz(30), O._p(r, O._SZ))
+        assert O.frame_dose(frame, roi) == pytest.approx(ref, abs=0) or O.frame_dose(frame, roi) == ref
