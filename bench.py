@@ -224,7 +224,7 @@ def run_mr(args):
     fdk = pipe32.fdk
     filt = torch.empty((nproj, nv, nu), device=device)
     proj = pipe32._lognorm_into(counts)
-    wgt, X, Y, Z, s2, sc, uni = fdk._geo
+    wgt, X, Y, Z, s2, sc, uni, box = fdk._geo
     st = stream.cuda_stream
     L.check(L.lib().mr_fdk_filter(proj.data_ptr(), nu, nv, nproj, wgt.data_ptr(), s2, sc, L.MR_F32, filt.data_ptr(),
                                   None, st))
@@ -232,18 +232,19 @@ def run_mr(args):
 
     def bp32():
         L.check(L.lib().mr_fdk_backproject(filt.data_ptr(), L.MR_F32, None, nu, nv, nproj, X.data_ptr(), Y.data_ptr(),
-                                           Z.data_ptr(), uni, fdk._mask.data_ptr(), 0, vol.data_ptr(), st))
+                                           Z.data_ptr(), uni, fdk._mask.data_ptr(), box[0], box[1], 0, vol.data_ptr(), st))
 
     tbp = kernel_time(bp32, stream)
     q16 = torch.empty((nproj, nv, nu), dtype=torch.uint16, device=device)
     qs = torch.empty(nproj, device=device)
     L.check(L.lib().mr_quantize(filt.data_ptr(), nu * nv, nproj, L.MR_BF16, q16.data_ptr(), qs.data_ptr(), st))
     vol16 = torch.empty((nv, nu, nu), device=device)
+    box16 = pipe16.fdk._geo[-1]
 
     def bp16():
         L.check(L.lib().mr_fdk_backproject(q16.data_ptr(), L.MR_BF16, qs.data_ptr(), nu, nv, nproj, X.data_ptr(),
-                                           Y.data_ptr(), Z.data_ptr(), uni, fdk._mask.data_ptr(), 0, vol16.data_ptr(),
-                                           st))
+                                           Y.data_ptr(), Z.data_ptr(), uni, fdk._mask.data_ptr(), box16[0], box16[1], 0,
+                                           vol16.data_ptr(), st))
 
     tbp16 = kernel_time(bp16, stream)
     # precision: BF16-stored vs FP32 volumes on 16 seeded slices

@@ -61,7 +61,9 @@ _PROTOS = {
     "mr_fdk_filter": (c_int, [c_void, c_size, c_size, c_size, c_void, c_float, c_float, c_int, c_void, c_void,
                               c_void]),
     "mr_fdk_backproject": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_int,
-                                   c_void, c_int, c_void, c_void]),
+                                   c_void, c_int, c_int, c_int, c_void, c_void]),
+    "mr_fdk_box": (c_int, [P_float, P_float, P_float, c_size, c_size, c_size, c_int, P_int, P_int]),
+    "mr_device_status": (c_int, [P_int]),
 }
 
 EXPORTED = tuple(_PROTOS)

@@ -18,6 +18,10 @@
 
 namespace mr {
 
+mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
+                         const float *xip_d, const float *yip_d, const float *zip_d, const uint32_t *mask_d,
+                         int accumulate, float *vol_d, int bw, int bh, cudaStream_t s);
+
 static const float kFPi = 3.1415926535897932384626f;
 static const double kDPi = 3.1415926535897932384626433832795028841971693993751;
 
@@ -434,7 +438,7 @@ mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const floa
 
 mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
                              const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
-                             const uint32_t *mask_d, int accumulate, float *vol_d, void *stream)
+                             const uint32_t *mask_d, int box_w, int box_h, int accumulate, float *vol_d, void *stream)
 {
     if (!proj_d || !xip_d || !yip_d || !zip_d || !mask_d || !vol_d)
         return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: null pointer");
@@ -442,10 +446,15 @@ mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d
     if (dtype != MR_F32 && !scale_d) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: 16-bit projections need scale_d");
     if (nu == 0 || nv == 0 || nu > 65536 || nv > 65536) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: unsupported size");
     if (nproj > 0x7fffffff) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: too many projections");
+    cudaStream_t s = as_stream(stream);
+    if (uniform_z && box_w > 0 && box_h > 0 && nproj > 0) {
+        mr_status st = fdk_tma_launch(proj_d, dtype, scale_d, nu, nv, nproj, xip_d, yip_d, zip_d, mask_d, accumulate,
+                                      vol_d, box_w, box_h, s);
+        if (st != MR_ERR_UNSUPPORTED) return st;
+    }
     constexpr int CZ = 8;
     dim3 block(32, 4);
     dim3 grid(div_up(nu, 32), div_up(nu, 4), div_up(nv, CZ));
-    cudaStream_t s = as_stream(stream);
     const int np = static_cast<int>(nproj), iu = static_cast<int>(nu), iv = static_cast<int>(nv);
     switch (dtype) {
     case MR_F32:

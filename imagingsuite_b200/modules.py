@@ -448,6 +448,7 @@ class FDKbp_single(_BackProjectorBase):
     def __init__(self):
         super().__init__("FDKbp_single")
         self._first = True
+        self.staging = True  # TMA-staged footprints (False: direct global loads; same results)
 
     def SetROI(self, roi) -> None:
         self._roi = tuple(int(v) for v in roi)
@@ -511,10 +512,15 @@ class FDKbp_single(_BackProjectorBase):
         key = (angles.tobytes(), weights.tobytes(), str(dev))
         if getattr(self, "_geo_key", None) != key:
             xip, yip, zip_, s2, sc, uni = self.partials(angles)
+            bw, bh = ctypes.c_int(0), ctypes.c_int(0)
+            if uni:
+                check(L.lib().mr_fdk_box(xip.ctypes.data_as(L.P_float), yip.ctypes.data_as(L.P_float),
+                                         zip_.ctypes.data_as(L.P_float), nu, nv, nproj, _PRECISION[self.precision],
+                                         ctypes.byref(bw), ctypes.byref(bh)))
             self._geo = (torch.from_numpy(weights).to(dev), *(torch.from_numpy(a).to(dev) for a in (xip, yip, zip_)),
-                         s2, sc, uni)
+                         s2, sc, uni, (bw.value, bh.value))
             self._geo_key = key
-        w, X, Y, Z, s2, sc, uni = self._geo
+        w, X, Y, Z, s2, sc, uni, box = self._geo
         dtype = _PRECISION[self.precision]
         if dtype == L.MR_F32:
             filt = torch.empty_like(projections)
@@ -525,9 +531,10 @@ class FDKbp_single(_BackProjectorBase):
         st = _stream()
         check(L.lib().mr_fdk_filter(projections.data_ptr(), nu, nv, nproj, w.data_ptr(), s2, sc, dtype, filt.data_ptr(),
                                     _ptr(scale), st))
+        box = box if self.staging else (0, 0)
         check(L.lib().mr_fdk_backproject(filt.data_ptr(), dtype, _ptr(scale), nu, nv, nproj, X.data_ptr(), Y.data_ptr(),
-                                         Z.data_ptr(), uni, self._mask.data_ptr(), int(not self._first),
-                                         self.volume.data_ptr(), st))
+                                         Z.data_ptr(), uni, self._mask.data_ptr(), box[0], box[1],
+                                         int(not self._first), self.volume.data_ptr(), st))
         self._first = False
         return 0
 

@@ -189,7 +189,19 @@ mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, c
  * xip/yip/zip: device copies of mr_fdk_partials. mask_d: mr_bp_circle_mask(nu, nu, ...). */
 mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
                              size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
-                             const uint32_t *mask_d, int accumulate, float *vol_d, void *stream);
+                             const uint32_t *mask_d, int box_w, int box_h, int accumulate, float *vol_d, void *stream);
+/* Shared-memory staging box for mr_fdk_backproject (host): the largest detector footprint
+ * (columns box_w, rows box_h) of a 32 x 8 x 32 voxel tile over a sample of the geometry,
+ * from the host copies of the partials. With box_w = box_h = 0, or when the projection
+ * layout does not allow TMA (row pitch not a multiple of 16 bytes), or without uniform_z,
+ * mr_fdk_backproject uses direct global loads; tiles whose footprint exceeds the box fall
+ * back to direct loads for that projection. Results are identical on every path. */
+mr_status mr_fdk_box(const float *xip_h, const float *yip_h, const float *zip_h, size_t nu, size_t nv, size_t nproj,
+                     int dtype, int *box_w, int *box_h);
+
+/* Device-side error word of bounded waits inside kernels (0 = none); reading it
+ * synchronizes the device and clears the word. */
+mr_status mr_device_status(int *status);
 
 #ifdef __cplusplus
 }

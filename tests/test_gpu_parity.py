@@ -6,6 +6,8 @@ FullLogNorm within 1 ulp (CUDA logf vs glibc logf); FFT-based filters within 1e-
 relative RMS (float FFT vs the oracle's FP64 FFT); full FP32 volumes within 1e-5
 relative RMS of the oracle.
 """
+import ctypes
+
 import numpy as np
 import pytest
 import torch
@@ -72,9 +74,11 @@ def test_fulllognorm_module(cuda, usenorm, method):
     else:
         dl = np.zeros(1, np.float32)
     exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, dl)
-    u = ulps(out, exp)
-    assert u.max() <= 2, u.max()
-    assert np.mean(u == 0) > 0.9
+    # CUDA logf and glibc logf may differ by 1 ulp of log(I - D); the difference of two logs
+    # carries that absolute error, so the bar is 2 ulp of the log terms' magnitude
+    tol = 2 * np.spacing(np.float32(np.abs(refs.logflat).max() + np.abs(dl).max()))
+    assert np.abs(out.astype(np.float64) - exp).max() <= tol
+    assert np.mean(out == exp) > 0.9
     assert np.array_equal(out == 0, exp == 0)  # the (I - D <= 0) mask is exact
 
 
@@ -87,7 +91,7 @@ def test_lognorm_f32_inplace_and_unaligned(cuda):
     L.check(L.lib().mr_lognorm_apply(p.data_ptr(), L.MR_F32, 91, 3, d.data_ptr(), lf.data_ptr(), dl.data_ptr(), 1, 1, 1,
                                      p.data_ptr(), stream()))
     exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, np.zeros(1, np.float32))
-    assert ulps(p.cpu().numpy(), exp).max() <= 2
+    assert np.abs(p.cpu().numpy().astype(np.float64) - exp).max() <= 2 * np.spacing(np.float32(np.abs(refs.logflat).max()))
 
 
 def test_lognorm_rejects_bad_arguments(cuda):
@@ -239,11 +243,36 @@ def test_fdk_filter(cuda):
     assert relrms(out.cpu().numpy(), exp) < 1e-5
 
 
+def _fdk_bp_gpu(cuda, mod, filt, ang, staged, dtype=L.MR_F32, scale=None, box=None):
+    nproj, nv, nu = filt.shape
+    xip, yip, zip_, s2, sc, uni = mod.partials(ang)
+    bw, bh = ctypes.c_int(0), ctypes.c_int(0)
+    if box is not None:
+        bw.value, bh.value = box
+    elif staged and uni:
+        L.check(L.lib().mr_fdk_box(xip.ctypes.data_as(L.P_float), yip.ctypes.data_as(L.P_float),
+                                   zip_.ctypes.data_as(L.P_float), nu, nv, nproj, dtype, ctypes.byref(bw),
+                                   ctypes.byref(bh)))
+        assert bw.value > 0 and bh.value > 0
+    vol = torch.empty((nv, nu, nu), device=cuda)
+    X, Y, Z = (dev(a, cuda) for a in (xip, yip, zip_))
+    src = dev(filt, cuda)
+    L.check(L.lib().mr_fdk_backproject(src.data_ptr(), dtype, None if scale is None else scale.data_ptr(), nu, nv,
+                                       nproj, X.data_ptr(), Y.data_ptr(), Z.data_ptr(), uni, mod._mask.data_ptr(),
+                                       bw.value, bh.value, 0, vol.data_ptr(), stream()))
+    status = ctypes.c_int(-1)
+    L.check(L.lib().mr_device_status(ctypes.byref(status)))
+    assert status.value == 0
+    return vol.cpu().numpy(), uni
+
+
+@pytest.mark.parametrize("staged", [True, False])
 @pytest.mark.parametrize("direction", [0, 1])
 @pytest.mark.parametrize("pp", [None, (40.0, 31.3)])
 @pytest.mark.parametrize("tilt", [False, True])
-def test_fdk_backproject_bit_exact(cuda, direction, pp, tilt):
-    """Given identical prepared projections the GPU FDK volume equals the oracle's bit for bit."""
+def test_fdk_backproject_bit_exact(cuda, staged, direction, pp, tilt):
+    """Given identical prepared projections the GPU FDK volume equals the oracle's bit for bit,
+    through the TMA-staged kernel and through the direct-load kernel."""
     rng = np.random.default_rng(12)
     nproj, nv, nu = 12, 40, 64
     cfg = _fdk_cfg(nu, nv, pp, direction, tilt)
@@ -254,14 +283,38 @@ def test_fdk_backproject_bit_exact(cuda, direction, pp, tilt):
     mod = M.FDKbp_single()
     mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
     mod.SetROI((0, 0, nu, nv))
-    xip, yip, zip_, s2, sc, uni = mod.partials(ang)
+    got, uni = _fdk_bp_gpu(cuda, mod, filt, ang, staged)
     assert uni == (0 if tilt else 1)
-    vol = torch.empty((nv, nu, nu), device=cuda)
-    X, Y, Z = (dev(a, cuda) for a in (xip, yip, zip_))
-    L.check(L.lib().mr_fdk_backproject(dev(filt, cuda).data_ptr(), L.MR_F32, None, nu, nv, nproj, X.data_ptr(),
-                                       Y.data_ptr(), Z.data_ptr(), uni, mod._mask.data_ptr(), 0, vol.data_ptr(),
-                                       stream()))
-    assert np.array_equal(vol.cpu().numpy(), exp)
+    assert np.array_equal(got, exp)
+
+
+def test_fdk_staged_box_too_small_falls_back(cuda):
+    """Footprints larger than the staging box take the direct-load path: same volume."""
+    rng = np.random.default_rng(14)
+    nproj, nv, nu = 6, 40, 64
+    cfg = _fdk_cfg(nu, nv)
+    filt = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 60.0).astype(np.float32)
+    mod = M.FDKbp_single()
+    mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
+    mod.SetROI((0, 0, nu, nv))
+    got, _ = _fdk_bp_gpu(cuda, mod, filt, ang, True, box=(8, 8))
+    assert np.array_equal(got, O.fdk_bp(filt, ang, _ogeom(cfg)))
+
+
+@pytest.mark.parametrize("shape", [(9, 72, 96), (5, 33, 40), (7, 64, 128)])
+def test_fdk_staged_shapes(cuda, shape):
+    """Partial slice tiles (nv not a multiple of 32), odd tile counts, wide detectors."""
+    rng = np.random.default_rng(shape[1])
+    nproj, nv, nu = shape
+    cfg = _fdk_cfg(nu, nv)
+    filt = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 360.0 / nproj + 3.0).astype(np.float32)
+    mod = M.FDKbp_single()
+    mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
+    mod.SetROI((0, 0, nu, nv))
+    got, _ = _fdk_bp_gpu(cuda, mod, filt, ang, True)
+    assert np.array_equal(got, O.fdk_bp(filt, ang, _ogeom(cfg)))
 
 
 def test_fdk_module_end_to_end(cuda):
