@@ -56,6 +56,7 @@ _PROTOS = {
     "mr_bp_parallel": (c_int, [c_void, c_int, c_void, c_void, c_void, c_void, c_void, c_void, c_size, c_size, c_size,
                                c_void, c_int, c_float, c_float, c_void, c_void]),
     "mr_quantize": (c_int, [c_void, c_size, c_size, c_int, c_void, c_void, c_void]),
+    "mr_quantize_noalloc": (c_int, [c_void, c_size, c_size, c_int, c_void, c_void, c_void]),
     "mr_fdk_partials": (c_int, [ctypes.POINTER(FdkGeom), c_size, c_size, P_float, c_size, P_float, P_float, P_float,
                                 P_float, P_float, P_int]),
     "mr_fdk_filter": (c_int, [c_void, c_size, c_size, c_size, c_void, c_float, c_float, c_int, c_void, c_void,

@@ -23,6 +23,7 @@
 #include <algorithm>
 #include <cctype>
 #include <cmath>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -305,6 +306,40 @@ mr_status quantize_projections(const float *x_d, size_t per, size_t nproj, int k
     return st;
 }
 
+// ---- allocation-free quantization (mr_quantize_noalloc)
+//
+// Scratch of the no-allocation entry point: the per-projection |max| (kQuantScratchMax
+// floats) followed by the reciprocal scales (kQuantScratchMax floats), 512 KiB in all.
+// Every device that loads this library holds the array until the process exits.
+constexpr size_t kQuantScratchMax = 65536;
+static __device__ __align__(256) float g_quant_scratch[2 * kQuantScratchMax];
+
+// Device address of g_quant_scratch per device ordinal, looked up on the first call made
+// with that device current. In host code the symbol itself is only a host-side stand-in,
+// never a device address, so kernels always receive the looked-up pointer.
+static float *quant_scratch_ptr(int device, mr_status *st)
+{
+    constexpr int kMaxDevices = 64;
+    static float *ptrs[kMaxDevices] = {};
+    static std::mutex mu;
+    if (device < 0 || device >= kMaxDevices) {
+        *st = fail(MR_ERR_UNSUPPORTED, "mr_quantize_noalloc: device ordinal %d above %d", device, kMaxDevices - 1);
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> lock(mu);
+    if (!ptrs[device]) {
+        void *p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_quant_scratch);
+        if (e != cudaSuccess || !p) {
+            *st = fail(MR_ERR_CUDA, "mr_quantize_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return nullptr;
+        }
+        ptrs[device] = static_cast<float *>(p);
+    }
+    *st = MR_OK;
+    return ptrs[device];
+}
+
 } // namespace mr
 
 using namespace mr;
@@ -467,6 +502,38 @@ mr_status mr_quantize(const float *in_d, size_t per, size_t nproj, int dtype, ui
     if (nproj > 65535) return fail(MR_ERR_ARGUMENT, "mr_quantize: more than 65535 projections per call");
     if (per == 0 || nproj == 0) return MR_OK;
     return quantize_projections(in_d, per, nproj, dtype, out_d, scale_d, as_stream(stream));
+}
+
+mr_status mr_quantize_noalloc(const float *in_d, size_t per, size_t nproj, int dtype, uint16_t *out_d, float *scale_d,
+                              void *stream)
+{
+    if (!in_d || !out_d || !scale_d) return fail(MR_ERR_ARGUMENT, "mr_quantize_noalloc: null pointer");
+    if (dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_quantize_noalloc: dtype must be bf16 or f16");
+    if (nproj > kQuantScratchMax)
+        return fail(MR_ERR_ARGUMENT, "mr_quantize_noalloc: %zu projections exceed the built-in scratch of %zu projections",
+                    nproj, kQuantScratchMax);
+    if (per == 0 || nproj == 0) return MR_OK;
+    int device = 0;
+    MR_CUDA_TRY(cudaGetDevice(&device));
+    mr_status st = MR_OK;
+    float *amax = quant_scratch_ptr(device, &st);
+    if (st != MR_OK) return st;
+    float *inv = amax + kQuantScratchMax;
+    cudaStream_t s = as_stream(stream);
+    // the array keeps the previous call's values: the running maxima must start at zero
+    MR_CUDA_TRY(cudaMemsetAsync(amax, 0, nproj * sizeof(float), s));
+    dim3 g(std::min<unsigned>(div_up(per, 256), 64u), static_cast<unsigned>(nproj));
+    k_absmax<<<g, 256, 0, s>>>(in_d, per, amax);
+    if ((st = check_launch("k_absmax")) != MR_OK) return st;
+    k_pow2_scales<<<div_up(nproj, 128), 128, 0, s>>>(amax, nproj, dtype, scale_d, inv);
+    if ((st = check_launch("k_pow2_scales")) != MR_OK) return st;
+    const size_t total = per * nproj;
+    const unsigned blocks = std::min<unsigned>(div_up(total, 256), 148u * 16u);
+    if (dtype == MR_BF16)
+        k_quantize<MR_BF16><<<blocks, 256, 0, s>>>(in_d, per, total, inv, out_d);
+    else
+        k_quantize<MR_F16><<<blocks, 256, 0, s>>>(in_d, per, total, inv, out_d);
+    return check_launch("k_quantize");
 }
 
 mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, const float *weight_d, float sad_sid_2,

@@ -110,6 +110,20 @@ mr_status mr_projfilter_apply(const mr_filter_plan *plan, const float *in_d, flo
  * maps into [2^13, 2^14) for MR_F16, into [0.5, 1) for MR_BF16). out_d holds bf16/f16 bits. */
 mr_status mr_quantize(const float *in_d, size_t per, size_t nproj, int dtype, uint16_t *out_d, float *scale_d,
                       void *stream);
+/* mr_quantize for callers that cannot allocate device memory: code running inside a
+ * framework that owns every allocation (a fixed memory pool, a plugin host that forbids
+ * cudaMalloc) or code that must not allocate while the stream is being used elsewhere.
+ * This entry point has no counterpart in the reference. It computes exactly what
+ * mr_quantize computes, but its per-projection scratch (the running |max| and the inverse
+ * scales) lives in a static device array built into the library instead of cudaMallocAsync
+ * memory: at most 65536 projections per call (512 KiB, held on every device that loads the
+ * library until the process exits); larger calls are rejected with MR_ERR_ARGUMENT. It
+ * allocates nothing. The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture. All calls share the one array, and each call clears the part it uses first, so
+ * calls that overlap on the GPU (on different streams without ordering) race. */
+mr_status mr_quantize_noalloc(const float *in_d, size_t per, size_t nproj, int dtype, uint16_t *out_d, float *scale_d,
+                              void *stream);
 
 /* ---------------------------------------------------------------------------------
  * Parallel-beam backprojection: MultiProjectionBPparallel
