@@ -233,6 +233,93 @@ class FullLogNorm:
         return out
 
 
+# ------------------------------------------------------------------- MorphSpotClean
+
+_CONN = {"conn4": 0, "conn8": 1}
+_DETECT = {"morphdetectholes": 0, "morphdetectpeaks": 1, "morphdetectboth": 2}
+
+
+def morph_spot_clean(img: torch.Tensor, detect: int = 0, conn8: bool = True, th=(0.025, 0.025), sigma=(0.0, 0.0),
+                     edge: int = 9, clamp: bool = False, minlevel: float = -0.1, maxlevel: float = 7.0,
+                     removeinfnan: bool = False) -> torch.Tensor:
+    """ImagingAlgorithms::MorphSpotClean::process (replace mode) in place on (n, nv, nu) or (nv, nu)."""
+    _require_cuda(img, "image")
+    if img.dtype != torch.float32:
+        raise ReconException("MorphSpotClean expects float32 images")
+    nv, nu = img.shape[-2:]
+    n = img.numel() // (nv * nu)
+    t = np.asarray(th, np.float32)
+    s = np.asarray(sigma, np.float32)
+    check(L.lib().mr_morphspotclean(img.data_ptr(), nu, nv, n, int(detect), int(conn8), t.ctypes.data_as(L.P_float),
+                                    s.ctypes.data_as(L.P_float), int(edge), int(clamp), float(minlevel),
+                                    float(maxlevel), int(removeinfnan), _stream()))
+    return img
+
+
+class MorphSpotCleanModule:
+    """MorphSpotCleanModule (StdPreprocModules/src/MorphSpotCleanModule.cpp:14-183). As in
+    the reference's single-threaded path (ProcessSingle :142-181) the cleaner runs with its
+    own edge smoothing length (9; the `edgesmooth` parameter is read but not applied) and
+    without inf/NaN removal (`removeinfnan` is read but not applied); clamping follows
+    `clampdata`."""
+
+    def __init__(self):
+        self.m_eConnectivity = "conn4"
+        self.m_eDetectionMethod = "morphdetectpeaks"
+        self.m_eCleanMethod = "morphcleanreplace"
+        self.m_fThreshold = [0.1, 0.1]
+        self.m_fSigma = [0.01, 0.01]
+        self.m_nEdgeSmoothLength = 5
+        self.m_nMaxArea = 30
+        self.m_bRemoveInfNaN = False
+        self.m_bClampData = False
+        self.m_fMinLevel = -0.1
+        self.m_fMaxLevel = 7.0
+        self.m_bThreading = False
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        try:
+            conn = _get(parameters, "connectivity")
+            clean = _get(parameters, "cleanmethod")
+            det = _get(parameters, "detectionmethod")
+            if conn not in _CONN or clean not in ("morphcleanreplace", "morphcleanfill") or det not in _DETECT:
+                return -1
+            self.m_eConnectivity, self.m_eCleanMethod, self.m_eDetectionMethod = conn, clean, det
+            self.m_fThreshold = [float(np.float32(v)) for v in _get(parameters, "threshold").split()]
+            self.m_fSigma = [float(np.float32(v)) for v in _get(parameters, "sigma").split()]
+            self.m_nEdgeSmoothLength = int(_get(parameters, "edgesmooth"))
+            self.m_nMaxArea = int(_get(parameters, "maxarea"))
+            self.m_bRemoveInfNaN = _string2bool(_get(parameters, "removeinfnan"))
+            self.m_bClampData = _string2bool(_get(parameters, "clampdata"))
+            self.m_fMinLevel = float(np.float32(_get(parameters, "minlevel")))
+            self.m_fMaxLevel = float(np.float32(_get(parameters, "maxlevel")))
+            self.m_bThreading = _string2bool(_get(parameters, "threading"))
+        except (ReconException, ValueError):
+            return -1
+        return 0
+
+    def GetParameters(self) -> dict:
+        return {"connectivity": self.m_eConnectivity, "cleanmethod": self.m_eCleanMethod,
+                "detectionmethod": self.m_eDetectionMethod, "threshold": " ".join(map(str, self.m_fThreshold)),
+                "sigma": " ".join(map(str, self.m_fSigma)), "edgesmooth": str(self.m_nEdgeSmoothLength),
+                "maxarea": str(self.m_nMaxArea), "removeinfnan": str(self.m_bRemoveInfNaN).lower(),
+                "clampdata": str(self.m_bClampData).lower(), "minlevel": str(self.m_fMinLevel),
+                "maxlevel": str(self.m_fMaxLevel), "threading": str(self.m_bThreading).lower()}
+
+    def SetROI(self, roi) -> bool:
+        return False
+
+    def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
+        return self.ProcessCore(img, coeff if coeff is not None else {})
+
+    def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
+        if self.m_eCleanMethod != "morphcleanreplace":
+            raise ReconException("MorphSpotClean: only morphcleanreplace is supported by this module")
+        return morph_spot_clean(img, _DETECT[self.m_eDetectionMethod], self.m_eConnectivity == "conn8",
+                                self.m_fThreshold[:2], self.m_fSigma[:2], edge=9, clamp=self.m_bClampData,
+                                minlevel=self.m_fMinLevel, maxlevel=self.m_fMaxLevel, removeinfnan=False)
+
+
 # ------------------------------------------------------------ ProjectionFilterSingle
 
 

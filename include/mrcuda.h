@@ -80,6 +80,22 @@ mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t n
                            float *out_d, void *stream);
 
 /* ---------------------------------------------------------------------------------
+ * MorphSpotClean, replace mode: ImagingAlgorithms::MorphSpotClean::process
+ * (core/algorithms/ImagingAlgorithms/src/MorphSpotClean.cpp:41-175,264-351) with
+ * kipl::morphology FillHole/FillPeaks (core/kipl/kipl/include/morphology/morphextrema.h:265-328,
+ * morphgeo.h:151-371), in place on nproj images [nproj][nv][nu].
+ * detect: 0 holes, 1 peaks, 2 both; conn8: 0 = 4-connectivity, 1 = 8-connectivity;
+ * th_h/sigma_h: two host floats each (holes, peaks); sigma == 0 for both selects threshold
+ * replacement, else the sigmoid blend; edge: length of the sliding median along the first
+ * and last padded rows (the reference default is 9); clamp/minlevel/maxlevel: LimitDynamics
+ * before cleaning; removeinfnan: replace inf/NaN by the largest finite value first.
+ * nv must be at least 5 (the reference mirrors 5 rows into its padding and reads outside
+ * smaller images). Scratch: three padded images per image in a batch (<= 1 GiB). */
+mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, int detect, int conn8,
+                            const float *th_h, const float *sigma_h, int edge, int clamp, float minlevel,
+                            float maxlevel, int removeinfnan, void *stream);
+
+/* ---------------------------------------------------------------------------------
  * ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:78-376)
  * Plan = ProjectionFilterBase::Configure/BuildFilter/PreparePadding (:78-93,254-299,364-376):
  *   nfft = 2^(ceil(log2 nu) + paddingdoubler); filter over bins 0..nfft/2-1.

@@ -328,3 +328,63 @@ def circle_mask(nx, ny, correcttilt=False, tiltangle=0.0, nslices=0) -> np.ndarr
     m = np.zeros(2 * ny, np.uintp)
     orc().orc_circle_mask(_sz(nx), _sz(ny), int(correcttilt), _f(tiltangle), _sz(nslices), _p(m, _SZ))
     return m.astype(np.uint32)
+
+
+# --------------------------------------------------------------------- MorphSpotClean
+
+DETECT = {"holes": 0, "peaks": 1, "both": 2}
+
+
+def morphspotclean(img, detect="holes", conn8=True, th=(0.1, 0.1), sigma=(0.01, 0.01), edge=9, clamp=False,
+                   minlevel=-0.1, maxlevel=7.0, removeinfnan=False, use_ref=False) -> np.ndarray:
+    """MorphSpotClean::process, MorphCleanReplace, on one image (nv, nu) or a stack (n, nv, nu)."""
+    out = np.array(img, dtype=np.float32, copy=True, order="C")
+    stack = out.reshape((-1,) + out.shape[-2:])
+    t = np.asarray(th, np.float32)
+    s = np.asarray(sigma, np.float32)
+    h, w = stack.shape[1:]
+    for im in stack:
+        if use_ref:
+            _check_ref(ref().ref_morphspotclean(_p(im), _sz(w), _sz(h), DETECT[detect], 0, int(conn8), _p(t), _p(s),
+                                                int(edge), 100, int(clamp), _f(minlevel), _f(maxlevel),
+                                                int(removeinfnan)))
+        else:
+            rc = orc().orc_morphspotclean(_p(im), _sz(w), _sz(h), DETECT[detect], int(conn8), _p(t), _p(s),
+                                          _sz(edge), int(clamp), _f(minlevel), _f(maxlevel), int(removeinfnan))
+            if rc != 0:
+                raise RuntimeError("RecByDilation: f>g")
+    return out
+
+
+def ref_morphspotclean_module(proj, connectivity="conn4", detectionmethod="morphdetectpeaks", threshold="0.1 0.1",
+                              sigma="0.01 0.01", edgesmooth=5, maxarea=30, removeinfnan=False, clampdata=False,
+                              minlevel=-0.1, maxlevel=7.0):
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    nproj, nv, nu = out.shape
+    _check_ref(ref().ref_morphspotclean_module(_p(out), _sz(nu), _sz(nv), _sz(nproj), connectivity.encode(),
+                                               b"morphcleanreplace", detectionmethod.encode(), threshold.encode(),
+                                               sigma.encode(), int(edgesmooth), int(maxarea), int(removeinfnan),
+                                               int(clampdata), _f(minlevel), _f(maxlevel)))
+    return out
+
+
+def fill_hole(img, conn8=True) -> np.ndarray:
+    img = _f32(img)
+    out = np.empty_like(img)
+    orc().orc_fill_hole(_p(img), _sz(img.shape[1]), _sz(img.shape[0]), int(conn8), _p(out))
+    return out
+
+
+def fill_peaks(img, conn8=True) -> np.ndarray:
+    img = _f32(img)
+    out = np.empty_like(img)
+    if orc().orc_fill_peaks(_p(img), _sz(img.shape[1]), _sz(img.shape[0]), int(conn8), _p(out)) != 0:
+        raise RuntimeError("RecByDilation: f>g")
+    return out
+
+
+def fill_peaks_forward(img, conn8=True) -> np.ndarray:
+    img = _f32(img)
+    out = np.empty_like(img)
+    orc().orc_fill_peaks_forward(_p(img), _sz(img.shape[1]), _sz(img.shape[0]), int(conn8), _p(out))
+    return out

@@ -639,3 +639,289 @@ void orc_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, siz
 {
     circle_mask(nx, ny, correcttilt, tiltangle, nslices, mask);
 }
+
+/* ------------------------------------------------------- morphology (kipl) */
+
+/* 2-D neighbourhoods of kipl::morphology::CNeighborhood (core/kipl/kipl/src/morphology/
+ * morphology.cpp:25-40): backward half NGm = {0,-1,-sx,-sx-1,-sx+1}, forward half
+ * NGp = {0,1,sx,sx+1,sx-1}, full NG = {1,-1,-sx,sx,-sx-1,-sx+1,sx-1,sx+1}; 4-connectivity
+ * uses the first 3 / 4 entries. Positions outside the image are rejected (-1), which is
+ * what the edge tables of forward2D/backward2D/neighbor2D (:183-470) amount to. */
+static const int kBwd[5][2] = {{0, 0}, {-1, 0}, {0, -1}, {-1, -1}, {1, -1}};
+static const int kFwd[5][2] = {{0, 0}, {1, 0}, {0, 1}, {1, 1}, {-1, 1}};
+static const int kNbr[8][2] = {{1, 0}, {-1, 0}, {0, -1}, {0, 1}, {-1, -1}, {1, -1}, {-1, 1}, {1, 1}};
+
+static long nb(size_t pos, size_t w, size_t h, const int *d)
+{
+    long x = (long)(pos % w) + d[0], y = (long)(pos / w) + d[1];
+    if (x < 0 || x >= (long)w || y < 0 || y >= (long)h) return -1;
+    return y * (long)w + x;
+}
+
+typedef struct {
+    size_t *v;
+    size_t n, cap;
+} stack_t_;
+
+static void st_push(stack_t_ *s, size_t x)
+{
+    if (s->n == s->cap) {
+        s->cap = s->cap ? 2 * s->cap : 1024;
+        s->v = (size_t *)realloc(s->v, s->cap * sizeof(size_t));
+    }
+    s->v[s->n++] = x;
+}
+
+/* RecByDilation (core/kipl/kipl/include/morphology/morphgeo.h:151-266), including the
+ * forward scan that compares the running image but assigns the marker value (:213-214).
+ * g: mask, f: marker (f <= g), out: reconstruction. Returns -1 when f > g somewhere. */
+int orc_rec_dilation(const float *g, const float *f, size_t w, size_t h, int conn8, float *t)
+{
+    const size_t n = w * h;
+    for (size_t i = 0; i < n; ++i) {
+        if (g[i] < f[i]) return -1;
+        t[i] = f[i];
+    }
+    const int cpm = conn8 ? 5 : 3, cng = conn8 ? 8 : 4;
+    for (size_t pos = 0; pos < n; ++pos) {
+        float mx = t[pos];
+        for (int i = 1; i < cpm; ++i) {
+            long q = nb(pos, w, h, kBwd[i]);
+            if (q != -1 && t[q] > mx) mx = f[q];
+        }
+        t[pos] = mx < g[pos] ? mx : g[pos];
+    }
+    stack_t_ st = {0};
+    for (long pos = (long)n - 1; pos >= 0; --pos) {
+        float mx = t[pos];
+        for (int i = 1; i < cpm; ++i) {
+            long q = nb((size_t)pos, w, h, kFwd[i]);
+            if (q != -1 && t[q] > mx) mx = t[q];
+        }
+        t[pos] = mx < g[pos] ? mx : g[pos];
+        const float tp = t[pos];
+        for (int i = 1; i < cpm; ++i) {
+            long q = nb((size_t)pos, w, h, kFwd[i]);
+            if (q != -1 && t[q] < tp && t[q] < g[q]) {
+                st_push(&st, (size_t)pos);
+                break;
+            }
+        }
+    }
+    while (st.n) {
+        size_t pos = st.v[--st.n];
+        const float tp = t[pos];
+        for (int i = 0; i < cng; ++i) {
+            long q = nb(pos, w, h, kNbr[i]);
+            if (q != -1 && t[q] < tp && g[q] != t[q]) {
+                t[q] = tp < g[q] ? tp : g[q];
+                st_push(&st, (size_t)q);
+            }
+        }
+    }
+    free(st.v);
+    return 0;
+}
+
+/* RecByErosion (morphgeo.h:278-371). g: mask, f: marker (f >= g), out: reconstruction. */
+void orc_rec_erosion(const float *g, const float *f, size_t w, size_t h, int conn8, float *t)
+{
+    const size_t n = w * h;
+    memcpy(t, f, n * sizeof(float));
+    const int cpm = conn8 ? 5 : 3, cng = conn8 ? 8 : 4;
+    for (size_t pos = 0; pos < n; ++pos) {
+        float mn = t[pos];
+        for (int i = 1; i < cpm; ++i) {
+            long q = nb(pos, w, h, kBwd[i]);
+            if (q != -1 && t[q] < mn) mn = t[q];
+        }
+        t[pos] = mn > g[pos] ? mn : g[pos];
+    }
+    stack_t_ st = {0};
+    for (long pos = (long)n - 1; pos >= 0; --pos) {
+        float mn = t[pos];
+        for (int i = 1; i < cpm; ++i) {
+            long q = nb((size_t)pos, w, h, kFwd[i]);
+            if (q != -1 && t[q] < mn) mn = t[q];
+        }
+        t[pos] = mn > g[pos] ? mn : g[pos];
+        const float tp = t[pos];
+        for (int i = 1; i < cpm; ++i) {
+            long q = nb((size_t)pos, w, h, kFwd[i]);
+            if (q != -1 && t[q] > tp && t[q] > g[q]) {
+                st_push(&st, (size_t)pos);
+                break;
+            }
+        }
+    }
+    while (st.n) {
+        size_t pos = st.v[--st.n];
+        const float tp = t[pos];
+        for (int i = 0; i < cng; ++i) {
+            long q = nb(pos, w, h, kNbr[i]);
+            if (q != -1 && t[q] > tp && g[q] != t[q]) {
+                t[q] = tp > g[q] ? tp : g[q];
+                st_push(&st, (size_t)q);
+            }
+        }
+    }
+    free(st.v);
+}
+
+/* FillHole / FillPeaks (core/kipl/kipl/include/morphology/morphextrema.h:265-328): marker
+ * = the image on its border, the image maximum (holes) or minimum (peaks) inside. */
+static void extrema_marker(const float *img, size_t w, size_t h, int peaks, float *fm)
+{
+    float mn = img[0], mx = img[0];
+    for (size_t i = 1; i < w * h; ++i) {
+        if (img[i] < mn) mn = img[i];
+        if (img[i] > mx) mx = img[i];
+    }
+    for (size_t i = 0; i < w * h; ++i) fm[i] = peaks ? mn : mx;
+    memcpy(fm, img, w * sizeof(float));
+    memcpy(fm + (h - 1) * w, img + (h - 1) * w, w * sizeof(float));
+    for (size_t r = 1; r + 1 < h; ++r) {
+        fm[r * w] = img[r * w];
+        fm[r * w + w - 1] = img[r * w + w - 1];
+    }
+}
+
+void orc_fill_hole(const float *img, size_t w, size_t h, int conn8, float *out)
+{
+    float *fm = (float *)malloc(w * h * sizeof(float));
+    extrema_marker(img, w, h, 0, fm);
+    orc_rec_erosion(img, fm, w, h, conn8, out);
+    free(fm);
+}
+
+int orc_fill_peaks(const float *img, size_t w, size_t h, int conn8, float *out)
+{
+    float *fm = (float *)malloc(w * h * sizeof(float));
+    extrema_marker(img, w, h, 1, fm);
+    int rc = orc_rec_dilation(img, fm, w, h, conn8, out);
+    free(fm);
+    return rc;
+}
+
+/* The forward raster scan of RecByDilation alone (the marker after :207-215): exposed so
+ * the GPU's border-band replay can be checked directly. */
+void orc_fill_peaks_forward(const float *img, size_t w, size_t h, int conn8, float *t)
+{
+    float *fm = (float *)malloc(w * h * sizeof(float));
+    extrema_marker(img, w, h, 1, fm);
+    memcpy(t, fm, w * h * sizeof(float));
+    const int cpm = conn8 ? 5 : 3;
+    for (size_t pos = 0; pos < w * h; ++pos) {
+        float mx = t[pos];
+        for (int i = 1; i < cpm; ++i) {
+            long q = nb(pos, w, h, kBwd[i]);
+            if (q != -1 && t[q] > mx) mx = fm[q];
+        }
+        t[pos] = mx < img[pos] ? mx : img[pos];
+    }
+    free(fm);
+}
+
+/* ------------------------------------------------------------- MorphSpotClean */
+
+/* MorphSpotClean::PadEdges (core/algorithms/ImagingAlgorithms/src/MorphSpotClean.cpp:264-300):
+ * margin 5, zero columns, the first/last 5 rows mirrored, then an in-place sliding median of
+ * `edge` samples along the first and the last padded row. */
+static void pad_edges(const float *img, size_t w, size_t h, size_t edge, float *p)
+{
+    const size_t m = 5, pw = w + 2 * m, ph = h + 2 * m;
+    memset(p, 0, pw * ph * sizeof(float));
+    for (size_t i = 0; i < h; ++i) memcpy(p + (i + m) * pw + m, img + i * w, w * sizeof(float));
+    for (size_t i = 0; i < m; ++i) {
+        memcpy(p + (m - 1 - i) * pw + m, img + i * w, w * sizeof(float));
+        memcpy(p + (ph - m + i) * pw + m, img + (h - 1 - i) * w, w * sizeof(float));
+    }
+    const size_t l2 = edge / 2, n = pw - l2;
+    float *buf = (float *)malloc(edge * sizeof(float));
+    for (int e = 0; e < 2; ++e) {
+        float *row = p + (e ? (ph - 1) * pw : 0);
+        for (size_t i = l2; i < n; ++i) {
+            memcpy(buf, row + i - l2, edge * sizeof(float));
+            row[i] = median_f(buf, edge);
+        }
+    }
+    free(buf);
+}
+
+/* kipl::math::SigmoidWeights (core/kipl/kipl/include/math/core/mathfunctions.hpp:92-99) */
+static float sigmoid_weights(float val, float a, float b, float level, float width)
+{
+    float w = 1.0f / (1.0f + expf((level - val) / width));
+    return a + (b - a) * w;
+}
+
+enum { ORC_DETECT_HOLES = 0, ORC_DETECT_PEAKS = 1, ORC_DETECT_BOTH = 2 };
+
+/* MorphSpotClean::process with MorphCleanReplace (MorphSpotClean.cpp:41-175) on one image
+ * [h][w]: optional inf/NaN replacement and clamping, padding, FillHole / FillPeaks /
+ * both (FillHole of the negated image for peaks), threshold replacement (sigma == 0) or
+ * sigmoid blend, unpadding. Returns -1 on a reconstruction error. */
+int orc_morphspotclean(float *img, size_t w, size_t h, int detect, int conn8, const float *th, const float *sigma,
+                       size_t edge, int clamp, float minlevel, float maxlevel, int removeinfnan)
+{
+    const size_t n0 = w * h;
+    if (removeinfnan) {
+        float mx = -3.402823466e38f;
+        for (size_t i = 0; i < n0; ++i)
+            if (isfinite(img[i]) && mx < img[i]) mx = img[i];
+        for (size_t i = 0; i < n0; ++i)
+            if (!isfinite(img[i])) img[i] = mx;
+    }
+    if (clamp)
+        for (size_t i = 0; i < n0; ++i) {
+            if (img[i] < minlevel) img[i] = minlevel;
+            else if (img[i] > maxlevel) img[i] = maxlevel;
+        }
+    const size_t pw = w + 10, ph = h + 10, n = pw * ph;
+    float *p = (float *)malloc(n * sizeof(float));
+    float *holes = (float *)malloc(n * sizeof(float));
+    float *peaks = (float *)malloc(n * sizeof(float));
+    pad_edges(img, w, h, edge, p);
+    int rc = 0;
+    if (detect == ORC_DETECT_HOLES || detect == ORC_DETECT_BOTH) orc_fill_hole(p, pw, ph, conn8, holes);
+    if (detect == ORC_DETECT_PEAKS) rc = orc_fill_peaks(p, pw, ph, conn8, peaks);
+    if (detect == ORC_DETECT_BOTH) {
+        for (size_t i = 0; i < n; ++i) p[i] = -p[i];
+        orc_fill_hole(p, pw, ph, conn8, peaks);
+        for (size_t i = 0; i < n; ++i) {
+            p[i] = -p[i];
+            peaks[i] = -peaks[i];
+        }
+    }
+    if (rc == 0) {
+        if (sigma[0] == 0.0f && sigma[1] == 0.0f) {
+            for (size_t i = 0; i < n; ++i) {
+                const float val = p[i];
+                if ((detect == ORC_DETECT_HOLES || detect == ORC_DETECT_BOTH) && th[0] < fabsf(val - holes[i]))
+                    p[i] = holes[i];
+                if ((detect == ORC_DETECT_PEAKS || detect == ORC_DETECT_BOTH) && th[1] < fabsf(peaks[i] - val))
+                    p[i] = peaks[i];
+            }
+        } else {
+            for (size_t i = 0; i < n; ++i) {
+                const float val = p[i];
+                if (detect == ORC_DETECT_HOLES)
+                    p[i] = sigmoid_weights(holes[i] - val, val, holes[i], th[0], sigma[0]);
+                else if (detect == ORC_DETECT_PEAKS)
+                    p[i] = sigmoid_weights(val - peaks[i], val, peaks[i], th[1], sigma[1]);
+                else {
+                    const float dp = val - peaks[i], dh = holes[i] - val;
+                    if (fabsf(dh) < fabsf(dp))
+                        p[i] = sigmoid_weights(dp, val, peaks[i], th[0], sigma[0]);
+                    else
+                        p[i] = sigmoid_weights(dh, val, holes[i], th[1], sigma[1]);
+                }
+            }
+        }
+        for (size_t i = 0; i < h; ++i) memcpy(img + i * w, p + (i + 5) * pw + 5, w * sizeof(float));
+    }
+    free(p);
+    free(holes);
+    free(peaks);
+    return rc;
+}

@@ -75,6 +75,15 @@ int orc_fdk_bp(const float *filtered, size_t nu, size_t nv, size_t nproj, const 
 void orc_fdk_ramp(float *img, size_t width, size_t height);
 void orc_fdk_projmatrix(const orc_fdk_geom *g, size_t nu, float angle, float *pm /*12*/);
 
+/* kipl morphology and MorphSpotClean (core/kipl/kipl/include/morphology/morphgeo.h,
+ * morphextrema.h; core/algorithms/ImagingAlgorithms/src/MorphSpotClean.cpp). Images [h][w]. */
+int orc_rec_dilation(const float *g, const float *f, size_t w, size_t h, int conn8, float *out);
+void orc_rec_erosion(const float *g, const float *f, size_t w, size_t h, int conn8, float *out);
+void orc_fill_hole(const float *img, size_t w, size_t h, int conn8, float *out);
+int orc_fill_peaks(const float *img, size_t w, size_t h, int conn8, float *out);
+void orc_fill_peaks_forward(const float *img, size_t w, size_t h, int conn8, float *out);
+int orc_morphspotclean(float *img, size_t w, size_t h, int detect, int conn8, const float *th, const float *sigma,
+                       size_t edge, int clamp, float minlevel, float maxlevel, int removeinfnan);
 
 #ifdef __cplusplus
 }

@@ -126,3 +126,42 @@ def test_frame_dose(ref_lib):
         r = np.asarray(roi, np.uintp)
         ref = O.ref().ref_frame_dose(O._p(frame), O._sz(30), O._p(r, O._SZ))
         assert O.frame_dose(frame, roi) == pytest.approx(ref, abs=0) or O.frame_dose(frame, roi) == ref
+
+
+@pytest.mark.parametrize("detect", ["holes", "peaks", "both"])
+@pytest.mark.parametrize("conn8", [True, False])
+@pytest.mark.parametrize("sigma", [(0.0, 0.0), (0.05, 0.02)])
+def test_morphspotclean_bit_exact(ref_lib, detect, conn8, sigma):
+    rng = _rng(70)
+    for t in range(6):
+        h, w = rng.integers(5, 40, 2)  # the reference reads outside images of fewer than 5 rows
+        img = rng.standard_normal((h, w)).astype(np.float32)
+        if t % 2:
+            img = np.round(img * 3).astype(np.float32)  # plateaus and ties
+        e = int(rng.choice([3, 5, 9]))
+        a = O.morphspotclean(img, detect, conn8, (0.5, 0.4), sigma, edge=e)
+        b = O.morphspotclean(img, detect, conn8, (0.5, 0.4), sigma, edge=e, use_ref=True)
+        assert np.array_equal(a, b)
+
+
+def test_morphspotclean_clamp_infnan(ref_lib):
+    rng = _rng(71)
+    img = rng.standard_normal((12, 20)).astype(np.float32) * 5
+    img[3, 4] = np.inf
+    img[7, 9] = np.nan
+    a = O.morphspotclean(img, "peaks", True, (0.5, 0.5), (0.0, 0.0), clamp=True, minlevel=-2, maxlevel=3,
+                         removeinfnan=True)
+    b = O.morphspotclean(img, "peaks", True, (0.5, 0.5), (0.0, 0.0), clamp=True, minlevel=-2, maxlevel=3,
+                         removeinfnan=True, use_ref=True)
+    assert np.array_equal(a, b)
+
+
+def test_morphspotclean_module_defaults(ref_lib):
+    """MorphSpotCleanModule's single-threaded path uses the cleaner's edge length 9, whatever
+    `edgesmooth` says (MorphSpotCleanModule.cpp:142-181)."""
+    rng = _rng(72)
+    proj = (rng.standard_normal((3, 16, 24)) * 0.2 + 1).astype(np.float32)
+    proj[:, 5, 7] = 5.0
+    a = O.ref_morphspotclean_module(proj, edgesmooth=5)
+    b = O.morphspotclean(proj, "peaks", False, (0.1, 0.1), (0.01, 0.01), edge=9)
+    assert np.array_equal(a, b)
