@@ -19,6 +19,7 @@
 // bit-reversed out) and the crop window is gathered out. Twiddles are a float2 table
 // exp(-2 pi i k / N), k < N/2, built in double on the host.
 #include "mr_common.cuh"
+#include "mr_fft.cuh"
 
 #include <algorithm>
 #include <cctype>
@@ -56,13 +57,6 @@ struct RowFilterArgs {
     float scale;     // projection filter: pi/(4*N/2); FDK: 1/padwidth
     float post1, post2; // FDK: sad_sid_2, scale (two sequential products); 1 for the projection filter
 };
-
-__device__ __forceinline__ unsigned bitrev(unsigned x, int logn) { return __brev(x) >> (32 - logn); }
-
-__device__ __forceinline__ float2 cmul(float2 a, float2 b)
-{
-    return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
 
 // Value of padded position p (0 <= p < n) of one row, reference padding rules.
 __device__ __forceinline__ float padded_value(const RowFilterArgs &a, const float *row, size_t rowidx, int p)
@@ -123,57 +117,17 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
     for (int p = threadIdx.x; p < n; p += blockDim.x) {
         float x0 = padded_value(a, row0, r0, p);
         float x1 = has1 ? padded_value(a, row1, r1, p) : 0.0f;
-        buf[bitrev(p, a.logn)] = make_float2(x0, x1);
+        buf[fft_bitrev(p, a.logn)] = make_float2(x0, x1);
     }
     __syncthreads();
 
-    // forward DIT, natural-order output
-    const int nh = n >> 1;
-    for (int s = 1; s <= a.logn; ++s) {
-        const int half = 1 << (s - 1);
-        const int tstride = n >> s;
-        for (int b = threadIdx.x; b < nh; b += blockDim.x) {
-            const int j = b & (half - 1);
-            const int i0 = ((b >> (s - 1)) << s) + j;
-            const int i1 = i0 + half;
-            const float2 w = __ldg(a.twiddle + j * tstride);
-            const float2 x = buf[i0];
-            const float2 t = cmul(buf[i1], w);
-            buf[i0] = make_float2(x.x + t.x, x.y + t.y);
-            buf[i1] = make_float2(x.x - t.x, x.y - t.y);
-        }
-        __syncthreads();
-    }
-
-    // frequency response (real, even)
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        const float h = __ldg(a.response + k);
-        const float2 v = buf[k];
-        buf[k] = make_float2(v.x * h, v.y * h);
-    }
-    __syncthreads();
-
-    // inverse DIF (conjugate twiddles), bit-reversed output
-    for (int s = a.logn; s >= 1; --s) {
-        const int half = 1 << (s - 1);
-        const int tstride = n >> s;
-        for (int b = threadIdx.x; b < nh; b += blockDim.x) {
-            const int j = b & (half - 1);
-            const int i0 = ((b >> (s - 1)) << s) + j;
-            const int i1 = i0 + half;
-            const float2 w = __ldg(a.twiddle + j * tstride);
-            const float2 x = buf[i0];
-            const float2 y = buf[i1];
-            buf[i0] = make_float2(x.x + y.x, x.y + y.y);
-            const float2 d = make_float2(x.x - y.x, x.y - y.y);
-            buf[i1] = make_float2(d.x * w.x + d.y * w.y, d.y * w.x - d.x * w.y); // d * conj(w)
-        }
-        __syncthreads();
-    }
+    fft_forward_dit(buf, n, a.logn, a.twiddle);
+    fft_apply_response(buf, n, a.response);
+    fft_inverse_dif(buf, n, a.logn, a.twiddle);
 
     // crop and write
     for (int i = threadIdx.x; i < a.nu; i += blockDim.x) {
-        const float2 v = buf[bitrev(i + a.ninsert, a.logn)];
+        const float2 v = buf[fft_bitrev(i + a.ninsert, a.logn)];
         float y0 = __fmul_rn(v.x, a.scale);
         float y1 = __fmul_rn(v.y, a.scale);
         if (a.mode == kPadProjFilter) {

@@ -320,6 +320,63 @@ class MorphSpotCleanModule:
                                 minlevel=self.m_fMinLevel, maxlevel=self.m_fMaxLevel, removeinfnan=False)
 
 
+# ------------------------------------------------------------------ WaveletRingClean
+
+
+def stripe_filter(sino: torch.Tensor, wname: str = "daub15", decnum: int = 2, sigma: float = 0.05) -> torch.Tensor:
+    """ImagingAlgorithms::StripeFilter::process (VerticalComponentFFT) in place on sinograms
+    (n, ntheta, nu) or (ntheta, nu)."""
+    _require_cuda(sino, "sinogram")
+    ntheta, nu = sino.shape[-2:]
+    n = sino.numel() // (ntheta * nu)
+    check(L.lib().mr_stripefilter(sino.data_ptr(), nu, ntheta, n, wname.encode(), int(decnum), float(sigma),
+                                  _stream()))
+    return sino
+
+
+class WaveletRingClean:
+    """WaveletRingClean (StdPreprocModules/src/WaveletRingClean.cpp:17-146). As in the
+    reference, `method` is read but every sinogram is filtered with VerticalComponentFFT."""
+
+    def __init__(self):
+        self.m_sWName = "daub15"
+        self.m_fSigma = 0.05
+        self.m_nDecNum = 2
+        self.m_bParallelProcessing = False
+        self.m_eCleanMethod = "verticalfft"
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        self.m_sWName = _get(parameters, "wname")
+        self.m_fSigma = float(np.float32(_get(parameters, "sigma")))
+        self.m_nDecNum = int(_get(parameters, "decnum"))
+        self.m_bParallelProcessing = _string2bool(_get(parameters, "parallel"))
+        method = _get(parameters, "method")
+        if method not in ("verticalzero", "verticalfft"):
+            raise ReconException(f"Could not translate string ({method}) to stripe filter operation")
+        self.m_eCleanMethod = method
+        return 0
+
+    def GetParameters(self) -> dict:
+        return {"wname": self.m_sWName, "sigma": str(self.m_fSigma), "decnum": str(self.m_nDecNum),
+                "parallel": "true" if self.m_bParallelProcessing else "false", "method": self.m_eCleanMethod}
+
+    def SetROI(self, roi) -> bool:
+        return False
+
+    def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
+        return self.ProcessCore(img, coeff if coeff is not None else {})
+
+    def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
+        _require_cuda(img, "projections")
+        nproj, nv, nu = img.shape
+        st = L.lib().mr_waveletringclean(img.data_ptr(), nu, nv, nproj, self.m_sWName.encode(), self.m_nDecNum,
+                                         self.m_fSigma, _stream())
+        if st != L.MR_OK:
+            raise ReconException("Failed to process the projections using stripe filter: " +
+                                 L.lib().mr_last_error().decode())
+        return img
+
+
 # ------------------------------------------------------------ ProjectionFilterSingle
 
 

@@ -96,6 +96,26 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
                             float maxlevel, int removeinfnan, void *stream);
 
 /* ---------------------------------------------------------------------------------
+ * Wavelet-FFT ring cleaning
+ * mr_stripefilter replaces ImagingAlgorithms::StripeFilter::process with
+ * VerticalComponentFFT (core/algorithms/ImagingAlgorithms/src/StripeFilter.cpp:68-250,
+ * kipl::wavelets::WaveletTransform core/kipl/kipl/include/wavelets/core/wavelets.hpp:452-862)
+ * on nsino contiguous sinograms [nsino][ntheta][nu], in place.
+ * mr_waveletringclean replaces WaveletRingClean::ProcessCore (frameworks/tomography/
+ * Preprocessing/StdPreprocModules/src/WaveletRingClean.cpp:63-103): every detector row's
+ * sinogram of projections [nproj][nv][nu], in place.
+ * wname: "daub1".."daub30" (Daubechies filters computed from their definition; daub3 keeps the
+ * reference's sign of its fifth coefficient); decnum: decomposition levels; sigma: damping
+ * width. Scratch: up to about 1 GiB per call.
+ * mr_wavelet_kernel (host) returns begin/end and the four filters (analysis H, analysis G,
+ * synthesis H, synthesis G; 4*(end-begin+1) floats) of WaveletKernel<float>. */
+mr_status mr_wavelet_kernel(const char *wname, int *begin, int *end, float *taps_h);
+mr_status mr_stripefilter(float *sino_d, size_t nu, size_t ntheta, size_t nsino, const char *wname, int decnum,
+                          float sigma, void *stream);
+mr_status mr_waveletringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, const char *wname, int decnum,
+                              float sigma, void *stream);
+
+/* ---------------------------------------------------------------------------------
  * ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:78-376)
  * Plan = ProjectionFilterBase::Configure/BuildFilter/PreparePadding (:78-93,254-299,364-376):
  *   nfft = 2^(ceil(log2 nu) + paddingdoubler); filter over bins 0..nfft/2-1.

@@ -388,3 +388,71 @@ def fill_peaks_forward(img, conn8=True) -> np.ndarray:
     out = np.empty_like(img)
     orc().orc_fill_peaks_forward(_p(img), _sz(img.shape[1]), _sz(img.shape[0]), int(conn8), _p(out))
     return out
+
+
+# ------------------------------------------------------------------------ StripeFilter
+
+_DAUB = None
+
+
+def daubechies(n: int) -> np.ndarray:
+    """dbN scaling filter (float64) from the table generated from the spectral factorisation
+    (imagingsuite_b200/csrc/gen_daubechies.py)."""
+    global _DAUB
+    if _DAUB is None:
+        import re
+
+        src = open(os.path.join(os.path.dirname(_HERE), "imagingsuite_b200", "csrc", "mr_daubechies.h")).read()
+        _DAUB = [np.array([float(v) for v in row.split(",")]) for row in re.findall(r"\{([^{}]*)\},", src)]
+    return _DAUB[n - 1]
+
+
+def wavelet_kernel(name: str):
+    """WaveletKernel<float>::CopyKernel (wavelets.hpp:387-405) for 'daubN': returns
+    (begin, end, float32 array [4, K] = analysis H, analysis G, synthesis H, synthesis G).
+    The reference's daub3 table has the sign of its fifth coefficient flipped; it is
+    reproduced here."""
+    if not name.startswith("daub"):
+        raise ValueError(f"unsupported wavelet {name}")
+    n = int(name[4:])
+    k = daubechies(n).copy()
+    if n == 3:
+        k[4] = -k[4]
+    end = len(k) - 1
+    tH = np.array([k[end - i] for i in range(len(k))])
+    sgn = -1.0
+    tG = np.empty_like(k)
+    for i in range(len(k)):
+        tG[i] = sgn * k[i]
+        sgn = -sgn
+    sH = k.copy()
+    sG = np.array([tG[end - i] for i in range(len(k))])
+    return 0, end, np.stack([tH, tG, sH, sG]).astype(np.float32)
+
+
+def stripefilter(sino, wname="daub15", scale=2, sigma=0.05, use_ref=False) -> np.ndarray:
+    """StripeFilter::process (VerticalComponentFFT) on one sinogram (ntheta, nu)."""
+    out = np.array(sino, dtype=np.float32, copy=True, order="C")
+    h, w = out.shape
+    if use_ref:
+        _check_ref(ref().ref_stripefilter(_p(out), _sz(w), _sz(h), wname.encode(), int(scale), _f(sigma), 1))
+    else:
+        b, e, k = wavelet_kernel(wname)
+        k = np.ascontiguousarray(k)
+        if orc().orc_stripefilter(_p(out), _sz(w), _sz(h), _p(k), b, e, int(scale), _f(sigma)) != 0:
+            raise RuntimeError("Image smaller than wavelet kernel size")
+    return out
+
+
+def waveletringclean(proj, wname="daub15", decnum=2, sigma=0.05, use_ref=False) -> np.ndarray:
+    """WaveletRingClean::ProcessSingle on projections (nproj, nv, nu): every detector row's
+    sinogram through StripeFilter."""
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    nproj, nv, nu = out.shape
+    if use_ref:
+        _check_ref(ref().ref_waveletringclean(_p(out), _sz(nu), _sz(nv), _sz(nproj), wname.encode(), int(decnum),
+                                              _f(sigma)))
+        return out
+    for j in range(nv):
+        out[:, j, :] = stripefilter(out[:, j, :], wname, decnum, sigma)
+    return out

@@ -925,3 +925,166 @@ int orc_morphspotclean(float *img, size_t w, size_t h, int detect, int conn8, co
     free(peaks);
     return rc;
 }
+
+/* ------------------------------------------------------------ StripeFilter */
+
+/* WaveletTransform::pad_mirror (core/kipl/kipl/include/wavelets/core/wavelets.hpp:648-667):
+ * value at position p of the mirrored buffer (the odd-length extra sample is never read). */
+static float mirror_at(const float *src, int n, int fw, int p)
+{
+    if (p < fw) return src[fw - 1 - p];
+    if (p < fw + n) return src[p - fw];
+    return src[n - 1 - (p - fw - n)];
+}
+
+/* One analysis level (wavelets.hpp:474-600): rows with `hr`, columns with `vc`, output
+ * (dx, dy) = ((sx + K - 1 + (sx & 1))/2, (sy + K - 1 + (sy & 1))/2); each output is the sum
+ * over the taps in order from 0. */
+static void dwt_pass(const float *src, int sx, int sy, const float *hr, const float *vc, int begin, int end, float *dst,
+                     int dx, int dy)
+{
+    const int fw = end - begin + 1;
+    float *tmp = (float *)calloc((size_t)dx * sy, sizeof(float));
+    for (int y = 0; y < sy; ++y)
+        for (int k = 0; k < dx; ++k) {
+            float acc = 0.0f;
+            for (int j = begin; j <= end; ++j) acc = acc + hr[j] * mirror_at(src + (size_t)y * sx, sx, fw, fw + 2 * k - j + 1);
+            tmp[(size_t)y * dx + k] = acc;
+        }
+    float *col = (float *)malloc(sy * sizeof(float));
+    for (int x = 0; x < dx; ++x) {
+        for (int y = 0; y < sy; ++y) col[y] = tmp[(size_t)y * dx + x];
+        for (int k = 0; k < dy; ++k) {
+            float acc = 0.0f;
+            for (int m = begin; m <= end; ++m) acc = acc + vc[m] * mirror_at(col, sy, fw, fw + 2 * k - m + 1);
+            dst[(size_t)k * dx + x] = acc;
+        }
+    }
+    free(col);
+    free(tmp);
+}
+
+/* value at position q of pad_mirror(dyadup(src, n), 2n, fw) (wavelets.hpp:741-748, 771-780) */
+static float up_at(const float *src, int n, int fw, int q, int stride)
+{
+    int t;
+    if (q < fw) t = fw - 1 - q;
+    else if (q < fw + 2 * n) t = q - fw;
+    else t = 2 * n - 1 - (q - fw - 2 * n);
+    return (t & 1) ? 0.0f : src[(size_t)(t / 2) * stride];
+}
+
+/* WaveletTransform::upsconvRC (wavelets.hpp:750-862): src (w, h) -> dst (dx, dy). */
+static void upsconv(const float *src, int w, int h, float *dst, int dx, int dy, const float *kh, const float *kv,
+                    int begin, int end)
+{
+    const int fw = end - begin + 1, c = fw - 2;
+    float *rows = (float *)calloc((size_t)dx * h, sizeof(float));
+    for (int y = 0; y < h; ++y)
+        for (int k = 0; k < dx; ++k) {
+            float acc = 0.0f;
+            for (int m = begin; m <= end; ++m) acc = acc + up_at(src + (size_t)y * w, w, fw, fw + k + c - m, 1) * kh[m];
+            rows[(size_t)y * dx + k] = acc;
+        }
+    for (int x = 0; x < dx; ++x)
+        for (int k = 0; k < dy; ++k) {
+            float acc = 0.0f;
+            for (int m = begin; m <= end; ++m) acc = acc + up_at(rows + x, h, fw, fw + k + c - m, dx) * kv[m];
+            dst[(size_t)k * dx + x] = acc;
+        }
+    free(rows);
+}
+
+/* kipl::math::fft::NextPower2 (core/kipl/kipl/src/fft/zeropadding.cpp:10-15) */
+static size_t next_power2(size_t n)
+{
+    const double logtwo = log(2.0);
+    return (size_t)floor(exp(logtwo * ceil(log((double)n) / logtwo)) + 0.5);
+}
+
+/* StripeFilter::process with VerticalComponentFFT (core/algorithms/ImagingAlgorithms/src/
+ * StripeFilter.cpp:68-135,214-250) on one sinogram [ntheta][nu]. kern: the four float
+ * filters of WaveletKernel (analysis H, analysis G, synthesis H, synthesis G), each
+ * end-begin+1 long. Returns -1 when the image is smaller than the kernel. */
+int orc_stripefilter(float *img, size_t nu, size_t ntheta, const float *kern, int begin, int end, int nlevels,
+                     float sigma)
+{
+    const int K = end - begin + 1;
+    const float *tH = kern, *tG = kern + K, *sH = kern + 2 * K, *sG = kern + 3 * K;
+    int sx[17], sy[17];
+    float *a[17], *h[17], *v[17], *d[17];
+    sx[0] = (int)nu;
+    sy[0] = (int)ntheta;
+    a[0] = img;
+    for (int l = 0; l < nlevels; ++l) {
+        if (sx[l] < K || sy[l] < K) {
+            for (int q = 1; q <= l; ++q) { free(a[q]); free(h[q]); free(v[q]); free(d[q]); }
+            return -1;
+        }
+        sx[l + 1] = (sx[l] + K - 1 + (sx[l] & 1)) / 2;
+        sy[l + 1] = (sy[l] + K - 1 + (sy[l] & 1)) / 2;
+        size_t n = (size_t)sx[l + 1] * sy[l + 1];
+        a[l + 1] = (float *)malloc(n * sizeof(float));
+        h[l + 1] = (float *)malloc(n * sizeof(float));
+        v[l + 1] = (float *)malloc(n * sizeof(float));
+        d[l + 1] = (float *)malloc(n * sizeof(float));
+        dwt_pass(a[l], sx[l], sy[l], tH, tH, begin, end, a[l + 1], sx[l + 1], sy[l + 1]);
+        dwt_pass(a[l], sx[l], sy[l], tH, tG, begin, end, h[l + 1], sx[l + 1], sy[l + 1]);
+        dwt_pass(a[l], sx[l], sy[l], tG, tH, begin, end, v[l + 1], sx[l + 1], sy[l + 1]);
+        dwt_pass(a[l], sx[l], sy[l], tG, tG, begin, end, d[l + 1], sx[l + 1], sy[l + 1]);
+    }
+    /* FilterVerticalStripes on every level's v band (:114-135) with CreateFilterWindow (:68-81) */
+    const float s = -1.0f / (2.0f * sigma * sigma);
+    for (int l = 0; l < nlevels; ++l) {
+        const size_t L = next_power2((size_t)(1.25 * (double)(int)ntheta) >> l);
+        const size_t N = 2 * L;
+        const float scale = 1.0f / (2.0f * L);
+        float *damp = (float *)malloc(N * sizeof(float));
+        for (size_t i = 0; i < N; ++i) {
+            float w = (float)i * scale;
+            damp[i] = (1.0f - expf(w * w * s)) * scale;
+        }
+        double *re = (double *)malloc(N * sizeof(double)), *im = (double *)malloc(N * sizeof(double));
+        float *band = v[l + 1];
+        const int bw = sx[l + 1], bh = sy[l + 1];
+        for (int x = 0; x < bw; ++x) {
+            for (size_t i = 0; i < N; ++i) { re[i] = (int)i < bh ? band[(size_t)i * bw + x] : 0.0; im[i] = 0.0; }
+            fft_c2c(re, im, N, -1);
+            for (size_t i = 0; i <= N / 2; ++i) {
+                re[i] = (double)(float)((float)re[i] * damp[i]);
+                im[i] = (double)(float)((float)im[i] * damp[i]);
+            }
+            im[0] = 0.0;
+            im[N / 2] = 0.0;
+            for (size_t k = 1; k < N / 2; ++k) { re[N - k] = re[k]; im[N - k] = -im[k]; }
+            fft_c2c(re, im, N, +1);
+            for (int i = 0; i < bh; ++i) band[(size_t)i * bw + x] = (float)re[i];
+        }
+        free(re);
+        free(im);
+        free(damp);
+    }
+    /* synthesize (wavelets.hpp:603-645): approximation of level l from level l+1 */
+    for (int l = nlevels - 1; l >= 0; --l) {
+        const int dx = l == 0 ? 2 * sx[1] : sx[l], dy = l == 0 ? 2 * sy[1] : sy[l];
+        const size_t n = (size_t)dx * dy;
+        float *acc = (float *)malloc(n * sizeof(float)), *tmp = (float *)malloc(n * sizeof(float));
+        const int w = sx[l + 1], hh = sy[l + 1];
+        upsconv(a[l + 1], w, hh, acc, dx, dy, sH, sH, begin, end);
+        upsconv(h[l + 1], w, hh, tmp, dx, dy, sH, sG, begin, end);
+        for (size_t i = 0; i < n; ++i) acc[i] += tmp[i];
+        upsconv(v[l + 1], w, hh, tmp, dx, dy, sG, sH, begin, end);
+        for (size_t i = 0; i < n; ++i) acc[i] += tmp[i];
+        upsconv(d[l + 1], w, hh, tmp, dx, dy, sG, sG, begin, end);
+        for (size_t i = 0; i < n; ++i) acc[i] += tmp[i];
+        if (l == 0) {
+            for (size_t y = 0; y < ntheta; ++y) memcpy(img + y * nu, acc + y * (size_t)dx, nu * sizeof(float));
+        } else {
+            memcpy(a[l], acc, n * sizeof(float));
+        }
+        free(acc);
+        free(tmp);
+    }
+    for (int q = 1; q <= nlevels; ++q) { free(a[q]); free(h[q]); free(v[q]); free(d[q]); }
+    return 0;
+}

@@ -85,6 +85,12 @@ void orc_fill_peaks_forward(const float *img, size_t w, size_t h, int conn8, flo
 int orc_morphspotclean(float *img, size_t w, size_t h, int detect, int conn8, const float *th, const float *sigma,
                        size_t edge, int clamp, float minlevel, float maxlevel, int removeinfnan);
 
+/* StripeFilter / WaveletRingClean (core/algorithms/ImagingAlgorithms/src/StripeFilter.cpp,
+ * core/kipl/kipl/include/wavelets/core/wavelets.hpp). kern: analysis H, analysis G,
+ * synthesis H, synthesis G, each end-begin+1 floats. Sinogram [ntheta][nu], in place. */
+int orc_stripefilter(float *img, size_t nu, size_t ntheta, const float *kern, int begin, int end, int nlevels,
+                     float sigma);
+
 #ifdef __cplusplus
 }
 #endif

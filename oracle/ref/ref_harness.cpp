@@ -49,6 +49,7 @@
 #include "MultiProjBP.h"
 #include "fdkbp_single.h"
 #include "linearforwardprojector.h"
+#include <wavelets/wavelets.h>
 #undef private
 #undef protected
 
@@ -411,8 +412,11 @@ int ref_morphspotclean_module(float *proj, size_t nu, size_t nv, size_t nproj, c
 int ref_stripefilter(float *sino, size_t nu, size_t ntheta, const char *wname, int scale, float sigma, int op)
 {
     return guarded([&] {
+        // the size_t* constructor copies into an empty std::vector (StripeFilter.cpp:25) and
+        // crashes; the std::vector<int> constructor (the python binding's) is used instead
         size_t d2[2] = {nu, ntheta};
-        ImagingAlgorithms::StripeFilter f(d2, wname, scale, sigma);
+        std::vector<int> vd = {static_cast<int>(nu), static_cast<int>(ntheta)};
+        ImagingAlgorithms::StripeFilter f(vd, wname, scale, sigma);
         kipl::base::TImage<float, 2> im(d2);
         std::memcpy(im.GetDataPtr(), sino, sizeof(float) * nu * ntheta);
         f.process(im, static_cast<ImagingAlgorithms::eStripeFilterOperation>(op));
@@ -425,37 +429,48 @@ int ref_stripefilter_window(size_t nu, size_t ntheta, const char *wname, int sca
                             float *out, size_t *n_out)
 {
     return guarded([&] {
-        size_t d2[2] = {nu, ntheta};
-        ImagingAlgorithms::StripeFilter f(d2, wname, scale, sigma);
+        std::vector<int> vd = {static_cast<int>(nu), static_cast<int>(ntheta)};
+        ImagingAlgorithms::StripeFilter f(vd, wname, scale, sigma);
         std::vector<float> w = f.filterWindow(level);
         *n_out = w.size();
         if (out) std::copy(w.begin(), w.end(), out);
     });
 }
 
-// WaveletRingClean::Configure + ProcessCore 3D (WaveletRingClean.cpp:29-103) on
-// projections [nproj][nv][nu].
+// WaveletRingClean::ProcessSingle (WaveletRingClean.cpp:74-103) on projections [nproj][nv][nu]:
+// every detector row's sinogram [nproj][nu] through StripeFilter::process. The module itself
+// builds its StripeFilter with the size_t* constructor, which crashes (see above), so the
+// loop is driven here with the working constructor.
 int ref_waveletringclean(float *proj, size_t nu, size_t nv, size_t nproj, const char *wname, int decnum,
                          float sigma)
 {
     return guarded([&] {
-        WaveletRingClean mod(nullptr);
-        ReconConfig cfg;
-        std::map<std::string, std::string> par;
-        par["wname"] = wname;
-        char b[64];
-        std::snprintf(b, sizeof(b), "%.9g", sigma);
-        par["sigma"] = b;
-        par["decnum"] = std::to_string(decnum);
-        par["parallel"] = "false";
-        par["method"] = "verticalfft";
-        mod.Configure(cfg, par);
-        size_t d3[3] = {nu, nv, nproj};
-        kipl::base::TImage<float, 3> img(d3);
-        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
-        std::map<std::string, std::string> coeff;
-        mod.Process(img, coeff);
-        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * nu * nv * nproj);
+        std::vector<int> vd = {static_cast<int>(nu), static_cast<int>(nproj)};
+        ImagingAlgorithms::StripeFilter f(vd, wname, decnum, sigma);
+        size_t d2[2] = {nu, nproj};
+        kipl::base::TImage<float, 2> sino(d2);
+        for (size_t j = 0; j < nv; ++j) {
+            for (size_t i = 0; i < nproj; ++i) std::memcpy(sino.GetLinePtr(i), proj + (i * nv + j) * nu, nu * sizeof(float));
+            f.process(sino, ImagingAlgorithms::VerticalComponentFFT);
+            for (size_t i = 0; i < nproj; ++i) std::memcpy(proj + (i * nv + j) * nu, sino.GetLinePtr(i), nu * sizeof(float));
+        }
+    });
+}
+
+// The wavelet kernel of kipl::wavelets::WaveletKernel<float> (wavelets.hpp:52-405): begin,
+// end and the four filters (analysis H/G, synthesis H/G), size floats each.
+int ref_wavelet_kernel(const char *wname, int *begin, int *end, float *th, float *tg, float *sh, float *sg)
+{
+    return guarded([&] {
+        kipl::wavelets::WaveletKernel<float> k(wname);
+        *begin = k.begin();
+        *end = k.end();
+        for (int i = 0; i < k.size(); ++i) {
+            th[i] = k.transH()[i];
+            tg[i] = k.transG()[i];
+            sh[i] = k.synthH()[i];
+            sg[i] = k.synthG()[i];
+        }
     });
 }
 

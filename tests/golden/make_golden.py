@@ -42,6 +42,13 @@ def main(ref_root="/root/reference"):
     out["spot_peaks_conn4_thr"] = O.morphspotclean(spot, "peaks", False, (0.1, 0.1), (0.0, 0.0), edge=9, use_ref=True)
     out["spot_both_conn8_sig"] = O.morphspotclean(spot, "both", True, (1.0, 1.0), (0.05, 0.05), edge=9, use_ref=True)
 
+    # StripeFilter on the reference's sinogram (testBindStripeFilter.py: daub7, 2 levels, sigma 0.1)
+    wood = tiff(os.path.join(data, "woodsino_0200.tif"))
+    out["wood_input"] = wood
+    crop = wood[100:260, 50:250].copy()
+    out["wood_crop_daub15_2_005"] = O.stripefilter(crop, "daub15", 2, 0.05, use_ref=True)
+    out["wood_crop_daub3_3_002"] = O.stripefilter(crop, "daub3", 3, 0.02, use_ref=True)
+
     # the 7x7 KAT fixture
     holes = (np.arange(49, dtype=np.float32) / np.float32(10.0)).reshape(7, 7)
     holes.flat[24] = 0.0

@@ -135,3 +135,21 @@ def test_fdk_partials_tilt_not_uniform():
     g.tiltpivot = 5.0
     *_, uni = _partials(g, 32, 24, np.array([0.0, 90.0], np.float32))
     assert uni == 0
+
+
+@pytest.mark.parametrize("n", list(range(1, 31)))
+def test_wavelet_kernel_abi(n):
+    b, e = ctypes.c_int(), ctypes.c_int()
+    taps = np.zeros(4 * 60, np.float32)
+    L.check(L.lib().mr_wavelet_kernel(f"daub{n}".encode(), ctypes.byref(b), ctypes.byref(e),
+                                      taps.ctypes.data_as(L.P_float)))
+    ob, oe, k = O.wavelet_kernel(f"daub{n}")
+    K = oe - ob + 1
+    assert (b.value, e.value) == (ob, oe)
+    assert np.array_equal(taps[: 4 * K].reshape(4, K), k)
+
+
+def test_wavelet_kernel_rejects_unknown():
+    b, e = ctypes.c_int(), ctypes.c_int()
+    assert L.lib().mr_wavelet_kernel(b"haar", ctypes.byref(b), ctypes.byref(e), None) == L.MR_ERR_UNSUPPORTED
+    assert L.lib().mr_wavelet_kernel(b"daub31", ctypes.byref(b), ctypes.byref(e), None) == L.MR_ERR_UNSUPPORTED

@@ -65,3 +65,18 @@ def test_bp_parallel_golden():
 def test_fdk_golden():
     g = O.fdk_geom(300.0, 600.0, (15.5, 11.5), 15.7, (0.2, 0.2), (0.1, 0.1, 0.1))
     assert np.array_equal(O.fdk(G["fdk_input"], G["fdk_angles"], G["fdk_weights"], g), G["fdk_out"])
+
+
+def test_stripefilter_python_test_mse():
+    # core/algorithms/UnitTests/python/testBindStripeFilter.py: daub7, 2 levels, sigma 0.1,
+    # VerticalComponentFFT -> mse(sino, out) == 1.8129678e-05 (rel 1e-6)
+    wood = G["wood_input"]
+    out = O.stripefilter(wood, "daub7", 2, 0.1)
+    mse = float(((wood - out) ** 2).mean())
+    assert np.isclose(mse, 1.8129678e-05, rtol=1e-6)
+
+
+def test_stripefilter_golden_crops():
+    crop = G["wood_input"][100:260, 50:250]
+    assert np.array_equal(O.stripefilter(crop, "daub15", 2, 0.05), G["wood_crop_daub15_2_005"])
+    assert np.array_equal(O.stripefilter(crop, "daub3", 3, 0.02), G["wood_crop_daub3_3_002"])

@@ -165,3 +165,38 @@ def test_morphspotclean_module_defaults(ref_lib):
     a = O.ref_morphspotclean_module(proj, edgesmooth=5)
     b = O.morphspotclean(proj, "peaks", False, (0.1, 0.1), (0.01, 0.01), edge=9)
     assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("n", list(range(1, 16)))
+def test_wavelet_kernels_match_reference(ref_lib, n):
+    """dbN from the spectral factorisation equals the reference's float kernels for N <= 15
+    (daub3 with the reference's sign of h[4]); the reference's daub16..30 tables are less
+    accurate than float and are not reproduced."""
+    import ctypes
+
+    b, e, k = O.wavelet_kernel(f"daub{n}")
+    th = np.zeros(64, np.float32)
+    tg, sh, sg = th.copy(), th.copy(), th.copy()
+    rb, re_ = ctypes.c_int(), ctypes.c_int()
+    assert ref_lib.ref_wavelet_kernel(f"daub{n}".encode(), ctypes.byref(rb), ctypes.byref(re_), O._p(th), O._p(tg),
+                                      O._p(sh), O._p(sg)) == 0
+    K = re_.value - rb.value + 1
+    assert (rb.value, re_.value) == (b, e)
+    for ours, theirs in zip(k, (th, tg, sh, sg)):
+        assert np.array_equal(ours, theirs[:K])
+
+
+@pytest.mark.parametrize("name,levels,sigma", [("daub2", 1, 0.05), ("daub3", 3, 0.02), ("daub7", 2, 0.1),
+                                               ("daub15", 2, 0.05), ("daub5", 3, 0.2)])
+def test_stripefilter_bit_exact(ref_lib, name, levels, sigma):
+    rng = _rng(90)
+    for _ in range(3):
+        h, w = rng.integers(70, 140, 2)
+        s = rng.standard_normal((h, w)).astype(np.float32)
+        assert np.array_equal(O.stripefilter(s, name, levels, sigma), O.stripefilter(s, name, levels, sigma, use_ref=True))
+
+
+def test_waveletringclean_bit_exact(ref_lib):
+    rng = _rng(91)
+    proj = rng.standard_normal((80, 3, 70)).astype(np.float32)
+    assert np.array_equal(O.waveletringclean(proj, "daub7", 2, 0.1), O.waveletringclean(proj, "daub7", 2, 0.1, use_ref=True))
