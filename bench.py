@@ -112,14 +112,21 @@ def make_inputs(w, seed, device):
     return counts, flats, darks
 
 
+def geometry_centres(w):
+    """Piercing point and centre of rotation (pixels), off the pixel grid by fixed fractions as
+    on a real scanner: with both exactly at the detector centre, voxel centres project exactly
+    onto pixel boundaries at 0/90/180/270 degrees and the nearest-neighbour rule then depends
+    on the last bit of the arithmetic."""
+    return ((w["nu"] - 1) / 2.0 + 0.13, (w["nv"] - 1) / 2.0 - 0.21), (w["nu"] - 1) / 2.0 + 0.07
+
+
 def make_config(w):
     from imagingsuite_b200 import modules as M
 
     cfg = M.ReconConfig()
     pi = cfg.ProjectionInfo
     pi.fSOD, pi.fSDD = w["sod"], w["sdd"]
-    pi.fpPoint = ((w["nu"] - 1) / 2.0, (w["nv"] - 1) / 2.0)
-    pi.fCenter = (w["nu"] - 1) / 2.0
+    pi.fpPoint, pi.fCenter = geometry_centres(w)
     pi.fResolution = (w["pitch"], w["pitch"])
     pi.roi = pi.projection_roi = (0, 0, w["nu"], w["nv"])
     pi.nDims = (w["nu"], w["nv"], w["nproj"])
@@ -212,19 +219,21 @@ def run_mr(args):
     weights = np.full(nproj, np.float32(1.0 / nproj), np.float32)
     pipe32 = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="fp32")
     pipe16 = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="bf16")
+    pipeh = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="fp16")
     stream = torch.cuda.current_stream()
 
     sampler = ClockSampler(local)
     sampler.start()
     t32 = time_steps(lambda: pipe32.run_device(counts), args.steps, args.warmup, stream, dctx)
     clocks = sampler.stop()
-    t16 = time_steps(lambda: pipe16.run_device(counts), args.steps, max(3, args.warmup // 2), stream, dctx)
+    t16 = time_steps(lambda: pipe16.run_device(counts), args.steps, args.warmup, stream, dctx)
+    th16 = time_steps(lambda: pipeh.run_device(counts), args.steps, args.warmup, stream, dctx)
 
     # dominant kernel (FDK backprojection) alone, on the launching stream
     fdk = pipe32.fdk
     filt = torch.empty((nproj, nv, nu), device=device)
     proj = pipe32._lognorm_into(counts)
-    wgt, X, Y, Z, s2, sc, uni, box = fdk._geo
+    wgt, X, Y, Z, s2, sc, uni, box, _ = fdk._geo
     st = stream.cuda_stream
     L.check(L.lib().mr_fdk_filter(proj.data_ptr(), nu, nv, nproj, wgt.data_ptr(), s2, sc, L.MR_F32, filt.data_ptr(),
                                   None, st))
@@ -235,24 +244,46 @@ def run_mr(args):
                                            Z.data_ptr(), uni, fdk._mask.data_ptr(), box[0], box[1], 0, vol.data_ptr(), st))
 
     tbp = kernel_time(bp32, stream)
+    # precision form: 16-bit filtered projections through the FP64-derived maps
+    *_, box16, maps = pipe16.fdk._geo
     q16 = torch.empty((nproj, nv, nu), dtype=torch.uint16, device=device)
     qs = torch.empty(nproj, device=device)
-    L.check(L.lib().mr_quantize(filt.data_ptr(), nu * nv, nproj, L.MR_BF16, q16.data_ptr(), qs.data_ptr(), st))
     vol16 = torch.empty((nv, nu, nu), device=device)
-    box16 = pipe16.fdk._geo[-1]
+    tfast = {}
+    for name, dt in (("bf16", L.MR_BF16), ("fp16", L.MR_F16)):
+        L.check(L.lib().mr_quantize(filt.data_ptr(), nu * nv, nproj, dt, q16.data_ptr(), qs.data_ptr(), st))
 
-    def bp16():
-        L.check(L.lib().mr_fdk_backproject(q16.data_ptr(), L.MR_BF16, qs.data_ptr(), nu, nv, nproj, X.data_ptr(),
-                                           Y.data_ptr(), Z.data_ptr(), uni, fdk._mask.data_ptr(), box16[0], box16[1], 0,
-                                           vol16.data_ptr(), st))
+        def bpf(dt=dt):
+            L.check(L.lib().mr_fdk_backproject_fast(q16.data_ptr(), dt, qs.data_ptr(), nu, nv, nproj, maps.data_ptr(),
+                                                    fdk._mask.data_ptr(), box16[0], box16[1], 0, vol16.data_ptr(), st))
 
-    tbp16 = kernel_time(bp16, stream)
-    # precision: BF16-stored vs FP32 volumes on 16 seeded slices
+        tfast[name] = kernel_time(bpf, stream)
+    # FP64 error oracle on 16 seeded slices of the final volume
     rng = np.random.default_rng(16)
-    sl = torch.from_numpy(np.sort(rng.choice(nv, 16, replace=False))).to(device)
-    a, b = vol16.index_select(0, sl).double(), vol.index_select(0, sl).double()
-    rel16 = float(torch.sqrt(((a - b) ** 2).mean() / (b ** 2).mean()).item())
-    del filt, q16, vol16, vol
+    sl_np = np.sort(rng.choice(nv, 16, replace=False)).astype(np.int32)
+    sl = torch.from_numpy(sl_np).to(device)
+    m64 = torch.from_numpy(pipe16.fdk.maps64(angles)).to(device)
+    out64 = torch.empty((16, nu, nu), dtype=torch.float64, device=device)
+    L.check(L.lib().mr_fdk_backproject_f64(filt.data_ptr(), nu, nv, nproj, m64.data_ptr(), fdk._mask.data_ptr(),
+                                           sl.data_ptr(), 16, out64.data_ptr(), st))
+
+    def errs(v):
+        d = v.index_select(0, sl.long()).double() - out64
+        return {"rel_rms_vs_fp64": float(torch.sqrt((d ** 2).mean() / (out64 ** 2).mean()).item()),
+                "max_abs_vs_fp64": float(d.abs().max().item())}
+
+    err32 = errs(vol)
+    err16 = {}
+    for name, dt in (("bf16", L.MR_BF16), ("fp16", L.MR_F16)):
+        L.check(L.lib().mr_quantize(filt.data_ptr(), nu * nv, nproj, dt, q16.data_ptr(), qs.data_ptr(), st))
+        L.check(L.lib().mr_fdk_backproject_fast(q16.data_ptr(), dt, qs.data_ptr(), nu, nv, nproj, maps.data_ptr(),
+                                                fdk._mask.data_ptr(), box16[0], box16[1], 0, vol16.data_ptr(), st))
+        err16[name] = errs(vol16)
+        d = vol16.index_select(0, sl.long()).double() - vol.index_select(0, sl.long()).double()
+        ref = vol.index_select(0, sl.long()).double()
+        err16[name]["rel_rms_vs_fp32"] = float(torch.sqrt((d ** 2).mean() / (ref ** 2).mean()).item())
+    vref_max = float(out64.abs().max().item())
+    del filt, q16, vol16, vol, out64, m64
 
     # end to end through the pipeline with pinned host buffers
     counts_h = counts.cpu().pin_memory()
@@ -289,12 +320,18 @@ def run_mr(args):
                        "chain": "FullLogNorm(u16) -> FDK ramp filter -> FDK NN backprojection",
                        "l2": "inputs larger than L2 (2.1 GB counts per step)", "parallelism": f"z-slab x{n}"},
             "projections_per_s": n * nproj * args.steps / t32,
-            "bf16": {"value": n * updates * args.steps / t16 / 1e9,
-                     "unit": "GUPS", "ms_per_step": t16 / args.steps * 1e3,
-                     "backprojection_gups": updates / tbp16 / 1e9, "rel_rms_vs_fp32_16_slices": rel16},
             "backprojection_gups": updates / tbp / 1e9,
+            "precision": {
+                "fp64_oracle": f"FP64 geometry and accumulation on 16 seeded slices {sl_np.tolist()} of the final "
+                               f"volume (max |value| {vref_max:.4g})",
+                "fp32": dict(err32, backprojection_gups=updates / tbp / 1e9),
+                "bf16": dict(err16["bf16"], value=n * updates * args.steps / t16 / 1e9, unit="GUPS",
+                             ms_per_step=t16 / args.steps * 1e3, backprojection_gups=updates / tfast["bf16"] / 1e9),
+                "fp16": dict(err16["fp16"], value=n * updates * args.steps / th16 / 1e9, unit="GUPS",
+                             ms_per_step=th16 / args.steps * 1e3, backprojection_gups=updates / tfast["fp16"] / 1e9),
+            },
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                         "traffic": None, "kernel": "k_fdk<f32>",
+                         "traffic": None, "kernel": "k_fdk_staged<f32, exact>",
                          "note": f"algorithmic bytes = 4 B/update gathered; peak {peak_src}"},
             "e2e": {"value": n * updates * e2e_steps / te2e / 1e9, "unit": "GUPS",
                     "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(nu * nu * nv * 4)},
@@ -323,8 +360,8 @@ def cpu_baseline(w, counts, flats, darks, angles, weights, budget_s=20.0, nsampl
     dark = darks.float().mean(0).cpu().numpy()
     flat = flats.float().mean(0).cpu().numpy()
     p1 = np.where(c - dark > 0, np.log(np.maximum(flat - dark, 1e-3)) - np.log(np.maximum(c - dark, 1e-3)), 0)
-    g = oracle.fdk_geom(w["sod"], w["sdd"], ((nu - 1) / 2.0, (nv - 1) / 2.0), (nu - 1) / 2.0, (w["pitch"],) * 2,
-                        (w["voxel"],) * 3)
+    pp, centre = geometry_centres(w)
+    g = oracle.fdk_geom(w["sod"], w["sdd"], pp, centre, (w["pitch"],) * 2, (w["voxel"],) * 3)
     t0 = time.perf_counter()
     oracle.fdk(p1, angles[:1], weights[:1], g, use_ref=True)
     t1 = time.perf_counter() - t0
@@ -355,8 +392,8 @@ def run_reference(args):
     proj = rng.standard_normal((nsample, nv, nu)).astype(np.float32)
     angles = np.arange(nsample, dtype=np.float32) * np.float32(360.0 / w["nproj"])
     weights = np.full(nsample, np.float32(1.0 / w["nproj"]))
-    g = oracle.fdk_geom(w["sod"], w["sdd"], ((nu - 1) / 2.0, (nv - 1) / 2.0), (nu - 1) / 2.0, (w["pitch"],) * 2,
-                        (w["voxel"],) * 3)
+    pp, centre = geometry_centres(w)
+    g = oracle.fdk_geom(w["sod"], w["sdd"], pp, centre, (w["pitch"],) * 2, (w["voxel"],) * 3)
     for _ in range(args.warmup):
         oracle.fdk(proj[:1], angles[:1], weights[:1], g, use_ref=True)
     t0 = time.perf_counter()

@@ -19,6 +19,7 @@ P_float = ctypes.POINTER(ctypes.c_float)
 P_size = ctypes.POINTER(ctypes.c_size_t)
 P_int = ctypes.POINTER(ctypes.c_int)
 P_u32 = ctypes.POINTER(ctypes.c_uint32)
+P_double = ctypes.POINTER(ctypes.c_double)
 
 MR_OK, MR_ERR_ARGUMENT, MR_ERR_CUDA, MR_ERR_ALLOCATION, MR_ERR_UNSUPPORTED, MR_ERR_DEVICE = range(6)
 MR_F32, MR_BF16, MR_F16, MR_U16 = 0, 1, 2, 3
@@ -69,6 +70,12 @@ _PROTOS = {
     "mr_fdk_backproject": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_int,
                                    c_void, c_int, c_int, c_int, c_void, c_void]),
     "mr_fdk_box": (c_int, [P_float, P_float, P_float, c_size, c_size, c_size, c_int, P_int, P_int]),
+    "mr_fdk_maps64": (c_int, [ctypes.POINTER(FdkGeom), c_size, c_size, P_float, c_size, P_double]),
+    "mr_fdk_box_maps": (c_int, [P_double, c_size, c_size, c_size, c_int, P_int, P_int]),
+    "mr_fdk_backproject_fast": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_int, c_int,
+                                        c_int, c_void, c_void]),
+    "mr_fdk_backproject_f64": (c_int, [c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_size, c_void,
+                                       c_void]),
     "mr_device_status": (c_int, [P_int]),
 }
 

@@ -355,25 +355,23 @@ static void fdk_projmatrix(const mr_fdk_geom *g, float roi0, float angles, float
         }
 }
 
-mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const float *angles_h, size_t nproj,
-                          float *xip_h, float *yip_h, float *zip_h, float *sad_sid_2, float *scale, int *uniform_z)
+// Volume origin and the CBCT row window of project_volume_onto_image_c (fdkbp_single.cpp:302-372)
+// for roi = projection_roi = {0, 0, nu, nv} and a volume of nu x nu x nv, float as written there.
+static void fdk_frame(const mr_fdk_geom *g, size_t nu, size_t nv, float origin[3], size_t cb[4])
 {
-    if (!g || (nproj && (!angles_h || !xip_h || !yip_h || !zip_h)) || !sad_sid_2 || !scale || !uniform_z)
-        return fail(MR_ERR_ARGUMENT, "mr_fdk_partials: null pointer");
-    if (nu == 0 || nv == 0) return fail(MR_ERR_ARGUMENT, "mr_fdk_partials: empty detector");
-    // project_volume_onto_image_c (fdkbp_single.cpp:302-386) for roi = projection_roi =
-    // {0, 0, nu, nv} and a volume of nu x nu x nv
     const size_t roi[4] = {0, 0, nu, nv};
     const size_t proi3 = nv;
     const float *spacing = g->voxelsize;
     const float U = static_cast<float>(roi[2] - roi[0]);
     const float V = static_cast<float>(roi[3] - roi[1]);
-    float origin[3];
     origin[0] = -(U - g->center) * spacing[0] - spacing[0] / 2;
     origin[1] = -(U - g->center) * spacing[1] - spacing[1] / 2;
     origin[2] = -(V - (g->ppoint[1] - roi[1])) * spacing[2] - spacing[2] / 2;
     const float radius = static_cast<float>(nu) * g->voxelsize[0] / 2;
-    size_t cb[4] = {roi[0], 0, roi[2], 0};
+    cb[0] = roi[0];
+    cb[1] = 0;
+    cb[2] = roi[2];
+    cb[3] = 0;
     const float fp1 = g->ppoint[1];
     const float r1 = static_cast<float>(roi[1]), r3 = static_cast<float>(roi[3]);
     const float vx = g->voxelsize[0], sdd = g->sdd, sod = g->sod, res0 = g->resolution[0];
@@ -396,6 +394,19 @@ mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const floa
     }
     if (cb[1] != 0) cb[1] -= 8; // the reference's unsigned test cb[1]-8 >= 0 always holds (:369-372)
     if (cb[3] + 8 <= proi3) cb[3] += 8;
+}
+
+mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const float *angles_h, size_t nproj,
+                          float *xip_h, float *yip_h, float *zip_h, float *sad_sid_2, float *scale, int *uniform_z)
+{
+    if (!g || (nproj && (!angles_h || !xip_h || !yip_h || !zip_h)) || !sad_sid_2 || !scale || !uniform_z)
+        return fail(MR_ERR_ARGUMENT, "mr_fdk_partials: null pointer");
+    if (nu == 0 || nv == 0) return fail(MR_ERR_ARGUMENT, "mr_fdk_partials: empty detector");
+    const size_t roi[4] = {0, 0, nu, nv};
+    const float *spacing = g->voxelsize;
+    float origin[3];
+    size_t cb[4];
+    fdk_frame(g, nu, nv, origin, cb);
     const float ic[2] = {g->ppoint[0] - cb[0], g->ppoint[1] - cb[1]};
     *sad_sid_2 = (g->sod * g->sod) / (g->sdd * g->sdd);
     *scale = g->sod / g->sdd;
@@ -433,6 +444,87 @@ mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const floa
         }
     }
     *uniform_z = uniform;
+    return MR_OK;
+}
+
+// FDKbp::getProjMatrix (fdkbp.cpp:83-255): the projection matrix in double.
+static void fdk_projmatrix64(const mr_fdk_geom *g, double angle, double *pm)
+{
+    double ext[16] = {0}, intr[12] = {0};
+    const double sad = g->sod, sid = g->sdd;
+    const double offcenter = (static_cast<double>(g->ppoint[0]) - g->center) * g->voxelsize[0];
+    const double a = (g->direction == 0 ? -angle : angle) * kDPi / 180.0;
+    const double cam[3] = {sad * std::cos(a), sad * std::sin(a), 0.0};
+    const double nn = std::sqrt(cam[0] * cam[0] + cam[1] * cam[1] + cam[2] * cam[2]);
+    const double nrm[3] = {cam[0] / nn, cam[1] / nn, cam[2] / nn};
+    // plt = nrm x vup, pup = plt x nrm with vup = (0, 0, 1)
+    double plt[3] = {nrm[1], -nrm[0], 0.0};
+    const double np = std::sqrt(plt[0] * plt[0] + plt[1] * plt[1]);
+    plt[0] /= np;
+    plt[1] /= np;
+    double pup[3] = {plt[1] * nrm[2] - plt[2] * nrm[1], plt[2] * nrm[0] - plt[0] * nrm[2], plt[0] * nrm[1] - plt[1] * nrm[0]};
+    const double nq = std::sqrt(pup[0] * pup[0] + pup[1] * pup[1] + pup[2] * pup[2]);
+    pup[0] /= nq;
+    pup[1] /= nq;
+    pup[2] /= nq;
+    for (int c = 0; c < 3; ++c) {
+        ext[c] = -plt[c];
+        ext[4 + c] = -pup[c];
+        ext[8 + c] = -nrm[c];
+    }
+    ext[3] = -offcenter;
+    ext[7] = 0.0;
+    ext[11] = sad;
+    ext[15] = 1.0;
+    intr[0] = 1.0 / g->resolution[0];
+    intr[5] = 1.0 / g->resolution[1];
+    intr[10] = 1.0 / sid;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < 4; ++k) acc += intr[i * 4 + k] * ext[k * 4 + j];
+            pm[i * 4 + j] = acc;
+        }
+}
+
+mr_status mr_fdk_maps64(const mr_fdk_geom *g, size_t nu, size_t nv, const float *angles_h, size_t nproj,
+                        double *maps_h)
+{
+    if (!g || (nproj && (!angles_h || !maps_h))) return fail(MR_ERR_ARGUMENT, "mr_fdk_maps64: null pointer");
+    if (nu == 0 || nv == 0) return fail(MR_ERR_ARGUMENT, "mr_fdk_maps64: empty detector");
+    float originf[3];
+    size_t cb[4];
+    fdk_frame(g, nu, nv, originf, cb); // the row window decides the image centre as in the float path
+    const double s0 = g->voxelsize[0], s1 = g->voxelsize[1], s2 = g->voxelsize[2];
+    const double U = static_cast<double>(nu), V = static_cast<double>(nv);
+    const double o0 = -(U - g->center) * s0 - s0 / 2, o1 = -(U - g->center) * s1 - s1 / 2;
+    const double o2 = -(V - static_cast<double>(g->ppoint[1])) * s2 - s2 / 2;
+    const double ic0 = static_cast<double>(g->ppoint[0]) - static_cast<double>(cb[0]);
+    const double ic1 = static_cast<double>(g->ppoint[1]) - static_cast<double>(cb[1]);
+    // tilt: pm[3] of slice k = ((cor(k) - ppoint[0]) * vx) / res0, cor(k) = tan(-tilt) (cb3 - k - pivot) + centre
+    const double tt = g->correcttilt ? std::tan(-static_cast<double>(g->tiltangle) * kDPi / 180.0) : 0.0;
+    for (size_t p = 0; p < nproj; ++p) {
+        double pm[12];
+        fdk_projmatrix64(g, angles_h[p], pm);
+        double pm3 = pm[3], pm3k = 0.0;
+        if (g->correcttilt) {
+            const double c0 = tt * (static_cast<double>(cb[3]) - g->tiltpivot) + g->center;
+            pm3 = ((c0 - g->ppoint[0]) * g->voxelsize[0]) / g->resolution[0];
+            pm3k = -tt * g->voxelsize[0] / g->resolution[0];
+        }
+        const double A[3] = {pm[0] + ic0 * pm[8], pm[4] + ic1 * pm[8], pm[8]};
+        const double B[3] = {pm[1] + ic0 * pm[9], pm[5] + ic1 * pm[9], pm[9]};
+        const double C[3] = {pm[2] + ic0 * pm[10], pm[6] + ic1 * pm[10], pm[10]};
+        const double D[3] = {ic0 * pm[11] + pm3, ic1 * pm[11] + pm[7], pm[11]};
+        const double Dk[3] = {pm3k, 0.0, 0.0};
+        double *m = maps_h + p * 12;
+        for (int r = 0; r < 3; ++r) {
+            m[4 * r + 0] = A[r] * s0;
+            m[4 * r + 1] = B[r] * s1;
+            m[4 * r + 2] = C[r] * s2 + Dk[r];
+            m[4 * r + 3] = A[r] * o0 + B[r] * o1 + C[r] * o2 + D[r];
+        }
+    }
     return MR_OK;
 }
 

@@ -1,22 +1,35 @@
 // FDK backprojection with TMA-staged projection footprints (sm_100a).
 //
-// Same arithmetic as FDKbp_single::project_volume_onto_image_c (fdkbp_single.cpp:488-525)
-// and get_pixel_value_c (:641-683), evaluated per voxel in the reference's order with
-// explicitly rounded intrinsics, so the FP32 volume is bit-identical to the reference's
-// for identical filtered projections. What changes is where the samples come from:
+// Two kernels share one tiling and pipeline:
 //
+//  * k_fdk_exact (FP32, the reference path): the arithmetic of
+//    FDKbp_single::project_volume_onto_image_c (fdkbp_single.cpp:488-525) and
+//    get_pixel_value_c (:641-683), every per-voxel float operation in the reference's order
+//    with explicitly rounded intrinsics, so the FP32 volume is bit-identical to the
+//    reference's for identical filtered projections. Two slices share most instructions
+//    through the f32x2 operations of sm_100, arranged so that none is fused into an fma. The warp-uniform sums zip+yip of every slice are formed once per warp
+//    and projection in shared memory.
+//  * k_fdk_fast (16-bit projections, the precision form): per-projection affine detector
+//    maps computed in FP64 on the host (FDKbp, fdkbp.cpp:83-640, is the double-geometry
+//    variant of the same backprojector) and rounded once to float; per voxel column and
+//    projection the distance weight and the detector column are formed once, the detector
+//    row advances by a constant step per slice, and the weighted sample is accumulated in
+//    FP32 by one mixed-precision fma (f32 += bf16 x bf16, or f16 x f16) with the weight
+//    rounded to the storage type.
+//
+// Tiling and staging (both kernels):
 //  * CTA tile = 32 (x) x 8 (y) voxel columns x 32 slices; a thread owns one (x, y) column
 //    and keeps its 32 slices in registers for all projections.
-//  * Projections are consumed in batches of 4. For every projection one warp projects the
-//    8 tile corners (the same float formulas as the voxels), takes the footprint's row and
-//    column range with a 1-pixel margin and issues one TMA tile load of a fixed box
-//    (bw x bh) of the projection into shared memory. Rows/columns outside the detector are
-//    zero-filled by the TMA unit, which is exactly the reference's "outside -> 0" rule, so
-//    the per-voxel loop needs no bounds test. Two stages are in flight (double buffering
-//    on two mbarriers with bounded waits).
-//  * The detector row is floor(r) of r = dw*(a1+x1)+0.5 (the reference truncates r >= 0
-//    and rejects r < 0; floor sends r < 0 to a zero row), computed as the bit pattern of
-//    r + 1.5*2^23 added with round-toward-minus-infinity: one FP32 add, no F2I.
+//  * Projections are consumed in batches of NB (4 or 8). For every projection a producer
+//    warp projects the 8 tile corners with the same formulas as the voxels, takes the
+//    footprint's row and column range with a 1-pixel margin and issues one TMA tile load of
+//    a fixed box (bw x bh) of the projection into shared memory. Rows/columns outside the
+//    detector are zero-filled by the TMA unit, which is exactly the reference's
+//    "outside -> 0" rule, so the per-voxel loop needs no bounds test. Two stages are in
+//    flight (double buffering on two mbarriers with bounded waits).
+//  * The detector row is floor(r), taken from the bit pattern of r + 1.5*2^23 added with
+//    round-toward-minus-infinity; the shared-memory address of the sample is one integer
+//    multiply-add of those bits.
 //  * When a footprint does not fit the box, that projection falls back to guarded global
 //    loads for this tile (same arithmetic, same result).
 #include "mr_common.cuh"
@@ -35,22 +48,27 @@ __device__ int g_device_error = 0;
 
 namespace fdk2 {
 
-constexpr int TI = 32, TJ = 8, TK = 32, NB = 4, THREADS = TI * TJ;
+constexpr int TI = 32, TJ = 8, TK = 32, THREADS = TI * TJ, NWARPS = THREADS / 32;
 constexpr float kMagic = 12582912.0f; // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
 constexpr int kWaitLimit = 1 << 22;
+// per-projection geometry staged in shared memory (floats)
+constexpr int GEO_EXACT = TK + 3 * TI + 3 * TJ + 4; // zip1[TK], xip[TI][3], yip[TJ][3], Z0, Z2
+constexpr int GEO_FAST = 16;                        // map[12], scale, pad
 
 struct Params {
     const void *proj;
     const float *scale;
-    const float *xip, *yip, *zip;
+    const float *xip, *yip, *zip; // exact kernel
+    const float *maps;            // fast kernel: [nproj][12]
     const uint32_t *mask;
     float *vol;
     int nu, nv, nproj;
-    int bw, bh;        // TMA box (elements)
-    int boxbytes;      // per-projection shared buffer, 128-byte multiple
+    int bw, bh;       // TMA box (elements)
+    int boxbytes;     // per-projection shared buffer, 128-byte multiple
+    int rowbytes;     // bw * element size
     int accumulate;
-    int xalign;        // x coordinate alignment of a TMA load (elements)
+    int xalign;       // x coordinate alignment of a TMA load (elements)
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -93,16 +111,41 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
                  : "memory");
 }
 
+// f32 accumulator += a * b with a, b in 16-bit storage (one instruction on sm_100).
 template <int DT>
-__device__ __forceinline__ float to_f32(typename Sample<DT>::T v)
+__device__ __forceinline__ float mixed_fma(unsigned short a, unsigned short b, float c)
 {
-    if constexpr (DT == MR_F32) return v;
-    else if constexpr (DT == MR_BF16) return __bfloat162float(v);
-    else return __half2float(v);
+    float d;
+    if constexpr (DT == MR_BF16)
+        asm("fma.rn.f32.bf16 %0, %1, %2, %3;" : "=f"(d) : "h"(a), "h"(b), "f"(c));
+    else
+        asm("fma.rn.f32.f16 %0, %1, %2, %3;" : "=f"(d) : "h"(a), "h"(b), "f"(c));
+    return d;
 }
 
+template <int DT>
+__device__ __forceinline__ unsigned short to_storage(float w)
+{
+    if constexpr (DT == MR_BF16) return __bfloat16_as_ushort(__float2bfloat16_rn(w));
+    else return __half_as_ushort(__float2half_rn(w));
+}
+
+template <int DT>
+__device__ __forceinline__ float from_storage(unsigned short v)
+{
+    if constexpr (DT == MR_BF16) return __bfloat162float(__ushort_as_bfloat16(v));
+    else return __half2float(__ushort_as_half(v));
+}
+
+// Paired f32 operations of sm_100. Each lane of an f32x2 add or mul rounds exactly like the
+// scalar add.rn / mul.rn, but ptxas fuses an f32x2 mul feeding an f32x2 add into an f32x2 fma,
+// even with explicit rounding modifiers and with contraction disabled (measured: 12 % of
+// results differ from mul-then-add on random operands). A paired mul followed by scalar
+// explicit-rounding adds, or scalar muls followed by a paired add, stays unfused (measured
+// bit-identical), so the exact path only pairs chains of those shapes.
+
 // Exact per-voxel detector coordinates (float, reference order), for the corner footprints.
-__device__ __forceinline__ void project(const Params &P, int p, int i, int j, int k, float &r, float &c)
+__device__ __forceinline__ void project_exact(const Params &P, int p, int i, int j, int k, float &r, float &c)
 {
     const float *X = P.xip + (static_cast<size_t>(p) * P.nu + i) * 3;
     const float *Y = P.yip + (static_cast<size_t>(p) * P.nu + j) * 3;
@@ -113,38 +156,202 @@ __device__ __forceinline__ void project(const Params &P, int p, int i, int j, in
     c = __fadd_rn(__fmul_rn(dw, __fadd_rn(a0, X[0])), 0.5f);
 }
 
-// Slices of one voxel column for one staged projection. FULL: all TK slices exist.
-template <int DT, bool FULL>
-__device__ __forceinline__ void staged_column(float (&acc)[TK], const typename Sample<DT>::T *col, const float4 *z4,
-                                              float dw, float dw2, float x1f, float y1f, int off, int bw, float sc,
-                                              int kmax)
+// Fast-path coordinates of voxel column (i, j) at slice k0 of the tile: column c, row r0 of
+// slice k0, row step dr per slice, inverse depth dw. The corner footprints and the voxels
+// use this same function.
+struct FastCol {
+    float c, r0, dr, dw;
+};
+
+__device__ __forceinline__ FastCol fast_column(const float *m, float fi, float fj, float fk0)
 {
+    FastCol f;
+    const float w = fmaf(m[8], fi, fmaf(m[9], fj, m[11]));
+    f.dw = __frcp_rn(w);
+    const float u = fmaf(m[0], fi, fmaf(m[1], fj, m[3]));
+    const float v = fmaf(m[4], fi, fmaf(m[5], fj, fmaf(m[6], fk0, m[7])));
+    f.c = fmaf(u, f.dw, 0.5f);
+    f.r0 = fmaf(v, f.dw, 0.5f);
+    f.dr = m[6] * f.dw;
+    return f;
+}
+
+// Slices of one voxel column for one staged projection (exact arithmetic). a1: the 32
+// per-slice sums zip1 + yip1 of this warp. FULL: all TK slices exist.
+template <bool FULL>
+__device__ __forceinline__ void exact_column(float2 (&acc)[TK / 2], const unsigned char *smem, uint32_t base,
+                                             uint32_t rowbytes, const float *a1, float x1f, float dw, float dw2,
+                                             int kmax)
+{
+    const float2 x1 = make_float2(x1f, x1f), d = make_float2(dw, dw);
+    const float2 mg = make_float2(kMagic, kMagic), d2 = make_float2(dw2, dw2);
 #pragma unroll
-    for (int q4 = 0; q4 < TK / 4; ++q4) {
-        const float4 zz = z4[q4];
-        const float zv[4] = {zz.x, zz.y, zz.z, zz.w};
+    for (int q = 0; q < TK / 2; ++q) {
+        if (!FULL && 2 * q >= kmax) break;
+        const float4 a4 = reinterpret_cast<const float4 *>(a1)[q >> 1];
+        const float2 a = (q & 1) ? make_float2(a4.z, a4.w) : make_float2(a4.x, a4.y);
+        const float2 p = __fmul2_rn(d, __fadd2_rn(a, x1));
+        const float2 r = make_float2(__fadd_rn(p.x, 0.5f), __fadd_rn(p.y, 0.5f));
+        const float2 b = __fadd2_rd(r, mg);
+        const float v0 = *reinterpret_cast<const float *>(smem + (__float_as_uint(b.x) * rowbytes + base));
+        float v1 = 0.0f;
+        if (FULL || 2 * q + 1 < kmax)
+            v1 = *reinterpret_cast<const float *>(smem + (__float_as_uint(b.y) * rowbytes + base));
+        const float2 w = __fmul2_rn(d2, make_float2(v0, v1));
+        acc[q] = make_float2(__fadd_rn(acc[q].x, w.x), __fadd_rn(acc[q].y, w.y));
+    }
+}
+
+// Slices of one voxel column for one staged projection (fast arithmetic, 16-bit samples).
+template <int DT, bool FULL>
+__device__ __forceinline__ void fast_column_staged(float2 (&acc)[TK / 2], const unsigned char *smem, uint32_t base,
+                                                   uint32_t rowbytes, float r0, float dr, unsigned short wt, int kmax)
+{
+    float2 rr = make_float2(r0, __fadd_rn(r0, dr));
+    const float2 step = make_float2(2.0f * dr, 2.0f * dr), mg = make_float2(kMagic, kMagic);
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            if (!FULL && q4 * 4 + e >= kmax) continue;
-            const float a1 = __fadd_rn(zv[e], y1f);
-            const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, x1f)), 0.5f);
-            const int row = __float_as_int(__fadd_rd(r, kMagic)) - off;
-            float v = to_f32<DT>(col[row * bw]);
-            if constexpr (DT != MR_F32) v = v * sc;
-            acc[q4 * 4 + e] = __fadd_rn(acc[q4 * 4 + e], __fmul_rn(dw2, v));
+    for (int q = 0; q < TK / 2; ++q) {
+        if (!FULL && 2 * q >= kmax) break;
+        const float2 b = __fadd2_rd(rr, mg);
+        const unsigned short v0 = *reinterpret_cast<const unsigned short *>(smem + (__float_as_uint(b.x) * rowbytes + base));
+        acc[q].x = mixed_fma<DT>(v0, wt, acc[q].x);
+        if (FULL || 2 * q + 1 < kmax) {
+            const unsigned short v1 =
+                *reinterpret_cast<const unsigned short *>(smem + (__float_as_uint(b.y) * rowbytes + base));
+            acc[q].y = mixed_fma<DT>(v1, wt, acc[q].y);
+        }
+        rr = __fadd2_rn(rr, step);
+    }
+}
+
+// Shared-memory layout of both kernels.
+template <int NB, int GEO, bool A1>
+struct Smem {
+    unsigned char *stage; // [2][NB] boxes
+    float *geo;           // [2][NB][GEO]
+    float *a1;            // [NWARPS][NB][TK] (exact kernel)
+    int4 *meta;           // [2][NB]: x0, y0, mode
+    uint64_t *bars;       // [2]
+    __device__ Smem(unsigned char *base, int boxbytes)
+    {
+        stage = base;
+        geo = reinterpret_cast<float *>(base + 2 * NB * boxbytes);
+        a1 = geo + 2 * NB * GEO;
+        meta = reinterpret_cast<int4 *>(a1 + (A1 ? NWARPS * NB * TK : 0));
+        bars = reinterpret_cast<uint64_t *>(meta + 2 * NB);
+    }
+    static size_t bytes(int boxbytes)
+    {
+        return 2 * NB * static_cast<size_t>(boxbytes) + (2 * NB * GEO + (A1 ? NWARPS * NB * TK : 0)) * sizeof(float) +
+               2 * NB * sizeof(int4) + 2 * sizeof(uint64_t);
+    }
+};
+
+// Producer: footprints of NB projections (4 per producer warp, 8 corner lanes each), TMA
+// issue, and the per-projection geometry staged by all threads.
+template <int DT, bool EXACT, int NB>
+__device__ __forceinline__ void produce(const Params &P, const CUtensorMap *tmap, Smem<NB, EXACT ? GEO_EXACT : GEO_FAST, EXACT> &S,
+                                        int s, int st, int i0, int j0, int k0, int i_hi, int j_hi, int kmax)
+{
+    using T = typename Sample<DT>::T;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp < NB / 4) {
+        const int b = warp * 4 + (lane >> 3), corner = lane & 7;
+        const int p = s * NB + b;
+        int rmin = 0, rmax = 0, cmin = 0, cmax = 0;
+        bool ok = p < P.nproj;
+        if (ok) {
+            const int ci = (corner & 1) ? i_hi : i0, cj = (corner & 2) ? j_hi : j0;
+            float r, c;
+            if constexpr (EXACT) {
+                project_exact(P, p, ci, cj, (corner & 4) ? k0 + kmax - 1 : k0, r, c);
+            } else {
+                const float *m = P.maps + static_cast<size_t>(p) * 12;
+                const float mm[12] = {__ldg(m), __ldg(m + 1), __ldg(m + 2), __ldg(m + 3), __ldg(m + 4), __ldg(m + 5),
+                                      __ldg(m + 6), __ldg(m + 7), __ldg(m + 8), __ldg(m + 9), __ldg(m + 10), __ldg(m + 11)};
+                const float w = fmaf(mm[8], static_cast<float>(ci), fmaf(mm[9], static_cast<float>(cj), mm[11]));
+                const FastCol f = fast_column(mm, static_cast<float>(ci), static_cast<float>(cj), static_cast<float>(k0));
+                c = f.c;
+                r = (corner & 4) ? fmaf(static_cast<float>(kmax - 1), f.dr, f.r0) : f.r0;
+                ok = w > 0.0f;
+            }
+            ok = ok && fabsf(r) < 4.0e6f && fabsf(c) < 4.0e6f;
+            rmin = rmax = ok ? __float2int_rd(r) : 0;
+            cmin = cmax = ok ? __float2int_rd(c) : 0;
+        }
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1) {
+            rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+            rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+            cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+            cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+            ok = __shfl_xor_sync(0xffffffffu, static_cast<int>(ok), o) && ok;
+        }
+        // 0: footprint does not fit (global fallback), 1: staged, 2: nothing to read
+        int mode = 0, x0 = 0, y0 = 0;
+        if (p < P.nproj && ok) {
+            if (cmax < -1 || cmin > P.nu || rmax < -1 || rmin > P.nv) {
+                mode = 2;
+            } else {
+                x0 = cmin - 1;
+                x0 = x0 >= 0 ? (x0 / P.xalign) * P.xalign : -(((-x0) + P.xalign - 1) / P.xalign) * P.xalign;
+                y0 = rmin - 1;
+                if (cmax + 1 < x0 + P.bw && rmax + 1 < y0 + P.bh) mode = 1;
+            }
+        }
+        const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
+        if (lane == 0)
+            mbar_expect_tx(&S.bars[st], static_cast<uint32_t>(__popc(staged)) * P.bw * P.bh * sizeof(T));
+        __syncwarp();
+        if (corner == 0 && p < P.nproj) {
+            S.meta[st * NB + b] = make_int4(x0, y0, mode, 0);
+            if (mode == 1) {
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                tma_load_3d(S.stage + (st * NB + b) * P.boxbytes, tmap, x0, y0, p, &S.bars[st]);
+            }
+        }
+    }
+    if constexpr (EXACT) {
+        for (int idx = threadIdx.x; idx < NB * GEO_EXACT; idx += THREADS) {
+            const int b = idx / GEO_EXACT, e = idx % GEO_EXACT, p = s * NB + b;
+            float v = 0.0f;
+            if (p < P.nproj) {
+                if (e < TK) {
+                    if (e < kmax) v = P.zip[(static_cast<size_t>(p) * P.nv + k0 + e) * 3 + 1];
+                } else if (e < TK + 3 * TI) {
+                    const int ii = i0 + (e - TK) / 3;
+                    if (ii < P.nu) v = P.xip[(static_cast<size_t>(p) * P.nu + ii) * 3 + (e - TK) % 3];
+                } else if (e < TK + 3 * TI + 3 * TJ) {
+                    const int jj = j0 + (e - TK - 3 * TI) / 3;
+                    if (jj < P.nu) v = P.yip[(static_cast<size_t>(p) * P.nu + jj) * 3 + (e - TK - 3 * TI) % 3];
+                } else if (e == TK + 3 * TI + 3 * TJ) {
+                    v = P.zip[static_cast<size_t>(p) * P.nv * 3];
+                } else if (e == TK + 3 * TI + 3 * TJ + 1) {
+                    v = P.zip[static_cast<size_t>(p) * P.nv * 3 + 2];
+                }
+            }
+            S.geo[st * NB * GEO_EXACT + idx] = v;
+        }
+    } else {
+        for (int idx = threadIdx.x; idx < NB * GEO_FAST; idx += THREADS) {
+            const int b = idx / GEO_FAST, e = idx % GEO_FAST, p = s * NB + b;
+            float v = 0.0f;
+            if (p < P.nproj) {
+                if (e < 12) v = P.maps[static_cast<size_t>(p) * 12 + e];
+                else if (e == 12) v = P.scale[p];
+            }
+            S.geo[st * NB * GEO_FAST + idx] = v;
         }
     }
 }
 
-template <int DT>
-__global__ void __launch_bounds__(THREADS, 2) k_fdk_tma(const __grid_constant__ CUtensorMap tmap, const Params P)
+template <int DT, bool EXACT, int NB>
+__global__ void __launch_bounds__(THREADS, 2) k_fdk_staged(const __grid_constant__ CUtensorMap tmap, const Params P)
 {
+    constexpr int GEO = EXACT ? GEO_EXACT : GEO_FAST;
     using T = typename Sample<DT>::T;
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *stage = smem;                                                      // [2][NB] boxes
-    float *zipbuf = reinterpret_cast<float *>(smem + 2 * NB * P.boxbytes);            // [2][NB][TK]
-    int4 *meta = reinterpret_cast<int4 *>(zipbuf + 2 * NB * TK);                     // [2][NB]
-    uint64_t *bars = reinterpret_cast<uint64_t *>(meta + 2 * NB);                     // [2]
+    Smem<NB, GEO, EXACT> S(smem, P.boxbytes);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
@@ -155,160 +362,251 @@ __global__ void __launch_bounds__(THREADS, 2) k_fdk_tma(const __grid_constant__ 
     const size_t plane = static_cast<size_t>(P.nu) * P.nu;
     const size_t out_xy = valid ? static_cast<size_t>(j) * P.nu + (P.nu - 1 - i) : 0;
 
-    float acc[TK];
+    // 16-bit storage: weights are scaled by 2^-G (G = largest scale exponent), the sum by 2^G
+    float gscale = 1.0f, ginv = 1.0f;
+    if constexpr (!EXACT && DT == MR_F16) {
+        float mx = 0.0f;
+        for (int p = threadIdx.x; p < P.nproj; p += THREADS) mx = fmaxf(mx, P.scale[p]);
+        mx = __uint_as_float(__reduce_max_sync(0xffffffffu, __float_as_uint(mx))); // non-negative floats order as integers
+        __shared__ float wmax[NWARPS];
+        if (lane == 0) wmax[warp] = mx;
+        __syncthreads();
+        mx = 0.0f;
 #pragma unroll
-    for (int q = 0; q < TK; ++q)
-        acc[q] = (valid && P.accumulate && q < kmax) ? P.vol[static_cast<size_t>(P.nv - 1 - (k0 + q)) * plane + out_xy]
-                                                     : 0.0f;
+        for (int w = 0; w < NWARPS; ++w) mx = fmaxf(mx, wmax[w]);
+        if (mx > 0.0f) {
+            gscale = mx;            // a power of two
+            ginv = 1.0f / mx;       // exact
+        }
+    }
 
-    if (!__syncthreads_or(inside)) {
+    // slices 2q, 2q+1 of the column in acc[q].x, acc[q].y
+    float2 acc[TK / 2];
+#pragma unroll
+    for (int q = 0; q < TK; ++q) {
+        const float v = (valid && P.accumulate && q < kmax)
+                            ? P.vol[static_cast<size_t>(P.nv - 1 - (k0 + q)) * plane + out_xy] * ginv
+                            : 0.0f;
+        if (q & 1) acc[q >> 1].y = v; else acc[q >> 1].x = v;
+    }
+
+    auto write_out = [&]() {
         if (valid) {
 #pragma unroll
             for (int q = 0; q < TK; ++q)
-                if (q < kmax) P.vol[static_cast<size_t>(P.nv - 1 - (k0 + q)) * plane + out_xy] = acc[q];
+                if (q < kmax)
+                    P.vol[static_cast<size_t>(P.nv - 1 - (k0 + q)) * plane + out_xy] =
+                        ((q & 1) ? acc[q >> 1].y : acc[q >> 1].x) * gscale;
         }
+    };
+
+    if (!__syncthreads_or(inside)) {
+        write_out();
         return;
     }
 
     if (threadIdx.x == 0) {
-        mbar_init(&bars[0], 1);
-        mbar_init(&bars[1], 1);
+        mbar_init(&S.bars[0], NB / 4);
+        mbar_init(&S.bars[1], NB / 4);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
 
-    const int i_hi = min(i0 + TI - 1, P.nu - 1), j_hi = min(j0 + TJ - 1, P.nu - 1), k_hi = k0 + kmax - 1;
+    const int i_hi = min(i0 + TI - 1, P.nu - 1), j_hi = min(j0 + TJ - 1, P.nu - 1);
     const int nbatch = (P.nproj + NB - 1) / NB;
 
-    // Footprints + TMA issue for batch s into stage st (warp 0); zip rows for all threads.
-    auto produce = [&](int s, int st) {
-        if (warp == 0) {
-            const int b = lane >> 3, corner = lane & 7;
-            const int p = s * NB + b;
-            int rmin = 0, rmax = 0, cmin = 0, cmax = 0;
-            bool ok = p < P.nproj;
-            if (ok) {
-                float r, c;
-                project(P, p, (corner & 1) ? i_hi : i0, (corner & 2) ? j_hi : j0, (corner & 4) ? k_hi : k0, r, c);
-                ok = fabsf(r) < 4.0e6f && fabsf(c) < 4.0e6f;
-                rmin = rmax = ok ? __float2int_rd(r) : 0;
-                cmin = cmax = ok ? __float2int_rd(c) : 0;
-            }
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
-                rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-                cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
-                cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
-                ok = __shfl_xor_sync(0xffffffffu, static_cast<int>(ok), o) && ok;
-            }
-            // 0: footprint does not fit (global fallback), 1: staged, 2: nothing to read
-            int mode = 0, x0 = 0, y0 = 0;
-            if (p < P.nproj && ok) {
-                if (cmax < -1 || cmin > P.nu || rmax < -1 || rmin > P.nv) {
-                    mode = 2;
-                } else {
-                    x0 = cmin - 1;
-                    x0 = x0 >= 0 ? (x0 / P.xalign) * P.xalign : -(((-x0) + P.xalign - 1) / P.xalign) * P.xalign;
-                    y0 = rmin - 1;
-                    if (cmax + 1 < x0 + P.bw && rmax + 1 < y0 + P.bh) mode = 1;
-                }
-            }
-            const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
-            if (lane == 0) mbar_expect_tx(&bars[st], static_cast<uint32_t>(__popc(staged)) * P.bw * P.bh * sizeof(T));
-            __syncwarp();
-            if (corner == 0 && p < P.nproj) {
-                meta[st * NB + b] = make_int4(x0, y0, mode, 0);
-                if (mode == 1) {
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    tma_load_3d(stage + (st * NB + b) * P.boxbytes, &tmap, x0, y0, p, &bars[st]);
-                }
-            }
-        }
-        for (int idx = threadIdx.x; idx < NB * TK; idx += THREADS) {
-            const int b = idx / TK, q = idx % TK, p = s * NB + b;
-            zipbuf[st * NB * TK + idx] = (p < P.nproj && q < kmax) ? P.zip[(static_cast<size_t>(p) * P.nv + k0 + q) * 3 + 1] : 0.0f;
-        }
-    };
-
-    produce(0, 0);
-    if (nbatch > 1) produce(1, 1);
+    produce<DT, EXACT, NB>(P, &tmap, S, 0, 0, i0, j0, k0, i_hi, j_hi, kmax);
+    if (nbatch > 1) produce<DT, EXACT, NB>(P, &tmap, S, 1, 1, i0, j0, k0, i_hi, j_hi, kmax);
     __syncthreads();
 
     uint32_t phase0 = 0, phase1 = 0;
     bool failed = false;
     const float fw = static_cast<float>(P.nu), fh = static_cast<float>(P.nv);
+    const float fi = static_cast<float>(i), fj = static_cast<float>(j), fk0 = static_cast<float>(k0);
+    const uint32_t rowbytes = static_cast<uint32_t>(P.rowbytes);
+    const bool warp_inside = __any_sync(0xffffffffu, inside);
     for (int s = 0; s < nbatch; ++s) {
         const int st = s & 1;
         const uint32_t par = st ? phase1 : phase0;
-        if (!mbar_wait(&bars[st], par)) {
+        if (!mbar_wait(&S.bars[st], par)) {
             failed = true;
             atomicExch(&g_device_error, 1);
             break;
         }
         if (st) phase1 ^= 1; else phase0 ^= 1;
 
+        if constexpr (EXACT) {
+            // per-warp slice sums a1[k] = zip1[k] + yip1[j] (lane = slice)
+            if (warp_inside) {
+                for (int b = 0; b < NB; ++b) {
+                    const float *g = S.geo + (st * NB + b) * GEO_EXACT;
+                    S.a1[(warp * NB + b) * TK + lane] = __fadd_rn(g[lane], g[TK + 3 * TI + 3 * warp + 1]);
+                }
+                __syncwarp();
+            }
+        }
         if (inside) {
+            // projections in groups of G: the per-projection set-up of a group (reciprocal,
+            // detector column, shared-memory base) is formed first, so its latency overlaps
+            constexpr int G = 4;
 #pragma unroll 1
-            for (int b = 0; b < NB; ++b) {
-                const int p = s * NB + b;
-                if (p >= P.nproj) break;
-                const int4 m = meta[st * NB + b];
-                if (m.z == 2) continue;
-                const float *X = P.xip + (static_cast<size_t>(p) * P.nu + i) * 3;
-                const float *Y = P.yip + (static_cast<size_t>(p) * P.nu + j) * 3;
-                const float *Z = P.zip + static_cast<size_t>(p) * P.nv * 3;
-                const float x0f = __ldg(X), x1f = __ldg(X + 1), x2f = __ldg(X + 2);
-                const float y0f = __ldg(Y), y1f = __ldg(Y + 1), y2f = __ldg(Y + 2);
-                const float dw = __fdiv_rn(1.0f, __fadd_rn(__fadd_rn(__ldg(Z + 2), y2f), x2f));
-                const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(__ldg(Z), y0f), x0f)), 0.5f);
-                if (c < 0.0f || c >= fw) continue;
-                const int cc = static_cast<int>(c);
-                float dw2 = __fmul_rn(dw, dw);
-                const float sc = DT == MR_F32 ? 1.0f : __ldg(P.scale + p);
-                const float4 *z4 = reinterpret_cast<const float4 *>(zipbuf + (st * NB + b) * TK);
-                if (m.z == 1) {
-                    const T *col = reinterpret_cast<const T *>(stage + (st * NB + b) * P.boxbytes) + (cc - m.x);
-                    const int off = kMagicBits + m.y; // bits(r + magic) - off = floor(r) - y0
-                    if (kmax == TK)
-                        staged_column<DT, true>(acc, col, z4, dw, dw2, x1f, y1f, off, P.bw, sc, kmax);
-                    else
-                        staged_column<DT, false>(acc, col, z4, dw, dw2, x1f, y1f, off, P.bw, sc, kmax);
-                } else {
-                    const T *img = static_cast<const T *>(P.proj) + static_cast<size_t>(p) * P.nu * P.nv + cc;
+            for (int b0 = 0; b0 < NB; b0 += G) {
+                float q_a[G], q_b[G], q_c[G]; // exact: dw, dw2, x1; fast: r0, dr, (weight bits)
+                uint32_t q_base[G];
+                bool q_on[G];
 #pragma unroll
-                    for (int q4 = 0; q4 < TK / 4; ++q4) {
-                        const float4 zz = z4[q4];
-                        const float zv[4] = {zz.x, zz.y, zz.z, zz.w};
+                for (int e = 0; e < G; ++e) {
+                    const int b = b0 + e, p = s * NB + b;
+                    const int4 m = S.meta[st * NB + b];
+                    const float *g = S.geo + (st * NB + b) * GEO;
+                    const uint32_t boxoff = static_cast<uint32_t>((st * NB + b) * P.boxbytes);
+                    q_on[e] = false;
+                    q_a[e] = q_b[e] = q_c[e] = 0.0f;
+                    q_base[e] = 0;
+                    if (p < P.nproj && m.z == 1) {
+                        if constexpr (EXACT) {
+                            const float x0f = g[TK + 3 * lane], x1f = g[TK + 3 * lane + 1], x2f = g[TK + 3 * lane + 2];
+                            const float y0f = g[TK + 3 * TI + 3 * warp], y2f = g[TK + 3 * TI + 3 * warp + 2];
+                            const float Z0 = g[TK + 3 * TI + 3 * TJ], Z2 = g[TK + 3 * TI + 3 * TJ + 1];
+                            const float dw = __frcp_rn(__fadd_rn(__fadd_rn(Z2, y2f), x2f));
+                            const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(Z0, y0f), x0f)), 0.5f);
+                            const int cc = static_cast<int>(c);
+                            q_on[e] = c >= 0.0f && c < fw;
+                            q_a[e] = dw;
+                            q_b[e] = __fmul_rn(dw, dw);
+                            q_c[e] = x1f;
+                            // bits(r + magic) * rowbytes + base = (floor(r) - y0) * rowbytes + (cc - x0) * 4 + box
+                            q_base[e] = boxoff + static_cast<uint32_t>(cc - m.x) * 4u -
+                                        static_cast<uint32_t>(kMagicBits + m.y) * rowbytes;
+                        } else {
+                            const FastCol f = fast_column(g, fi, fj, fk0);
+                            const int cc = __float_as_int(__fadd_rd(f.c, kMagic)) - kMagicBits;
+                            q_on[e] = true;
+                            q_a[e] = f.r0;
+                            q_b[e] = f.dr;
+                            q_c[e] = __uint_as_float(to_storage<DT>(f.dw * f.dw * (g[12] * ginv)));
+                            q_base[e] = boxoff + static_cast<uint32_t>(cc - m.x) * 2u -
+                                        static_cast<uint32_t>(kMagicBits + m.y) * rowbytes;
+                        }
+                    }
+                }
 #pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            if (q4 * 4 + e >= kmax) continue;
-                            const float a1 = __fadd_rn(zv[e], y1f);
-                            const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, x1f)), 0.5f);
+                for (int e = 0; e < G; ++e) {
+                    if (!q_on[e]) continue;
+                    if constexpr (EXACT) {
+                        const float *a1 = S.a1 + (warp * NB + b0 + e) * TK;
+                        if (kmax == TK)
+                            exact_column<true>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
+                        else
+                            exact_column<false>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
+                    } else {
+                        const unsigned short wt = static_cast<unsigned short>(__float_as_uint(q_c[e]));
+                        if (kmax == TK)
+                            fast_column_staged<DT, true>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e], wt, kmax);
+                        else
+                            fast_column_staged<DT, false>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e], wt, kmax);
+                    }
+                }
+                // footprints that did not fit the box: guarded global loads (rare)
+#pragma unroll 1
+                for (int e = 0; e < G; ++e) {
+                    const int b = b0 + e, p = s * NB + b;
+                    if (p >= P.nproj || S.meta[st * NB + b].z != 0) continue;
+                    const float *g = S.geo + (st * NB + b) * GEO;
+                    if constexpr (EXACT) {
+                        const float x0f = g[TK + 3 * lane], x1f = g[TK + 3 * lane + 1], x2f = g[TK + 3 * lane + 2];
+                        const float y0f = g[TK + 3 * TI + 3 * warp], y2f = g[TK + 3 * TI + 3 * warp + 2];
+                        const float Z0 = g[TK + 3 * TI + 3 * TJ], Z2 = g[TK + 3 * TI + 3 * TJ + 1];
+                        const float dw = __frcp_rn(__fadd_rn(__fadd_rn(Z2, y2f), x2f));
+                        const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(Z0, y0f), x0f)), 0.5f);
+                        if (c < 0.0f || c >= fw) continue;
+                        const float dw2 = __fmul_rn(dw, dw);
+                        const float *a1 = S.a1 + (warp * NB + b) * TK;
+                        const float *img = static_cast<const float *>(P.proj) + static_cast<size_t>(p) * P.nu * P.nv +
+                                           static_cast<int>(c);
+#pragma unroll
+                        for (int q = 0; q < TK; ++q) {
+                            if (q >= kmax) break;
+                            const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1[q], x1f)), 0.5f);
                             if (r < 0.0f || r >= fh) continue;
-                            float v = to_f32<DT>(img[static_cast<size_t>(static_cast<int>(r)) * P.nu]);
-                            if constexpr (DT != MR_F32) v = v * sc;
-                            acc[q4 * 4 + e] = __fadd_rn(acc[q4 * 4 + e], __fmul_rn(dw2, v));
+                            const float v = __ldg(img + static_cast<size_t>(static_cast<int>(r)) * P.nu);
+                            float &a = (q & 1) ? acc[q >> 1].y : acc[q >> 1].x;
+                            a = __fadd_rn(a, __fmul_rn(dw2, v));
+                        }
+                    } else {
+                        const FastCol f = fast_column(g, fi, fj, fk0);
+                        if (f.c < 0.0f || f.c >= fw) continue;
+                        const unsigned short wt = to_storage<DT>(f.dw * f.dw * (g[12] * ginv));
+                        const T *img = static_cast<const T *>(P.proj) + static_cast<size_t>(p) * P.nu * P.nv +
+                                       static_cast<int>(f.c);
+                        const float wf = from_storage<DT>(wt);
+                        float r = f.r0;
+#pragma unroll
+                        for (int q = 0; q < TK; ++q, r = __fadd_rn(r, f.dr)) {
+                            if (q >= kmax) break;
+                            if (r < 0.0f || r >= fh) continue;
+                            const unsigned short v =
+                                reinterpret_cast<const unsigned short *>(img)[static_cast<size_t>(static_cast<int>(r)) * P.nu];
+                            float &a = (q & 1) ? acc[q >> 1].y : acc[q >> 1].x;
+                            a = fmaf(from_storage<DT>(v), wf, a);
                         }
                     }
                 }
             }
         }
         __syncthreads();
-        if (s + 2 < nbatch) {
-            produce(s + 2, st);
-        }
+        if (s + 2 < nbatch) produce<DT, EXACT, NB>(P, &tmap, S, s + 2, st, i0, j0, k0, i_hi, j_hi, kmax);
     }
     if (failed) {
         // the other stage may still have a copy in flight: wait for it (bounded) before exit
-        mbar_wait(&bars[0], phase0);
-        mbar_wait(&bars[1], phase1);
+        mbar_wait(&S.bars[0], phase0);
+        mbar_wait(&S.bars[1], phase1);
     }
-    if (valid) {
+    write_out();
+}
+
+// ---------------------------------------------------------------- FP64 error oracle
+
+// FP64 backprojection of FP32 filtered projections through the FP64 maps, for the listed
+// output slices (out[s][j][i] = final volume slice slices[s]). One thread per voxel column.
+__global__ void k_fdk_f64(const float *__restrict__ proj, int nu, int nv, int nproj, const double *__restrict__ maps,
+                          const uint32_t *__restrict__ mask, const int *__restrict__ slices, int nslices,
+                          double *__restrict__ out)
+{
+    constexpr int MAXS = 16;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y;
+    if (i >= nu || j >= nu) return;
+    double acc[MAXS];
+    int ks[MAXS];
 #pragma unroll
-        for (int q = 0; q < TK; ++q)
-            if (q < kmax) P.vol[static_cast<size_t>(P.nv - 1 - (k0 + q)) * plane + out_xy] = acc[q];
+    for (int s = 0; s < MAXS; ++s) {
+        acc[s] = 0.0;
+        ks[s] = s < nslices ? nv - 1 - slices[s] : 0;
     }
+    const bool inside = static_cast<uint32_t>(i) > mask[2 * j] && static_cast<uint32_t>(i) <= mask[2 * j + 1];
+    if (inside) {
+        const double di = i, dj = j;
+        for (int p = 0; p < nproj; ++p) {
+            const double *m = maps + static_cast<size_t>(p) * 12;
+            const float *img = proj + static_cast<size_t>(p) * nu * nv;
+#pragma unroll
+            for (int s = 0; s < MAXS; ++s) {
+                if (s >= nslices) break;
+                const double dk = ks[s];
+                const double u = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[0], di), __dmul_rn(m[1], dj)), __dmul_rn(m[2], dk)), m[3]);
+                const double v = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[4], di), __dmul_rn(m[5], dj)), __dmul_rn(m[6], dk)), m[7]);
+                const double w = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[8], di), __dmul_rn(m[9], dj)), __dmul_rn(m[10], dk)), m[11]);
+                const double dw = __ddiv_rn(1.0, w);
+                const double r = __dadd_rn(__dmul_rn(dw, v), 0.5), c = __dadd_rn(__dmul_rn(dw, u), 0.5);
+                if (r < 0.0 || r >= nv || c < 0.0 || c >= nu) continue;
+                const double val = img[static_cast<size_t>(static_cast<int>(r)) * nu + static_cast<int>(c)];
+                acc[s] = __dadd_rn(acc[s], __dmul_rn(__dmul_rn(dw, dw), val));
+            }
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < MAXS; ++s)
+        if (s < nslices) out[(static_cast<size_t>(s) * nu + j) * nu + (nu - 1 - i)] = acc[s];
 }
 
 // ---------------------------------------------------------------- host side
@@ -349,32 +647,45 @@ static void tile_footprint(const float *X, const float *Y, const float *Z, int i
     cspan = std::floor(cmax) - std::floor(cmin);
 }
 
-} // namespace fdk2
-
-// Box size (bw, bh) that holds the tile footprints of (a sample of) the geometry.
-static void fdk_box_guess(const float *xip_h, const float *yip_h, const float *zip_h, size_t nu, size_t nv, size_t nproj,
-                          int xalign, int &bw, int &bh)
+static void tile_footprint_maps(const double *m, int i0, int i1, int j0, int j1, int k0, int k1, double &rspan,
+                                double &cspan)
 {
-    using namespace fdk2;
+    double rmin = 1e30, rmax = -1e30, cmin = 1e30, cmax = -1e30;
+    for (int corner = 0; corner < 8; ++corner) {
+        const double i = corner & 1 ? i1 : i0, j = corner & 2 ? j1 : j0, k = corner & 4 ? k1 : k0;
+        const double dw = 1.0 / (m[8] * i + m[9] * j + m[10] * k + m[11]);
+        const double r = dw * (m[4] * i + m[5] * j + m[6] * k + m[7]) + 0.5;
+        const double c = dw * (m[0] * i + m[1] * j + m[2] * k + m[3]) + 0.5;
+        rmin = std::min(rmin, r);
+        rmax = std::max(rmax, r);
+        cmin = std::min(cmin, c);
+        cmax = std::max(cmax, c);
+    }
+    rspan = std::floor(rmax) - std::floor(rmin);
+    cspan = std::floor(cmax) - std::floor(cmin);
+}
+
+// Largest footprint over a sample of tiles and projections -> box (bw, bh).
+template <typename F>
+static void box_guess(size_t nu, size_t nv, size_t nproj, int xalign, int &bw, int &bh, F footprint)
+{
     double rs = 0, cs = 0;
     const int ti = static_cast<int>((nu + TI - 1) / TI), tj = static_cast<int>((nu + TJ - 1) / TJ);
     const int tk = static_cast<int>((nv + TK - 1) / TK);
     const size_t pstep = std::max<size_t>(1, nproj / 64);
     const int istep = std::max(1, ti / 8), jstep = std::max(1, tj / 16);
-    for (size_t p = 0; p < nproj; p += pstep) {
-        const float *X = xip_h + p * nu * 3, *Y = yip_h + p * nu * 3, *Z = zip_h + p * nv * 3;
+    for (size_t p = 0; p < nproj; p += pstep)
         for (int a = 0; a < ti; a += (a + istep < ti ? istep : std::max(1, ti - 1 - a)))
             for (int b = 0; b < tj; b += (b + jstep < tj ? jstep : std::max(1, tj - 1 - b)))
                 for (int kk : {0, tk - 1}) {
                     const int i0 = a * TI, j0 = b * TJ, k0 = kk * TK;
                     double r, c;
-                    tile_footprint(X, Y, Z, i0, std::min<int>(i0 + TI - 1, static_cast<int>(nu) - 1), j0,
-                                   std::min<int>(j0 + TJ - 1, static_cast<int>(nu) - 1), k0,
-                                   std::min<int>(k0 + TK - 1, static_cast<int>(nv) - 1), r, c);
+                    footprint(p, i0, std::min<int>(i0 + TI - 1, static_cast<int>(nu) - 1), j0,
+                              std::min<int>(j0 + TJ - 1, static_cast<int>(nu) - 1), k0,
+                              std::min<int>(k0 + TK - 1, static_cast<int>(nv) - 1), r, c);
                     rs = std::max(rs, r);
                     cs = std::max(cs, c);
                 }
-    }
     // +1 margin each side, +1 for the inclusive range, + alignment slack on x
     bw = static_cast<int>(cs) + 3 + (xalign - 1);
     bh = static_cast<int>(rs) + 3;
@@ -383,11 +694,14 @@ static void fdk_box_guess(const float *xip_h, const float *yip_h, const float *z
     bh = std::min(bh, 256);
 }
 
-// Launches the TMA-staged FDK kernel; returns MR_ERR_UNSUPPORTED when the layout does not
-// allow TMA (the caller then uses the plain kernel).
-mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
-                         const float *xip_d, const float *yip_d, const float *zip_d, const uint32_t *mask_d,
-                         int accumulate, float *vol_d, int bw, int bh, cudaStream_t s)
+} // namespace fdk2
+
+// Launches a staged FDK kernel; returns MR_ERR_UNSUPPORTED when the layout does not allow
+// TMA or the box does not fit shared memory (the caller then uses the plain kernel).
+static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
+                               size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d,
+                               const float *maps_d, const uint32_t *mask_d, int accumulate, float *vol_d, int bw,
+                               int bh, cudaStream_t s)
 {
     using namespace fdk2;
     const size_t es = dtype == MR_F32 ? 4 : 2;
@@ -396,6 +710,18 @@ mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, si
     if (bw <= 0 || bh <= 0 || bw > 256 || bh > 256 || bw % xalign) return MR_ERR_UNSUPPORTED;
     PFN_cuTensorMapEncodeTiled enc = encode_fn();
     if (!enc) return fail(MR_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+    constexpr size_t kMaxSmem = 112 * 1024; // two CTAs per SM
+    // Row pitch a multiple of 128 bytes when it fits: lanes of a warp read one or two adjacent
+    // rows of consecutive columns, and with such a pitch a row change moves no lane to
+    // another lane's bank.
+    {
+        const int wide = std::min(256, (bw + static_cast<int>(128 / es) - 1) / static_cast<int>(128 / es) *
+                                           static_cast<int>(128 / es));
+        const size_t boxw = (wide * bh * es + 127) / 128 * 128;
+        const size_t need = exact ? Smem<4, GEO_EXACT, true>::bytes(static_cast<int>(boxw))
+                                  : Smem<4, GEO_FAST, false>::bytes(static_cast<int>(boxw));
+        if (need <= kMaxSmem) bw = wide;
+    }
     CUtensorMap map;
     cuuint64_t dims[3] = {nu, nv, nproj};
     cuuint64_t strides[2] = {nu * es, nu * nv * es};
@@ -413,6 +739,7 @@ mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, si
     P.xip = xip_d;
     P.yip = yip_d;
     P.zip = zip_d;
+    P.maps = maps_d;
     P.mask = mask_d;
     P.vol = vol_d;
     P.nu = static_cast<int>(nu);
@@ -421,33 +748,50 @@ mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, si
     P.bw = bw;
     P.bh = bh;
     P.boxbytes = static_cast<int>((bw * bh * es + 127) / 128 * 128);
+    P.rowbytes = static_cast<int>(bw * es);
     P.accumulate = accumulate;
     P.xalign = xalign;
-    const size_t smem = 2 * NB * static_cast<size_t>(P.boxbytes) + 2 * NB * TK * sizeof(float) + 2 * NB * sizeof(int4) +
-                        2 * sizeof(uint64_t);
-    if (smem > 110 * 1024) return MR_ERR_UNSUPPORTED;
     dim3 grid(div_up(nu, TI), div_up(nu, TJ), div_up(nv, TK));
-    switch (dtype) {
-    case MR_F32:
-        MR_CUDA_TRY(cudaFuncSetAttribute(k_fdk_tma<MR_F32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
-        k_fdk_tma<MR_F32><<<grid, THREADS, smem, s>>>(map, P);
-        break;
-    case MR_BF16:
-        MR_CUDA_TRY(cudaFuncSetAttribute(k_fdk_tma<MR_BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
-        k_fdk_tma<MR_BF16><<<grid, THREADS, smem, s>>>(map, P);
-        break;
-    default:
-        MR_CUDA_TRY(cudaFuncSetAttribute(k_fdk_tma<MR_F16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024));
-        k_fdk_tma<MR_F16><<<grid, THREADS, smem, s>>>(map, P);
+    auto go = [&](auto kernel, size_t smem) -> mr_status {
+        MR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem)));
+        kernel<<<grid, THREADS, smem, s>>>(map, P);
+        return check_launch(exact ? "k_fdk_exact" : "k_fdk_fast");
+    };
+    if (exact) {
+        if (dtype != MR_F32) return MR_ERR_UNSUPPORTED;
+        const size_t s8 = Smem<8, GEO_EXACT, true>::bytes(P.boxbytes), s4 = Smem<4, GEO_EXACT, true>::bytes(P.boxbytes);
+        if (s8 <= kMaxSmem) return go(k_fdk_staged<MR_F32, true, 8>, s8);
+        if (s4 <= kMaxSmem) return go(k_fdk_staged<MR_F32, true, 4>, s4);
+        return MR_ERR_UNSUPPORTED;
     }
-    return check_launch("k_fdk_tma");
+    const size_t s8 = Smem<8, GEO_FAST, false>::bytes(P.boxbytes), s4 = Smem<4, GEO_FAST, false>::bytes(P.boxbytes);
+    if (dtype == MR_BF16) {
+        if (s8 <= kMaxSmem) return go(k_fdk_staged<MR_BF16, false, 8>, s8);
+        if (s4 <= kMaxSmem) return go(k_fdk_staged<MR_BF16, false, 4>, s4);
+    } else if (dtype == MR_F16) {
+        if (s8 <= kMaxSmem) return go(k_fdk_staged<MR_F16, false, 8>, s8);
+        if (s4 <= kMaxSmem) return go(k_fdk_staged<MR_F16, false, 4>, s4);
+    }
+    return MR_ERR_UNSUPPORTED;
+}
+
+mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
+                         const float *xip_d, const float *yip_d, const float *zip_d, const uint32_t *mask_d,
+                         int accumulate, float *vol_d, int bw, int bh, cudaStream_t s)
+{
+    return staged_launch(true, proj_d, dtype, scale_d, nu, nv, nproj, xip_d, yip_d, zip_d, nullptr, mask_d, accumulate,
+                         vol_d, bw, bh, s);
 }
 
 mr_status fdk_box_for(const float *xip_h, const float *yip_h, const float *zip_h, size_t nu, size_t nv, size_t nproj,
                       int dtype, int *bw, int *bh)
 {
     const int xalign = dtype == MR_F32 ? 4 : 8;
-    fdk_box_guess(xip_h, yip_h, zip_h, nu, nv, nproj, xalign, *bw, *bh);
+    fdk2::box_guess(nu, nv, nproj, xalign, *bw, *bh,
+                    [&](size_t p, int i0, int i1, int j0, int j1, int k0, int k1, double &r, double &c) {
+                        fdk2::tile_footprint(xip_h + p * nu * 3, yip_h + p * nu * 3, zip_h + p * nv * 3, i0, i1, j0, j1,
+                                             k0, k1, r, c);
+                    });
     return MR_OK;
 }
 
@@ -467,6 +811,58 @@ mr_status mr_fdk_box(const float *xip_h, const float *yip_h, const float *zip_h,
         return MR_OK;
     }
     return fdk_box_for(xip_h, yip_h, zip_h, nu, nv, nproj, dtype, box_w, box_h);
+}
+
+mr_status mr_fdk_box_maps(const double *maps_h, size_t nu, size_t nv, size_t nproj, int dtype, int *box_w, int *box_h)
+{
+    if (!maps_h || !box_w || !box_h) return fail(MR_ERR_ARGUMENT, "mr_fdk_box_maps: null pointer");
+    if (dtype != MR_F32 && dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_fdk_box_maps: dtype");
+    if (nu == 0 || nv == 0 || nproj == 0) {
+        *box_w = *box_h = 0;
+        return MR_OK;
+    }
+    const int xalign = dtype == MR_F32 ? 4 : 8;
+    fdk2::box_guess(nu, nv, nproj, xalign, *box_w, *box_h,
+                    [&](size_t p, int i0, int i1, int j0, int j1, int k0, int k1, double &r, double &c) {
+                        fdk2::tile_footprint_maps(maps_h + p * 12, i0, i1, j0, j1, k0, k1, r, c);
+                    });
+    return MR_OK;
+}
+
+mr_status mr_fdk_backproject_fast(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
+                                  size_t nproj, const float *maps_d, const uint32_t *mask_d, int box_w, int box_h,
+                                  int accumulate, float *vol_d, void *stream)
+{
+    if (!proj_d || !scale_d || !maps_d || !mask_d || !vol_d)
+        return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_fast: null pointer");
+    if (dtype != MR_BF16 && dtype != MR_F16)
+        return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_fast: dtype must be MR_BF16 or MR_F16");
+    if (nu == 0 || nv == 0 || nu > 65536 || nv > 65536)
+        return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_fast: unsupported size");
+    if (nproj == 0 || nproj > 0x7fffffff) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_fast: projection count");
+    mr_status st = staged_launch(false, proj_d, dtype, scale_d, nu, nv, nproj, nullptr, nullptr, nullptr, maps_d,
+                                 mask_d, accumulate, vol_d, box_w, box_h, as_stream(stream));
+    if (st == MR_ERR_UNSUPPORTED)
+        return fail(MR_ERR_UNSUPPORTED,
+                    "mr_fdk_backproject_fast: layout or box not supported (row pitch must be a multiple of 16 bytes, "
+                    "box from mr_fdk_box_maps)");
+    return st;
+}
+
+mr_status mr_fdk_backproject_f64(const float *proj_d, size_t nu, size_t nv, size_t nproj, const double *maps_d,
+                                 const uint32_t *mask_d, const int *slices_d, size_t nslices, double *out_d,
+                                 void *stream)
+{
+    if (!proj_d || !maps_d || !mask_d || !slices_d || !out_d)
+        return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_f64: null pointer");
+    if (nslices == 0 || nslices > 16) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_f64: 1 to 16 slices");
+    if (nu == 0 || nv == 0 || nu > 65536 || nv > 65536 || nproj > 0x7fffffff)
+        return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_f64: unsupported size");
+    dim3 grid(div_up(nu, 128), static_cast<unsigned>(nu));
+    fdk2::k_fdk_f64<<<grid, 128, 0, as_stream(stream)>>>(proj_d, static_cast<int>(nu), static_cast<int>(nv),
+                                                         static_cast<int>(nproj), maps_d, mask_d, slices_d,
+                                                         static_cast<int>(nslices), out_d);
+    return check_launch("k_fdk_f64");
 }
 
 mr_status mr_device_status(int *status)

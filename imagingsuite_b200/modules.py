@@ -639,6 +639,15 @@ class FDKbp_single(_BackProjectorBase):
                                       ctypes.byref(uni)))
         return xip, yip, zip_, s2.value, sc.value, uni.value
 
+    def maps64(self, angles: np.ndarray) -> np.ndarray:
+        """FP64 per-projection detector maps (nproj, 12) (mr_fdk_maps64)."""
+        a = np.ascontiguousarray(angles, np.float32)
+        m = np.zeros((a.size, 12), np.float64)
+        g = self.geometry()
+        check(L.lib().mr_fdk_maps64(ctypes.byref(g), self.SizeU, self.SizeV, a.ctypes.data_as(L.P_float), a.size,
+                                    m.ctypes.data_as(L.P_double)))
+        return m
+
     def Process(self, projections: torch.Tensor, parameters: dict) -> int:
         if self.volume is None:
             raise ReconException("The target matrix is not allocated.")
@@ -653,19 +662,26 @@ class FDKbp_single(_BackProjectorBase):
         dev = projections.device
         # per-projection geometry depends only on the configuration and the angles: keep the
         # device copies while they stay the same
-        key = (angles.tobytes(), weights.tobytes(), str(dev))
+        dtype = _PRECISION[self.precision]
+        key = (angles.tobytes(), weights.tobytes(), str(dev), dtype)
         if getattr(self, "_geo_key", None) != key:
             xip, yip, zip_, s2, sc, uni = self.partials(angles)
             bw, bh = ctypes.c_int(0), ctypes.c_int(0)
-            if uni:
+            maps = None
+            if uni and dtype != L.MR_F32:
+                # precision form: FP64 detector maps, rounded once to float for the kernel
+                m64 = self.maps64(angles)
+                check(L.lib().mr_fdk_box_maps(m64.ctypes.data_as(L.P_double), nu, nv, nproj, dtype, ctypes.byref(bw),
+                                              ctypes.byref(bh)))
+                maps = torch.from_numpy(m64.astype(np.float32)).to(dev)
+            elif uni:
                 check(L.lib().mr_fdk_box(xip.ctypes.data_as(L.P_float), yip.ctypes.data_as(L.P_float),
-                                         zip_.ctypes.data_as(L.P_float), nu, nv, nproj, _PRECISION[self.precision],
+                                         zip_.ctypes.data_as(L.P_float), nu, nv, nproj, dtype,
                                          ctypes.byref(bw), ctypes.byref(bh)))
             self._geo = (torch.from_numpy(weights).to(dev), *(torch.from_numpy(a).to(dev) for a in (xip, yip, zip_)),
-                         s2, sc, uni, (bw.value, bh.value))
+                         s2, sc, uni, (bw.value, bh.value), maps)
             self._geo_key = key
-        w, X, Y, Z, s2, sc, uni, box = self._geo
-        dtype = _PRECISION[self.precision]
+        w, X, Y, Z, s2, sc, uni, box, maps = self._geo
         if dtype == L.MR_F32:
             filt = torch.empty_like(projections)
             scale = None
@@ -676,9 +692,15 @@ class FDKbp_single(_BackProjectorBase):
         check(L.lib().mr_fdk_filter(projections.data_ptr(), nu, nv, nproj, w.data_ptr(), s2, sc, dtype, filt.data_ptr(),
                                     _ptr(scale), st))
         box = box if self.staging else (0, 0)
-        check(L.lib().mr_fdk_backproject(filt.data_ptr(), dtype, _ptr(scale), nu, nv, nproj, X.data_ptr(), Y.data_ptr(),
-                                         Z.data_ptr(), uni, self._mask.data_ptr(), box[0], box[1],
-                                         int(not self._first), self.volume.data_ptr(), st))
+        if maps is not None and box[0] > 0 and nu % 8 == 0:
+            check(L.lib().mr_fdk_backproject_fast(filt.data_ptr(), dtype, scale.data_ptr(), nu, nv, nproj,
+                                                  maps.data_ptr(), self._mask.data_ptr(), box[0], box[1],
+                                                  int(not self._first), self.volume.data_ptr(), st))
+        else:
+            check(L.lib().mr_fdk_backproject(filt.data_ptr(), dtype, _ptr(scale), nu, nv, nproj, X.data_ptr(),
+                                             Y.data_ptr(), Z.data_ptr(), uni, self._mask.data_ptr(),
+                                             box[0] if maps is None else 0, box[1] if maps is None else 0,
+                                             int(not self._first), self.volume.data_ptr(), st))
         self._first = False
         return 0
 

@@ -249,6 +249,37 @@ mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d
 mr_status mr_fdk_box(const float *xip_h, const float *yip_h, const float *zip_h, size_t nu, size_t nv, size_t nproj,
                      int dtype, int *box_w, int *box_h);
 
+/* ---- FDK precision form (no counterpart in the reference's API; the geometry restates
+ * FDKbp, the double-geometry variant of the cone-beam backprojector, fdkbp.cpp:83-640).
+ *
+ * Per-projection detector maps in FP64 (host): for voxel (i, j, k) of the nu x nu x nv grid
+ * of project_volume_onto_image_c, with m = maps_h + 12 p,
+ *   u = m[0] i + m[1] j + m[2] k + m[3],  v = m[4] i + m[5] j + m[6] k + m[7],
+ *   w = m[8] i + m[9] j + m[10] k + m[11];
+ * the voxel samples detector column floor(u/w + 0.5), row floor(v/w + 0.5) with weight
+ * 1/w^2. The row window that sets the image centre is the float path's. */
+mr_status mr_fdk_maps64(const mr_fdk_geom *g, size_t nu, size_t nv, const float *angles_h, size_t nproj,
+                        double *maps_h);
+/* Staging box of mr_fdk_backproject_fast from the FP64 maps (host). */
+mr_status mr_fdk_box_maps(const double *maps_h, size_t nu, size_t nv, size_t nproj, int dtype, int *box_w, int *box_h);
+/* Nearest-neighbour FDK backprojection of 16-bit filtered projections (MR_BF16 or MR_F16,
+ * value = stored * scale_d[p], from mr_fdk_filter or mr_quantize) through the maps rounded
+ * to float (maps_d [nproj][12] float, m[2] = m[10] = 0: no tilt correction), FP32
+ * accumulation, into the final volume layout of mr_fdk_backproject. Each weighted sample
+ * is one mixed-precision fma with the weight 1/w^2 * scale rounded to the storage type.
+ * Requires a TMA-compatible layout (row pitch a multiple of 16 bytes) and a box from
+ * mr_fdk_box_maps; returns MR_ERR_UNSUPPORTED otherwise. Accuracy against the FP64
+ * backprojection is reported by the tests and the benchmark, not bit-exact. */
+mr_status mr_fdk_backproject_fast(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
+                                  size_t nproj, const float *maps_d, const uint32_t *mask_d, int box_w, int box_h,
+                                  int accumulate, float *vol_d, void *stream);
+/* FP64 error oracle on the device: backprojection of FP32 filtered projections through the
+ * FP64 maps with FP64 accumulation, for 1..16 output slices (indices into the final volume's
+ * z); out_d [nslices][nu][nu] in the final layout. Restated on the CPU by the oracle. */
+mr_status mr_fdk_backproject_f64(const float *proj_d, size_t nu, size_t nv, size_t nproj, const double *maps_d,
+                                 const uint32_t *mask_d, const int *slices_d, size_t nslices, double *out_d,
+                                 void *stream);
+
 /* Device-side error word of bounded waits inside kernels (0 = none); reading it
  * synchronizes the device and clears the word. */
 mr_status mr_device_status(int *status);

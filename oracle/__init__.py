@@ -317,6 +317,28 @@ def fdk_bp(filtered, angles, geom: FdkGeom) -> np.ndarray:
     return vol
 
 
+def fdk_maps64(geom: FdkGeom, nu, nv, angles) -> np.ndarray:
+    """FP64 detector maps (nproj, 12) of the FDK geometry (FDKbp's double geometry)."""
+    a = _f32(angles)
+    m = np.zeros((a.size, 12), np.float64)
+    orc().orc_fdk_maps64(ctypes.byref(geom), _sz(nu), _sz(nv), _p(a), _sz(a.size), _p(m, ctypes.POINTER(ctypes.c_double)))
+    return m
+
+
+def fdk_bp64(filtered, maps, slices, mask=None) -> np.ndarray:
+    """FP64 backprojection of FP32 filtered projections for output slices ``slices`` of the
+    final volume. Returns (len(slices), nu, nu) float64."""
+    filtered = _f32(filtered)
+    nproj, nv, nu = filtered.shape
+    maps = np.ascontiguousarray(maps, np.float64)
+    sl = np.ascontiguousarray(slices, np.int32)
+    m = np.ascontiguousarray(circle_mask(nu, nu) if mask is None else mask, np.uintp)
+    out = np.zeros((sl.size, nu, nu), np.float64)
+    orc().orc_fdk_bp64(_p(filtered), _sz(nu), _sz(nv), _sz(nproj), _p(maps, ctypes.POINTER(ctypes.c_double)), _p(m, _SZ),
+                       _p(sl, ctypes.POINTER(ctypes.c_int)), _sz(sl.size), _p(out, ctypes.POINTER(ctypes.c_double)))
+    return out
+
+
 def bp_geometry(angles, nu, center, direction=0):
     a = _f32(angles)
     s, c, su = (np.empty_like(a) for _ in range(3))

@@ -470,34 +470,20 @@ void orc_fdk_ramp(float *img, size_t width, size_t height)
     free(pad);
 }
 
-/* FdkReconBase::Process 3D + FDKbp_single::reconstruct/project_volume_onto_image_c
- * (fdkreconbase.cpp:217-277, fdkbp_single.cpp:259-531,641-683). Full detector ROI
- * (roi = projection_roi = {0,0,nu,nv}), volume nu x nu x nv. */
-static int fdk_core(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
-                    const orc_fdk_geom *g, int prefiltered, float *vol)
+/* Volume origin and CBCT row window of project_volume_onto_image_c (fdkbp_single.cpp:302-372)
+ * for roi = projection_roi = {0, 0, nu, nv}, volume nu x nu x nv. */
+static void fdk_frame(const orc_fdk_geom *g, size_t nu, size_t nv, float origin[3], size_t cb[4])
 {
-    const size_t sx = nu, sy = nu, sz = nv;
-    const size_t npix = nu * nv;
-    size_t *mask = (size_t *)malloc(2 * sy * sizeof(size_t));
-    circle_mask(sx, sy, g->correcttilt, g->tiltangle, nv, mask);
-    float *cbct = (float *)calloc(sx * sy * sz, sizeof(float));
-    float *img = (float *)malloc(npix * sizeof(float));
-    float *xip = (float *)malloc(3 * sx * sizeof(float));
-    float *yip = (float *)malloc(3 * sy * sizeof(float));
-    float *zip = (float *)malloc(3 * sz * sizeof(float));
+    const size_t sy = nu;
     const size_t roi[4] = {0, 0, nu, nv}, proi3 = nv;
-
-    /* geometry constants of project_volume_onto_image_c (fdkbp_single.cpp:302-386) */
-    const float scale = g->sod / g->sdd;
     const float *spacing = g->voxelsize;
     const float U = (float)(roi[2] - roi[0]);
     const float V = (float)(roi[3] - roi[1]);
-    float origin[3];
     origin[0] = -(U - g->center) * spacing[0] - spacing[0] / 2;
     origin[1] = -(U - g->center) * spacing[1] - spacing[1] / 2;
     origin[2] = -(V - (g->ppoint[1] - (float)roi[1])) * spacing[2] - spacing[2] / 2;
     const float radius = (float)sy * g->voxelsize[0] / 2;
-    size_t cb[4] = {roi[0], 0, roi[2], 0};
+    cb[0] = roi[0]; cb[1] = 0; cb[2] = roi[2]; cb[3] = 0;
     const float fp1 = g->ppoint[1], r1 = (float)roi[1], r3 = (float)roi[3];
     const float vx = g->voxelsize[0], sdd = g->sdd, sod = g->sod, res0 = g->resolution[0];
     if (fp1 >= r1 && fp1 >= r3) {
@@ -519,6 +505,30 @@ static int fdk_core(const float *proj, size_t nu, size_t nv, size_t nproj, const
     }
     if (cb[1] != 0) cb[1] -= 8;
     if (cb[3] + 8 <= proi3) cb[3] += 8;
+}
+
+/* FdkReconBase::Process 3D + FDKbp_single::reconstruct/project_volume_onto_image_c
+ * (fdkreconbase.cpp:217-277, fdkbp_single.cpp:259-531,641-683). Full detector ROI
+ * (roi = projection_roi = {0,0,nu,nv}), volume nu x nu x nv. */
+static int fdk_core(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
+                    const orc_fdk_geom *g, int prefiltered, float *vol)
+{
+    const size_t sx = nu, sy = nu, sz = nv;
+    const size_t npix = nu * nv;
+    size_t *mask = (size_t *)malloc(2 * sy * sizeof(size_t));
+    circle_mask(sx, sy, g->correcttilt, g->tiltangle, nv, mask);
+    float *cbct = (float *)calloc(sx * sy * sz, sizeof(float));
+    float *img = (float *)malloc(npix * sizeof(float));
+    float *xip = (float *)malloc(3 * sx * sizeof(float));
+    float *yip = (float *)malloc(3 * sy * sizeof(float));
+    float *zip = (float *)malloc(3 * sz * sizeof(float));
+    const size_t roi[4] = {0, 0, nu, nv};
+
+    const float scale = g->sod / g->sdd;
+    const float *spacing = g->voxelsize;
+    float origin[3];
+    size_t cb[4];
+    fdk_frame(g, nu, nv, origin, cb);
     const float ic[2] = {g->ppoint[0] - (float)cb[0], g->ppoint[1] - (float)cb[1]};
     const float sad_sid_2 = (g->sod * g->sod) / (g->sdd * g->sdd);
 
@@ -611,6 +621,113 @@ void orc_fdk_prepare(float *proj, size_t nu, size_t nv, size_t nproj, const floa
         for (size_t i = 0; i < nu * nv; ++i) {
             img[i] *= sad_sid_2;
             img[i] *= scale;
+        }
+    }
+}
+
+/* ---------------------------------------------------- FDK in FP64 (error oracle)
+ *
+ * FDKbp (fdkbp.cpp:83-640) is FDKbp_single with double geometry. This is that geometry in
+ * double, folded into affine maps of the voxel indices (u, v, w rows; 12 doubles per
+ * projection): voxel (i, j, k) samples column floor(u/w + 0.5), row floor(v/w + 0.5) with
+ * weight (1/w)^2. The row window and the image centre come from the float frame, as in
+ * FDKbp_single. Tilt correction folds its per-slice pm[3] (fdkbp_single.cpp:438-444) into
+ * the k coefficient of u. */
+static void projmatrix64(const orc_fdk_geom *g, double angle, double *pm)
+{
+    double ext[16] = {0}, intr[12] = {0};
+    const double sad = g->sod, sid = g->sdd;
+    const double offcenter = ((double)g->ppoint[0] - g->center) * g->voxelsize[0];
+    const double a = (g->direction == 0 ? -angle : angle) * kDPi / 180.0;
+    const double cam[3] = {sad * cos(a), sad * sin(a), 0.0};
+    const double nn = sqrt(cam[0] * cam[0] + cam[1] * cam[1] + cam[2] * cam[2]);
+    const double nrm[3] = {cam[0] / nn, cam[1] / nn, cam[2] / nn};
+    double plt[3] = {nrm[1], -nrm[0], 0.0}; /* nrm x (0, 0, 1) */
+    const double np = sqrt(plt[0] * plt[0] + plt[1] * plt[1]);
+    plt[0] /= np;
+    plt[1] /= np;
+    double pup[3] = {plt[1] * nrm[2] - plt[2] * nrm[1], plt[2] * nrm[0] - plt[0] * nrm[2], plt[0] * nrm[1] - plt[1] * nrm[0]};
+    const double nq = sqrt(pup[0] * pup[0] + pup[1] * pup[1] + pup[2] * pup[2]);
+    for (int c = 0; c < 3; ++c) {
+        pup[c] /= nq;
+        ext[c] = -plt[c];
+        ext[4 + c] = -pup[c];
+        ext[8 + c] = -nrm[c];
+    }
+    ext[3] = -offcenter;
+    ext[11] = sad;
+    ext[15] = 1.0;
+    intr[0] = 1.0 / g->resolution[0];
+    intr[5] = 1.0 / g->resolution[1];
+    intr[10] = 1.0 / sid;
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 4; ++j) {
+            double acc = 0.0;
+            for (int k = 0; k < 4; ++k) acc += intr[i * 4 + k] * ext[k * 4 + j];
+            pm[i * 4 + j] = acc;
+        }
+}
+
+void orc_fdk_maps64(const orc_fdk_geom *g, size_t nu, size_t nv, const float *angles, size_t nproj, double *maps)
+{
+    float originf[3];
+    size_t cb[4];
+    fdk_frame(g, nu, nv, originf, cb);
+    const double s0 = g->voxelsize[0], s1 = g->voxelsize[1], s2 = g->voxelsize[2];
+    const double o0 = -((double)nu - g->center) * s0 - s0 / 2, o1 = -((double)nu - g->center) * s1 - s1 / 2;
+    const double o2 = -((double)nv - (double)g->ppoint[1]) * s2 - s2 / 2;
+    const double ic0 = (double)g->ppoint[0] - (double)cb[0], ic1 = (double)g->ppoint[1] - (double)cb[1];
+    const double tt = g->correcttilt ? tan(-(double)g->tiltangle * kDPi / 180.0) : 0.0;
+    for (size_t p = 0; p < nproj; ++p) {
+        double pm[12];
+        projmatrix64(g, angles[p], pm);
+        double pm3 = pm[3], pm3k = 0.0;
+        if (g->correcttilt) {
+            const double c0 = tt * ((double)cb[3] - g->tiltpivot) + g->center;
+            pm3 = ((c0 - g->ppoint[0]) * g->voxelsize[0]) / g->resolution[0];
+            pm3k = -tt * g->voxelsize[0] / g->resolution[0];
+        }
+        const double A[3] = {pm[0] + ic0 * pm[8], pm[4] + ic1 * pm[8], pm[8]};
+        const double B[3] = {pm[1] + ic0 * pm[9], pm[5] + ic1 * pm[9], pm[9]};
+        const double C[3] = {pm[2] + ic0 * pm[10], pm[6] + ic1 * pm[10], pm[10]};
+        const double D[3] = {ic0 * pm[11] + pm3, ic1 * pm[11] + pm[7], pm[11]};
+        const double Dk[3] = {pm3k, 0.0, 0.0};
+        double *m = maps + p * 12;
+        for (int r = 0; r < 3; ++r) {
+            m[4 * r + 0] = A[r] * s0;
+            m[4 * r + 1] = B[r] * s1;
+            m[4 * r + 2] = C[r] * s2 + Dk[r];
+            m[4 * r + 3] = A[r] * o0 + B[r] * o1 + C[r] * o2 + D[r];
+        }
+    }
+}
+
+/* FP64 backprojection of FP32 filtered projections for the listed output slices of the
+ * final volume (z reversed, x mirrored as in fdkreconbase.cpp:259-270); projections are
+ * accumulated in order, as FdkReconBase::Process does. out [nslices][nu][nu]. */
+void orc_fdk_bp64(const float *filtered, size_t nu, size_t nv, size_t nproj, const double *maps, const size_t *mask,
+                  const int *slices, size_t nslices, double *out)
+{
+#pragma omp parallel for schedule(dynamic)
+    for (long js = 0; js < (long)(nu * nslices); ++js) {
+        const size_t s = (size_t)js / nu, j = (size_t)js % nu;
+        const double k = (double)(nv - 1 - (size_t)slices[s]);
+        double *line = out + (s * nu + j) * nu;
+        for (size_t i = 0; i < nu; ++i) line[nu - 1 - i] = 0.0;
+        for (size_t i = mask[2 * j] + 1; i <= mask[2 * j + 1] && i < nu; ++i) {
+            double acc = 0.0;
+            for (size_t p = 0; p < nproj; ++p) {
+                const double *m = maps + p * 12;
+                const double u = m[0] * (double)i + m[1] * (double)j + m[2] * k + m[3];
+                const double v = m[4] * (double)i + m[5] * (double)j + m[6] * k + m[7];
+                const double w = m[8] * (double)i + m[9] * (double)j + m[10] * k + m[11];
+                const double dw = 1.0 / w;
+                const double r = dw * v + 0.5, c = dw * u + 0.5;
+                if (r < 0 || r >= (double)nv || c < 0 || c >= (double)nu) continue;
+                const double val = filtered[p * nu * nv + (size_t)(int)r * nu + (size_t)(int)c];
+                acc += dw * dw * val;
+            }
+            line[nu - 1 - i] = acc;
         }
     }
 }

@@ -74,6 +74,10 @@ int orc_fdk_bp(const float *filtered, size_t nu, size_t nv, size_t nproj, const 
                float *vol);
 void orc_fdk_ramp(float *img, size_t width, size_t height);
 void orc_fdk_projmatrix(const orc_fdk_geom *g, size_t nu, float angle, float *pm /*12*/);
+/* FP64 error oracle: detector maps in double and the FP64 backprojection of listed slices */
+void orc_fdk_maps64(const orc_fdk_geom *g, size_t nu, size_t nv, const float *angles, size_t nproj, double *maps);
+void orc_fdk_bp64(const float *filtered, size_t nu, size_t nv, size_t nproj, const double *maps, const size_t *mask,
+                  const int *slices, size_t nslices, double *out);
 
 /* kipl morphology and MorphSpotClean (core/kipl/kipl/include/morphology/morphgeo.h,
  * morphextrema.h; core/algorithms/ImagingAlgorithms/src/MorphSpotClean.cpp). Images [h][w]. */

@@ -153,3 +153,65 @@ def test_wavelet_kernel_rejects_unknown():
     b, e = ctypes.c_int(), ctypes.c_int()
     assert L.lib().mr_wavelet_kernel(b"haar", ctypes.byref(b), ctypes.byref(e), None) == L.MR_ERR_UNSUPPORTED
     assert L.lib().mr_wavelet_kernel(b"daub31", ctypes.byref(b), ctypes.byref(e), None) == L.MR_ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("tilt", [0.0, 0.4])
+@pytest.mark.parametrize("direction", [0, 1])
+def test_fdk_maps64_match_oracle_and_partials(tilt, direction):
+    """FP64 detector maps equal the oracle's restatement bit for bit and agree with the float
+    partials of FDKbp_single to float rounding (1e-4 pixel)."""
+    nu, nv = 40, 36
+    ang = (np.arange(16) * 22.5 + 3.3).astype(np.float32)
+    og = O.fdk_geom(300.0, 600.0, (20.3, 17.1), 19.7, (0.2, 0.2), (0.1, 0.1, 0.1), direction=direction,
+                    correcttilt=bool(tilt), tiltangle=tilt, tiltpivot=3.0)
+    g = L.FdkGeom()
+    ctypes.memmove(ctypes.byref(g), ctypes.byref(og), ctypes.sizeof(g))
+    m = np.zeros((ang.size, 12), np.float64)
+    L.check(L.lib().mr_fdk_maps64(ctypes.byref(g), nu, nv, ang.ctypes.data_as(L.P_float), ang.size,
+                                  m.ctypes.data_as(L.P_double)))
+    assert np.array_equal(m, O.fdk_maps64(og, nu, nv, ang))
+    xip, yip, zip_, *_ = _partials(g, nu, nv, ang)
+    i, j, k = np.meshgrid(np.arange(0, nu, 7), np.arange(0, nu, 5), np.arange(0, nv, 6), indexing="ij")
+    for p in range(ang.size):
+        a = [zip_[p, k, e].astype(np.float64) + yip[p, j, e] + xip[p, i, e] for e in range(3)]
+        M_ = m[p]
+        u = M_[0] * i + M_[1] * j + M_[2] * k + M_[3]
+        v = M_[4] * i + M_[5] * j + M_[6] * k + M_[7]
+        w = M_[8] * i + M_[9] * j + M_[10] * k + M_[11]
+        assert np.abs(a[0] / a[2] - u / w).max() < 1e-4
+        assert np.abs(a[1] / a[2] - v / w).max() < 1e-4
+        assert np.abs(a[2] / w - 1).max() < 1e-5
+    if not tilt:
+        assert np.all(m[:, 2] == 0) and np.all(m[:, 10] == 0)  # column and depth do not depend on the slice
+
+
+def test_fdk_box_maps_covers_partials_box():
+    nu, nv, n = 64, 48, 32
+    ang = (np.arange(n) * 360.0 / n).astype(np.float32)
+    og = O.fdk_geom(300.0, 600.0, (31.7, 23.2), 31.6, (0.2, 0.2), (0.1, 0.1, 0.1))
+    g = L.FdkGeom()
+    ctypes.memmove(ctypes.byref(g), ctypes.byref(og), ctypes.sizeof(g))
+    xip, yip, zip_, *_ = _partials(g, nu, nv, ang)
+    m = O.fdk_maps64(og, nu, nv, ang)
+    a, b, c, d = (ctypes.c_int() for _ in range(4))
+    L.check(L.lib().mr_fdk_box(xip.ctypes.data_as(L.P_float), yip.ctypes.data_as(L.P_float),
+                               zip_.ctypes.data_as(L.P_float), nu, nv, n, L.MR_BF16, ctypes.byref(a), ctypes.byref(b)))
+    L.check(L.lib().mr_fdk_box_maps(m.ctypes.data_as(L.P_double), nu, nv, n, L.MR_BF16, ctypes.byref(c), ctypes.byref(d)))
+    assert (a.value, b.value) == (c.value, d.value)
+    assert c.value % 8 == 0 and c.value > 32 and d.value > 32
+
+
+def test_fdk_bp64_oracle_close_to_float_path():
+    """The FP64 oracle and the reference's float arithmetic differ only where a voxel centre
+    projects within float rounding of a pixel boundary (nearest-neighbour ties)."""
+    rng = np.random.default_rng(5)
+    nu, nv, n = 48, 40, 24
+    proj = rng.standard_normal((n, nv, nu)).astype(np.float32)
+    ang = np.sort(rng.uniform(0, 360, n)).astype(np.float32)
+    og = O.fdk_geom(300.0, 600.0, (23.37, 19.61), 23.71, (0.2, 0.2), (0.1, 0.1, 0.1))
+    f32 = O.fdk_bp(proj, ang, og)
+    sl = np.array([0, 5, 17, 39], np.int32)
+    f64 = O.fdk_bp64(proj, O.fdk_maps64(og, nu, nv, ang), sl)
+    d = np.abs(f32[sl] - f64)
+    assert (d > 1e-4).sum() <= 10  # a handful of tie voxels out of 9216
+    assert np.median(d) < 1e-6
