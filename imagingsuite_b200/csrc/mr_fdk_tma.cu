@@ -6,8 +6,7 @@
 //    FDKbp_single::project_volume_onto_image_c (fdkbp_single.cpp:488-525) and
 //    get_pixel_value_c (:641-683), every per-voxel float operation in the reference's order
 //    with explicitly rounded intrinsics, so the FP32 volume is bit-identical to the
-//    reference's for identical filtered projections. Two slices share most instructions
-//    through the f32x2 operations of sm_100, arranged so that none is fused into an fma. The warp-uniform sums zip+yip of every slice are formed once per warp
+//    reference's for identical filtered projections. The warp-uniform sums zip+yip of every slice are formed once per warp
 //    and projection in shared memory.
 //  * k_fdk_fast (16-bit projections, the precision form): per-projection affine detector
 //    maps computed in FP64 on the host (FDKbp, fdkbp.cpp:83-640, is the double-geometry
@@ -49,6 +48,7 @@ __device__ int g_device_error = 0;
 namespace fdk2 {
 
 constexpr int TI = 32, TJ = 8, TK = 32, THREADS = TI * TJ, NWARPS = THREADS / 32;
+constexpr int CTAS_PER_SM = 2;
 constexpr float kMagic = 12582912.0f; // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
 constexpr int kWaitLimit = 1 << 22;
@@ -137,13 +137,6 @@ __device__ __forceinline__ float from_storage(unsigned short v)
     else return __half2float(__ushort_as_half(v));
 }
 
-// Paired f32 operations of sm_100. Each lane of an f32x2 add or mul rounds exactly like the
-// scalar add.rn / mul.rn, but ptxas fuses an f32x2 mul feeding an f32x2 add into an f32x2 fma,
-// even with explicit rounding modifiers and with contraction disabled (measured: 12 % of
-// results differ from mul-then-add on random operands). A paired mul followed by scalar
-// explicit-rounding adds, or scalar muls followed by a paired add, stays unfused (measured
-// bit-identical), so the exact path only pairs chains of those shapes.
-
 // Exact per-voxel detector coordinates (float, reference order), for the corner footprints.
 __device__ __forceinline__ void project_exact(const Params &P, int p, int i, int j, int k, float &r, float &c)
 {
@@ -183,22 +176,20 @@ __device__ __forceinline__ void exact_column(float2 (&acc)[TK / 2], const unsign
                                              uint32_t rowbytes, const float *a1, float x1f, float dw, float dw2,
                                              int kmax)
 {
-    const float2 x1 = make_float2(x1f, x1f), d = make_float2(dw, dw);
-    const float2 mg = make_float2(kMagic, kMagic), d2 = make_float2(dw2, dw2);
 #pragma unroll
-    for (int q = 0; q < TK / 2; ++q) {
-        if (!FULL && 2 * q >= kmax) break;
-        const float4 a4 = reinterpret_cast<const float4 *>(a1)[q >> 1];
-        const float2 a = (q & 1) ? make_float2(a4.z, a4.w) : make_float2(a4.x, a4.y);
-        const float2 p = __fmul2_rn(d, __fadd2_rn(a, x1));
-        const float2 r = make_float2(__fadd_rn(p.x, 0.5f), __fadd_rn(p.y, 0.5f));
-        const float2 b = __fadd2_rd(r, mg);
-        const float v0 = *reinterpret_cast<const float *>(smem + (__float_as_uint(b.x) * rowbytes + base));
-        float v1 = 0.0f;
-        if (FULL || 2 * q + 1 < kmax)
-            v1 = *reinterpret_cast<const float *>(smem + (__float_as_uint(b.y) * rowbytes + base));
-        const float2 w = __fmul2_rn(d2, make_float2(v0, v1));
-        acc[q] = make_float2(__fadd_rn(acc[q].x, w.x), __fadd_rn(acc[q].y, w.y));
+    for (int q4 = 0; q4 < TK / 4; ++q4) {
+        const float4 a4 = reinterpret_cast<const float4 *>(a1)[q4];
+        const float av[4] = {a4.x, a4.y, a4.z, a4.w};
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int q = 4 * q4 + e;
+            if (!FULL && q >= kmax) break;
+            const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(av[e], x1f)), 0.5f);
+            const uint32_t bits = __float_as_uint(__fadd_rd(r, kMagic));
+            const float v = *reinterpret_cast<const float *>(smem + (bits * rowbytes + base));
+            float &a = (q & 1) ? acc[q >> 1].y : acc[q >> 1].x;
+            a = __fadd_rn(a, __fmul_rn(dw2, v));
+        }
     }
 }
 
@@ -346,7 +337,7 @@ __device__ __forceinline__ void produce(const Params &P, const CUtensorMap *tmap
 }
 
 template <int DT, bool EXACT, int NB>
-__global__ void __launch_bounds__(THREADS, 2) k_fdk_staged(const __grid_constant__ CUtensorMap tmap, const Params P)
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __grid_constant__ CUtensorMap tmap, const Params P)
 {
     constexpr int GEO = EXACT ? GEO_EXACT : GEO_FAST;
     using T = typename Sample<DT>::T;
@@ -438,9 +429,9 @@ __global__ void __launch_bounds__(THREADS, 2) k_fdk_staged(const __grid_constant
         if constexpr (EXACT) {
             // per-warp slice sums a1[k] = zip1[k] + yip1[j] (lane = slice)
             if (warp_inside) {
-                for (int b = 0; b < NB; ++b) {
-                    const float *g = S.geo + (st * NB + b) * GEO_EXACT;
-                    S.a1[(warp * NB + b) * TK + lane] = __fadd_rn(g[lane], g[TK + 3 * TI + 3 * warp + 1]);
+                for (int idx = lane; idx < NB * TK; idx += 32) {
+                    const float *g = S.geo + (st * NB + idx / TK) * GEO_EXACT;
+                    S.a1[warp * NB * TK + idx] = __fadd_rn(g[idx % TK], g[TK + 3 * TI + 3 * warp + 1]);
                 }
                 __syncwarp();
             }
@@ -710,18 +701,7 @@ static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const 
     if (bw <= 0 || bh <= 0 || bw > 256 || bh > 256 || bw % xalign) return MR_ERR_UNSUPPORTED;
     PFN_cuTensorMapEncodeTiled enc = encode_fn();
     if (!enc) return fail(MR_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
-    constexpr size_t kMaxSmem = 112 * 1024; // two CTAs per SM
-    // Row pitch a multiple of 128 bytes when it fits: lanes of a warp read one or two adjacent
-    // rows of consecutive columns, and with such a pitch a row change moves no lane to
-    // another lane's bank.
-    {
-        const int wide = std::min(256, (bw + static_cast<int>(128 / es) - 1) / static_cast<int>(128 / es) *
-                                           static_cast<int>(128 / es));
-        const size_t boxw = (wide * bh * es + 127) / 128 * 128;
-        const size_t need = exact ? Smem<4, GEO_EXACT, true>::bytes(static_cast<int>(boxw))
-                                  : Smem<4, GEO_FAST, false>::bytes(static_cast<int>(boxw));
-        if (need <= kMaxSmem) bw = wide;
-    }
+    constexpr size_t kMaxSmem = (227 * 1024) / CTAS_PER_SM - 1024; // CTAS_PER_SM CTAs per SM
     CUtensorMap map;
     cuuint64_t dims[3] = {nu, nv, nproj};
     cuuint64_t strides[2] = {nu * es, nu * nv * es};
