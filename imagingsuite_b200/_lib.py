@@ -76,6 +76,12 @@ _PROTOS = {
                                         c_int, c_void, c_void]),
     "mr_fdk_backproject_f64": (c_int, [c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_size, c_void,
                                        c_void]),
+    "mr_joseph_geometry": (c_int, [P_float, c_size, c_size, P_float]),
+    "mr_joseph_forward": (c_int, [c_void, c_void, c_size, c_size, c_void, c_size, c_size, c_float, c_float, c_float,
+                                  c_void, c_void, c_void]),
+    "mr_joseph_adjoint": (c_int, [c_void, c_size, c_size, c_void, c_size, c_size, c_float, c_float, c_float, c_int,
+                                  c_void, c_void]),
+    "mr_slice_dot": (c_int, [c_void, c_void, c_size, c_size, c_size, c_void, c_void]),
     "mr_device_status": (c_int, [P_int]),
 }
 

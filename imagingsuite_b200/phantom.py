@@ -174,3 +174,27 @@ def cone_integrals_torch(ells, nproj: int, nu: int, nv: int, sod: float, sdd: fl
             tot += mu * torch.where(disc > 0, torch.sqrt(torch.clamp(disc, min=0)) / a, torch.zeros_like(a))
         out[k0:k0 + len(ks)] = tot
     return out
+
+
+def voxelize_torch(ells, n: int, nz: int, device, supersample: int = 1):
+    """Attenuation volume (nz, n, n), x fastest, of the ellipsoids on an n x n x nz voxel grid
+    whose x/y extent is the unit box and whose voxels are cubes (z covers nz/n of the box,
+    centred). Values are mu per voxel length (mu per box / n); supersample^3 points per voxel."""
+    import torch
+
+    s = supersample
+    off = (torch.arange(s, dtype=torch.float64, device=device) + 0.5) / s - 0.5
+    xs = ((torch.arange(n, dtype=torch.float64, device=device)[:, None] + off[None, :]).reshape(-1) - (n - 1) / 2) / n
+    zs = ((torch.arange(nz, dtype=torch.float64, device=device)[:, None] + off[None, :]).reshape(-1) - (nz - 1) / 2) / n
+    out = torch.zeros((nz, n, n), dtype=torch.float32, device=device)
+    for zi in range(nz):
+        z = zs[zi * s:(zi + 1) * s]
+        acc = torch.zeros((s, n * s, n * s), dtype=torch.float64, device=device)
+        pz, py, px = torch.meshgrid(z, xs, xs, indexing="ij")
+        p = torch.stack([px, py, pz], dim=-1)
+        for e in ells:
+            rot = torch.as_tensor(e.rot, dtype=torch.float64, device=device)
+            q = ((p - torch.as_tensor(e.center, device=device)) @ rot) / torch.as_tensor(e.axes, device=device)
+            acc += e.mu * ((q * q).sum(-1) <= 1.0)
+        out[zi] = (acc.reshape(s, n, s, n, s).mean(dim=(0, 2, 4)) / n).float()
+    return out

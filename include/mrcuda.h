@@ -280,6 +280,31 @@ mr_status mr_fdk_backproject_f64(const float *proj_d, size_t nu, size_t nv, size
                                  const uint32_t *mask_d, const int *slices_d, size_t nslices, double *out_d,
                                  void *stream);
 
+/* ---- Differentiable parallel-beam projector pair (the Joseph projector of
+ * LinearForwardProjector::project, ReconAlgorithms/linearforwardprojector.cpp:15-144, and its
+ * exact transpose; the reference has no adjoint and no multi-slice form).
+ *
+ * Volume [nz][n][n] (x fastest), projections [nproj][nz][nu] (detector bin fastest), angles
+ * in degrees. Slice z uses the detector centre c_z = centre + tan_tilt * (z - pivot), in
+ * detector bins; centre = nu/2 (integer division) and tan_tilt = 0 give the reference's
+ * geometry. */
+/* Per-angle parameters in FP64, rounded once to float: params_h [nproj][8]. */
+mr_status mr_joseph_geometry(const float *angles_h, size_t nproj, size_t n, float *params_h);
+/* proj_d = A(centre, tilt) vol_d; when dproj_d is not NULL it receives d proj / d centre.
+ * volt_d: caller scratch of nz * n * n floats (the transposed slices). */
+mr_status mr_joseph_forward(const float *vol_d, float *volt_d, size_t n, size_t nz, const float *params_d,
+                            size_t nproj, size_t nu, float centre, float tan_tilt, float pivot, float *proj_d,
+                            float *dproj_d, void *stream);
+/* vol_d (=|+=) A^T proj_d: the exact transpose of mr_joseph_forward (same weights, same
+ * sample set), voxel-driven. */
+mr_status mr_joseph_adjoint(const float *proj_d, size_t n, size_t nz, const float *params_d, size_t nproj, size_t nu,
+                            float centre, float tan_tilt, float pivot, int accumulate, float *vol_d, void *stream);
+/* out_d[z] = sum over projections and bins of a_d * b_d for every slice z (FP64), e.g. the
+ * centre derivative against a residual: d/d centre = sum_z out_d[z], d/d tan_tilt =
+ * sum_z (z - pivot) out_d[z]. */
+mr_status mr_slice_dot(const float *a_d, const float *b_d, size_t nproj, size_t nz, size_t nu, double *out_d,
+                       void *stream);
+
 /* Device-side error word of bounded waits inside kernels (0 = none); reading it
  * synchronizes the device and clears the word. */
 mr_status mr_device_status(int *status);

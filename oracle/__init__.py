@@ -478,3 +478,44 @@ def waveletringclean(proj, wname="daub15", decnum=2, sigma=0.05, use_ref=False) 
     for j in range(nv):
         out[:, j, :] = stripefilter(out[:, j, :], wname, decnum, sigma)
     return out
+
+
+# --------------------------------------------------------------------- Joseph projector pair
+
+_DP = ctypes.POINTER(ctypes.c_double)
+
+
+def joseph_forward64(vol, angles, nu, centre, tan_tilt=0.0, pivot=0.0, derivative=False):
+    """FP64 Joseph forward projection of vol (nz, n, n); returns proj (nproj, nz, nu) and, with
+    derivative=True, d proj / d centre."""
+    vol = _f32(vol)
+    nz, n, _ = vol.shape
+    a = _f32(angles)
+    proj = np.zeros((a.size, nz, nu), np.float64)
+    d = np.zeros_like(proj) if derivative else None
+    orc().orc_joseph_forward64(_p(vol), _sz(n), _sz(nz), _p(a), _sz(a.size), _sz(nu), ctypes.c_double(centre),
+                               ctypes.c_double(tan_tilt), ctypes.c_double(pivot), _p(proj, _DP),
+                               _p(d, _DP) if derivative else None)
+    return (proj, d) if derivative else proj
+
+
+def joseph_adjoint64(proj, angles, n, centre, tan_tilt=0.0, pivot=0.0):
+    """Exact transpose of joseph_forward64. proj (nproj, nz, nu) -> vol (nz, n, n) float64."""
+    proj = np.ascontiguousarray(proj, np.float64)
+    nproj, nz, nu = proj.shape
+    a = _f32(angles)
+    vol = np.zeros((nz, n, n), np.float64)
+    orc().orc_joseph_adjoint64(_p(proj, _DP), _sz(n), _sz(nz), _p(a), _sz(nproj), _sz(nu), ctypes.c_double(centre),
+                               ctypes.c_double(tan_tilt), ctypes.c_double(pivot), _p(vol, _DP))
+    return vol
+
+
+def ref_joseph_project(slice2d, angles) -> np.ndarray:
+    """The reference LinearForwardProjector on one slice (n, n); returns (nangles, n)."""
+    sl = _f32(slice2d)
+    n = sl.shape[0]
+    a = _f32(angles)
+    out = np.zeros((a.size, n), np.float32)
+    _check_ref(ref().ref_joseph_project(_p(sl), _sz(n), _p(a), _sz(a.size), _p(out)))
+    return out
+

@@ -1205,3 +1205,107 @@ int orc_stripefilter(float *img, size_t nu, size_t ntheta, const float *kern, in
     for (int q = 1; q <= nlevels; ++q) { free(a[q]); free(h[q]); free(v[q]); free(d[q]); }
     return 0;
 }
+
+/* ------------------------------------------------ Joseph projector pair (FP64)
+ *
+ * LinearForwardProjector::project 2-D (linearforwardprojector.cpp:15-144) applied to every
+ * slice z of a volume [nz][n][n] (x fastest), with the detector centre of slice z at
+ * centre + tan_tilt * (z - pivot) instead of the reference's fixed R/2 (rho = r - centre;
+ * centre = nu/2, tan_tilt = 0 is the reference's geometry). Angles in degrees. For
+ * |sin| > sqrt(1/2) the ray steps along x (m) and interpolates along y at
+ * nf = beta + m alpha, alpha = -cos/sin, beta = (rho - x_min (cos + sin)) / sin, weight
+ * 1/|sin|; otherwise it steps along y and interpolates along x with sin/cos swapped. A
+ * sample counts when 0 <= nf < n - 1 (the effective range of the reference's mmin/mmax
+ * window and in-loop test). Positions are formed as beta + m alpha, not accumulated.
+ * proj [nproj][nz][nu]. */
+typedef struct {
+    int major_y;
+    double alpha, inv, d, rho_off;
+} joseph_angle;
+
+static joseph_angle joseph_geometry(float angle_deg, size_t n)
+{
+    joseph_angle g;
+    const double x_min = -(double)(long)(n / 2);
+    const double th = (double)angle_deg * kDPi / 180.0;
+    const double sn = sin(th), cs = cos(th);
+    g.rho_off = x_min * (cs + sn);
+    if (fabs(sn) > sqrt(0.5)) {
+        g.major_y = 0;
+        g.alpha = -cs / sn;
+        g.inv = 1.0 / sn;
+        g.d = 1.0 / fabs(sn);
+    } else {
+        g.major_y = 1;
+        g.alpha = -sn / cs;
+        g.inv = 1.0 / cs;
+        g.d = 1.0 / fabs(cs);
+    }
+    return g;
+}
+
+void orc_joseph_forward64(const float *vol, size_t n, size_t nz, const float *angles, size_t nproj, size_t nu,
+                          double centre, double tan_tilt, double pivot, double *proj, double *dproj_dc)
+{
+#pragma omp parallel for collapse(2) schedule(static)
+    for (long t = 0; t < (long)nproj; ++t)
+        for (long z = 0; z < (long)nz; ++z) {
+            const joseph_angle g = joseph_geometry(angles[t], n);
+            const double cz = centre + tan_tilt * ((double)z - pivot);
+            const float *sl = vol + (size_t)z * n * n;
+            for (size_t r = 0; r < nu; ++r) {
+                const double beta = ((double)r - cz - g.rho_off) * g.inv;
+                double sum = 0.0, dsum = 0.0;
+                for (size_t k = 0; k < n; ++k) {
+                    const double f = beta + (double)k * g.alpha;
+                    if (!(f >= 0.0 && f < (double)(n - 1))) continue;
+                    const size_t i0 = (size_t)f;
+                    const double w = f - (double)i0;
+                    double s0, s1;
+                    if (g.major_y) {
+                        s0 = sl[k * n + i0];
+                        s1 = sl[k * n + i0 + 1];
+                    } else {
+                        s0 = sl[i0 * n + k];
+                        s1 = sl[(i0 + 1) * n + k];
+                    }
+                    sum += s0 + w * (s1 - s0);
+                    dsum += s1 - s0;
+                }
+                proj[((size_t)t * nz + z) * nu + r] = sum * g.d;
+                if (dproj_dc) dproj_dc[((size_t)t * nz + z) * nu + r] = -dsum * g.inv * g.d;
+            }
+        }
+}
+
+/* The exact transpose of orc_joseph_forward64 (scatter form). vol [nz][n][n] overwritten. */
+void orc_joseph_adjoint64(const double *proj, size_t n, size_t nz, const float *angles, size_t nproj, size_t nu,
+                          double centre, double tan_tilt, double pivot, double *vol)
+{
+#pragma omp parallel for schedule(static)
+    for (long z = 0; z < (long)nz; ++z) {
+        double *sl = vol + (size_t)z * n * n;
+        for (size_t i = 0; i < n * n; ++i) sl[i] = 0.0;
+        const double cz = centre + tan_tilt * ((double)z - pivot);
+        for (size_t t = 0; t < nproj; ++t) {
+            const joseph_angle g = joseph_geometry(angles[t], n);
+            for (size_t r = 0; r < nu; ++r) {
+                const double v = proj[(t * nz + (size_t)z) * nu + r] * g.d;
+                const double beta = ((double)r - cz - g.rho_off) * g.inv;
+                for (size_t k = 0; k < n; ++k) {
+                    const double f = beta + (double)k * g.alpha;
+                    if (!(f >= 0.0 && f < (double)(n - 1))) continue;
+                    const size_t i0 = (size_t)f;
+                    const double w = f - (double)i0;
+                    if (g.major_y) {
+                        sl[k * n + i0] += (1.0 - w) * v;
+                        sl[k * n + i0 + 1] += w * v;
+                    } else {
+                        sl[i0 * n + k] += (1.0 - w) * v;
+                        sl[(i0 + 1) * n + k] += w * v;
+                    }
+                }
+            }
+        }
+    }
+}

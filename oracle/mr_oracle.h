@@ -95,6 +95,12 @@ int orc_morphspotclean(float *img, size_t w, size_t h, int detect, int conn8, co
 int orc_stripefilter(float *img, size_t nu, size_t ntheta, const float *kern, int begin, int end, int nlevels,
                      float sigma);
 
+/* Joseph projector pair in FP64 (forward with its centre derivative, and the transpose) */
+void orc_joseph_forward64(const float *vol, size_t n, size_t nz, const float *angles, size_t nproj, size_t nu,
+                          double centre, double tan_tilt, double pivot, double *proj, double *dproj_dc);
+void orc_joseph_adjoint64(const double *proj, size_t n, size_t nz, const float *angles, size_t nproj, size_t nu,
+                          double centre, double tan_tilt, double pivot, double *vol);
+
 #ifdef __cplusplus
 }
 #endif

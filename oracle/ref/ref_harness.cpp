@@ -24,6 +24,7 @@
 #include <functional>
 #include <iostream>
 #include <iterator>
+#include <list>
 #include <map>
 #include <memory>
 #include <sstream>
@@ -471,6 +472,22 @@ int ref_wavelet_kernel(const char *wname, int *begin, int *end, float *th, float
             sh[i] = k.synthH()[i];
             sg[i] = k.synthG()[i];
         }
+    });
+}
+
+// LinearForwardProjector::project 2-D (linearforwardprojector.cpp:15-144): slice [n][n]
+// (x fastest), angles in degrees; proj [nangles][n] (detector bin fastest).
+int ref_joseph_project(const float *slice, size_t n, const float *angles, size_t nangles, float *proj)
+{
+    return guarded([&] {
+        size_t d[2] = {n, n};
+        kipl::base::TImage<float, 2> img(d);
+        std::memcpy(img.GetDataPtr(), slice, n * n * sizeof(float));
+        std::list<float> a(angles, angles + nangles);
+        kipl::base::TImage<float, 2> out;
+        LinearForwardProjector fp;
+        fp.project(img, a, out);
+        std::memcpy(proj, out.GetDataPtr(), n * nangles * sizeof(float));
     });
 }
 

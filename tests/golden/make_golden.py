@@ -7,7 +7,8 @@ oracle/_ref/libmuhrec_ref.so (make -C oracle ref), on:
   woodsino_0200.tif (read with PIL), with the settings of the reference's own python tests
   (core/algorithms/UnitTests/python/testBindMorphSpotClean.py, testBindStripeFilter.py);
 * the 7x7 fixture of core/algorithms/UnitTests/tImagingAlgorithms/tst_testImagingAlgorithms.cpp:54-73;
-* small seeded cases of FullLogNorm, ProjectionFilterSingle, MultiProjectionBPparallel and FDKbp_single.
+* small seeded cases of FullLogNorm, ProjectionFilterSingle, MultiProjectionBPparallel, FDKbp_single
+  and LinearForwardProjector (the Joseph projector).
 
 usage: python tests/golden/make_golden.py [reference root]
 The fixtures are committed; the tests never read the reference tree.
@@ -78,6 +79,17 @@ def main(ref_root="/root/reference"):
     out["fdk_input"], out["fdk_angles"], out["fdk_weights"] = fproj, fang, fw
     g = O.fdk_geom(300.0, 600.0, (15.5, 11.5), 15.7, (0.2, 0.2), (0.1, 0.1, 0.1))
     out["fdk_out"] = O.fdk(fproj, fang, fw, g, use_ref=True)
+
+    # LinearForwardProjector (Joseph) on a phantom slice and a random slice
+    import torch
+
+    from imagingsuite_b200 import phantom
+
+    ph = phantom.voxelize_torch(phantom.ellipsoids(1005), 64, 1, "cpu", supersample=2)[0].numpy()
+    jang = np.sort(rng.uniform(0, 180, 45)).astype(np.float32)
+    out["joseph_slices"] = np.stack([ph, rng.standard_normal((64, 64)).astype(np.float32)])
+    out["joseph_angles"] = jang
+    out["joseph_ref"] = np.stack([O.ref_joseph_project(s_, jang) for s_ in out["joseph_slices"]])
 
     np.savez_compressed(os.path.join(HERE, "reference_outputs.npz"), **out)
     print("wrote", os.path.join(HERE, "reference_outputs.npz"), sum(v.nbytes for v in out.values()), "bytes raw")
