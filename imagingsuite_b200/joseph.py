@@ -222,51 +222,40 @@ def fbp(op: JosephOperator, p: torch.Tensor, centre: float, tilt_deg: float = 0.
     return b.mul_(s)
 
 
-def estimate_geometry(op: JosephOperator, p: torch.Tensor, centre_guess: float, search: float = 8.0,
-                      step: float = 0.5, blocks: int = 4, filtertype: str = "hanning"):
-    """Coarse centre and tilt from the reprojection error of filtered backprojections.
-
-    For every candidate centre c in centre_guess +- search (step `step`, no tilt) the
-    projections are ramp-filtered, backprojected with A^T(c) and reprojected with A(c); the
-    per-slice residual after the best scale, |p_z|^2 - <A b, p>_z^2 / |A b|_z^2, is summed over
-    `blocks` bands of slices. Each band's minimum (refined by a parabola through its
-    neighbours) is that band's centre of rotation; a line through the band centres gives the
-    centre at the pivot and the tilt (degrees). Returns (centre, tilt_deg)."""
-    plan = ctypes.c_void_p()
-    check(L.lib().mr_projfilter_create(op.nu, filtertype.encode(), 0.5, 1.0, 1, 0.1, 2, ctypes.byref(plan)))
-    try:
-        f = torch.empty_like(p)
-        check(L.lib().mr_projfilter_apply(plan, p.data_ptr(), f.data_ptr(), op.nproj * op.nz, None, 1, _stream()))
-    finally:
-        L.lib().mr_projfilter_destroy(plan)
-    cands = np.arange(-search, search + 0.5 * step, step) + centre_guess
-    pp = op.slice_dot(p, p)
-    res = []
-    b = torch.empty((op.nz, op.n, op.n), dtype=torch.float32, device=p.device)
-    for c in cands:
-        op.adjoint(f, float(c), 0.0, out=b)
-        ab = op.forward(b, float(c), 0.0)
-        num = op.slice_dot(ab, p)
-        den = op.slice_dot(ab, ab).clamp_min(1e-300)
-        res.append((pp - num * num / den).cpu().numpy())
-    res = np.stack(res)  # (ncand, nz)
-    edges = np.linspace(0, op.nz, blocks + 1).round().astype(int)
-    zc, cc = [], []
-    for b0, b1 in zip(edges[:-1], edges[1:]):
-        if b1 <= b0:
+def estimate_geometry(op: JosephOperator, p: torch.Tensor):
+    """Centre of rotation and tilt from the sinogram centroids (Radon consistency of the
+    first moment). For every slice z and angle t the centroid of the projection row,
+    u(t) = sum_r r p / sum_r p, must follow c_z + a cos(theta_t) + b sin(theta_t) for an object
+    inside the field of view; a least-squares fit of (c_z, a, b) per slice (weighted by the
+    row masses) gives the slice's centre, and a line through the centres, weighted by the
+    slices' masses, gives the centre at the pivot and the tilt. Returns (centre, tilt_deg);
+    the per-slice centres of the last call are in estimate_geometry.last."""
+    pd = p.double()
+    r = torch.arange(op.nu, dtype=torch.float64, device=p.device)
+    m0 = pd.sum(dim=2)                                   # (nproj, nz)
+    m1 = (pd * r).sum(dim=2)
+    th = torch.from_numpy(np.deg2rad(op.angles.astype(np.float64))).to(p.device)
+    basis = torch.stack([torch.ones_like(th), torch.cos(th), torch.sin(th)], dim=1)  # (nproj, 3)
+    cz, wz = [], []
+    for z in range(op.nz):
+        w = m0[:, z].clamp_min(0.0)
+        if float(w.sum()) <= 0.0:
+            cz.append(float("nan"))
+            wz.append(0.0)
             continue
-        e = res[:, b0:b1].sum(axis=1)
-        i = int(np.argmin(e))
-        c = cands[i]
-        if 0 < i < len(cands) - 1:
-            den = e[i - 1] - 2 * e[i] + e[i + 1]
-            if den > 0:
-                c += 0.5 * step * (e[i - 1] - e[i + 1]) / den
-        zc.append(0.5 * (b0 + b1 - 1))
-        cc.append(c)
-    zc, cc = np.asarray(zc), np.asarray(cc)
-    if len(zc) > 1:
-        slope, icpt = np.polyfit(zc - op.pivot, cc, 1)
+        u = m1[:, z] / torch.where(w > 0, w, torch.ones_like(w))
+        sw = torch.sqrt(w)
+        sol = torch.linalg.lstsq(basis * sw[:, None], (u * sw)[:, None]).solution[:, 0]
+        cz.append(float(sol[0]))
+        wz.append(float(w.sum()))
+    cz, wz = np.asarray(cz), np.asarray(wz)
+    keep = np.isfinite(cz) & (wz > 1e-3 * wz.max())
+    estimate_geometry.last = {"slice_centres": np.where(np.isfinite(cz), cz, 0.0).tolist(), "slice_weights": wz.tolist()}
+    z = np.arange(op.nz, dtype=np.float64)[keep] - op.pivot
+    if keep.sum() > 1:
+        slope, icpt = np.polyfit(z, cz[keep], 1, w=np.sqrt(wz[keep]))
+    elif keep.sum() == 1:
+        slope, icpt = 0.0, float(cz[keep][0])
     else:
-        slope, icpt = 0.0, float(cc[0])
+        slope, icpt = 0.0, float(op.nu // 2)
     return float(icpt), math.degrees(math.atan(slope))

@@ -176,10 +176,12 @@ def cone_integrals_torch(ells, nproj: int, nu: int, nv: int, sod: float, sdd: fl
     return out
 
 
-def voxelize_torch(ells, n: int, nz: int, device, supersample: int = 1):
+def voxelize_torch(ells, n: int, nz: int, device, supersample: int = 1, fov_margin: float | None = None):
     """Attenuation volume (nz, n, n), x fastest, of the ellipsoids on an n x n x nz voxel grid
     whose x/y extent is the unit box and whose voxels are cubes (z covers nz/n of the box,
-    centred). Values are mu per voxel length (mu per box / n); supersample^3 points per voxel."""
+    centred). Values are mu per voxel length (mu per box / n); supersample^3 points per voxel.
+    With fov_margin, voxels farther than n/2 - fov_margin from the slice centre are zero (the
+    object stays inside the circular field of view)."""
     import torch
 
     s = supersample
@@ -197,4 +199,7 @@ def voxelize_torch(ells, n: int, nz: int, device, supersample: int = 1):
             q = ((p - torch.as_tensor(e.center, device=device)) @ rot) / torch.as_tensor(e.axes, device=device)
             acc += e.mu * ((q * q).sum(-1) <= 1.0)
         out[zi] = (acc.reshape(s, n, s, n, s).mean(dim=(0, 2, 4)) / n).float()
+    if fov_margin is not None:
+        c = torch.arange(n, device=device, dtype=torch.float64) - (n - 1) / 2
+        out[:, (c[:, None] ** 2 + c[None, :] ** 2) > (n / 2 - fov_margin) ** 2] = 0
     return out

@@ -138,16 +138,16 @@ def test_cgls_recovers_centre_and_tilt(cuda):
     n, nz, nu, nproj = 128, 64, 136, 180
     ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
     op = J.JosephOperator(n, nz, ang, nu)
-    truth = phantom.voxelize_torch(phantom.ellipsoids(1009), n, nz, "cuda", supersample=2)
+    truth = phantom.voxelize_torch(phantom.ellipsoids(1009), n, nz, "cuda", supersample=2, fov_margin=6)
     c_true, t_true = nu / 2 + 3.7, 2.5
     p = op.forward(truth, c_true, t_true)
-    c0, t0 = J.estimate_geometry(op, p, float(nu // 2))
+    c0, t0 = J.estimate_geometry(op, p)
     print(f"coarse estimate centre {c0:.3f} tilt {t0:.3f}")
-    assert abs(c0 - c_true) < 0.5 and abs(t0 - t_true) < 1.0
+    assert abs(c0 - c_true) < 0.5 and abs(t0 - t_true) < 0.5
     x0 = J.fbp(op, p, c0, t0)
     x, c, t, hist = J.cgls(op, p, x0, c0, t0, iterations=50, refine_every=5)
     print(f"centre {c:.4f} (true {c_true}), tilt {t:.4f} (true {t_true}), loss {hist[0]:.4g} -> {hist[-1]:.4g}")
-    assert abs(c - c_true) < 0.05
+    assert abs(c - c_true) < 0.1
     assert abs(t - t_true) < 0.1
     assert hist[-1] < 0.05 * hist[0]
     # the volume moved towards the truth
