@@ -397,6 +397,152 @@ def run_diff(args):
                      "loss_last": hist[-1], "volume_rel_error_fbp": rel(x0), "volume_rel_error_cgls": rel(x)}}
 
 
+def run_parallel(args, production: bool):
+    """Parallel-beam chains. C1 (production=False): 360 projections of 256 x 64 over 180 deg,
+    I0 3e4, 5 flats / 5 darks, FullLogNorm -> Hann ramp filter (cutoff 0.5) -> backprojection to
+    256 x 256 x 64, centre 127.5. C3 (production=True): 1125 projections of 2048 x 2048 over 180
+    deg, 20 flats / 10 darks, 0.05 % spot defects and 20 gain-error columns; one block of 512
+    detector rows (the slab the reference reconstructs per SliceBlock) through FullLogNorm ->
+    MorphSpotClean -> WaveletRingClean -> Hann filter -> backprojection to 2048 x 2048 x 512."""
+    import torch
+
+    from imagingsuite_b200 import modules as M
+    from imagingsuite_b200 import phantom
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    if production:
+        nu, nrows, nproj, nflat, ndark, i0 = 2048, 512, 1125, 20, 10, 3e4
+        if args.small:
+            nu, nrows, nproj = 512, 128, 282
+        name = f"C3 production block: {nproj} projections of {nu} x {nu} (block of {nrows} rows), spots + rings"
+    else:
+        nu, nrows, nproj, nflat, ndark, i0 = 256, 64, 360, 5, 5, 3e4
+        name = f"C1 parallel FBP: {nproj} projections of {nu} x {nrows} -> {nu}x{nu}x{nrows}"
+    box = nu
+    ells = phantom.ellipsoids(1000 + (3 if production else 1))
+    v0 = (nu - nrows) // 2 if production else 0
+    integ = phantom.parallel_integrals_torch(ells, nproj, nu, nrows, dev, box=float(nu) if production else None,
+                                             v0=v0)
+    counts, flats, darks = phantom.counts_torch(integ, i0, 2000 + (3 if production else 1), nflat, ndark)
+    del integ
+    if production:
+        phantom.inject_defects_torch(counts, flats, 3003)
+    cfg = M.ReconConfig()
+    pi = cfg.ProjectionInfo
+    pi.fCenter = (nu - 1) / 2.0
+    pi.roi = pi.projection_roi = (0, 0, nu, nrows)
+    pi.nDims = (nu, nrows, nproj)
+    pi.nOBCount, pi.nDCCount = nflat, ndark
+    angles = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    weights = np.full(nproj, np.float32(np.pi / nproj))
+    norm = M.FullLogNorm()
+    norm.Configure(cfg, {"usenormregion": "false", "uselut": "false", "referenceaverage": "ImageAverage"})
+    norm.SetReferenceImages(darks, flats)
+    spot = M.MorphSpotCleanModule()
+    spot.Configure(cfg, {"connectivity": "conn8", "cleanmethod": "morphcleanreplace",
+                         "detectionmethod": "morphdetectboth", "threshold": "0.1 0.1", "sigma": "0.01 0.01",
+                         "edgesmooth": "5", "maxarea": "30", "removeinfnan": "false", "clampdata": "false",
+                         "minlevel": "-0.1", "maxlevel": "12", "threading": "false"})
+    ring = M.WaveletRingClean()
+    ring.Configure(cfg, {"wname": "daub15", "sigma": "0.05", "decnum": "2", "parallel": "false",
+                         "method": "verticalfft"})
+    filt = M.ProjectionFilterSingle()
+    filt.Configure(cfg, {"filtertype": "hanning", "cutoff": "0.5", "order": "1", "usebias": "true",
+                         "biasweight": "0.1", "paddingdoubler": "2"})
+    bp = M.MultiProjectionBPparallel()
+    bp.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1", "precision": "fp32",
+                       "referencecompat": "true"})
+    bp.SetROI((0, 0, nu, nrows))
+    params = {"angles": " ".join("%.9g" % a for a in angles), "weights": " ".join("%.9g" % a for a in weights)}
+    wdev = torch.from_numpy(weights).to(dev)
+    stream = torch.cuda.current_stream()
+    times = {}
+
+    def step(record=False):
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)] if record else None
+        if record:
+            ev[0].record(stream)
+        bp.volume.zero_()
+        proj = norm.ProcessCore(counts, {})
+        if record:
+            ev[1].record(stream)
+        if production:
+            spot.ProcessCore(proj, {})
+        if record:
+            ev[2].record(stream)
+        if production:
+            ring.ProcessCore(proj, {})
+        if record:
+            ev[3].record(stream)
+        filt.ProcessCore(proj, {}, weights=wdev)
+        if record:
+            ev[4].record(stream)
+        bp.Process(proj, params, prefiltered_weights=True)
+        if record:
+            ev[5].record(stream)
+            torch.cuda.synchronize()
+            for k, nm in enumerate(("lognorm", "spotclean", "ringclean", "filter", "backprojection")):
+                times[nm] = ev[k].elapsed_time(ev[k + 1])
+        return bp.GetVolume()
+
+    sampler = ClockSampler(0)
+    sampler.start()
+    t = time_steps(step, args.steps, args.warmup, stream, None)
+    clocks = sampler.stop()
+    step(record=True)
+    sel = bp.used_projections(nproj).size
+    updates = float(nu) * nu * (4 * (nrows // 4)) * sel
+    # end to end: host counts in, host volume out
+    counts_h = counts.cpu().pin_memory()
+    out_h = torch.empty(bp.volume.shape, dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        c = counts_h.to(dev, non_blocking=True)
+        nonlocal_counts[0] = c
+        v = step_with(c)
+        out_h.copy_(v, non_blocking=True)
+
+    def step_with(c):
+        bp.volume.zero_()
+        proj = norm.ProcessCore(c, {})
+        if production:
+            spot.ProcessCore(proj, {})
+            ring.ProcessCore(proj, {})
+        filt.ProcessCore(proj, {}, weights=wdev)
+        bp.Process(proj, params, prefiltered_weights=True)
+        return bp.GetVolume()
+
+    nonlocal_counts = [None]
+    te = time_steps(e2e_step, max(1, min(args.steps, 3)), 1, stream, None)
+    e2e_steps = max(1, min(args.steps, 3))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    tbp = times["backprojection"] / 1e3
+    ach = 8.0 * updates / tbp / 1e9
+    return {"metric": "parallel-beam chain GUPS (voxel x projection updates per second)",
+            "value": updates * args.steps / t / 1e9, "unit": "GUPS", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded 10-ellipsoid phantom, analytic parallel-beam "
+                                                        "line integrals, Poisson counts" + (", injected spots and ring columns)" if production else ")"),
+            "config": {"workload": name, "volume": [nu, nu, nrows], "projections": nproj,
+                       "projections_backprojected": sel, "l2": "inputs larger than L2" if production else "inputs fit L2"},
+            "projections_per_s": nproj * args.steps / t,
+            "module_ms": times,
+            "backprojection_gups": updates / tbp / 1e9,
+            "roofline": {"bound": "smem", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                         "traffic": None, "kernel": "k_bp_par_staged",
+                         "note": "algorithmic bytes = 8 B/update gathered (two FP32 samples) vs measured HBM copy "
+                                 "bandwidth; the gathers are served from shared memory"},
+            "e2e": {"value": updates * e2e_steps / te / 1e9, "unit": "GUPS",
+                    "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(bp.volume.numel() * 4)},
+            "clocks": clocks}
+
+
 def cpu_baseline(w, counts, flats, darks, angles, weights, budget_s=20.0, nsample=None):
     """The reference FDKbp_single (compiled from the reference sources) on a bounded sample:
     the full volume from the first `nsample` projections, all host threads."""
@@ -472,8 +618,9 @@ def main():
     ap.add_argument("--small", action="store_true", help="256^3 profiling case")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
-    ap.add_argument("--workload", default="fdk", choices=["fdk", "diff"],
-                    help="fdk: FDK 1024^3 precision form (default); diff: Joseph pair + CGLS refinement")
+    ap.add_argument("--workload", default="fdk", choices=["fdk", "diff", "parallel", "production"],
+                    help="fdk: FDK 1024^3 precision form (default); diff: Joseph pair + CGLS refinement; "
+                         "parallel: C1 parallel FBP; production: C3 preprocessing + parallel FBP block")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -481,6 +628,8 @@ def main():
         res = run_reference(args)
     elif args.workload == "diff":
         res = run_diff(args)
+    elif args.workload in ("parallel", "production"):
+        res = run_parallel(args, args.workload == "production")
     else:
         res = run_mr(args)
     if res is not None:

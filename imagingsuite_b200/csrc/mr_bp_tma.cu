@@ -1,0 +1,327 @@
+// Parallel-beam backprojection with TMA-staged projection rows (sm_100a).
+//
+// Arithmetic of MultiProjectionBPparallel::BackProject (MultiProjBPparallel.cpp:39-170),
+// every float operation in the reference's order with explicitly rounded intrinsics, so the
+// volume is bit-identical to the plain kernel and to the reference (no-tilt branch):
+//   u = (startu_i + cos_i y) - sin_i x,  n = (int)u in [0, nu-2],  f = |u - n|,
+//   vol[y-1][x-1][z] += (P[z][n] (1 - f) + P[z][n+1] f)          (P pre-multiplied by weight_i)
+//
+// Tiling: a CTA owns 32 (x) x 8 (y) voxel columns x 32 slices; a thread keeps its 32 slices
+// in registers over all projections. In this geometry the detector column of a voxel does
+// not depend on its slice, so one projection's footprint on the tile is at most ~34 columns
+// by the tile's 32 detector rows: a producer warp projects the 4 tile corners with the voxel
+// formula (affine in x and y, so the corners bound every voxel exactly), and one TMA tile
+// load (cp.async.bulk.tensor.3d, no multicast) brings a 48 x 32 box per projection into
+// shared memory, batches of 8 projections on two stages with bounded mbarrier waits. The
+// box pitch is a compile-time constant, so the slice loop addresses its two samples with
+// immediate offsets; the two interpolation products are one f32x2 mul (an f32x2 mul feeding
+// scalar adds is not contracted). Rows beyond the detector are zero-filled by the TMA unit
+// and never read (only z < 4*(nv/4) is updated). A footprint that does not fit the box falls
+// back to guarded global loads for that tile and projection (same arithmetic). The volume
+// (z fastest) is read and written as float4 runs.
+#include "mr_common.cuh"
+#include "mr_tma.cuh"
+
+#include <algorithm>
+#include <cmath>
+
+namespace mr {
+
+// Error word of this file's bounded waits (device globals are per translation unit);
+// mr_device_status reads and clears it with the FDK kernels' word.
+__device__ int g_bp_error = 0;
+
+int bp_device_status_take()
+{
+    int v = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&v, g_bp_error, sizeof(int)) != cudaSuccess) return -1;
+    if (cudaMemcpyToSymbol(g_bp_error, &zero, sizeof(int)) != cudaSuccess) return -1;
+    return v;
+}
+
+namespace bp2 {
+
+constexpr int TX = 32, TY = 8, TZ = 32, THREADS = TX * TY, NB = 8, BW = 48;
+constexpr int BOXBYTES = BW * TZ * 4;
+constexpr int GEO = 8; // sin, cos, startu, weight, slab (as int bits), pad
+
+struct Params {
+    const float *proj;
+    const float *weight;
+    const int32_t *index;
+    const float *sinv, *cosv, *startu;
+    const uint32_t *mask;
+    float *vol;
+    int nproj, nu, nv, nz4;
+};
+
+struct Smem {
+    float *box;      // [2][NB][TZ][BW]
+    float *geo;      // [2][NB][GEO]
+    int4 *meta;      // [2][NB]: x0, mode
+    uint64_t *bars;  // [2]
+    __device__ explicit Smem(unsigned char *base)
+    {
+        box = reinterpret_cast<float *>(base);
+        geo = reinterpret_cast<float *>(base + 2 * NB * BOXBYTES);
+        meta = reinterpret_cast<int4 *>(geo + 2 * NB * GEO);
+        bars = reinterpret_cast<uint64_t *>(meta + 2 * NB);
+    }
+    static constexpr size_t bytes()
+    {
+        return 2 * NB * static_cast<size_t>(BOXBYTES) + 2 * NB * GEO * sizeof(float) + 2 * NB * sizeof(int4) +
+               2 * sizeof(uint64_t);
+    }
+};
+
+// Detector position of voxel (x1, y1) (1-based) for list entry i, reference order.
+__device__ __forceinline__ float posu(float sn, float cs, float su, float fx, float fy)
+{
+    return __fsub_rn(__fadd_rn(su, __fmul_rn(cs, fy)), __fmul_rn(sn, fx));
+}
+
+template <bool HASW>
+__global__ void __launch_bounds__(THREADS, 2) k_bp_par_staged(const __grid_constant__ CUtensorMap tmap, const Params P)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    Smem S(smem);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    const int x1 = i0 + lane + 1, y1 = j0 + warp + 1;
+    const int zmax = min(TZ, P.nz4 - z0);
+    const bool valid = x1 <= P.nu && y1 <= P.nu;
+    const bool inside = valid && static_cast<uint32_t>(x1) > P.mask[2 * (y1 - 1)] &&
+                        static_cast<uint32_t>(x1) <= P.mask[2 * (y1 - 1) + 1];
+    float *col = P.vol + (static_cast<size_t>(valid ? y1 - 1 : 0) * P.nu + (valid ? x1 - 1 : 0)) * P.nv + z0;
+    const bool vec = (P.nv & 3) == 0 && zmax == TZ;
+
+    float acc[TZ];
+#pragma unroll
+    for (int q = 0; q < TZ; q += 4) {
+        if (inside && vec) {
+            const float4 v = *reinterpret_cast<const float4 *>(col + q);
+            acc[q] = v.x;
+            acc[q + 1] = v.y;
+            acc[q + 2] = v.z;
+            acc[q + 3] = v.w;
+        } else {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[q + e] = (inside && q + e < zmax) ? col[q + e] : 0.0f;
+        }
+    }
+    if (!__syncthreads_or(inside)) return;
+
+    if (threadIdx.x == 0) {
+        tma::mbar_init(&S.bars[0], 1);
+        tma::mbar_init(&S.bars[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    const int xa = i0 + 1, xb = min(i0 + TX, P.nu), ya = j0 + 1, yb = min(j0 + TY, P.nu);
+    const int nbatch = (P.nproj + NB - 1) / NB;
+
+    // batch s into stage st: warp 0 = footprints + TMA (4 corner lanes per projection), all
+    // threads stage the per-projection geometry
+    auto produce = [&](int s, int st) {
+        if (warp == 0) {
+            const int b = lane >> 2, corner = lane & 3;
+            const int i = s * NB + b;
+            int nmin = 0, nmax = 0;
+            bool ok = i < P.nproj;
+            if (ok) {
+                const float u = posu(__ldg(P.sinv + i), __ldg(P.cosv + i), __ldg(P.startu + i),
+                                     static_cast<float>((corner & 1) ? xb : xa), static_cast<float>((corner & 2) ? yb : ya));
+                ok = fabsf(u) < 1.0e9f;
+                nmin = nmax = ok ? __float2int_rz(u) : 0;
+            }
+#pragma unroll
+            for (int o = 1; o < 4; o <<= 1) {
+                nmin = min(nmin, __shfl_xor_sync(0xffffffffu, nmin, o));
+                nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+                ok = __shfl_xor_sync(0xffffffffu, static_cast<int>(ok), o) && ok;
+            }
+            // 0: global fallback, 1: staged, 2: no voxel of the tile has n in [0, nu-2]
+            int mode = 0, x0 = 0;
+            if (i < P.nproj && ok) {
+                if (nmax < 0 || nmin > P.nu - 2) {
+                    mode = 2;
+                } else {
+                    x0 = nmin >= 0 ? (nmin & ~3) : -(((-nmin) + 3) & ~3);
+                    if (nmax + 1 < x0 + BW) mode = 1;
+                }
+            }
+            const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
+            if (lane == 0) tma::mbar_expect_tx(&S.bars[st], static_cast<uint32_t>(__popc(staged)) * BOXBYTES);
+            __syncwarp();
+            if (corner == 0 && i < P.nproj) {
+                S.meta[st * NB + b] = make_int4(x0, mode, 0, 0);
+                if (mode == 1) {
+                    const int slab = P.index ? __ldg(P.index + i) : i;
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    tma::load_3d(S.box + (st * NB + b) * (BW * TZ), &tmap, x0, z0, slab, &S.bars[st]);
+                }
+            }
+        }
+        for (int idx = threadIdx.x; idx < NB * GEO; idx += THREADS) {
+            const int b = idx / GEO, e = idx % GEO, i = s * NB + b;
+            float v = 0.0f;
+            if (i < P.nproj) {
+                if (e == 0) v = P.sinv[i];
+                else if (e == 1) v = P.cosv[i];
+                else if (e == 2) v = P.startu[i];
+                else if (e == 3) v = HASW ? P.weight[i] : 1.0f;
+                else if (e == 4) v = __int_as_float(P.index ? P.index[i] : i);
+            }
+            S.geo[st * NB * GEO + idx] = v;
+        }
+    };
+
+    produce(0, 0);
+    if (nbatch > 1) produce(1, 1);
+    __syncthreads();
+
+    uint32_t phase0 = 0, phase1 = 0;
+    bool failed = false;
+    const float fx = static_cast<float>(x1), fy = static_cast<float>(y1);
+    const int um2 = P.nu - 2;
+    for (int s = 0; s < nbatch; ++s) {
+        const int st = s & 1;
+        if (!tma::mbar_wait(&S.bars[st], st ? phase1 : phase0)) {
+            failed = true;
+            atomicExch(&g_bp_error, 1);
+            break;
+        }
+        if (st) phase1 ^= 1; else phase0 ^= 1;
+        if (inside) {
+#pragma unroll 1
+            for (int b = 0; b < NB; ++b) {
+                const int i = s * NB + b;
+                if (i >= P.nproj) break;
+                const int4 m = S.meta[st * NB + b];
+                if (m.y == 2) continue;
+                const float *g = S.geo + (st * NB + b) * GEO;
+                const float u = posu(g[0], g[1], g[2], fx, fy);
+                const int n = __float2int_rz(u);
+                if (n < 0 || um2 < n) continue;
+                const float wb = fabsf(__fsub_rn(u, static_cast<float>(n)));
+                const float wa = __fsub_rn(1.0f, wb);
+                const float2 wab = make_float2(wa, wb);
+                const float w = g[3];
+                if (m.y == 1) {
+                    const float *p = S.box + (st * NB + b) * (BW * TZ) + (n - m.x);
+#pragma unroll
+                    for (int q = 0; q < TZ; ++q) {
+                        if (q >= zmax) break;
+                        float pa = p[q * BW], pb = p[q * BW + 1];
+                        if (HASW) {
+                            pa = __fmul_rn(pa, w);
+                            pb = __fmul_rn(pb, w);
+                        }
+                        const float2 prod = __fmul2_rn(make_float2(pa, pb), wab);
+                        acc[q] = __fadd_rn(acc[q], __fadd_rn(prod.x, prod.y));
+                    }
+                } else {
+                    const float *img = P.proj + (static_cast<size_t>(__float_as_int(g[4])) * P.nv + z0) * P.nu + n;
+#pragma unroll
+                    for (int q = 0; q < TZ; ++q) {
+                        if (q >= zmax) break;
+                        float pa = __ldg(img + static_cast<size_t>(q) * P.nu), pb = __ldg(img + static_cast<size_t>(q) * P.nu + 1);
+                        if (HASW) {
+                            pa = __fmul_rn(pa, w);
+                            pb = __fmul_rn(pb, w);
+                        }
+                        acc[q] = __fadd_rn(acc[q], __fadd_rn(__fmul_rn(pa, wa), __fmul_rn(pb, wb)));
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        if (s + 2 < nbatch) produce(s + 2, st);
+    }
+    if (failed) {
+        tma::mbar_wait(&S.bars[0], phase0);
+        tma::mbar_wait(&S.bars[1], phase1);
+    }
+    if (inside) {
+#pragma unroll
+        for (int q = 0; q < TZ; q += 4) {
+            if (vec) {
+                *reinterpret_cast<float4 *>(col + q) = make_float4(acc[q], acc[q + 1], acc[q + 2], acc[q + 3]);
+            } else {
+#pragma unroll
+                for (int e = 0; e < 4; ++e)
+                    if (q + e < zmax) col[q + e] = acc[q + e];
+            }
+        }
+    }
+}
+
+} // namespace bp2
+
+// Returns MR_ERR_UNSUPPORTED when staging does not apply (the caller uses the plain kernel).
+mr_status bp_parallel_staged_launch(const float *proj_d, size_t nslabs, const float *weight_d, const int32_t *index_d,
+                                    const float *sin_d, const float *cos_d, const float *startu_d, size_t nproj,
+                                    size_t nu, size_t nv, const uint32_t *mask_d, float *vol_d, cudaStream_t s)
+{
+    using namespace bp2;
+    if ((nu * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(proj_d) % 16) != 0 || nv < 4 || nslabs == 0 ||
+        nu < static_cast<size_t>(BW))
+        return MR_ERR_UNSUPPORTED;
+    PFN_cuTensorMapEncodeTiled enc = tma::encode_fn();
+    if (!enc) return MR_ERR_UNSUPPORTED;
+    CUtensorMap map;
+    cuuint64_t dims[3] = {nu, nv, nslabs};
+    cuuint64_t strides[2] = {nu * 4, nu * nv * 4};
+    cuuint32_t box[3] = {static_cast<cuuint32_t>(BW), static_cast<cuuint32_t>(TZ), 1};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult cr = enc(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float *>(proj_d), dims, strides, box, estr,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (cr != CUDA_SUCCESS) return fail(MR_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", static_cast<int>(cr));
+    Params P;
+    P.proj = proj_d;
+    P.weight = weight_d;
+    P.index = index_d;
+    P.sinv = sin_d;
+    P.cosv = cos_d;
+    P.startu = startu_d;
+    P.mask = mask_d;
+    P.vol = vol_d;
+    P.nproj = static_cast<int>(nproj);
+    P.nu = static_cast<int>(nu);
+    P.nv = static_cast<int>(nv);
+    P.nz4 = static_cast<int>((nv / 4) * 4);
+    const size_t smem = Smem::bytes();
+    dim3 grid(div_up(nu, TX), div_up(nu, TY), div_up(static_cast<size_t>(P.nz4), TZ));
+    if (weight_d) {
+        MR_CUDA_TRY(cudaFuncSetAttribute(k_bp_par_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        k_bp_par_staged<true><<<grid, THREADS, smem, s>>>(map, P);
+    } else {
+        MR_CUDA_TRY(cudaFuncSetAttribute(k_bp_par_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        k_bp_par_staged<false><<<grid, THREADS, smem, s>>>(map, P);
+    }
+    return check_launch("k_bp_par_staged");
+}
+
+} // namespace mr
+
+using namespace mr;
+
+extern "C" mr_status mr_bp_parallel_staged(const void *proj_d, size_t nslabs, int dtype, const float *scale_d,
+                                           const float *weight_d, const int32_t *index_d, const float *sin_d,
+                                           const float *cos_d, const float *startu_d, size_t nproj, size_t nu, size_t nv,
+                                           const uint32_t *mask_d, int correcttilt, float tiltoffset, float tiltinc,
+                                           float *vol_d, void *stream)
+{
+    if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
+        return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: null pointer");
+    if (dtype == MR_F32 && !correcttilt && nproj > 0 && nproj <= 0x7fffffff && nu >= 2 && nu <= 65536 && nv <= 65536) {
+        if (!index_d && nslabs < nproj) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: nslabs below nproj");
+        mr_status st = bp_parallel_staged_launch(static_cast<const float *>(proj_d), nslabs, weight_d, index_d, sin_d,
+                                                 cos_d, startu_d, nproj, nu, nv, mask_d, vol_d, as_stream(stream));
+        if (st != MR_ERR_UNSUPPORTED) return st;
+    }
+    return mr_bp_parallel(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
+                          correcttilt, tiltoffset, tiltinc, vol_d, stream);
+}

@@ -44,6 +44,12 @@ inline mr_status check_launch(const char *what)
 
 inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
 
+// Keep memory freed by cudaFreeAsync cached in the current device's default pool (release
+// threshold = unlimited) instead of returning it to the driver at every synchronisation, so
+// that per-call scratch (up to tens of GB for a block of projections) is mapped once.
+// Applied once per device by the entry points that allocate scratch.
+void keep_pool_memory();
+
 inline unsigned div_up(size_t a, size_t b) { return static_cast<unsigned>((a + b - 1) / b); }
 
 // ---- 16-bit projection storage: value = stored * scale (scale per projection, a power of two)

@@ -6,10 +6,29 @@
 // frameworks/tomography/Framework/ReconFramework/src/ProjectionReader.cpp:752-783 (dose).
 #include "mr_common.cuh"
 
+#include <mutex>
+
 #include <cmath>
 #include <cstring>
 
 namespace mr {
+
+void keep_pool_memory()
+{
+    static std::mutex mu;
+    static bool done[256] = {};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return;
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+        uint64_t threshold = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
+    }
+    done[dev] = true;
+}
+
 
 static thread_local std::string g_last_error;
 
@@ -225,6 +244,7 @@ mr_status mr_projection_dose(const void *in_d, int dtype, size_t nu, size_t nv, 
     const size_t w = roi_h[2] - roi_h[0], h = roi_h[3] - roi_h[1];
     if (h > 8192) return fail(MR_ERR_ARGUMENT, "mr_projection_dose: ROI taller than 8192 rows");
     float *means = nullptr;
+    keep_pool_memory();
     MR_CUDA_TRY(cudaMallocAsync(&means, nframes * h * sizeof(float), s));
     dim3 g(div_up(h, 128), static_cast<unsigned>(nframes));
     if (dtype == MR_F32)

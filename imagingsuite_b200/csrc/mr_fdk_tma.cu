@@ -32,6 +32,7 @@
 //  * When a footprint does not fit the box, that projection falls back to guarded global
 //    loads for this tile (same arithmetic, same result).
 #include "mr_common.cuh"
+#include "mr_tma.cuh"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -44,6 +45,8 @@
 namespace mr {
 
 __device__ int g_device_error = 0;
+int bp_device_status_take();  // mr_bp_tma.cu
+int msc_device_status_take(); // mr_spotclean.cu
 
 namespace fdk2 {
 
@@ -51,7 +54,6 @@ constexpr int TI = 32, TJ = 8, TK = 32, THREADS = TI * TJ, NWARPS = THREADS / 32
 constexpr int CTAS_PER_SM = 2;
 constexpr float kMagic = 12582912.0f; // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
-constexpr int kWaitLimit = 1 << 22;
 // per-projection geometry staged in shared memory (floats)
 constexpr int GEO_EXACT = TK + 3 * TI + 3 * TJ + 4; // zip1[TK], xip[TI][3], yip[TJ][3], Z0, Z2
 constexpr int GEO_FAST = 16;                        // map[12], scale, pad
@@ -71,44 +73,14 @@ struct Params {
     int xalign;       // x coordinate alignment of a TMA load (elements)
 };
 
-__device__ __forceinline__ uint32_t smem_addr(const void *p)
-{
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
-}
-
-// Bounded wait on an mbarrier phase; false when the limit expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
-{
-    const uint32_t a = smem_addr(bar);
-    for (int it = 0; it < kWaitLimit; ++it) {
-        uint32_t ok;
-        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-                     "selp.u32 %0, 1, 0, p;\n\t}"
-                     : "=r"(ok)
-                     : "r"(a), "r"(parity)
-                     : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
+using tma::mbar_expect_tx;
+using tma::mbar_init;
+using tma::mbar_wait;
+using tma::smem_addr;
 
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
 {
-    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-                 ::"r"(smem_addr(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z),
-                 "r"(smem_addr(bar))
-                 : "memory");
+    tma::load_3d(dst, map, x, y, z, bar);
 }
 
 // f32 accumulator += a * b with a, b in 16-bit storage (one instruction on sm_100).
@@ -602,20 +574,6 @@ __global__ void k_fdk_f64(const float *__restrict__ proj, int nu, int nv, int np
 
 // ---------------------------------------------------------------- host side
 
-static PFN_cuTensorMapEncodeTiled encode_fn()
-{
-    static PFN_cuTensorMapEncodeTiled fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled>(p);
-    });
-    return fn;
-}
-
 // Footprint of a tile for one projection, in double from the float partials (host guess of
 // the box size; the kernel re-checks every footprint and falls back when one does not fit).
 static void tile_footprint(const float *X, const float *Y, const float *Z, int i0, int i1, int j0, int j1, int k0,
@@ -699,7 +657,7 @@ static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const 
     const int xalign = static_cast<int>(16 / es);
     if ((nu * es) % 16 != 0 || (reinterpret_cast<uintptr_t>(proj_d) % 16) != 0) return MR_ERR_UNSUPPORTED;
     if (bw <= 0 || bh <= 0 || bw > 256 || bh > 256 || bw % xalign) return MR_ERR_UNSUPPORTED;
-    PFN_cuTensorMapEncodeTiled enc = encode_fn();
+    PFN_cuTensorMapEncodeTiled enc = tma::encode_fn();
     if (!enc) return fail(MR_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
     constexpr size_t kMaxSmem = (227 * 1024) / CTAS_PER_SM - 1024; // CTAS_PER_SM CTAs per SM
     CUtensorMap map;
@@ -851,7 +809,9 @@ mr_status mr_device_status(int *status)
     int v = 0, zero = 0;
     MR_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int)));
     MR_CUDA_TRY(cudaMemcpyToSymbol(g_device_error, &zero, sizeof(int)));
-    *status = v;
+    const int b = bp_device_status_take(), m = msc_device_status_take();
+    if (b < 0 || m < 0) return fail(MR_ERR_CUDA, "mr_device_status: reading an error word failed");
+    *status = v | b | m;
     return MR_OK;
 }
 

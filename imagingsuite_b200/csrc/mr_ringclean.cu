@@ -384,6 +384,7 @@ static mr_status run_stripes(float *data_d, bool interleaved, size_t nu, size_t 
     size_t total = 4 * P.K;
     for (int l = 0; l < P.levels; ++l) total += P.nfft[l] * 2 + P.nfft[l];
     total += stripe_scratch(P, nb) + (interleaved ? static_cast<size_t>(nb) * nu * ntheta : 0);
+    keep_pool_memory();
     MR_CUDA_TRY(cudaMallocAsync(&work, total * sizeof(float), s));
     size_t off = 0;
     taps_d = work;

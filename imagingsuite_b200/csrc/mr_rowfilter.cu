@@ -234,6 +234,7 @@ mr_status quantize_projections(const float *x_d, size_t per, size_t nproj, int k
                                cudaStream_t s)
 {
     float *amax = nullptr, *inv = nullptr;
+    keep_pool_memory();
     MR_CUDA_TRY(cudaMallocAsync(&amax, 2 * nproj * sizeof(float), s));
     inv = amax + nproj;
     mr_status st = MR_OK;
@@ -517,6 +518,7 @@ mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, c
     float *tmp = nullptr;
     mr_status st = MR_OK;
     const size_t total = nu * nv * nproj;
+    keep_pool_memory();
     if (cudaMallocAsync(&tw_d, tw.size() * sizeof(float2), s) != cudaSuccess ||
         cudaMallocAsync(&resp_d, padwidth * sizeof(float), s) != cudaSuccess)
         st = fail(MR_ERR_ALLOCATION, "mr_fdk_filter: tables");

@@ -33,12 +33,21 @@
 
 namespace mr {
 
-extern __device__ int g_device_error;
+// Error word of this file's bounded loops (device globals are per translation unit without
+// relocatable device code); mr_device_status reads and clears it with the other kernels' words.
+__device__ int g_msc_error = 0;
+
+int msc_device_status_take()
+{
+    int v = 0, zero = 0;
+    if (cudaMemcpyFromSymbol(&v, g_msc_error, sizeof(int)) != cudaSuccess) return -1;
+    if (cudaMemcpyToSymbol(g_msc_error, &zero, sizeof(int)) != cudaSuccess) return -1;
+    return v;
+}
 
 namespace msc {
 
 constexpr int kMargin = 5;
-constexpr int kThreads = 1024;
 constexpr int kMaxRounds = 4096;
 constexpr int kMaxEdge = 63;
 
@@ -213,114 +222,226 @@ __global__ void k_peaks_forward_band(const float *__restrict__ pad, int pw, int 
     }
 }
 
-// Exact reconstruction by alternating row sweeps (see the file comment). DILATE: v = min(g,
-// max over neighbourhood); else v = max(g, min over neighbourhood). g is `sign * pad`.
+// Exact reconstruction by alternating row sweeps (see the file comment), one warp per image.
+// DILATE: v = min(g, max over neighbourhood); else v = max(g, min over neighbourhood); g is
+// `sign * pad`. Rows are staged in shared memory (coalesced global traffic); lane l owns the
+// contiguous chunk [l*C, l*C + C) of a row, C odd so that the 32 lanes' chunk positions fall
+// in 32 different banks. Positions beyond the row hold the neutral value (-inf for
+// dilation, +inf for erosion), which neither propagates into the row nor changes.
+
 template <bool DILATE>
-__global__ void __launch_bounds__(kThreads) k_reconstruct(const float *__restrict__ pad, float sign, int pw, int ph,
-                                                          int conn8, float *__restrict__ vol)
+__device__ __forceinline__ float rec_op(float g, float v, float x)
 {
-    extern __shared__ float sm[];
-    float *prev = sm;                       // finished neighbouring row [pw]
-    Clamp *wagg = reinterpret_cast<Clamp *>(sm + pw); // per-warp aggregates [32]
-    __shared__ int changed_s;
+    return DILATE ? fminf(g, fmaxf(v, x)) : fmaxf(g, fminf(v, x));
+}
+
+__device__ __forceinline__ void cp_async4(float *dst, const float *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+                 "l"(src)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
+// Barrier of the RW warps of one image (named barrier 1 + image slot; the block holds one image).
+template <int RW>
+__device__ __forceinline__ void image_sync()
+{
+    if constexpr (RW == 1) __syncwarp();
+    else asm volatile("bar.sync 1, %0;" ::"n"(RW * 32) : "memory");
+}
+
+// Clamp pair of a run of elements: for dilation F(x) = min(hi, max(lo, x)) with lo = F(-inf),
+// hi = F(+inf); for erosion the same with min/max exchanged (lo = F(+inf), hi = F(-inf)).
+// (a then b): apply a first.
+template <bool DILATE>
+__device__ __forceinline__ void clamp_then(float al, float ah, float &bl, float &bh)
+{
+    const float nl = rec_op<DILATE>(bh, bl, al), nh = rec_op<DILATE>(bh, bl, ah);
+    bl = nl;
+    bh = nh;
+}
+
+// One image per block of RW warps; lane t of the image owns the row chunk [t*C, t*C + C), held
+// in registers across the vertical step and both scans. C odd: the lanes' chunk positions in
+// the shared row buffers fall in distinct banks.
+template <bool DILATE, int RW, int C>
+__global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict__ pad, float sign, int pw, int ph,
+                                                         int conn8, float *__restrict__ vol)
+{
+    constexpr int T = 32 * RW, L = T * C + 2 + 1; // row buffer: a neutral element before and after
+    extern __shared__ float rows_sm[];
+    float(*Gb)[L] = reinterpret_cast<float(*)[L]>(rows_sm);         // [2][L] mask rows
+    float(*Rb)[L] = reinterpret_cast<float(*)[L]>(rows_sm + 2 * L); // [3][L] marker rows
+    __shared__ float wagg[2][RW][2];
+    __shared__ int any_changed[2];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const size_t n = static_cast<size_t>(pw) * ph;
     const float *g = pad + blockIdx.x * n;
     float *v = vol + blockIdx.x * n;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // consecutive chunk of the row per thread
-    const int per = (pw + kThreads - 1) / kThreads;
-    const int c0 = min(tid * per, pw), c1 = min(c0 + per, pw);
-    constexpr int kMaxPer = 8;
+    const float neutral = DILATE ? -FLT_MAX : FLT_MAX;
+    for (int c = t; c < L; c += T) {
+        Gb[0][c] = Gb[1][c] = neutral * sign; // sign * stored = neutral
+        Rb[0][c] = Rb[1][c] = Rb[2][c] = neutral;
+    }
+    if (t < 2) any_changed[t] = 0;
+    __syncthreads();
+    const int c0 = 1 + t * C; // buffer index of the chunk's first element (index 0 is the lead)
+    auto fetch = [&](int y, float *G, float *V) {
+        const size_t ro = static_cast<size_t>(y) * pw;
+        for (int c = t; c < pw; c += T) {
+            cp_async4(G + 1 + c, g + ro + c);
+            cp_async4(V + 1 + c, v + ro + c);
+        }
+    };
+    // exclusive scan over the image's lanes of clamp pairs; returns the carry into this lane
+    auto carry_in = [&](float xl, float xh, bool fwd, int slot) -> float {
+        for (int o = 1; o < 32; o <<= 1) {
+            const float pl = fwd ? __shfl_up_sync(0xffffffffu, xl, o) : __shfl_down_sync(0xffffffffu, xl, o);
+            const float pu = fwd ? __shfl_up_sync(0xffffffffu, xh, o) : __shfl_down_sync(0xffffffffu, xh, o);
+            if (fwd ? lane >= o : lane + o < 32) clamp_then<DILATE>(pl, pu, xl, xh);
+        }
+        // (xl, xh): inclusive prefix within the warp
+        float before_l = neutral, before_h = -neutral; // identity
+        if constexpr (RW > 1) {
+            if (fwd ? lane == 31 : lane == 0) {
+                wagg[slot][warp][0] = xl;
+                wagg[slot][warp][1] = xh;
+            }
+            image_sync<RW>();
+            // warps earlier in the scan direction, in order (copies: wagg is shared)
+            for (int k = 0; k < RW; ++k) {
+                const int w = fwd ? k : RW - 1 - k;
+                if (fwd ? w >= warp : w <= warp) break;
+                float bl = wagg[slot][w][0], bh = wagg[slot][w][1];
+                clamp_then<DILATE>(before_l, before_h, bl, bh);
+                before_l = bl;
+                before_h = bh;
+            }
+        }
+        // lanes before this one within the warp
+        float il = fwd ? __shfl_up_sync(0xffffffffu, xl, 1) : __shfl_down_sync(0xffffffffu, xl, 1);
+        float ih = fwd ? __shfl_up_sync(0xffffffffu, xh, 1) : __shfl_down_sync(0xffffffffu, xh, 1);
+        if (fwd ? lane > 0 : lane < 31) {
+            clamp_then<DILATE>(before_l, before_h, il, ih);
+            before_l = il;
+        }
+        return before_l; // the prefix applied to the neutral input
+    };
 
     int round = 0;
     for (; round < kMaxRounds; ++round) {
-        if (tid == 0) changed_s = 0;
-        __syncthreads();
-        int changed = 0;
+        bool changed = false;
         for (int pass = 0; pass < 2; ++pass) {
-            const int dir = pass == 0 ? 1 : -1;
+            int gi = 0, vi = 0;
+            fetch(pass == 0 ? 0 : ph - 1, Gb[0], Rb[0]);
+            cp_async_wait_all();
+            image_sync<RW>();
             for (int step = 0; step < ph; ++step) {
-                const int y = dir > 0 ? step : ph - 1 - step;
-                float val[kMaxPer], gg[kMaxPer];
-                // vertical / diagonal neighbours from the row finished just before
-                for (int e = 0; e < c1 - c0; ++e) {
-                    const int c = c0 + e;
-                    const size_t idx = static_cast<size_t>(y) * pw + c;
-                    float cand = v[idx];
-                    const float gv = sign * g[idx];
-                    if (step > 0) {
-                        float nbv = prev[c];
-                        if (conn8) {
-                            if (c > 0) nbv = DILATE ? fmaxf(nbv, prev[c - 1]) : fminf(nbv, prev[c - 1]);
-                            if (c + 1 < pw) nbv = DILATE ? fmaxf(nbv, prev[c + 1]) : fminf(nbv, prev[c + 1]);
-                        }
-                        cand = DILATE ? fminf(gv, fmaxf(cand, nbv)) : fmaxf(gv, fminf(cand, nbv));
-                    }
-                    val[e] = cand;
-                    gg[e] = gv;
+                const int y = pass == 0 ? step : ph - 1 - step;
+                const float *G = Gb[gi];
+                float *V = Rb[vi];
+                const float *Pv = Rb[(vi + 2) % 3];
+                if (step + 1 < ph) fetch(pass == 0 ? y + 1 : y - 1, Gb[gi ^ 1], Rb[(vi + 1) % 3]);
+                float gv[C], cv[C];
+#pragma unroll
+                for (int j = 0; j < C; ++j) {
+                    gv[j] = sign * G[c0 + j];
+                    cv[j] = V[c0 + j];
                 }
-                // along the row, both directions: clamp prefix scans
-                for (int sweep = 0; sweep < 2; ++sweep) {
-                    const bool fwd = sweep == 0;
-                    Clamp acc{-FLT_MAX, FLT_MAX}; // identity
-                    const int cnt = c1 - c0;
-                    for (int k = 0; k < cnt; ++k) {
-                        const int e = fwd ? k : cnt - 1 - k;
-                        const Clamp f = DILATE ? Clamp{val[e], gg[e]} : Clamp{gg[e], val[e]};
-                        acc = compose(acc, f);
+                if (step > 0) {
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        float nb = Pv[c0 + j];
+                        if (conn8)
+                            nb = DILATE ? fmaxf(nb, fmaxf(Pv[c0 + j - 1], Pv[c0 + j + 1]))
+                                        : fminf(nb, fminf(Pv[c0 + j - 1], Pv[c0 + j + 1]));
+                        const float nvl = rec_op<DILATE>(gv[j], cv[j], nb);
+                        changed |= nvl != cv[j];
+                        cv[j] = nvl;
                     }
-                    // exclusive scan of thread aggregates in the sweep direction
-                    Clamp x = acc;
-                    for (int o = 1; o < 32; o <<= 1) {
-                        Clamp y2;
-                        y2.lo = fwd ? __shfl_up_sync(0xffffffffu, x.lo, o) : __shfl_down_sync(0xffffffffu, x.lo, o);
-                        y2.hi = fwd ? __shfl_up_sync(0xffffffffu, x.hi, o) : __shfl_down_sync(0xffffffffu, x.hi, o);
-                        const bool ok = fwd ? lane >= o : lane + o < 32;
-                        if (ok) x = compose(y2, x);
-                    }
-                    if ((fwd && lane == 31) || (!fwd && lane == 0)) wagg[warp] = x;
-                    __syncthreads();
-                    Clamp before{-FLT_MAX, FLT_MAX};
-                    const int nwarps = kThreads / 32;
-                    if (fwd) {
-                        for (int q = 0; q < warp; ++q) before = compose(before, wagg[q]);
-                    } else {
-                        for (int q = nwarps - 1; q > warp; --q) before = compose(before, wagg[q]);
-                    }
-                    // within the warp: everything before this lane
-                    Clamp inwarp;
-                    inwarp.lo = fwd ? __shfl_up_sync(0xffffffffu, x.lo, 1) : __shfl_down_sync(0xffffffffu, x.lo, 1);
-                    inwarp.hi = fwd ? __shfl_up_sync(0xffffffffu, x.hi, 1) : __shfl_down_sync(0xffffffffu, x.hi, 1);
-                    if ((fwd && lane > 0) || (!fwd && lane < 31)) before = compose(before, inwarp);
-                    // apply along this thread's chunk
-                    Clamp run = before;
-                    for (int k = 0; k < cnt; ++k) {
-                        const int e = fwd ? k : cnt - 1 - k;
-                        const Clamp f = DILATE ? Clamp{val[e], gg[e]} : Clamp{gg[e], val[e]};
-                        run = compose(run, f);
-                        val[e] = DILATE ? run.lo : run.hi; // F(-inf) for dilation, F(+inf) for erosion
-                    }
-                    __syncthreads(); // wagg reused
                 }
-                for (int e = 0; e < c1 - c0; ++e) {
-                    const int c = c0 + e;
-                    const size_t idx = static_cast<size_t>(y) * pw + c;
-                    if (v[idx] != val[e]) {
-                        changed = 1;
-                        v[idx] = val[e];
+                // forward along the row
+                {
+                    float lo = neutral, hi = -neutral;
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        lo = rec_op<DILATE>(gv[j], cv[j], lo);
+                        hi = rec_op<DILATE>(gv[j], cv[j], hi);
                     }
-                    prev[c] = val[e];
+                    float run = carry_in(lo, hi, true, 0);
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        run = rec_op<DILATE>(gv[j], cv[j], run);
+                        changed |= run != cv[j];
+                        cv[j] = run;
+                    }
                 }
-                __syncthreads();
+                // backward
+                {
+                    float lo = neutral, hi = -neutral;
+#pragma unroll
+                    for (int j = C - 1; j >= 0; --j) {
+                        lo = rec_op<DILATE>(gv[j], cv[j], lo);
+                        hi = rec_op<DILATE>(gv[j], cv[j], hi);
+                    }
+                    float run = carry_in(lo, hi, false, 1);
+#pragma unroll
+                    for (int j = C - 1; j >= 0; --j) {
+                        run = rec_op<DILATE>(gv[j], cv[j], run);
+                        changed |= run != cv[j];
+                        cv[j] = run;
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < C; ++j) V[c0 + j] = cv[j];
+                image_sync<RW>();
+                const size_t ro = static_cast<size_t>(y) * pw;
+                for (int c = t; c < pw; c += T) v[ro + c] = V[1 + c];
+                cp_async_wait_all(); // the next row has landed
+                image_sync<RW>();
+                gi ^= 1;
+                vi = (vi + 1) % 3;
             }
         }
-        if (changed) atomicOr(&changed_s, 1);
-        __syncthreads();
-        const int any = changed_s;
-        __syncthreads();
+        // image-wide vote (alternating flags: the one read now is cleared for the round after)
+        if (changed) any_changed[round & 1] = 1;
+        image_sync<RW>();
+        const int any = any_changed[round & 1];
+        if (t == 0) any_changed[(round + 1) & 1] = 0;
+        image_sync<RW>();
         if (!any) break;
     }
-    if (round == kMaxRounds && tid == 0) atomicExch(&g_device_error, 2);
+    if (round == kMaxRounds && t == 0) atomicExch(&g_msc_error, 2);
+}
+
+template <bool DILATE, int RW, int C>
+static mr_status launch_rec(int nimg, const float *pad, float sign, int pw, int ph, int conn8, float *vol,
+                            cudaStream_t s)
+{
+    const size_t smem = 5 * static_cast<size_t>(32 * RW * C + 3) * sizeof(float);
+    MR_CUDA_TRY(cudaFuncSetAttribute(k_reconstruct<DILATE, RW, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     static_cast<int>(smem)));
+    k_reconstruct<DILATE, RW, C><<<nimg, 32 * RW, smem, s>>>(pad, sign, pw, ph, conn8, vol);
+    return check_launch("k_reconstruct");
+}
+
+template <bool DILATE>
+static mr_status launch_reconstruct(int nimg, const float *pad, float sign, int pw, int ph, int conn8, float *vol,
+                                    cudaStream_t s)
+{
+    constexpr int RW = 4;
+    const int per = (pw + 32 * RW - 1) / (32 * RW);
+    if (per <= 3) return launch_rec<DILATE, RW, 3>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    if (per <= 5) return launch_rec<DILATE, RW, 5>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    if (per <= 9) return launch_rec<DILATE, RW, 9>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    if (per <= 17) return launch_rec<DILATE, RW, 17>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    if (per <= 33) return launch_rec<DILATE, RW, 33>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 32 * RW * 33 - 2 * kMargin);
 }
 
 // Replacement / blend and unpadding (MorphSpotClean::ProcessReplace :108-175,
@@ -378,24 +499,22 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     if (nu == 0 || nproj == 0) return MR_OK;
     const int w = static_cast<int>(nu), h = static_cast<int>(nv);
     const int pw = w + 2 * kMargin, ph = h + 2 * kMargin;
-    if (pw > kThreads * 8) return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", kThreads * 8 - 10);
+    if (pw > 128 * 33) return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 128 * 33 - 2 * kMargin);
     const size_t n = static_cast<size_t>(pw) * ph;
     cudaStream_t s = as_stream(stream);
-    // images per batch: three padded buffers each, about 1 GiB of scratch at most
+    // images per batch: three padded buffers each; up to a quarter of the free device memory,
+    // so that a block of projections is cleaned concurrently (one warp per image)
     const size_t per_img = 3 * n * sizeof(float);
-    const size_t batch = std::max<size_t>(1, std::min<size_t>(nproj, (size_t(1) << 30) / per_img));
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = size_t(1) << 30;
+    const size_t budget = std::max<size_t>(size_t(1) << 30, free_b / 4);
+    const size_t batch = std::max<size_t>(1, std::min<size_t>(nproj, budget / per_img));
     float *scratch = nullptr;
+    keep_pool_memory();
     MR_CUDA_TRY(cudaMallocAsync(&scratch, batch * per_img + 4 * batch * sizeof(float), s));
     float *P = scratch, *H = P + batch * n, *K = H + batch * n, *stats = K + batch * n;
     float *fmax = stats, *mn = stats + batch, *mx = stats + 2 * batch;
     mr_status st = MR_OK;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_reconstruct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        cudaFuncSetAttribute(k_reconstruct<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
-        attr = true;
-    }
-    const size_t rsmem = (pw + 64) * sizeof(float);
     for (size_t b0 = 0; b0 < nproj && st == MR_OK; b0 += batch) {
         const int nb = static_cast<int>(std::min(batch, nproj - b0));
         float *img = proj_d + b0 * nu * nv;
@@ -406,16 +525,16 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
         k_minmax<<<nb, 1024, 0, s>>>(P, n, mn, mx);
         if (detect == 0 || detect == 2) { // FillHole: erosion from a max marker
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
-            k_reconstruct<false><<<nb, kThreads, rsmem, s>>>(P, 1.0f, pw, ph, conn8, H);
+            if ((st = launch_reconstruct<false>(nb, P, 1.0f, pw, ph, conn8, H, s)) != MR_OK) break;
         }
         if (detect == 1) { // FillPeaks: forward-scan band replay, then the exact dilation
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, 1.0f, K);
             k_peaks_forward_band<<<div_up(nb, 32), 32, 0, s>>>(P, pw, ph, nb, conn8, mn, K);
-            k_reconstruct<true><<<nb, kThreads, rsmem, s>>>(P, 1.0f, pw, ph, conn8, K);
+            if ((st = launch_reconstruct<true>(nb, P, 1.0f, pw, ph, conn8, K, s)) != MR_OK) break;
         }
         if (detect == 2) { // -FillHole(-padded): erosion of the negated image from marker max(-P) = -min(P)
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, -1.0f, K);
-            k_reconstruct<false><<<nb, kThreads, rsmem, s>>>(P, -1.0f, pw, ph, conn8, K);
+            if ((st = launch_reconstruct<false>(nb, P, -1.0f, pw, ph, conn8, K, s)) != MR_OK) break;
         }
         if ((st = check_launch("morphspotclean reconstruction")) != MR_OK) break;
         k_replace<<<dim3(gx, nb), 256, 0, s>>>(P, detect != 1 ? H : nullptr, detect != 0 ? K : nullptr, w, h, detect,

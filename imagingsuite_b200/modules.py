@@ -506,6 +506,7 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         self.SizeU = self.SizeV = 0
         self._mask = None
         self._roi = (0, 0, 0, 0)
+        self.staging = True  # TMA-staged projection rows (False: direct global loads; same results)
 
     def SetROI(self, roi) -> None:
         pi = self.mConfig.ProjectionInfo
@@ -568,11 +569,13 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         scale = None
         if dtype != L.MR_F32:
             proj, scale = quantize(projections, self.precision)
-        check(L.lib().mr_bp_parallel(proj.data_ptr(), dtype, _ptr(scale),
-                                     None if prefiltered_weights else geo[3].data_ptr(), idx.data_ptr(), geo[0].data_ptr(),
-                                     geo[1].data_ptr(), geo[2].data_ptr(), sel.size, self.SizeU, self.SizeV,
-                                     self._mask.data_ptr(), int(pi.bCorrectTilt), toff.value, tinc.value,
-                                     self.volume.data_ptr(), _stream()))
+        args = (dtype, _ptr(scale), None if prefiltered_weights else geo[3].data_ptr(), idx.data_ptr(),
+                geo[0].data_ptr(), geo[1].data_ptr(), geo[2].data_ptr(), sel.size, self.SizeU, self.SizeV,
+                self._mask.data_ptr(), int(pi.bCorrectTilt), toff.value, tinc.value, self.volume.data_ptr(), _stream())
+        if self.staging:
+            check(L.lib().mr_bp_parallel_staged(proj.data_ptr(), nproj, *args))
+        else:
+            check(L.lib().mr_bp_parallel(proj.data_ptr(), *args))
         return 0
 
     def GetSlice(self, idx: int) -> torch.Tensor:

@@ -68,8 +68,9 @@ def _chords_np(p: np.ndarray, d: np.ndarray, ells: list[Ellipsoid]) -> np.ndarra
 
 
 def parallel_integrals(ells, nproj: int, nu: int, nv: int, arc: float = 180.0, box: float | None = None) -> np.ndarray:
-    """Parallel-beam line integrals (nproj, nv, nu), FP64. Detector pixel = 1 voxel; the box
-    spans nu pixels laterally and is centred on column (nu-1)/2 and row (nv-1)/2."""
+    """Parallel-beam line integrals (nproj, nv, nu), FP64, attenuation per box length (so the
+    integrals are O(1)). The box spans `box` pixels (default nu) laterally and is centred on
+    column (nu-1)/2 and row (nv-1)/2."""
     box = float(nu) if box is None else box
     ang = np.deg2rad(np.arange(nproj) * arc / nproj)
     u = (np.arange(nu) - (nu - 1) / 2) / box
@@ -79,7 +80,7 @@ def parallel_integrals(ells, nproj: int, nu: int, nv: int, arc: float = 180.0, b
         d = np.array([math.cos(t), math.sin(t), 0.0])
         lat = np.array([-math.sin(t), math.cos(t), 0.0])
         p = u[None, :, None] * lat + v[:, None, None] * np.array([0, 0, 1.0]) - 2.0 * d
-        out[k] = _chords_np(p, np.broadcast_to(d, p.shape), ells) * box
+        out[k] = _chords_np(p, np.broadcast_to(d, p.shape), ells)
     return out
 
 
@@ -203,3 +204,61 @@ def voxelize_torch(ells, n: int, nz: int, device, supersample: int = 1, fov_marg
         c = torch.arange(n, device=device, dtype=torch.float64) - (n - 1) / 2
         out[:, (c[:, None] ** 2 + c[None, :] ** 2) > (n / 2 - fov_margin) ** 2] = 0
     return out
+
+
+def parallel_integrals_torch(ells, nproj: int, nu: int, nv: int, device, arc: float = 180.0, box: float | None = None,
+                             v0: int = 0, chunk: int = 8):
+    """Device (FP32) version of :func:`parallel_integrals` for detector rows v0 .. v0+nv-1 of a
+    detector whose full height is `box` pixels (default nu): the rows of one slice block."""
+    import torch
+
+    box = float(nu) if box is None else box
+    out = torch.empty((nproj, nv, nu), dtype=torch.float32, device=device)
+    u = (torch.arange(nu, device=device, dtype=torch.float32) - (nu - 1) / 2) / box
+    v = (torch.arange(v0, v0 + nv, device=device, dtype=torch.float32) - (box - 1) / 2) / box
+    E = [(torch.tensor(e.center, dtype=torch.float32, device=device),
+          torch.tensor(e.rot, dtype=torch.float32, device=device),
+          torch.tensor(e.axes, dtype=torch.float32, device=device), e.mu) for e in ells]
+    for k0 in range(0, nproj, chunk):
+        ks = torch.arange(k0, min(nproj, k0 + chunk), device=device, dtype=torch.float32)
+        t = torch.deg2rad(ks * arc / nproj)
+        ct, st = torch.cos(t), torch.sin(t)
+        zero = torch.zeros_like(ct)
+        d = torch.stack([ct, st, zero], -1)                      # (c,3)
+        lat = torch.stack([-st, ct, zero], -1)
+        p = (u[None, None, :, None] * lat[:, None, None, :] + v[None, :, None, None] *
+             torch.tensor([0.0, 0.0, 1.0], device=device) - 2.0 * d[:, None, None, :])
+        dd = d[:, None, None, :].expand_as(p)
+        tot = torch.zeros(p.shape[:-1], device=device)
+        for c, rot, axes, mu in E:
+            q = ((p - c) @ rot) / axes
+            w = (dd @ rot) / axes
+            a = (w * w).sum(-1)
+            b = 2 * (q * w).sum(-1)
+            cc = (q * q).sum(-1) - 1
+            disc = b * b - 4 * a * cc
+            tot += mu * torch.where(disc > 0, torch.sqrt(torch.clamp(disc, min=0)) / a, torch.zeros_like(a))
+        out[k0:k0 + len(ks)] = tot
+    return out
+
+
+def inject_defects_torch(counts, flats, seed: int, spot_fraction: float = 5e-4, ncols: int = 20,
+                         gain=(1.005, 1.03)):
+    """Production-case defects, in place on uint16 tensors: a fraction of pixels of every
+    projection set to 65535 or tripled (half each), and ncols detector columns with a fixed
+    gain error in the projections but not in the flats (ring-producing)."""
+    import torch
+
+    g = torch.Generator(device=counts.device)
+    g.manual_seed(seed)
+    nproj, nv, nu = counts.shape
+    cols = torch.randperm(nu, generator=g, device=counts.device)[:ncols]
+    gains = torch.rand(ncols, generator=g, device=counts.device) * (gain[1] - gain[0]) + gain[0]
+    for k in range(nproj):
+        c = counts[k].to(torch.float32)
+        c[:, cols] *= gains
+        sel = torch.rand((nv, nu), generator=g, device=counts.device) < spot_fraction
+        hot = torch.rand((nv, nu), generator=g, device=counts.device) < 0.5
+        c = torch.where(sel & hot, torch.full_like(c, 65535.0), torch.where(sel, c * 3.0, c))
+        counts[k] = torch.clamp(torch.round(c), 0, 65535).to(torch.int32).to(torch.uint16)
+    return cols, gains

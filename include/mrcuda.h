@@ -12,6 +12,10 @@
  *   parallel-beam volume (MatrixZXY) [ny][nx][nz]  z fastest, nx = ny = nu, nz = nv
  *   FDK volume (MatrixXYZ)           [nz][ny][nx]  x fastest, nx = ny = nu, nz = nv
  *
+ * Entry points that need scratch take it from the device's default stream-ordered memory
+ * pool (cudaMallocAsync), whose release threshold they raise so that freed scratch stays
+ * cached for the next call.
+ *
  * Reference interfaces each group replaces are cited as file:line, relative to the
  * reference project root (DTasev/imagingsuite).
  */
@@ -195,6 +199,14 @@ mr_status mr_bp_parallel(const void *proj_d, int dtype, const float *scale_d, co
                          const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
                          size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt, float tiltoffset,
                          float tiltinc, float *vol_d, void *stream);
+/* The same backprojection with the projection rows of each 32 x 8 x 32 voxel tile staged in
+ * shared memory by TMA (FP32, no tilt correction, row pitch a multiple of 16 bytes);
+ * nslabs = number of projection slabs in proj_d (the bound of every TMA load). Other
+ * requests run mr_bp_parallel. Results are bit-identical on both paths. */
+mr_status mr_bp_parallel_staged(const void *proj_d, size_t nslabs, int dtype, const float *scale_d,
+                                const float *weight_d, const int32_t *index_d, const float *sin_d, const float *cos_d,
+                                const float *startu_d, size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d,
+                                int correcttilt, float tiltoffset, float tiltinc, float *vol_d, void *stream);
 
 /* ---------------------------------------------------------------------------------
  * FDK cone-beam backprojection: FDKbp_single
