@@ -34,6 +34,9 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "backprojection GUPS + projections/s, FP32 vs BF16-proj at <=1e-3 rel RMS vs FP64"
+# DRAM bytes (read + write) of one k_fdk_staged<f32, exact> launch, measured with ncu on this
+# workload (detector width -> bytes): 1024^3 268.61 GB + 5.51 GB, 256^3 69.8 MB + 39.7 MB
+MEASURED_TRAFFIC = {1024: 274.12e9, 256: 109.5e6}
 
 
 def workload(small: bool):
@@ -331,8 +334,10 @@ def run_mr(args):
                              ms_per_step=th16 / args.steps * 1e3, backprojection_gups=updates / tfast["fp16"] / 1e9),
             },
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
-                         "traffic": None, "kernel": "k_fdk_staged<f32, exact>",
-                         "note": f"algorithmic bytes = 4 B/update gathered; peak {peak_src}"},
+                         "traffic": MEASURED_TRAFFIC.get(nu), "kernel": "k_fdk_staged<f32, exact>",
+                         "note": f"algorithmic bytes = 4 B/update gathered, served from shared memory and L2; "
+                                 f"peak {peak_src}; traffic = dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                 f"launch (ncu, profiles/k_fdk_staged_fdk256_fdk1024.md)"},
             "e2e": {"value": n * updates * e2e_steps / te2e / 1e9, "unit": "GUPS",
                     "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(nu * nu * nv * 4)},
             "gpu_launches": 3 * args.steps,
