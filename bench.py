@@ -162,29 +162,6 @@ def time_steps(fn, steps, warmup, stream, dist_ctx, events_kernel=None):
     return t
 
 
-class Dist:
-    def __init__(self):
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-
-        self.dist = dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-        self.rank, self.world = dist.get_rank(), dist.get_world_size()
-        self.dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", 0)))
-
-    def barrier(self):
-        self.dist.barrier()
-
-    def max(self, v: float) -> float:
-        import torch
-
-        t = torch.tensor([v], dtype=torch.float64, device=self.dev)
-        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
-        return float(t.item())
-
-
 def kernel_time(fn, stream, reps=2):
     """Average device duration of one call of fn (CUDA events on `stream`)."""
     import torch
@@ -207,7 +184,9 @@ def run_mr(args):
     from imagingsuite_b200 import pipeline
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
-    dctx = Dist() if world > 1 else None
+    from imagingsuite_b200.distributed import DistContext
+
+    dctx = DistContext("nccl") if world > 1 else None
     rank = dctx.rank if dctx else 0
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
@@ -347,7 +326,7 @@ def run_mr(args):
             res["cpu_baseline"] = cpu_baseline(w, counts, flats, darks, angles, weights, budget_s=args.cpu_budget)
     if dctx:
         dctx.barrier()
-        dctx.dist.destroy_process_group()
+        dctx.close()
     return res
 
 
