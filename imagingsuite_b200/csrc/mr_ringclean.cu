@@ -72,58 +72,6 @@ __global__ void k_scatter(const float *__restrict__ s, int nu, int nv, int nproj
     }
 }
 
-// Row pass of one analysis level: tmpH/tmpG [B][sy][dx] from src [B][sy][sx].
-__global__ void k_dwt_rows(const float *__restrict__ src, int sx, int sy, int nb, const float *__restrict__ taps,
-                           int K, int dx, float *__restrict__ tmpH, float *__restrict__ tmpG)
-{
-    const float *tH = taps, *tG = taps + K;
-    const size_t total = static_cast<size_t>(nb) * sy * dx;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int k = static_cast<int>(i % dx);
-        const size_t row = i / dx;
-        const float *r = src + row * sx;
-        float aH = 0.0f, aG = 0.0f;
-        for (int j = 0; j < K; ++j) {
-            const float x = r[mirror_index(sx, K, K + 2 * k - j + 1)];
-            aH = __fadd_rn(aH, __fmul_rn(tH[j], x));
-            aG = __fadd_rn(aG, __fmul_rn(tG[j], x));
-        }
-        tmpH[i] = aH;
-        tmpG[i] = aG;
-    }
-}
-
-// Column pass: a = cols_H(tmpH), h = cols_G(tmpH), v = cols_H(tmpG), d = cols_G(tmpG),
-// each [B][dy][dx] (wavelets.hpp:474-487).
-__global__ void k_dwt_cols(const float *__restrict__ tmpH, const float *__restrict__ tmpG, int dx, int sy, int nb,
-                           const float *__restrict__ taps, int K, int dy, float *__restrict__ a,
-                           float *__restrict__ h, float *__restrict__ v, float *__restrict__ d)
-{
-    const float *tH = taps, *tG = taps + K;
-    const size_t total = static_cast<size_t>(nb) * dy * dx;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int x = static_cast<int>(i % dx);
-        const size_t r = i / dx;
-        const int k = static_cast<int>(r % dy), b = static_cast<int>(r / dy);
-        const size_t base = static_cast<size_t>(b) * sy * dx + x;
-        float sa = 0.0f, sh = 0.0f, sv = 0.0f, sd = 0.0f;
-        for (int m = 0; m < K; ++m) {
-            const size_t idx = base + static_cast<size_t>(mirror_index(sy, K, K + 2 * k - m + 1)) * dx;
-            const float ph = tmpH[idx], pg = tmpG[idx];
-            sa = __fadd_rn(sa, __fmul_rn(tH[m], ph));
-            sh = __fadd_rn(sh, __fmul_rn(tG[m], ph));
-            sv = __fadd_rn(sv, __fmul_rn(tH[m], pg));
-            sd = __fadd_rn(sd, __fmul_rn(tG[m], pg));
-        }
-        a[i] = sa;
-        h[i] = sh;
-        v[i] = sv;
-        d[i] = sd;
-    }
-}
-
 // FilterVerticalStripes (StripeFilter.cpp:114-135): every column of the vertical band
 // [B][bh][bw] zero-padded to n, filtered with the even real response, first bh samples kept.
 __global__ void k_stripe_fft(float *__restrict__ band, int bw, int bh, int ncols, int n, int logn,
@@ -153,64 +101,149 @@ __global__ void k_stripe_fft(float *__restrict__ band, int bw, int bh, int ncols
     }
 }
 
-// Row pass of upsconvRC (wavelets.hpp:750-808) for the four bands at once:
-// out[q][B][h][dx] from band q [B][h][w]; the row filter of band q is kh[q].
-__global__ void k_up_rows(const float *__restrict__ a, const float *__restrict__ hb, const float *__restrict__ vb,
-                          const float *__restrict__ db, int w, int h, int nb, const float *__restrict__ taps, int K,
-                          int dx, float *__restrict__ out)
+// ---- the four convolution passes: analysis rows (both filters per output) and columns (the
+// four sub-bands, wavelets.hpp:474-487); synthesis rows and columns of upsconvRC
+// (:750-858) summed as ((a + h) + v) + d (WaveletTransform::synthesize :626-645). Every output
+// is the sum over the taps in the reference's order; indices are 32-bit from the grid, the
+// taps sit in shared memory, and away from the borders (where the mirrored index is the
+// identity) the window is read directly. In the synthesis passes the interior skips the taps that meet
+// the zeros inserted by the dyadic upsampling (adding a product with 0 leaves a nonzero sum
+// unchanged, so only the sign of an exactly zero result can differ).
+constexpr int kConvThreads = 128;
+
+__device__ __forceinline__ void load_taps(const float *__restrict__ taps, int n, float *sm)
 {
-    const float *sH = taps + 2 * K, *sG = taps + 3 * K;
-    const size_t plane = static_cast<size_t>(nb) * h * dx;
-    const size_t total = 4 * plane;
-    const int c = K - 2;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int q = static_cast<int>(i / plane);
-        const size_t j = i % plane;
-        const int k = static_cast<int>(j % dx);
-        const size_t row = j / dx;
-        const float *src = (q == 0 ? a : q == 1 ? hb : q == 2 ? vb : db) + row * w;
-        const float *kh = q < 2 ? sH : sG;
-        float acc = 0.0f;
-        for (int m = 0; m < K; ++m) {
-            const int t = up_index(w, K, K + k + c - m);
-            const float x = (t & 1) ? 0.0f : src[t >> 1];
-            acc = __fadd_rn(acc, __fmul_rn(x, kh[m]));
+    for (int i = threadIdx.x; i < n; i += blockDim.x) sm[i] = taps[i];
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kConvThreads) k_dwt_rows2(const float *__restrict__ src, int sx, int nrows,
+                                                            const float *__restrict__ taps, int K, int dx,
+                                                            float *__restrict__ tmpH, float *__restrict__ tmpG)
+{
+    __shared__ float tp[2 * kMaxTaps];
+    load_taps(taps, 2 * K, tp);
+    const float *tH = tp, *tG = tp + K;
+    const int k = blockIdx.x * kConvThreads + threadIdx.x;
+    if (k >= dx) return;
+    const bool inner = 2 * k - K + 2 >= 0 && 2 * k + 1 < sx;
+    for (int row = blockIdx.y; row < nrows; row += gridDim.y) {
+        const float *r = src + static_cast<size_t>(row) * sx;
+        float aH = 0.0f, aG = 0.0f;
+        if (inner) {
+            const float *w = r + 2 * k + 1; // x_j = w[-j]
+            for (int j = 0; j < K; ++j) {
+                const float x = w[-j];
+                aH = __fadd_rn(aH, __fmul_rn(tH[j], x));
+                aG = __fadd_rn(aG, __fmul_rn(tG[j], x));
+            }
+        } else {
+            for (int j = 0; j < K; ++j) {
+                const float x = r[mirror_index(sx, K, K + 2 * k - j + 1)];
+                aH = __fadd_rn(aH, __fmul_rn(tH[j], x));
+                aG = __fadd_rn(aG, __fmul_rn(tG[j], x));
+            }
         }
-        out[i] = acc;
+        tmpH[static_cast<size_t>(row) * dx + k] = aH;
+        tmpG[static_cast<size_t>(row) * dx + k] = aG;
     }
 }
 
-// Column pass of upsconvRC (:810-858) for the four bands and their sum
-// ((a + h) + v) + d (WaveletTransform::synthesize :626-645); writes [B][oy][ox] of a
-// (dx, dy) result, ox <= dx, oy <= dy (the crop of the last level).
-__global__ void k_up_cols(const float *__restrict__ rows, int dx, int h, int nb, const float *__restrict__ taps, int K,
-                          int dy, int ox, int oy, float *__restrict__ out)
+__global__ void __launch_bounds__(kConvThreads) k_dwt_cols2(const float *__restrict__ tmpH,
+                                                            const float *__restrict__ tmpG, int dx, int sy,
+                                                            const float *__restrict__ taps, int K, int dy,
+                                                            float *__restrict__ a, float *__restrict__ h,
+                                                            float *__restrict__ v, float *__restrict__ d)
 {
-    const float *sH = taps + 2 * K, *sG = taps + 3 * K;
-    const size_t plane = static_cast<size_t>(nb) * h * dx;
-    const size_t total = static_cast<size_t>(nb) * oy * ox;
+    __shared__ float tp[2 * kMaxTaps];
+    load_taps(taps, 2 * K, tp);
+    const float *tH = tp, *tG = tp + K;
+    const int x = blockIdx.x * kConvThreads + threadIdx.x, k = blockIdx.y, b = blockIdx.z;
+    if (x >= dx) return;
+    const size_t base = static_cast<size_t>(b) * sy * dx + x;
+    const bool inner = 2 * k - K + 2 >= 0 && 2 * k + 1 < sy;
+    float sa = 0.0f, sh = 0.0f, sv = 0.0f, sd = 0.0f;
+    for (int m = 0; m < K; ++m) {
+        const int row = inner ? 2 * k - m + 1 : mirror_index(sy, K, K + 2 * k - m + 1);
+        const size_t idx = base + static_cast<size_t>(row) * dx;
+        const float ph = tmpH[idx], pg = tmpG[idx];
+        sa = __fadd_rn(sa, __fmul_rn(tH[m], ph));
+        sh = __fadd_rn(sh, __fmul_rn(tG[m], ph));
+        sv = __fadd_rn(sv, __fmul_rn(tH[m], pg));
+        sd = __fadd_rn(sd, __fmul_rn(tG[m], pg));
+    }
+    const size_t o = (static_cast<size_t>(b) * dy + k) * dx + x;
+    a[o] = sa;
+    h[o] = sh;
+    v[o] = sv;
+    d[o] = sd;
+}
+
+// out[q][row][k], q = blockIdx.z (a, h, v, d), rows over all batch images.
+__global__ void __launch_bounds__(kConvThreads) k_up_rows2(const float *__restrict__ a, const float *__restrict__ hb,
+                                                           const float *__restrict__ vb, const float *__restrict__ db,
+                                                           int w, int nrows, const float *__restrict__ taps, int K,
+                                                           int dx, float *__restrict__ out)
+{
+    __shared__ float tp[2 * kMaxTaps];
+    load_taps(taps + 2 * K, 2 * K, tp);
+    const int q = blockIdx.z;
+    const float *kh = q < 2 ? tp : tp + K;
+    const float *band = q == 0 ? a : q == 1 ? hb : q == 2 ? vb : db;
+    const int k = blockIdx.x * kConvThreads + threadIdx.x;
+    if (k >= dx) return;
     const int c = K - 2;
-    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int x = static_cast<int>(i % ox);
-        const size_t r = i / ox;
-        const int k = static_cast<int>(r % oy), b = static_cast<int>(r / oy);
-        const size_t base = static_cast<size_t>(b) * h * dx + x;
-        float s4[4];
-        for (int q = 0; q < 4; ++q) {
-            const float *kv = (q == 0 || q == 2) ? sH : sG;
-            const float *col = rows + q * plane + base;
-            float acc = 0.0f;
+    const bool inner = k >= 1 && k < 2 * w - K + 2;
+    const size_t plane = static_cast<size_t>(nrows) * dx;
+    for (int row = blockIdx.y; row < nrows; row += gridDim.y) {
+        const float *src = band + static_cast<size_t>(row) * w;
+        float acc = 0.0f;
+        if (inner) {
+            // t = k + c - m; even t only: m of the parity of k + c
+            for (int m = (k + c) & 1; m < K; m += 2) acc = __fadd_rn(acc, __fmul_rn(src[(k + c - m) >> 1], kh[m]));
+        } else {
+            for (int m = 0; m < K; ++m) {
+                const int t = up_index(w, K, K + k + c - m);
+                const float xv = (t & 1) ? 0.0f : src[t >> 1];
+                acc = __fadd_rn(acc, __fmul_rn(xv, kh[m]));
+            }
+        }
+        out[q * plane + static_cast<size_t>(row) * dx + k] = acc;
+    }
+}
+
+// out[b][k][x] = ((a + h) + v) + d of the column passes, cropped to (ox, oy).
+__global__ void __launch_bounds__(kConvThreads) k_up_cols2(const float *__restrict__ rows, int dx, int h, int nb,
+                                                           const float *__restrict__ taps, int K, int ox, int oy,
+                                                           float *__restrict__ out)
+{
+    __shared__ float tp[2 * kMaxTaps];
+    load_taps(taps + 2 * K, 2 * K, tp);
+    const int x = blockIdx.x * kConvThreads + threadIdx.x, k = blockIdx.y, b = blockIdx.z;
+    if (x >= ox) return;
+    const size_t plane = static_cast<size_t>(nb) * h * dx;
+    const size_t base = static_cast<size_t>(b) * h * dx + x;
+    const int c = K - 2;
+    const bool inner = k >= 1 && k < 2 * h - K + 2;
+    float s4[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float *kv = (q == 0 || q == 2) ? tp : tp + K;
+        const float *col = rows + q * plane + base;
+        float acc = 0.0f;
+        if (inner) {
+            for (int m = (k + c) & 1; m < K; m += 2)
+                acc = __fadd_rn(acc, __fmul_rn(col[static_cast<size_t>((k + c - m) >> 1) * dx], kv[m]));
+        } else {
             for (int m = 0; m < K; ++m) {
                 const int t = up_index(h, K, K + k + c - m);
                 const float xv = (t & 1) ? 0.0f : col[static_cast<size_t>(t >> 1) * dx];
                 acc = __fadd_rn(acc, __fmul_rn(xv, kv[m]));
             }
-            s4[q] = acc;
         }
-        out[i] = __fadd_rn(__fadd_rn(__fadd_rn(s4[0], s4[1]), s4[2]), s4[3]);
+        s4[q] = acc;
     }
+    out[(static_cast<size_t>(b) * oy + k) * ox + x] = __fadd_rn(__fadd_rn(__fadd_rn(s4[0], s4[1]), s4[2]), s4[3]);
 }
 
 struct Plan {
@@ -330,12 +363,15 @@ static mr_status stripe_batch(float *s_d, int nb, const rc::Plan &P, const float
         Db[l] = scratch + off; off += n;
     }
     float *tmp = scratch + off;
-    const unsigned blocks = 148 * 8;
     for (int l = 0; l < L; ++l) {
         const int sx = P.sx[l], sy = P.sy[l], dx = P.sx[l + 1], dy = P.sy[l + 1];
         float *tH = tmp, *tG = tmp + static_cast<size_t>(nb) * sy * dx;
-        k_dwt_rows<<<blocks, 256, 0, st>>>(A[l], sx, sy, nb, taps_d, K, dx, tH, tG);
-        k_dwt_cols<<<blocks, 256, 0, st>>>(tH, tG, dx, sy, nb, taps_d, K, dy, A[l + 1], Hb[l + 1], Vb[l + 1], Db[l + 1]);
+        const int rows = nb * sy;
+        k_dwt_rows2<<<dim3(div_up(dx, kConvThreads), std::min(rows, 65535)), kConvThreads, 0, st>>>(A[l], sx, rows,
+                                                                                                  taps_d, K, dx, tH, tG);
+        k_dwt_cols2<<<dim3(div_up(dx, kConvThreads), dy, nb), kConvThreads, 0, st>>>(tH, tG, dx, sy, taps_d, K, dy,
+                                                                                    A[l + 1], Hb[l + 1], Vb[l + 1],
+                                                                                    Db[l + 1]);
     }
     for (int l = 0; l < L; ++l) {
         const int bw = P.sx[l + 1], bh = P.sy[l + 1], n = P.nfft[l];
@@ -346,9 +382,12 @@ static mr_status stripe_batch(float *s_d, int nb, const rc::Plan &P, const float
     for (int l = L - 1; l >= 0; --l) {
         const int w = P.sx[l + 1], h = P.sy[l + 1];
         const int dx = l == 0 ? 2 * P.sx[1] : P.sx[l], dy = l == 0 ? 2 * P.sy[1] : P.sy[l];
-        k_up_rows<<<blocks, 256, 0, st>>>(A[l + 1], Hb[l + 1], Vb[l + 1], Db[l + 1], w, h, nb, taps_d, K, dx, tmp);
+        const int rows = nb * h;
+        k_up_rows2<<<dim3(div_up(dx, kConvThreads), std::min(rows, 65535), 4), kConvThreads, 0, st>>>(
+            A[l + 1], Hb[l + 1], Vb[l + 1], Db[l + 1], w, rows, taps_d, K, dx, tmp);
         const int ox = l == 0 ? P.sx[0] : dx, oy = l == 0 ? P.sy[0] : dy;
-        k_up_cols<<<blocks, 256, 0, st>>>(tmp, dx, h, nb, taps_d, K, dy, ox, oy, A[l]);
+        k_up_cols2<<<dim3(div_up(ox, kConvThreads), oy, nb), kConvThreads, 0, st>>>(tmp, dx, h, nb, taps_d, K, ox, oy,
+                                                                                  A[l]);
     }
     return check_launch("stripe filter");
 }
