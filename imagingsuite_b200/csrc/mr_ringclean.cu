@@ -88,14 +88,14 @@ __global__ void k_stripe_fft(float *__restrict__ band, int bw, int bh, int ncols
             x0 = band[base0 + static_cast<size_t>(p) * bw];
             if (has1) x1 = band[base1 + static_cast<size_t>(p) * bw];
         }
-        buf[fft_bitrev(p, logn)] = make_float2(x0, x1);
+        buf[p] = make_float2(x0, x1);
     }
     __syncthreads();
-    fft_forward_dit(buf, n, logn, twiddle);
+    fft_forward(buf, logn, twiddle);
     fft_apply_response(buf, n, response);
-    fft_inverse_dif(buf, n, logn, twiddle);
+    fft_inverse(buf, logn, twiddle);
     for (int p = threadIdx.x; p < bh; p += blockDim.x) {
-        const float2 v = buf[fft_bitrev(p, logn)];
+        const float2 v = buf[p];
         band[base0 + static_cast<size_t>(p) * bw] = v.x;
         if (has1) band[base1 + static_cast<size_t>(p) * bw] = v.y;
     }
@@ -291,6 +291,13 @@ static size_t next_power2(size_t n)
     return static_cast<size_t>(std::floor(std::exp(logtwo * std::ceil(std::log(static_cast<double>(n)) / logtwo)) + 0.5));
 }
 
+static int ilog2i(int n)
+{
+    int l = 0;
+    while ((1 << l) < n) ++l;
+    return l;
+}
+
 static mr_status make_plan(size_t nu, size_t ntheta, const char *wname, int decnum, float sigma, rc::Plan &P)
 {
     mr_status st = wavelet_taps(wname, &P.begin, &P.end, P.taps);
@@ -323,26 +330,12 @@ static mr_status make_plan(size_t nu, size_t ntheta, const char *wname, int decn
         // the c2r reads bins 0..N/2: response damp[k] on 0..N/2, mirrored above
         P.resp[l].resize(N);
         for (size_t k = 0; k < N; ++k) P.resp[l][k] = damp[k <= N / 2 ? k : N - k];
+        // in the order of the forward transform's output
+        P.resp[l] = fft_permute_response(P.resp[l], ilog2i(static_cast<int>(N)));
     }
     return MR_OK;
 }
 
-static std::vector<float2> twiddles_for(int n)
-{
-    std::vector<float2> t(n / 2);
-    for (int k = 0; k < n / 2; ++k) {
-        const double ang = -2.0 * M_PI * static_cast<double>(k) / n;
-        t[k] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang)));
-    }
-    return t;
-}
-
-static int ilog2i(int n)
-{
-    int l = 0;
-    while ((1 << l) < n) ++l;
-    return l;
-}
 
 // Stripe filter of nb contiguous sinograms s [nb][ntheta][nu], in place.
 static mr_status stripe_batch(float *s_d, int nb, const rc::Plan &P, const float *taps_d,
@@ -430,12 +423,11 @@ static mr_status run_stripes(float *data_d, bool interleaved, size_t nu, size_t 
     off += 4 * P.K;
     std::vector<std::vector<float2>> tws(P.levels);
     for (int l = 0; l < P.levels; ++l) {
-        tw_d[l] = reinterpret_cast<float2 *>(work + off);
-        off += P.nfft[l];          // n/2 float2 = n floats
+        tw_d[l] = reinterpret_cast<float2 *>(work + off); // n float2 (offsets stay even: 8-byte aligned)
+        off += 2 * static_cast<size_t>(P.nfft[l]);
         resp_d[l] = work + off;
         off += P.nfft[l];
-        off += P.nfft[l];          // keep 8-byte alignment slack
-        tws[l] = twiddles_for(P.nfft[l]);
+        tws[l] = fft_twiddles(P.nfft[l]);
     }
     float *scratch = work + off;
     off += stripe_scratch(P, nb);

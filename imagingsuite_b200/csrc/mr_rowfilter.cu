@@ -113,21 +113,21 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
     const float *row0 = a.in + src0 * a.nu;
     const float *row1 = a.in + src1 * a.nu;
 
-    // padded complex row, stored bit-reversed
+    // padded complex row (two real rows as re/im), natural order
     for (int p = threadIdx.x; p < n; p += blockDim.x) {
         float x0 = padded_value(a, row0, r0, p);
         float x1 = has1 ? padded_value(a, row1, r1, p) : 0.0f;
-        buf[fft_bitrev(p, a.logn)] = make_float2(x0, x1);
+        buf[p] = make_float2(x0, x1);
     }
     __syncthreads();
 
-    fft_forward_dit(buf, n, a.logn, a.twiddle);
+    fft_forward(buf, a.logn, a.twiddle);
     fft_apply_response(buf, n, a.response);
-    fft_inverse_dif(buf, n, a.logn, a.twiddle);
+    fft_inverse(buf, a.logn, a.twiddle);
 
     // crop and write
     for (int i = threadIdx.x; i < a.nu; i += blockDim.x) {
-        const float2 v = buf[fft_bitrev(i + a.ninsert, a.logn)];
+        const float2 v = buf[i + a.ninsert];
         float y0 = __fmul_rn(v.x, a.scale);
         float y1 = __fmul_rn(v.y, a.scale);
         if (a.mode == kPadProjFilter) {
@@ -154,17 +154,6 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
             if (has1) a.out[r1 * a.nu + i] = y1;
         }
     }
-}
-
-// Host-side twiddle table exp(-2 pi i k / n), k < n/2, in double then rounded.
-static std::vector<float2> twiddles(int n)
-{
-    std::vector<float2> t(n / 2);
-    for (int k = 0; k < n / 2; ++k) {
-        const double ang = -2.0 * M_PI * static_cast<double>(k) / n;
-        t[k] = make_float2(static_cast<float>(std::cos(ang)), static_cast<float>(std::sin(ang)));
-    }
-    return t;
 }
 
 static int ilog2(size_t n)
@@ -381,7 +370,8 @@ mr_status mr_projfilter_create(size_t nu, const char *filtertype, float cutoff, 
     // full-length response: filter on 0..n2-1 and mirrored, Nyquist bin passes
     std::vector<float> resp(nfft);
     for (size_t k = 0; k < nfft; ++k) resp[k] = k == n2 ? 1.0f : filter[k < n2 ? k : nfft - k];
-    std::vector<float2> tw = twiddles(static_cast<int>(nfft));
+    resp = fft_permute_response(resp, ilog2(nfft)); // in the order of the forward transform's output
+    std::vector<float2> tw = fft_twiddles(static_cast<int>(nfft));
 
     mr_filter_plan *p = new mr_filter_plan;
     p->nu = nu;
@@ -511,7 +501,8 @@ mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, c
         ramp[i] *= (0.54 + 0.46 * (std::cos(i * degtorad * 360 / padwidth) + 1));
         ramp[i] /= padwidth * 0.5;
     }
-    std::vector<float2> tw = twiddles(static_cast<int>(padwidth));
+    ramp = fft_permute_response(ramp, ilog2(padwidth)); // in the order of the forward transform's output
+    std::vector<float2> tw = fft_twiddles(static_cast<int>(padwidth));
     cudaStream_t s = as_stream(stream);
     float2 *tw_d = nullptr;
     float *resp_d = nullptr;
