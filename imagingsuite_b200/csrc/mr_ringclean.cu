@@ -369,7 +369,7 @@ static mr_status stripe_batch(float *s_d, int nb, const rc::Plan &P, const float
     for (int l = 0; l < L; ++l) {
         const int bw = P.sx[l + 1], bh = P.sy[l + 1], n = P.nfft[l];
         const int ncols = nb * bw;
-        k_stripe_fft<<<(ncols + 1) / 2, std::min(512, std::max(64, n / 4)), n * sizeof(float2), st>>>(
+        k_stripe_fft<<<(ncols + 1) / 2, std::min(512, std::max(64, n / 8)), n * sizeof(float2), st>>>(
             Vb[l + 1], bw, bh, ncols, n, ilog2i(n), tw_d[l], resp_d[l]);
     }
     for (int l = L - 1; l >= 0; --l) {

@@ -172,7 +172,7 @@ mr_status launch_rowfilter(RowFilterArgs a, cudaStream_t s)
         MR_CUDA_TRY(cudaFuncSetAttribute(k_rowfilter, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         attr_set = true;
     }
-    const unsigned threads = static_cast<unsigned>(std::min(512, std::max(64, a.n / 4)));
+    const unsigned threads = static_cast<unsigned>(std::min(512, std::max(64, a.n / 8))); // one radix-8 butterfly each
     const size_t blocks = (a.nrows + 1) / 2;
     if (blocks > 0x7fffffffu) return fail(MR_ERR_ARGUMENT, "row filter: too many rows in one call");
     k_rowfilter<<<static_cast<unsigned>(blocks), threads, smem, s>>>(a);
