@@ -26,6 +26,9 @@
 //    detector are zero-filled by the TMA unit, which is exactly the reference's
 //    "outside -> 0" rule, so the per-voxel loop needs no bounds test. Two stages are in
 //    flight (double buffering on two mbarriers with bounded waits).
+//  * The per-projection geometry (detector maps, or the exact kernel's xip/yip/zip entries
+//    of the tile) is copied with cp.async three batches ahead, and the footprints are formed
+//    from those shared-memory copies, so no global load sits between two block barriers.
 //  * The detector row is floor(r), taken from the bit pattern of r + 1.5*2^23 added with
 //    round-toward-minus-infinity; the shared-memory address of the sample is one integer
 //    multiply-add of those bits.
@@ -76,6 +79,8 @@ struct Params {
 using tma::mbar_expect_tx;
 using tma::mbar_init;
 using tma::mbar_wait;
+using tma::copy4_zfill;
+using tma::copy_wait_all;
 using tma::smem_addr;
 
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
@@ -107,18 +112,6 @@ __device__ __forceinline__ float from_storage(unsigned short v)
 {
     if constexpr (DT == MR_BF16) return __bfloat162float(__ushort_as_bfloat16(v));
     else return __half2float(__ushort_as_half(v));
-}
-
-// Exact per-voxel detector coordinates (float, reference order), for the corner footprints.
-__device__ __forceinline__ void project_exact(const Params &P, int p, int i, int j, int k, float &r, float &c)
-{
-    const float *X = P.xip + (static_cast<size_t>(p) * P.nu + i) * 3;
-    const float *Y = P.yip + (static_cast<size_t>(p) * P.nu + j) * 3;
-    const float *Z = P.zip + (static_cast<size_t>(p) * P.nv + k) * 3;
-    const float a0 = __fadd_rn(Z[0], Y[0]), a1 = __fadd_rn(Z[1], Y[1]), a2 = __fadd_rn(Z[2], Y[2]);
-    const float dw = __fdiv_rn(1.0f, __fadd_rn(a2, X[2]));
-    r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, X[1])), 0.5f);
-    c = __fadd_rn(__fmul_rn(dw, __fadd_rn(a0, X[0])), 0.5f);
 }
 
 // Fast-path coordinates of voxel column (i, j) at slice k0 of the tile: column c, row r0 of
@@ -187,11 +180,12 @@ __device__ __forceinline__ void fast_column_staged(float2 (&acc)[TK / 2], const 
     }
 }
 
-// Shared-memory layout of both kernels.
+// Shared-memory layout of both kernels. Geometry is triple-buffered: batch s+3's copies
+// are in flight while batch s is consumed, and batch s+2's is complete for its footprints.
 template <int NB, int GEO, bool A1>
 struct Smem {
     unsigned char *stage; // [2][NB] boxes
-    float *geo;           // [2][NB][GEO]
+    float *geo;           // [3][NB][GEO]
     float *a1;            // [NWARPS][NB][TK] (exact kernel)
     int4 *meta;           // [2][NB]: x0, y0, mode
     uint64_t *bars;       // [2]
@@ -199,111 +193,125 @@ struct Smem {
     {
         stage = base;
         geo = reinterpret_cast<float *>(base + 2 * NB * boxbytes);
-        a1 = geo + 2 * NB * GEO;
+        a1 = geo + 3 * NB * GEO;
         meta = reinterpret_cast<int4 *>(a1 + (A1 ? NWARPS * NB * TK : 0));
         bars = reinterpret_cast<uint64_t *>(meta + 2 * NB);
     }
     static size_t bytes(int boxbytes)
     {
-        return 2 * NB * static_cast<size_t>(boxbytes) + (2 * NB * GEO + (A1 ? NWARPS * NB * TK : 0)) * sizeof(float) +
+        return 2 * NB * static_cast<size_t>(boxbytes) + (3 * NB * GEO + (A1 ? NWARPS * NB * TK : 0)) * sizeof(float) +
                2 * NB * sizeof(int4) + 2 * sizeof(uint64_t);
     }
 };
 
-// Producer: footprints of NB projections (4 per producer warp, 8 corner lanes each), TMA
-// issue, and the per-projection geometry staged by all threads.
-template <int DT, bool EXACT, int NB>
-__device__ __forceinline__ void produce(const Params &P, const CUtensorMap *tmap, Smem<NB, EXACT ? GEO_EXACT : GEO_FAST, EXACT> &S,
-                                        int s, int st, int i0, int j0, int k0, int i_hi, int j_hi, int kmax)
+// Starts the asynchronous copy of batch s's per-projection geometry into geometry buffer gb
+// (all threads; zero where a projection, column, row or slice does not exist).
+template <bool EXACT, int NB>
+__device__ __forceinline__ void stage_geometry(const Params &P, float *geo, int s, int i0, int j0, int k0, int kmax)
 {
-    using T = typename Sample<DT>::T;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    if (warp < NB / 4) {
-        const int b = warp * 4 + (lane >> 3), corner = lane & 7;
-        const int p = s * NB + b;
-        int rmin = 0, rmax = 0, cmin = 0, cmax = 0;
-        bool ok = p < P.nproj;
-        if (ok) {
-            const int ci = (corner & 1) ? i_hi : i0, cj = (corner & 2) ? j_hi : j0;
-            float r, c;
-            if constexpr (EXACT) {
-                project_exact(P, p, ci, cj, (corner & 4) ? k0 + kmax - 1 : k0, r, c);
-            } else {
-                const float *m = P.maps + static_cast<size_t>(p) * 12;
-                const float mm[12] = {__ldg(m), __ldg(m + 1), __ldg(m + 2), __ldg(m + 3), __ldg(m + 4), __ldg(m + 5),
-                                      __ldg(m + 6), __ldg(m + 7), __ldg(m + 8), __ldg(m + 9), __ldg(m + 10), __ldg(m + 11)};
-                const float w = fmaf(mm[8], static_cast<float>(ci), fmaf(mm[9], static_cast<float>(cj), mm[11]));
-                const FastCol f = fast_column(mm, static_cast<float>(ci), static_cast<float>(cj), static_cast<float>(k0));
-                c = f.c;
-                r = (corner & 4) ? fmaf(static_cast<float>(kmax - 1), f.dr, f.r0) : f.r0;
-                ok = w > 0.0f;
-            }
-            ok = ok && fabsf(r) < 4.0e6f && fabsf(c) < 4.0e6f;
-            rmin = rmax = ok ? __float2int_rd(r) : 0;
-            cmin = cmax = ok ? __float2int_rd(c) : 0;
-        }
-#pragma unroll
-        for (int o = 1; o < 8; o <<= 1) {
-            rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
-            rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
-            cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
-            cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
-            ok = __shfl_xor_sync(0xffffffffu, static_cast<int>(ok), o) && ok;
-        }
-        // 0: footprint does not fit (global fallback), 1: staged, 2: nothing to read
-        int mode = 0, x0 = 0, y0 = 0;
-        if (p < P.nproj && ok) {
-            if (cmax < -1 || cmin > P.nu || rmax < -1 || rmin > P.nv) {
-                mode = 2;
-            } else {
-                x0 = cmin - 1;
-                x0 = x0 >= 0 ? (x0 / P.xalign) * P.xalign : -(((-x0) + P.xalign - 1) / P.xalign) * P.xalign;
-                y0 = rmin - 1;
-                if (cmax + 1 < x0 + P.bw && rmax + 1 < y0 + P.bh) mode = 1;
-            }
-        }
-        const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
-        if (lane == 0)
-            mbar_expect_tx(&S.bars[st], static_cast<uint32_t>(__popc(staged)) * P.bw * P.bh * sizeof(T));
-        __syncwarp();
-        if (corner == 0 && p < P.nproj) {
-            S.meta[st * NB + b] = make_int4(x0, y0, mode, 0);
-            if (mode == 1) {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                tma_load_3d(S.stage + (st * NB + b) * P.boxbytes, tmap, x0, y0, p, &S.bars[st]);
-            }
-        }
-    }
     if constexpr (EXACT) {
         for (int idx = threadIdx.x; idx < NB * GEO_EXACT; idx += THREADS) {
             const int b = idx / GEO_EXACT, e = idx % GEO_EXACT, p = s * NB + b;
-            float v = 0.0f;
+            const float *src = P.zip;
+            bool ok = false;
             if (p < P.nproj) {
                 if (e < TK) {
-                    if (e < kmax) v = P.zip[(static_cast<size_t>(p) * P.nv + k0 + e) * 3 + 1];
+                    ok = e < kmax;
+                    src = P.zip + (static_cast<size_t>(p) * P.nv + k0 + e) * 3 + 1;
                 } else if (e < TK + 3 * TI) {
                     const int ii = i0 + (e - TK) / 3;
-                    if (ii < P.nu) v = P.xip[(static_cast<size_t>(p) * P.nu + ii) * 3 + (e - TK) % 3];
+                    ok = ii < P.nu;
+                    src = P.xip + (static_cast<size_t>(p) * P.nu + ii) * 3 + (e - TK) % 3;
                 } else if (e < TK + 3 * TI + 3 * TJ) {
                     const int jj = j0 + (e - TK - 3 * TI) / 3;
-                    if (jj < P.nu) v = P.yip[(static_cast<size_t>(p) * P.nu + jj) * 3 + (e - TK - 3 * TI) % 3];
+                    ok = jj < P.nu;
+                    src = P.yip + (static_cast<size_t>(p) * P.nu + jj) * 3 + (e - TK - 3 * TI) % 3;
                 } else if (e == TK + 3 * TI + 3 * TJ) {
-                    v = P.zip[static_cast<size_t>(p) * P.nv * 3];
+                    ok = true;
+                    src = P.zip + static_cast<size_t>(p) * P.nv * 3;
                 } else if (e == TK + 3 * TI + 3 * TJ + 1) {
-                    v = P.zip[static_cast<size_t>(p) * P.nv * 3 + 2];
+                    ok = true;
+                    src = P.zip + static_cast<size_t>(p) * P.nv * 3 + 2;
                 }
             }
-            S.geo[st * NB * GEO_EXACT + idx] = v;
+            copy4_zfill(geo + idx, ok ? src : P.zip, ok);
         }
     } else {
         for (int idx = threadIdx.x; idx < NB * GEO_FAST; idx += THREADS) {
             const int b = idx / GEO_FAST, e = idx % GEO_FAST, p = s * NB + b;
-            float v = 0.0f;
-            if (p < P.nproj) {
-                if (e < 12) v = P.maps[static_cast<size_t>(p) * 12 + e];
-                else if (e == 12) v = P.scale[p];
-            }
-            S.geo[st * NB * GEO_FAST + idx] = v;
+            const bool ok = p < P.nproj && e <= 12;
+            const float *src = !ok ? P.maps : e < 12 ? P.maps + static_cast<size_t>(p) * 12 + e : P.scale + p;
+            copy4_zfill(geo + idx, src, ok);
+        }
+    }
+}
+
+// Footprints of batch s's NB projections from its staged geometry (4 projections per producer
+// warp, 8 corner lanes each, the same arithmetic as the voxels), then the TMA copies into
+// stage st.
+template <int DT, bool EXACT, int NB>
+__device__ __forceinline__ void issue_batch(const Params &P, const CUtensorMap *tmap, Smem<NB, EXACT ? GEO_EXACT : GEO_FAST, EXACT> &S,
+                                            const float *geo, int s, int st, int i0, int j0, int k0, int i_hi, int j_hi,
+                                            int kmax)
+{
+    using T = typename Sample<DT>::T;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp >= NB / 4) return;
+    const int b = warp * 4 + (lane >> 3), corner = lane & 7;
+    const int p = s * NB + b;
+    int rmin = 0, rmax = 0, cmin = 0, cmax = 0;
+    bool ok = p < P.nproj;
+    if (ok) {
+        const int ci = (corner & 1) ? i_hi : i0, cj = (corner & 2) ? j_hi : j0;
+        float r, c;
+        if constexpr (EXACT) {
+            const float *g = geo + b * GEO_EXACT;
+            const float *X = g + TK + 3 * (ci - i0), *Y = g + TK + 3 * TI + 3 * (cj - j0);
+            const float Z0 = g[TK + 3 * TI + 3 * TJ], Z2 = g[TK + 3 * TI + 3 * TJ + 1];
+            const float a1 = __fadd_rn(g[(corner & 4) ? kmax - 1 : 0], Y[1]);
+            const float dw = __frcp_rn(__fadd_rn(__fadd_rn(Z2, Y[2]), X[2]));
+            r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, X[1])), 0.5f);
+            c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(Z0, Y[0]), X[0])), 0.5f);
+        } else {
+            const float *mm = geo + b * GEO_FAST;
+            const float w = fmaf(mm[8], static_cast<float>(ci), fmaf(mm[9], static_cast<float>(cj), mm[11]));
+            const FastCol f = fast_column(mm, static_cast<float>(ci), static_cast<float>(cj), static_cast<float>(k0));
+            c = f.c;
+            r = (corner & 4) ? fmaf(static_cast<float>(kmax - 1), f.dr, f.r0) : f.r0;
+            ok = w > 0.0f;
+        }
+        ok = ok && fabsf(r) < 4.0e6f && fabsf(c) < 4.0e6f;
+        rmin = rmax = ok ? __float2int_rd(r) : 0;
+        cmin = cmax = ok ? __float2int_rd(c) : 0;
+    }
+#pragma unroll
+    for (int o = 1; o < 8; o <<= 1) {
+        rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+        rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, o));
+        cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, o));
+        cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+        ok = __shfl_xor_sync(0xffffffffu, static_cast<int>(ok), o) && ok;
+    }
+    // 0: footprint does not fit (global fallback), 1: staged, 2: nothing to read
+    int mode = 0, x0 = 0, y0 = 0;
+    if (p < P.nproj && ok) {
+        if (cmax < -1 || cmin > P.nu || rmax < -1 || rmin > P.nv) {
+            mode = 2;
+        } else {
+            x0 = cmin - 1;
+            x0 = x0 >= 0 ? (x0 / P.xalign) * P.xalign : -(((-x0) + P.xalign - 1) / P.xalign) * P.xalign;
+            y0 = rmin - 1;
+            if (cmax + 1 < x0 + P.bw && rmax + 1 < y0 + P.bh) mode = 1;
+        }
+    }
+    const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
+    if (lane == 0) mbar_expect_tx(&S.bars[st], static_cast<uint32_t>(__popc(staged)) * P.bw * P.bh * sizeof(T));
+    __syncwarp();
+    if (corner == 0 && p < P.nproj) {
+        S.meta[st * NB + b] = make_int4(x0, y0, mode, 0);
+        if (mode == 1) {
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            tma_load_3d(S.stage + (st * NB + b) * P.boxbytes, tmap, x0, y0, p, &S.bars[st]);
         }
     }
 }
@@ -378,8 +386,12 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
     const int i_hi = min(i0 + TI - 1, P.nu - 1), j_hi = min(j0 + TJ - 1, P.nu - 1);
     const int nbatch = (P.nproj + NB - 1) / NB;
 
-    produce<DT, EXACT, NB>(P, &tmap, S, 0, 0, i0, j0, k0, i_hi, j_hi, kmax);
-    if (nbatch > 1) produce<DT, EXACT, NB>(P, &tmap, S, 1, 1, i0, j0, k0, i_hi, j_hi, kmax);
+    // geometry of batches 0-2, footprints and copies of batches 0-1
+    for (int s = 0; s < 3 && s < nbatch; ++s) stage_geometry<EXACT, NB>(P, S.geo + s * NB * GEO, s, i0, j0, k0, kmax);
+    copy_wait_all();
+    __syncthreads();
+    for (int s = 0; s < 2 && s < nbatch; ++s)
+        issue_batch<DT, EXACT, NB>(P, &tmap, S, S.geo + s * NB * GEO, s, s, i0, j0, k0, i_hi, j_hi, kmax);
     __syncthreads();
 
     uint32_t phase0 = 0, phase1 = 0;
@@ -388,27 +400,31 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
     const float fi = static_cast<float>(i), fj = static_cast<float>(j), fk0 = static_cast<float>(k0);
     const uint32_t rowbytes = static_cast<uint32_t>(P.rowbytes);
     const bool warp_inside = __any_sync(0xffffffffu, inside);
-    for (int s = 0; s < nbatch; ++s) {
-        const int st = s & 1;
+    for (int s = 0, gb = 0; s < nbatch; ++s, gb = gb == 2 ? 0 : gb + 1) {
+        const int st = s & 1;  // stage buffer
+        const float *geo = S.geo + gb * NB * GEO; // geometry buffer s % 3
         const uint32_t par = st ? phase1 : phase0;
-        if (!mbar_wait(&S.bars[st], par)) {
+        // a wait that timed out skips the batch in its whole warp; the block then leaves the
+        // loop together at the barrier below
+        const bool got = __all_sync(0xffffffffu, mbar_wait(&S.bars[st], par));
+        if (got) {
+            if (st) phase1 ^= 1; else phase0 ^= 1;
+        } else {
             failed = true;
-            atomicExch(&g_device_error, 1);
-            break;
+            if (lane == 0) atomicExch(&g_device_error, 1);
         }
-        if (st) phase1 ^= 1; else phase0 ^= 1;
 
         if constexpr (EXACT) {
             // per-warp slice sums a1[k] = zip1[k] + yip1[j] (lane = slice)
-            if (warp_inside) {
+            if (got && warp_inside) {
                 for (int idx = lane; idx < NB * TK; idx += 32) {
-                    const float *g = S.geo + (st * NB + idx / TK) * GEO_EXACT;
+                    const float *g = geo + (idx / TK) * GEO_EXACT;
                     S.a1[warp * NB * TK + idx] = __fadd_rn(g[idx % TK], g[TK + 3 * TI + 3 * warp + 1]);
                 }
                 __syncwarp();
             }
         }
-        if (inside) {
+        if (got && inside) {
             // projections in groups of G: the per-projection set-up of a group (reciprocal,
             // detector column, shared-memory base) is formed first, so its latency overlaps
             constexpr int G = 4;
@@ -421,7 +437,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                 for (int e = 0; e < G; ++e) {
                     const int b = b0 + e, p = s * NB + b;
                     const int4 m = S.meta[st * NB + b];
-                    const float *g = S.geo + (st * NB + b) * GEO;
+                    const float *g = geo + b * GEO;
                     const uint32_t boxoff = static_cast<uint32_t>((st * NB + b) * P.boxbytes);
                     q_on[e] = false;
                     q_a[e] = q_b[e] = q_c[e] = 0.0f;
@@ -475,7 +491,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                 for (int e = 0; e < G; ++e) {
                     const int b = b0 + e, p = s * NB + b;
                     if (p >= P.nproj || S.meta[st * NB + b].z != 0) continue;
-                    const float *g = S.geo + (st * NB + b) * GEO;
+                    const float *g = geo + b * GEO;
                     if constexpr (EXACT) {
                         const float x0f = g[TK + 3 * lane], x1f = g[TK + 3 * lane + 1], x2f = g[TK + 3 * lane + 2];
                         const float y0f = g[TK + 3 * TI + 3 * warp], y2f = g[TK + 3 * TI + 3 * warp + 2];
@@ -517,8 +533,15 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                 }
             }
         }
-        __syncthreads();
-        if (s + 2 < nbatch) produce<DT, EXACT, NB>(P, &tmap, S, s + 2, st, i0, j0, k0, i_hi, j_hi, kmax);
+        // batch s+2's geometry (in flight since batch s-1) complete and published; stage st and
+        // geometry buffer gb free
+        copy_wait_all();
+        if (__syncthreads_or(failed)) break;
+        if (s + 2 < nbatch) {
+            const int g2 = gb == 0 ? 2 : gb - 1;
+            issue_batch<DT, EXACT, NB>(P, &tmap, S, S.geo + g2 * NB * GEO, s + 2, st, i0, j0, k0, i_hi, j_hi, kmax);
+        }
+        if (s + 3 < nbatch) stage_geometry<EXACT, NB>(P, S.geo + gb * NB * GEO, s + 3, i0, j0, k0, kmax);
     }
     if (failed) {
         // the other stage may still have a copy in flight: wait for it (bounded) before exit

@@ -57,6 +57,20 @@ __device__ __forceinline__ void load_3d(void *dst, const CUtensorMap *map, int x
                  : "memory");
 }
 
+// Asynchronous 4-byte global -> shared copy (cp.async); when !valid nothing is read (src may
+// be any mapped address) and dst receives zero.
+__device__ __forceinline__ void copy4_zfill(float *dst, const float *src, bool valid)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_addr(dst)), "l"(src), "r"(valid ? 4 : 0)
+                 : "memory");
+}
+
+// Completes this thread's outstanding cp.async copies (a barrier then publishes them).
+__device__ __forceinline__ void copy_wait_all()
+{
+    asm volatile("cp.async.commit_group;\n\tcp.async.wait_group 0;" ::: "memory");
+}
+
 inline PFN_cuTensorMapEncodeTiled encode_fn()
 {
     static PFN_cuTensorMapEncodeTiled fn = nullptr;
