@@ -10,7 +10,9 @@
 // in registers over all projections. In this geometry the detector column of a voxel does
 // not depend on its slice, so one projection's footprint on the tile is at most ~34 columns
 // by the tile's 32 detector rows: a producer warp projects the 4 tile corners with the voxel
-// formula (affine in x and y, so the corners bound every voxel exactly), and one TMA tile
+// formula (affine in x and y, so the corners bound every voxel exactly; the per-projection
+// sin/cos/startu are copied into shared memory with cp.async three batches ahead and the
+// corners use those copies, as the voxels do), and one TMA tile
 // load (cp.async.bulk.tensor.3d, no multicast) brings a 48 x 32 box per projection into
 // shared memory, batches of 8 projections on two stages with bounded mbarrier waits. The
 // box pitch is a compile-time constant, so the slice loop addresses its two samples with
@@ -57,19 +59,19 @@ struct Params {
 
 struct Smem {
     float *box;      // [2][NB][TZ][BW]
-    float *geo;      // [2][NB][GEO]
+    float *geo;      // [3][NB][GEO]
     int4 *meta;      // [2][NB]: x0, mode
     uint64_t *bars;  // [2]
     __device__ explicit Smem(unsigned char *base)
     {
         box = reinterpret_cast<float *>(base);
         geo = reinterpret_cast<float *>(base + 2 * NB * BOXBYTES);
-        meta = reinterpret_cast<int4 *>(geo + 2 * NB * GEO);
+        meta = reinterpret_cast<int4 *>(geo + 3 * NB * GEO);
         bars = reinterpret_cast<uint64_t *>(meta + 2 * NB);
     }
     static constexpr size_t bytes()
     {
-        return 2 * NB * static_cast<size_t>(BOXBYTES) + 2 * NB * GEO * sizeof(float) + 2 * NB * sizeof(int4) +
+        return 2 * NB * static_cast<size_t>(BOXBYTES) + 3 * NB * GEO * sizeof(float) + 2 * NB * sizeof(int4) +
                2 * sizeof(uint64_t);
     }
 };
@@ -121,86 +123,90 @@ __global__ void __launch_bounds__(THREADS, 2) k_bp_par_staged(const __grid_const
     const int xa = i0 + 1, xb = min(i0 + TX, P.nu), ya = j0 + 1, yb = min(j0 + TY, P.nu);
     const int nbatch = (P.nproj + NB - 1) / NB;
 
-    // batch s into stage st: warp 0 = footprints + TMA (4 corner lanes per projection), all
-    // threads stage the per-projection geometry
-    auto produce = [&](int s, int st) {
-        if (warp == 0) {
-            const int b = lane >> 2, corner = lane & 3;
-            const int i = s * NB + b;
-            int nmin = 0, nmax = 0;
-            bool ok = i < P.nproj;
-            if (ok) {
-                const float u = posu(__ldg(P.sinv + i), __ldg(P.cosv + i), __ldg(P.startu + i),
-                                     static_cast<float>((corner & 1) ? xb : xa), static_cast<float>((corner & 2) ? yb : ya));
-                ok = fabsf(u) < 1.0e9f;
-                nmin = nmax = ok ? __float2int_rz(u) : 0;
-            }
-#pragma unroll
-            for (int o = 1; o < 4; o <<= 1) {
-                nmin = min(nmin, __shfl_xor_sync(0xffffffffu, nmin, o));
-                nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
-                ok = __shfl_xor_sync(0xffffffffu, static_cast<int>(ok), o) && ok;
-            }
-            // 0: global fallback, 1: staged, 2: no voxel of the tile has n in [0, nu-2]
-            int mode = 0, x0 = 0;
-            if (i < P.nproj && ok) {
-                if (nmax < 0 || nmin > P.nu - 2) {
-                    mode = 2;
-                } else {
-                    x0 = nmin >= 0 ? (nmin & ~3) : -(((-nmin) + 3) & ~3);
-                    if (nmax + 1 < x0 + BW) mode = 1;
-                }
-            }
-            const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
-            if (lane == 0) tma::mbar_expect_tx(&S.bars[st], static_cast<uint32_t>(__popc(staged)) * BOXBYTES);
-            __syncwarp();
-            if (corner == 0 && i < P.nproj) {
-                S.meta[st * NB + b] = make_int4(x0, mode, 0, 0);
-                if (mode == 1) {
-                    const int slab = P.index ? __ldg(P.index + i) : i;
-                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                    tma::load_3d(S.box + (st * NB + b) * (BW * TZ), &tmap, x0, z0, slab, &S.bars[st]);
-                }
-            }
-        }
+    // Geometry of batch s into geometry buffer gb (cp.async by all threads, three batches
+    // ahead; the weight only with HASW, the slab only with an index list).
+    auto stage_geometry = [&](int s, int gb) {
         for (int idx = threadIdx.x; idx < NB * GEO; idx += THREADS) {
             const int b = idx / GEO, e = idx % GEO, i = s * NB + b;
-            float v = 0.0f;
-            if (i < P.nproj) {
-                if (e == 0) v = P.sinv[i];
-                else if (e == 1) v = P.cosv[i];
-                else if (e == 2) v = P.startu[i];
-                else if (e == 3) v = HASW ? P.weight[i] : 1.0f;
-                else if (e == 4) v = __int_as_float(P.index ? P.index[i] : i);
+            const float *src = e == 0 ? P.sinv : e == 1 ? P.cosv : e == 2 ? P.startu : e == 3 ? P.weight
+                                                                                              : reinterpret_cast<const float *>(P.index);
+            const bool ok = i < P.nproj && (e < 3 || (e == 3 && HASW) || (e == 4 && P.index));
+            tma::copy4_zfill(S.geo + gb * NB * GEO + idx, ok ? src + i : P.sinv, ok);
+        }
+    };
+    // Batch s (geometry in buffer gb) into stage st: warp 0 forms the footprints from the
+    // staged geometry (4 corner lanes per projection) and issues the TMA copies.
+    auto issue_batch = [&](int s, int st, int gb) {
+        if (warp != 0) return;
+        const int b = lane >> 2, corner = lane & 3;
+        const int i = s * NB + b;
+        const float *g = S.geo + (gb * NB + b) * GEO;
+        int nmin = 0, nmax = 0;
+        bool ok = i < P.nproj;
+        if (ok) {
+            const float u = posu(g[0], g[1], g[2], static_cast<float>((corner & 1) ? xb : xa),
+                                 static_cast<float>((corner & 2) ? yb : ya));
+            ok = fabsf(u) < 1.0e9f;
+            nmin = nmax = ok ? __float2int_rz(u) : 0;
+        }
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            nmin = min(nmin, __shfl_xor_sync(0xffffffffu, nmin, o));
+            nmax = max(nmax, __shfl_xor_sync(0xffffffffu, nmax, o));
+            ok = __shfl_xor_sync(0xffffffffu, static_cast<int>(ok), o) && ok;
+        }
+        // 0: global fallback, 1: staged, 2: no voxel of the tile has n in [0, nu-2]
+        int mode = 0, x0 = 0;
+        if (i < P.nproj && ok) {
+            if (nmax < 0 || nmin > P.nu - 2) {
+                mode = 2;
+            } else {
+                x0 = nmin >= 0 ? (nmin & ~3) : -(((-nmin) + 3) & ~3);
+                if (nmax + 1 < x0 + BW) mode = 1;
             }
-            S.geo[st * NB * GEO + idx] = v;
+        }
+        const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
+        if (lane == 0) tma::mbar_expect_tx(&S.bars[st], static_cast<uint32_t>(__popc(staged)) * BOXBYTES);
+        __syncwarp();
+        if (corner == 0 && i < P.nproj) {
+            S.meta[st * NB + b] = make_int4(x0, mode, 0, 0);
+            if (mode == 1) {
+                const int slab = P.index ? __float_as_int(g[4]) : i;
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                tma::load_3d(S.box + (st * NB + b) * (BW * TZ), &tmap, x0, z0, slab, &S.bars[st]);
+            }
         }
     };
 
-    produce(0, 0);
-    if (nbatch > 1) produce(1, 1);
+    for (int s = 0; s < 3 && s < nbatch; ++s) stage_geometry(s, s);
+    tma::copy_wait_all();
+    __syncthreads();
+    for (int s = 0; s < 2 && s < nbatch; ++s) issue_batch(s, s, s);
     __syncthreads();
 
     uint32_t phase0 = 0, phase1 = 0;
     bool failed = false;
     const float fx = static_cast<float>(x1), fy = static_cast<float>(y1);
     const int um2 = P.nu - 2;
-    for (int s = 0; s < nbatch; ++s) {
-        const int st = s & 1;
-        if (!tma::mbar_wait(&S.bars[st], st ? phase1 : phase0)) {
+    for (int s = 0, gb = 0; s < nbatch; ++s, gb = gb == 2 ? 0 : gb + 1) {
+        const int st = s & 1; // stage buffer; geometry buffer gb = s % 3
+        // a wait that timed out skips the batch in its whole warp; the block then leaves the
+        // loop together at the barrier below
+        const bool got = __all_sync(0xffffffffu, tma::mbar_wait(&S.bars[st], st ? phase1 : phase0));
+        if (got) {
+            if (st) phase1 ^= 1; else phase0 ^= 1;
+        } else {
             failed = true;
-            atomicExch(&g_bp_error, 1);
-            break;
+            if (lane == 0) atomicExch(&g_bp_error, 1);
         }
-        if (st) phase1 ^= 1; else phase0 ^= 1;
-        if (inside) {
+        if (got && inside) {
 #pragma unroll 1
             for (int b = 0; b < NB; ++b) {
                 const int i = s * NB + b;
                 if (i >= P.nproj) break;
                 const int4 m = S.meta[st * NB + b];
                 if (m.y == 2) continue;
-                const float *g = S.geo + (st * NB + b) * GEO;
+                const float *g = S.geo + (gb * NB + b) * GEO;
                 const float u = posu(g[0], g[1], g[2], fx, fy);
                 const int n = __float2int_rz(u);
                 if (n < 0 || um2 < n) continue;
@@ -222,7 +228,8 @@ __global__ void __launch_bounds__(THREADS, 2) k_bp_par_staged(const __grid_const
                         acc[q] = __fadd_rn(acc[q], __fadd_rn(prod.x, prod.y));
                     }
                 } else {
-                    const float *img = P.proj + (static_cast<size_t>(__float_as_int(g[4])) * P.nv + z0) * P.nu + n;
+                    const int slab = P.index ? __float_as_int(g[4]) : i;
+                    const float *img = P.proj + (static_cast<size_t>(slab) * P.nv + z0) * P.nu + n;
 #pragma unroll
                     for (int q = 0; q < TZ; ++q) {
                         if (q >= zmax) break;
@@ -236,8 +243,11 @@ __global__ void __launch_bounds__(THREADS, 2) k_bp_par_staged(const __grid_const
                 }
             }
         }
-        __syncthreads();
-        if (s + 2 < nbatch) produce(s + 2, st);
+        // batch s+2's geometry complete and published; stage st and geometry buffer gb free
+        tma::copy_wait_all();
+        if (__syncthreads_or(failed)) break;
+        if (s + 2 < nbatch) issue_batch(s + 2, st, gb == 0 ? 2 : gb - 1);
+        if (s + 3 < nbatch) stage_geometry(s + 3, gb);
     }
     if (failed) {
         tma::mbar_wait(&S.bars[0], phase0);
