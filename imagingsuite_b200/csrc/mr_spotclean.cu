@@ -19,16 +19,20 @@
 // (every other value stays the marker's interior minimum), so one thread per image replays
 // the scan over that band in raster order, and the exact reconstruction follows.
 //
-// The reconstruction kernel runs one CTA per image and alternates downward and upward row
-// sweeps until a full round changes nothing (bounded; the bound sets the device error
-// word). A sweep combines each row with the neighbouring row just finished (vertical and,
-// for 8-connectivity, diagonal neighbours), then propagates along the row in both
-// directions with a CTA-wide scan: the row update v[c] = min(g[c], max(v[c], v[c-1]))
+// Each reconstruction runs in two kernels, one CTA per image in both. The sweep kernel
+// alternates downward and upward row sweeps for a few rounds (it stops early when a round
+// changes nothing). A sweep combines each row with the neighbouring row just finished
+// (vertical and, for 8-connectivity, diagonal neighbours), then propagates along the row in
+// both directions with a CTA-wide scan: the row update v[c] = min(g[c], max(v[c], v[c-1]))
 // (dilation) or max(g[c], min(v[c], v[c-1])) (erosion) is a clamp x -> min(hi, max(lo, x)),
-// and clamps compose into clamps, so the sequential recurrence is a parallel prefix.
+// and clamps compose into clamps, so the sequential recurrence is a parallel prefix. On noisy
+// projections the sweeps alone need 20-30 rounds (every change of vertical direction along a
+// propagation path costs a round), while after a few rounds only a thin set of pixels still
+// changes; the completion kernel finishes from there with a worklist (k_complete).
 #include "mr_common.cuh"
 
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 namespace mr {
@@ -48,7 +52,7 @@ int msc_device_status_take()
 namespace msc {
 
 constexpr int kMargin = 5;
-constexpr int kMaxRounds = 4096;
+constexpr int kSweepRounds = 4; // dense sweep rounds before the worklist completion
 constexpr int kMaxEdge = 63;
 
 struct Clamp {
@@ -271,7 +275,7 @@ __device__ __forceinline__ void clamp_then(float al, float ah, float &bl, float 
 // the shared row buffers fall in distinct banks.
 template <bool DILATE, int RW, int C>
 __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict__ pad, float sign, int pw, int ph,
-                                                         int conn8, float *__restrict__ vol)
+                                                         int conn8, int rounds, float *__restrict__ vol)
 {
     constexpr int T = 32 * RW, L = T * C + 2 + 1; // row buffer: a neutral element before and after
     extern __shared__ float rows_sm[];
@@ -333,8 +337,7 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
         return before_l; // the prefix applied to the neutral input
     };
 
-    int round = 0;
-    for (; round < kMaxRounds; ++round) {
+    for (int round = 0; round < rounds; ++round) {
         bool changed = false;
         for (int pass = 0; pass < 2; ++pass) {
             int gi = 0, vi = 0;
@@ -416,7 +419,6 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
         image_sync<RW>();
         if (!any) break;
     }
-    if (round == kMaxRounds && t == 0) atomicExch(&g_msc_error, 2);
 }
 
 template <bool DILATE, int RW, int C>
@@ -426,22 +428,169 @@ static mr_status launch_rec(int nimg, const float *pad, float sign, int pw, int 
     const size_t smem = 5 * static_cast<size_t>(32 * RW * C + 3) * sizeof(float);
     MR_CUDA_TRY(cudaFuncSetAttribute(k_reconstruct<DILATE, RW, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-    k_reconstruct<DILATE, RW, C><<<nimg, 32 * RW, smem, s>>>(pad, sign, pw, ph, conn8, vol);
+    k_reconstruct<DILATE, RW, C><<<nimg, 32 * RW, smem, s>>>(pad, sign, pw, ph, conn8, kSweepRounds, vol);
     return check_launch("k_reconstruct");
 }
 
+// ---- completion: worklist relaxation
+//
+// After the sweeps the remaining changes are sparse (thin, winding paths through the noise),
+// so each image's CTA finishes the reconstruction with a worklist. Values are handled as
+// order-preserving integer keys so that the relaxation is one atomicMin (erosion:
+// v[q] = min(v[q], max(g[q], v[p]))) or atomicMax (dilation: v[q] = max(v[q], min(g[q], v[p])))
+// per neighbour. A pixel whose value moved is put on the next iteration's list once (a stamp
+// per pixel and iteration); it then relaxes its neighbours with its current value. When a
+// list overflows, the next iteration relaxes every pixel from its neighbours instead (the
+// first iteration always does). The reconstruction ends when an iteration moves nothing:
+// every pixel then satisfies the fixpoint equations with all its neighbours, and the fixpoint
+// is unique, so the result equals the reference's whatever the order of the updates.
+// Values are read through L2 (ld.cg), where the atomics resolve.
+
+constexpr int kFrontThreads = 256;
+constexpr int kMaxIterations = 1 << 22;
+
+__device__ __forceinline__ int fkey(float f)
+{
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+
+__device__ __forceinline__ float funkey(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
+
+template <bool DILATE, bool CONN8>
+__global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restrict__ pad, float sign, int pw, int ph,
+                                                            float *__restrict__ vol, int *__restrict__ stamps,
+                                                            int *__restrict__ lists, int cap)
+{
+    const int t = threadIdx.x;
+    const size_t n = static_cast<size_t>(pw) * ph;
+    const float *g = pad + blockIdx.x * n;
+    int *v = reinterpret_cast<int *>(vol + blockIdx.x * n);
+    int *stamp = stamps + blockIdx.x * n;
+    int *cur = lists + blockIdx.x * 2 * static_cast<size_t>(cap), *next = cur + cap;
+    __shared__ int count[3];
+    for (size_t i = t; i < n; i += kFrontThreads) {
+        __stcg(v + i, fkey(__int_as_float(__ldcg(v + i))));
+        stamp[i] = 0;
+    }
+    if (t < 3) count[t] = 0;
+    __syncthreads();
+
+    // candidate for q from a neighbour value kp; moves v[q] when it improves on it
+    auto relax = [&](int q, int kp, int it) {
+        const int kg = fkey(sign * __ldg(g + q));
+        const int c = DILATE ? min(kg, kp) : max(kg, kp);
+        if (DILATE ? c > __ldcg(v + q) : c < __ldcg(v + q)) {
+            const int old = DILATE ? atomicMax(v + q, c) : atomicMin(v + q, c);
+            if ((DILATE ? c > old : c < old) && atomicExch(stamp + q, it + 1) != it + 1) {
+                const int pos = atomicAdd(&count[it % 3], 1);
+                if (pos < cap) next[pos] = q;
+            }
+        }
+    };
+    const int nx[8] = {-1, 1, 0, 0, -1, 1, -1, 1}, ny[8] = {0, 0, -1, 1, -1, -1, 1, 1};
+    constexpr int NN = CONN8 ? 8 : 4;
+
+    bool dense = true;
+    int nf = 0, it = 0;
+    for (; it < kMaxIterations; ++it) {
+        if (dense) {
+            // every pixel from the extreme of its neighbours
+            for (size_t i = t; i < n; i += kFrontThreads) {
+                const int y = static_cast<int>(i / pw), x = static_cast<int>(i % pw);
+                int kn = DILATE ? INT_MIN : INT_MAX;
+#pragma unroll
+                for (int k = 0; k < NN; ++k) {
+                    const int qx = x + nx[k], qy = y + ny[k];
+                    if (qx < 0 || qx >= pw || qy < 0 || qy >= ph) continue;
+                    const int kq = __ldcg(v + static_cast<size_t>(qy) * pw + qx);
+                    kn = DILATE ? max(kn, kq) : min(kn, kq);
+                }
+                relax(static_cast<int>(i), kn, it);
+            }
+        } else {
+            // all neighbour loads of an entry are issued before its first compare (one round
+            // trip to L2 per entry); U > 1 entries per thread at a time measured slower (registers)
+            constexpr int U = 1;
+            for (int e0 = t; e0 < nf; e0 += U * kFrontThreads) {
+                int p[U], kp[U], kg[U][NN], kv[U][NN];
+                unsigned ok[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int e = e0 + u * kFrontThreads;
+                    p[u] = e < nf ? cur[e] : -1;
+                    const int y = p[u] / pw, x = p[u] % pw;
+                    ok[u] = 0;
+#pragma unroll
+                    for (int k = 0; k < NN; ++k) {
+                        const int qx = x + nx[k], qy = y + ny[k];
+                        if (p[u] >= 0 && qx >= 0 && qx < pw && qy >= 0 && qy < ph) ok[u] |= 1u << k;
+                    }
+                    kp[u] = p[u] >= 0 ? __ldcg(v + p[u]) : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int k = 0; k < NN; ++k) {
+                        const int q = p[u] + ny[k] * pw + nx[k];
+                        kg[u][k] = (ok[u] >> k) & 1 ? fkey(sign * __ldg(g + q)) : 0;
+                        kv[u][k] = (ok[u] >> k) & 1 ? __ldcg(v + q) : 0;
+                    }
+#pragma unroll
+                for (int u = 0; u < U; ++u)
+#pragma unroll
+                    for (int k = 0; k < NN; ++k) {
+                        if (!((ok[u] >> k) & 1)) continue;
+                        const int q = p[u] + ny[k] * pw + nx[k];
+                        const int c = DILATE ? min(kg[u][k], kp[u]) : max(kg[u][k], kp[u]);
+                        if (DILATE ? c > kv[u][k] : c < kv[u][k]) {
+                            const int old = DILATE ? atomicMax(v + q, c) : atomicMin(v + q, c);
+                            if ((DILATE ? c > old : c < old) && atomicExch(stamp + q, it + 1) != it + 1) {
+                                const int pos = atomicAdd(&count[it % 3], 1);
+                                if (pos < cap) next[pos] = q;
+                            }
+                        }
+                    }
+            }
+        }
+        __syncthreads();
+        // count[it % 3] is final; count[(it + 2) % 3] was read by everyone before this barrier
+        // and is next written in iteration it + 2
+        const int pushed = count[it % 3];
+        if (t == 0) count[(it + 2) % 3] = 0;
+        int *tmp = cur;
+        cur = next;
+        next = tmp;
+        if (pushed == 0) break;
+        dense = pushed > cap;
+        nf = min(pushed, cap);
+    }
+    if (it == kMaxIterations && t == 0) atomicExch(&g_msc_error, 2);
+    __syncthreads();
+    for (size_t i = t; i < n; i += kFrontThreads) __stcg(v + i, __float_as_int(funkey(__ldcg(v + i))));
+}
+
+// Worklist capacity per image (entries); a larger frontier falls back to a dense iteration.
+inline int complete_cap(size_t n) { return static_cast<int>(std::min<size_t>(n, std::max<size_t>(256, n / 16))); }
+
 template <bool DILATE>
 static mr_status launch_reconstruct(int nimg, const float *pad, float sign, int pw, int ph, int conn8, float *vol,
-                                    cudaStream_t s)
+                                    int *stamps, int *lists, cudaStream_t s)
 {
     constexpr int RW = 4;
     const int per = (pw + 32 * RW - 1) / (32 * RW);
-    if (per <= 3) return launch_rec<DILATE, RW, 3>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    if (per <= 5) return launch_rec<DILATE, RW, 5>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    if (per <= 9) return launch_rec<DILATE, RW, 9>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    if (per <= 17) return launch_rec<DILATE, RW, 17>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    if (per <= 33) return launch_rec<DILATE, RW, 33>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 32 * RW * 33 - 2 * kMargin);
+    mr_status st;
+    if (per <= 3) st = launch_rec<DILATE, RW, 3>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    else if (per <= 5) st = launch_rec<DILATE, RW, 5>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    else if (per <= 9) st = launch_rec<DILATE, RW, 9>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    else if (per <= 17) st = launch_rec<DILATE, RW, 17>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    else if (per <= 33) st = launch_rec<DILATE, RW, 33>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    else return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 32 * RW * 33 - 2 * kMargin);
+    if (st != MR_OK) return st;
+    const int cap = complete_cap(static_cast<size_t>(pw) * ph);
+    if (conn8) k_complete<DILATE, true><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, stamps, lists, cap);
+    else k_complete<DILATE, false><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, stamps, lists, cap);
+    return check_launch("k_complete");
 }
 
 // Replacement / blend and unpadding (MorphSpotClean::ProcessReplace :108-175,
@@ -504,7 +653,8 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     cudaStream_t s = as_stream(stream);
     // images per batch: three padded buffers each; up to a quarter of the free device memory,
     // so that a block of projections is cleaned concurrently (one warp per image)
-    const size_t per_img = 3 * n * sizeof(float);
+    const size_t cap = static_cast<size_t>(complete_cap(n));
+    const size_t per_img = 3 * n * sizeof(float) + (n + 2 * cap) * sizeof(int);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = size_t(1) << 30;
     const size_t budget = std::max<size_t>(size_t(1) << 30, free_b / 4);
@@ -514,6 +664,7 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     MR_CUDA_TRY(cudaMallocAsync(&scratch, batch * per_img + 4 * batch * sizeof(float), s));
     float *P = scratch, *H = P + batch * n, *K = H + batch * n, *stats = K + batch * n;
     float *fmax = stats, *mn = stats + batch, *mx = stats + 2 * batch;
+    int *stamps = reinterpret_cast<int *>(stats + 4 * batch), *lists = stamps + batch * n;
     mr_status st = MR_OK;
     for (size_t b0 = 0; b0 < nproj && st == MR_OK; b0 += batch) {
         const int nb = static_cast<int>(std::min(batch, nproj - b0));
@@ -525,16 +676,16 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
         k_minmax<<<nb, 1024, 0, s>>>(P, n, mn, mx);
         if (detect == 0 || detect == 2) { // FillHole: erosion from a max marker
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
-            if ((st = launch_reconstruct<false>(nb, P, 1.0f, pw, ph, conn8, H, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<false>(nb, P, 1.0f, pw, ph, conn8, H, stamps, lists, s)) != MR_OK) break;
         }
         if (detect == 1) { // FillPeaks: forward-scan band replay, then the exact dilation
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, 1.0f, K);
             k_peaks_forward_band<<<div_up(nb, 32), 32, 0, s>>>(P, pw, ph, nb, conn8, mn, K);
-            if ((st = launch_reconstruct<true>(nb, P, 1.0f, pw, ph, conn8, K, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<true>(nb, P, 1.0f, pw, ph, conn8, K, stamps, lists, s)) != MR_OK) break;
         }
         if (detect == 2) { // -FillHole(-padded): erosion of the negated image from marker max(-P) = -min(P)
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, -1.0f, K);
-            if ((st = launch_reconstruct<false>(nb, P, -1.0f, pw, ph, conn8, K, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<false>(nb, P, -1.0f, pw, ph, conn8, K, stamps, lists, s)) != MR_OK) break;
         }
         if ((st = check_launch("morphspotclean reconstruction")) != MR_OK) break;
         k_replace<<<dim3(gx, nb), 256, 0, s>>>(P, detect != 1 ? H : nullptr, detect != 0 ? K : nullptr, w, h, detect,

@@ -80,6 +80,23 @@ def test_wide_and_tall_images(cuda):
     assert np.array_equal(got, O.morphspotclean(tall, "peaks", False, (0.5, 0.5), (0.0, 0.0)))
 
 
+@pytest.mark.parametrize("conn8", [True, False])
+def test_noisy_profile_worklist_completion(cuda, conn8):
+    """A smooth attenuation profile with noise and spots: the row sweeps alone would need many
+    rounds (paths wind up and down through the noise), so most of the reconstruction is done by
+    the worklist completion, whose list overflows into dense passes at first."""
+    rng = np.random.default_rng(84)
+    h, w = 96, 700
+    yy, xx = np.mgrid[:h, :w]
+    base = 1.5 * np.exp(-((xx - 350) / 200.0) ** 2 - ((yy - 48) / 60.0) ** 2)
+    img = (base + rng.normal(0, 0.03, (2, h, w))).astype(np.float32)
+    img[0, 30, 100] += 1.0
+    img[1, 60, 500] -= 1.0
+    for d in ("holes", "peaks", "both"):
+        got = gpu_clean(img, d, conn8, (0.1, 0.1), (0.0, 0.0), edge=5)
+        assert np.array_equal(got, O.morphspotclean(img, d, conn8, (0.1, 0.1), (0.0, 0.0), edge=5)), d
+
+
 def test_clamp_and_infnan(cuda):
     rng = np.random.default_rng(82)
     img = (rng.standard_normal((2, 12, 20)) * 5).astype(np.float32)
