@@ -43,7 +43,8 @@ int bp_device_status_take()
 
 namespace bp2 {
 
-constexpr int TX = 32, TY = 8, TZ = 32, THREADS = TX * TY, NB = 8, BW = 48;
+constexpr int TX = 32, TY = 8, TZ = 32, THREADS = TX * TY, NB = 8, G = 4, BW = 48;
+constexpr int CTAS_PER_SM = 2;
 constexpr int BOXBYTES = BW * TZ * 4;
 constexpr int GEO = 8; // sin, cos, startu, weight, slab (as int bits), pad
 
@@ -82,8 +83,27 @@ __device__ __forceinline__ float posu(float sn, float cs, float su, float fx, fl
     return __fsub_rn(__fadd_rn(su, __fmul_rn(cs, fy)), __fmul_rn(sn, fx));
 }
 
+// Slices of one voxel column for one staged projection: p points at the sample pair of slice 0
+// (row pitch BW). FULL: all TZ slices exist.
+template <bool HASW, bool FULL>
+__device__ __forceinline__ void staged_column(float (&acc)[TZ], const float *p, float wa, float wb, float w, int zmax)
+{
+    const float2 wab = make_float2(wa, wb);
+#pragma unroll
+    for (int q = 0; q < TZ; ++q) {
+        if (!FULL && q >= zmax) break;
+        float pa = p[q * BW], pb = p[q * BW + 1];
+        if (HASW) {
+            pa = __fmul_rn(pa, w);
+            pb = __fmul_rn(pb, w);
+        }
+        const float2 prod = __fmul2_rn(make_float2(pa, pb), wab);
+        acc[q] = __fadd_rn(acc[q], __fadd_rn(prod.x, prod.y));
+    }
+}
+
 template <bool HASW>
-__global__ void __launch_bounds__(THREADS, 2) k_bp_par_staged(const __grid_constant__ CUtensorMap tmap, const Params P)
+__global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __grid_constant__ CUtensorMap tmap, const Params P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
     Smem S(smem);
@@ -200,45 +220,71 @@ __global__ void __launch_bounds__(THREADS, 2) k_bp_par_staged(const __grid_const
             if (lane == 0) atomicExch(&g_bp_error, 1);
         }
         if (got && inside) {
+            // projections in groups of G: the set-up of a group (detector position, weights,
+            // sample offset) is formed first so its latency overlaps, then the group's slice
+            // loops run in projection order (the reference's summation order)
 #pragma unroll 1
-            for (int b = 0; b < NB; ++b) {
-                const int i = s * NB + b;
-                if (i >= P.nproj) break;
-                const int4 m = S.meta[st * NB + b];
-                if (m.y == 2) continue;
-                const float *g = S.geo + (gb * NB + b) * GEO;
-                const float u = posu(g[0], g[1], g[2], fx, fy);
-                const int n = __float2int_rz(u);
-                if (n < 0 || um2 < n) continue;
-                const float wb = fabsf(__fsub_rn(u, static_cast<float>(n)));
-                const float wa = __fsub_rn(1.0f, wb);
-                const float2 wab = make_float2(wa, wb);
-                const float w = g[3];
-                if (m.y == 1) {
-                    const float *p = S.box + (st * NB + b) * (BW * TZ) + (n - m.x);
+            for (int b0 = 0; b0 < NB; b0 += G) {
+                int q_mode[G], q_n[G]; // 0: nothing to add, 1: staged, 2: guarded global loads
+                uint32_t q_off[G];
+                float q_wa[G], q_wb[G];
 #pragma unroll
-                    for (int q = 0; q < TZ; ++q) {
-                        if (q >= zmax) break;
-                        float pa = p[q * BW], pb = p[q * BW + 1];
-                        if (HASW) {
-                            pa = __fmul_rn(pa, w);
-                            pb = __fmul_rn(pb, w);
+                for (int e = 0; e < G; ++e) {
+                    const int b = b0 + e, i = s * NB + b;
+                    q_mode[e] = 0;
+                    q_n[e] = 0;
+                    q_off[e] = 0;
+                    q_wa[e] = q_wb[e] = 0.0f;
+                    if (i < P.nproj) {
+                        const int4 m = S.meta[st * NB + b];
+                        const float *g = S.geo + (gb * NB + b) * GEO;
+                        const float u = posu(g[0], g[1], g[2], fx, fy);
+                        const int n = __float2int_rz(u);
+                        if (m.y != 2 && n >= 0 && n <= um2) {
+                            q_mode[e] = m.y == 1 ? 1 : 2;
+                            q_n[e] = n;
+                            q_off[e] = static_cast<uint32_t>((st * NB + b) * (BW * TZ) + (n - m.x));
+                            q_wb[e] = fabsf(__fsub_rn(u, static_cast<float>(n)));
+                            q_wa[e] = __fsub_rn(1.0f, q_wb[e]);
                         }
-                        const float2 prod = __fmul2_rn(make_float2(pa, pb), wab);
-                        acc[q] = __fadd_rn(acc[q], __fadd_rn(prod.x, prod.y));
                     }
-                } else {
-                    const int slab = P.index ? __float_as_int(g[4]) : i;
-                    const float *img = P.proj + (static_cast<size_t>(slab) * P.nv + z0) * P.nu + n;
+                }
+                // a footprint that did not fit its box (rare; uniform over the CTA) sends the
+                // whole group through the in-order path with guarded global loads
+                bool fallback = false;
 #pragma unroll
-                    for (int q = 0; q < TZ; ++q) {
-                        if (q >= zmax) break;
-                        float pa = __ldg(img + static_cast<size_t>(q) * P.nu), pb = __ldg(img + static_cast<size_t>(q) * P.nu + 1);
-                        if (HASW) {
-                            pa = __fmul_rn(pa, w);
-                            pb = __fmul_rn(pb, w);
+                for (int e = 0; e < G; ++e)
+                    fallback |= s * NB + b0 + e < P.nproj && S.meta[st * NB + b0 + e].y == 0;
+                if (!fallback) {
+#pragma unroll
+                    for (int e = 0; e < G; ++e) {
+                        if (q_mode[e] != 1) continue;
+                        const float w = HASW ? S.geo[(gb * NB + b0 + e) * GEO + 3] : 1.0f;
+                        if (zmax == TZ) staged_column<HASW, true>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
+                        else staged_column<HASW, false>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
+                    }
+                    continue;
+                }
+#pragma unroll 1
+                for (int e = 0; e < G; ++e) {
+                    const float w = HASW ? S.geo[(gb * NB + b0 + e) * GEO + 3] : 1.0f;
+                    if (q_mode[e] == 1) {
+                        staged_column<HASW, false>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
+                    } else if (q_mode[e] == 2) {
+                        const int i = s * NB + b0 + e;
+                        const int slab = P.index ? __float_as_int(S.geo[(gb * NB + b0 + e) * GEO + 4]) : i;
+                        const float *img = P.proj + (static_cast<size_t>(slab) * P.nv + z0) * P.nu + q_n[e];
+                        const float wa = q_wa[e], wb = q_wb[e];
+#pragma unroll
+                        for (int q = 0; q < TZ; ++q) {
+                            if (q >= zmax) break;
+                            float pa = __ldg(img + static_cast<size_t>(q) * P.nu), pb = __ldg(img + static_cast<size_t>(q) * P.nu + 1);
+                            if (HASW) {
+                                pa = __fmul_rn(pa, w);
+                                pb = __fmul_rn(pb, w);
+                            }
+                            acc[q] = __fadd_rn(acc[q], __fadd_rn(__fmul_rn(pa, wa), __fmul_rn(pb, wb)));
                         }
-                        acc[q] = __fadd_rn(acc[q], __fadd_rn(__fmul_rn(pa, wa), __fmul_rn(pb, wb)));
                     }
                 }
             }

@@ -469,27 +469,45 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                         }
                     }
                 }
+                // a footprint that did not fit its box (rare; uniform over the CTA) sends the
+                // whole group through the in-order path below, so that every voxel still sums
+                // its projections in the reference's order
+                bool fallback = false;
 #pragma unroll
-                for (int e = 0; e < G; ++e) {
-                    if (!q_on[e]) continue;
-                    if constexpr (EXACT) {
-                        const float *a1 = S.a1 + (warp * NB + b0 + e) * TK;
-                        if (kmax == TK)
-                            exact_column<true>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
-                        else
-                            exact_column<false>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
-                    } else {
-                        const unsigned short wt = static_cast<unsigned short>(__float_as_uint(q_c[e]));
-                        if (kmax == TK)
-                            fast_column_staged<DT, true>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e], wt, kmax);
-                        else
-                            fast_column_staged<DT, false>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e], wt, kmax);
+                for (int e = 0; e < G; ++e) fallback |= s * NB + b0 + e < P.nproj && S.meta[st * NB + b0 + e].z == 0;
+                if (!fallback) {
+#pragma unroll
+                    for (int e = 0; e < G; ++e) {
+                        if (!q_on[e]) continue;
+                        if constexpr (EXACT) {
+                            const float *a1 = S.a1 + (warp * NB + b0 + e) * TK;
+                            if (kmax == TK)
+                                exact_column<true>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
+                            else
+                                exact_column<false>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
+                        } else {
+                            const unsigned short wt = static_cast<unsigned short>(__float_as_uint(q_c[e]));
+                            if (kmax == TK)
+                                fast_column_staged<DT, true>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e], wt, kmax);
+                            else
+                                fast_column_staged<DT, false>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e], wt, kmax);
+                        }
                     }
+                    continue;
                 }
-                // footprints that did not fit the box: guarded global loads (rare)
+                // in order: staged footprints from shared memory, the others by guarded global loads
 #pragma unroll 1
                 for (int e = 0; e < G; ++e) {
                     const int b = b0 + e, p = s * NB + b;
+                    if (q_on[e]) {
+                        if constexpr (EXACT)
+                            exact_column<false>(acc, smem, q_base[e], rowbytes, S.a1 + (warp * NB + b) * TK, q_c[e], q_a[e],
+                                                q_b[e], kmax);
+                        else
+                            fast_column_staged<DT, false>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e],
+                                                          static_cast<unsigned short>(__float_as_uint(q_c[e])), kmax);
+                        continue;
+                    }
                     if (p >= P.nproj || S.meta[st * NB + b].z != 0) continue;
                     const float *g = geo + b * GEO;
                     if constexpr (EXACT) {

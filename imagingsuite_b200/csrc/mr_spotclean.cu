@@ -110,28 +110,37 @@ __global__ void k_pad(const float *__restrict__ img, int w, int h, const float *
     }
 }
 
-// In-place sliding median of `edge` samples along padded rows 0 and ph-1 (:283-299).
-__global__ void k_edge_median(float *__restrict__ pad, int pw, int ph, int nimg, int edge)
+// In-place sliding median of `edge` samples along padded rows 0 and ph-1 (:283-299). One warp
+// per edge row: the row is staged in shared memory, lane 0 runs the sequential in-place loop
+// there (each median sees the medians already written to its left, as in the reference), and
+// the warp writes the row back.
+__global__ void k_edge_median(float *__restrict__ pad, int pw, int ph, int edge)
 {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 2 * nimg) return;
-    float *row = pad + static_cast<size_t>(t >> 1) * pw * ph + ((t & 1) ? static_cast<size_t>(ph - 1) * pw : 0);
-    const int l2 = edge / 2;
-    float buf[kMaxEdge];
-    for (int i = l2; i < pw - l2; ++i) {
-        for (int q = 0; q < edge; ++q) buf[q] = row[i - l2 + q];
-        for (int a = 1; a < edge; ++a) { // insertion sort
-            float key = buf[a];
-            int c = a - 1;
-            while (c >= 0 && buf[c] > key) {
-                buf[c + 1] = buf[c];
-                --c;
+    extern __shared__ float srow[];
+    const int lane = threadIdx.x;
+    float *row = pad + static_cast<size_t>(blockIdx.x >> 1) * pw * ph + ((blockIdx.x & 1) ? static_cast<size_t>(ph - 1) * pw : 0);
+    for (int i = lane; i < pw; i += 32) srow[i] = row[i];
+    __syncwarp();
+    if (lane == 0) {
+        const int l2 = edge / 2;
+        float buf[kMaxEdge];
+        for (int i = l2; i < pw - l2; ++i) {
+            for (int q = 0; q < edge; ++q) buf[q] = srow[i - l2 + q];
+            for (int a = 1; a < edge; ++a) { // insertion sort
+                float key = buf[a];
+                int c = a - 1;
+                while (c >= 0 && buf[c] > key) {
+                    buf[c + 1] = buf[c];
+                    --c;
+                }
+                buf[c + 1] = key;
             }
-            buf[c + 1] = key;
+            srow[i] = (edge & 1) ? buf[edge / 2]
+                                 : static_cast<float>(0.5 * (static_cast<double>(buf[edge / 2 - 1]) + buf[edge / 2]));
         }
-        row[i] = (edge & 1) ? buf[edge / 2]
-                            : static_cast<float>(0.5 * (static_cast<double>(buf[edge / 2 - 1]) + buf[edge / 2]));
     }
+    __syncwarp();
+    for (int i = lane; i < pw; i += 32) row[i] = srow[i];
 }
 
 __global__ void k_minmax(const float *__restrict__ pad, size_t n, float *__restrict__ mn, float *__restrict__ mx)
@@ -672,7 +681,7 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
         const unsigned gx = std::min<unsigned>(div_up(n, 256), 128u);
         if (removeinfnan) k_finite_max<<<nb, 256, 0, s>>>(img, nu * nv, fmax);
         k_pad<<<dim3(gx, nb), 256, 0, s>>>(img, w, h, removeinfnan ? fmax : nullptr, clamp, minlevel, maxlevel, P);
-        k_edge_median<<<div_up(2 * nb, 64), 64, 0, s>>>(P, pw, ph, nb, edge);
+        k_edge_median<<<2 * nb, 32, pw * sizeof(float), s>>>(P, pw, ph, edge);
         k_minmax<<<nb, 1024, 0, s>>>(P, n, mn, mx);
         if (detect == 0 || detect == 2) { // FillHole: erosion from a max marker
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);

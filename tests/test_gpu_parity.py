@@ -302,6 +302,23 @@ def test_fdk_staged_box_too_small_falls_back(cuda):
     assert np.array_equal(got, O.fdk_bp(filt, ang, _ogeom(cfg)))
 
 
+@pytest.mark.parametrize("box", [(20, 44), (28, 40), (36, 36)])
+def test_fdk_staged_mixed_fallback_groups(cuda, box):
+    """Boxes that hold the footprints of some projections of a batch but not of others (the
+    footprint's width on the detector turns with the angle): the staged and the direct-load
+    projections of one group still accumulate in projection order, bit for bit."""
+    rng = np.random.default_rng(15)
+    nproj, nv, nu = 24, 40, 64
+    cfg = _fdk_cfg(nu, nv)
+    filt = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 15.0 + 2.0).astype(np.float32)
+    mod = M.FDKbp_single()
+    mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
+    mod.SetROI((0, 0, nu, nv))
+    got, _ = _fdk_bp_gpu(cuda, mod, filt, ang, True, box=box)
+    assert np.array_equal(got, O.fdk_bp(filt, ang, _ogeom(cfg)))
+
+
 @pytest.mark.parametrize("shape", [(9, 72, 96), (5, 33, 40), (7, 64, 128)])
 def test_fdk_staged_shapes(cuda, shape):
     """Partial slice tiles (nv not a multiple of 32), odd tile counts, wide detectors."""
