@@ -59,13 +59,16 @@ constexpr float kMagic = 12582912.0f; // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
 // per-projection geometry staged in shared memory (floats)
 constexpr int GEO_EXACT = TK + 3 * TI + 3 * TJ + 4; // zip1[TK], xip[TI][3], yip[TJ][3], Z0, Z2
-constexpr int GEO_FAST = 16;                        // map[12], scale, pad
+constexpr int GEO_FAST = 32;                        // FP64 map[12] (24 words), scale, pad
+// per-projection tile geometry of the fast kernel (floats, formed from the FP64 map)
+constexpr int TGEO = 16;
+enum { TG_W0, TG_M8, TG_M9, TG_AU, TG_BU, TG_AV, TG_BV, TG_M6, TG_FC, TG_FR, TG_C0, TG_R0, TG_SCALE };
 
 struct Params {
     const void *proj;
     const float *scale;
     const float *xip, *yip, *zip; // exact kernel
-    const float *maps;            // fast kernel: [nproj][12]
+    const double *maps;           // fast kernel: [nproj][12] (FP64)
     const uint32_t *mask;
     float *vol;
     int nu, nv, nproj;
@@ -114,24 +117,54 @@ __device__ __forceinline__ float from_storage(unsigned short v)
     else return __half2float(__ushort_as_half(v));
 }
 
-// Fast-path coordinates of voxel column (i, j) at slice k0 of the tile: column c, row r0 of
-// slice k0, row step dr per slice, inverse depth dw. The corner footprints and the voxels
-// use this same function.
-struct FastCol {
-    float c, r0, dr, dw;
-};
-
-__device__ __forceinline__ FastCol fast_column(const float *m, float fi, float fj, float fk0)
+// Fast-kernel coordinates. The detector column and row of the tile's origin voxel
+// (i0, j0, k0) are formed in FP64 from the FP64 map and split into an integer part and an FP32
+// fraction; the other voxels add FP32 offsets from the origin, which stay within the tile's
+// footprint (tens of pixels), so a coordinate carries an error of a few 1e-6 pixel instead of
+// the ~1e-4 of an FP32 evaluation at detector magnitudes. With the map
+// u = m0 i + m1 j + m3, v = m4 i + m5 j + m6 k + m7, w = m8 i + m9 j + m11 and
+// c = u/w + 1/2, r = v/w + 1/2 (the FP64 oracle's formulas), the offsets from the origin are
+// exactly  c - c0 = (au di + bu dj) / w,  r - r0 = (av di + bv dj + m6 dk) / w  with
+// au = m0 - (c0 - 1/2) m8, bu = m1 - (c0 - 1/2) m9, av = m4 - (r0 - 1/2) m8,
+// bv = m5 - (r0 - 1/2) m9. False when the origin is behind the source or out of range.
+__device__ __forceinline__ bool tile_geometry(const double *m, int i0, int j0, int k0, float scale, float (&t)[TGEO])
 {
-    FastCol f;
-    const float w = fmaf(m[8], fi, fmaf(m[9], fj, m[11]));
-    f.dw = __frcp_rn(w);
-    const float u = fmaf(m[0], fi, fmaf(m[1], fj, m[3]));
-    const float v = fmaf(m[4], fi, fmaf(m[5], fj, fmaf(m[6], fk0, m[7])));
-    f.c = fmaf(u, f.dw, 0.5f);
-    f.r0 = fmaf(v, f.dw, 0.5f);
-    f.dr = m[6] * f.dw;
-    return f;
+    const double fi = i0, fj = j0, fk = k0;
+    const double w0 = m[8] * fi + m[9] * fj + m[11];
+    const double u0 = m[0] * fi + m[1] * fj + m[3];
+    const double v0 = m[4] * fi + m[5] * fj + m[6] * fk + m[7];
+    const bool ok = w0 > 0.0;
+    const double cu = ok ? u0 / w0 : 0.0, rv = ok ? v0 / w0 : 0.0;
+    const bool inrange = fabs(cu) < 1.0e9 && fabs(rv) < 1.0e9;
+    const double c = inrange ? cu + 0.5 : 0.0, r = inrange ? rv + 0.5 : 0.0;
+    const double cf = floor(c), rf = floor(r);
+    t[TG_W0] = static_cast<float>(w0);
+    t[TG_M8] = static_cast<float>(m[8]);
+    t[TG_M9] = static_cast<float>(m[9]);
+    t[TG_AU] = static_cast<float>(m[0] - cu * m[8]);
+    t[TG_BU] = static_cast<float>(m[1] - cu * m[9]);
+    t[TG_AV] = static_cast<float>(m[4] - rv * m[8]);
+    t[TG_BV] = static_cast<float>(m[5] - rv * m[9]);
+    t[TG_M6] = static_cast<float>(m[6]);
+    t[TG_FC] = static_cast<float>(c - cf);
+    t[TG_FR] = static_cast<float>(r - rf);
+    t[TG_C0] = __int_as_float(static_cast<int>(cf));
+    t[TG_R0] = __int_as_float(static_cast<int>(rf));
+    t[TG_SCALE] = scale;
+    return ok && inrange;
+}
+
+// Voxel (i0 + di, j0 + dj) relative to the tile origin: inverse depth dw, column
+// c0 + tc, row of slice k0 + q: r0 + tr0 + q dr (tc, tr0 fractions relative to the integer
+// parts TG_C0, TG_R0). The footprints and the voxels use this same function.
+template <typename TG>
+__device__ __forceinline__ void fast_coord(const TG &t, float di, float dj, float &dw, float &tc, float &tr0, float &dr)
+{
+    const float w = fmaf(t[TG_M8], di, fmaf(t[TG_M9], dj, t[TG_W0]));
+    dw = __frcp_rn(w);
+    tc = fmaf(fmaf(t[TG_AU], di, t[TG_BU] * dj), dw, t[TG_FC]);
+    tr0 = fmaf(fmaf(t[TG_AV], di, t[TG_BV] * dj), dw, t[TG_FR]);
+    dr = t[TG_M6] * dw;
 }
 
 // Slices of one voxel column for one staged projection (exact arithmetic). a1: the 32
@@ -187,6 +220,7 @@ struct Smem {
     unsigned char *stage; // [2][NB] boxes
     float *geo;           // [3][NB][GEO]
     float *a1;            // [NWARPS][NB][TK] (exact kernel)
+    float *tg;            // [2][NB][TGEO] (fast kernel)
     int4 *meta;           // [2][NB]: x0, y0, mode
     uint64_t *bars;       // [2]
     __device__ Smem(unsigned char *base, int boxbytes)
@@ -194,13 +228,15 @@ struct Smem {
         stage = base;
         geo = reinterpret_cast<float *>(base + 2 * NB * boxbytes);
         a1 = geo + 3 * NB * GEO;
-        meta = reinterpret_cast<int4 *>(a1 + (A1 ? NWARPS * NB * TK : 0));
+        tg = a1 + (A1 ? NWARPS * NB * TK : 0);
+        meta = reinterpret_cast<int4 *>(tg + (A1 ? 0 : 2 * NB * TGEO));
         bars = reinterpret_cast<uint64_t *>(meta + 2 * NB);
     }
     static size_t bytes(int boxbytes)
     {
-        return 2 * NB * static_cast<size_t>(boxbytes) + (3 * NB * GEO + (A1 ? NWARPS * NB * TK : 0)) * sizeof(float) +
-               2 * NB * sizeof(int4) + 2 * sizeof(uint64_t);
+        return 2 * NB * static_cast<size_t>(boxbytes) +
+               (3 * NB * GEO + (A1 ? NWARPS * NB * TK : 2 * NB * TGEO)) * sizeof(float) + 2 * NB * sizeof(int4) +
+               2 * sizeof(uint64_t);
     }
 };
 
@@ -237,10 +273,11 @@ __device__ __forceinline__ void stage_geometry(const Params &P, float *geo, int 
             copy4_zfill(geo + idx, ok ? src : P.zip, ok);
         }
     } else {
+        const float *maps = reinterpret_cast<const float *>(P.maps); // 24 words per projection
         for (int idx = threadIdx.x; idx < NB * GEO_FAST; idx += THREADS) {
             const int b = idx / GEO_FAST, e = idx % GEO_FAST, p = s * NB + b;
-            const bool ok = p < P.nproj && e <= 12;
-            const float *src = !ok ? P.maps : e < 12 ? P.maps + static_cast<size_t>(p) * 12 + e : P.scale + p;
+            const bool ok = p < P.nproj && e <= 24;
+            const float *src = !ok ? P.scale : e < 24 ? maps + static_cast<size_t>(p) * 24 + e : P.scale + p;
             copy4_zfill(geo + idx, src, ok);
         }
     }
@@ -273,16 +310,31 @@ __device__ __forceinline__ void issue_batch(const Params &P, const CUtensorMap *
             r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, X[1])), 0.5f);
             c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(Z0, Y[0]), X[0])), 0.5f);
         } else {
-            const float *mm = geo + b * GEO_FAST;
-            const float w = fmaf(mm[8], static_cast<float>(ci), fmaf(mm[9], static_cast<float>(cj), mm[11]));
-            const FastCol f = fast_column(mm, static_cast<float>(ci), static_cast<float>(cj), static_cast<float>(k0));
-            c = f.c;
-            r = (corner & 4) ? fmaf(static_cast<float>(kmax - 1), f.dr, f.r0) : f.r0;
-            ok = w > 0.0f;
+            // every lane of the projection forms the tile geometry (same inputs, same values);
+            // the first stores it for the voxels
+            const float *g = geo + b * GEO_FAST;
+            float t[TGEO];
+            ok = tile_geometry(reinterpret_cast<const double *>(g), i0, j0, k0, g[24], t);
+            if (corner == 0) {
+#pragma unroll
+                for (int e = 0; e < TGEO; ++e) S.tg[(st * NB + b) * TGEO + e] = t[e];
+            }
+            float dw, tc, tr0, dr;
+            fast_coord(t, static_cast<float>(ci - i0), static_cast<float>(cj - j0), dw, tc, tr0, dr);
+            c = tc;
+            r = (corner & 4) ? fmaf(static_cast<float>(kmax - 1), dr, tr0) : tr0;
+            ok = ok && dw > 0.0f && fabsf(r) < 4.0e6f && fabsf(c) < 4.0e6f;
+            if (ok) {
+                // footprint in detector pixels: integer part + floor of the fraction
+                rmin = rmax = __float_as_int(t[TG_R0]) + __float2int_rd(r);
+                cmin = cmax = __float_as_int(t[TG_C0]) + __float2int_rd(c);
+            }
         }
-        ok = ok && fabsf(r) < 4.0e6f && fabsf(c) < 4.0e6f;
-        rmin = rmax = ok ? __float2int_rd(r) : 0;
-        cmin = cmax = ok ? __float2int_rd(c) : 0;
+        if constexpr (EXACT) {
+            ok = ok && fabsf(r) < 4.0e6f && fabsf(c) < 4.0e6f;
+            rmin = rmax = ok ? __float2int_rd(r) : 0;
+            cmin = cmax = ok ? __float2int_rd(c) : 0;
+        }
     }
 #pragma unroll
     for (int o = 1; o < 8; o <<= 1) {
@@ -397,7 +449,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
     uint32_t phase0 = 0, phase1 = 0;
     bool failed = false;
     const float fw = static_cast<float>(P.nu), fh = static_cast<float>(P.nv);
-    const float fi = static_cast<float>(i), fj = static_cast<float>(j), fk0 = static_cast<float>(k0);
+    const float fdi = static_cast<float>(lane), fdj = static_cast<float>(warp); // voxel offset in the tile
     const uint32_t rowbytes = static_cast<uint32_t>(P.rowbytes);
     const bool warp_inside = __any_sync(0xffffffffu, inside);
     for (int s = 0, gb = 0; s < nbatch; ++s, gb = gb == 2 ? 0 : gb + 1) {
@@ -458,14 +510,17 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                             q_base[e] = boxoff + static_cast<uint32_t>(cc - m.x) * 4u -
                                         static_cast<uint32_t>(kMagicBits + m.y) * rowbytes;
                         } else {
-                            const FastCol f = fast_column(g, fi, fj, fk0);
-                            const int cc = __float_as_int(__fadd_rd(f.c, kMagic)) - kMagicBits;
+                            const float *t = S.tg + (st * NB + b) * TGEO;
+                            float dw, tc, tr0, dr;
+                            fast_coord(t, fdi, fdj, dw, tc, tr0, dr);
+                            const int cc = __float_as_int(__fadd_rd(tc, kMagic)) - kMagicBits + __float_as_int(t[TG_C0]);
                             q_on[e] = true;
-                            q_a[e] = f.r0;
-                            q_b[e] = f.dr;
-                            q_c[e] = __uint_as_float(to_storage<DT>(f.dw * f.dw * (g[12] * ginv)));
+                            q_a[e] = tr0;
+                            q_b[e] = dr;
+                            q_c[e] = __uint_as_float(to_storage<DT>(dw * dw * (t[TG_SCALE] * ginv)));
+                            // bits(t + magic) * rowbytes + base = (r0 + floor(t) - y0) * rowbytes + ...
                             q_base[e] = boxoff + static_cast<uint32_t>(cc - m.x) * 2u -
-                                        static_cast<uint32_t>(kMagicBits + m.y) * rowbytes;
+                                        static_cast<uint32_t>(kMagicBits + m.y - __float_as_int(t[TG_R0])) * rowbytes;
                         }
                     }
                 }
@@ -531,19 +586,25 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                             a = __fadd_rn(a, __fmul_rn(dw2, v));
                         }
                     } else {
-                        const FastCol f = fast_column(g, fi, fj, fk0);
-                        if (f.c < 0.0f || f.c >= fw) continue;
-                        const unsigned short wt = to_storage<DT>(f.dw * f.dw * (g[12] * ginv));
-                        const T *img = static_cast<const T *>(P.proj) + static_cast<size_t>(p) * P.nu * P.nv +
-                                       static_cast<int>(f.c);
+                        const float *t = S.tg + (st * NB + b) * TGEO;
+                        float dw, tc, tr0, dr;
+                        fast_coord(t, fdi, fdj, dw, tc, tr0, dr);
+                        const int col = __float_as_int(t[TG_C0]) + __float2int_rd(tc);
+                        if (col < 0 || col >= P.nu) continue;
+                        const unsigned short wt = to_storage<DT>(dw * dw * (t[TG_SCALE] * ginv));
+                        const T *img = static_cast<const T *>(P.proj) + static_cast<size_t>(p) * P.nu * P.nv + col;
                         const float wf = from_storage<DT>(wt);
-                        float r = f.r0;
+                        const int r0 = __float_as_int(t[TG_R0]);
+                        float2 rr = make_float2(tr0, __fadd_rn(tr0, dr));
+                        const float2 step = make_float2(2.0f * dr, 2.0f * dr);
 #pragma unroll
-                        for (int q = 0; q < TK; ++q, r = __fadd_rn(r, f.dr)) {
+                        for (int q = 0; q < TK; ++q) {
                             if (q >= kmax) break;
-                            if (r < 0.0f || r >= fh) continue;
-                            const unsigned short v =
-                                reinterpret_cast<const unsigned short *>(img)[static_cast<size_t>(static_cast<int>(r)) * P.nu];
+                            // the rows of the staged loop: pairs advanced by 2 dr
+                            const int row = r0 + __float2int_rd((q & 1) ? rr.y : rr.x);
+                            if (q & 1) rr = __fadd2_rn(rr, step);
+                            if (row < 0 || row >= P.nv) continue;
+                            const unsigned short v = reinterpret_cast<const unsigned short *>(img)[static_cast<size_t>(row) * P.nu];
                             float &a = (q & 1) ? acc[q >> 1].y : acc[q >> 1].x;
                             a = fmaf(from_storage<DT>(v), wf, a);
                         }
@@ -690,7 +751,7 @@ static void box_guess(size_t nu, size_t nv, size_t nproj, int xalign, int &bw, i
 // TMA or the box does not fit shared memory (the caller then uses the plain kernel).
 static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
                                size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d,
-                               const float *maps_d, const uint32_t *mask_d, int accumulate, float *vol_d, int bw,
+                               const double *maps_d, const uint32_t *mask_d, int accumulate, float *vol_d, int bw,
                                int bh, cudaStream_t s)
 {
     using namespace fdk2;
@@ -809,7 +870,7 @@ mr_status mr_fdk_box_maps(const double *maps_h, size_t nu, size_t nv, size_t npr
 }
 
 mr_status mr_fdk_backproject_fast(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
-                                  size_t nproj, const float *maps_d, const uint32_t *mask_d, int box_w, int box_h,
+                                  size_t nproj, const double *maps_d, const uint32_t *mask_d, int box_w, int box_h,
                                   int accumulate, float *vol_d, void *stream)
 {
     if (!proj_d || !scale_d || !maps_d || !mask_d || !vol_d)

@@ -672,11 +672,11 @@ class FDKbp_single(_BackProjectorBase):
             bw, bh = ctypes.c_int(0), ctypes.c_int(0)
             maps = None
             if uni and dtype != L.MR_F32:
-                # precision form: FP64 detector maps, rounded once to float for the kernel
+                # precision form: FP64 detector maps (the kernel forms each tile origin in FP64)
                 m64 = self.maps64(angles)
                 check(L.lib().mr_fdk_box_maps(m64.ctypes.data_as(L.P_double), nu, nv, nproj, dtype, ctypes.byref(bw),
                                               ctypes.byref(bh)))
-                maps = torch.from_numpy(m64.astype(np.float32)).to(dev)
+                maps = torch.from_numpy(m64).to(dev)
             elif uni:
                 check(L.lib().mr_fdk_box(xip.ctypes.data_as(L.P_float), yip.ctypes.data_as(L.P_float),
                                          zip_.ctypes.data_as(L.P_float), nu, nv, nproj, dtype,

@@ -275,15 +275,17 @@ mr_status mr_fdk_maps64(const mr_fdk_geom *g, size_t nu, size_t nv, const float 
 /* Staging box of mr_fdk_backproject_fast from the FP64 maps (host). */
 mr_status mr_fdk_box_maps(const double *maps_h, size_t nu, size_t nv, size_t nproj, int dtype, int *box_w, int *box_h);
 /* Nearest-neighbour FDK backprojection of 16-bit filtered projections (MR_BF16 or MR_F16,
- * value = stored * scale_d[p], from mr_fdk_filter or mr_quantize) through the maps rounded
- * to float (maps_d [nproj][12] float, m[2] = m[10] = 0: no tilt correction), FP32
- * accumulation, into the final volume layout of mr_fdk_backproject. Each weighted sample
- * is one mixed-precision fma with the weight 1/w^2 * scale rounded to the storage type.
+ * value = stored * scale_d[p], from mr_fdk_filter or mr_quantize) through the FP64 maps
+ * (maps_d [nproj][12] double from mr_fdk_maps64, m[2] = m[10] = 0: no tilt correction), FP32
+ * accumulation, into the final volume layout of mr_fdk_backproject. The detector coordinates
+ * of each 32 x 8 x 32 voxel tile's origin are formed in FP64; the other voxels add FP32
+ * offsets to them. Each weighted sample is one mixed-precision fma with the weight
+ * 1/w^2 * scale rounded to the storage type.
  * Requires a TMA-compatible layout (row pitch a multiple of 16 bytes) and a box from
  * mr_fdk_box_maps; returns MR_ERR_UNSUPPORTED otherwise. Accuracy against the FP64
  * backprojection is reported by the tests and the benchmark, not bit-exact. */
 mr_status mr_fdk_backproject_fast(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
-                                  size_t nproj, const float *maps_d, const uint32_t *mask_d, int box_w, int box_h,
+                                  size_t nproj, const double *maps_d, const uint32_t *mask_d, int box_w, int box_h,
                                   int accumulate, float *vol_d, void *stream);
 /* FP64 error oracle on the device: backprojection of FP32 filtered projections through the
  * FP64 maps with FP64 accumulation, for 1..16 output slices (indices into the final volume's

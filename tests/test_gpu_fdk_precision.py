@@ -116,7 +116,7 @@ def test_fast_paths_against_fp64(cuda, nu):
     b16w, b16h = ctypes.c_int(), ctypes.c_int()
     L.check(L.lib().mr_fdk_box_maps(maps.ctypes.data_as(L.P_double), nu, nv, n, L.MR_BF16, ctypes.byref(b16w),
                                     ctypes.byref(b16h)))
-    mf = torch.from_numpy(maps.astype(np.float32)).cuda()
+    mf = torch.from_numpy(maps).cuda()
     errs = {}
     for name, dt in (("bf16", L.MR_BF16), ("fp16", L.MR_F16)):
         q, s = M.quantize(filt, name)
@@ -141,7 +141,7 @@ def test_fast_accumulate_in_batches(cuda):
     bw, bh = ctypes.c_int(), ctypes.c_int()
     L.check(L.lib().mr_fdk_box_maps(maps.ctypes.data_as(L.P_double), nu, nv, n, L.MR_BF16, ctypes.byref(bw),
                                     ctypes.byref(bh)))
-    mf = torch.from_numpy(maps.astype(np.float32)).cuda()
+    mf = torch.from_numpy(maps).cuda()
     st = torch.cuda.current_stream().cuda_stream
     q, s = M.quantize(filt, "fp16")
     whole = torch.empty((nv, nu, nu), device="cuda")
