@@ -220,35 +220,33 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
             if (lane == 0) atomicExch(&g_bp_error, 1);
         }
         if (got && inside) {
-            // projections in groups of G: the set-up of a group (detector position, weights,
-            // sample offset) is formed first so its latency overlaps, then the group's slice
-            // loops run in projection order (the reference's summation order)
+            // per-projection set-up of this voxel column: 0 nothing to add, 1 staged, 2 guarded
+            // global loads; n the detector column, off the sample offset in the stage
+            auto setup = [&](int b, int &n, uint32_t &off, float &wa, float &wb) -> int {
+                const int i = s * NB + b;
+                n = 0;
+                off = 0;
+                wa = wb = 0.0f;
+                if (i >= P.nproj) return 0;
+                const int4 m = S.meta[st * NB + b];
+                const float *g = S.geo + (gb * NB + b) * GEO;
+                const float u = posu(g[0], g[1], g[2], fx, fy);
+                n = __float2int_rz(u);
+                if (m.y == 2 || n < 0 || n > um2) return 0;
+                off = static_cast<uint32_t>((st * NB + b) * (BW * TZ) + (n - m.x));
+                wb = fabsf(__fsub_rn(u, static_cast<float>(n)));
+                wa = __fsub_rn(1.0f, wb);
+                return m.y == 1 ? 1 : 2;
+            };
 #pragma unroll 1
             for (int b0 = 0; b0 < NB; b0 += G) {
-                int q_mode[G], q_n[G]; // 0: nothing to add, 1: staged, 2: guarded global loads
+                // the set-up of a group is formed first so its latency overlaps, then the
+                // group's slice loops run in projection order (the reference's summation order)
+                int q_mode[G], q_n[G];
                 uint32_t q_off[G];
                 float q_wa[G], q_wb[G];
 #pragma unroll
-                for (int e = 0; e < G; ++e) {
-                    const int b = b0 + e, i = s * NB + b;
-                    q_mode[e] = 0;
-                    q_n[e] = 0;
-                    q_off[e] = 0;
-                    q_wa[e] = q_wb[e] = 0.0f;
-                    if (i < P.nproj) {
-                        const int4 m = S.meta[st * NB + b];
-                        const float *g = S.geo + (gb * NB + b) * GEO;
-                        const float u = posu(g[0], g[1], g[2], fx, fy);
-                        const int n = __float2int_rz(u);
-                        if (m.y != 2 && n >= 0 && n <= um2) {
-                            q_mode[e] = m.y == 1 ? 1 : 2;
-                            q_n[e] = n;
-                            q_off[e] = static_cast<uint32_t>((st * NB + b) * (BW * TZ) + (n - m.x));
-                            q_wb[e] = fabsf(__fsub_rn(u, static_cast<float>(n)));
-                            q_wa[e] = __fsub_rn(1.0f, q_wb[e]);
-                        }
-                    }
-                }
+                for (int e = 0; e < G; ++e) q_mode[e] = setup(b0 + e, q_n[e], q_off[e], q_wa[e], q_wb[e]);
                 // a footprint that did not fit its box (rare; uniform over the CTA) sends the
                 // whole group through the in-order path with guarded global loads
                 bool fallback = false;
@@ -267,14 +265,18 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
                 }
 #pragma unroll 1
                 for (int e = 0; e < G; ++e) {
-                    const float w = HASW ? S.geo[(gb * NB + b0 + e) * GEO + 3] : 1.0f;
-                    if (q_mode[e] == 1) {
-                        staged_column<HASW, false>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
-                    } else if (q_mode[e] == 2) {
-                        const int i = s * NB + b0 + e;
-                        const int slab = P.index ? __float_as_int(S.geo[(gb * NB + b0 + e) * GEO + 4]) : i;
-                        const float *img = P.proj + (static_cast<size_t>(slab) * P.nv + z0) * P.nu + q_n[e];
-                        const float wa = q_wa[e], wb = q_wb[e];
+                    const int b = b0 + e;
+                    int n;
+                    uint32_t off;
+                    float wa, wb;
+                    const int mode = setup(b, n, off, wa, wb); // formed again: no indexed arrays
+                    const float w = HASW ? S.geo[(gb * NB + b) * GEO + 3] : 1.0f;
+                    if (mode == 1) {
+                        staged_column<HASW, false>(acc, S.box + off, wa, wb, w, zmax);
+                    } else if (mode == 2) {
+                        const int i = s * NB + b;
+                        const int slab = P.index ? __float_as_int(S.geo[(gb * NB + b) * GEO + 4]) : i;
+                        const float *img = P.proj + (static_cast<size_t>(slab) * P.nv + z0) * P.nu + n;
 #pragma unroll
                         for (int q = 0; q < TZ; ++q) {
                             if (q >= zmax) break;

@@ -479,51 +479,52 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
         if (got && inside) {
             // projections in groups of G: the per-projection set-up of a group (reciprocal,
             // detector column, shared-memory base) is formed first, so its latency overlaps
+            // per-projection set-up of this voxel column: false when the projection adds
+            // nothing here or is not staged (exact: dw, dw^2, x1; fast: row fraction, row
+            // step, weight bits; base: shared-memory address of row 0 in magic-bit form)
+            auto setup = [&](int b, float &qa, float &qb, float &qc, uint32_t &qbase) -> bool {
+                const int p = s * NB + b;
+                const int4 m = S.meta[st * NB + b];
+                const uint32_t boxoff = static_cast<uint32_t>((st * NB + b) * P.boxbytes);
+                qa = qb = qc = 0.0f;
+                qbase = 0;
+                if (p >= P.nproj || m.z != 1) return false;
+                if constexpr (EXACT) {
+                    const float *g = geo + b * GEO;
+                    const float x0f = g[TK + 3 * lane], x1f = g[TK + 3 * lane + 1], x2f = g[TK + 3 * lane + 2];
+                    const float y0f = g[TK + 3 * TI + 3 * warp], y2f = g[TK + 3 * TI + 3 * warp + 2];
+                    const float Z0 = g[TK + 3 * TI + 3 * TJ], Z2 = g[TK + 3 * TI + 3 * TJ + 1];
+                    const float dw = __frcp_rn(__fadd_rn(__fadd_rn(Z2, y2f), x2f));
+                    const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(Z0, y0f), x0f)), 0.5f);
+                    const int cc = static_cast<int>(c);
+                    qa = dw;
+                    qb = __fmul_rn(dw, dw);
+                    qc = x1f;
+                    // bits(r + magic) * rowbytes + base = (floor(r) - y0) * rowbytes + (cc - x0) * 4 + box
+                    qbase = boxoff + static_cast<uint32_t>(cc - m.x) * 4u - static_cast<uint32_t>(kMagicBits + m.y) * rowbytes;
+                    return c >= 0.0f && c < fw;
+                } else {
+                    const float *t = S.tg + (st * NB + b) * TGEO;
+                    float dw, tc, tr0, dr;
+                    fast_coord(t, fdi, fdj, dw, tc, tr0, dr);
+                    const int cc = __float_as_int(__fadd_rd(tc, kMagic)) - kMagicBits + __float_as_int(t[TG_C0]);
+                    qa = tr0;
+                    qb = dr;
+                    qc = __uint_as_float(to_storage<DT>(dw * dw * (t[TG_SCALE] * ginv)));
+                    // bits(t + magic) * rowbytes + base = (r0 + floor(t) - y0) * rowbytes + ...
+                    qbase = boxoff + static_cast<uint32_t>(cc - m.x) * 2u -
+                            static_cast<uint32_t>(kMagicBits + m.y - __float_as_int(t[TG_R0])) * rowbytes;
+                    return true;
+                }
+            };
             constexpr int G = 4;
 #pragma unroll 1
             for (int b0 = 0; b0 < NB; b0 += G) {
-                float q_a[G], q_b[G], q_c[G]; // exact: dw, dw2, x1; fast: r0, dr, (weight bits)
+                float q_a[G], q_b[G], q_c[G];
                 uint32_t q_base[G];
                 bool q_on[G];
 #pragma unroll
-                for (int e = 0; e < G; ++e) {
-                    const int b = b0 + e, p = s * NB + b;
-                    const int4 m = S.meta[st * NB + b];
-                    const float *g = geo + b * GEO;
-                    const uint32_t boxoff = static_cast<uint32_t>((st * NB + b) * P.boxbytes);
-                    q_on[e] = false;
-                    q_a[e] = q_b[e] = q_c[e] = 0.0f;
-                    q_base[e] = 0;
-                    if (p < P.nproj && m.z == 1) {
-                        if constexpr (EXACT) {
-                            const float x0f = g[TK + 3 * lane], x1f = g[TK + 3 * lane + 1], x2f = g[TK + 3 * lane + 2];
-                            const float y0f = g[TK + 3 * TI + 3 * warp], y2f = g[TK + 3 * TI + 3 * warp + 2];
-                            const float Z0 = g[TK + 3 * TI + 3 * TJ], Z2 = g[TK + 3 * TI + 3 * TJ + 1];
-                            const float dw = __frcp_rn(__fadd_rn(__fadd_rn(Z2, y2f), x2f));
-                            const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(Z0, y0f), x0f)), 0.5f);
-                            const int cc = static_cast<int>(c);
-                            q_on[e] = c >= 0.0f && c < fw;
-                            q_a[e] = dw;
-                            q_b[e] = __fmul_rn(dw, dw);
-                            q_c[e] = x1f;
-                            // bits(r + magic) * rowbytes + base = (floor(r) - y0) * rowbytes + (cc - x0) * 4 + box
-                            q_base[e] = boxoff + static_cast<uint32_t>(cc - m.x) * 4u -
-                                        static_cast<uint32_t>(kMagicBits + m.y) * rowbytes;
-                        } else {
-                            const float *t = S.tg + (st * NB + b) * TGEO;
-                            float dw, tc, tr0, dr;
-                            fast_coord(t, fdi, fdj, dw, tc, tr0, dr);
-                            const int cc = __float_as_int(__fadd_rd(tc, kMagic)) - kMagicBits + __float_as_int(t[TG_C0]);
-                            q_on[e] = true;
-                            q_a[e] = tr0;
-                            q_b[e] = dr;
-                            q_c[e] = __uint_as_float(to_storage<DT>(dw * dw * (t[TG_SCALE] * ginv)));
-                            // bits(t + magic) * rowbytes + base = (r0 + floor(t) - y0) * rowbytes + ...
-                            q_base[e] = boxoff + static_cast<uint32_t>(cc - m.x) * 2u -
-                                        static_cast<uint32_t>(kMagicBits + m.y - __float_as_int(t[TG_R0])) * rowbytes;
-                        }
-                    }
-                }
+                for (int e = 0; e < G; ++e) q_on[e] = setup(b0 + e, q_a[e], q_b[e], q_c[e], q_base[e]);
                 // a footprint that did not fit its box (rare; uniform over the CTA) sends the
                 // whole group through the in-order path below, so that every voxel still sums
                 // its projections in the reference's order
@@ -554,13 +555,14 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
 #pragma unroll 1
                 for (int e = 0; e < G; ++e) {
                     const int b = b0 + e, p = s * NB + b;
-                    if (q_on[e]) {
+                    float qa, qb, qc;
+                    uint32_t qbase;
+                    if (setup(b, qa, qb, qc, qbase)) { // set-up formed again: no indexed arrays
                         if constexpr (EXACT)
-                            exact_column<false>(acc, smem, q_base[e], rowbytes, S.a1 + (warp * NB + b) * TK, q_c[e], q_a[e],
-                                                q_b[e], kmax);
+                            exact_column<false>(acc, smem, qbase, rowbytes, S.a1 + (warp * NB + b) * TK, qc, qa, qb, kmax);
                         else
-                            fast_column_staged<DT, false>(acc, smem, q_base[e], rowbytes, q_a[e], q_b[e],
-                                                          static_cast<unsigned short>(__float_as_uint(q_c[e])), kmax);
+                            fast_column_staged<DT, false>(acc, smem, qbase, rowbytes, qa, qb,
+                                                          static_cast<unsigned short>(__float_as_uint(qc)), kmax);
                         continue;
                     }
                     if (p >= P.nproj || S.meta[st * NB + b].z != 0) continue;
