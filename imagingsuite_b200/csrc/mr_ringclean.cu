@@ -149,36 +149,6 @@ __global__ void __launch_bounds__(kConvThreads) k_dwt_rows2(const float *__restr
     }
 }
 
-__global__ void __launch_bounds__(kConvThreads) k_dwt_cols2(const float *__restrict__ tmpH,
-                                                            const float *__restrict__ tmpG, int dx, int sy,
-                                                            const float *__restrict__ taps, int K, int dy,
-                                                            float *__restrict__ a, float *__restrict__ h,
-                                                            float *__restrict__ v, float *__restrict__ d)
-{
-    __shared__ float tp[2 * kMaxTaps];
-    load_taps(taps, 2 * K, tp);
-    const float *tH = tp, *tG = tp + K;
-    const int x = blockIdx.x * kConvThreads + threadIdx.x, k = blockIdx.y, b = blockIdx.z;
-    if (x >= dx) return;
-    const size_t base = static_cast<size_t>(b) * sy * dx + x;
-    const bool inner = 2 * k - K + 2 >= 0 && 2 * k + 1 < sy;
-    float sa = 0.0f, sh = 0.0f, sv = 0.0f, sd = 0.0f;
-    for (int m = 0; m < K; ++m) {
-        const int row = inner ? 2 * k - m + 1 : mirror_index(sy, K, K + 2 * k - m + 1);
-        const size_t idx = base + static_cast<size_t>(row) * dx;
-        const float ph = tmpH[idx], pg = tmpG[idx];
-        sa = __fadd_rn(sa, __fmul_rn(tH[m], ph));
-        sh = __fadd_rn(sh, __fmul_rn(tG[m], ph));
-        sv = __fadd_rn(sv, __fmul_rn(tH[m], pg));
-        sd = __fadd_rn(sd, __fmul_rn(tG[m], pg));
-    }
-    const size_t o = (static_cast<size_t>(b) * dy + k) * dx + x;
-    a[o] = sa;
-    h[o] = sh;
-    v[o] = sv;
-    d[o] = sd;
-}
-
 // out[q][row][k], q = blockIdx.z (a, h, v, d), rows over all batch images.
 __global__ void __launch_bounds__(kConvThreads) k_up_rows2(const float *__restrict__ a, const float *__restrict__ hb,
                                                            const float *__restrict__ vb, const float *__restrict__ db,
@@ -212,38 +182,138 @@ __global__ void __launch_bounds__(kConvThreads) k_up_rows2(const float *__restri
     }
 }
 
-// out[b][k][x] = ((a + h) + v) + d of the column passes, cropped to (ox, oy).
-__global__ void __launch_bounds__(kConvThreads) k_up_cols2(const float *__restrict__ rows, int dx, int h, int nb,
+// Column passes with kColBlock consecutive outputs per thread. The outputs of a block share
+// most of their input rows, so the thread walks the rows it needs once, from the last to
+// the first, and adds each row into every output whose tap m = (output position) - (row
+// position) falls in [0, K): per output the rows arrive in descending order, i.e. the taps
+// in the reference's ascending order, so every sum equals the one-output-per-thread form
+// bit for bit. Blocks that reach a border (mirrored or upsampled-zero indices) use the
+// per-output form.
+constexpr int kColBlock = 8;
+
+__global__ void __launch_bounds__(kConvThreads) k_dwt_cols3(const float *__restrict__ tmpH,
+                                                            const float *__restrict__ tmpG, int dx, int sy,
+                                                            const float *__restrict__ taps, int K, int dy,
+                                                            float *__restrict__ a, float *__restrict__ h,
+                                                            float *__restrict__ v, float *__restrict__ d)
+{
+    __shared__ float tp[2 * kMaxTaps];
+    load_taps(taps, 2 * K, tp);
+    const float *tH = tp, *tG = tp + K;
+    const int x = blockIdx.x * kConvThreads + threadIdx.x, k0 = blockIdx.y * kColBlock, b = blockIdx.z;
+    if (x >= dx) return;
+    const size_t base = static_cast<size_t>(b) * sy * dx + x;
+    const int k1 = min(k0 + kColBlock, dy); // outputs k0 .. k1-1
+    const bool inner = 2 * k0 - K + 2 >= 0 && 2 * (k1 - 1) + 1 < sy;
+    if (inner && k1 - k0 == kColBlock) {
+        float sa[kColBlock], sh[kColBlock], sv[kColBlock], sd[kColBlock];
+#pragma unroll
+        for (int r = 0; r < kColBlock; ++r) sa[r] = sh[r] = sv[r] = sd[r] = 0.0f;
+        // output k uses rows 2k + 1 - m, m = 0 .. K-1
+        for (int i = 2 * (k0 + kColBlock - 1) + 1; i >= 2 * k0 + 2 - K; --i) {
+            const size_t idx = base + static_cast<size_t>(i) * dx;
+            const float ph = tmpH[idx], pg = tmpG[idx];
+#pragma unroll
+            for (int r = 0; r < kColBlock; ++r) {
+                const int m = 2 * (k0 + r) + 1 - i;
+                if (static_cast<unsigned>(m) < static_cast<unsigned>(K)) {
+                    const float th = tH[m], tg = tG[m];
+                    sa[r] = __fadd_rn(sa[r], __fmul_rn(th, ph));
+                    sh[r] = __fadd_rn(sh[r], __fmul_rn(tg, ph));
+                    sv[r] = __fadd_rn(sv[r], __fmul_rn(th, pg));
+                    sd[r] = __fadd_rn(sd[r], __fmul_rn(tg, pg));
+                }
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < kColBlock; ++r) {
+            const size_t o = (static_cast<size_t>(b) * dy + k0 + r) * dx + x;
+            a[o] = sa[r];
+            h[o] = sh[r];
+            v[o] = sv[r];
+            d[o] = sd[r];
+        }
+        return;
+    }
+    for (int k = k0; k < k1; ++k) {
+        const bool in = 2 * k - K + 2 >= 0 && 2 * k + 1 < sy;
+        float sa = 0.0f, sh = 0.0f, sv = 0.0f, sd = 0.0f;
+        for (int m = 0; m < K; ++m) {
+            const int row = in ? 2 * k - m + 1 : mirror_index(sy, K, K + 2 * k - m + 1);
+            const size_t idx = base + static_cast<size_t>(row) * dx;
+            const float ph = tmpH[idx], pg = tmpG[idx];
+            sa = __fadd_rn(sa, __fmul_rn(tH[m], ph));
+            sh = __fadd_rn(sh, __fmul_rn(tG[m], ph));
+            sv = __fadd_rn(sv, __fmul_rn(tH[m], pg));
+            sd = __fadd_rn(sd, __fmul_rn(tG[m], pg));
+        }
+        const size_t o = (static_cast<size_t>(b) * dy + k) * dx + x;
+        a[o] = sa;
+        h[o] = sh;
+        v[o] = sv;
+        d[o] = sd;
+    }
+}
+
+__global__ void __launch_bounds__(kConvThreads) k_up_cols3(const float *__restrict__ rows, int dx, int h, int nb,
                                                            const float *__restrict__ taps, int K, int ox, int oy,
                                                            float *__restrict__ out)
 {
     __shared__ float tp[2 * kMaxTaps];
     load_taps(taps + 2 * K, 2 * K, tp);
-    const int x = blockIdx.x * kConvThreads + threadIdx.x, k = blockIdx.y, b = blockIdx.z;
+    const int x = blockIdx.x * kConvThreads + threadIdx.x, k0 = blockIdx.y * kColBlock, b = blockIdx.z;
     if (x >= ox) return;
     const size_t plane = static_cast<size_t>(nb) * h * dx;
     const size_t base = static_cast<size_t>(b) * h * dx + x;
     const int c = K - 2;
-    const bool inner = k >= 1 && k < 2 * h - K + 2;
-    float s4[4];
+    const int k1 = min(k0 + kColBlock, oy);
+    const bool inner = k0 >= 1 && k1 - 1 < 2 * h - K + 2;
+    if (inner && k1 - k0 == kColBlock) {
+        // output k uses rows (k + c - m) / 2 for the m of the parity of k + c
+        float s4[4][kColBlock];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const float *kv = (q == 0 || q == 2) ? tp : tp + K;
-        const float *col = rows + q * plane + base;
-        float acc = 0.0f;
-        if (inner) {
-            for (int m = (k + c) & 1; m < K; m += 2)
-                acc = __fadd_rn(acc, __fmul_rn(col[static_cast<size_t>((k + c - m) >> 1) * dx], kv[m]));
-        } else {
-            for (int m = 0; m < K; ++m) {
-                const int t = up_index(h, K, K + k + c - m);
-                const float xv = (t & 1) ? 0.0f : col[static_cast<size_t>(t >> 1) * dx];
-                acc = __fadd_rn(acc, __fmul_rn(xv, kv[m]));
+        for (int q = 0; q < 4; ++q) {
+            const float *kv = (q == 0 || q == 2) ? tp : tp + K;
+            const float *col = rows + q * plane + base;
+#pragma unroll
+            for (int r = 0; r < kColBlock; ++r) s4[q][r] = 0.0f;
+            for (int i = (k0 + kColBlock - 1 + c) >> 1; 2 * i >= k0 + c - (K - 1); --i) {
+                const float xv = col[static_cast<size_t>(i) * dx];
+#pragma unroll
+                for (int r = 0; r < kColBlock; ++r) {
+                    const int m = k0 + r + c - 2 * i;
+                    if (static_cast<unsigned>(m) < static_cast<unsigned>(K)) s4[q][r] = __fadd_rn(s4[q][r], __fmul_rn(xv, kv[m]));
+                }
             }
         }
-        s4[q] = acc;
+#pragma unroll
+        for (int r = 0; r < kColBlock; ++r)
+            out[(static_cast<size_t>(b) * oy + k0 + r) * ox + x] =
+                __fadd_rn(__fadd_rn(__fadd_rn(s4[0][r], s4[1][r]), s4[2][r]), s4[3][r]);
+        return;
     }
-    out[(static_cast<size_t>(b) * oy + k) * ox + x] = __fadd_rn(__fadd_rn(__fadd_rn(s4[0], s4[1]), s4[2]), s4[3]);
+    for (int k = k0; k < k1; ++k) {
+        const bool in = k >= 1 && k < 2 * h - K + 2;
+        float s4[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float *kv = (q == 0 || q == 2) ? tp : tp + K;
+            const float *col = rows + q * plane + base;
+            float acc = 0.0f;
+            if (in) {
+                for (int m = (k + c) & 1; m < K; m += 2)
+                    acc = __fadd_rn(acc, __fmul_rn(col[static_cast<size_t>((k + c - m) >> 1) * dx], kv[m]));
+            } else {
+                for (int m = 0; m < K; ++m) {
+                    const int t = up_index(h, K, K + k + c - m);
+                    const float xv = (t & 1) ? 0.0f : col[static_cast<size_t>(t >> 1) * dx];
+                    acc = __fadd_rn(acc, __fmul_rn(xv, kv[m]));
+                }
+            }
+            s4[q] = acc;
+        }
+        out[(static_cast<size_t>(b) * oy + k) * ox + x] = __fadd_rn(__fadd_rn(__fadd_rn(s4[0], s4[1]), s4[2]), s4[3]);
+    }
 }
 
 struct Plan {
@@ -362,9 +432,8 @@ static mr_status stripe_batch(float *s_d, int nb, const rc::Plan &P, const float
         const int rows = nb * sy;
         k_dwt_rows2<<<dim3(div_up(dx, kConvThreads), std::min(rows, 65535)), kConvThreads, 0, st>>>(A[l], sx, rows,
                                                                                                   taps_d, K, dx, tH, tG);
-        k_dwt_cols2<<<dim3(div_up(dx, kConvThreads), dy, nb), kConvThreads, 0, st>>>(tH, tG, dx, sy, taps_d, K, dy,
-                                                                                    A[l + 1], Hb[l + 1], Vb[l + 1],
-                                                                                    Db[l + 1]);
+        k_dwt_cols3<<<dim3(div_up(dx, kConvThreads), div_up(dy, kColBlock), nb), kConvThreads, 0, st>>>(
+            tH, tG, dx, sy, taps_d, K, dy, A[l + 1], Hb[l + 1], Vb[l + 1], Db[l + 1]);
     }
     for (int l = 0; l < L; ++l) {
         const int bw = P.sx[l + 1], bh = P.sy[l + 1], n = P.nfft[l];
@@ -379,8 +448,8 @@ static mr_status stripe_batch(float *s_d, int nb, const rc::Plan &P, const float
         k_up_rows2<<<dim3(div_up(dx, kConvThreads), std::min(rows, 65535), 4), kConvThreads, 0, st>>>(
             A[l + 1], Hb[l + 1], Vb[l + 1], Db[l + 1], w, rows, taps_d, K, dx, tmp);
         const int ox = l == 0 ? P.sx[0] : dx, oy = l == 0 ? P.sy[0] : dy;
-        k_up_cols2<<<dim3(div_up(ox, kConvThreads), oy, nb), kConvThreads, 0, st>>>(tmp, dx, h, nb, taps_d, K, ox, oy,
-                                                                                  A[l]);
+        k_up_cols3<<<dim3(div_up(ox, kConvThreads), div_up(oy, kColBlock), nb), kConvThreads, 0, st>>>(
+            tmp, dx, h, nb, taps_d, K, ox, oy, A[l]);
     }
     return check_launch("stripe filter");
 }
