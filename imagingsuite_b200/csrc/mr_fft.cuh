@@ -11,6 +11,11 @@
 // spectrum and returns the natural-order, unnormalised inverse transform. A real frequency
 // response is applied at the digit-reversed positions (fft_permute_response on the host).
 // Twiddles: exp(-2 pi i k / n), k < n (fft_twiddles on the host).
+//
+// Element e of a sequence sits at fft_slot(e) = e + e/16 of the shared buffer (one float2 of
+// padding after every 16): the strided stages would otherwise put up to 16 lanes of a warp on
+// one bank (8x the minimum wavefronts in the last radix-8 stage of n = 4096); with the padding
+// every stage of n = 2^9 .. 2^13 runs at the minimum of two wavefronts per warp access.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -21,6 +26,11 @@
 namespace mr {
 
 constexpr int kFftMaxStages = 16;
+
+__host__ __device__ __forceinline__ int fft_slot(int e) { return e + (e >> 4); }
+
+// float2 slots of the shared buffer of an n-point transform
+__host__ __device__ __forceinline__ int fft_buffer_slots(int n) { return n + n / 16; }
 
 // radix (as log2) of each stage, from the full length down
 __host__ __device__ __forceinline__ int fft_stages(int logn, int *rl)
@@ -87,11 +97,11 @@ __device__ __forceinline__ void fft_dif_stage(float2 *buf, int logn, int nsl, co
         const int base = ((b >> qsl) << nsl) + j;
         float2 x[R];
 #pragma unroll
-        for (int q = 0; q < R; ++q) x[q] = buf[base + (q << qsl)];
+        for (int q = 0; q < R; ++q) x[q] = buf[fft_slot(base + (q << qsl))];
         dft_small<R>(x);
-        buf[base] = x[0];
+        buf[fft_slot(base)] = x[0];
 #pragma unroll
-        for (int m = 1; m < R; ++m) buf[base + (m << qsl)] = cmul(x[m], __ldg(tw + ((j * m) << tws)));
+        for (int m = 1; m < R; ++m) buf[fft_slot(base + (m << qsl))] = cmul(x[m], __ldg(tw + ((j * m) << tws)));
     }
 }
 
@@ -107,16 +117,16 @@ __device__ __forceinline__ void fft_inv_stage(float2 *buf, int logn, int nsl, co
         const int j = b & ((1 << qsl) - 1);
         const int base = ((b >> qsl) << nsl) + j;
         float2 x[R];
-        x[0] = conj2(buf[base]);
+        x[0] = conj2(buf[fft_slot(base)]);
 #pragma unroll
-        for (int m = 1; m < R; ++m) x[m] = conj2(cmulc(buf[base + (m << qsl)], __ldg(tw + ((j * m) << tws))));
+        for (int m = 1; m < R; ++m) x[m] = conj2(cmulc(buf[fft_slot(base + (m << qsl))], __ldg(tw + ((j * m) << tws))));
         dft_small<R>(x); // inverse DFT = conj(DFT(conj(.)))
 #pragma unroll
-        for (int q = 0; q < R; ++q) buf[base + (q << qsl)] = conj2(x[q]);
+        for (int q = 0; q < R; ++q) buf[fft_slot(base + (q << qsl))] = conj2(x[q]);
     }
 }
 
-// Forward transform: natural order -> digit-reversed spectrum.
+// Forward transform: natural order -> digit-reversed spectrum (buffer slots fft_slot(e)).
 __device__ __forceinline__ void fft_forward(float2 *buf, int logn, const float2 *__restrict__ tw)
 {
     int rl[kFftMaxStages];
@@ -151,8 +161,8 @@ __device__ __forceinline__ void fft_apply_response(float2 *buf, int n, const flo
 {
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         const float r = __ldg(h + k);
-        const float2 v = buf[k];
-        buf[k] = make_float2(v.x * r, v.y * r);
+        const float2 v = buf[fft_slot(k)];
+        buf[fft_slot(k)] = make_float2(v.x * r, v.y * r);
     }
     __syncthreads();
 }

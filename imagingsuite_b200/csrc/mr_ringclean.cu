@@ -88,14 +88,14 @@ __global__ void k_stripe_fft(float *__restrict__ band, int bw, int bh, int ncols
             x0 = band[base0 + static_cast<size_t>(p) * bw];
             if (has1) x1 = band[base1 + static_cast<size_t>(p) * bw];
         }
-        buf[p] = make_float2(x0, x1);
+        buf[fft_slot(p)] = make_float2(x0, x1);
     }
     __syncthreads();
     fft_forward(buf, logn, twiddle);
     fft_apply_response(buf, n, response);
     fft_inverse(buf, logn, twiddle);
     for (int p = threadIdx.x; p < bh; p += blockDim.x) {
-        const float2 v = buf[p];
+        const float2 v = buf[fft_slot(p)];
         band[base0 + static_cast<size_t>(p) * bw] = v.x;
         if (has1) band[base1 + static_cast<size_t>(p) * bw] = v.y;
     }
@@ -438,7 +438,7 @@ static mr_status stripe_batch(float *s_d, int nb, const rc::Plan &P, const float
     for (int l = 0; l < L; ++l) {
         const int bw = P.sx[l + 1], bh = P.sy[l + 1], n = P.nfft[l];
         const int ncols = nb * bw;
-        k_stripe_fft<<<(ncols + 1) / 2, std::min(512, std::max(64, n / 8)), n * sizeof(float2), st>>>(
+        k_stripe_fft<<<(ncols + 1) / 2, std::min(512, std::max(64, n / 8)), fft_buffer_slots(n) * sizeof(float2), st>>>(
             Vb[l + 1], bw, bh, ncols, n, ilog2i(n), tw_d[l], resp_d[l]);
     }
     for (int l = L - 1; l >= 0; --l) {
@@ -502,7 +502,8 @@ static mr_status run_stripes(float *data_d, bool interleaved, size_t nu, size_t 
     off += stripe_scratch(P, nb);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(rc::k_stripe_fft, cudaFuncAttributeMaxDynamicSharedMemorySize, 16384 * sizeof(float2));
+        cudaFuncSetAttribute(rc::k_stripe_fft, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             fft_buffer_slots(16384) * sizeof(float2));
         attr = true;
     }
     float *gathered = interleaved ? work + off : nullptr;

@@ -117,7 +117,7 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
     for (int p = threadIdx.x; p < n; p += blockDim.x) {
         float x0 = padded_value(a, row0, r0, p);
         float x1 = has1 ? padded_value(a, row1, r1, p) : 0.0f;
-        buf[p] = make_float2(x0, x1);
+        buf[fft_slot(p)] = make_float2(x0, x1);
     }
     __syncthreads();
 
@@ -127,7 +127,7 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
 
     // crop and write
     for (int i = threadIdx.x; i < a.nu; i += blockDim.x) {
-        const float2 v = buf[i + a.ninsert];
+        const float2 v = buf[fft_slot(i + a.ninsert)];
         float y0 = __fmul_rn(v.x, a.scale);
         float y1 = __fmul_rn(v.y, a.scale);
         if (a.mode == kPadProjFilter) {
@@ -166,7 +166,7 @@ static int ilog2(size_t n)
 mr_status launch_rowfilter(RowFilterArgs a, cudaStream_t s)
 {
     if (a.nrows == 0) return MR_OK;
-    const size_t smem = static_cast<size_t>(a.n) * sizeof(float2);
+    const size_t smem = static_cast<size_t>(fft_buffer_slots(a.n)) * sizeof(float2);
     static bool attr_set = false;
     if (!attr_set) {
         MR_CUDA_TRY(cudaFuncSetAttribute(k_rowfilter, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
