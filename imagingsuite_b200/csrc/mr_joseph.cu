@@ -10,10 +10,12 @@
 //
 // Adjoint: the exact transpose, voxel-driven. A voxel (x, y) receives weight (1 - w) from the
 // rays whose sample at its major index falls in [minor, minor + 1) and w from those in
-// [minor - 1, minor). Candidate rays are bracketed analytically with a half-pixel margin and
-// every candidate's sample position is recomputed with the forward's own expression
-// (joseph_pos), so forward and adjoint use bit-identical weights and the same sample set:
-// <A x, y> = <x, A^T y> up to the summation order.
+// [minor - 1, minor). Those rays form the interval rc -+ |s| of detector positions (s = 1/inv);
+// the candidates are the integers within it widened by a margin of 0.02 + 1e-5 (n + nu) bins,
+// far above the float error of the bracket and of a sample position (which grows with the
+// magnitudes involved: below 4e-4 bin for n, nu up to 4096), and every candidate's sample position is recomputed with the forward's own
+// expression (joseph_pos), so forward and adjoint use bit-identical weights and the same
+// sample set: <A x, y> = <x, A^T y> up to the summation order.
 //
 // Centre derivative: d(A x)/d centre = -inv d sum_k (s1 - s0) for a ray (the interpolation
 // is linear within a pixel), produced by the forward kernel on request; per-slice dot
@@ -33,7 +35,8 @@ namespace joseph {
 struct Angle {
     float major_y; // 1: rays step along y
     float alpha, inv, d, rho_off;
-    float pad[3];
+    float s;       // 1 / inv (sin or cos), for the adjoint's ray bracket
+    float pad[2];
 };
 
 static_assert(sizeof(Angle) == 32, "Angle layout");
@@ -99,7 +102,8 @@ __global__ void __launch_bounds__(128) k_forward(const float *__restrict__ vol, 
 // One thread per voxel (x, y, z): gather over angles and candidate rays.
 __global__ void __launch_bounds__(128) k_adjoint(const float *__restrict__ proj, int n, int nz,
                                                  const Angle *__restrict__ ang, int nproj, int nu, float centre,
-                                                 float tan_tilt, float pivot, int accumulate, float *__restrict__ vol)
+                                                 float tan_tilt, float pivot, float margin, int accumulate,
+                                                 float *__restrict__ vol)
 {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
     if (x >= n) return;
@@ -111,10 +115,10 @@ __global__ void __launch_bounds__(128) k_adjoint(const float *__restrict__ proj,
         const bool my = g.major_y != 0.0f;
         const int k = my ? y : x, minor = my ? x : y;
         // f(r) = (r - cz - rho_off) inv + k alpha; rays with f in [minor - 1, minor + 1)
-        const float s = 1.0f / g.inv;
-        const float rc = (static_cast<float>(minor) - static_cast<float>(k) * g.alpha) * s + cz + g.rho_off;
-        const float hw = fabsf(s) + 0.5f;
-        const int r0 = max(0, static_cast<int>(floorf(rc - hw))), r1 = min(nu - 1, static_cast<int>(ceilf(rc + hw)));
+        const float rc = (static_cast<float>(minor) - static_cast<float>(k) * g.alpha) * g.s + cz + g.rho_off;
+        const float hw = fabsf(g.s) + margin;
+        // the integers within [rc - hw, rc + hw]: at most 2|s| + 1 rays
+        const int r0 = max(0, static_cast<int>(ceilf(rc - hw))), r1 = min(nu - 1, static_cast<int>(floorf(rc + hw)));
         const float *p = proj + (static_cast<size_t>(t) * nz + z) * nu;
         for (int r = r0; r <= r1; ++r) {
             const float f = joseph_pos(joseph_beta(r, cz, g), k, g);
@@ -193,11 +197,13 @@ mr_status mr_joseph_geometry(const float *angles_h, size_t nproj, size_t n, floa
             g.major_y = 0.0f;
             g.alpha = static_cast<float>(-cs / sn);
             g.inv = static_cast<float>(1.0 / sn);
+            g.s = static_cast<float>(sn);
             g.d = static_cast<float>(1.0 / std::fabs(sn));
         } else {
             g.major_y = 1.0f;
             g.alpha = static_cast<float>(-sn / cs);
             g.inv = static_cast<float>(1.0 / cs);
+            g.s = static_cast<float>(cs);
             g.d = static_cast<float>(1.0 / std::fabs(cs));
         }
         std::memcpy(params_h + t * 8, &g, sizeof(Angle));
@@ -234,7 +240,8 @@ mr_status mr_joseph_adjoint(const float *proj_d, size_t n, size_t nz, const floa
     k_adjoint<<<grid, 128, 0, as_stream(stream)>>>(proj_d, static_cast<int>(n), static_cast<int>(nz),
                                                    reinterpret_cast<const Angle *>(params_d),
                                                    static_cast<int>(nproj), static_cast<int>(nu), centre, tan_tilt,
-                                                   pivot, accumulate, vol_d);
+                                                   pivot, 0.02f + 1e-5f * static_cast<float>(n + nu), accumulate,
+                                                   vol_d);
     return check_launch("k_adjoint");
 }
 
