@@ -99,36 +99,52 @@ __global__ void __launch_bounds__(128) k_forward(const float *__restrict__ vol, 
     if (dproj) dproj[o] = -dsum * g.inv * g.d;
 }
 
-// One thread per voxel (x, y, z): gather over angles and candidate rays.
+// One thread per voxel (x, y, z): gather over angles and candidate rays. The per-angle
+// parameters are staged in shared memory in chunks of kAngleChunk.
+constexpr int kAngleChunk = 256;
+
 __global__ void __launch_bounds__(128) k_adjoint(const float *__restrict__ proj, int n, int nz,
                                                  const Angle *__restrict__ ang, int nproj, int nu, float centre,
                                                  float tan_tilt, float pivot, float margin, int accumulate,
                                                  float *__restrict__ vol)
 {
+    __shared__ Angle sa[kAngleChunk];
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
-    if (x >= n) return;
     const float cz = __fmaf_rn(tan_tilt, static_cast<float>(z) - pivot, centre);
     const float lim = static_cast<float>(n - 1);
     float acc = 0.0f;
-    for (int t = 0; t < nproj; ++t) {
-        const Angle g = ang[t];
-        const bool my = g.major_y != 0.0f;
-        const int k = my ? y : x, minor = my ? x : y;
-        // f(r) = (r - cz - rho_off) inv + k alpha; rays with f in [minor - 1, minor + 1)
-        const float rc = (static_cast<float>(minor) - static_cast<float>(k) * g.alpha) * g.s + cz + g.rho_off;
-        const float hw = fabsf(g.s) + margin;
-        // the integers within [rc - hw, rc + hw]: at most 2|s| + 1 rays
-        const int r0 = max(0, static_cast<int>(ceilf(rc - hw))), r1 = min(nu - 1, static_cast<int>(floorf(rc + hw)));
-        const float *p = proj + (static_cast<size_t>(t) * nz + z) * nu;
-        for (int r = r0; r <= r1; ++r) {
-            const float f = joseph_pos(joseph_beta(r, cz, g), k, g);
-            if (!(f >= 0.0f && f < lim)) continue;
-            const int i0 = static_cast<int>(f);
-            const float w = f - static_cast<float>(i0);
-            if (i0 == minor) acc = __fmaf_rn((1.0f - w) * g.d, __ldg(p + r), acc);
-            else if (i0 == minor - 1) acc = __fmaf_rn(w * g.d, __ldg(p + r), acc);
+    for (int t0 = 0; t0 < nproj; t0 += kAngleChunk) {
+        const int nt = min(kAngleChunk, nproj - t0);
+        __syncthreads();
+        for (int i = threadIdx.x; i < nt; i += blockDim.x) sa[i] = ang[t0 + i];
+        __syncthreads();
+        if (x >= n) continue;
+        for (int tt = 0; tt < nt; ++tt) {
+            const Angle g = sa[tt];
+            const bool my = g.major_y != 0.0f;
+            const int k = my ? y : x, minor = my ? x : y;
+            // f(r) = (r - cz - rho_off) inv + k alpha; rays with f in [minor - 1, minor + 1)
+            const float rc = (static_cast<float>(minor) - static_cast<float>(k) * g.alpha) * g.s + cz + g.rho_off;
+            const float hw = fabsf(g.s) + margin;
+            // the integers within [rc - hw, rc + hw]: 2|s| + 1 <= 3 rays, a fourth only when the
+            // margin exceeds half a bin (very large sizes)
+            const int r0 = max(0, static_cast<int>(ceilf(rc - hw))), r1 = min(nu - 1, static_cast<int>(floorf(rc + hw)));
+            const float *p = proj + (static_cast<size_t>(t0 + tt) * nz + z) * nu;
+            auto ray = [&](int r) {
+                const float f = joseph_pos(joseph_beta(r, cz, g), k, g);
+                if (!(f >= 0.0f && f < lim)) return;
+                const int i0 = static_cast<int>(f);
+                const float w = f - static_cast<float>(i0);
+                if (i0 == minor) acc = __fmaf_rn((1.0f - w) * g.d, __ldg(p + r), acc);
+                else if (i0 == minor - 1) acc = __fmaf_rn(w * g.d, __ldg(p + r), acc);
+            };
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+                if (r0 + j <= r1) ray(r0 + j);
+            for (int r = r0 + 3; r <= r1; ++r) ray(r);
         }
     }
+    if (x >= n) return;
     float *o = vol + (static_cast<size_t>(z) * n + y) * n + x;
     *o = accumulate ? *o + acc : acc;
 }
