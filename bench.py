@@ -35,8 +35,8 @@ sys.path.insert(0, ROOT)
 
 METRIC = "backprojection GUPS + projections/s, FP32 vs BF16-proj at <=1e-3 rel RMS vs FP64"
 # DRAM bytes (read + write) of one k_fdk_staged<f32, exact> launch, measured with ncu on this
-# workload (detector width -> bytes): 1024^3 268.61 GB + 5.51 GB, 256^3 69.8 MB + 39.7 MB
-MEASURED_TRAFFIC = {1024: 274.12e9, 256: 109.5e6}
+# workload (detector width -> bytes): 1024^3 547.23 GB + 6.27 GB, 256^3 69.9 MB + 41.8 MB
+MEASURED_TRAFFIC = {1024: 553.50e9, 256: 111.7e6}
 
 
 def workload(small: bool):

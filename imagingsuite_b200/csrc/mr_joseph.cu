@@ -67,13 +67,15 @@ __device__ __forceinline__ void major_range(float beta, float alpha, int n, int 
 }
 
 // One thread per ray (r, z, t). vol: [nz][n][n] slices; volt: the same slices transposed
-// ([nz][x][y]), so that both stepping directions read consecutive minor positions.
+// ([nz][x][y]), so that both stepping directions read consecutive minor positions. The grid
+// runs the angles of a slice together (t = blockIdx.y, z = blockIdx.z), so the resident
+// blocks read a few slices from L2 instead of streaming the volume from DRAM per angle.
 __global__ void __launch_bounds__(128) k_forward(const float *__restrict__ vol, const float *__restrict__ volt, int n,
                                                  int nz, const Angle *__restrict__ ang, int nu, float centre,
                                                  float tan_tilt, float pivot, float *__restrict__ proj,
                                                  float *__restrict__ dproj)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x, z = blockIdx.y, t = blockIdx.z;
+    const int r = blockIdx.x * blockDim.x + threadIdx.x, t = blockIdx.y, z = blockIdx.z;
     if (r >= nu) return;
     const Angle g = ang[t];
     const float cz = __fmaf_rn(tan_tilt, static_cast<float>(z) - pivot, centre);
@@ -239,7 +241,7 @@ mr_status mr_joseph_forward(const float *vol_d, float *volt_d, size_t n, size_t 
     k_transpose<<<tg, tb, 0, s>>>(vol_d, static_cast<int>(n), volt_d);
     mr_status st = check_launch("k_transpose");
     if (st != MR_OK) return st;
-    dim3 grid(div_up(nu, 128), static_cast<unsigned>(nz), static_cast<unsigned>(nproj));
+    dim3 grid(div_up(nu, 128), static_cast<unsigned>(nproj), static_cast<unsigned>(nz));
     k_forward<<<grid, 128, 0, s>>>(vol_d, volt_d, static_cast<int>(n), static_cast<int>(nz),
                                    reinterpret_cast<const Angle *>(params_d), static_cast<int>(nu), centre, tan_tilt,
                                    pivot, proj_d, dproj_d);
