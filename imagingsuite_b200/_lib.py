@@ -71,6 +71,8 @@ _PROTOS = {
                               c_void]),
     "mr_fdk_backproject": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_int,
                                    c_void, c_int, c_int, c_int, c_void, c_void]),
+    "mr_fdk_backproject_slab": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_int,
+                                        c_void, c_int, c_int, c_int, c_size, c_size, c_void, c_void]),
     "mr_fdk_box": (c_int, [P_float, P_float, P_float, c_size, c_size, c_size, c_int, P_int, P_int]),
     "mr_fdk_maps64": (c_int, [ctypes.POINTER(FdkGeom), c_size, c_size, P_float, c_size, P_double]),
     "mr_fdk_box_maps": (c_int, [P_double, c_size, c_size, c_size, c_int, P_int, P_int]),

@@ -20,7 +20,7 @@ namespace mr {
 
 mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
                          const float *xip_d, const float *yip_d, const float *zip_d, const uint32_t *mask_d,
-                         int accumulate, float *vol_d, int bw, int bh, cudaStream_t s);
+                         int accumulate, int kbegin, int kend, float *vol_d, int bw, int bh, cudaStream_t s);
 
 static const float kFPi = 3.1415926535897932384626f;
 static const double kDPi = 3.1415926535897932384626433832795028841971693993751;
@@ -120,19 +120,19 @@ __global__ void __launch_bounds__(128) k_bp_parallel(const void *__restrict__ pr
 // ------------------------------------------------------------------ FDK
 
 // FDKbp_single::project_volume_onto_image_c main loop (fdkbp_single.cpp:488-525) with
-// get_pixel_value_c (:641-683); i, j, k index cbct_volume (x fastest). The result is
-// stored at the final position of FdkReconBase::Process (fdkreconbase.cpp:259-270):
-// volume[nv-1-k][j][nu-1-i].
+// get_pixel_value_c (:641-683); i, j, k index cbct_volume (x fastest), k in [kbegin, kend).
+// The result is stored at the final position of FdkReconBase::Process
+// (fdkreconbase.cpp:259-270): volume[nv-1-k][j][nu-1-i].
 template <int DT, int CZ>
 __global__ void __launch_bounds__(128) k_fdk(const void *__restrict__ proj, const float *__restrict__ scale, int nu,
                                              int nv, int nproj, const float *__restrict__ xip,
                                              const float *__restrict__ yip, const float *__restrict__ zip,
                                              int uniform_z, const uint32_t *__restrict__ mask, int accumulate,
-                                             float *__restrict__ vol)
+                                             int kend, int kbegin, float *__restrict__ vol)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int k0 = blockIdx.z * CZ;
+    const int k0 = kbegin + blockIdx.z * CZ;
     if (i >= nu || j >= nu) return;
     const size_t plane = static_cast<size_t>(nu) * nu;
     const size_t out_xy = static_cast<size_t>(j) * nu + (nu - 1 - i);
@@ -140,7 +140,7 @@ __global__ void __launch_bounds__(128) k_fdk(const void *__restrict__ proj, cons
 #pragma unroll
     for (int c = 0; c < CZ; ++c) {
         const int k = k0 + c;
-        acc[c] = (accumulate && k < nv) ? vol[static_cast<size_t>(nv - 1 - k) * plane + out_xy] : 0.0f;
+        acc[c] = (accumulate && k < kend) ? vol[static_cast<size_t>(nv - 1 - k) * plane + out_xy] : 0.0f;
     }
     const bool inside = static_cast<uint32_t>(i) > mask[2 * j] && static_cast<uint32_t>(i) <= mask[2 * j + 1];
     if (inside) {
@@ -165,7 +165,7 @@ __global__ void __launch_bounds__(128) k_fdk(const void *__restrict__ proj, cons
 #pragma unroll
                 for (int q = 0; q < CZ; ++q) {
                     const int k = k0 + q;
-                    if (k >= nv) break;
+                    if (k >= kend) break;
                     const float a1 = __fadd_rn(Z[3 * k + 1], y1);
                     const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, x1)), 0.5f);
                     if (r < 0.0f || r >= fh) continue; // value 0: acc + dw2*0 == acc
@@ -177,7 +177,7 @@ __global__ void __launch_bounds__(128) k_fdk(const void *__restrict__ proj, cons
 #pragma unroll
                 for (int q = 0; q < CZ; ++q) {
                     const int k = k0 + q;
-                    if (k >= nv) break;
+                    if (k >= kend) break;
                     const float a0 = __fadd_rn(Z[3 * k], y0);
                     const float a1 = __fadd_rn(Z[3 * k + 1], y1);
                     const float a2 = __fadd_rn(Z[3 * k + 2], y2);
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(128) k_fdk(const void *__restrict__ proj, cons
 #pragma unroll
     for (int c = 0; c < CZ; ++c) {
         const int k = k0 + c;
-        if (k < nv) vol[static_cast<size_t>(nv - 1 - k) * plane + out_xy] = acc[c];
+        if (k < kend) vol[static_cast<size_t>(nv - 1 - k) * plane + out_xy] = acc[c];
     }
 }
 
@@ -528,9 +528,10 @@ mr_status mr_fdk_maps64(const mr_fdk_geom *g, size_t nu, size_t nv, const float 
     return MR_OK;
 }
 
-mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
-                             const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
-                             const uint32_t *mask_d, int box_w, int box_h, int accumulate, float *vol_d, void *stream)
+mr_status mr_fdk_backproject_slab(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
+                                  size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
+                                  const uint32_t *mask_d, int box_w, int box_h, int accumulate, size_t k_begin,
+                                  size_t k_end, float *vol_d, void *stream)
 {
     if (!proj_d || !xip_d || !yip_d || !zip_d || !mask_d || !vol_d)
         return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: null pointer");
@@ -538,30 +539,41 @@ mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d
     if (dtype != MR_F32 && !scale_d) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: 16-bit projections need scale_d");
     if (nu == 0 || nv == 0 || nu > 65536 || nv > 65536) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: unsupported size");
     if (nproj > 0x7fffffff) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: too many projections");
+    if (k_begin > k_end || k_end > nv) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: slice range outside [0, nv]");
+    if (k_begin == k_end) return MR_OK;
     cudaStream_t s = as_stream(stream);
     if (uniform_z && box_w > 0 && box_h > 0 && nproj > 0) {
         mr_status st = fdk_tma_launch(proj_d, dtype, scale_d, nu, nv, nproj, xip_d, yip_d, zip_d, mask_d, accumulate,
-                                      vol_d, box_w, box_h, s);
+                                      static_cast<int>(k_begin), static_cast<int>(k_end), vol_d, box_w, box_h, s);
         if (st != MR_ERR_UNSUPPORTED) return st;
     }
     constexpr int CZ = 8;
     dim3 block(32, 4);
-    dim3 grid(div_up(nu, 32), div_up(nu, 4), div_up(nv, CZ));
+    dim3 grid(div_up(nu, 32), div_up(nu, 4), div_up(k_end - k_begin, CZ));
     const int np = static_cast<int>(nproj), iu = static_cast<int>(nu), iv = static_cast<int>(nv);
+    const int kb = static_cast<int>(k_begin), ke = static_cast<int>(k_end);
     switch (dtype) {
     case MR_F32:
         k_fdk<MR_F32, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, iu, iv, np, xip_d, yip_d, zip_d, uniform_z, mask_d,
-                                                 accumulate, vol_d);
+                                                 accumulate, ke, kb, vol_d);
         break;
     case MR_BF16:
         k_fdk<MR_BF16, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, iu, iv, np, xip_d, yip_d, zip_d, uniform_z, mask_d,
-                                                  accumulate, vol_d);
+                                                  accumulate, ke, kb, vol_d);
         break;
     default:
         k_fdk<MR_F16, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, iu, iv, np, xip_d, yip_d, zip_d, uniform_z, mask_d,
-                                                 accumulate, vol_d);
+                                                 accumulate, ke, kb, vol_d);
     }
     return check_launch("k_fdk");
+}
+
+mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
+                             const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
+                             const uint32_t *mask_d, int box_w, int box_h, int accumulate, float *vol_d, void *stream)
+{
+    return mr_fdk_backproject_slab(proj_d, dtype, scale_d, nu, nv, nproj, xip_d, yip_d, zip_d, uniform_z, mask_d, box_w,
+                                   box_h, accumulate, 0, nv, vol_d, stream);
 }
 
 } // extern "C"

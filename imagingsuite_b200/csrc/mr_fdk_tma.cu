@@ -76,6 +76,7 @@ struct Params {
     int boxbytes;     // per-projection shared buffer, 128-byte multiple
     int rowbytes;     // bw * element size
     int accumulate;
+    int kbegin, kend; // cbct slices backprojected: [kbegin, kend)
     int xalign;       // x coordinate alignment of a TMA load (elements)
 };
 
@@ -377,9 +378,9 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
     Smem<NB, GEO, EXACT> S(smem, P.boxbytes);
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = blockIdx.z * TK;
+    const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = P.kbegin + blockIdx.z * TK;
     const int i = i0 + lane, j = j0 + warp;
-    const int kmax = min(TK, P.nv - k0);
+    const int kmax = min(TK, P.kend - k0);
     const bool valid = i < P.nu && j < P.nu;
     const bool inside = valid && static_cast<uint32_t>(i) > P.mask[2 * j] && static_cast<uint32_t>(i) <= P.mask[2 * j + 1];
     const size_t plane = static_cast<size_t>(P.nu) * P.nu;
@@ -753,7 +754,8 @@ static void box_guess(size_t nu, size_t nv, size_t nproj, int xalign, int &bw, i
 // TMA or the box does not fit shared memory (the caller then uses the plain kernel).
 static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
                                size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d,
-                               const double *maps_d, const uint32_t *mask_d, int accumulate, float *vol_d, int bw,
+                               const double *maps_d, const uint32_t *mask_d, int accumulate, int kbegin, int kend,
+                               float *vol_d, int bw,
                                int bh, cudaStream_t s)
 {
     using namespace fdk2;
@@ -792,8 +794,10 @@ static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const 
     P.boxbytes = static_cast<int>((bw * bh * es + 127) / 128 * 128);
     P.rowbytes = static_cast<int>(bw * es);
     P.accumulate = accumulate;
+    P.kbegin = kbegin;
+    P.kend = kend;
     P.xalign = xalign;
-    dim3 grid(div_up(nu, TI), div_up(nu, TJ), div_up(nv, TK));
+    dim3 grid(div_up(nu, TI), div_up(nu, TJ), div_up(static_cast<size_t>(kend - kbegin), TK));
     auto go = [&](auto kernel, size_t smem) -> mr_status {
         MR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem)));
         kernel<<<grid, THREADS, smem, s>>>(map, P);
@@ -819,10 +823,10 @@ static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const 
 
 mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
                          const float *xip_d, const float *yip_d, const float *zip_d, const uint32_t *mask_d,
-                         int accumulate, float *vol_d, int bw, int bh, cudaStream_t s)
+                         int accumulate, int kbegin, int kend, float *vol_d, int bw, int bh, cudaStream_t s)
 {
     return staged_launch(true, proj_d, dtype, scale_d, nu, nv, nproj, xip_d, yip_d, zip_d, nullptr, mask_d, accumulate,
-                         vol_d, bw, bh, s);
+                         kbegin, kend, vol_d, bw, bh, s);
 }
 
 mr_status fdk_box_for(const float *xip_h, const float *yip_h, const float *zip_h, size_t nu, size_t nv, size_t nproj,
@@ -883,7 +887,7 @@ mr_status mr_fdk_backproject_fast(const void *proj_d, int dtype, const float *sc
         return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_fast: unsupported size");
     if (nproj == 0 || nproj > 0x7fffffff) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_fast: projection count");
     mr_status st = staged_launch(false, proj_d, dtype, scale_d, nu, nv, nproj, nullptr, nullptr, nullptr, maps_d,
-                                 mask_d, accumulate, vol_d, box_w, box_h, as_stream(stream));
+                                 mask_d, accumulate, 0, static_cast<int>(nv), vol_d, box_w, box_h, as_stream(stream));
     if (st == MR_ERR_UNSUPPORTED)
         return fail(MR_ERR_UNSUPPORTED,
                     "mr_fdk_backproject_fast: layout or box not supported (row pitch must be a multiple of 16 bytes, "

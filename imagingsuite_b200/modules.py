@@ -662,9 +662,17 @@ class FDKbp_single(_BackProjectorBase):
             raise ReconException(f"Projection size ({nu}, {nv}) does not match the ROI ({self.SizeU}, {self.SizeV})")
         weights = _float_vector(_get(parameters, "weights"), nproj)
         angles = _float_vector(_get(parameters, "angles"), nproj)
-        dev = projections.device
-        # per-projection geometry depends only on the configuration and the angles: keep the
-        # device copies while they stay the same
+        geo = self.prepare(angles, weights, projections.device)
+        filt, scale = self.ramp_filter(projections, geo)
+        self.backproject(filt, scale, geo)
+        self._first = False
+        return 0
+
+    def prepare(self, angles: np.ndarray, weights: np.ndarray, dev):
+        """Per-projection geometry (partials or FP64 maps, staging box, filter weights) on the
+        device; it depends only on the configuration and the angles, so it is kept while they
+        stay the same."""
+        nu, nv, nproj = self.SizeU, self.SizeV, angles.size
         dtype = _PRECISION[self.precision]
         key = (angles.tobytes(), weights.tobytes(), str(dev), dtype)
         if getattr(self, "_geo_key", None) != key:
@@ -684,28 +692,43 @@ class FDKbp_single(_BackProjectorBase):
             self._geo = (torch.from_numpy(weights).to(dev), *(torch.from_numpy(a).to(dev) for a in (xip, yip, zip_)),
                          s2, sc, uni, (bw.value, bh.value), maps)
             self._geo_key = key
-        w, X, Y, Z, s2, sc, uni, box, maps = self._geo
-        if dtype == L.MR_F32:
-            filt = torch.empty_like(projections)
-            scale = None
-        else:
-            filt = torch.empty(projections.shape, dtype=torch.uint16, device=dev)
-            scale = torch.empty(nproj, dtype=torch.float32, device=dev)
+        return self._geo
+
+    def ramp_filter(self, projections: torch.Tensor, geo, first: int = 0, out=None, scale=None):
+        """FDK ramp filter (mr_fdk_filter) of projections, which are projections first,
+        first+1, ... of the geometry; returns (filtered, per-projection scale or None)."""
+        w, X, Y, Z, s2, sc, uni, box, maps = geo
+        nproj, nv, nu = projections.shape
+        dtype = _PRECISION[self.precision]
+        if out is None:
+            out = torch.empty_like(projections) if dtype == L.MR_F32 else \
+                torch.empty(projections.shape, dtype=torch.uint16, device=projections.device)
+            scale = None if dtype == L.MR_F32 else torch.empty(nproj, dtype=torch.float32, device=projections.device)
+        check(L.lib().mr_fdk_filter(projections.data_ptr(), nu, nv, nproj, w[first:].data_ptr(), s2, sc, dtype,
+                                    out.data_ptr(), _ptr(scale), _stream()))
+        return out, scale
+
+    def backproject(self, filt: torch.Tensor, scale, geo, k_range=None) -> None:
+        """Backprojection of filtered projections into the volume (overwriting it for the first
+        batch of projections, adding afterwards); k_range = (k_begin, k_end) restricts it to
+        those cbct slices (final volume slices nv-1-k), FP32 only."""
+        w, X, Y, Z, s2, sc, uni, box, maps = geo
+        nproj, nv, nu = filt.shape
+        dtype = _PRECISION[self.precision]
         st = _stream()
-        check(L.lib().mr_fdk_filter(projections.data_ptr(), nu, nv, nproj, w.data_ptr(), s2, sc, dtype, filt.data_ptr(),
-                                    _ptr(scale), st))
         box = box if self.staging else (0, 0)
         if maps is not None and box[0] > 0 and nu % 8 == 0:
+            if k_range is not None:
+                raise ReconException("FDKbp_single: slice ranges are supported in FP32 only")
             check(L.lib().mr_fdk_backproject_fast(filt.data_ptr(), dtype, scale.data_ptr(), nu, nv, nproj,
                                                   maps.data_ptr(), self._mask.data_ptr(), box[0], box[1],
                                                   int(not self._first), self.volume.data_ptr(), st))
         else:
-            check(L.lib().mr_fdk_backproject(filt.data_ptr(), dtype, _ptr(scale), nu, nv, nproj, X.data_ptr(),
-                                             Y.data_ptr(), Z.data_ptr(), uni, self._mask.data_ptr(),
-                                             box[0] if maps is None else 0, box[1] if maps is None else 0,
-                                             int(not self._first), self.volume.data_ptr(), st))
-        self._first = False
-        return 0
+            kb, ke = k_range if k_range is not None else (0, nv)
+            check(L.lib().mr_fdk_backproject_slab(filt.data_ptr(), dtype, _ptr(scale), nu, nv, nproj, X.data_ptr(),
+                                                  Y.data_ptr(), Z.data_ptr(), uni, self._mask.data_ptr(),
+                                                  box[0] if maps is None else 0, box[1] if maps is None else 0,
+                                                  int(not self._first), kb, ke, self.volume.data_ptr(), st))
 
     def GetSlice(self, idx: int) -> torch.Tensor:
         if idx >= self.volume.shape[0]:

@@ -47,22 +47,71 @@ class FdkPipeline:
         self.fdk.Process(proj, self._params)
         return self.fdk.GetVolume()
 
-    def _lognorm_into(self, counts):
+    def _lognorm_into(self, counts, out=None):
         from . import _lib as L
 
         nproj, nv, nu = counts.shape
+        out = self._norm_buf if out is None else out
         dl = torch.zeros(1, device=counts.device)
         L.check(L.lib().mr_lognorm_apply(counts.data_ptr(), L.MR_U16, nv * nu, nproj, self.norm.mDark.data_ptr(),
                                          self.norm.mFlatField.data_ptr(), dl.data_ptr(), 1,
                                          int(self.norm.nDCCount > 0), int(self.norm.nOBCount > 0),
-                                         self._norm_buf.data_ptr(), torch.cuda.current_stream().cuda_stream))
-        return self._norm_buf
+                                         out.data_ptr(), torch.cuda.current_stream().cuda_stream))
+        return out
 
-    def run_host(self, counts_host: torch.Tensor, out_host: torch.Tensor, device) -> torch.Tensor:
-        """counts_host: pinned uint16 (nproj, nv, nu); out_host: pinned float32 (nv, nu, nu)."""
-        counts = counts_host.to(device, non_blocking=True)
-        vol = self.run_device(counts)
-        out_host.copy_(vol, non_blocking=True)
+    def run_host(self, counts_host: torch.Tensor, out_host: torch.Tensor, device, chunks: int = 8,
+                 slabs: int = 8) -> torch.Tensor:
+        """counts_host: pinned uint16 (nproj, nv, nu); out_host: pinned float32 (nv, nu, nu).
+
+        FP32: the counts go to the device in `chunks` groups of projections on a copy stream,
+        and FullLogNorm and the ramp filter of a group start as soon as it has landed; the
+        volume is then backprojected in `slabs` blocks of slices (ReconEngine's slice blocks)
+        and each finished block is copied to the host while the next one is computed. Every
+        value equals the one-shot path's. The result is complete when the current stream is
+        synchronised. Other precisions copy, reconstruct and copy back in sequence."""
+        if self.fdk.precision != "fp32":
+            counts = counts_host.to(device, non_blocking=True)
+            vol = self.run_device(counts)
+            out_host.copy_(vol, non_blocking=True)
+            return out_host
+        nproj, nv, nu = counts_host.shape
+        comp = torch.cuda.current_stream(device)
+        if getattr(self, "_copy_stream", None) is None:
+            self._copy_stream = torch.cuda.Stream(device)
+            self._counts_d = torch.empty(counts_host.shape, dtype=torch.uint16, device=device)
+            self._norm_buf = torch.empty(counts_host.shape, dtype=torch.float32, device=device)
+            self._filt_d = torch.empty(counts_host.shape, dtype=torch.float32, device=device)
+        cs, counts, proj, filt = self._copy_stream, self._counts_d, self._norm_buf, self._filt_d
+        geo = self.fdk.prepare(self.angles, self.weights, device)
+        cs.wait_stream(comp)  # buffers are free once the previous work on them is done
+        bounds = [nproj * c // chunks for c in range(chunks + 1)]
+        landed = []
+        with torch.cuda.stream(cs):
+            for a, b in zip(bounds[:-1], bounds[1:]):
+                counts[a:b].copy_(counts_host[a:b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(cs)
+                landed.append(ev)
+        for (a, b), ev in zip(zip(bounds[:-1], bounds[1:]), landed):
+            if b == a:
+                continue
+            comp.wait_event(ev)
+            self._lognorm_into(counts[a:b], proj[a:b])
+            self.fdk.ramp_filter(proj[a:b], geo, first=a, out=filt[a:b])
+        # slabs of cbct slices k (multiples of 32, the backprojector's slice tile); cbct slice k
+        # is final volume slice nv - 1 - k
+        step = max(32, -(-nv // (slabs * 32)) * 32)
+        self.fdk._first = True
+        for k0 in range(0, nv, step):
+            k1 = min(nv, k0 + step)
+            self.fdk.backproject(filt, None, geo, k_range=(k0, k1))
+            done = torch.cuda.Event()
+            done.record(comp)
+            cs.wait_event(done)
+            with torch.cuda.stream(cs):
+                out_host[nv - k1:nv - k0].copy_(self.fdk.volume[nv - k1:nv - k0], non_blocking=True)
+        self.fdk._first = False
+        comp.wait_stream(cs)
         return out_host
 
 

@@ -252,6 +252,15 @@ mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, c
 mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
                              size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
                              const uint32_t *mask_d, int box_w, int box_h, int accumulate, float *vol_d, void *stream);
+/* mr_fdk_backproject for the cbct_volume slices k in [k_begin, k_end) only (final volume
+ * slices nv-1-k; vol_d is still the whole [nv][nu][nu] volume): the slice blocks
+ * ReconEngine reconstructs one at a time (ReconEngine.cpp:954-1008), here used to copy
+ * finished slabs to the host while the next slab is backprojected. Every voxel gets the
+ * value the whole-volume call gives it. */
+mr_status mr_fdk_backproject_slab(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv,
+                                  size_t nproj, const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
+                                  const uint32_t *mask_d, int box_w, int box_h, int accumulate, size_t k_begin,
+                                  size_t k_end, float *vol_d, void *stream);
 /* Shared-memory staging box for mr_fdk_backproject (host): the largest detector footprint
  * (columns box_w, rows box_h) of a 32 x 8 x 32 voxel tile over a sample of the geometry,
  * from the host copies of the partials. With box_w = box_h = 0, or when the projection

@@ -46,6 +46,15 @@ def test_argument_errors_need_no_gpu():
     assert lib.mr_last_error() == b"Could not convert filter string to enum."
     st = lib.mr_projfilter_tables(64, b"hanning", 0.75, 1.0, 1, 0.1, 2, None, None, None, None)
     assert st == L.MR_ERR_ARGUMENT and b"Cut off" in lib.mr_last_error()
+    # slice range outside the volume: rejected before any device access (the pointers are
+    # never dereferenced)
+    fake = 256
+    st = lib.mr_fdk_backproject_slab(fake, L.MR_F32, None, 64, 32, 4, fake, fake, fake, 1, fake, 0, 0, 0, 8, 40, fake,
+                                     None)
+    assert st == L.MR_ERR_ARGUMENT and b"slice range" in lib.mr_last_error()
+    st = lib.mr_fdk_backproject_slab(fake, L.MR_F32, None, 64, 32, 4, fake, fake, fake, 1, fake, 0, 0, 0, 9, 8, fake,
+                                     None)
+    assert st == L.MR_ERR_ARGUMENT
 
 
 @pytest.mark.parametrize("direction", [0, 1])
