@@ -391,7 +391,7 @@ def run_parallel(args, production: bool):
     import torch
 
     from imagingsuite_b200 import modules as M
-    from imagingsuite_b200 import phantom
+    from imagingsuite_b200 import phantom, pipeline
 
     torch.cuda.set_device(0)
     dev = torch.device("cuda", 0)
@@ -481,23 +481,12 @@ def run_parallel(args, production: bool):
     counts_h = counts.cpu().pin_memory()
     out_h = torch.empty(bp.volume.shape, dtype=torch.float32).pin_memory()
 
+    chain = pipeline.ParallelChain(norm, filt, bp, angles, weights, spot=spot if production else None,
+                                   ring=ring if production else None)
+
     def e2e_step():
-        c = counts_h.to(dev, non_blocking=True)
-        nonlocal_counts[0] = c
-        v = step_with(c)
-        out_h.copy_(v, non_blocking=True)
+        chain.run_host(counts_h, out_h, dev)
 
-    def step_with(c):
-        bp.volume.zero_()
-        proj = norm.ProcessCore(c, {})
-        if production:
-            spot.ProcessCore(proj, {})
-            ring.ProcessCore(proj, {})
-        filt.ProcessCore(proj, {}, weights=wdev)
-        bp.Process(proj, params, prefiltered_weights=True)
-        return bp.GetVolume()
-
-    nonlocal_counts = [None]
     te = time_steps(e2e_step, max(1, min(args.steps, 3)), 1, stream, None)
     e2e_steps = max(1, min(args.steps, 3))
     peaks = {}

@@ -63,6 +63,8 @@ _PROTOS = {
                                c_void, c_int, c_float, c_float, c_void, c_void]),
     "mr_bp_parallel_staged": (c_int, [c_void, c_size, c_int, c_void, c_void, c_void, c_void, c_void, c_void, c_size,
                                       c_size, c_size, c_void, c_int, c_float, c_float, c_void, c_void]),
+    "mr_bp_parallel_rows": (c_int, [c_void, c_size, c_int, c_void, c_void, c_void, c_void, c_void, c_void, c_size,
+                                    c_size, c_size, c_void, c_int, c_float, c_float, c_size, c_size, c_void, c_void]),
     "mr_quantize": (c_int, [c_void, c_size, c_size, c_int, c_void, c_void, c_void]),
     "mr_quantize_noalloc": (c_int, [c_void, c_size, c_size, c_int, c_void, c_void, c_void]),
     "mr_fdk_partials": (c_int, [ctypes.POINTER(FdkGeom), c_size, c_size, P_float, c_size, P_float, P_float, P_float,

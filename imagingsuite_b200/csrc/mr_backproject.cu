@@ -34,19 +34,21 @@ __device__ __forceinline__ float sample(const void *base, size_t idx)
 // ------------------------------------------------------------------ parallel beam
 
 // MultiProjectionBPparallel::BackProject (MultiProjBPparallel.cpp:39-170). x1, y1 are the
-// reference's 1-based loop indices; the voxel is vol[y1-1][x1-1][z].
+// reference's 1-based loop indices; the voxel is vol[y1-1][x1-1][z]; rows y1-1 in
+// [ybegin, yend) are processed.
 template <int DT, int CZ>
 __global__ void __launch_bounds__(128) k_bp_parallel(const void *__restrict__ proj, const float *__restrict__ scale,
                                                      const float *__restrict__ weight, const int32_t *__restrict__ index,
                                                      const float *__restrict__ sinv,
                                                      const float *__restrict__ cosv, const float *__restrict__ startu,
                                                      int nproj, int nu, int nv, const uint32_t *__restrict__ mask,
-                                                     int tilt, float toff, float tinc, float *__restrict__ vol)
+                                                     int tilt, float toff, float tinc, int ybegin, int yend,
+                                                     float *__restrict__ vol)
 {
     const int x1 = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int y1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int y1 = ybegin + blockIdx.y * blockDim.y + threadIdx.y + 1;
     const int z0 = blockIdx.z * CZ;
-    if (x1 > nu || y1 > nu) return;
+    if (x1 > nu || y1 > yend) return;
     const uint32_t first = mask[2 * (y1 - 1)], second = mask[2 * (y1 - 1) + 1];
     if (static_cast<uint32_t>(x1) <= first || static_cast<uint32_t>(x1) > second) return;
     const int nz4 = (nv / 4) * 4;
@@ -259,10 +261,14 @@ mr_status mr_bp_parallel_tilt(float tiltangle, float tiltpivot, size_t roi_y0, f
     return MR_OK;
 }
 
-mr_status mr_bp_parallel(const void *proj_d, int dtype, const float *scale_d, const float *weight_d,
-                         const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
-                         size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt, float tiltoffset,
-                         float tiltinc, float *vol_d, void *stream)
+} // extern "C"
+
+namespace mr {
+// mr_bp_parallel for the volume rows [y_begin, y_end) (y_end <= nu, checked by the callers)
+mr_status bp_parallel_rows(const void *proj_d, int dtype, const float *scale_d, const float *weight_d,
+                           const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
+                           size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt,
+                           float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, float *vol_d, void *stream)
 {
     if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
         return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: null pointer");
@@ -270,26 +276,40 @@ mr_status mr_bp_parallel(const void *proj_d, int dtype, const float *scale_d, co
     if (dtype != MR_F32 && !scale_d) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: 16-bit projections need scale_d");
     if (nu < 2 || nu > 65536 || nv > 65536) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: unsupported size");
     if (nproj > 0x7fffffff) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: too many projections");
-    if (nproj == 0 || nv < 4) return MR_OK;
+    if (y_begin > y_end || y_end > nu) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: row range outside [0, nu]");
+    if (nproj == 0 || nv < 4 || y_begin == y_end) return MR_OK;
     constexpr int CZ = 8;
     dim3 block(32, 4);
-    dim3 grid(div_up(nu, 32), div_up(nu, 4), div_up(nv, CZ));
+    dim3 grid(div_up(nu, 32), div_up(y_end - y_begin, 4), div_up(nv, CZ));
     cudaStream_t s = as_stream(stream);
     const int np = static_cast<int>(nproj), iu = static_cast<int>(nu), iv = static_cast<int>(nv);
+    const int yb = static_cast<int>(y_begin), ye = static_cast<int>(y_end);
     switch (dtype) {
     case MR_F32:
         k_bp_parallel<MR_F32, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, np, iu, iv,
-                                                         mask_d, correcttilt, tiltoffset, tiltinc, vol_d);
+                                                         mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, vol_d);
         break;
     case MR_BF16:
         k_bp_parallel<MR_BF16, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, np, iu, iv,
-                                                          mask_d, correcttilt, tiltoffset, tiltinc, vol_d);
+                                                          mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, vol_d);
         break;
     default:
         k_bp_parallel<MR_F16, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, np, iu, iv,
-                                                         mask_d, correcttilt, tiltoffset, tiltinc, vol_d);
+                                                         mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, vol_d);
     }
     return check_launch("k_bp_parallel");
+}
+} // namespace mr
+
+extern "C" {
+
+mr_status mr_bp_parallel(const void *proj_d, int dtype, const float *scale_d, const float *weight_d,
+                         const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
+                         size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt, float tiltoffset,
+                         float tiltinc, float *vol_d, void *stream)
+{
+    return bp_parallel_rows(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
+                            correcttilt, tiltoffset, tiltinc, 0, nu, vol_d, stream);
 }
 
 // FDKbp_single::getProjMatrix (fdkbp_single.cpp:83-255), float arithmetic as written there.

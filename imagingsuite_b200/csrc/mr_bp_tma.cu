@@ -56,6 +56,7 @@ struct Params {
     const uint32_t *mask;
     float *vol;
     int nproj, nu, nv, nz4;
+    int ybegin, yend; // volume rows y1 - 1 in [ybegin, yend)
 };
 
 struct Smem {
@@ -108,10 +109,10 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
     extern __shared__ __align__(1024) unsigned char smem[];
     Smem S(smem);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    const int i0 = blockIdx.x * TX, j0 = P.ybegin + blockIdx.y * TY, z0 = blockIdx.z * TZ;
     const int x1 = i0 + lane + 1, y1 = j0 + warp + 1;
     const int zmax = min(TZ, P.nz4 - z0);
-    const bool valid = x1 <= P.nu && y1 <= P.nu;
+    const bool valid = x1 <= P.nu && y1 <= P.yend;
     const bool inside = valid && static_cast<uint32_t>(x1) > P.mask[2 * (y1 - 1)] &&
                         static_cast<uint32_t>(x1) <= P.mask[2 * (y1 - 1) + 1];
     float *col = P.vol + (static_cast<size_t>(valid ? y1 - 1 : 0) * P.nu + (valid ? x1 - 1 : 0)) * P.nv + z0;
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
     }
     __syncthreads();
 
-    const int xa = i0 + 1, xb = min(i0 + TX, P.nu), ya = j0 + 1, yb = min(j0 + TY, P.nu);
+    const int xa = i0 + 1, xb = min(i0 + TX, P.nu), ya = j0 + 1, yb = min(j0 + TY, P.yend);
     const int nbatch = (P.nproj + NB - 1) / NB;
 
     // Geometry of batch s into geometry buffer gb (cp.async by all threads, three batches
@@ -320,7 +321,8 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
 // Returns MR_ERR_UNSUPPORTED when staging does not apply (the caller uses the plain kernel).
 mr_status bp_parallel_staged_launch(const float *proj_d, size_t nslabs, const float *weight_d, const int32_t *index_d,
                                     const float *sin_d, const float *cos_d, const float *startu_d, size_t nproj,
-                                    size_t nu, size_t nv, const uint32_t *mask_d, float *vol_d, cudaStream_t s)
+                                    size_t nu, size_t nv, const uint32_t *mask_d, size_t y_begin, size_t y_end,
+                                    float *vol_d, cudaStream_t s)
 {
     using namespace bp2;
     if ((nu * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(proj_d) % 16) != 0 || nv < 4 || nslabs == 0 ||
@@ -350,8 +352,10 @@ mr_status bp_parallel_staged_launch(const float *proj_d, size_t nslabs, const fl
     P.nu = static_cast<int>(nu);
     P.nv = static_cast<int>(nv);
     P.nz4 = static_cast<int>((nv / 4) * 4);
+    P.ybegin = static_cast<int>(y_begin);
+    P.yend = static_cast<int>(y_end);
     const size_t smem = Smem::bytes();
-    dim3 grid(div_up(nu, TX), div_up(nu, TY), div_up(static_cast<size_t>(P.nz4), TZ));
+    dim3 grid(div_up(nu, TX), div_up(y_end - y_begin, TY), div_up(static_cast<size_t>(P.nz4), TZ));
     if (weight_d) {
         MR_CUDA_TRY(cudaFuncSetAttribute(k_bp_par_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
         k_bp_par_staged<true><<<grid, THREADS, smem, s>>>(map, P);
@@ -362,9 +366,36 @@ mr_status bp_parallel_staged_launch(const float *proj_d, size_t nslabs, const fl
     return check_launch("k_bp_par_staged");
 }
 
+// mr_backproject.cu: the direct-load kernel for a range of volume rows
+mr_status bp_parallel_rows(const void *proj_d, int dtype, const float *scale_d, const float *weight_d,
+                           const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
+                           size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt,
+                           float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, float *vol_d, void *stream);
+
 } // namespace mr
 
 using namespace mr;
+
+extern "C" mr_status mr_bp_parallel_rows(const void *proj_d, size_t nslabs, int dtype, const float *scale_d,
+                                         const float *weight_d, const int32_t *index_d, const float *sin_d,
+                                         const float *cos_d, const float *startu_d, size_t nproj, size_t nu, size_t nv,
+                                         const uint32_t *mask_d, int correcttilt, float tiltoffset, float tiltinc,
+                                         size_t y_begin, size_t y_end, float *vol_d, void *stream)
+{
+    if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
+        return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: null pointer");
+    if (y_begin > y_end || y_end > nu) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: row range outside [0, nu]");
+    if (dtype == MR_F32 && !correcttilt && nproj > 0 && nproj <= 0x7fffffff && nu >= 2 && nu <= 65536 && nv <= 65536 &&
+        y_begin < y_end) {
+        if (!index_d && nslabs < nproj) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: nslabs below nproj");
+        mr_status st = bp_parallel_staged_launch(static_cast<const float *>(proj_d), nslabs, weight_d, index_d, sin_d,
+                                                 cos_d, startu_d, nproj, nu, nv, mask_d, y_begin, y_end, vol_d,
+                                                 as_stream(stream));
+        if (st != MR_ERR_UNSUPPORTED) return st;
+    }
+    return bp_parallel_rows(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
+                            correcttilt, tiltoffset, tiltinc, y_begin, y_end, vol_d, stream);
+}
 
 extern "C" mr_status mr_bp_parallel_staged(const void *proj_d, size_t nslabs, int dtype, const float *scale_d,
                                            const float *weight_d, const int32_t *index_d, const float *sin_d,
@@ -372,14 +403,6 @@ extern "C" mr_status mr_bp_parallel_staged(const void *proj_d, size_t nslabs, in
                                            const uint32_t *mask_d, int correcttilt, float tiltoffset, float tiltinc,
                                            float *vol_d, void *stream)
 {
-    if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
-        return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: null pointer");
-    if (dtype == MR_F32 && !correcttilt && nproj > 0 && nproj <= 0x7fffffff && nu >= 2 && nu <= 65536 && nv <= 65536) {
-        if (!index_d && nslabs < nproj) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: nslabs below nproj");
-        mr_status st = bp_parallel_staged_launch(static_cast<const float *>(proj_d), nslabs, weight_d, index_d, sin_d,
-                                                 cos_d, startu_d, nproj, nu, nv, mask_d, vol_d, as_stream(stream));
-        if (st != MR_ERR_UNSUPPORTED) return st;
-    }
-    return mr_bp_parallel(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
-                          correcttilt, tiltoffset, tiltinc, vol_d, stream);
+    return mr_bp_parallel_rows(proj_d, nslabs, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv,
+                               mask_d, correcttilt, tiltoffset, tiltinc, 0, nu, vol_d, stream);
 }

@@ -206,8 +206,9 @@ class FullLogNorm:
     def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
         return self.ProcessCore(img, coeff if coeff is not None else {})
 
-    def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
-        """ProcessCore 3D. ``img`` is float32 or uint16 (raw counts); returns float32.
+    def ProcessCore(self, img: torch.Tensor, coeff: dict, out: torch.Tensor | None = None) -> torch.Tensor:
+        """ProcessCore 3D. ``img`` is float32 or uint16 (raw counts); returns float32 (in
+        ``out`` when given, else in place for float32 input or in a new tensor).
         Doses come from ``coeff['dose']`` (text, as the engine passes them) or, when absent,
         are computed on the device over the dose ROI (ProjectionReader::GetProjectionDose)."""
         _require_cuda(img, "projections")
@@ -226,7 +227,10 @@ class FullLogNorm:
         else:
             dl = np.zeros(1, np.float32)
         doselog = torch.from_numpy(dl).to(img.device)
-        out = img if img.dtype == torch.float32 else torch.empty(img.shape, dtype=torch.float32, device=img.device)
+        if out is None:
+            out = img if img.dtype == torch.float32 else torch.empty(img.shape, dtype=torch.float32, device=img.device)
+        elif out.shape != img.shape or out.dtype != torch.float32 or not out.is_contiguous():
+            raise ReconException("FullLogNorm: out must be a contiguous float32 tensor of the projections' shape")
         check(L.lib().mr_lognorm_apply(img.data_ptr(), _DT[img.dtype], nv * nu, nproj, self.mDark.data_ptr(),
                                        self.mFlatField.data_ptr(), doselog.data_ptr(), doselog.numel(),
                                        int(self.nDCCount > 0), int(self.nOBCount > 0), out.data_ptr(), _stream()))
@@ -533,11 +537,13 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         b = self.nProjectionBufferSize
         return k[(k % b) != (b - 1)]
 
-    def Process(self, projections: torch.Tensor, parameters: dict, prefiltered_weights: bool = False) -> int:
+    def Process(self, projections: torch.Tensor, parameters: dict, prefiltered_weights: bool = False,
+                rows: tuple | None = None) -> int:
         """Backprojects projections (nproj, nv, nu) with ``parameters['angles']`` and
         ``parameters['weights']`` (space separated text, as ReconEngine passes them).
         ``prefiltered_weights`` marks projections already multiplied by their weights
-        (the fused filter path); the weights are then not applied again."""
+        (the fused filter path); the weights are then not applied again. ``rows`` = (y0, y1)
+        restricts the backprojection to the volume rows y0 <= y < y1 (mr_bp_parallel_rows)."""
         if self.volume is None:
             raise ReconException("The target matrix is not allocated.")
         _require_cuda(projections, "projections")
@@ -550,20 +556,28 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         sel = self.used_projections(nproj)
         if sel.size == 0:
             return 0
-        ang = np.ascontiguousarray(angles[sel])
-        s = np.empty_like(ang)
-        c = np.empty_like(ang)
-        su = np.empty_like(ang)
-        check(L.lib().mr_bp_parallel_geometry(ang.ctypes.data_as(L.P_float), ang.size, self.SizeU, float(pi.fCenter),
-                                              int(pi.eDirection), s.ctypes.data_as(L.P_float),
-                                              c.ctypes.data_as(L.P_float), su.ctypes.data_as(L.P_float)))
-        toff, tinc = ctypes.c_float(0), ctypes.c_float(0)
-        if pi.bCorrectTilt:
-            check(L.lib().mr_bp_parallel_tilt(float(pi.fTiltAngle), float(pi.fTiltPivotPosition), self._roi[1],
-                                              ctypes.byref(toff), ctypes.byref(tinc)))
         dev = projections.device
-        geo = torch.from_numpy(np.stack([s, c, su, weights[sel]])).to(dev)
-        idx = torch.from_numpy(sel.astype(np.int32)).to(dev)
+        # per-projection geometry on the device, kept while the angles, weights and geometry
+        # settings stay the same (a block backprojected in row ranges reuses it)
+        key = (angles.tobytes(), weights.tobytes(), sel.tobytes(), str(dev), self.SizeU, float(pi.fCenter),
+               int(pi.eDirection), bool(pi.bCorrectTilt), float(pi.fTiltAngle), float(pi.fTiltPivotPosition),
+               self._roi[1])
+        if getattr(self, "_geo_key", None) != key:
+            ang = np.ascontiguousarray(angles[sel])
+            s = np.empty_like(ang)
+            c = np.empty_like(ang)
+            su = np.empty_like(ang)
+            check(L.lib().mr_bp_parallel_geometry(ang.ctypes.data_as(L.P_float), ang.size, self.SizeU,
+                                                  float(pi.fCenter), int(pi.eDirection), s.ctypes.data_as(L.P_float),
+                                                  c.ctypes.data_as(L.P_float), su.ctypes.data_as(L.P_float)))
+            toff, tinc = ctypes.c_float(0), ctypes.c_float(0)
+            if pi.bCorrectTilt:
+                check(L.lib().mr_bp_parallel_tilt(float(pi.fTiltAngle), float(pi.fTiltPivotPosition), self._roi[1],
+                                                  ctypes.byref(toff), ctypes.byref(tinc)))
+            self._geo = (torch.from_numpy(np.stack([s, c, su, weights[sel]])).to(dev),
+                         torch.from_numpy(sel.astype(np.int32)).to(dev), toff, tinc)
+            self._geo_key = key
+        geo, idx, toff, tinc = self._geo
         proj = projections
         dtype = _PRECISION[self.precision]
         scale = None
@@ -572,7 +586,10 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         args = (dtype, _ptr(scale), None if prefiltered_weights else geo[3].data_ptr(), idx.data_ptr(),
                 geo[0].data_ptr(), geo[1].data_ptr(), geo[2].data_ptr(), sel.size, self.SizeU, self.SizeV,
                 self._mask.data_ptr(), int(pi.bCorrectTilt), toff.value, tinc.value, self.volume.data_ptr(), _stream())
-        if self.staging:
+        if rows is not None:
+            check(L.lib().mr_bp_parallel_rows(proj.data_ptr(), nproj, *args[:-2], int(rows[0]), int(rows[1]),
+                                              *args[-2:]))
+        elif self.staging:
             check(L.lib().mr_bp_parallel_staged(proj.data_ptr(), nproj, *args))
         else:
             check(L.lib().mr_bp_parallel(proj.data_ptr(), *args))

@@ -3,9 +3,12 @@ frameworks/tomography/Framework/ReconFramework/src/ReconEngine.cpp:1314-1714, fo
 
 ``FdkPipeline``: FullLogNorm -> FDKbp_single (ramp filter + cone-beam backprojection),
 ``ParallelPipeline``: FullLogNorm -> ProjectionFilterSingle (+ fused projection weights) ->
-MultiProjectionBPparallel. Projections stay in HBM between modules; ``run_host`` is the
-end-to-end form that takes uint16 counts in host memory and returns the volume in host
-memory (one H2D and one D2H copy per block).
+MultiProjectionBPparallel, ``ParallelChain``: the same with MorphSpotClean and
+WaveletRingClean between normalisation and filter, from configured module instances.
+Projections stay in HBM between modules; ``run_host`` is the end-to-end form that takes
+uint16 counts in host memory and returns the volume in host memory, with the copies
+overlapped with the computation (counts in by groups of projections, the volume out by
+blocks of slices or rows while the next block is backprojected).
 """
 from __future__ import annotations
 
@@ -143,3 +146,93 @@ class ParallelPipeline:
         self.filter.ProcessCore(proj, {}, weights=w)
         self.bp.Process(proj, self._params, prefiltered_weights=True)
         return self.bp.GetVolume()
+
+
+class ParallelChain:
+    """ReconEngine's block chain for parallel beam from configured modules: FullLogNorm ->
+    [MorphSpotClean] -> [WaveletRingClean] -> ProjectionFilterSingle (projection weights
+    fused) -> MultiProjectionBPparallel (weights not applied again)."""
+
+    def __init__(self, norm: M.FullLogNorm, filt: M.ProjectionFilterSingle, bp: M.MultiProjectionBPparallel,
+                 angles, weights, spot: M.MorphSpotCleanModule | None = None, ring: M.WaveletRingClean | None = None):
+        self.norm, self.filt, self.bp, self.spot, self.ring = norm, filt, bp, spot, ring
+        self.angles = np.asarray(angles, np.float32)
+        self.weights = np.asarray(weights, np.float32)
+        self._params = {"angles": _text(self.angles), "weights": _text(self.weights)}
+        self._w = None
+        self._copy_stream = None
+
+    def _weights_on(self, device):
+        if self._w is None or self._w.device != device:
+            self._w = torch.from_numpy(self.weights).to(device)
+        return self._w
+
+    def run_device(self, counts: torch.Tensor) -> torch.Tensor:
+        """counts: uint16 (nproj, nv, nu) on the device. Returns the volume (ny, nx, nz)."""
+        self.bp.volume.zero_()
+        proj = self.norm.ProcessCore(counts, {})
+        if self.spot is not None:
+            self.spot.ProcessCore(proj, {})
+        if self.ring is not None:
+            self.ring.ProcessCore(proj, {})
+        self.filt.ProcessCore(proj, {}, weights=self._weights_on(counts.device))
+        self.bp.Process(proj, self._params, prefiltered_weights=True)
+        return self.bp.GetVolume()
+
+    def run_host(self, counts_host: torch.Tensor, out_host: torch.Tensor, device, chunks: int = 2,
+                 blocks: int = 8) -> torch.Tensor:
+        """counts_host: pinned uint16 (nproj, nv, nu); out_host: pinned float32 volume (ny, nx, nz).
+
+        The counts go to the device in `chunks` groups of projections on a copy stream;
+        FullLogNorm and MorphSpotClean (per projection) of a group start as soon as it has
+        landed (few groups: MorphSpotClean runs one image per CTA and needs hundreds of images
+        per launch to fill the GPU). Ring cleaning (per sinogram) and the filter then run on
+        the whole block, and the volume is backprojected in `blocks` blocks of rows
+        (contiguous in the z-fastest layout), each copied to the host while the next one is
+        computed. Blocks below 64 MiB of counts or of volume are not split. Every value equals
+        run_device's. The result is complete when the current stream is synchronised."""
+        nproj, nv, nu = counts_host.shape
+        if counts_host.numel() * 2 < (64 << 20):
+            chunks = 1
+        if out_host.numel() * 4 < (64 << 20):
+            blocks = 1
+        comp = torch.cuda.current_stream(device)
+        if self._copy_stream is None or getattr(self, "_shape", None) != tuple(counts_host.shape):
+            self._copy_stream = torch.cuda.Stream(device)
+            self._counts_d = torch.empty(counts_host.shape, dtype=torch.uint16, device=device)
+            self._proj_d = torch.empty(counts_host.shape, dtype=torch.float32, device=device)
+            self._shape = tuple(counts_host.shape)
+        cs, counts, proj = self._copy_stream, self._counts_d, self._proj_d
+        w = self._weights_on(device)
+        cs.wait_stream(comp)  # the buffers are free once the previous work on them is done
+        bounds = [nproj * c // chunks for c in range(chunks + 1)]
+        landed = []
+        with torch.cuda.stream(cs):
+            for a, b in zip(bounds[:-1], bounds[1:]):
+                counts[a:b].copy_(counts_host[a:b], non_blocking=True)
+                ev = torch.cuda.Event()
+                ev.record(cs)
+                landed.append(ev)
+        for (a, b), ev in zip(zip(bounds[:-1], bounds[1:]), landed):
+            if b == a:
+                continue
+            comp.wait_event(ev)
+            self.norm.ProcessCore(counts[a:b], {}, out=proj[a:b])
+            if self.spot is not None:
+                self.spot.ProcessCore(proj[a:b], {})
+        if self.ring is not None:
+            self.ring.ProcessCore(proj, {})
+        self.filt.ProcessCore(proj, {}, weights=w)
+        ny = self.bp.volume.shape[0]
+        self.bp.volume.zero_()
+        step = max(8, -(-ny // (blocks * 8)) * 8)  # multiples of the backprojector's 8-row tiles
+        for y0 in range(0, ny, step):
+            y1 = min(ny, y0 + step)
+            self.bp.Process(proj, self._params, prefiltered_weights=True, rows=(y0, y1))
+            done = torch.cuda.Event()
+            done.record(comp)
+            cs.wait_event(done)
+            with torch.cuda.stream(cs):
+                out_host[y0:y1].copy_(self.bp.volume[y0:y1], non_blocking=True)
+        comp.wait_stream(cs)
+        return out_host

@@ -207,6 +207,15 @@ mr_status mr_bp_parallel_staged(const void *proj_d, size_t nslabs, int dtype, co
                                 const float *weight_d, const int32_t *index_d, const float *sin_d, const float *cos_d,
                                 const float *startu_d, size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d,
                                 int correcttilt, float tiltoffset, float tiltinc, float *vol_d, void *stream);
+/* mr_bp_parallel_staged for the volume rows y in [y_begin, y_end) only (vol_d is still the
+ * whole [nu][nu][nv] volume; a row block is contiguous in it): used to copy finished row
+ * blocks to the host while the next block is backprojected. Every voxel gets the value the
+ * whole-volume call gives it. */
+mr_status mr_bp_parallel_rows(const void *proj_d, size_t nslabs, int dtype, const float *scale_d,
+                              const float *weight_d, const int32_t *index_d, const float *sin_d, const float *cos_d,
+                              const float *startu_d, size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d,
+                              int correcttilt, float tiltoffset, float tiltinc, size_t y_begin, size_t y_end,
+                              float *vol_d, void *stream);
 
 /* ---------------------------------------------------------------------------------
  * FDK cone-beam backprojection: FDKbp_single
