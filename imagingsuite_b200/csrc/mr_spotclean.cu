@@ -447,16 +447,20 @@ static mr_status launch_rec(int nimg, const float *pad, float sign, int pw, int 
 // so each image's CTA finishes the reconstruction with a worklist. Values are handled as
 // order-preserving integer keys so that the relaxation is one atomicMin (erosion:
 // v[q] = min(v[q], max(g[q], v[p]))) or atomicMax (dilation: v[q] = max(v[q], min(g[q], v[p])))
-// per neighbour. A pixel whose value moved is put on the next iteration's list once (a stamp
-// per pixel and iteration); it then relaxes its neighbours with its current value. When a
+// per neighbour. A pixel whose value moved is put on the next iteration's list (once per
+// move: a pixel moved twice in one iteration is listed twice, and its second visit finds its
+// neighbours already relaxed); it then relaxes its neighbours with its current value. When a
 // list overflows, the next iteration relaxes every pixel from its neighbours instead (the
 // first iteration always does). The reconstruction ends when an iteration moves nothing:
 // every pixel then satisfies the fixpoint equations with all its neighbours, and the fixpoint
 // is unique, so the result equals the reference's whatever the order of the updates.
-// Values are read through L2 (ld.cg), where the atomics resolve.
+// Values are read through L2 (ld.cg), where the atomics resolve. Latency shapes the code: an
+// entry issues all its neighbour loads, then all its atomics, before it looks at any result,
+// and the dense passes handle kUnroll pixels per thread at a time.
 
 constexpr int kFrontThreads = 256;
 constexpr int kMaxIterations = 1 << 22;
+constexpr int kUnroll = 4;
 
 __device__ __forceinline__ int fkey(float f)
 {
@@ -468,98 +472,100 @@ __device__ __forceinline__ float funkey(int k) { return __int_as_float(k >= 0 ? 
 
 template <bool DILATE, bool CONN8>
 __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restrict__ pad, float sign, int pw, int ph,
-                                                            float *__restrict__ vol, int *__restrict__ stamps,
-                                                            int *__restrict__ lists, int cap)
+                                                            float *__restrict__ vol, int *__restrict__ lists, int cap)
 {
     const int t = threadIdx.x;
-    const size_t n = static_cast<size_t>(pw) * ph;
-    const float *g = pad + blockIdx.x * n;
-    int *v = reinterpret_cast<int *>(vol + blockIdx.x * n);
-    int *stamp = stamps + blockIdx.x * n;
+    const int n = pw * ph;
+    const float *g = pad + blockIdx.x * static_cast<size_t>(n);
+    int *v = reinterpret_cast<int *>(vol + blockIdx.x * static_cast<size_t>(n));
     int *cur = lists + blockIdx.x * 2 * static_cast<size_t>(cap), *next = cur + cap;
     __shared__ int count[3];
-    for (size_t i = t; i < n; i += kFrontThreads) {
-        __stcg(v + i, fkey(__int_as_float(__ldcg(v + i))));
-        stamp[i] = 0;
+    // floats -> keys, kUnroll pixels per thread at a time
+    for (int i0 = t; i0 < n; i0 += kUnroll * kFrontThreads) {
+        int k[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int i = i0 + u * kFrontThreads;
+            k[u] = i < n ? fkey(__int_as_float(__ldcg(v + i))) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            if (i0 + u * kFrontThreads < n) __stcg(v + i0 + u * kFrontThreads, k[u]);
     }
     if (t < 3) count[t] = 0;
     __syncthreads();
 
-    // candidate for q from a neighbour value kp; moves v[q] when it improves on it
-    auto relax = [&](int q, int kp, int it) {
-        const int kg = fkey(sign * __ldg(g + q));
-        const int c = DILATE ? min(kg, kp) : max(kg, kp);
-        if (DILATE ? c > __ldcg(v + q) : c < __ldcg(v + q)) {
-            const int old = DILATE ? atomicMax(v + q, c) : atomicMin(v + q, c);
-            if ((DILATE ? c > old : c < old) && atomicExch(stamp + q, it + 1) != it + 1) {
-                const int pos = atomicAdd(&count[it % 3], 1);
-                if (pos < cap) next[pos] = q;
-            }
-        }
-    };
     const int nx[8] = {-1, 1, 0, 0, -1, 1, -1, 1}, ny[8] = {0, 0, -1, 1, -1, -1, 1, 1};
     constexpr int NN = CONN8 ? 8 : 4;
+    auto improves = [](int c, int old) { return DILATE ? c > old : c < old; };
+    auto push = [&](int q, int it) {
+        const int pos = atomicAdd(&count[it % 3], 1);
+        if (pos < cap) next[pos] = q;
+    };
 
     bool dense = true;
     int nf = 0, it = 0;
     for (; it < kMaxIterations; ++it) {
         if (dense) {
-            // every pixel from the extreme of its neighbours
-            for (size_t i = t; i < n; i += kFrontThreads) {
-                const int y = static_cast<int>(i / pw), x = static_cast<int>(i % pw);
-                int kn = DILATE ? INT_MIN : INT_MAX;
+            // every pixel from the extreme of its neighbours, kUnroll pixels at a time
+            for (int i0 = t; i0 < n; i0 += kUnroll * kFrontThreads) {
+                int c[kUnroll], kv[kUnroll];
 #pragma unroll
-                for (int k = 0; k < NN; ++k) {
-                    const int qx = x + nx[k], qy = y + ny[k];
-                    if (qx < 0 || qx >= pw || qy < 0 || qy >= ph) continue;
-                    const int kq = __ldcg(v + static_cast<size_t>(qy) * pw + qx);
-                    kn = DILATE ? max(kn, kq) : min(kn, kq);
-                }
-                relax(static_cast<int>(i), kn, it);
-            }
-        } else {
-            // all neighbour loads of an entry are issued before its first compare (one round
-            // trip to L2 per entry); U > 1 entries per thread at a time measured slower (registers)
-            constexpr int U = 1;
-            for (int e0 = t; e0 < nf; e0 += U * kFrontThreads) {
-                int p[U], kp[U], kg[U][NN], kv[U][NN];
-                unsigned ok[U];
-#pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int e = e0 + u * kFrontThreads;
-                    p[u] = e < nf ? cur[e] : -1;
-                    const int y = p[u] / pw, x = p[u] % pw;
-                    ok[u] = 0;
+                for (int u = 0; u < kUnroll; ++u) {
+                    const int i = i0 + u * kFrontThreads;
+                    const int y = i / pw, x = i % pw;
+                    int kn = DILATE ? INT_MIN : INT_MAX;
 #pragma unroll
                     for (int k = 0; k < NN; ++k) {
                         const int qx = x + nx[k], qy = y + ny[k];
-                        if (p[u] >= 0 && qx >= 0 && qx < pw && qy >= 0 && qy < ph) ok[u] |= 1u << k;
+                        if (i >= n || qx < 0 || qx >= pw || qy < 0 || qy >= ph) continue;
+                        const int kq = __ldcg(v + qy * pw + qx);
+                        kn = DILATE ? max(kn, kq) : min(kn, kq);
                     }
-                    kp[u] = p[u] >= 0 ? __ldcg(v + p[u]) : 0;
+                    const int kg = i < n ? fkey(sign * __ldg(g + i)) : 0;
+                    c[u] = DILATE ? min(kg, kn) : max(kg, kn);
+                    kv[u] = i < n ? __ldcg(v + i) : c[u];
+                }
+                int old[kUnroll];
+#pragma unroll
+                for (int u = 0; u < kUnroll; ++u) {
+                    old[u] = c[u];
+                    if (improves(c[u], kv[u]))
+                        old[u] = DILATE ? atomicMax(v + i0 + u * kFrontThreads, c[u]) : atomicMin(v + i0 + u * kFrontThreads, c[u]);
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u)
+                for (int u = 0; u < kUnroll; ++u)
+                    if (improves(c[u], old[u])) push(i0 + u * kFrontThreads, it);
+            }
+        } else {
+            for (int e = t; e < nf; e += kFrontThreads) {
+                const int p = cur[e];
+                const int y = p / pw, x = p % pw;
+                const int kp = __ldcg(v + p);
+                int c[NN], kv[NN];
+                unsigned ok = 0;
 #pragma unroll
-                    for (int k = 0; k < NN; ++k) {
-                        const int q = p[u] + ny[k] * pw + nx[k];
-                        kg[u][k] = (ok[u] >> k) & 1 ? fkey(sign * __ldg(g + q)) : 0;
-                        kv[u][k] = (ok[u] >> k) & 1 ? __ldcg(v + q) : 0;
+                for (int k = 0; k < NN; ++k) {
+                    const int qx = x + nx[k], qy = y + ny[k];
+                    const bool in = qx >= 0 && qx < pw && qy >= 0 && qy < ph;
+                    const int q = qy * pw + qx;
+                    const int kg = in ? fkey(sign * __ldg(g + q)) : 0;
+                    kv[k] = in ? __ldcg(v + q) : 0;
+                    c[k] = DILATE ? min(kg, kp) : max(kg, kp);
+                    if (in) ok |= 1u << k;
+                }
+                int old[NN];
+#pragma unroll
+                for (int k = 0; k < NN; ++k) {
+                    old[k] = c[k];
+                    if (((ok >> k) & 1) && improves(c[k], kv[k])) {
+                        const int q = p + ny[k] * pw + nx[k];
+                        old[k] = DILATE ? atomicMax(v + q, c[k]) : atomicMin(v + q, c[k]);
                     }
+                }
 #pragma unroll
-                for (int u = 0; u < U; ++u)
-#pragma unroll
-                    for (int k = 0; k < NN; ++k) {
-                        if (!((ok[u] >> k) & 1)) continue;
-                        const int q = p[u] + ny[k] * pw + nx[k];
-                        const int c = DILATE ? min(kg[u][k], kp[u]) : max(kg[u][k], kp[u]);
-                        if (DILATE ? c > kv[u][k] : c < kv[u][k]) {
-                            const int old = DILATE ? atomicMax(v + q, c) : atomicMin(v + q, c);
-                            if ((DILATE ? c > old : c < old) && atomicExch(stamp + q, it + 1) != it + 1) {
-                                const int pos = atomicAdd(&count[it % 3], 1);
-                                if (pos < cap) next[pos] = q;
-                            }
-                        }
-                    }
+                for (int k = 0; k < NN; ++k)
+                    if (((ok >> k) & 1) && improves(c[k], old[k])) push(p + ny[k] * pw + nx[k], it);
             }
         }
         __syncthreads();
@@ -576,7 +582,17 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
     }
     if (it == kMaxIterations && t == 0) atomicExch(&g_msc_error, 2);
     __syncthreads();
-    for (size_t i = t; i < n; i += kFrontThreads) __stcg(v + i, __float_as_int(funkey(__ldcg(v + i))));
+    for (int i0 = t; i0 < n; i0 += kUnroll * kFrontThreads) {
+        int k[kUnroll];
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+            const int i = i0 + u * kFrontThreads;
+            k[u] = i < n ? __ldcg(v + i) : 0;
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u)
+            if (i0 + u * kFrontThreads < n) __stcg(v + i0 + u * kFrontThreads, __float_as_int(funkey(k[u])));
+    }
 }
 
 // Worklist capacity per image (entries); a larger frontier falls back to a dense iteration.
@@ -584,7 +600,7 @@ inline int complete_cap(size_t n) { return static_cast<int>(std::min<size_t>(n, 
 
 template <bool DILATE>
 static mr_status launch_reconstruct(int nimg, const float *pad, float sign, int pw, int ph, int conn8, float *vol,
-                                    int *stamps, int *lists, cudaStream_t s)
+                                    int *lists, cudaStream_t s)
 {
     constexpr int RW = 4;
     const int per = (pw + 32 * RW - 1) / (32 * RW);
@@ -597,8 +613,8 @@ static mr_status launch_reconstruct(int nimg, const float *pad, float sign, int 
     else return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 32 * RW * 33 - 2 * kMargin);
     if (st != MR_OK) return st;
     const int cap = complete_cap(static_cast<size_t>(pw) * ph);
-    if (conn8) k_complete<DILATE, true><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, stamps, lists, cap);
-    else k_complete<DILATE, false><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, stamps, lists, cap);
+    if (conn8) k_complete<DILATE, true><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, lists, cap);
+    else k_complete<DILATE, false><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, lists, cap);
     return check_launch("k_complete");
 }
 
@@ -660,10 +676,11 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     if (pw > 128 * 33) return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 128 * 33 - 2 * kMargin);
     const size_t n = static_cast<size_t>(pw) * ph;
     cudaStream_t s = as_stream(stream);
-    // images per batch: three padded buffers each; up to a quarter of the free device memory,
-    // so that a block of projections is cleaned concurrently (one warp per image)
+    // images per batch: three padded buffers and two worklists each; up to a quarter of the
+    // free device memory, so that a block of projections is cleaned concurrently (one CTA per
+    // image)
     const size_t cap = static_cast<size_t>(complete_cap(n));
-    const size_t per_img = 3 * n * sizeof(float) + (n + 2 * cap) * sizeof(int);
+    const size_t per_img = 3 * n * sizeof(float) + 2 * cap * sizeof(int);
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = size_t(1) << 30;
     const size_t budget = std::max<size_t>(size_t(1) << 30, free_b / 4);
@@ -673,7 +690,7 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     MR_CUDA_TRY(cudaMallocAsync(&scratch, batch * per_img + 4 * batch * sizeof(float), s));
     float *P = scratch, *H = P + batch * n, *K = H + batch * n, *stats = K + batch * n;
     float *fmax = stats, *mn = stats + batch, *mx = stats + 2 * batch;
-    int *stamps = reinterpret_cast<int *>(stats + 4 * batch), *lists = stamps + batch * n;
+    int *lists = reinterpret_cast<int *>(stats + 4 * batch);
     mr_status st = MR_OK;
     for (size_t b0 = 0; b0 < nproj && st == MR_OK; b0 += batch) {
         const int nb = static_cast<int>(std::min(batch, nproj - b0));
@@ -685,16 +702,16 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
         k_minmax<<<nb, 1024, 0, s>>>(P, n, mn, mx);
         if (detect == 0 || detect == 2) { // FillHole: erosion from a max marker
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
-            if ((st = launch_reconstruct<false>(nb, P, 1.0f, pw, ph, conn8, H, stamps, lists, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<false>(nb, P, 1.0f, pw, ph, conn8, H, lists, s)) != MR_OK) break;
         }
         if (detect == 1) { // FillPeaks: forward-scan band replay, then the exact dilation
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, 1.0f, K);
             k_peaks_forward_band<<<div_up(nb, 32), 32, 0, s>>>(P, pw, ph, nb, conn8, mn, K);
-            if ((st = launch_reconstruct<true>(nb, P, 1.0f, pw, ph, conn8, K, stamps, lists, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<true>(nb, P, 1.0f, pw, ph, conn8, K, lists, s)) != MR_OK) break;
         }
         if (detect == 2) { // -FillHole(-padded): erosion of the negated image from marker max(-P) = -min(P)
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, -1.0f, K);
-            if ((st = launch_reconstruct<false>(nb, P, -1.0f, pw, ph, conn8, K, stamps, lists, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<false>(nb, P, -1.0f, pw, ph, conn8, K, lists, s)) != MR_OK) break;
         }
         if ((st = check_launch("morphspotclean reconstruction")) != MR_OK) break;
         k_replace<<<dim3(gx, nb), 256, 0, s>>>(P, detect != 1 ? H : nullptr, detect != 0 ? K : nullptr, w, h, detect,

@@ -95,8 +95,8 @@ mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t n
  * before cleaning; removeinfnan: replace inf/NaN by the largest finite value first.
  * nv must be at least 5 (the reference mirrors 5 rows into its padding and reads outside
  * smaller images). Scratch from the stream-ordered pool: per image in a batch three padded
- * float images, an int stamp per padded pixel and two worklists of 1/16 of them; a batch is
- * as many images as fit in max(1 GiB, a quarter of the free device memory). */
+ * float images and two worklists of 1/16 of their pixels; a batch is as many images as fit
+ * in max(1 GiB, a quarter of the free device memory). */
 mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, int detect, int conn8,
                             const float *th_h, const float *sigma_h, int edge, int clamp, float minlevel,
                             float maxlevel, int removeinfnan, void *stream);
