@@ -461,6 +461,7 @@ static mr_status launch_rec(int nimg, const float *pad, float sign, int pw, int 
 constexpr int kFrontThreads = 256;
 constexpr int kMaxIterations = 1 << 22;
 constexpr int kUnroll = 4;
+constexpr int kChase = 32; // pixels one thread follows within an iteration
 
 __device__ __forceinline__ int fkey(float f)
 {
@@ -539,33 +540,45 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
             }
         } else {
             for (int e = t; e < nf; e += kFrontThreads) {
-                const int p = cur[e];
-                const int y = p / pw, x = p % pw;
-                const int kp = __ldcg(v + p);
-                int c[NN], kv[NN];
-                unsigned ok = 0;
+                // relax the neighbours of p; the thread then follows the first neighbour it moved
+                // (chasing) for up to kChase steps and lists the others it moved, so a change
+                // travels along a path without waiting for a barrier per pixel. Every moved
+                // pixel is relaxed afterwards, by this thread's chase or from the next list.
+                int p = cur[e];
+                for (int step = 0; p >= 0; ++step) {
+                    const int y = p / pw, x = p % pw;
+                    const int kp = __ldcg(v + p);
+                    int c[NN], kv[NN];
+                    unsigned ok = 0;
 #pragma unroll
-                for (int k = 0; k < NN; ++k) {
-                    const int qx = x + nx[k], qy = y + ny[k];
-                    const bool in = qx >= 0 && qx < pw && qy >= 0 && qy < ph;
-                    const int q = qy * pw + qx;
-                    const int kg = in ? fkey(sign * __ldg(g + q)) : 0;
-                    kv[k] = in ? __ldcg(v + q) : 0;
-                    c[k] = DILATE ? min(kg, kp) : max(kg, kp);
-                    if (in) ok |= 1u << k;
-                }
-                int old[NN];
-#pragma unroll
-                for (int k = 0; k < NN; ++k) {
-                    old[k] = c[k];
-                    if (((ok >> k) & 1) && improves(c[k], kv[k])) {
-                        const int q = p + ny[k] * pw + nx[k];
-                        old[k] = DILATE ? atomicMax(v + q, c[k]) : atomicMin(v + q, c[k]);
+                    for (int k = 0; k < NN; ++k) {
+                        const int qx = x + nx[k], qy = y + ny[k];
+                        const bool in = qx >= 0 && qx < pw && qy >= 0 && qy < ph;
+                        const int q = qy * pw + qx;
+                        const int kg = in ? fkey(sign * __ldg(g + q)) : 0;
+                        kv[k] = in ? __ldcg(v + q) : 0;
+                        c[k] = DILATE ? min(kg, kp) : max(kg, kp);
+                        if (in) ok |= 1u << k;
                     }
-                }
+                    int old[NN];
 #pragma unroll
-                for (int k = 0; k < NN; ++k)
-                    if (((ok >> k) & 1) && improves(c[k], old[k])) push(p + ny[k] * pw + nx[k], it);
+                    for (int k = 0; k < NN; ++k) {
+                        old[k] = c[k];
+                        if (((ok >> k) & 1) && improves(c[k], kv[k])) {
+                            const int q = p + ny[k] * pw + nx[k];
+                            old[k] = DILATE ? atomicMax(v + q, c[k]) : atomicMin(v + q, c[k]);
+                        }
+                    }
+                    int follow = -1;
+#pragma unroll
+                    for (int k = 0; k < NN; ++k) {
+                        if (!(((ok >> k) & 1) && improves(c[k], old[k]))) continue;
+                        const int q = p + ny[k] * pw + nx[k];
+                        if (follow < 0 && step + 1 < kChase) follow = q;
+                        else push(q, it);
+                    }
+                    p = follow;
+                }
             }
         }
         __syncthreads();
