@@ -725,12 +725,16 @@ class FDKbp_single(_BackProjectorBase):
                                     out.data_ptr(), _ptr(scale), _stream()))
         return out, scale
 
-    def backproject(self, filt: torch.Tensor, scale, geo, k_range=None) -> None:
+    def backproject(self, filt: torch.Tensor, scale, geo, k_range=None, first: int = 0,
+                    accumulate: bool | None = None) -> None:
         """Backprojection of filtered projections into the volume (overwriting it for the first
-        batch of projections, adding afterwards); k_range = (k_begin, k_end) restricts it to
-        those cbct slices (final volume slices nv-1-k), FP32 only."""
+        batch of projections, adding afterwards, unless `accumulate` says otherwise); filt
+        holds projections first, first+1, ... of the geometry; k_range = (k_begin, k_end)
+        restricts it to those cbct slices (final volume slices nv-1-k), FP32 only."""
         w, X, Y, Z, s2, sc, uni, box, maps = geo
         nproj, nv, nu = filt.shape
+        acc = int(not self._first) if accumulate is None else int(accumulate)
+        X, Y, Z = X[first:first + nproj], Y[first:first + nproj], Z[first:first + nproj]
         dtype = _PRECISION[self.precision]
         st = _stream()
         box = box if self.staging else (0, 0)
@@ -738,14 +742,14 @@ class FDKbp_single(_BackProjectorBase):
             if k_range is not None:
                 raise ReconException("FDKbp_single: slice ranges are supported in FP32 only")
             check(L.lib().mr_fdk_backproject_fast(filt.data_ptr(), dtype, scale.data_ptr(), nu, nv, nproj,
-                                                  maps.data_ptr(), self._mask.data_ptr(), box[0], box[1],
-                                                  int(not self._first), self.volume.data_ptr(), st))
+                                                  maps[first:first + nproj].data_ptr(), self._mask.data_ptr(), box[0],
+                                                  box[1], acc, self.volume.data_ptr(), st))
         else:
             kb, ke = k_range if k_range is not None else (0, nv)
             check(L.lib().mr_fdk_backproject_slab(filt.data_ptr(), dtype, _ptr(scale), nu, nv, nproj, X.data_ptr(),
                                                   Y.data_ptr(), Z.data_ptr(), uni, self._mask.data_ptr(),
                                                   box[0] if maps is None else 0, box[1] if maps is None else 0,
-                                                  int(not self._first), kb, ke, self.volume.data_ptr(), st))
+                                                  acc, kb, ke, self.volume.data_ptr(), st))
 
     def GetSlice(self, idx: int) -> torch.Tensor:
         if idx >= self.volume.shape[0]:

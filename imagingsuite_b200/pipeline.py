@@ -67,11 +67,14 @@ class FdkPipeline:
         """counts_host: pinned uint16 (nproj, nv, nu); out_host: pinned float32 (nv, nu, nu).
 
         FP32: the counts go to the device in `chunks` groups of projections on a copy stream,
-        and FullLogNorm and the ramp filter of a group start as soon as it has landed; the
-        volume is then backprojected in `slabs` blocks of slices (ReconEngine's slice blocks)
-        and each finished block is copied to the host while the next one is computed. Every
-        value equals the one-shot path's. The result is complete when the current stream is
-        synchronised. Other precisions copy, reconstruct and copy back in sequence."""
+        and FullLogNorm, the ramp filter and the backprojection of the first slice block
+        (ReconEngine's slice blocks) for a group start as soon as it has landed; the other
+        `slabs` - 1 blocks are then backprojected with all projections, and each finished block
+        is copied to the host while the next one is computed. A voxel still adds its
+        projections in order (the first block continues its sums from the volume between
+        groups), so every value equals the one-shot path's. The result is complete when the
+        current stream is synchronised. Other precisions copy, reconstruct and copy back in
+        sequence."""
         if self.fdk.precision != "fp32":
             counts = counts_host.to(device, non_blocking=True)
             vol = self.run_device(counts)
@@ -95,19 +98,23 @@ class FdkPipeline:
                 ev = torch.cuda.Event()
                 ev.record(cs)
                 landed.append(ev)
+        # slabs of cbct slices k (multiples of 32, the backprojector's slice tile); cbct slice k
+        # is final volume slice nv - 1 - k
+        step = max(32, -(-nv // (slabs * 32)) * 32)
+        started = False
         for (a, b), ev in zip(zip(bounds[:-1], bounds[1:]), landed):
             if b == a:
                 continue
             comp.wait_event(ev)
             self._lognorm_into(counts[a:b], proj[a:b])
             self.fdk.ramp_filter(proj[a:b], geo, first=a, out=filt[a:b])
-        # slabs of cbct slices k (multiples of 32, the backprojector's slice tile); cbct slice k
-        # is final volume slice nv - 1 - k
-        step = max(32, -(-nv // (slabs * 32)) * 32)
+            self.fdk.backproject(filt[a:b], None, geo, k_range=(0, min(nv, step)), first=a, accumulate=started)
+            started = True
         self.fdk._first = True
         for k0 in range(0, nv, step):
             k1 = min(nv, k0 + step)
-            self.fdk.backproject(filt, None, geo, k_range=(k0, k1))
+            if k0 > 0:
+                self.fdk.backproject(filt, None, geo, k_range=(k0, k1))
             done = torch.cuda.Event()
             done.record(comp)
             cs.wait_event(done)
