@@ -226,6 +226,15 @@ def run_mr(args):
                                            Z.data_ptr(), uni, fdk._mask.data_ptr(), box[0], box[1], 0, vol.data_ptr(), st))
 
     tbp = kernel_time(bp32, stream)
+    # slice serialisation (ReconEngine::Serialize's TIFF16 cast) of the whole volume on the device
+    out16 = torch.empty((nv, nu, nu), dtype=torch.uint16, device=device)
+
+    def ser():
+        L.check(L.lib().mr_slices_u16(vol.data_ptr(), L.MR_PLANE_XY, nu, nu, nv, 0, nv, None, -0.001, 0.004,
+                                      out16.data_ptr(), st))
+
+    tser = kernel_time(ser, stream)
+    del out16
     # precision form: 16-bit filtered projections through the FP64-derived maps
     *_, box16, maps = pipe16.fdk._geo
     q16 = torch.empty((nproj, nv, nu), dtype=torch.uint16, device=device)
@@ -303,6 +312,9 @@ def run_mr(args):
                        "l2": "inputs larger than L2 (2.1 GB counts per step)", "parallelism": f"z-slab x{n}"},
             "projections_per_s": n * nproj * args.steps / t32,
             "backprojection_gups": updates / tbp / 1e9,
+            "serialize_u16": {"ms": tser * 1e3, "achieved_gbs": 6.0 * nu * nu * nv / tser / 1e9,
+                              "frac_of_hbm": 6.0 * nu * nu * nv / tser / 1e9 / hbm,
+                              "note": "mr_slices_u16: float volume -> uint16 slices (4 B read + 2 B written per voxel)"},
             "precision": {
                 "fp64_oracle": f"FP64 geometry and accumulation on 16 seeded slices {sl_np.tolist()} of the final "
                                f"volume (max |value| {vref_max:.4g})",

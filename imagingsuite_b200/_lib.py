@@ -23,6 +23,7 @@ P_double = ctypes.POINTER(ctypes.c_double)
 
 MR_OK, MR_ERR_ARGUMENT, MR_ERR_CUDA, MR_ERR_ALLOCATION, MR_ERR_UNSUPPORTED, MR_ERR_DEVICE = range(6)
 MR_F32, MR_BF16, MR_F16, MR_U16 = 0, 1, 2, 3
+MR_PLANE_XY, MR_PLANE_YZ = 1, 4
 
 
 class FdkGeom(ctypes.Structure):
@@ -82,6 +83,8 @@ _PROTOS = {
                                         c_int, c_void, c_void]),
     "mr_fdk_backproject_f64": (c_int, [c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_size, c_void,
                                        c_void]),
+    "mr_slices_u16": (c_int, [c_void, c_int, c_size, c_size, c_size, c_size, c_size, P_size, c_float, c_float, c_void,
+                              c_void]),
     "mr_joseph_geometry": (c_int, [P_float, c_size, c_size, P_float]),
     "mr_joseph_forward": (c_int, [c_void, c_void, c_size, c_size, c_void, c_size, c_size, c_float, c_float, c_float,
                                   c_void, c_void, c_void]),

@@ -771,3 +771,41 @@ def quantize(proj: torch.Tensor, precision: str):
     check(L.lib().mr_quantize(proj.data_ptr(), per, nproj, _PRECISION[precision], out.data_ptr(), scale.data_ptr(),
                               _stream()))
     return out, scale
+
+
+# ------------------------------------------------------------------- slice serialisation
+
+
+def slices_u16(volume: torch.Tensor, matrix_alignment: str, gray_interval, first: int = 0, count: int | None = None,
+               roi=None) -> torch.Tensor:
+    """The uint16 slices ReconEngine::Serialize writes as TIFF16 (ReconEngine.cpp:576-700 ->
+    kipl::io::WriteImageStack), cast on the device (mr_slices_u16): ``volume`` is a
+    backprojector's volume tensor, ``matrix_alignment`` "MatrixXYZ" (FDK, tensor (nz, ny, nx),
+    slices along z, plane XY) or "MatrixZXY" (parallel beam, tensor (ny, nx, nz), slices
+    along z, plane YZ); ``gray_interval`` = MatrixInfo.fGrayInterval (lo, hi); ``roi`` =
+    MatrixInfo.roi (x0, y0, x1, y1, inclusive) or None. Returns (count, h, w) uint16."""
+    _require_cuda(volume, "volume")
+    if volume.dtype != torch.float32 or volume.dim() != 3 or not volume.is_contiguous():
+        raise ReconException("slices_u16: volume must be a contiguous float32 3-D tensor")
+    if matrix_alignment == "MatrixXYZ":
+        plane = L.MR_PLANE_XY
+        nz, ny, nx = volume.shape
+        d0, d1, d2, nslices, na, nb = nx, ny, nz, nz, nx, ny
+    elif matrix_alignment == "MatrixZXY":
+        plane = L.MR_PLANE_YZ
+        ny, nx, nz = volume.shape
+        d0, d1, d2, nslices, na, nb = nz, nx, ny, nz, nx, ny
+    else:
+        raise ReconException(f"slices_u16: unknown matrix alignment {matrix_alignment}")
+    count = nslices - first if count is None else count
+    if roi is None:
+        w, h, r = na, nb, None
+    else:
+        x0, x1 = sorted((int(roi[0]), int(roi[2])))
+        y0, y1 = sorted((int(roi[1]), int(roi[3])))
+        w, h = x1 - x0 + 1, y1 - y0 + 1
+        r = (ctypes.c_size_t * 4)(*[int(v) for v in roi])
+    out = torch.empty((max(count, 0), h, w), dtype=torch.uint16, device=volume.device)
+    check(L.lib().mr_slices_u16(volume.data_ptr(), plane, d0, d1, d2, first, count, r, float(gray_interval[0]),
+                                float(gray_interval[1]), out.data_ptr(), _stream()))
+    return out

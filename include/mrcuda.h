@@ -314,6 +314,23 @@ mr_status mr_fdk_backproject_f64(const float *proj_d, size_t nu, size_t nv, size
                                  const uint32_t *mask_d, const int *slices_d, size_t nslices, double *out_d,
                                  void *stream);
 
+/* ---------------------------------------------------------------------------------
+ * Slice serialisation to 16 bits: the slices ReconEngine::Serialize (frameworks/tomography/
+ * Framework/ReconFramework/src/ReconEngine.cpp:576-700) writes through kipl::io::
+ * WriteImageStack (core/kipl/kipl/include/io/io_stack.h:114-230) as TIFF16: ExtractSlice
+ * (base/core/textractor.hpp:17-125) of plane XY (MatrixXYZ volumes, FDK) or YZ (MatrixZXY
+ * volumes, parallel beam), then ImageCaster<unsigned short, float>::cast (base/core/
+ * imagecast.hpp:33-52) with the gray interval [lo, hi]:
+ *     out = unsigned short((min(max(v, lo), hi) - lo) * (float(65535) / (hi - lo)))
+ * (float arithmetic, truncation; NaN gives 0). vol_d: the volume as a kipl TImage of dims
+ * (d0, d1, d2), d0 fastest (MatrixXYZ: (nx, ny, nz); MatrixZXY: (nz, nx, ny)); slices
+ * first .. first + count - 1 along the plane's slice axis (d2 for XY, d0 for YZ); roi_h:
+ * NULL or (x0, y0, x1, y1), inclusive, over the slice's two axes; out_d [count][h][w]
+ * uint16 with w, h the slice (or roi) size. Requires lo < hi and dims up to 65535. */
+enum { MR_PLANE_XY = 1, MR_PLANE_YZ = 4 }; /* kipl::base::eImagePlanes values */
+mr_status mr_slices_u16(const float *vol_d, int plane, size_t d0, size_t d1, size_t d2, size_t first, size_t count,
+                        const size_t *roi_h, float lo, float hi, uint16_t *out_d, void *stream);
+
 /* ---- Differentiable parallel-beam projector pair (the Joseph projector of
  * LinearForwardProjector::project, ReconAlgorithms/linearforwardprojector.cpp:15-144, and its
  * exact transpose; the reference has no adjoint and no multi-slice form).

@@ -519,3 +519,43 @@ def ref_joseph_project(slice2d, angles) -> np.ndarray:
     _check_ref(ref().ref_joseph_project(_p(sl), _sz(n), _p(a), _sz(a.size), _p(out)))
     return out
 
+
+
+# ----------------------------------------------------------------- slice serialisation
+
+_U16 = ctypes.POINTER(ctypes.c_uint16)
+
+
+def _slices_args(vol, plane, first, count, roi):
+    v = _f32(vol)  # numpy shape (d2, d1, d0): d0 fastest
+    d2, d1, d0 = v.shape
+    na, nb = (d0, d1) if plane == 1 else (d1, d2)
+    if roi is None:
+        w, h, r = na, nb, None
+    else:
+        x0, x1 = sorted((roi[0], roi[2]))
+        y0, y1 = sorted((roi[1], roi[3]))
+        w, h = x1 - x0 + 1, y1 - y0 + 1
+        r = np.asarray(roi, np.uint64)
+    return v, d0, d1, d2, w, h, r
+
+
+def slices_u16(vol, plane: int, first: int, count: int, lo: float, hi: float, roi=None) -> np.ndarray:
+    """Restated slice serialisation (orc_slices_u16): uint16 slices (count, h, w) of the volume
+    (numpy (d2, d1, d0), d0 fastest), plane 1 = XY or 4 = YZ."""
+    v, d0, d1, d2, w, h, r = _slices_args(vol, plane, first, count, roi)
+    out = np.zeros((count, h, w), np.uint16)
+    rc = orc().orc_slices_u16(_p(v), _sz(d0), _sz(d1), _sz(d2), ctypes.c_int(plane), _sz(first), _sz(count),
+                              None if r is None else _p(r, _SZ), _f(lo), _f(hi), _p(out, _U16))
+    if rc != 0:
+        raise ValueError("orc_slices_u16: bad arguments")
+    return out
+
+
+def ref_slices_u16(vol, plane: int, first: int, count: int, lo: float, hi: float, roi=None) -> np.ndarray:
+    """The reference's ExtractSlice + ImageCaster<unsigned short, float> on the same volume."""
+    v, d0, d1, d2, w, h, r = _slices_args(vol, plane, first, count, roi)
+    out = np.zeros((count, h, w), np.uint16)
+    _check_ref(ref().ref_slices_u16(_p(v), _sz(d0), _sz(d1), _sz(d2), ctypes.c_int(plane), _sz(first), _sz(count),
+                                    None if r is None else _p(r, _SZ), _f(lo), _f(hi), _p(out, _U16)))
+    return out

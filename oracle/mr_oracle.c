@@ -1309,3 +1309,42 @@ void orc_joseph_adjoint64(const double *proj, size_t n, size_t nz, const float *
         }
     }
 }
+
+/* Slice serialisation: ReconEngine::Serialize (frameworks/tomography/Framework/ReconFramework/
+ * src/ReconEngine.cpp:576-700) -> kipl::io::WriteImageStack (core/kipl/kipl/include/io/
+ * io_stack.h:114-230): each slice cut out by ExtractSlice (base/core/textractor.hpp:17-125,
+ * plane XY = 1 or YZ = 4, optional inclusive ROI, swapped when reversed) and cast by
+ * ImageCaster<unsigned short, float>::cast (base/core/imagecast.hpp:33-52):
+ * scale = float(65535) / (hi - lo); out = (unsigned short)((min(max(v, lo), hi) - lo) * scale)
+ * with std::max / std::min (a NaN passes both; its cast is undefined in C and gives 0 on x86,
+ * which is what is written here). vol: dims (d0, d1, d2), d0 fastest. */
+int orc_slices_u16(const float *vol, size_t d0, size_t d1, size_t d2, int plane, size_t first, size_t count,
+                   const size_t *roi, float lo, float hi, unsigned short *out)
+{
+    const size_t nslices = plane == 1 ? d2 : d0;
+    const size_t na = plane == 1 ? d0 : d1, nb = plane == 1 ? d1 : d2;
+    size_t a0 = 0, b0 = 0, w = na, h = nb;
+    if ((plane != 1 && plane != 4) || first + count > nslices) return -1;
+    if (roi) {
+        const size_t x0 = roi[0] < roi[2] ? roi[0] : roi[2], x1 = roi[0] < roi[2] ? roi[2] : roi[0];
+        const size_t y0 = roi[1] < roi[3] ? roi[1] : roi[3], y1 = roi[1] < roi[3] ? roi[3] : roi[1];
+        if (x1 >= na || y1 >= nb) return -1;
+        a0 = x0;
+        b0 = y0;
+        w = x1 - x0 + 1;
+        h = y1 - y0 + 1;
+    }
+    const float scale = 65535.0f / (hi - lo);
+    for (size_t s = 0; s < count; ++s)
+        for (size_t b = 0; b < h; ++b)
+            for (size_t a = 0; a < w; ++a) {
+                const size_t src = plane == 1 ? ((first + s) * d1 + (b0 + b)) * d0 + (a0 + a)
+                                              : ((b0 + b) * d1 + (a0 + a)) * d0 + (first + s);
+                const float v = vol[src];
+                const float m = v < lo ? lo : v;
+                const float c = hi < m ? hi : m;
+                const float val = (c - lo) * scale;
+                out[(s * h + b) * w + a] = val != val ? 0 : (unsigned short)val;
+            }
+    return 0;
+}

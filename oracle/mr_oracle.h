@@ -101,6 +101,10 @@ void orc_joseph_forward64(const float *vol, size_t n, size_t nz, const float *an
 void orc_joseph_adjoint64(const double *proj, size_t n, size_t nz, const float *angles, size_t nproj, size_t nu,
                           double centre, double tan_tilt, double pivot, double *vol);
 
+/* Slice serialisation to 16 bits (ReconEngine::Serialize -> kipl::io::WriteImageStack). */
+int orc_slices_u16(const float *vol, size_t d0, size_t d1, size_t d2, int plane, size_t first, size_t count,
+                   const size_t *roi, float lo, float hi, unsigned short *out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -36,6 +36,8 @@
 #define protected public
 #define private public
 #include <base/timage.h>
+#include <base/textractor.h>
+#include <base/imagecast.h>
 #include <ReconConfig.h>
 #include <ParameterHandling.h>
 #include <averageimage.h>
@@ -488,6 +490,30 @@ int ref_joseph_project(const float *slice, size_t n, const float *angles, size_t
         LinearForwardProjector fp;
         fp.project(img, a, out);
         std::memcpy(proj, out.GetDataPtr(), n * nangles * sizeof(float));
+    });
+}
+
+// The uint16 slices ReconEngine::Serialize writes as TIFF16 (ReconEngine.cpp:576-700 ->
+// kipl::io::WriteImageStack, io_stack.h:114-230): kipl's own ExtractSlice and the
+// ImageCaster<unsigned short, float> cast that WriteTIFF(src, fname, lo, hi) applies
+// (io_tiff.h:181-200), without the file. plane: kipl::base::eImagePlanes value (1 XY, 4 YZ).
+int ref_slices_u16(const float *vol, size_t d0, size_t d1, size_t d2, int plane, size_t first, size_t count,
+                   const size_t *roi, float lo, float hi, unsigned short *out)
+{
+    return guarded([&] {
+        size_t d[3] = {d0, d1, d2};
+        kipl::base::TImage<float, 3> img(d);
+        std::memcpy(img.GetDataPtr(), vol, d0 * d1 * d2 * sizeof(float));
+        size_t o = 0;
+        for (size_t i = first; i < first + count; ++i) {
+            size_t r[4];
+            if (roi) std::memcpy(r, roi, sizeof(r));
+            kipl::base::TImage<float, 2> sl =
+                kipl::base::ExtractSlice(img, i, static_cast<kipl::base::eImagePlanes>(plane), roi ? r : nullptr);
+            kipl::base::TImage<unsigned short, 2> u = kipl::base::ImageCaster<unsigned short, float, 2>::cast(sl, lo, hi);
+            std::memcpy(out + o, u.GetDataPtr(), u.Size() * sizeof(unsigned short));
+            o += u.Size();
+        }
     });
 }
 

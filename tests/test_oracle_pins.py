@@ -200,3 +200,19 @@ def test_waveletringclean_bit_exact(ref_lib):
     rng = _rng(91)
     proj = rng.standard_normal((80, 3, 70)).astype(np.float32)
     assert np.array_equal(O.waveletringclean(proj, "daub7", 2, 0.1), O.waveletringclean(proj, "daub7", 2, 0.1, use_ref=True))
+
+
+@pytest.mark.parametrize("plane", [1, 4])
+@pytest.mark.parametrize("roi", [None, (2, 1, 9, 6), (9, 6, 2, 1)])
+def test_slices_u16_matches_reference(ref_lib, plane, roi):
+    """Slice serialisation (ExtractSlice + ImageCaster<unsigned short, float>) restated in C,
+    against the reference's own templates: planes XY and YZ, ROIs (also reversed), the clamps
+    at the gray interval, infinities and NaN."""
+    rng = np.random.default_rng(plane * 7 + (0 if roi is None else 1))
+    vol = (rng.standard_normal((12, 10, 14)) * 0.02).astype(np.float32)
+    vol[0, 0, 0], vol[1, 2, 3], vol[2, 3, 4], vol[3, 4, 5] = np.inf, -np.inf, np.nan, 0.05
+    nsl = 12 if plane == 1 else 14
+    for lo, hi in ((-0.03, 0.04), (0.0, 1e-3), (-1.0, 1.0)):
+        got = O.slices_u16(vol, plane, 1, nsl - 2, lo, hi, roi)
+        exp = O.ref_slices_u16(vol, plane, 1, nsl - 2, lo, hi, roi)
+        assert np.array_equal(got, exp)
