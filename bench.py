@@ -487,6 +487,24 @@ def run_parallel(args, production: bool):
     t = time_steps(step, args.steps, args.warmup, stream, None)
     clocks = sampler.stop()
     step(record=True)
+    alt = None
+    if production:
+        # the alternative ring cleaners a configuration can name instead of WaveletRingClean, each
+        # timed alone on the normalised block (in place, CUDA events on the launching stream)
+        blk = norm.ProcessCore(counts, {})
+        basic, mix = M.BasicRingClean(), M.MedianMixRingClean()
+        mix.Configure(cfg, {"threshold": "0.025", "width": "0.0025"})
+        px = float(blk.numel())
+        tb = kernel_time(lambda: basic.ProcessCore(blk, {}), stream)
+        tm = kernel_time(lambda: mix.ProcessCore(blk, {}), stream)
+        alt = {"block": [nproj, nrows, nu],
+               "basicringclean_ms": tb * 1e3, "basicringclean_gbs": 12.0 * px / tb / 1e9,
+               "medianmixringclean_ms": tm * 1e3, "medianmixringclean_gbs": 12.0 * px / tm / 1e9,
+               "medianmixringclean_gpx_s": px / tm / 1e9,
+               "note": "algorithmic bytes 12 B/px for both: BasicRingClean reads the block for the mean, then "
+                       "reads and writes it; MedianMixRingClean reads it for the mean, then reads it for the 5x5 "
+                       "median and writes the mixed value"}
+        del blk
     sel = bp.used_projections(nproj).size
     updates = float(nu) * nu * (4 * (nrows // 4)) * sel
     # end to end: host counts in, host volume out
@@ -530,6 +548,7 @@ def run_parallel(args, production: bool):
                        "projections_backprojected": sel, "l2": "inputs larger than L2" if production else "inputs fit L2"},
             "projections_per_s": nproj * args.steps / t,
             "module_ms": times,
+            **({"alt_ring_cleaners": alt} if alt else {}),
             "backprojection_gups": updates / tbp / 1e9,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                          "traffic": None, "kernel": "k_bp_par_staged",

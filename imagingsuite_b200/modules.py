@@ -381,6 +381,127 @@ class WaveletRingClean:
         return img
 
 
+# ------------------------------------------------------------ alternative ring cleaners
+
+
+def _require_f32(t: torch.Tensor, what: str) -> None:
+    _require_cuda(t, what)
+    if t.dtype != torch.float32:
+        raise ReconException(f"{what} must be float32")
+
+
+def median_filter(img: torch.Tensor, kx: int, ky: int) -> torch.Tensor:
+    """kipl TMedianFilter<float,2> with a kx x ky window (odd sizes up to 5) on one image (nv, nu)
+    or a stack (n, nv, nu); returns a new tensor."""
+    _require_f32(img, "image")
+    src = img
+    nv, nu = src.shape[-2:]
+    n = src.numel() // (nu * nv) if src.numel() else 0
+    out = torch.empty_like(src)
+    st = L.lib().mr_median_filter(src.data_ptr(), nu, nv, n, kx, ky, out.data_ptr(), _stream())
+    if st != L.MR_OK:
+        raise ReconException("median filter failed: " + L.lib().mr_last_error().decode())
+    return out
+
+
+class BasicRingClean:
+    """BasicRingClean (StdPreprocModules/src/BasicRingClean.cpp:17-95): every projection minus
+    (mean projection - its 3x3 median). No parameters. The reference also writes mean.tif,
+    med.tif and diff.tif to its working directory as debug output; these are not written."""
+
+    def __init__(self):
+        pass
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        return 0
+
+    def GetParameters(self) -> dict:
+        return {}
+
+    def SetROI(self, roi) -> bool:
+        return False
+
+    def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
+        return self.ProcessCore(img, coeff if coeff is not None else {})
+
+    def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
+        _require_f32(img, "projections")
+        nproj, nv, nu = img.shape
+        st = L.lib().mr_basicringclean(img.data_ptr(), nu, nv, nproj, _stream())
+        if st != L.MR_OK:
+            raise ReconException("BasicRingClean failed: " + L.lib().mr_last_error().decode())
+        return img
+
+
+class MedianMixRingClean:
+    """MedianMixRingClean (StdPreprocModules/src/MedianMixRingClean.cpp:21-138): weights from
+    a sigmoid of |mean projection - its 3x3 median| (threshold = sigmoid level, width = sigmoid
+    width), then each projection mixed with its 5x5 median by those weights."""
+
+    def __init__(self):
+        self.m_fSigma = float(np.float32(0.0025))
+        self.m_fLambda = float(np.float32(0.025))
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        self.m_fSigma = float(np.float32(_get(parameters, "width")))
+        self.m_fLambda = float(np.float32(_get(parameters, "threshold")))
+        return 0
+
+    def GetParameters(self) -> dict:
+        return {"threshold": "0.025", "width": "0.0025"}
+
+    def SetROI(self, roi) -> bool:
+        return False
+
+    def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
+        return self.ProcessCore(img, coeff if coeff is not None else {})
+
+    def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
+        _require_f32(img, "projections")
+        nproj, nv, nu = img.shape
+        st = L.lib().mr_medianmixringclean(img.data_ptr(), nu, nv, nproj, self.m_fLambda, self.m_fSigma, _stream())
+        if st != L.MR_OK:
+            raise ReconException("MedianMixRingClean failed: " + L.lib().mr_last_error().decode())
+        return img
+
+
+class GammaSpotClean:
+    """GammaSpotCleanModule (StdPreprocModules/src/GammaSpotCleanModule.cpp:10-153). The
+    reference keeps the parameters but its ProcessCore returns without touching the
+    projections (the cleaning calls are commented out there), so this module does the same:
+    the projections pass through unchanged and no device work is issued."""
+
+    def __init__(self):
+        self.m_fSigma = float(np.float32(0.8))
+        self.m_fThreshold3 = 25.0
+        self.m_fThreshold5 = 100.0
+        self.m_fThreshold7 = 400.0
+        self.m_nMedianSize = 3
+
+    def Configure(self, config: ReconConfig, parameters: dict) -> int:
+        self.m_fThreshold3 = float(np.float32(_get(parameters, "threshold3")))
+        self.m_fThreshold5 = float(np.float32(_get(parameters, "threshold5")))
+        self.m_fThreshold7 = float(np.float32(_get(parameters, "threshold7")))
+        self.m_fSigma = float(np.float32(_get(parameters, "sigma")))
+        self.m_nMedianSize = int(_get(parameters, "mediansize"))
+        return 0
+
+    def GetParameters(self) -> dict:
+        return {"threshold3": f"{self.m_fThreshold3:g}", "threshold5": f"{self.m_fThreshold5:g}",
+                "threshold7": f"{self.m_fThreshold7:g}", "sigma": f"{self.m_fSigma:g}",
+                "mediansize": str(self.m_nMedianSize)}
+
+    def SetROI(self, roi) -> bool:
+        return False
+
+    def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
+        return self.ProcessCore(img, coeff if coeff is not None else {})
+
+    def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
+        _require_cuda(img, "projections")
+        return img
+
+
 # ------------------------------------------------------------ ProjectionFilterSingle
 
 

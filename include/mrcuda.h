@@ -122,6 +122,35 @@ mr_status mr_waveletringclean(float *proj_d, size_t nu, size_t nv, size_t nproj,
                               float sigma, void *stream);
 
 /* ---------------------------------------------------------------------------------
+ * Alternative ring cleaners and the kipl median filter they use
+ * mr_median_filter replaces kipl::filters::TMedianFilter<float,2>::operator()
+ *   (core/kipl/kipl/include/filters/core/medianfilter.hpp:28-199, HeapSortMedianFilter with
+ *   ExtractNeighborhood) on nimg images [nimg][nv][nu], out of place: odd kx, ky up to 5,
+ *   nu >= 2*(kx/2), nv >= 2*(ky/2) (at smaller sizes the reference rejects the edge code or
+ *   reads outside the image). The reference's window near the bottom-right corner reaches a few
+ *   values past the image end; those values are taken as 0. Results equal the reference's
+ *   heap-sort median bit for bit, NaN and signed zeros included.
+ * mr_basicringclean replaces BasicRingClean::ProcessCore (frameworks/tomography/Preprocessing/
+ *   StdPreprocModules/src/BasicRingClean.cpp:50-95): every projection minus (mean projection -
+ *   its 3x3 median); nu, nv >= 2. The debug images the reference writes to its working
+ *   directory are not written. Scratch: two images.
+ * mr_medianmixringclean replaces MedianMixRingClean::ProcessCore / ComputeProfile
+ *   (StdPreprocModules/src/MedianMixRingClean.cpp:57-138): w = SigmoidLUT(1024, threshold,
+ *   width)(|mean - 3x3 median of mean|) (5x1 when nv < 3), then every projection becomes
+ *   (1 - w) * p + w * (its 5x5 median; 5x1 when nv < 5). nu >= 4, width > 0. Scratch: two
+ *   images and about 512 MiB of filtered projections.
+ * mr_sigmoid_lut (host) returns kipl::math::SigmoidLUT's table (len floats) and param = lo, hi,
+ *   slope, intercept (core/kipl/kipl/src/math/LUTCollection.cpp:38-82, LUTbase.cpp:12-20).
+ * GammaSpotClean needs no entry point: GammaSpotCleanModule::ProcessCore returns without
+ *   touching the projections (StdPreprocModules/src/GammaSpotCleanModule.cpp:58-68). */
+mr_status mr_median_filter(const float *img_d, size_t nu, size_t nv, size_t nimg, int kx, int ky, float *out_d,
+                           void *stream);
+mr_status mr_basicringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, void *stream);
+mr_status mr_medianmixringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, float threshold, float width,
+                                void *stream);
+mr_status mr_sigmoid_lut(size_t len, float lambda, float sigma, float *lut_h, float *param_h);
+
+/* ---------------------------------------------------------------------------------
  * ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:78-376)
  * Plan = ProjectionFilterBase::Configure/BuildFilter/PreparePadding (:78-93,254-299,364-376):
  *   nfft = 2^(ceil(log2 nu) + paddingdoubler); filter over bins 0..nfft/2-1.

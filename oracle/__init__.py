@@ -559,3 +559,61 @@ def ref_slices_u16(vol, plane: int, first: int, count: int, lo: float, hi: float
     _check_ref(ref().ref_slices_u16(_p(v), _sz(d0), _sz(d1), _sz(d2), ctypes.c_int(plane), _sz(first), _sz(count),
                                     None if r is None else _p(r, _SZ), _f(lo), _f(hi), _p(out, _U16)))
     return out
+
+
+# ------------------------------------------------------- alternative ring cleaners
+
+
+def median_filter(img, kx: int, ky: int, use_ref: bool = False) -> np.ndarray:
+    """kipl TMedianFilter<float,2> with a kx x ky window on one image (h, w): the restatement
+    (orc_median_filter) or, with use_ref, the reference template itself."""
+    a = _f32(img)
+    h, w = a.shape
+    out = np.empty_like(a)
+    if use_ref:
+        _check_ref(ref().ref_median_filter(_p(a), _sz(w), _sz(h), ctypes.c_int(kx), ctypes.c_int(ky), _p(out)))
+    elif orc().orc_median_filter(_p(a), _sz(w), _sz(h), ctypes.c_int(kx), ctypes.c_int(ky), _p(out)) != 0:
+        raise ValueError("orc_median_filter: unsupported size")
+    return out
+
+
+def basicringclean(proj, use_ref: bool = False) -> np.ndarray:
+    """BasicRingClean on projections (n, h, w); returns the cleaned copy."""
+    p = _f32(proj).copy()
+    n, h, w = p.shape
+    if use_ref:
+        _check_ref(ref().ref_basicringclean(_p(p), _sz(w), _sz(h), _sz(n)))
+    elif orc().orc_basicringclean(_p(p), _sz(w), _sz(h), _sz(n)) != 0:
+        raise ValueError("orc_basicringclean: unsupported size")
+    return p
+
+
+def sigmoid_lut(length: int, lam: float, sigma: float, use_ref: bool = False):
+    """kipl SigmoidLUT: (table, (lo, hi, slope, intercept))."""
+    lut = np.empty(length, np.float32)
+    param = np.empty(4, np.float32)
+    if use_ref:
+        _check_ref(ref().ref_sigmoid_lut(_sz(length), _f(lam), _f(sigma), _p(lut), _p(param)))
+    else:
+        orc().orc_sigmoid_lut(_sz(length), _f(lam), _f(sigma), _p(lut), _p(param))
+    return lut, param
+
+
+def medianmixringclean(proj, threshold: float = 0.025, width: float = 0.0025, use_ref: bool = False) -> np.ndarray:
+    """MedianMixRingClean on projections (n, h, w); returns the cleaned copy."""
+    p = _f32(proj).copy()
+    n, h, w = p.shape
+    if use_ref:
+        _check_ref(ref().ref_medianmixringclean(_p(p), _sz(w), _sz(h), _sz(n), _f(threshold), _f(width)))
+    elif orc().orc_medianmixringclean(_p(p), _sz(w), _sz(h), _sz(n), _f(threshold), _f(width)) != 0:
+        raise ValueError("orc_medianmixringclean: unsupported size")
+    return p
+
+
+def ref_gammaspotclean(proj, threshold3=25.0, threshold5=100.0, threshold7=400.0, sigma=0.8, mediansize=3):
+    """The reference's GammaSpotCleanModule on projections (n, h, w); returns its output."""
+    p = _f32(proj).copy()
+    n, h, w = p.shape
+    _check_ref(ref().ref_gammaspotclean(_p(p), _sz(w), _sz(h), _sz(n), _f(threshold3), _f(threshold5),
+                                        _f(threshold7), _f(sigma), ctypes.c_int(mediansize)))
+    return p

@@ -1348,3 +1348,219 @@ int orc_slices_u16(const float *vol, size_t d0, size_t d1, size_t d2, int plane,
             }
     return 0;
 }
+
+/* ------------------------------------------------------- alternative ring cleaners */
+
+/* Heap sort as kipl::heapsort does it (core/kipl/kipl/include/algorithms/sortalg.h:10-45):
+ * the Numerical Recipes sift-down form with 1-based positions and strict '<' comparisons, so
+ * that equal keys of different bits (+0 / -0) and NaN (false in both directions) end where
+ * the reference puts them. */
+static void nr_heapsort(float *a, int n)
+{
+    if (n < 2) return;
+    int l = (n >> 1) + 1, ir = n;
+    for (;;) {
+        float v;
+        if (l > 1) {
+            --l;
+            v = a[l - 1];
+        } else {
+            v = a[ir - 1];
+            a[ir - 1] = a[0];
+            if (--ir == 1) {
+                a[0] = v;
+                break;
+            }
+        }
+        int i = l, j = l + l;
+        while (j <= ir) {
+            if (j < ir && a[j - 1] < a[j]) j++;
+            if (v < a[j - 1]) {
+                a[i - 1] = a[j - 1];
+                i = j;
+                j <<= 1;
+            } else {
+                j = ir + 1;
+            }
+        }
+        a[i - 1] = v;
+    }
+}
+
+/* Element idx of an image of n values; positions at or past its end read 0 (the reference's
+ * edge handling reads a few values past the last row; the zero there is the convention this
+ * restatement and the CUDA path share, and the reference oracle gives its buffers a zeroed
+ * tail so that it reads the same). */
+static float img_at(const float *img, size_t n, long long idx)
+{
+    return idx >= 0 && (size_t)idx < n ? img[idx] : 0.0f;
+}
+
+/* The kx*ky window (row-major) that TMedianFilter::ExtractNeighborhood builds at (x, y)
+ * (core/kipl/kipl/include/filters/core/medianfilter.hpp:52-159): the edge code from the
+ * unsigned comparisons, the per-code ranges (including the bottom-right range that reaches past
+ * the row), the zero start, then the left, right, top and bottom replications in that order.
+ * Returns -1 for the codes the reference rejects. */
+static int kipl_window(const float *img, size_t w, size_t h, int kx, int ky, size_t x, size_t y, float *win)
+{
+    const int hx = kx >> 1, hy = ky >> 1;
+    const int code = (x < (size_t)hx) + 2 * ((w - (size_t)hx - 1) < x) + 4 * (y < (size_t)hy) +
+                     8 * ((h - (size_t)hy - 1) < y);
+    long long sx = -hx, ex = kx - hx, sy = -hy, ey = ky - hy;
+    const long long rx = (long long)kx - hx - (long long)(w - x), ry = (long long)ky - hy - (long long)(h - y);
+    switch (code) {
+    case 1: sx = -(long long)x; break;
+    case 2: ex = rx; break;
+    case 3: case 7: return -1;
+    case 4: sy = -(long long)y; break;
+    case 5: sx = -(long long)x; sy = -(long long)y; break;
+    case 6: ex = rx; sy = -(long long)y; break;
+    case 8: ey = ry; break;
+    case 9: sx = -(long long)x; ey = ry; break;
+    case 10: ey = ry; ex = rx + 1; break;
+    default: break;
+    }
+    const size_t n = w * h;
+    for (int i = 0; i < kx * ky; ++i) win[i] = 0.0f;
+    const long long base = (long long)(y * w + x);
+    for (long long dy = sy; dy < ey; ++dy)
+        for (long long dx = sx; dx < ex; ++dx)
+            win[(dy + hy) * kx + (dx + hx)] = img_at(img, n, base + dy * (long long)w + dx);
+    if (code & 1)
+        for (int r = 0; r < ky; ++r)
+            for (long long d = sx - 1, s = sx; d >= -hx; --d, ++s) win[r * kx + d + hx] = win[r * kx + s + hx];
+    if (code & 2)
+        for (int r = 0; r < ky; ++r)
+            for (long long s = ex - 1, d = ex; d < kx - hx; --s, ++d) win[r * kx + d + hx] = win[r * kx + s + hx];
+    if (code & 4)
+        for (long long d = sy - 1, s = sy; d >= -hy; --d, ++s)
+            for (int c = 0; c < kx; ++c) win[(d + hy) * kx + c] = win[(s + hy) * kx + c];
+    if (code & 8)
+        for (long long s = ey - 1, d = ey; d < ky - hy; --s, ++d)
+            for (int c = 0; c < kx; ++c) win[(d + hy) * kx + c] = win[(s + hy) * kx + c];
+    return code;
+}
+
+/* kipl::filters::TMedianFilter<float,2>::operator() with odd kx, ky (HeapSortMedianFilter,
+ * medianfilter.hpp:173-199, and kipl::math::median, math/core/median.hpp:10-22): per pixel the
+ * window above, heap-sorted, middle element. Needs w >= 2*(kx/2) and h >= 2*(ky/2), the sizes
+ * at which the reference reads only inside the image and the value-past-the-end above. */
+int orc_median_filter(const float *img, size_t w, size_t h, int kx, int ky, float *out)
+{
+    if (kx < 1 || ky < 1 || !(kx & 1) || !(ky & 1) || kx * ky > 49 || w < 1 || h < 1 ||
+        w < (size_t)(2 * (kx >> 1)) || h < (size_t)(2 * (ky >> 1)))
+        return -1;
+    float win[49];
+    for (size_t y = 0; y < h; ++y)
+        for (size_t x = 0; x < w; ++x) {
+            if (kipl_window(img, w, h, kx, ky, x, y, win) < 0) return -1;
+            nr_heapsort(win, kx * ky);
+            out[y * w + x] = win[(kx * ky) / 2];
+        }
+    return 0;
+}
+
+/* Mean projection of n projections of npix values, accumulated in projection order:
+ * from_zero = 0 starts from a copy of the first (BasicRingClean.cpp:56-63), 1 from zero
+ * (MedianMixRingClean.cpp:113-121); then times 1.0f / n. */
+static void mean_projection(const float *proj, size_t npix, size_t n, int from_zero, float *mean)
+{
+    size_t i0 = 0;
+    if (from_zero) {
+        for (size_t j = 0; j < npix; ++j) mean[j] = 0.0f;
+    } else {
+        memcpy(mean, proj, npix * sizeof(float));
+        i0 = 1;
+    }
+    for (size_t i = i0; i < n; ++i)
+        for (size_t j = 0; j < npix; ++j) mean[j] += proj[i * npix + j];
+    const float scale = 1.0f / (float)n;
+    for (size_t j = 0; j < npix; ++j) mean[j] *= scale;
+}
+
+/* BasicRingClean::ProcessCore (frameworks/tomography/Preprocessing/StdPreprocModules/src/
+ * BasicRingClean.cpp:50-95): mean projection, its 3x3 median, and every projection minus
+ * (mean - median). The debug images the reference writes (mean.tif, med.tif, diff.tif in the
+ * working directory) are not part of the result. Projections [n][h][w], in place. */
+int orc_basicringclean(float *proj, size_t w, size_t h, size_t n)
+{
+    if (w < 2 || h < 2) return -1;
+    if (n == 0) return 0;
+    const size_t npix = w * h;
+    float *mean = (float *)malloc(npix * sizeof(float)), *med = (float *)malloc(npix * sizeof(float));
+    mean_projection(proj, npix, n, 0, mean);
+    orc_median_filter(mean, w, h, 3, 3, med);
+    for (size_t j = 0; j < npix; ++j) med[j] = mean[j] - med[j];
+    for (size_t i = 0; i < n; ++i)
+        for (size_t j = 0; j < npix; ++j) proj[i * npix + j] -= med[j];
+    free(mean);
+    free(med);
+    return 0;
+}
+
+/* kipl::math::SigmoidLUT (core/kipl/kipl/src/math/LUTCollection.cpp:38-82) on LUTbase
+ * (core/kipl/kipl/src/math/LUTbase.cpp:12-20): limits from epsilon = sigma * 1e-3 with the
+ * double log the reference calls, slope (len - 1) / (hi - lo) and intercept -slope * lo + 0.5 in
+ * float, entries 1 / (1 + exp((lambda - x) / sigma)) in double stored as float with x stepping
+ * by 1 / slope in float, first entry 0 and last 1. param: lo, hi, slope, intercept. */
+void orc_sigmoid_lut(size_t len, float lambda, float sigma, float *lut, float *param)
+{
+    const float eps = sigma * 1e-3f;
+    const float lo = (float)((double)lambda - (double)sigma * log((double)(1.0f / eps)));
+    const float hi = (float)((double)lambda - (double)sigma * log((double)(1.0f / (1.0f - eps) - 1.0f)));
+    const float slope = (float)(len - 1) / (hi - lo);
+    const float intercept = -slope * lo + 0.5f;
+    const float invwidth = 1.0f / sigma, delta = 1.0f / slope;
+    float x = lo;
+    for (size_t i = 0; i < len; ++i, x += delta) lut[i] = (float)(1.0f / (1.0f + exp((double)((lambda - x) * invwidth))));
+    lut[0] = 0.0f;
+    lut[len - 1] = 1.0f;
+    param[0] = lo;
+    param[1] = hi;
+    param[2] = slope;
+    param[3] = intercept;
+}
+
+/* LUTbase::BasicLUT (LUTbase.cpp:57-75) for one value. Where the reference's index leaves the
+ * table (a NaN value, or a cancellation in slope * value + intercept when lambda is far larger
+ * than the width; the reference then reads past its table) the index is clamped to it. */
+static float lut_apply(const float *lut, size_t len, const float *param, float v)
+{
+    if (v < param[0]) return lut[0];
+    if (param[1] < v) return lut[len - 1];
+    const float f = v * param[2] + param[3];
+    if (!(f >= 0.0f)) return lut[0];
+    if (f >= (float)len) return lut[len - 1];
+    size_t idx = (size_t)f;
+    return lut[idx > len - 1 ? len - 1 : idx];
+}
+
+/* MedianMixRingClean::ProcessCore and ComputeProfile (frameworks/tomography/Preprocessing/
+ * StdPreprocModules/src/MedianMixRingClean.cpp:57-138): weights = SigmoidLUT(1024, threshold,
+ * width) of |mean projection - its 3x3 median| (5x1 when h < 3); every projection becomes
+ * (1 - w) * p + w * (its 5x5 median, 5x1 when h < 5). Projections [n][h][w], in place. */
+int orc_medianmixringclean(float *proj, size_t w, size_t h, size_t n, float threshold, float width)
+{
+    if (w < 4 || h < 1) return -1;
+    if (n == 0) return 0;
+    const size_t npix = w * h, len = 1024;
+    float *mean = (float *)malloc(npix * sizeof(float)), *wt = (float *)malloc(npix * sizeof(float));
+    float *med = (float *)malloc(npix * sizeof(float)), lut[1024], param[4];
+    mean_projection(proj, npix, n, 1, mean);
+    if (h < 3)
+        orc_median_filter(mean, w, h, 5, 1, wt);
+    else
+        orc_median_filter(mean, w, h, 3, 3, wt);
+    for (size_t j = 0; j < npix; ++j) wt[j] = fabsf(mean[j] - wt[j]);
+    orc_sigmoid_lut(len, threshold, width, lut, param);
+    for (size_t j = 0; j < npix; ++j) wt[j] = lut_apply(lut, len, param, wt[j]);
+    for (size_t i = 0; i < n; ++i) {
+        float *p = proj + i * npix;
+        orc_median_filter(p, w, h, 5, h < 5 ? 1 : 5, med);
+        for (size_t j = 0; j < npix; ++j) p[j] = (1.0f - wt[j]) * p[j] + wt[j] * med[j];
+    }
+    free(mean);
+    free(wt);
+    free(med);
+    return 0;
+}

@@ -105,6 +105,14 @@ void orc_joseph_adjoint64(const double *proj, size_t n, size_t nz, const float *
 int orc_slices_u16(const float *vol, size_t d0, size_t d1, size_t d2, int plane, size_t first, size_t count,
                    const size_t *roi, float lo, float hi, unsigned short *out);
 
+/* Alternative ring cleaners: kipl TMedianFilter<float,2> (odd kx, ky), BasicRingClean,
+ * kipl SigmoidLUT (param: lo, hi, slope, intercept) and MedianMixRingClean. Images [h][w],
+ * projections [n][h][w] in place. */
+int orc_median_filter(const float *img, size_t w, size_t h, int kx, int ky, float *out);
+int orc_basicringclean(float *proj, size_t w, size_t h, size_t n);
+void orc_sigmoid_lut(size_t len, float lambda, float sigma, float *lut, float *param);
+int orc_medianmixringclean(float *proj, size_t w, size_t h, size_t n, float threshold, float width);
+
 #ifdef __cplusplus
 }
 #endif

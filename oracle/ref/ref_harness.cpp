@@ -47,6 +47,11 @@
 #include "NormPlugins.h"
 #include "ProjectionFilter.h"
 #include "MorphSpotCleanModule.h"
+#include "BasicRingClean.h"
+#include "MedianMixRingClean.h"
+#include "GammaSpotCleanModule.h"
+#include <filters/medianfilter.h>
+#include <math/LUTCollection.h>
 #include "WaveletRingClean.h"
 #include "MultiProjBPparallel.h"
 #include "MultiProjBP.h"
@@ -55,6 +60,7 @@
 #include <wavelets/wavelets.h>
 #undef private
 #undef protected
+#include <tiffio.h>
 
 namespace {
 
@@ -516,5 +522,117 @@ int ref_slices_u16(const float *vol, size_t d0, size_t d1, size_t d2, int plane,
         }
     });
 }
+
+// kipl::filters::TMedianFilter<float,2> (core/kipl/kipl/include/filters/core/medianfilter.hpp)
+// on one image [h][w].
+int ref_median_filter(const float *img, size_t w, size_t h, int kx, int ky, float *out)
+{
+    return guarded([&] {
+        size_t d[2] = {w, h}, k[2] = {static_cast<size_t>(kx), static_cast<size_t>(ky)};
+        kipl::base::TImage<float, 2> src(d);
+        std::memcpy(src.GetDataPtr(), img, w * h * sizeof(float));
+        kipl::filters::TMedianFilter<float, 2> filt(k);
+        kipl::base::TImage<float, 2> r = filt(src);
+        std::memcpy(out, r.GetDataPtr(), w * h * sizeof(float));
+    });
+}
+
+// BasicRingClean::ProcessCore (StdPreprocModules/src/BasicRingClean.cpp:50-95) on
+// projections [n][h][w], in place.
+int ref_basicringclean(float *proj, size_t w, size_t h, size_t n)
+{
+    return guarded([&] {
+        BasicRingClean mod;
+        ReconConfig cfg;
+        std::map<std::string, std::string> par;
+        mod.Configure(cfg, par);
+        size_t d3[3] = {w, h, n};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * w * h * n);
+        std::map<std::string, std::string> coeff;
+        mod.Process(img, coeff);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * w * h * n);
+    });
+}
+
+// kipl::math::SigmoidLUT (core/kipl/kipl/src/math/LUTCollection.cpp:38-82): the table and
+// LUTbase's lo, hi, slope, intercept.
+int ref_sigmoid_lut(size_t len, float lambda, float sigma, float *lut, float *param)
+{
+    return guarded([&] {
+        kipl::math::SigmoidLUT t(len, lambda, sigma);
+        std::memcpy(lut, t.fLUT, len * sizeof(float));
+        param[0] = t.Low();
+        param[1] = t.High();
+        param[2] = t.Slope();
+        param[3] = t.Intercept();
+    });
+}
+
+// MedianMixRingClean::ProcessCore (StdPreprocModules/src/MedianMixRingClean.cpp:57-138) on
+// projections [n][h][w], in place.
+int ref_medianmixringclean(float *proj, size_t w, size_t h, size_t n, float threshold, float width)
+{
+    return guarded([&] {
+        MedianMixRingClean mod;
+        ReconConfig cfg;
+        std::map<std::string, std::string> par;
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.9g", threshold);
+        par["threshold"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", width);
+        par["width"] = b;
+        mod.Configure(cfg, par);
+        size_t d3[3] = {w, h, n};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * w * h * n);
+        std::map<std::string, std::string> coeff;
+        mod.Process(img, coeff);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * w * h * n);
+    });
+}
+
+// GammaSpotCleanModule::ProcessCore (StdPreprocModules/src/GammaSpotCleanModule.cpp:58-68)
+// on projections [n][h][w], in place, with its parameters.
+int ref_gammaspotclean(float *proj, size_t w, size_t h, size_t n, float threshold3, float threshold5,
+                       float threshold7, float sigma, int mediansize)
+{
+    return guarded([&] {
+        GammaSpotCleanModule mod;
+        ReconConfig cfg;
+        std::map<std::string, std::string> par;
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.9g", threshold3);
+        par["threshold3"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", threshold5);
+        par["threshold5"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", threshold7);
+        par["threshold7"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", sigma);
+        par["sigma"] = b;
+        par["mediansize"] = std::to_string(mediansize);
+        mod.Configure(cfg, par);
+        size_t d3[3] = {w, h, n};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * w * h * n);
+        std::map<std::string, std::string> coeff;
+        mod.Process(img, coeff);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * w * h * n);
+    });
+}
+
+// libtiff writers for the debug images BasicRingClean saves to the working directory
+// (mean.tif, med.tif, diff.tif; libtiff is absent here): opening for writing gives a handle
+// that discards everything, so the module runs to the end without touching the file system.
+// Opening for reading still fails.
+static char g_tiff_sink;
+TIFF *TIFFOpen(const char *, const char *mode)
+{
+    return mode && mode[0] == 'w' ? reinterpret_cast<TIFF *>(&g_tiff_sink) : nullptr;
+}
+int TIFFSetField(TIFF *, ttag_t, ...) { return 1; }
+int TIFFWriteDirectory(TIFF *) { return 1; }
+tsize_t TIFFWriteEncodedStrip(TIFF *, tstrip_t, tdata_t, tsize_t cc) { return cc; }
+void TIFFClose(TIFF *) {}
 
 } // extern "C"
