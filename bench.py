@@ -492,6 +492,7 @@ def run_parallel(args, production: bool):
         # the alternative ring cleaners a configuration can name instead of WaveletRingClean, each
         # timed alone on the normalised block (in place, CUDA events on the launching stream)
         blk = norm.ProcessCore(counts, {})
+        sample = None if args.no_cpu_baseline else blk[:16].cpu().numpy()
         basic, mix = M.BasicRingClean(), M.MedianMixRingClean()
         mix.Configure(cfg, {"threshold": "0.025", "width": "0.0025"})
         px = float(blk.numel())
@@ -504,6 +505,8 @@ def run_parallel(args, production: bool):
                "note": "algorithmic bytes 12 B/px for both: BasicRingClean reads the block for the mean, then "
                        "reads and writes it; MedianMixRingClean reads it for the mean, then reads it for the 5x5 "
                        "median and writes the mixed value"}
+        if sample is not None:
+            alt["cpu_baseline"] = alt_cleaners_cpu(sample)
         del blk
     sel = bp.used_projections(nproj).size
     updates = float(nu) * nu * (4 * (nrows // 4)) * sel
@@ -562,6 +565,27 @@ def run_parallel(args, production: bool):
             "e2e": {"value": updates * e2e_steps / te / 1e9, "unit": "GUPS",
                     "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(bp.volume.numel() * 4)},
             "clocks": clocks}
+
+
+def alt_cleaners_cpu(sample):
+    """The reference's BasicRingClean and MedianMixRingClean (compiled from the reference
+    sources) on a sample of normalised projections, all host threads."""
+    import oracle
+
+    cores = os.cpu_count() or 1
+    if not oracle.ref_available():
+        return {"kind": "reference", "cores": 0, "sample": "reference library absent"}
+    n, h, w = sample.shape
+    t0 = time.perf_counter()
+    oracle.basicringclean(sample, use_ref=True)
+    tb = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.medianmixringclean(sample, use_ref=True)
+    tm = time.perf_counter() - t0
+    return {"kind": "reference", "cores": cores,
+            "sample": f"{n} normalised projections of {w} x {h} (OMP_NUM_THREADS="
+                      f"{os.environ.get('OMP_NUM_THREADS', cores)})",
+            "basicringclean_ms_per_projection": tb / n * 1e3, "medianmixringclean_ms_per_projection": tm / n * 1e3}
 
 
 def cpu_baseline(w, counts, flats, darks, angles, weights, budget_s=20.0, nsample=None):

@@ -188,6 +188,18 @@ __device__ __forceinline__ float window_median(const float *img, int w, int h, i
 
 enum { MODE_MEDIAN = 0, MODE_DIFF = 1, MODE_ABSDIFF = 2, MODE_MIX = 3 };
 
+template <int MODE>
+__device__ __forceinline__ float median_epilogue(const float *img, const float *wt, size_t i, float m)
+{
+    if (MODE == MODE_DIFF) return __fsub_rn(__ldg(img + i), m);
+    if (MODE == MODE_ABSDIFF) return fabsf(__fsub_rn(__ldg(img + i), m));
+    if (MODE == MODE_MIX) {
+        const float a = __ldg(wt + i);
+        return __fadd_rn(__fmul_rn(__fsub_rn(1.0f, a), __ldg(img + i)), __fmul_rn(a, m));
+    }
+    return m;
+}
+
 // One pixel per thread, images along z. MODE_MEDIAN writes the median, MODE_DIFF the image
 // minus it (BasicRingClean.cpp:84-86), MODE_ABSDIFF its absolute difference
 // (MedianMixRingClean.cpp:133-135), MODE_MIX (1 - wt) * p + wt * median
@@ -200,17 +212,63 @@ __global__ void __launch_bounds__(256) k_median(const float *__restrict__ src, i
     if (x >= w || y >= h) return;
     const size_t npix = static_cast<size_t>(w) * h, i = static_cast<size_t>(y) * w + x;
     const float *img = src + blockIdx.z * npix;
-    const float m = window_median<KX, KY>(img, w, h, x, y);
-    float out = m;
-    if (MODE == MODE_DIFF) {
-        out = __fsub_rn(__ldg(img + i), m);
-    } else if (MODE == MODE_ABSDIFF) {
-        out = fabsf(__fsub_rn(__ldg(img + i), m));
-    } else if (MODE == MODE_MIX) {
-        const float a = __ldg(wt + i);
-        out = __fadd_rn(__fmul_rn(__fsub_rn(1.0f, a), __ldg(img + i)), __fmul_rn(a, m));
+    dst[blockIdx.z * npix + i] = median_epilogue<MODE>(img, wt, i, window_median<KX, KY>(img, w, h, x, y));
+}
+
+// 5x5 median of two horizontally adjacent pixels per thread. Their windows share the 20 values
+// of columns x-1 .. x+2. A value of rank r among those 20 has rank r .. r+5 in either window,
+// so only ranks 7..12 (0-based) can be a window's middle (rank 12 of 25), and that middle is
+// the middle of the 6 candidates and the window's own 5 values: 168 min/max for the shared
+// ranks plus 54 per window, instead of 202 per window. Pixels whose windows leave the image go
+// through window_median one by one.
+template <int MODE>
+__global__ void __launch_bounds__(256) k_median55_pair(const float *__restrict__ src, int w, int h,
+                                                       const float *__restrict__ wt, float *__restrict__ dst)
+{
+    const int x = 2 * (blockIdx.x * 32 + threadIdx.x), y = blockIdx.y * 8 + threadIdx.y;
+    if (x >= w || y >= h) return;
+    const size_t npix = static_cast<size_t>(w) * h, i = static_cast<size_t>(y) * w + x;
+    const float *img = src + blockIdx.z * npix;
+    float *out = dst + blockIdx.z * npix;
+    if (x >= 2 && x + 3 < w && y >= 2 && y + 2 < h) {
+        float c[20], a[5], b[5];
+        const float *p = img + static_cast<size_t>(y - 2) * w + (x - 2);
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            const float *q = p + static_cast<size_t>(r) * w;
+            a[r] = __ldg(q);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) c[r * 4 + k] = __ldg(q + 1 + k);
+            b[r] = __ldg(q + 5);
+        }
+        float sc = 0.0f, sa = 0.0f, sb = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 20; ++k) sc += c[k];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            sa += a[r];
+            sb += b[r];
+        }
+        sa += sc; // NaN iff a NaN (or +inf and -inf) is in the window
+        sb += sc;
+        rank_net20_7_12(c);
+        float va[11], vb[11];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) va[k] = vb[k] = c[7 + k];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) {
+            va[6 + r] = a[r];
+            vb[6 + r] = b[r];
+        }
+        float m0 = median_net11(va), m1 = median_net11(vb);
+        if (isnan(sa) || m0 == 0.0f) m0 = careful_median<5, 5>(img, w, h, x, y, isnan(sa));
+        if (isnan(sb) || m1 == 0.0f) m1 = careful_median<5, 5>(img, w, h, x + 1, y, isnan(sb));
+        out[i] = median_epilogue<MODE>(img, wt, i, m0);
+        out[i + 1] = median_epilogue<MODE>(img, wt, i + 1, m1);
+    } else {
+        out[i] = median_epilogue<MODE>(img, wt, i, window_median<5, 5>(img, w, h, x, y));
+        if (x + 1 < w) out[i + 1] = median_epilogue<MODE>(img, wt, i + 1, window_median<5, 5>(img, w, h, x + 1, y));
     }
-    dst[blockIdx.z * npix + i] = out;
 }
 
 // Mean projection accumulated in projection order (BasicRingClean.cpp:56-69 starts from a copy
@@ -345,6 +403,10 @@ static mr_status launch_median(const float *src, int w, int h, size_t nimg, int 
         const dim3 grid(div_up(w, 32), div_up(h, 8), nz), block(32, 8);
         const float *a = src + i0 * npix;
         float *b = dst + i0 * npix;
+        if (kx == 5 && ky == 5) {
+            k_median55_pair<MODE><<<dim3(div_up(w, 64), div_up(h, 8), nz), block, 0, s>>>(a, w, h, wt, b);
+            continue;
+        }
 #define MR_MEDIAN_CASE(KX, KY)                                                                                         \
     if (kx == KX && ky == KY) {                                                                                        \
         k_median<KX, KY, MODE><<<grid, block, 0, s>>>(a, w, h, wt, b);                                                \
@@ -358,7 +420,6 @@ static mr_status launch_median(const float *src, int w, int h, size_t nimg, int 
         MR_MEDIAN_CASE(1, 5)
         MR_MEDIAN_CASE(5, 3)
         MR_MEDIAN_CASE(3, 5)
-        MR_MEDIAN_CASE(5, 5)
 #undef MR_MEDIAN_CASE
         return fail(MR_ERR_UNSUPPORTED, "median filter: kernel %dx%d", kx, ky);
     }

@@ -72,6 +72,7 @@ def ref() -> ctypes.CDLL:
         lib = ctypes.CDLL(path)
         lib.ref_last_error.restype = ctypes.c_char_p
         lib.ref_frame_dose.restype = ctypes.c_float
+        lib.ref_quiet_logging()
         _ref = lib
     return _ref
 

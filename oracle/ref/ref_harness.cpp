@@ -117,6 +117,10 @@ extern "C" {
 
 const char *ref_last_error() { return g_error.c_str(); }
 
+// The reference modules log through kipl::logging::Logger to standard output. Callers keep
+// only errors (which are also thrown), so that their own standard output stays clean.
+void ref_quiet_logging() { kipl::logging::Logger::SetLogLevel(kipl::logging::Logger::LogError); }
+
 float ref_frame_dose(const float *frame, size_t nu, const size_t *roi) { return frame_dose(frame, nu, roi); }
 
 // ImagingAlgorithms::AverageImage::operator() (averageimage.cpp:35-61)
