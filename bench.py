@@ -489,19 +489,26 @@ def run_parallel(args, production: bool):
     step(record=True)
     alt = None
     if production:
-        # the alternative ring cleaners a configuration can name instead of WaveletRingClean, each
-        # timed alone on the normalised block (in place, CUDA events on the launching stream)
+        # the alternative cleaners a configuration can name instead of MorphSpotClean or
+        # WaveletRingClean, each timed alone on the normalised block (in place, CUDA events on
+        # the launching stream)
         blk = norm.ProcessCore(counts, {})
         sample = None if args.no_cpu_baseline else blk[:16].cpu().numpy()
         basic, mix = M.BasicRingClean(), M.MedianMixRingClean()
         mix.Configure(cfg, {"threshold": "0.025", "width": "0.0025"})
+        spot2 = M.SpotClean2()
+        spot2.Configure(cfg, {"gamma": "0.1", "sigma": "0.001", "iterations": "1", "maxlevel": "5", "minlevel": "-0.1",
+                              "maxarea": "20", "detectionmethod": "ring"})
         px = float(blk.numel())
+        ts = kernel_time(lambda: spot2.ProcessCore(blk, {}), stream, reps=1)
         tb = kernel_time(lambda: basic.ProcessCore(blk, {}), stream)
         tm = kernel_time(lambda: mix.ProcessCore(blk, {}), stream)
         alt = {"block": [nproj, nrows, nu],
                "basicringclean_ms": tb * 1e3, "basicringclean_gbs": 12.0 * px / tb / 1e9,
                "medianmixringclean_ms": tm * 1e3, "medianmixringclean_gbs": 12.0 * px / tm / 1e9,
                "medianmixringclean_gpx_s": px / tm / 1e9,
+               "spotclean2_ms": ts * 1e3, "spotclean2_gpx_s": px / ts / 1e9,
+               "spotclean2_config": "ring detection, gamma 0.1, sigma 0.001, maxarea 20, levels [-0.1, 5]",
                "note": "algorithmic bytes 12 B/px for both: BasicRingClean reads the block for the mean, then "
                        "reads and writes it; MedianMixRingClean reads it for the mean, then reads it for the 5x5 "
                        "median and writes the mixed value"}
@@ -568,8 +575,8 @@ def run_parallel(args, production: bool):
 
 
 def alt_cleaners_cpu(sample):
-    """The reference's BasicRingClean and MedianMixRingClean (compiled from the reference
-    sources) on a sample of normalised projections, all host threads."""
+    """The reference's BasicRingClean, MedianMixRingClean and SpotClean2 (compiled from the
+    reference sources) on a sample of normalised projections, all host threads."""
     import oracle
 
     cores = os.cpu_count() or 1
@@ -582,10 +589,14 @@ def alt_cleaners_cpu(sample):
     t0 = time.perf_counter()
     oracle.medianmixringclean(sample, use_ref=True)
     tm = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.spotclean2(sample, "ring", 0.1, 0.001, 1, -0.1, 5.0, 20, use_ref=True)
+    ts = time.perf_counter() - t0
     return {"kind": "reference", "cores": cores,
             "sample": f"{n} normalised projections of {w} x {h} (OMP_NUM_THREADS="
                       f"{os.environ.get('OMP_NUM_THREADS', cores)})",
-            "basicringclean_ms_per_projection": tb / n * 1e3, "medianmixringclean_ms_per_projection": tm / n * 1e3}
+            "basicringclean_ms_per_projection": tb / n * 1e3, "medianmixringclean_ms_per_projection": tm / n * 1e3,
+            "spotclean2_ms_per_projection": ts / n * 1e3}
 
 
 def cpu_baseline(w, counts, flats, darks, angles, weights, budget_s=20.0, nsample=None):

@@ -54,6 +54,8 @@ _PROTOS = {
     "mr_basicringclean": (c_int, [c_void, c_size, c_size, c_size, c_void]),
     "mr_medianmixringclean": (c_int, [c_void, c_size, c_size, c_size, c_float, c_float, c_void]),
     "mr_sigmoid_lut": (c_int, [c_size, c_float, c_float, P_float, P_float]),
+    "mr_spotclean2": (c_int, [c_void, c_size, c_size, c_size, c_int, c_float, c_float, c_int, c_float, c_float, c_int,
+                              c_void]),
     "mr_projfilter_tables": (c_int, [c_size, ctypes.c_char_p, c_float, c_float, c_int, c_float, c_int, P_size, P_size,
                                      P_float, P_float]),
     "mr_projfilter_create": (c_int, [c_size, ctypes.c_char_p, c_float, c_float, c_int, c_float, c_int,

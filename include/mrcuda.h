@@ -151,6 +151,26 @@ mr_status mr_medianmixringclean(float *proj_d, size_t nu, size_t nv, size_t npro
 mr_status mr_sigmoid_lut(size_t len, float lambda, float sigma, float *lut_h, float *param_h);
 
 /* ---------------------------------------------------------------------------------
+ * SpotClean2
+ * replaces SpotClean2::ProcessCore 3D (frameworks/tomography/Preprocessing/StdPreprocModules/
+ *   src/SpotClean2.cpp:117-130) -> ImagingAlgorithms::SpotClean::Process (core/algorithms/
+ *   ImagingAlgorithms/src/SpotClean.cpp:78-545) on projections [nproj][nv][nu], in place:
+ *   `iterations` passes of detection (method below, kipl filters with EdgeMirror edges),
+ *   SigmoidLUT(1 << 15, gamma, sigma), exclusion of 8-connected regions larger than maxarea
+ *   (0: none) by the reference's RemoveConnectedRegion rule, spots outside [minlevel, maxlevel]
+ *   or with a nonzero weight, and the neighbour-mean fill rounds of CleanByArray.
+ *   nu, nv >= 16; sigma > 0. Synchronises the stream once per batch of projections (a batch
+ *   is about 1 GiB of scratch: five images per projection). A round that corrects nothing while
+ *   spots remain (the reference would loop forever) returns MR_ERR_DEVICE; with the value past
+ *   the image end read as 0 the last pixel always has an unmarked neighbour, so this is a
+ *   guard, not an expected outcome. TriKernel's level
+ *   statistics are fixed-order double sums (the reference's running update differs below
+ *   1e-15 relative). */
+enum { MR_SPOT_STDDEV = 0, MR_SPOT_RING = 1, MR_SPOT_MEDIAN = 2, MR_SPOT_MINMAX = 3, MR_SPOT_TRIKERNEL = 4 };
+mr_status mr_spotclean2(float *proj_d, size_t nu, size_t nv, size_t nproj, int method, float gamma, float sigma,
+                        int iterations, float minlevel, float maxlevel, int maxarea, void *stream);
+
+/* ---------------------------------------------------------------------------------
  * ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:78-376)
  * Plan = ProjectionFilterBase::Configure/BuildFilter/PreparePadding (:78-93,254-299,364-376):
  *   nfft = 2^(ceil(log2 nu) + paddingdoubler); filter over bins 0..nfft/2-1.

@@ -618,3 +618,22 @@ def ref_gammaspotclean(proj, threshold3=25.0, threshold5=100.0, threshold7=400.0
     _check_ref(ref().ref_gammaspotclean(_p(p), _sz(w), _sz(h), _sz(n), _f(threshold3), _f(threshold5),
                                         _f(threshold7), _f(sigma), ctypes.c_int(mediansize)))
     return p
+
+
+SPOT_METHODS = {"stddev": 0, "ring": 1, "median": 2, "minmax": 3, "trikernel": 4}
+
+
+def spotclean2(proj, method: str = "ring", gamma: float = 0.1, sigma: float = 0.001, iterations: int = 1,
+               minlevel: float = -0.1, maxlevel: float = 5.0, maxarea: int = 20, use_ref: bool = False) -> np.ndarray:
+    """SpotClean2 (ImagingAlgorithms::SpotClean) on projections (n, h, w); returns the cleaned copy."""
+    p = _f32(proj).copy()
+    n, h, w = p.shape
+    if use_ref:
+        _check_ref(ref().ref_spotclean2(_p(p), _sz(w), _sz(h), _sz(n), method.encode(), _f(gamma), _f(sigma),
+                                        ctypes.c_int(iterations), _f(minlevel), _f(maxlevel), ctypes.c_int(maxarea)))
+    else:
+        rc = orc().orc_spotclean(_p(p), _sz(w), _sz(h), _sz(n), ctypes.c_int(SPOT_METHODS[method]), _f(gamma),
+                                 _f(sigma), ctypes.c_int(iterations), _f(minlevel), _f(maxlevel), ctypes.c_int(maxarea))
+        if rc != 0:
+            raise ValueError(f"orc_spotclean failed ({rc})")
+    return p

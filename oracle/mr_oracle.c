@@ -1564,3 +1564,291 @@ int orc_medianmixringclean(float *proj, size_t w, size_t h, size_t n, float thre
     free(med);
     return 0;
 }
+
+/* ----------------------------------------------------------- SpotClean (SpotClean2) */
+
+/* Source value for output (x, y) at (xx, yy) as kipl TFilterBase<float,2> with EdgeMirror
+ * reads it (core/kipl/kipl/include/filters/core/filterbase.hpp:83-128,246-408): outputs in the
+ * top and bottom ky/2 rows come from buffers mirrored vertically about the edge row (no
+ * repeat) and padded horizontally with the edge value; outputs in the left and right kx/2
+ * columns of the remaining rows from buffers mirrored horizontally; the rest read the image. */
+static float mirror_src(const float *img, int w, int h, int kx, int ky, int x, int y, int xx, int yy)
+{
+    const int cx = kx / 2, cy = ky / 2;
+    if (y < cy || y >= h - cy) {
+        if (yy < 0) yy = -yy;
+        else if (yy >= h) yy = 2 * (h - 1) - yy;
+        if (xx < 0) xx = 0;
+        else if (xx >= w) xx = w - 1;
+    } else if (x < cx || x >= w - cx) {
+        if (xx < 0) xx = -xx;
+        else if (xx >= w) xx = 2 * (w - 1) - xx;
+    }
+    return img[(size_t)yy * w + xx];
+}
+
+enum { KF_SUM = 0, KF_MIN = 1, KF_MAX = 2 };
+
+/* TFilter (sum of value * kernel from 0, filter.hpp:10-15), TErode (min from FLT_MAX) and
+ * TDilate (max from -FLT_MAX, morphology/core/morphfilters.hpp:10-75): the kernel's nonzero
+ * entries in row-major order (ProcessCore, filterbase.hpp:83-128), EdgeMirror edges. */
+static void kipl_filter(const float *img, int w, int h, const float *k, int kx, int ky, int op, float *out)
+{
+    const int cx = kx / 2, cy = ky / 2;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            float acc = op == KF_SUM ? 0.0f : op == KF_MIN ? 3.402823466e+38f : -3.402823466e+38f;
+            for (int i = 0; i < kx * ky; ++i) {
+                if (k[i] == 0.0f) continue;
+                const float v = mirror_src(img, w, h, kx, ky, x, y, x + i % kx - cx, y + i / kx - cy);
+                if (op == KF_SUM) acc = acc + v * k[i];
+                else if (op == KF_MIN) acc = v < acc ? v : acc; /* std::min(dest, src) */
+                else acc = acc < v ? v : acc;                  /* std::max(dest, src) */
+            }
+            out[(size_t)y * w + x] = acc;
+        }
+}
+
+/* SpotClean::BoxFilter (core/algorithms/ImagingAlgorithms/src/SpotClean.cpp:447-465): a sum
+ * over dim values along x, then along y, each with EdgeMirror edges. */
+static void box_filter(const float *img, int w, int h, int dim, float *tmp, float *out)
+{
+    float ones[7] = {1, 1, 1, 1, 1, 1, 1};
+    kipl_filter(img, w, h, ones, dim, 1, KF_SUM, tmp);
+    kipl_filter(tmp, w, h, ones, 1, dim, KF_SUM, out);
+}
+
+/* kipl::math::statistics (core/kipl/kipl/include/math/core/image_statistics.hpp:197-219):
+ * running mean and variance in double, variance / N, standard deviation. */
+static void running_stats(const float *x, size_t n, double *mean, double *sd)
+{
+    double m = 0.0, var = 0.0;
+    for (size_t i = 0; i < n;) {
+        const double value = x[i];
+        const double delta = value - m;
+        i++;
+        m += delta / (double)i;
+        var += delta * (value - m);
+    }
+    var = var / (double)n;
+    *mean = m;
+    *sd = sqrt(var);
+}
+
+/* SpotClean::DetectionImage (SpotClean.cpp:388-545) for method 0 stddev, 1 ring, 2 median,
+ * 3 minmax, 4 trikernel; gamma is the TriKernel level factor. */
+static int spot_detection(const float *img, int w, int h, int method, float gamma, float *det)
+{
+    const size_t n = (size_t)w * h;
+    float *a = (float *)malloc(n * sizeof(float)), *b = (float *)malloc(n * sizeof(float));
+    float *c = (float *)malloc(n * sizeof(float)), *d = (float *)malloc(n * sizeof(float));
+    int rc = 0;
+    if (method == 1) { /* RingDetection: 5x5 ring of 1/12, centre -1, then |.| */
+        const float wv = 1.0f / 12.0f, cv = -1.0f, z = 0.0f;
+        const float k[25] = {z, wv, wv, wv, z, wv, z, z, z, wv, wv, z, cv, z, wv, wv, z, z, z, wv, z, wv, wv, wv, z};
+        kipl_filter(img, w, h, k, 5, 5, KF_SUM, det);
+        for (size_t i = 0; i < n; ++i) det[i] = fabsf(det[i]);
+    } else if (method == 0) { /* StdDevDetection(img, 3) */
+        for (size_t i = 0; i < n; ++i) a[i] = img[i] * img[i];
+        box_filter(a, w, h, 3, c, b); /* s2 */
+        box_filter(img, w, h, 3, c, d); /* m */
+        const float M = 1 / (float)(3 * 3), M1 = 1 / (float)(3 * 3 - 1);
+        for (size_t i = 0; i < n; ++i) det[i] = (float)sqrt((double)(M1 * (b[i] - M * d[i] * d[i])));
+    } else if (method == 2) { /* MedianDetection: 1x5 then 5x1 median, |img - median| */
+        orc_median_filter(img, (size_t)w, (size_t)h, 1, 5, a);
+        orc_median_filter(a, (size_t)w, (size_t)h, 5, 1, b);
+        for (size_t i = 0; i < n; ++i) det[i] = fabsf(img[i] - b[i]);
+    } else if (method == 3) { /* MinMaxDetection: 1x5 then 5x1 erosion and dilation */
+        const float se[5] = {1, 1, 1, 1, 1};
+        kipl_filter(img, w, h, se, 1, 5, KF_MIN, a);
+        kipl_filter(a, w, h, se, 5, 1, KF_MIN, b);
+        kipl_filter(img, w, h, se, 1, 5, KF_MAX, a);
+        kipl_filter(a, w, h, se, 5, 1, KF_MAX, c);
+        for (size_t i = 0; i < n; ++i) det[i] = fabsf(c[i] - b[i]);
+    } else if (method == 4) { /* TriKernel: OneKernel for 3, 5, 7 */
+        for (size_t i = 0; i < n; ++i) det[i] = 0.0f;
+        for (int size = 3; size <= 7; size += 2) {
+            box_filter(img, w, h, size, c, a);
+            for (size_t i = 0; i < n; ++i) a[i] = fabsf(img[i] - a[i]);
+            double m, sd;
+            running_stats(a, n, &m, &sd);
+            const float level = (float)(m + (double)gamma * sd);
+            for (size_t i = 0; i < n; ++i) det[i] = (det[i] != 0.0f || level < a[i]) ? 1.0f : 0.0f;
+        }
+    } else {
+        rc = -1;
+    }
+    free(a);
+    free(b);
+    free(c);
+    free(d);
+    return rc;
+}
+
+/* SpotClean::ExcludeLargeRegions (SpotClean.cpp:248-285) with kipl LabelImage (8-connected
+ * components of s != 0), LabelArea (every label's count and LAST index, the background label 0
+ * included) and RemoveConnectedRegion (morphology/label.h): each label with area > maxarea
+ * is removed by a flood from its last pixel through nonzero labels; the flood from the
+ * background's last pixel removes the components next to it. Then s = 0 on label 0. */
+static void exclude_large_regions(float *s, int w, int h, int maxarea)
+{
+    if (maxarea == 0) return;
+    const size_t n = (size_t)w * h;
+    int *lbl = (int *)calloc(n, sizeof(int));
+    size_t *stack = (size_t *)malloc(n * sizeof(size_t));
+    size_t cnt = 0;
+    for (size_t p = 0; p < n; ++p) {
+        if (lbl[p] || s[p] == 0.0f) continue;
+        ++cnt;
+        size_t top = 0;
+        lbl[p] = (int)cnt;
+        stack[top++] = p;
+        while (top) {
+            const size_t q = stack[--top];
+            for (int j = 0; j < 8; ++j) {
+                const long r = nb(q, (size_t)w, (size_t)h, kNbr[j]);
+                if (r >= 0 && s[r] != 0.0f && !lbl[r]) {
+                    lbl[r] = (int)cnt;
+                    stack[top++] = (size_t)r;
+                }
+            }
+        }
+    }
+    size_t *area = (size_t *)calloc(cnt + 1, sizeof(size_t)), *last = (size_t *)calloc(cnt + 1, sizeof(size_t));
+    for (size_t i = 0; i < n; ++i) {
+        area[lbl[i]]++;
+        last[lbl[i]] = i;
+    }
+    size_t nseed = 0;
+    size_t *seeds = (size_t *)malloc((cnt + 1) * sizeof(size_t));
+    for (size_t l = 0; l <= cnt; ++l)
+        if ((size_t)maxarea < area[l]) seeds[nseed++] = last[l];
+    for (size_t i = 0; i < nseed; ++i) lbl[seeds[i]] = 0;
+    for (size_t i = 0; i < nseed; ++i) {
+        size_t top = 0;
+        stack[top++] = seeds[i];
+        while (top) {
+            const size_t q = stack[--top];
+            for (int j = 0; j < 8; ++j) {
+                const long r = nb(q, (size_t)w, (size_t)h, kNbr[j]);
+                if (r >= 0 && lbl[r] != 0) {
+                    lbl[r] = 0;
+                    stack[top++] = (size_t)r;
+                }
+            }
+        }
+    }
+    for (size_t i = 0; i < n; ++i)
+        if (lbl[i] == 0) s[i] = 0.0f;
+    free(lbl);
+    free(stack);
+    free(area);
+    free(last);
+    free(seeds);
+}
+
+/* One projection of SpotClean::Process (SpotClean.cpp:78-108): DetectSpots (:185-246: the
+ * detection image through SigmoidLUT(1 << 15, gamma, sigma), large regions excluded, pixels
+ * outside [minlevel, maxlevel] or with a nonzero weight become spots and are marked with
+ * FLT_MAX) and CleanByArray (:287-336 with PrepareNeighborhood / Neighborhood :338-365: every
+ * round, each remaining spot with unmarked neighbours among the linear offsets
+ * {-w-1,-w,-w+1,-1,1,w-1,w,w+1} (the first row, up to index w, skips the row above; index 0
+ * also the left one; the last row skips the row below; nothing wraps differently at the side
+ * columns) moves by weight * (mean - value); the new values are written after the round).
+ * Returns -2 when a round corrects nothing while spots remain (the reference loops forever). */
+static int spotclean_one(float *img, int w, int h, int method, float gamma, float sigma, float minlevel,
+                         float maxlevel, int maxarea, const float *lut, const float *param, size_t len)
+{
+    const size_t n = (size_t)w * h;
+    const float mark = 3.402823466e+38f;
+    float *s = (float *)malloc(n * sizeof(float)), *res = (float *)malloc(n * sizeof(float));
+    size_t *pos = (size_t *)malloc(n * sizeof(size_t)), *next = (size_t *)malloc(n * sizeof(size_t));
+    float *val = (float *)malloc(n * sizeof(float)), *wt = (float *)malloc(n * sizeof(float));
+    float *nval = (float *)malloc(n * sizeof(float)), *nwt = (float *)malloc(n * sizeof(float));
+    int rc = spot_detection(img, w, h, method, gamma, s);
+    if (rc == 0) {
+        for (size_t i = 0; i < n; ++i) s[i] = lut_apply(lut, len, param, s[i]);
+        exclude_large_regions(s, w, h, maxarea);
+        memcpy(res, img, n * sizeof(float));
+        size_t np = 0;
+        for (size_t i = 0; i < n; ++i) {
+            if (res[i] < minlevel || maxlevel < res[i]) {
+                pos[np] = i; val[np] = res[i]; wt[np] = 1.0f; np++;
+                res[i] = mark;
+            } else if (s[i] != 0.0f) {
+                pos[np] = i; val[np] = res[i]; wt[np] = s[i]; np++;
+                res[i] = mark;
+            }
+        }
+        static const int off_dx[8] = {-1, 0, 1, -1, 1, -1, 0, 1}, off_dy[8] = {-1, -1, -1, 0, 0, 1, 1, 1};
+        float *newv = (float *)malloc((np ? np : 1) * sizeof(float));
+        unsigned char *done = (unsigned char *)malloc(np ? np : 1);
+        while (np) {
+            size_t nc = 0;
+            for (size_t k = 0; k < np; ++k) {
+                const long long idx = (long long)pos[k];
+                const int start = (long long)w < idx ? 0 : (idx != 0 ? 3 : 4);
+                const int stop = idx < (long long)(n - w) ? 8 : 5;
+                float sum = 0.0f;
+                int cntn = 0;
+                for (int i = start; i < stop; ++i) {
+                    const float v = img_at(res, n, idx + off_dy[i] * (long long)w + off_dx[i]);
+                    if (v != mark) {
+                        sum += v;
+                        cntn++;
+                    }
+                }
+                done[k] = cntn != 0;
+                if (cntn) {
+                    const float mean = sum / (float)cntn;
+                    newv[k] = val[k] + wt[k] * (mean - val[k]);
+                    nc++;
+                }
+            }
+            if (nc == 0) {
+                rc = -2;
+                break;
+            }
+            size_t nr = 0;
+            for (size_t k = 0; k < np; ++k) {
+                if (done[k]) {
+                    res[pos[k]] = newv[k];
+                } else {
+                    next[nr] = pos[k]; nval[nr] = val[k]; nwt[nr] = wt[k]; nr++;
+                }
+            }
+            memcpy(pos, next, nr * sizeof(size_t));
+            memcpy(val, nval, nr * sizeof(float));
+            memcpy(wt, nwt, nr * sizeof(float));
+            np = nr;
+        }
+        free(newv);
+        free(done);
+        if (rc == 0) {
+            for (size_t i = 0; i < n; ++i)
+                if (res[i] == mark) rc = -3;
+            memcpy(img, res, n * sizeof(float));
+        }
+    }
+    free(s); free(res); free(pos); free(next); free(val); free(wt); free(nval); free(nwt);
+    return rc;
+}
+
+/* SpotClean2::ProcessCore 3D -> ImagingAlgorithms::SpotClean::Process (SpotClean.cpp:78-108):
+ * `iterations` passes over every projection [n][h][w], in place. method: 0 stddev, 1 ring,
+ * 2 median, 3 minmax, 4 trikernel. */
+int orc_spotclean(float *proj, size_t w, size_t h, size_t n, int method, float gamma, float sigma, int iterations,
+                  float minlevel, float maxlevel, int maxarea)
+{
+    if (w < 16 || h < 16 || method < 0 || method > 4) return -1;
+    const size_t len = (size_t)1 << 15;
+    float *lut = (float *)malloc(len * sizeof(float)), param[4];
+    orc_sigmoid_lut(len, gamma, sigma, lut, param);
+    int rc = 0;
+    for (int it = 0; it < iterations && rc == 0; ++it)
+        for (size_t i = 0; i < n && rc == 0; ++i)
+            rc = spotclean_one(proj + i * w * h, (int)w, (int)h, method, gamma, sigma, minlevel, maxlevel, maxarea, lut,
+                               param, len);
+    free(lut);
+    return rc;
+}

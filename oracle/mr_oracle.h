@@ -113,6 +113,12 @@ int orc_basicringclean(float *proj, size_t w, size_t h, size_t n);
 void orc_sigmoid_lut(size_t len, float lambda, float sigma, float *lut, float *param);
 int orc_medianmixringclean(float *proj, size_t w, size_t h, size_t n, float threshold, float width);
 
+/* SpotClean2 (ImagingAlgorithms::SpotClean): method 0 stddev, 1 ring, 2 median, 3 minmax,
+ * 4 trikernel. Projections [n][h][w] in place, w, h >= 16. Returns -2 when the reference would
+ * loop forever (a round with no spot next to an unmarked pixel). */
+int orc_spotclean(float *proj, size_t w, size_t h, size_t n, int method, float gamma, float sigma, int iterations,
+                  float minlevel, float maxlevel, int maxarea);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,7 @@
 #include "BasicRingClean.h"
 #include "MedianMixRingClean.h"
 #include "GammaSpotCleanModule.h"
+#include "SpotClean2.h"
 #include <filters/medianfilter.h>
 #include <math/LUTCollection.h>
 #include "WaveletRingClean.h"
@@ -615,6 +616,38 @@ int ref_gammaspotclean(float *proj, size_t w, size_t h, size_t n, float threshol
         std::snprintf(b, sizeof(b), "%.9g", sigma);
         par["sigma"] = b;
         par["mediansize"] = std::to_string(mediansize);
+        mod.Configure(cfg, par);
+        size_t d3[3] = {w, h, n};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * w * h * n);
+        std::map<std::string, std::string> coeff;
+        mod.Process(img, coeff);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * w * h * n);
+    });
+}
+
+// SpotClean2::ProcessCore 3D (StdPreprocModules/src/SpotClean2.cpp:117-130 ->
+// ImagingAlgorithms::SpotClean::Process, SpotClean.cpp:78-108) on projections [n][h][w], in
+// place. method: the reference's detection method names.
+int ref_spotclean2(float *proj, size_t w, size_t h, size_t n, const char *method, float gamma, float sigma,
+                   int iterations, float minlevel, float maxlevel, int maxarea)
+{
+    return guarded([&] {
+        SpotClean2 mod;
+        ReconConfig cfg;
+        std::map<std::string, std::string> par;
+        char b[64];
+        std::snprintf(b, sizeof(b), "%.9g", gamma);
+        par["gamma"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", sigma);
+        par["sigma"] = b;
+        par["iterations"] = std::to_string(iterations);
+        std::snprintf(b, sizeof(b), "%.9g", maxlevel);
+        par["maxlevel"] = b;
+        std::snprintf(b, sizeof(b), "%.9g", minlevel);
+        par["minlevel"] = b;
+        par["maxarea"] = std::to_string(maxarea);
+        par["detectionmethod"] = method;
         mod.Configure(cfg, par);
         size_t d3[3] = {w, h, n};
         kipl::base::TImage<float, 3> img(d3);

@@ -170,3 +170,63 @@ def test_ringalt_argument_errors_need_no_gpu():
     lut = np.empty(4, np.float32)
     assert lib.mr_sigmoid_lut(4, 0.1, -1.0, lut.ctypes.data_as(L.P_float), lut.ctypes.data_as(L.P_float)) == \
         L.MR_ERR_ARGUMENT
+
+
+def spot_phantom(rng, n, h, w, density=0.004):
+    """Smooth projections with spots: single pixels, small blobs, a few outside the level range."""
+    yy, xx = np.mgrid[0:h, 0:w].astype(np.float32)
+    base = 0.3 + 0.2 * np.sin(xx / 7.0) * np.cos(yy / 11.0)
+    p = np.empty((n, h, w), np.float32)
+    for i in range(n):
+        q = base + rng.normal(0, 0.004, (h, w))
+        k = max(1, int(h * w * density))
+        idx = rng.integers(0, h * w, k)
+        q.reshape(-1)[idx] += rng.choice([0.3, 1.0, 6.0, -0.9], k)
+        y0, x0 = rng.integers(2, h - 6), rng.integers(2, w - 6)
+        q[y0:y0 + 3, x0:x0 + 4] += 1.5  # a blob of 12 pixels
+        p[i] = q
+    return p
+
+
+@pytest.mark.parametrize("method", ["ring", "median", "minmax", "stddev", "trikernel"])
+def test_spotclean2_matches_reference(ref_lib, method):
+    """The restatement of ImagingAlgorithms::SpotClean against the compiled SpotClean2 module:
+    every detection method, region exclusion on and off, two iterations, ragged sizes."""
+    rng = np.random.default_rng(len(method))
+    for n, h, w in ((2, 16, 16), (2, 23, 37), (1, 48, 64)):
+        p = spot_phantom(rng, n, h, w)
+        for gamma, sigma, maxarea, it in ((0.1, 0.001, 20, 1), (0.05, 0.01, 0, 2), (0.2, 0.005, 5, 1)):
+            a = O.spotclean2(p, method, gamma, sigma, it, -0.1, 5.0, maxarea)
+            b = O.spotclean2(p, method, gamma, sigma, it, -0.1, 5.0, maxarea, use_ref=True)
+            assert np.array_equal(_bits(a), _bits(b)), (method, n, h, w, gamma, sigma, maxarea, it)
+
+
+def test_spotclean2_background_neighbour_rule(ref_lib):
+    """RemoveConnectedRegion also floods from the background label's last pixel: a small spot
+    next to the last background pixel loses its weight although it is below maxarea, so it is
+    not cleaned (it stays in the level range)."""
+    p = np.full((1, 16, 16), 0.3, np.float32)
+    p[0, 15, 15] = 2.0  # the last pixel is a spot; the last background pixel is (15, 14)
+    p[0, 4, 4] = 2.0  # an isolated spot elsewhere
+    a = O.spotclean2(p, "ring", 0.1, 0.001, 1, -0.1, 5.0, 20)
+    assert np.array_equal(_bits(a), _bits(O.spotclean2(p, "ring", 0.1, 0.001, 1, -0.1, 5.0, 20, use_ref=True)))
+    assert a[0, 15, 15] == np.float32(2.0) and a[0, 4, 4] < 1.0
+
+
+def test_spotclean2_every_pixel_a_spot(ref_lib):
+    """All pixels above maxlevel: the reference still ends, because the last pixel's right
+    neighbour is the value past the image end (0 in both oracles)."""
+    p = np.full((2, 20, 24), 9.0, np.float32)
+    p[1, 3, 5] = 0.5
+    a = O.spotclean2(p, "ring", 0.1, 0.001, 1, -0.1, 5.0, 20)
+    assert np.array_equal(_bits(a), _bits(O.spotclean2(p, "ring", 0.1, 0.001, 1, -0.1, 5.0, 20, use_ref=True)))
+    assert not np.any(a == np.float32(9.0))
+
+
+def test_spotclean2_argument_errors_need_no_gpu():
+    lib = L.lib()
+    fake = 256
+    assert lib.mr_spotclean2(None, 32, 32, 1, 1, 0.1, 0.001, 1, -0.1, 5.0, 20, None) == L.MR_ERR_ARGUMENT
+    assert lib.mr_spotclean2(fake, 15, 32, 1, 1, 0.1, 0.001, 1, -0.1, 5.0, 20, None) == L.MR_ERR_ARGUMENT
+    assert lib.mr_spotclean2(fake, 32, 32, 1, 7, 0.1, 0.001, 1, -0.1, 5.0, 20, None) == L.MR_ERR_ARGUMENT
+    assert lib.mr_spotclean2(fake, 32, 32, 1, 1, 0.1, 0.0, 1, -0.1, 5.0, 20, None) == L.MR_ERR_ARGUMENT
