@@ -5,6 +5,7 @@
 // (FullLogNorm), core/algorithms/ImagingAlgorithms/src/averageimage.cpp (AverageImage),
 // frameworks/tomography/Framework/ReconFramework/src/ProjectionReader.cpp:752-783 (dose).
 #include "mr_common.cuh"
+#include "mr_kipl_filters.cuh"
 
 #include <mutex>
 
@@ -78,6 +79,25 @@ __global__ void k_average(const float *__restrict__ frames, size_t npix, int n, 
         }
         out[j] = (n & 1) ? col[n / 2] : __fdiv_rn(__fadd_rn(col[n / 2 - 1], col[n / 2]), 2.0f);
     }
+}
+
+// ComputeWeightedAverage (averageimage.cpp:123-172) after the per-frame 5x5 StdDevFilter:
+// weight 1/sigma, or 1/(number of pixels) where sigma is 0; weight sum and weighted sum in
+// frame order, then their quotient.
+__global__ void k_weighted_average(const float *__restrict__ frames, const float *__restrict__ sigma, size_t npix,
+                                   int n, float *__restrict__ out)
+{
+    const size_t j = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
+    if (j >= npix) return;
+    const float zw = __fdiv_rn(1.0f, static_cast<float>(npix));
+    float ws = 0.0f, acc = 0.0f;
+    for (int i = 0; i < n; ++i) {
+        const float sg = sigma[i * npix + j];
+        const float wt = sg != 0.0f ? __fdiv_rn(1.0f, sg) : zw;
+        ws = __fadd_rn(ws, wt);
+        acc = __fadd_rn(acc, __fmul_rn(wt, frames[i * npix + j]));
+    }
+    out[j] = __fdiv_rn(acc, ws);
 }
 
 // ------------------------------------------------------------------ projection dose
@@ -219,10 +239,27 @@ mr_status mr_reference_average(const float *frames_d, size_t nu, size_t nv, size
 {
     if (!frames_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_reference_average: null pointer");
     if (n == 0) return fail(MR_ERR_ARGUMENT, "mr_reference_average: no frames");
-    if (!(method == 0 || method == 1 || method == 2 || method == 4 || method == 5))
+    if (method < 0 || method > 5)
         return fail(MR_ERR_UNSUPPORTED, "mr_reference_average: method %d not supported", method);
     if (method == 2 && n > 64) return fail(MR_ERR_ARGUMENT, "mr_reference_average: median of more than 64 frames");
     const size_t npix = nu * nv;
+    if (method == 3) {
+        // ImageWeightedAverage: 5x5 StdDevFilter of every frame, then the weighted average
+        if (nu < 5 || nv < 5 || npix > (size_t(1) << 31) - 1 || n > 65535)
+            return fail(MR_ERR_ARGUMENT, "mr_reference_average: weighted average of %zu frames of %zux%zu "
+                                         "(at least 5x5, at most 65535 frames)", n, nu, nv);
+        cudaStream_t s = as_stream(stream);
+        float *work = nullptr;
+        keep_pool_memory();
+        MR_CUDA_TRY(cudaMallocAsync(&work, 4 * n * npix * sizeof(float), s));
+        float *sigma = work, *sq = work + n * npix, *tmp = sq + n * npix, *s2 = tmp + n * npix;
+        kf::stddev_filter<5>(frames_d, static_cast<int>(nu), static_cast<int>(nv), static_cast<unsigned>(n), sq, tmp,
+                             s2, sigma, s);
+        k_weighted_average<<<div_up(npix, 256), 256, 0, s>>>(frames_d, sigma, npix, static_cast<int>(n), out_d);
+        mr_status st = check_launch("k_weighted_average");
+        cudaFreeAsync(work, s);
+        return st;
+    }
     if (npix == 0) return MR_OK;
     k_average<<<div_up(npix, 256), 256, 0, as_stream(stream)>>>(frames_d, npix, static_cast<int>(n), method, out_d);
     return check_launch("k_average");

@@ -30,6 +30,7 @@
 // reference's running (Welford) update; both are exact to about 1e-15, far below the float
 // rounding of the level they produce.
 #include "mr_common.cuh"
+#include "mr_kipl_filters.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -38,23 +39,8 @@
 namespace mr {
 namespace spot2 {
 
-constexpr float kMark = 3.402823466e+38f; // std::numeric_limits<float>::max()
-
-// Source value for output (x, y) at (xx, yy) with kipl's EdgeMirror regions for a kx x ky
-// kernel: the top and bottom ky/2 output rows mirror vertically (no repeat) and clamp
-// horizontally, the left and right kx/2 columns of the other rows mirror horizontally.
-template <int KX, int KY>
-__device__ __forceinline__ float mirror_at(const float *img, int w, int h, int x, int y, int xx, int yy)
-{
-    constexpr int cx = KX / 2, cy = KY / 2;
-    if (y < cy || y >= h - cy) {
-        yy = yy < 0 ? -yy : (yy >= h ? 2 * (h - 1) - yy : yy);
-        xx = min(max(xx, 0), w - 1);
-    } else if (x < cx || x >= w - cx) {
-        xx = xx < 0 ? -xx : (xx >= w ? 2 * (w - 1) - xx : xx);
-    }
-    return __ldg(img + static_cast<size_t>(yy) * w + xx);
-}
+constexpr float kMark = kf::kFloatMax;
+using kf::mirror_at;
 
 // RingDetection (SpotClean.cpp:402-427): 5x5 kernel with 1/12 on the ring and -1 in the
 // centre, its 13 nonzero taps summed in row-major order from 0, then |.|.
@@ -76,50 +62,13 @@ __global__ void __launch_bounds__(256) k_ring(const float *__restrict__ src, int
     det[blockIdx.z * npix + static_cast<size_t>(y) * w + x] = fabsf(acc);
 }
 
-enum { OP_SUM = 0, OP_MIN = 1, OP_MAX = 2 };
-
-// A line of L ones along x or y: TFilter sum from 0 (BoxFilter's passes, SpotClean.cpp:447-465),
-// TErode min from FLT_MAX as std::min(dest, src), TDilate max from -FLT_MAX as std::max.
-template <int L, bool ALONG_Y, int OP>
-__global__ void __launch_bounds__(256) k_line(const float *__restrict__ src, int w, int h, float *__restrict__ dst)
-{
-    const int x = blockIdx.x * 32 + threadIdx.x, y = blockIdx.y * 8 + threadIdx.y;
-    if (x >= w || y >= h) return;
-    const size_t npix = static_cast<size_t>(w) * h;
-    const float *img = src + blockIdx.z * npix;
-    float acc = OP == OP_SUM ? 0.0f : (OP == OP_MIN ? kMark : -kMark);
-#pragma unroll
-    for (int t = 0; t < L; ++t) {
-        const int d = t - L / 2;
-        const float v = ALONG_Y ? mirror_at<1, L>(img, w, h, x, y, x, y + d) : mirror_at<L, 1>(img, w, h, x, y, x + d, y);
-        if (OP == OP_SUM) acc = __fadd_rn(acc, v);
-        else if (OP == OP_MIN) acc = v < acc ? v : acc;
-        else acc = acc < v ? v : acc;
-    }
-    dst[blockIdx.z * npix + static_cast<size_t>(y) * w + x] = acc;
-}
-
-enum { EW_SQR = 0, EW_ABSDIFF = 1, EW_STDDEV = 2 };
-
-// Elementwise steps: kipl::math::sqr, |a - b| (kipl::math::abs of an image difference), and
-// StdDevDetection's sqrt(M1 * (s2 - M * m * m)) with M = 1/9, M1 = 1/8 (SpotClean.cpp:521-545).
-template <int OP>
-__global__ void __launch_bounds__(256) k_elementwise(const float *__restrict__ a, const float *__restrict__ b,
-                                                     size_t n, float *__restrict__ out)
+// |a - b| (kipl::math::abs of an image difference).
+__global__ void __launch_bounds__(256) k_absdiff(const float *__restrict__ a, const float *__restrict__ b, size_t n,
+                                                 float *__restrict__ out)
 {
     for (size_t i = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n;
-         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const float x = a[i];
-        if (OP == EW_SQR) {
-            out[i] = __fmul_rn(x, x);
-        } else if (OP == EW_ABSDIFF) {
-            out[i] = fabsf(__fsub_rn(x, b[i]));
-        } else {
-            constexpr float M = 1.0f / 9.0f, M1 = 1.0f / 8.0f;
-            const float m = b[i];
-            out[i] = __fsqrt_rn(__fmul_rn(M1, __fsub_rn(x, __fmul_rn(__fmul_rn(M, m), m))));
-        }
-    }
+         i += static_cast<size_t>(gridDim.x) * blockDim.x)
+        out[i] = fabsf(__fsub_rn(a[i], b[i]));
 }
 
 // TriKernel statistics (kipl::math::statistics: mean and sqrt(sum (x - mean)^2 / N)) per image
@@ -429,29 +378,9 @@ extern "C" mr_status mr_sigmoid_lut(size_t len, float lambda, float sigma, float
 
 namespace {
 
-template <int L, bool ALONG_Y, int OP>
-void line(const float *src, int w, int h, unsigned nimg, float *dst, cudaStream_t s)
-{
-    spot2::k_line<L, ALONG_Y, OP><<<dim3(div_up(w, 32), div_up(h, 8), nimg), dim3(32, 8), 0, s>>>(src, w, h, dst);
-}
-
-// SpotClean::BoxFilter: sum over dim along x, then along y.
-void box(const float *src, int w, int h, unsigned nimg, int dim, float *tmp, float *dst, cudaStream_t s)
-{
-    using namespace spot2;
-    if (dim == 3) {
-        line<3, false, OP_SUM>(src, w, h, nimg, tmp, s);
-        line<3, true, OP_SUM>(tmp, w, h, nimg, dst, s);
-    } else if (dim == 5) {
-        line<5, false, OP_SUM>(src, w, h, nimg, tmp, s);
-        line<5, true, OP_SUM>(tmp, w, h, nimg, dst, s);
-    } else {
-        line<7, false, OP_SUM>(src, w, h, nimg, tmp, s);
-        line<7, true, OP_SUM>(tmp, w, h, nimg, dst, s);
-    }
-}
-
-unsigned ew_blocks(size_t n) { return static_cast<unsigned>(std::min<size_t>(div_up(n, 256), 148 * 16)); }
+using kf::box;
+using kf::line;
+unsigned ew_blocks(size_t n) { return kf::flat_blocks(n); }
 
 // Detection image of nimg projections into det; X1..X3 are scratch images of the batch.
 mr_status detection(const float *img, int w, int h, unsigned nimg, int method, float gamma, float *det, float *X1,
@@ -465,31 +394,28 @@ mr_status detection(const float *img, int w, int h, unsigned nimg, int method, f
         k_ring<<<grid, block, 0, s>>>(img, w, h, det);
         break;
     case MR_SPOT_STDDEV:
-        k_elementwise<EW_SQR><<<ew_blocks(n), 256, 0, s>>>(img, nullptr, n, X1);
-        box(X1, w, h, nimg, 3, X3, X2, s); // s2
-        box(img, w, h, nimg, 3, X3, X1, s); // m
-        k_elementwise<EW_STDDEV><<<ew_blocks(n), 256, 0, s>>>(X2, X1, n, det);
+        kf::stddev_filter<3>(img, w, h, nimg, X1, X3, X2, det, s);
         break;
     case MR_SPOT_MEDIAN: {
         mr_status st = mr_median_filter(img, w, h, nimg, 1, 5, X1, s);
         if (st == MR_OK) st = mr_median_filter(X1, w, h, nimg, 5, 1, X2, s);
         if (st != MR_OK) return st;
-        k_elementwise<EW_ABSDIFF><<<ew_blocks(n), 256, 0, s>>>(img, X2, n, det);
+        k_absdiff<<<ew_blocks(n), 256, 0, s>>>(img, X2, n, det);
         break;
     }
     case MR_SPOT_MINMAX:
-        line<5, true, OP_MIN>(img, w, h, nimg, X1, s);
-        line<5, false, OP_MIN>(X1, w, h, nimg, X2, s);
-        line<5, true, OP_MAX>(img, w, h, nimg, X1, s);
-        line<5, false, OP_MAX>(X1, w, h, nimg, X3, s);
-        k_elementwise<EW_ABSDIFF><<<ew_blocks(n), 256, 0, s>>>(X3, X2, n, det);
+        line<5, true, kf::OP_MIN>(img, w, h, nimg, X1, s);
+        line<5, false, kf::OP_MIN>(X1, w, h, nimg, X2, s);
+        line<5, true, kf::OP_MAX>(img, w, h, nimg, X1, s);
+        line<5, false, kf::OP_MAX>(X1, w, h, nimg, X3, s);
+        k_absdiff<<<ew_blocks(n), 256, 0, s>>>(X3, X2, n, det);
         break;
     case MR_SPOT_TRIKERNEL: {
         MR_CUDA_TRY(cudaMemsetAsync(det, 0, n * sizeof(float), s));
         double *partial = stats, *mean = stats + static_cast<size_t>(nimg) * kStatBlocks;
         for (int size = 3; size <= 7; size += 2) {
             box(img, w, h, nimg, size, X3, X1, s);
-            k_elementwise<EW_ABSDIFF><<<ew_blocks(n), 256, 0, s>>>(img, X1, n, X2);
+            k_absdiff<<<ew_blocks(n), 256, 0, s>>>(img, X1, n, X2);
             k_stat_partial<false><<<dim3(kStatBlocks, nimg), 256, 0, s>>>(X2, npix, mean, partial);
             k_stat_final<false><<<nimg, 32, 0, s>>>(partial, npix, gamma, mean, level);
             k_stat_partial<true><<<dim3(kStatBlocks, nimg), 256, 0, s>>>(X2, npix, mean, partial);

@@ -162,8 +162,6 @@ class FullLogNorm:
     def _average(self, frames: torch.Tensor) -> torch.Tensor:
         n, nv, nu = frames.shape
         m = _AVERAGE[self.referenceaverage.lower()]
-        if m == 3:
-            raise ReconException("ImageWeightedAverage is not supported by this module; use ImageAverage")
         out = torch.empty((nv, nu), dtype=torch.float32, device=frames.device)
         check(L.lib().mr_reference_average(frames.data_ptr(), nu, nv, n, m, out.data_ptr(), _stream()))
         return out

@@ -55,7 +55,9 @@ enum { MR_F32 = 0, MR_BF16 = 1, MR_F16 = 2 };
  *   (core/algorithms/ImagingAlgorithms/src/averageimage.cpp:35-61) and
  *   ProjectionReader::GetProjectionDose (frameworks/tomography/Framework/ReconFramework/
  *   src/ProjectionReader.cpp:752-783).
- * method: 0 ImageSum, 1 ImageAverage, 2 ImageMedian, 4 ImageMin, 5 ImageMax
+ * method: 0 ImageSum, 1 ImageAverage, 2 ImageMedian (at most 64 frames), 3 ImageWeightedAverage
+ * (per-frame 5x5 StdDevFilter with EdgeMirror edges, weights 1/sigma, or 1/(number of pixels)
+ * where sigma is 0; frames at least 5x5; scratch: four images per frame), 4 ImageMin, 5 ImageMax
  * (averageimage.h:16-23). frames_d: [n][nv][nu] float. */
 mr_status mr_reference_average(const float *frames_d, size_t nu, size_t nv, size_t n, int method, float *out_d,
                                void *stream);

@@ -71,13 +71,35 @@ static void fft_c2c(double *re, double *im, size_t n, int sign)
 
 /* ------------------------------------------------------- reference averaging */
 
-/* AverageImage::operator() (core/algorithms/ImagingAlgorithms/src/averageimage.cpp:35-219).
- * The weighted average (StdDevFilter weights, :123-172) is not restated here. */
+static void stddev_filter(const float *img, int w, int h, int dim, float *out);
+
+/* AverageImage::operator() (core/algorithms/ImagingAlgorithms/src/averageimage.cpp:35-219). */
 int orc_average(const float *stack, size_t nu, size_t nv, size_t n, int method, float *out)
 {
     const size_t npix = nu * nv;
     if (n == 0) return -1;
     switch (method) {
+    case ORC_AVG_WEIGHTED: {
+        /* ComputeWeightedAverage (:123-172): per frame a 5x5 StdDevFilter (EdgeMirror); per
+         * pixel weight 1/sigma, or 1/(number of pixels) where sigma is 0; the weighted sum and
+         * the weight sum in frame order, then their quotient. */
+        if (nu < 5 || nv < 5) return -1;
+        float *sig = (float *)malloc(n * npix * sizeof(float));
+        for (size_t i = 0; i < n; ++i) stddev_filter(stack + i * npix, (int)nu, (int)nv, 5, sig + i * npix);
+        const float zw = 1.0f / (float)npix;
+        for (size_t j = 0; j < npix; ++j) {
+            float ws = 0.0f, acc = 0.0f;
+            for (size_t i = 0; i < n; ++i) {
+                const float sg = sig[i * npix + j];
+                const float wt = sg != 0.0f ? 1.0f / sg : zw;
+                ws += wt;
+                acc += wt * stack[i * npix + j];
+            }
+            out[j] = acc / ws;
+        }
+        free(sig);
+        return 0;
+    }
     case ORC_AVG_SUM:
     case ORC_AVG_AVERAGE: {
         for (size_t j = 0; j < npix; ++j) out[j] = 0.0f;
@@ -1618,6 +1640,25 @@ static void box_filter(const float *img, int w, int h, int dim, float *tmp, floa
     kipl_filter(tmp, w, h, ones, 1, dim, KF_SUM, out);
 }
 
+/* kipl::filters::StdDevFilter(dim, EdgeMirror)::operator() (core/kipl/kipl/src/filters/
+ * stddevfilter.cpp:25-64): box sums of img^2 and img, sqrt(M1 * (s2 - M * m * m)) with
+ * M = 1/(dim*dim), M1 = 1/(dim*dim - 1) in float. */
+static void stddev_filter(const float *img, int w, int h, int dim, float *out)
+{
+    const size_t n = (size_t)w * h;
+    float *a = (float *)calloc(n, sizeof(float)), *b = (float *)malloc(n * sizeof(float));
+    float *c = (float *)malloc(n * sizeof(float)), *d = (float *)malloc(n * sizeof(float));
+    for (size_t i = 0; i < n; ++i) a[i] = img[i] * img[i];
+    box_filter(a, w, h, dim, c, b); /* s2 */
+    box_filter(img, w, h, dim, c, d); /* m */
+    const float M = 1 / (float)(dim * dim), M1 = 1 / (float)(dim * dim - 1);
+    for (size_t i = 0; i < n; ++i) out[i] = (float)sqrt((double)(M1 * (b[i] - M * d[i] * d[i])));
+    free(a);
+    free(b);
+    free(c);
+    free(d);
+}
+
 /* kipl::math::statistics (core/kipl/kipl/include/math/core/image_statistics.hpp:197-219):
  * running mean and variance in double, variance / N, standard deviation. */
 static void running_stats(const float *x, size_t n, double *mean, double *sd)
@@ -1648,12 +1689,8 @@ static int spot_detection(const float *img, int w, int h, int method, float gamm
         const float k[25] = {z, wv, wv, wv, z, wv, z, z, z, wv, wv, z, cv, z, wv, wv, z, z, z, wv, z, wv, wv, wv, z};
         kipl_filter(img, w, h, k, 5, 5, KF_SUM, det);
         for (size_t i = 0; i < n; ++i) det[i] = fabsf(det[i]);
-    } else if (method == 0) { /* StdDevDetection(img, 3) */
-        for (size_t i = 0; i < n; ++i) a[i] = img[i] * img[i];
-        box_filter(a, w, h, 3, c, b); /* s2 */
-        box_filter(img, w, h, 3, c, d); /* m */
-        const float M = 1 / (float)(3 * 3), M1 = 1 / (float)(3 * 3 - 1);
-        for (size_t i = 0; i < n; ++i) det[i] = (float)sqrt((double)(M1 * (b[i] - M * d[i] * d[i])));
+    } else if (method == 0) { /* StdDevDetection(img, 3): the same arithmetic as StdDevFilter */
+        stddev_filter(img, w, h, 3, det);
     } else if (method == 2) { /* MedianDetection: 1x5 then 5x1 median, |img - median| */
         orc_median_filter(img, (size_t)w, (size_t)h, 1, 5, a);
         orc_median_filter(a, (size_t)w, (size_t)h, 5, 1, b);

@@ -52,7 +52,7 @@ def _counts(seed, nproj, nv, nu):
 
 
 @pytest.mark.parametrize("usenorm", [False, True])
-@pytest.mark.parametrize("method", ["ImageAverage", "ImageSum", "ImageMedian", "ImageMax"])
+@pytest.mark.parametrize("method", ["ImageAverage", "ImageSum", "ImageMedian", "ImageMax", "ImageWeightedAverage"])
 def test_fulllognorm_module(cuda, usenorm, method):
     proj, flats, darks = _counts(1, 13, 20, 36)
     roi = (3, 2, 30, 17)
@@ -103,6 +103,21 @@ def test_lognorm_rejects_bad_arguments(cuda):
         mod = M.FullLogNorm()
         mod.Configure(M.ReconConfig(), {"usenormregion": "false", "referenceaverage": "ImageAverage"})
         mod.Process(torch.zeros((1, 4, 4), device=cuda), {})
+
+
+@pytest.mark.parametrize("shape", [(1, 5, 5), (3, 6, 7), (10, 33, 41), (20, 256, 300)])
+def test_weighted_average_matches_oracle(cuda, shape):
+    """ImageWeightedAverage on the GPU: per-frame 5x5 standard deviation (EdgeMirror) and the
+    1/sigma weights, bit for bit."""
+    rng = np.random.default_rng(sum(shape))
+    st = rng.poisson(1000, shape).astype(np.float32)
+    st[:, 2:5, 1:4] = 700.0
+    st[0, 0, :] = 1e4
+    out = torch.empty(shape[1:], device=cuda)
+    x = dev(st, cuda)
+    L.check(L.lib().mr_reference_average(x.data_ptr(), shape[2], shape[1], shape[0], 3, out.data_ptr(), stream()))
+    exp = O.average(st, "ImageWeightedAverage")
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), exp.view(np.uint32))
 
 
 # ------------------------------------------------------------ ProjectionFilterSingle

@@ -66,7 +66,8 @@ def test_fdk_prepare_then_bp_equals_fdk():
 
 
 @pytest.mark.parametrize("usenorm", [False, True])
-@pytest.mark.parametrize("method", ["ImageAverage", "ImageSum", "ImageMedian", "ImageMin", "ImageMax"])
+@pytest.mark.parametrize("method", ["ImageAverage", "ImageSum", "ImageMedian", "ImageMin", "ImageMax",
+                                    "ImageWeightedAverage"])
 def test_fulllognorm_bit_exact(ref_lib, usenorm, method):
     rng = _rng(30)
     nproj, nv, nu = 11, 10, 24
@@ -111,12 +112,25 @@ def test_projfilter_bad_cutoff(ref_lib):
         O.ref_projfilter(np.zeros((1, 2, 64), np.float32), "hanning", 0.7)
 
 
-@pytest.mark.parametrize("method", ["ImageSum", "ImageAverage", "ImageMedian", "ImageMin", "ImageMax"])
+@pytest.mark.parametrize("method", ["ImageSum", "ImageAverage", "ImageMedian", "ImageMin", "ImageMax",
+                                    "ImageWeightedAverage"])
 @pytest.mark.parametrize("n", [1, 4, 5])
 def test_average(ref_lib, method, n):
     rng = _rng(50 + n)
     stack = np.round(rng.normal(1000, 30, (n, 6, 9))).astype(np.float32)
     assert np.array_equal(O.average(stack, method), O.average(stack, method, use_ref=True))
+
+
+@pytest.mark.parametrize("shape", [(1, 5, 5), (3, 6, 7), (10, 33, 41), (20, 64, 64)])
+def test_weighted_average_bit_exact(ref_lib, shape):
+    """ImageWeightedAverage, FullLogNorm's default: 5x5 StdDevFilter weights with EdgeMirror
+    edges, flat patches (sigma 0: weight 1/number of pixels), a bright row."""
+    rng = _rng(sum(shape))
+    st = rng.poisson(1000, shape).astype(np.float32)
+    st[:, 2:5, 1:4] = 700.0
+    st[0, 0, :] = 1e4
+    a = O.average(st, "ImageWeightedAverage")
+    assert np.array_equal(a.view(np.uint32), O.average(st, "ImageWeightedAverage", use_ref=True).view(np.uint32))
 
 
 def test_frame_dose(ref_lib):
