@@ -45,6 +45,8 @@ _PROTOS = {
     "mr_lognorm_doselog": (c_int, [P_float, c_size, c_float, P_float]),
     "mr_lognorm_apply": (c_int, [c_void, c_int, c_size, c_size, c_void, c_void, c_void, c_size, c_int, c_int,
                                  c_void, c_void]),
+    "mr_lognorm_apply_lut": (c_int, [c_void, c_int, c_size, c_size, c_void, c_void, c_void, c_size, c_int, c_int,
+                                     c_void, c_void]),
     "mr_morphspotclean": (c_int, [c_void, c_size, c_size, c_size, c_int, c_int, P_float, P_float, c_int, c_int, c_float,
                                   c_float, c_int, c_void]),
     "mr_wavelet_kernel": (c_int, [ctypes.c_char_p, P_int, P_int, P_float]),

@@ -8,6 +8,7 @@
 #include "mr_kipl_filters.cuh"
 
 #include <mutex>
+#include <vector>
 
 #include <cmath>
 #include <cstring>
@@ -211,6 +212,62 @@ __global__ void k_lognorm(const T *__restrict__ in, size_t npix, const float *__
     }
 }
 
+// FullLogNorm with uselut (NormPlugins.cpp:455-480): LogLUT of I - D, then logflat - l + dose,
+// or -l + (dose - doselog[0]) without flats. table: len entries, then lo, hi, slope, intercept;
+// an index outside the table (NaN, or a value the float arithmetic maps past it) is clamped.
+template <typename T>
+__global__ void k_lognorm_lut(const T *__restrict__ in, size_t npix, const float *__restrict__ dark,
+                              const float *__restrict__ logflat, const float *__restrict__ doselog, size_t ndose,
+                              int ndc, int nob, const float *__restrict__ table, int len, float *__restrict__ out)
+{
+    const size_t j = blockIdx.y;
+    float dose = ndose != 1 ? doselog[j] : doselog[0];
+    if (!nob) dose = __fsub_rn(dose, doselog[0]);
+    const float lo = table[len], hi = table[len + 1], slope = table[len + 2], icpt = table[len + 3];
+    const T *src = in + j * npix;
+    float *dst = out + j * npix;
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < npix;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const float v = ndc ? __fsub_rn(static_cast<float>(src[i]), dark[i]) : static_cast<float>(src[i]);
+        int idx;
+        if (v < lo) {
+            idx = 0;
+        } else if (hi < v) {
+            idx = len - 1;
+        } else {
+            const float f = __fadd_rn(__fmul_rn(v, slope), icpt);
+            idx = f >= static_cast<float>(len) ? len - 1 : (f >= 0.0f ? min(static_cast<int>(f), len - 1) : 0);
+        }
+        const float l = __ldg(table + idx);
+        dst[i] = nob ? __fadd_rn(__fsub_rn(logflat[i], l), dose) : __fadd_rn(-l, dose);
+    }
+}
+
+// LogLUT(1 << 16, 0, 65535) as FullLogNorm constructs it (NormPlugins.cpp:245;
+// core/kipl/kipl/src/math/LUTCollection.cpp:11-36): with lo = 0 the first entry is log(1/slope),
+// entry i >= 1 is log(x) with x stepping by 1/slope in float from 1/slope, in the double log
+// the reference calls (host code, glibc, no contraction). Built once per process.
+static const std::vector<float> &log_lut_table()
+{
+    static std::vector<float> table;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        const size_t len = size_t(1) << 16;
+        const float lo = 0.0f, hi = static_cast<float>((1 << 16) - 1);
+        const float slope = static_cast<float>(len - 1) / (hi - lo), icpt = -slope * lo + 0.5f;
+        const float delta = 1.0f / slope;
+        table.resize(len + 4);
+        table[0] = static_cast<float>(std::log(static_cast<double>(delta)));
+        float x = delta;
+        for (size_t i = 1; i < len; ++i, x += delta) table[i] = static_cast<float>(std::log(static_cast<double>(x)));
+        table[len] = lo;
+        table[len + 1] = hi;
+        table[len + 2] = slope;
+        table[len + 3] = icpt;
+    });
+    return table;
+}
+
 } // namespace mr
 
 using namespace mr;
@@ -346,6 +403,40 @@ mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t n
         k_lognorm<float><<<g, 256, 0, as_stream(stream)>>>(static_cast<const float *>(in_d), npix, dark_d, logflat_d,
                                                            doselog_d, ndose, ndc, nob, vec, out_d);
     return check_launch("k_lognorm");
+}
+
+mr_status mr_lognorm_apply_lut(const void *in_d, int in_dtype, size_t npix, size_t nproj, const float *dark_d,
+                               const float *logflat_d, const float *doselog_d, size_t ndose, int ndc, int nob,
+                               float *out_d, void *stream)
+{
+    if (!in_d || !out_d || !doselog_d || (ndc && !dark_d) || (nob && !logflat_d))
+        return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply_lut: null pointer");
+    if (in_dtype != MR_U16 && in_dtype != MR_F32)
+        return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply_lut: input must be u16 or f32");
+    if (ndose != 1 && ndose != nproj) return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply_lut: ndose must be 1 or nproj");
+    if (nproj > 65535) return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply_lut: more than 65535 projections per call");
+    if (npix == 0 || nproj == 0) return MR_OK;
+    const std::vector<float> &table = log_lut_table();
+    cudaStream_t s = as_stream(stream);
+    float *lut = nullptr;
+    keep_pool_memory();
+    MR_CUDA_TRY(cudaMallocAsync(&lut, table.size() * sizeof(float), s));
+    mr_status st = MR_OK;
+    cudaError_t e = cudaMemcpyAsync(lut, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) st = fail(MR_ERR_CUDA, "mr_lognorm_apply_lut: table upload: %s", cudaGetErrorString(e));
+    if (st == MR_OK) {
+        const int len = static_cast<int>(table.size() - 4);
+        dim3 g(std::min<unsigned>(div_up(npix, 256), 256u), static_cast<unsigned>(nproj));
+        if (in_dtype == MR_U16)
+            k_lognorm_lut<uint16_t><<<g, 256, 0, s>>>(static_cast<const uint16_t *>(in_d), npix, dark_d, logflat_d,
+                                                      doselog_d, ndose, ndc, nob, lut, len, out_d);
+        else
+            k_lognorm_lut<float><<<g, 256, 0, s>>>(static_cast<const float *>(in_d), npix, dark_d, logflat_d, doselog_d,
+                                                   ndose, ndc, nob, lut, len, out_d);
+        st = check_launch("k_lognorm_lut");
+    }
+    cudaFreeAsync(lut, s);
+    return st;
 }
 
 } // extern "C"

@@ -139,8 +139,6 @@ class FullLogNorm:
         self.nOBCount, self.nDCCount = int(pi.nOBCount), int(pi.nDCCount)
         self.bUseNormROI = _string2bool(_get(parameters, "usenormregion"))
         self.bUseLUT = _string2bool(parameters.get("uselut", "false"))
-        if self.bUseLUT:
-            raise ReconException("FullLogNorm: uselut=true is not supported by this module")
         self.referenceaverage = _get(parameters, "referenceaverage")
         if self.referenceaverage.lower() not in _AVERAGE:
             raise ReconException(f"Unknown reference average method {self.referenceaverage}")
@@ -148,8 +146,8 @@ class FullLogNorm:
         return 0
 
     def GetParameters(self) -> dict:
-        return {"usenormregion": "true" if self.bUseNormROI else "false", "uselut": "false",
-                "referenceaverage": self.referenceaverage}
+        return {"usenormregion": "true" if self.bUseNormROI else "false",
+                "uselut": "true" if self.bUseLUT else "false", "referenceaverage": self.referenceaverage}
 
     def _frame_doses(self, frames: torch.Tensor) -> np.ndarray:
         n, nv, nu = frames.shape
@@ -229,9 +227,10 @@ class FullLogNorm:
             out = img if img.dtype == torch.float32 else torch.empty(img.shape, dtype=torch.float32, device=img.device)
         elif out.shape != img.shape or out.dtype != torch.float32 or not out.is_contiguous():
             raise ReconException("FullLogNorm: out must be a contiguous float32 tensor of the projections' shape")
-        check(L.lib().mr_lognorm_apply(img.data_ptr(), _DT[img.dtype], nv * nu, nproj, self.mDark.data_ptr(),
-                                       self.mFlatField.data_ptr(), doselog.data_ptr(), doselog.numel(),
-                                       int(self.nDCCount > 0), int(self.nOBCount > 0), out.data_ptr(), _stream()))
+        apply = L.lib().mr_lognorm_apply_lut if self.bUseLUT else L.lib().mr_lognorm_apply
+        check(apply(img.data_ptr(), _DT[img.dtype], nv * nu, nproj, self.mDark.data_ptr(), self.mFlatField.data_ptr(),
+                    doselog.data_ptr(), doselog.numel(), int(self.nDCCount > 0), int(self.nOBCount > 0),
+                    out.data_ptr(), _stream()))
         return out
 
 

@@ -84,6 +84,14 @@ mr_status mr_lognorm_doselog(const float *dose_h, size_t n, float darkdose, floa
 mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t nproj, const float *dark_d,
                            const float *logflat_d, const float *doselog_d, size_t ndose, int ndc, int nob,
                            float *out_d, void *stream);
+/* mr_lognorm_apply_lut: the module's uselut path (NormPlugins.cpp:455-480): LogLUT(1 << 16, 0,
+ * 65535) of I - D (log of the value rounded half up, log(1) = 0 at and below 0, log(65535)
+ * above), then logflat - l + dose, or -l + (dose - doselog[0]) without flats. The table is
+ * built on the host with the reference's double log, so results equal the reference bit for
+ * bit. Same arguments as mr_lognorm_apply; scratch: the 256 KiB table. */
+mr_status mr_lognorm_apply_lut(const void *in_d, int in_dtype, size_t npix, size_t nproj, const float *dark_d,
+                               const float *logflat_d, const float *doselog_d, size_t ndose, int ndc, int nob,
+                               float *out_d, void *stream);
 
 /* ---------------------------------------------------------------------------------
  * MorphSpotClean, replace mode: ImagingAlgorithms::MorphSpotClean::process

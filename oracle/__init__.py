@@ -148,18 +148,28 @@ def lognorm_doselog(doses, darkdose: float) -> np.ndarray:
     return out
 
 
-def lognorm_apply(proj, dark, logflat, doselog, ndc=True, nob=True) -> np.ndarray:
-    """FullLogNorm::ProcessCore 3D (NormPlugins.cpp:411-552) on float projections."""
+def lognorm_apply(proj, dark, logflat, doselog, ndc=True, nob=True, uselut=False) -> np.ndarray:
+    """FullLogNorm::ProcessCore 3D (NormPlugins.cpp:411-552) on float projections; uselut
+    selects the LogLUT path."""
     out = np.array(proj, dtype=np.float32, copy=True, order="C")
     dark, logflat, doselog = _f32(dark), _f32(logflat), _f32(doselog)
     nproj = out.shape[0]
     npix = out[0].size
-    orc().orc_lognorm_apply(_p(out), _sz(npix), _sz(nproj), _p(dark), _p(logflat), _p(doselog),
-                            _sz(doselog.size), int(ndc), int(nob))
+    fn = orc().orc_lognorm_apply_lut if uselut else orc().orc_lognorm_apply
+    fn(_p(out), _sz(npix), _sz(nproj), _p(dark), _p(logflat), _p(doselog), _sz(doselog.size), int(ndc), int(nob))
     return out
 
 
-def ref_fulllognorm(proj, darks, flats, method="ImageAverage", usenormregion=False, dose_roi=(0, 0, 0, 0)):
+def log_lut():
+    """FullLogNorm's LogLUT(1 << 16, 0, 65535): (table, (lo, hi, slope, intercept))."""
+    lut = np.empty(1 << 16, np.float32)
+    param = np.empty(4, np.float32)
+    orc().orc_log_lut(_p(lut), _p(param))
+    return lut, param
+
+
+def ref_fulllognorm(proj, darks, flats, method="ImageAverage", usenormregion=False, dose_roi=(0, 0, 0, 0),
+                    uselut=False):
     """The reference FullLogNorm module on float projections. Returns (out, dark, logflat, doses, (dd, fd))."""
     out = np.array(proj, dtype=np.float32, copy=True, order="C")
     darks, flats = _f32(darks), _f32(flats)
@@ -171,7 +181,7 @@ def ref_fulllognorm(proj, darks, flats, method="ImageAverage", usenormregion=Fal
     roi = np.asarray(dose_roi, dtype=np.uintp)
     _check_ref(ref().ref_fulllognorm(_p(out), _sz(nu), _sz(nv), _sz(nproj), _p(darks), _sz(darks.shape[0]),
                                      _p(flats), _sz(flats.shape[0]), AVERAGE[method], int(usenormregion),
-                                     _p(roi, _SZ), _p(dark), _p(logflat), _p(doses), _p(rd)))
+                                     _p(roi, _SZ), _p(dark), _p(logflat), _p(doses), _p(rd), int(uselut)))
     return out, dark, logflat, doses, (float(rd[0]), float(rd[1]))
 
 

@@ -72,6 +72,7 @@ static void fft_c2c(double *re, double *im, size_t n, int sign)
 /* ------------------------------------------------------- reference averaging */
 
 static void stddev_filter(const float *img, int w, int h, int dim, float *out);
+static float lut_apply(const float *lut, size_t len, const float *param, float v);
 
 /* AverageImage::operator() (core/algorithms/ImagingAlgorithms/src/averageimage.cpp:35-219). */
 int orc_average(const float *stack, size_t nu, size_t nv, size_t n, int method, float *out)
@@ -192,6 +193,49 @@ void orc_lognorm_apply(float *proj, size_t npix, size_t nproj, const float *dark
                 p[i] = nob ? (logflat[i] - logf(v)) + dose : -logf(v) + dose;
         }
     }
+}
+
+/* kipl::math::LogLUT(1 << 16, 0, 65535) as FullLogNorm builds it (NormPlugins.cpp:245;
+ * core/kipl/kipl/src/math/LUTCollection.cpp:11-36 over LUTbase.cpp:12-20): slope
+ * (len - 1) / (hi - lo) and intercept -slope * lo + 0.5 in float; with lo = 0 the first entry
+ * is log(1 / slope) and entry i >= 1 log(x), x stepping from 1 / slope by 1 / slope in float;
+ * the double log the reference calls, stored as float. param: lo, hi, slope, intercept. */
+void orc_log_lut(float *lut, float *param)
+{
+    const size_t len = (size_t)1 << 16;
+    const float lo = 0.0f, hi = (float)((1 << 16) - 1);
+    const float slope = (float)(len - 1) / (hi - lo), intercept = -slope * lo + 0.5f;
+    const float delta = 1.0f / slope;
+    float x = delta;
+    lut[0] = (float)log((double)delta);
+    for (size_t i = 1; i < len; ++i, x += delta) lut[i] = (float)log((double)x);
+    param[0] = lo;
+    param[1] = hi;
+    param[2] = slope;
+    param[3] = intercept;
+}
+
+/* FullLogNorm::ProcessCore 3D with uselut (NormPlugins.cpp:455-480): I - D (when there are
+ * darks), the LogLUT of that (BasicLUT: below lo the first entry, above hi the last, else entry
+ * (size_t)(v * slope + intercept), clamped to the table where the reference reads past it),
+ * then logflat - l + dose, or -l + (dose - doselog[0]) without flats. */
+void orc_lognorm_apply_lut(float *proj, size_t npix, size_t nproj, const float *dark, const float *logflat,
+                           const float *doselog, size_t ndose, int ndc, int nob)
+{
+    const size_t len = (size_t)1 << 16;
+    float *lut = (float *)malloc(len * sizeof(float)), param[4];
+    orc_log_lut(lut, param);
+    for (size_t j = 0; j < nproj; ++j) {
+        float *p = proj + j * npix;
+        float dose = ndose != 1 ? doselog[j] : doselog[0];
+        if (!nob) dose -= doselog[0];
+        for (size_t i = 0; i < npix; ++i) {
+            const float v = ndc ? p[i] - dark[i] : p[i];
+            const float l = lut_apply(lut, len, param, v);
+            p[i] = nob ? (logflat[i] - l) + dose : -l + dose;
+        }
+    }
+    free(lut);
 }
 
 /* -------------------------------------------------- ProjectionFilterSingle */

@@ -33,6 +33,9 @@ void orc_lognorm_logflat(const float *dark, const float *flat, size_t npix, int 
 void orc_lognorm_doselog(const float *doses, size_t nproj, float darkdose, float *doselog);
 void orc_lognorm_apply(float *proj, size_t npix, size_t nproj, const float *dark, const float *logflat,
                        const float *doselog, size_t ndose, int ndc, int nob);
+void orc_log_lut(float *lut, float *param);
+void orc_lognorm_apply_lut(float *proj, size_t npix, size_t nproj, const float *dark, const float *logflat,
+                           const float *doselog, size_t ndose, int ndc, int nob);
 
 /* ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:120-376) */
 enum { ORC_FILTER_RAMLAK = 0, ORC_FILTER_SHEPPLOGAN, ORC_FILTER_HANNING, ORC_FILTER_HAMMING, ORC_FILTER_BUTTERWORTH };

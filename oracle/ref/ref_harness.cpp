@@ -140,10 +140,11 @@ int ref_average(const float *stack, size_t nu, size_t nv, size_t n, int method, 
 // FullLogNorm: reference preparation (ReferenceLoader + SetReferenceImages) and
 // ProcessCore 3D (NormPlugins.cpp:411-552) on projections [nproj][nv][nu].
 // dose_roi is in projection coordinates (x0,y0,x1,y1); all-zero disables dose ROI use.
+// uselut selects the module's LogLUT path.
 int ref_fulllognorm(float *proj, size_t nu, size_t nv, size_t nproj,
                     const float *darks, size_t ndark, const float *flats, size_t nflat,
                     int refavg, int usenormregion, const size_t *dose_roi,
-                    float *dark_out, float *flat_out, float *doses_out, float *refdoses_out)
+                    float *dark_out, float *flat_out, float *doses_out, float *refdoses_out, int uselut)
 {
     return guarded([&] {
         FullLogNorm mod;
@@ -153,7 +154,7 @@ int ref_fulllognorm(float *proj, size_t nu, size_t nv, size_t nproj,
         std::memcpy(cfg.ProjectionInfo.dose_roi, dose_roi, 4 * sizeof(size_t));
         std::map<std::string, std::string> par;
         par["usenormregion"] = usenormregion ? "true" : "false";
-        par["uselut"] = "false";
+        par["uselut"] = uselut ? "true" : "false";
         ImagingAlgorithms::AverageImage::eAverageMethod m =
             static_cast<ImagingAlgorithms::AverageImage::eAverageMethod>(refavg);
         par["referenceaverage"] = enum2string(m);

@@ -105,6 +105,42 @@ def test_lognorm_rejects_bad_arguments(cuda):
         mod.Process(torch.zeros((1, 4, 4), device=cuda), {})
 
 
+@pytest.mark.parametrize("dtype", ["u16", "f32"])
+@pytest.mark.parametrize("ndc,nob", [(1, 1), (0, 1), (1, 0), (0, 0)])
+def test_lognorm_lut_bit_exact(cuda, dtype, ndc, nob):
+    """The uselut path through the C ABI with the oracle's reference images: the LogLUT is
+    built on the host with the reference's double log, so the GPU equals the oracle bit for bit
+    (values at or below 0, above 65535, and per-projection doses included)."""
+    proj, flats, darks = _counts(3, 13, 20, 36)
+    proj[0, 1, :3] = 65000
+    refs = O.lognorm_refs(darks.astype(np.float32), flats.astype(np.float32))
+    dl = np.linspace(-0.1, 0.2, proj.shape[0]).astype(np.float32)
+    exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, dl, ndc=bool(ndc), nob=bool(nob),
+                          uselut=True)
+    src = dev(proj, cuda) if dtype == "u16" else dev(proj.astype(np.float32), cuda)
+    out = torch.empty(proj.shape, dtype=torch.float32, device=cuda)
+    d, lf, dd = dev(refs.dark, cuda), dev(refs.logflat, cuda), dev(dl, cuda)
+    L.check(L.lib().mr_lognorm_apply_lut(src.data_ptr(), L.MR_U16 if dtype == "u16" else L.MR_F32, 20 * 36,
+                                         proj.shape[0], d.data_ptr(), lf.data_ptr(), dd.data_ptr(), dl.size, ndc, nob,
+                                         out.data_ptr(), stream()))
+    assert np.array_equal(out.cpu().numpy().view(np.uint32), exp.view(np.uint32))
+
+
+def test_fulllognorm_lut_module(cuda):
+    """The module with uselut=true: the LUT path after the module's own reference images (whose
+    log(flat) is CUDA logf, within 1 ulp of glibc)."""
+    proj, flats, darks = _counts(4, 13, 20, 36)
+    mod = M.FullLogNorm()
+    mod.Configure(M.ReconConfig(), {"usenormregion": "false", "uselut": "true", "referenceaverage": "ImageAverage"})
+    assert mod.GetParameters()["uselut"] == "true"
+    mod.SetReferenceImages(dev(darks, cuda), dev(flats, cuda))
+    out = mod.Process(dev(proj, cuda), {}).cpu().numpy()
+    refs = O.lognorm_refs(darks.astype(np.float32), flats.astype(np.float32))
+    exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, np.zeros(1, np.float32), uselut=True)
+    tol = 2 * np.spacing(np.float32(np.abs(refs.logflat).max() + 12.0))
+    assert np.abs(out.astype(np.float64) - exp).max() <= tol
+
+
 @pytest.mark.parametrize("shape", [(1, 5, 5), (3, 6, 7), (10, 33, 41), (20, 256, 300)])
 def test_weighted_average_matches_oracle(cuda, shape):
     """ImageWeightedAverage on the GPU: per-frame 5x5 standard deviation (EdgeMirror) and the

@@ -91,6 +91,33 @@ def test_fulllognorm_bit_exact(ref_lib, usenorm, method):
     assert np.array_equal(out, out_r)
 
 
+@pytest.mark.parametrize("usenorm", [False, True])
+@pytest.mark.parametrize("refs_present", [(4, 5), (0, 5), (4, 0)])
+@pytest.mark.parametrize("method", ["ImageAverage", "ImageWeightedAverage"])
+def test_fulllognorm_lut_bit_exact(ref_lib, usenorm, refs_present, method):
+    """FullLogNorm with uselut=true: LogLUT of I - D (values at or below 0, above 65535, and
+    exactly half way between integers included), with and without darks or flats."""
+    rng = _rng(31)
+    ndark, nflat = refs_present
+    nproj, nv, nu = 11, 10, 24
+    darks = np.round(rng.normal(100, 3, (4, nv, nu))).astype(np.float32)[:ndark]
+    flats = (rng.poisson(30000, (5, nv, nu)) + 100).astype(np.float32)[:nflat]
+    proj = (rng.poisson(20000, (nproj, nv, nu)) + 100).astype(np.float32)
+    proj[0, 0, :5] = 50
+    proj[1, 1, :3] = 70000.0
+    proj[2, 2, :4] = [100.5, 101.5, 102.25, 65635.5]
+    roi = (2, 2, 20, 9)
+    out_r, _, _, _, _ = O.ref_fulllognorm(proj, darks, flats, method, usenorm, roi, uselut=True)
+    refs = O.lognorm_refs(darks, flats, method, usenorm, roi)
+    if usenorm:
+        doses = np.array([O.frame_dose(proj[i], roi) for i in range(nproj)], np.float32)
+        dl = O.lognorm_doselog(doses, refs.darkdose)
+    else:
+        dl = np.zeros(1, np.float32)
+    out = O.lognorm_apply(proj, refs.dark, refs.logflat, dl, ndc=ndark > 0, nob=nflat > 0, uselut=True)
+    assert np.array_equal(out.view(np.uint32), out_r.view(np.uint32))
+
+
 @pytest.mark.parametrize("ftype", ["ram-lak", "shepp-logan", "hanning", "hamming", "butterworth"])
 @pytest.mark.parametrize("nu,pd,cutoff", [(64, 2, 0.5), (50, 1, 0.35), (33, 0, 0.2)])
 def test_projfilter(ref_lib, ftype, nu, pd, cutoff):
