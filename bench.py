@@ -43,7 +43,7 @@ def workload(small: bool):
     if small:
         return dict(name="FDK 256^3 from 256 projections of 256x256 (profiling case)", nu=256, nv=256, nproj=256,
                     sod=300.0, sdd=600.0, pitch=0.8, voxel=0.4, i0=50000.0)
-    # BASELINE precision form: FDK cone-beam geometry of the 512^3 case scaled x2
+    # precision form: the FDK cone-beam geometry of the 512^3 case scaled x2
     return dict(name="FDK 1024^3 from 1024 projections of 1024x1024", nu=1024, nv=1024, nproj=1024, sod=300.0,
                 sdd=600.0, pitch=0.2, voxel=0.1, i0=50000.0)
 

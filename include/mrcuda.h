@@ -35,7 +35,7 @@ enum {
     MR_ERR_ARGUMENT = 1,    /* invalid size, pointer or parameter (nothing launched) */
     MR_ERR_CUDA = 2,        /* a CUDA runtime call failed */
     MR_ERR_ALLOCATION = 3,  /* device or host allocation failed */
-    MR_ERR_UNSUPPORTED = 4, /* valid request this build does not implement */
+    MR_ERR_UNSUPPORTED = 4, /* valid request the library does not implement */
     MR_ERR_DEVICE = 5       /* a kernel reported an error status (bounded wait expired, ...) */
 };
 
