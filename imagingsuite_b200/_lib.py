@@ -56,6 +56,7 @@ _PROTOS = {
     "mr_basicringclean": (c_int, [c_void, c_size, c_size, c_size, c_void]),
     "mr_medianmixringclean": (c_int, [c_void, c_size, c_size, c_size, c_float, c_float, c_void]),
     "mr_sigmoid_lut": (c_int, [c_size, c_float, c_float, P_float, P_float]),
+    "mr_compute_weights": (c_int, [P_float, c_size, P_float, c_int, P_float, P_float, P_size]),
     "mr_spotclean2": (c_int, [c_void, c_size, c_size, c_size, c_int, c_float, c_float, c_int, c_float, c_float, c_int,
                               c_void]),
     "mr_projfilter_tables": (c_int, [c_size, ctypes.c_char_p, c_float, c_float, c_int, c_float, c_int, P_size, P_size,

@@ -7,6 +7,7 @@
 #include "mr_common.cuh"
 #include "mr_kipl_filters.cuh"
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -268,6 +269,88 @@ static const std::vector<float> &log_lut_table()
     return table;
 }
 
+// ComputeWeights (frameworks/tomography/Framework/ReconFramework/src/ReconHelpers.cpp:365-488)
+// on the projection list BuildFileList makes (:100-110, :150-160): each projection keyed by its
+// angle modulo 180 in a multimap (equal keys in acquisition order), weight 1 to start.
+// Interior weights (next key - previous key) / 360, 0 for a repeated key; over a full arc
+// (arc > 175 degrees) the last weight wraps through the first key + 180 (0 when it repeats the
+// one before), the first weight wraps through the last key - 180 and is divided by 180 (by 360
+// after a repeated last key or for a golden-section scan); over a short arc both ends copy
+// the second weight. Runs of repeated keys share the weight of the entry before them. The
+// result is a map keyed by the projection angle (a repeated angle keeps the last entry); when
+// the weights of all entries sum to 0.5 within 0.001, every weight is doubled. Fewer than 3
+// projections: weight 1/n each, keyed by the reduced angle (the first entry of a repeated key
+// kept). Outputs in map order; returns the number of entries.
+static size_t compute_weights(const float *angles, size_t n, float arc0, float arc1, bool golden, float *out_angles,
+                              float *out_weights)
+{
+    struct Entry {
+        float key, angle, weight;
+    };
+    std::vector<Entry> e(n);
+    for (size_t i = 0; i < n; ++i) e[i] = {std::fmod(angles[i], 180.0f), angles[i], 1.0f};
+    std::stable_sort(e.begin(), e.end(), [](const Entry &a, const Entry &b) { return a.key < b.key; });
+    if (n < 3) {
+        // std::map keyed by the reduced angle: a repeated key keeps its first entry
+        size_t m = 0;
+        for (size_t i = 0; i < n; ++i) {
+            if (i > 0 && e[i].key == e[i - 1].key) continue;
+            out_angles[m] = e[i].angle;
+            out_weights[m] = static_cast<float>(1.0 / static_cast<double>(n));
+            ++m;
+        }
+        return m;
+    }
+    for (size_t i = 1; i + 1 < n; ++i)
+        e[i].weight = e[i].key != e[i - 1].key ? (e[i + 1].key - e[i - 1].key) / 360.0f : 0.0f;
+    if (175.0f < arc1 - arc0) {
+        bool repeated_last = false;
+        if (e[n - 1].key != e[n - 2].key) {
+            e[n - 1].weight = ((e[0].key + 180) - e[n - 2].key) / 360.0f;
+        } else {
+            e[n - 1].weight = 0.0f;
+            repeated_last = true;
+        }
+        const float span = e[1].key - (e[n - 1].key - 180);
+        e[0].weight = (repeated_last || golden) ? span / 360.0f : span / 180.0f;
+    } else {
+        e[0].weight = e[1].weight;
+        e[n - 1].weight = e[1].weight;
+    }
+    for (size_t q = 1; q < n;) {
+        if (e[q].weight == 0.0f) {
+            const size_t before = q - 1;
+            size_t run = 0;
+            do {
+                ++run;
+                ++q;
+            } while (q < n && e[q].weight == 0.0f);
+            const float w = e[before].weight / static_cast<float>(run + 1);
+            for (size_t k = before; k < before + run + 1; ++k) e[k].weight = w;
+        } else {
+            ++q;
+        }
+    }
+    float sum = 0.0f;
+    std::vector<Entry> byangle;
+    byangle.reserve(n);
+    for (size_t i = 0; i < n; ++i) {
+        sum += e[i].weight;
+        byangle.push_back(e[i]);
+    }
+    // std::map<float, .>: sorted by angle, a repeated angle keeps the last entry in list order
+    std::stable_sort(byangle.begin(), byangle.end(), [](const Entry &a, const Entry &b) { return a.angle < b.angle; });
+    const bool twice = std::fabs(sum - 0.5f) < 0.001f;
+    size_t m = 0;
+    for (size_t i = 0; i < n; ++i) {
+        if (i + 1 < n && byangle[i + 1].angle == byangle[i].angle) continue;
+        out_angles[m] = byangle[i].angle;
+        out_weights[m] = twice ? byangle[i].weight * 2 : byangle[i].weight;
+        ++m;
+    }
+    return m;
+}
+
 } // namespace mr
 
 using namespace mr;
@@ -403,6 +486,16 @@ mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t n
         k_lognorm<float><<<g, 256, 0, as_stream(stream)>>>(static_cast<const float *>(in_d), npix, dark_d, logflat_d,
                                                            doselog_d, ndose, ndc, nob, vec, out_d);
     return check_launch("k_lognorm");
+}
+
+mr_status mr_compute_weights(const float *angles_h, size_t n, const float *scanarc_h, int golden_section,
+                             float *angles_out_h, float *weights_out_h, size_t *nout_h)
+{
+    if ((n && (!angles_h || !angles_out_h || !weights_out_h)) || !scanarc_h || !nout_h)
+        return fail(MR_ERR_ARGUMENT, "mr_compute_weights: null pointer");
+    *nout_h = compute_weights(angles_h, n, scanarc_h[0], scanarc_h[1], golden_section != 0, angles_out_h,
+                              weights_out_h);
+    return MR_OK;
 }
 
 mr_status mr_lognorm_apply_lut(const void *in_d, int in_dtype, size_t npix, size_t nproj, const float *dark_d,

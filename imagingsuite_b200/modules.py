@@ -387,6 +387,22 @@ def _require_f32(t: torch.Tensor, what: str) -> None:
         raise ReconException(f"{what} must be float32")
 
 
+def compute_weights(angles, scan_arc=(0.0, 360.0), golden_section: bool = False):
+    """ComputeWeights (frameworks/tomography/Framework/ReconFramework/src/ReconHelpers.cpp:
+    365-488) on projection angles in acquisition order, as BuildFileList lists them: returns the
+    (angles, weights) of the weighted projection map in its order (host computation). The
+    backprojectors' `weights` list is these weights times 1 / (0.1 * pixel size)."""
+    a = np.ascontiguousarray(angles, dtype=np.float32)
+    arc = np.asarray(scan_arc, dtype=np.float32)
+    oa = np.zeros(max(a.size, 1), np.float32)
+    ow = np.zeros(max(a.size, 1), np.float32)
+    m = ctypes.c_size_t(0)
+    check(L.lib().mr_compute_weights(a.ctypes.data_as(L.P_float), a.size, arc.ctypes.data_as(L.P_float),
+                                     int(golden_section), oa.ctypes.data_as(L.P_float), ow.ctypes.data_as(L.P_float),
+                                     ctypes.byref(m)))
+    return oa[:m.value].copy(), ow[:m.value].copy()
+
+
 def median_filter(img: torch.Tensor, kx: int, ky: int) -> torch.Tensor:
     """kipl TMedianFilter<float,2> with a kx x ky window (odd sizes up to 5) on one image (nv, nu)
     or a stack (n, nv, nu); returns a new tensor."""

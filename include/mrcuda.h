@@ -132,6 +132,18 @@ mr_status mr_waveletringclean(float *proj_d, size_t nu, size_t nv, size_t nproj,
                               float sigma, void *stream);
 
 /* ---------------------------------------------------------------------------------
+ * Projection weights (host)
+ * replaces ComputeWeights (frameworks/tomography/Framework/ReconFramework/src/ReconHelpers.cpp:
+ *   365-488) on the list BuildFileList makes (:100-110): angles_h in acquisition order;
+ *   scanarc_h = ProjectionInfo.fScanArc (first, last); golden_section: GoldenSectionScan.
+ *   Writes the weighted projection map in its order (sorted by angle; a repeated angle keeps
+ *   its last entry; below 3 projections sorted by angle modulo 180) to angles_out_h /
+ *   weights_out_h (room for n each) and its size to *nout_h. Times 1 / (0.1 * pixel size)
+ *   (ProjectionReader.cpp:907-919) these are the `weights` list the backprojectors take. */
+mr_status mr_compute_weights(const float *angles_h, size_t n, const float *scanarc_h, int golden_section,
+                             float *angles_out_h, float *weights_out_h, size_t *nout_h);
+
+/* ---------------------------------------------------------------------------------
  * Alternative ring cleaners and the kipl median filter they use
  * mr_median_filter replaces kipl::filters::TMedianFilter<float,2>::operator()
  *   (core/kipl/kipl/include/filters/core/medianfilter.hpp:28-199, HeapSortMedianFilter with

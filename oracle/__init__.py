@@ -647,3 +647,29 @@ def spotclean2(proj, method: str = "ring", gamma: float = 0.1, sigma: float = 0.
         if rc != 0:
             raise ValueError(f"orc_spotclean failed ({rc})")
     return p
+
+
+def compute_weights(angles, scanarc=(0.0, 360.0), golden=False, use_ref=False, use_lib=False):
+    """ComputeWeights on projection angles in acquisition order: (angles, weights) of the
+    resulting map, in its order. use_ref: the reference's function; use_lib: the library's
+    host implementation (mr_compute_weights)."""
+    a = _f32(angles)
+    n = a.size
+    oa = np.zeros(max(n, 1), np.float32)
+    ow = np.zeros(max(n, 1), np.float32)
+    if use_ref:
+        m = ctypes.c_size_t(0)
+        _check_ref(ref().ref_compute_weights(_p(a), _sz(n), _f(scanarc[0]), _f(scanarc[1]), int(golden), _p(oa), _p(ow),
+                                             ctypes.byref(m)))
+        m = m.value
+    elif use_lib:
+        from imagingsuite_b200 import _lib as L
+
+        arc = np.asarray(scanarc, np.float32)
+        m = ctypes.c_size_t(0)
+        L.check(L.lib().mr_compute_weights(_p(a), n, _p(arc), int(golden), _p(oa), _p(ow), ctypes.byref(m)))
+        m = m.value
+    else:
+        orc().orc_compute_weights.restype = ctypes.c_size_t
+        m = orc().orc_compute_weights(_p(a), _sz(n), _f(scanarc[0]), _f(scanarc[1]), int(golden), _p(oa), _p(ow))
+    return oa[:m].copy(), ow[:m].copy()

@@ -1933,3 +1933,94 @@ int orc_spotclean(float *proj, size_t w, size_t h, size_t n, int method, float g
     free(lut);
     return rc;
 }
+
+/* ------------------------------------------------------------- projection weights */
+
+/* ComputeWeights (frameworks/tomography/Framework/ReconFramework/src/ReconHelpers.cpp:365-488)
+ * on BuildFileList's multimap (:100-110): key = angle modulo 180, equal keys in acquisition
+ * order (a stable insertion sort here), weight 1 to start. Outputs the resulting map in its
+ * order (angle, weight); returns its size. arc0/arc1: ProjectionInfo.fScanArc. */
+size_t orc_compute_weights(const float *angles, size_t n, float arc0, float arc1, int golden, float *out_angles,
+                           float *out_weights)
+{
+    float *k = (float *)malloc((n ? n : 1) * sizeof(float)), *a = (float *)malloc((n ? n : 1) * sizeof(float));
+    float *w = (float *)malloc((n ? n : 1) * sizeof(float));
+    for (size_t i = 0; i < n; ++i) {
+        float key = fmodf(angles[i], 180.0f), ang = angles[i];
+        size_t j = i;
+        while (j > 0 && key < k[j - 1]) { /* after equal keys: multimap insertion order */
+            k[j] = k[j - 1];
+            a[j] = a[j - 1];
+            j--;
+        }
+        k[j] = key;
+        a[j] = ang;
+        w[i] = 1.0f;
+    }
+    size_t m = 0;
+    if (n < 3) {
+        for (size_t i = 0; i < n; ++i) {
+            if (i > 0 && k[i] == k[i - 1]) continue; /* map::insert keeps the first */
+            out_angles[m] = a[i];
+            out_weights[m++] = (float)(1.0 / (double)n);
+        }
+    } else {
+        for (size_t i = 1; i + 1 < n; ++i) w[i] = k[i] != k[i - 1] ? (k[i + 1] - k[i - 1]) / 360.0f : 0.0f;
+        if (175.0f < arc1 - arc0) {
+            int repeated_last = 0;
+            if (k[n - 1] != k[n - 2]) {
+                w[n - 1] = ((k[0] + 180) - k[n - 2]) / 360.0f;
+            } else {
+                w[n - 1] = 0.0f;
+                repeated_last = 1;
+            }
+            if (repeated_last || golden)
+                w[0] = (k[1] - (k[n - 1] - 180)) / 360.0f;
+            else
+                w[0] = (k[1] - (k[n - 1] - 180)) / 180.0f;
+        } else {
+            w[0] = w[1];
+            w[n - 1] = w[1];
+        }
+        /* runs of zero weights share the weight of the entry before them (the reference reads
+         * past the end of its list when the run reaches it; the run simply ends there) */
+        for (size_t q = 1; q < n;) {
+            if (w[q] == 0.0f) {
+                size_t before = q - 1, run = 0;
+                do {
+                    run++;
+                    q++;
+                } while (q < n && w[q] == 0.0f);
+                float v = w[before] / (float)(run + 1);
+                for (size_t t = before; t <= before + run; ++t) w[t] = v;
+            } else {
+                q++;
+            }
+        }
+        float sum = 0.0f;
+        for (size_t i = 0; i < n; ++i) sum += w[i];
+        int twice = fabsf(sum - 0.5f) < 0.001f;
+        /* std::map keyed by the angle: sorted, a repeated angle keeps the last entry */
+        for (size_t i = 0; i < n; ++i) {
+            size_t pos = 0;
+            while (pos < m && out_angles[pos] < a[i]) pos++;
+            if (pos < m && out_angles[pos] == a[i]) {
+                out_weights[pos] = w[i];
+                continue;
+            }
+            for (size_t t = m; t > pos; --t) {
+                out_angles[t] = out_angles[t - 1];
+                out_weights[t] = out_weights[t - 1];
+            }
+            out_angles[pos] = a[i];
+            out_weights[pos] = w[i];
+            m++;
+        }
+        if (twice)
+            for (size_t i = 0; i < m; ++i) out_weights[i] *= 2;
+    }
+    free(k);
+    free(a);
+    free(w);
+    return m;
+}

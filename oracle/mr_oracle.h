@@ -122,6 +122,11 @@ int orc_medianmixringclean(float *proj, size_t w, size_t h, size_t n, float thre
 int orc_spotclean(float *proj, size_t w, size_t h, size_t n, int method, float gamma, float sigma, int iterations,
                   float minlevel, float maxlevel, int maxarea);
 
+/* ComputeWeights (ReconHelpers.cpp:365-488): projection angles in acquisition order -> the
+ * weighted projection map (angle, weight), in map order; returns its size. */
+size_t orc_compute_weights(const float *angles, size_t n, float arc0, float arc1, int golden, float *out_angles,
+                           float *out_weights);
+
 #ifdef __cplusplus
 }
 #endif

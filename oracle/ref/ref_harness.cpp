@@ -51,6 +51,7 @@
 #include "MedianMixRingClean.h"
 #include "GammaSpotCleanModule.h"
 #include "SpotClean2.h"
+#include <ReconHelpers.h>
 #include <filters/medianfilter.h>
 #include <math/LUTCollection.h>
 #include "WaveletRingClean.h"
@@ -656,6 +657,33 @@ int ref_spotclean2(float *proj, size_t w, size_t h, size_t n, const char *method
         std::map<std::string, std::string> coeff;
         mod.Process(img, coeff);
         std::memcpy(proj, img.GetDataPtr(), sizeof(float) * w * h * n);
+    });
+}
+
+// ComputeWeights (ReconFramework/src/ReconHelpers.cpp:365-488) on the multimap BuildFileList
+// makes (:100-110: key = fmod(angle, 180), ProjectionInfo(name, angle)); the resulting map is
+// copied out in its order as (info.angle, info.weight).
+int ref_compute_weights(const float *angles, size_t n, float arc0, float arc1, int golden, float *out_angles,
+                        float *out_weights, size_t *nout)
+{
+    return guarded([&] {
+        ReconConfig cfg;
+        cfg.ProjectionInfo.fScanArc[0] = arc0;
+        cfg.ProjectionInfo.fScanArc[1] = arc1;
+        cfg.ProjectionInfo.scantype = golden ? ReconConfig::cProjections::GoldenSectionScan
+                                             : ReconConfig::cProjections::SequentialScan;
+        std::multimap<float, ProjectionInfo> mm;
+        for (size_t i = 0; i < n; ++i)
+            mm.insert(std::make_pair(std::fmod(angles[i], 180.0f), ProjectionInfo("p", angles[i])));
+        std::map<float, ProjectionInfo> out;
+        ComputeWeights(&cfg, mm, &out);
+        size_t m = 0;
+        for (auto &kv : out) {
+            out_angles[m] = kv.second.angle;
+            out_weights[m] = kv.second.weight;
+            ++m;
+        }
+        *nout = m;
     });
 }
 

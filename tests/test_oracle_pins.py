@@ -257,3 +257,50 @@ def test_slices_u16_matches_reference(ref_lib, plane, roi):
         got = O.slices_u16(vol, plane, 1, nsl - 2, lo, hi, roi)
         exp = O.ref_slices_u16(vol, plane, 1, nsl - 2, lo, hi, roi)
         assert np.array_equal(got, exp)
+
+
+def _weight_cases(trailing_repeats: bool):
+    rng = _rng(70)
+    cases = []
+    for n in (1, 2, 3, 5, 10, 360, 375, 1125):
+        cases.append((np.arange(n, dtype=np.float32) * np.float32(180.0 / n), (0, 180), False))
+        cases.append((np.arange(n, dtype=np.float32) * np.float32(360.0 / n), (0, 360), False))
+        cases.append((np.arange(n, dtype=np.float32) * np.float32(180.0 / max(n - 1, 1)), (0, 180), False))
+    g = np.float32(0.5 * (1 + np.sqrt(5.0)))
+    for n, arc in ((50, 180.0), (100, 360.0)):
+        i = np.arange(n, dtype=np.float32)
+        cases.append((np.fmod(i * g * np.float32(arc), np.float32(arc)).astype(np.float32), (0, arc), True))
+    cases.append((np.linspace(0, 120, 40).astype(np.float32), (0, 120), False))  # short arc
+    cases.append((rng.permutation(np.arange(37, dtype=np.float32) * np.float32(5.0)), (0, 180), False))
+    cases.append((np.array([0, 0, 10, 20, 20, 20, 30, 190, 200], np.float32), (0, 360), False))  # repeats inside
+    if trailing_repeats:
+        # a run of repeated keys at the end of the list: the reference reads past the end of its
+        # multimap there (its result depends on memory behind the container), the restatements
+        # end the run at the list end
+        cases.append((np.repeat(np.arange(20, dtype=np.float32) * 9.0, 3), (0, 180), False))
+        cases.append((np.concatenate([np.arange(30, dtype=np.float32) * 6.0, np.full(3, 174.0, np.float32)]), (0, 180),
+                      False))
+    return cases
+
+
+def test_compute_weights_matches_reference(ref_lib):
+    """ComputeWeights (ReconHelpers.cpp:365-488): the oracle's restatement and the library's host
+    function (mr_compute_weights) against the reference on uniform half and full arcs (with and
+    without the end angle), golden-section scans, a short arc, unsorted and repeated angles."""
+    for ang, arc, gold in _weight_cases(False):
+        ra, rw = O.compute_weights(ang, arc, gold, use_ref=True)
+        for lib in (False, True):
+            oa, ow = O.compute_weights(ang, arc, gold, use_lib=lib)
+            assert np.array_equal(oa.view(np.uint32), ra.view(np.uint32)), (len(ang), arc, gold, lib)
+            assert np.array_equal(ow.view(np.uint32), rw.view(np.uint32)), (len(ang), arc, gold, lib)
+
+
+def test_compute_weights_library_matches_oracle():
+    for ang, arc, gold in _weight_cases(True):
+        oa, ow = O.compute_weights(ang, arc, gold)
+        la, lw = O.compute_weights(ang, arc, gold, use_lib=True)
+        assert np.array_equal(oa.view(np.uint32), la.view(np.uint32)) and np.array_equal(ow.view(np.uint32),
+                                                                                         lw.view(np.uint32))
+    # one projection per degree over a full turn: the weights sum to 1
+    _, w = O.compute_weights(np.arange(360, dtype=np.float32), (0, 360))
+    assert abs(float(w.sum()) - 1.0) < 1e-3
