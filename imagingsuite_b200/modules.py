@@ -794,6 +794,27 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         return self.volume.shape[2]
 
 
+class MultiProjectionBP(MultiProjectionBPparallel):
+    """MultiProjectionBP, the reference's serial backprojector (factory name "MultiProjBP",
+    StdBackProjectors/src/MultiProjBP.cpp:36-146). Without tilt correction it computes exactly
+    what MultiProjectionBPparallel computes (the same positions, weights and accumulation order,
+    pinned against the compiled reference), so it runs the same kernels. With tilt correction the
+    serial version shifts the interpolation weight by one `4 tan(tilt)` per group of 4 slices
+    (MultiProjBP.cpp:83) where the parallel one shifts it twice (MultiProjBPparallel.cpp:88-99);
+    that variant is not built here, and Process raises for it."""
+
+    def __init__(self):
+        super().__init__()
+        self.m_sModuleName = "Multi projection BP"
+
+    def Process(self, projections: torch.Tensor, parameters: dict, prefiltered_weights: bool = False,
+                rows: tuple | None = None) -> int:
+        if self.mConfig.ProjectionInfo.bCorrectTilt:
+            raise ReconException("MultiProjectionBP with tilt correction is not supported by this module "
+                                 "(MultiProjectionBPparallel is)")
+        return super().Process(projections, parameters, prefiltered_weights, rows)
+
+
 class FDKbp_single(_BackProjectorBase):
     """FDKbp_single (FDKBackProjectors/src/fdkbp_single.cpp) with the FdkReconBase driver
     (fdkreconbase.cpp). Volume is MatrixXYZ: tensor (nz, ny, nx) = (nv, nu, nu), x fastest."""

@@ -26,6 +26,49 @@ def test_bp_parallel_bit_exact(ref_lib, tilt, direction, buffersize):
     assert np.array_equal(a, b)
 
 
+@pytest.mark.parametrize("direction", [0, 1])
+@pytest.mark.parametrize("buffersize", [16, 7])
+def test_bp_serial_equals_parallel_without_tilt(ref_lib, direction, buffersize):
+    """The reference's serial MultiProjectionBP (MultiProjBP.cpp) gives the parallel
+    backprojector's volume bit for bit without tilt correction, so the module of that name runs
+    the same kernels."""
+    rng = _rng(20 + buffersize)
+    nproj, nv, nu = 37, 12, 48
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
+    kw = dict(direction=direction, buffersize=buffersize, roi_y0=3)
+    a = O.bp_parallel(proj, ang, w, 23.5, **kw)
+    assert np.array_equal(a, O.bp_parallel(proj, ang, w, 23.5, use_ref=True, serial=True, **kw))
+
+
+def test_bp_serial_tilt_shifts_once(ref_lib):
+    """With tilt correction the serial version differs from the parallel one from the second
+    group of 4 slices on (one shift of the interpolation weight per group instead of two); in
+    the first group only by the order in which the centre offset is subtracted (rounding)."""
+    rng = _rng(21)
+    nproj, nv, nu = 37, 12, 48
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    w = np.ones(nproj, np.float32)
+    kw = dict(direction=0, buffersize=16, correcttilt=True, tiltangle=0.6, tiltpivot=2.0, roi_y0=3)
+    par = O.bp_parallel(proj, ang, w, 23.5, use_ref=True, **kw)
+    ser = O.bp_parallel(proj, ang, w, 23.5, use_ref=True, serial=True, **kw)
+    assert np.abs(par[:, :, :4] - ser[:, :, :4]).max() < 1e-3
+    assert all(np.abs(par[:, :, z] - ser[:, :, z]).max() > 0.1 for z in range(4, 12))
+
+
+def test_bp_serial_module_rejects_tilt():
+    from imagingsuite_b200 import modules as M
+
+    cfg = M.ReconConfig()
+    cfg.ProjectionInfo.bCorrectTilt = True
+    mod = M.MultiProjectionBP()
+    mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
+    with pytest.raises(M.ReconException, match="tilt"):
+        mod.Process(None, {})
+
+
 def test_bp_parallel_ragged_sizes(ref_lib):
     # nv not a multiple of 4 (the reference only updates 4*(nv/4) slices), odd nu
     rng = _rng(3)
