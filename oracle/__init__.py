@@ -236,8 +236,9 @@ def ref_projfilter(proj, filtertype="hanning", cutoff=0.5, order=1.0, usebias=Tr
 
 
 def bp_parallel(proj, angles, weights, center, direction=0, buffersize=16, correcttilt=False, tiltangle=0.0,
-                tiltpivot=0.0, roi_y0=0, nslices=None, use_ref=False, serial=False) -> np.ndarray:
-    """MultiProjectionBPparallel through StdBackProjectorBase::Process 3D.
+                tiltpivot=0.0, roi_y0=0, nslices=None, use_ref=False, serial=False, nn=False) -> np.ndarray:
+    """MultiProjectionBPparallel through StdBackProjectorBase::Process 3D (serial: the serial
+    MultiProjectionBP; nn: NearestNeighborBP).
 
     Returns the ZXY volume, shape (nu [y], nu [x], nv [z])."""
     proj = _f32(proj)
@@ -247,11 +248,13 @@ def bp_parallel(proj, angles, weights, center, direction=0, buffersize=16, corre
     if use_ref:
         _check_ref(ref().ref_bp_parallel(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights), _f(center),
                                          int(direction), _sz(buffersize), int(correcttilt), _f(tiltangle),
-                                         _f(tiltpivot), _sz(roi_y0), int(serial), _p(vol)))
+                                         _f(tiltpivot), _sz(roi_y0), 2 if nn else int(serial), _p(vol)))
     else:
-        rc = orc().orc_bp_parallel(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights), _f(center),
-                                   int(direction), _sz(buffersize), int(correcttilt), _f(tiltangle), _f(tiltpivot),
-                                   _sz(roi_y0), _sz(nslices if nslices is not None else nv), _p(vol))
+        rc = orc().orc_bp_parallel_variant(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights),
+                                           _f(center), int(direction), _sz(buffersize), int(correcttilt),
+                                           _f(tiltangle), _f(tiltpivot), _sz(roi_y0),
+                                           _sz(nslices if nslices is not None else nv), 2 if nn else int(serial),
+                                           _p(vol))
         if rc != 0:
             raise ValueError("invalid parallel-beam backprojection arguments")
     return vol

@@ -353,9 +353,14 @@ static void circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, 
 
 /* One buffer flush of MultiProjectionBPparallel::BackProject (MultiProjBPparallel.cpp:39-170).
  * buf: [count][nu][nvpad] weighted, transposed projections. */
+/* variant 0: MultiProjectionBPparallel::BackProject (MultiProjBPparallel.cpp:39-170);
+ * 1: the serial MultiProjectionBP (MultiProjBP.cpp:36-146), which differs only under tilt
+ * correction (centre offset subtracted after the x term, one weight shift per 4-slice group);
+ * 2: NearestNeighborBP (NNMultiProjBP.cpp:36-121): the sample at the truncated position, no
+ * weights, under tilt a constant centre offset only. */
 static void bp_flush(const float *buf, size_t count, size_t nu, size_t nv, size_t nvpad, const float *fsin,
                      const float *fcos, const float *fstartu, const size_t *mask, int correcttilt,
-                     float tiltangle, float tiltpivot, size_t roi_y0, float *vol)
+                     float tiltangle, float tiltpivot, size_t roi_y0, int variant, float *vol)
 {
     const size_t sizez = nv / 4;
     const int sizeum2 = (int)(nu - 2);
@@ -365,17 +370,30 @@ static void bp_flush(const float *buf, size_t count, size_t nu, size_t nv, size_
     for (long y = 1; y <= (long)nu; ++y) {
         float local[1024 * 4];
         for (size_t i = 0; i < count; ++i)
-            local[i] = correcttilt ? (fstartu[i] + fcos[i] * (float)y) - centeroffset : fstartu[i] + fcos[i] * (float)y;
+            local[i] = correcttilt && variant == 0 ? (fstartu[i] + fcos[i] * (float)y) - centeroffset
+                                                   : fstartu[i] + fcos[i] * (float)y;
         const size_t x0 = mask[2 * (y - 1)], x1 = mask[2 * (y - 1) + 1];
         for (size_t x = x0 + 1; x <= x1; ++x) {
             float *col = vol + ((size_t)(y - 1) * nu + (x - 1)) * nv;
             for (size_t i = 0; i < count; ++i) {
                 float posu = local[i] - fsin[i] * (float)x;
+                if (correcttilt && variant != 0) posu = posu - centeroffset;
                 int n = (int)posu;
                 if (n < 0 || sizeum2 < n) continue;
                 const float *a = buf + (i * nu + (size_t)n) * nvpad;
                 const float *b = a + nvpad;
-                if (!correcttilt) {
+                if (variant == 2) {
+                    for (size_t z = 0; z < 4 * sizez; ++z) col[z] = col[z] + a[z];
+                } else if (correcttilt && variant == 1) {
+                    for (size_t zg = 0; zg < sizez; ++zg) {
+                        const float wb = fabsf((posu - (float)n) - (float)zg * centerinc);
+                        const float wa = 1.0f - wb;
+                        for (size_t q = 0; q < 4; ++q) {
+                            size_t z = 4 * zg + q;
+                            col[z] = col[z] + (a[z] * wa + b[z] * wb);
+                        }
+                    }
+                } else if (!correcttilt) {
                     const float wb = fabsf(posu - (float)n);
                     const float wa = 1.0f - wb;
                     for (size_t z = 0; z < 4 * sizez; ++z) col[z] = col[z] + (a[z] * wa + b[z] * wb);
@@ -400,6 +418,15 @@ int orc_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj, const
                     const float *weights, float center, int direction, size_t buffersize, int correcttilt,
                     float tiltangle, float tiltpivot, size_t roi_y0, size_t nslices, float *vol)
 {
+    return orc_bp_parallel_variant(proj, nu, nv, nproj, angles, weights, center, direction, buffersize, correcttilt,
+                                   tiltangle, tiltpivot, roi_y0, nslices, 0, vol);
+}
+
+int orc_bp_parallel_variant(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
+                            const float *weights, float center, int direction, size_t buffersize, int correcttilt,
+                            float tiltangle, float tiltpivot, size_t roi_y0, size_t nslices, int variant, float *vol)
+{
+    if (variant < 0 || variant > 2) return -1;
     if (buffersize == 0 || buffersize > 1024 || nu < 2) return -1;
     const size_t rest = (nv & 3) ? 4 - (nv & 3) : 0;
     const size_t nvpad = nv + rest;
@@ -425,7 +452,7 @@ int orc_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj, const
         if (last || buffersize <= counter) {
             if (buffersize <= counter) counter--; /* the buffer-full flush drops its last entry */
             bp_flush(buf, counter, nu, nv, nvpad, fsin, fcos, fstartu, mask, correcttilt, tiltangle, tiltpivot,
-                     roi_y0, vol);
+                     roi_y0, variant, vol);
             counter = 0;
         }
     }

@@ -51,6 +51,10 @@ void orc_projfilter_apply(float *proj, size_t nu, size_t nrows, const float *fil
 int orc_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
                     const float *weights, float center, int direction, size_t buffersize, int correcttilt,
                     float tiltangle, float tiltpivot, size_t roi_y0, size_t nslices, float *vol);
+/* variant 0 MultiProjectionBPparallel, 1 the serial MultiProjectionBP, 2 NearestNeighborBP */
+int orc_bp_parallel_variant(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
+                            const float *weights, float center, int direction, size_t buffersize, int correcttilt,
+                            float tiltangle, float tiltpivot, size_t roi_y0, size_t nslices, int variant, float *vol);
 
 void orc_bp_geometry(const float *angles, size_t n, size_t nu, float center, int direction, float *fsin, float *fcos,
                      float *fstartu);

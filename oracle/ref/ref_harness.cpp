@@ -57,6 +57,7 @@
 #include "WaveletRingClean.h"
 #include "MultiProjBPparallel.h"
 #include "MultiProjBP.h"
+#include "NNMultiProjBP.h"
 #include "fdkbp_single.h"
 #include "linearforwardprojector.h"
 #include <wavelets/wavelets.h>
@@ -254,7 +255,8 @@ int ref_projfilter(float *proj, size_t nu, size_t nv, size_t nproj, const char *
 // MultiProjectionBPparallel (MultiProjBPparallel.cpp:39-170) driven through
 // StdBackProjectorBase::Process 3D (StdBackProjectorBase.cpp:120-149).
 // proj: [nproj][nv][nu]; vol out: ZXY [nu (y)][nu (x)][nv (z)].
-// serial != 0 selects the serial MultiProjectionBP (MultiProjBP.cpp:36-146) instead.
+// variant 1 selects the serial MultiProjectionBP (MultiProjBP.cpp:36-146), 2 NearestNeighborBP
+// (NNMultiProjBP.cpp:36-121).
 int ref_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj,
                     const float *angles, const float *weights, float center, int direction,
                     size_t buffersize, int correcttilt, float tiltangle, float tiltpivot,
@@ -277,8 +279,10 @@ int ref_bp_parallel(const float *proj, size_t nu, size_t nv, size_t nproj,
         par["SliceBlock"] = "32";
         par["SubVolume"] = "1 1";
         StdBackProjectorBase *bp = nullptr;
-        if (serial)
+        if (serial == 1)
             bp = new MultiProjectionBP(nullptr);
+        else if (serial == 2)
+            bp = new NearestNeighborBP(nullptr);
         else
             bp = new MultiProjectionBPparallel(nullptr);
         std::unique_ptr<StdBackProjectorBase> hold(bp);

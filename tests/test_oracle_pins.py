@@ -58,6 +58,24 @@ def test_bp_serial_tilt_shifts_once(ref_lib):
     assert all(np.abs(par[:, :, z] - ser[:, :, z]).max() > 0.1 for z in range(4, 12))
 
 
+@pytest.mark.parametrize("variant", ["serial", "nn"])
+@pytest.mark.parametrize("tilt", [False, True])
+@pytest.mark.parametrize("direction", [0, 1])
+@pytest.mark.parametrize("buffersize", [16, 7])
+def test_bp_variants_bit_exact(ref_lib, variant, tilt, direction, buffersize):
+    """The factory's other parallel-beam backprojectors restated (orc_bp_parallel_variant): the
+    serial MultiProjectionBP (one weight shift per slice group under tilt) and NearestNeighborBP
+    (truncated position, no interpolation, constant tilt offset), against the compiled modules."""
+    rng = _rng(30 + buffersize + 2 * direction)
+    nproj, nv, nu = 37, 12, 48
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
+    kw = dict(direction=direction, buffersize=buffersize, correcttilt=tilt, tiltangle=0.6, tiltpivot=2.0, roi_y0=3,
+              serial=variant == "serial", nn=variant == "nn")
+    assert np.array_equal(O.bp_parallel(proj, ang, w, 23.5, **kw), O.bp_parallel(proj, ang, w, 23.5, use_ref=True, **kw))
+
+
 def test_bp_serial_module_rejects_tilt():
     from imagingsuite_b200 import modules as M
 
