@@ -676,3 +676,15 @@ def compute_weights(angles, scanarc=(0.0, 360.0), golden=False, use_ref=False, u
         orc().orc_compute_weights.restype = ctypes.c_size_t
         m = orc().orc_compute_weights(_p(a), _sz(n), _f(scanarc[0]), _f(scanarc[1]), int(golden), _p(oa), _p(ow))
     return oa[:m].copy(), ow[:m].copy()
+
+
+def ref_fdk_double(proj, angles, weights, geom: FdkGeom) -> np.ndarray:
+    """The reference's FDKbp (double-precision geometry, fdkbp.cpp) through FdkReconBase::Process
+    3D on the same inputs as fdk(). Returns the XYZ volume (nv, nu, nu)."""
+    proj = _f32(proj)
+    nproj, nv, nu = proj.shape
+    angles, weights = _f32(angles), _f32(weights)
+    vol = np.zeros((nv, nu, nu), np.float32)
+    _check_ref(ref().ref_fdk_double(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights),
+                                    ctypes.byref(geom), _p(vol), None))
+    return vol

@@ -59,6 +59,7 @@
 #include "MultiProjBP.h"
 #include "NNMultiProjBP.h"
 #include "fdkbp_single.h"
+#include "fdkbp.h"
 #include "linearforwardprojector.h"
 #include <wavelets/wavelets.h>
 #undef private
@@ -315,10 +316,31 @@ struct ref_fdk_geom {
 // FDKbp_single (fdkbp_single.cpp:83-994) through FdkReconBase::Process 3D
 // (fdkreconbase.cpp:217-277). proj: [nproj][nv][nu]; vol out: XYZ [nv][nu][nu]
 // after the final mirror/z-reversal; cbct_out (optional) before it.
+extern "C++" {
+template <typename Module>
+static void run_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
+                    const ref_fdk_geom *g, float *vol, float *cbct_out);
+}
+
 int ref_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
             const float *weights, const ref_fdk_geom *g, float *vol, float *cbct_out)
 {
-    return guarded([&] {
+    return guarded([&] { run_fdk<FDKbp_single>(proj, nu, nv, nproj, angles, weights, g, vol, cbct_out); });
+}
+
+// The factory's FDKbp (double-precision geometry, fdkbp.cpp) on the same inputs.
+int ref_fdk_double(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles,
+                   const float *weights, const ref_fdk_geom *g, float *vol, float *cbct_out)
+{
+    return guarded([&] { run_fdk<FDKbp>(proj, nu, nv, nproj, angles, weights, g, vol, cbct_out); });
+}
+
+extern "C++" {
+template <typename Module>
+static void run_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
+                    const ref_fdk_geom *g, float *vol, float *cbct_out)
+{
+    {
         ReconConfig cfg;
         cfg.ProjectionInfo.fSOD = g->sod;
         cfg.ProjectionInfo.fSDD = g->sdd;
@@ -352,7 +374,7 @@ int ref_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *
         par["ProjectionBufferSize"] = "16";
         par["SliceBlock"] = "32";
         par["SubVolume"] = "1 1";
-        FDKbp_single fdk(nullptr);
+        Module fdk(nullptr);
         fdk.Configure(cfg, par);
         fdk.SetROI(roi);
         size_t d3[3] = {nu, nv, nproj};
@@ -365,8 +387,9 @@ int ref_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *
         std::memcpy(vol, fdk.volume.GetDataPtr(), sizeof(float) * fdk.volume.Size());
         if (cbct_out) std::memcpy(cbct_out, fdk.cbct_volume.GetDataPtr(), sizeof(float) * fdk.cbct_volume.Size());
         delete[] fdk.proj_matrices;
-    });
+    }
 }
+} // extern "C++"
 
 // ImagingAlgorithms::MorphSpotClean::process on one image [nv][nu]
 // (MorphSpotClean.cpp:41-83), configured like the python binding tests.

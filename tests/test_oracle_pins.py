@@ -365,3 +365,21 @@ def test_compute_weights_library_matches_oracle():
     # one projection per degree over a full turn: the weights sum to 1
     _, w = O.compute_weights(np.arange(360, dtype=np.float32), (0, 360))
     assert abs(float(w.sum()) - 1.0) < 1e-3
+
+
+def test_reference_fdkbp_double_row_window(ref_lib):
+    """The factory's FDKbp (fdkbp.cpp) lowers its CBCT row window by 8 without the single
+    version's zero check (`if (CBCT_roi[1]-8>=0)` on a size_t): for a window that starts within
+    8 rows of the detector top the index wraps and every sample misses the detector, so the
+    volume stays 0. With the window further down it reconstructs (its projection scale also
+    carries 1/nproj). This pins why that module is not offered as a drop-in."""
+    rng = _rng(80)
+    nproj, nu = 8, 32
+    ang = (np.arange(nproj) * 45.0).astype(np.float32)
+    w = np.ones(nproj, np.float32)
+    proj = (rng.random((nproj, 24, nu)) + 0.5).astype(np.float32)
+    g = O.fdk_geom(250.0, 500.0, (15.5, 11.5), 15.5, (0.2, 0.2), (0.1, 0.1, 0.1))
+    assert not O.ref_fdk_double(proj, ang, w, g).any() and O.fdk(proj, ang, w, g, use_ref=True).any()
+    proj = (rng.random((nproj, 64, nu)) + 0.5).astype(np.float32)
+    g = O.fdk_geom(250.0, 500.0, (15.5, 60.0), 15.5, (0.2, 0.2), (0.05, 0.05, 0.05))
+    assert O.ref_fdk_double(proj, ang, w, g).any()
