@@ -403,6 +403,21 @@ def compute_weights(angles, scan_arc=(0.0, 360.0), golden_section: bool = False)
     return oa[:m.value].copy(), ow[:m.value].copy()
 
 
+def projection_lists(angles, weights, rotation: float = 0.0, resolution: float = 0.0) -> dict:
+    """The `angles` and `weights` texts ProjectionReader::Read hands the backprojectors
+    (frameworks/tomography/Framework/ReconFramework/src/ProjectionReader.cpp:907-919): angle +
+    MatrixInfo.fRotation and weight * 1 / (0.1 * pixel size) (1 when the pixel size is not
+    positive), in float, each written as a default-formatted stream value (6 significant
+    digits, `%g`). The backprojectors then read these rounded values, as in the engine."""
+    f32 = np.float32
+    res = f32(resolution)
+    rw = f32(1.0) / (res * f32(0.1) if f32(0) < res else f32(1.0))
+    a = [f32(v) + f32(rotation) for v in np.asarray(angles, np.float32)]
+    w = [f32(v) * rw for v in np.asarray(weights, np.float32)]
+    return {"angles": " ".join(f"{float(v):g}" for v in a) + " ",
+            "weights": " ".join(f"{float(v):g}" for v in w) + " "}
+
+
 def median_filter(img: torch.Tensor, kx: int, ky: int) -> torch.Tensor:
     """kipl TMedianFilter<float,2> with a kx x ky window (odd sizes up to 5) on one image (nv, nu)
     or a stack (n, nv, nu); returns a new tensor."""

@@ -714,6 +714,15 @@ int ref_compute_weights(const float *angles, size_t n, float arc0, float arc1, i
     });
 }
 
+// A float written to a std::ostringstream with its default format (how ProjectionReader::Read
+// writes the angle and weight lists, ProjectionReader.cpp:918-919); out receives the text.
+void ref_stream_float(float v, char *out, size_t len)
+{
+    std::ostringstream s;
+    s << v;
+    std::snprintf(out, len, "%s", s.str().c_str());
+}
+
 // libtiff writers for the debug images BasicRingClean saves to the working directory
 // (mean.tif, med.tif, diff.tif; libtiff is absent here): opening for writing gives a handle
 // that discards everything, so the module runs to the end without touching the file system.

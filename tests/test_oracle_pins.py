@@ -383,3 +383,28 @@ def test_reference_fdkbp_double_row_window(ref_lib):
     proj = (rng.random((nproj, 64, nu)) + 0.5).astype(np.float32)
     g = O.fdk_geom(250.0, 500.0, (15.5, 60.0), 15.5, (0.2, 0.2), (0.05, 0.05, 0.05))
     assert O.ref_fdk_double(proj, ang, w, g).any()
+
+
+def test_projection_lists_format_like_the_stream(ref_lib):
+    """The engine's angle / weight lists: float arithmetic, then the default ostream format of
+    each value, which the module helper reproduces."""
+    import ctypes
+
+    from imagingsuite_b200 import modules as M
+
+    rng = _rng(90)
+    ang = np.concatenate([np.arange(375, dtype=np.float32) * np.float32(180.0 / 375),
+                          rng.uniform(-1e-6, 1e6, 50).astype(np.float32), np.array([0.0, -0.0, 1e-5], np.float32)])
+    w = rng.uniform(1e-4, 2.0, ang.size).astype(np.float32)
+    lists = M.projection_lists(ang, w, rotation=0.25, resolution=0.139)
+    buf = ctypes.create_string_buffer(64)
+    f32 = np.float32
+    rw = f32(1.0) / (f32(0.139) * f32(0.1))
+    exp_a = []
+    exp_w = []
+    for a, b in zip(ang, w):
+        ref_lib.ref_stream_float(ctypes.c_float(f32(a) + f32(0.25)), buf, ctypes.c_size_t(64))
+        exp_a.append(buf.value.decode())
+        ref_lib.ref_stream_float(ctypes.c_float(f32(b) * rw), buf, ctypes.c_size_t(64))
+        exp_w.append(buf.value.decode())
+    assert lists["angles"] == " ".join(exp_a) + " " and lists["weights"] == " ".join(exp_w) + " "
