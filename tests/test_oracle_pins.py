@@ -408,3 +408,26 @@ def test_projection_lists_format_like_the_stream(ref_lib):
         ref_lib.ref_stream_float(ctypes.c_float(f32(b) * rw), buf, ctypes.c_size_t(64))
         exp_w.append(buf.value.decode())
     assert lists["angles"] == " ".join(exp_a) + " " and lists["weights"] == " ".join(exp_w) + " "
+
+
+@pytest.mark.parametrize("method,expected", [("ImageSum", 15.0), ("ImageAverage", 3.0), ("ImageWeightedAverage", 3.0),
+                                             ("ImageMedian", 3.0), ("ImageMin", 1.0), ("ImageMax", 5.0)])
+def test_average_known_answers(method, expected):
+    """The reference's AverageImage_Processing known answers (core/algorithms/UnitTests/
+    tImagingAlgorithms/tst_testImagingAlgorithms.cpp:209-249): five constant 11x11 frames of
+    1..5; the weighted average falls back to equal weights (sigma 0 everywhere)."""
+    stack = np.repeat(np.arange(1, 6, dtype=np.float32)[:, None, None], 121, axis=1).reshape(5, 11, 11)
+    out = O.average(stack, method)
+    assert np.all(out == np.float32(expected))
+
+
+def test_average_python_binding_cases():
+    """testBindAverageImage.py (core/algorithms/UnitTests/python): average, min, max and median
+    along the frame axis of x + 10 y + 100 z on an 11 x 10 x 12 grid are exact."""
+    a, b, c = np.linspace(0, 9, 10), np.linspace(0, 10, 11), np.linspace(0, 11, 12)
+    x, y, z = np.meshgrid(a, b, c)
+    img = (x + y * 10 + z * 100).astype(np.float32)
+    assert np.array_equal(O.average(img, "ImageAverage"), img.mean(axis=0, dtype=np.float64).astype(np.float32))
+    assert np.array_equal(O.average(img, "ImageMin"), img.min(axis=0))
+    assert np.array_equal(O.average(img, "ImageMax"), img.max(axis=0))
+    assert np.array_equal(O.average(img, "ImageMedian"), np.median(img, axis=0).astype(np.float32))
