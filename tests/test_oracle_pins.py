@@ -431,3 +431,27 @@ def test_average_python_binding_cases():
     assert np.array_equal(O.average(img, "ImageMin"), img.min(axis=0))
     assert np.array_equal(O.average(img, "ImageMax"), img.max(axis=0))
     assert np.array_equal(O.average(img, "ImageMedian"), np.median(img, axis=0).astype(np.float32))
+
+
+@pytest.mark.parametrize("refs_present", [(0, 5), (4, 0)])
+@pytest.mark.parametrize("usenorm", [False, True])
+def test_fulllognorm_without_darks_or_flats(ref_lib, refs_present, usenorm):
+    """The exact path's branches without darks (I alone) or without flats (-log(I - D) + dose,
+    NormPlugins.cpp:482-540), restated bit for bit."""
+    rng = _rng(32)
+    ndark, nflat = refs_present
+    nproj, nv, nu = 9, 10, 24
+    darks = np.round(rng.normal(100, 3, (4, nv, nu))).astype(np.float32)[:ndark]
+    flats = (rng.poisson(30000, (5, nv, nu)) + 100).astype(np.float32)[:nflat]
+    proj = (rng.poisson(20000, (nproj, nv, nu)) + 100).astype(np.float32)
+    proj[0, 0, :5] = 50
+    roi = (2, 2, 20, 9)
+    out_r, _, _, _, _ = O.ref_fulllognorm(proj, darks, flats, "ImageAverage", usenorm, roi)
+    refs = O.lognorm_refs(darks, flats, "ImageAverage", usenorm, roi)
+    if usenorm:
+        doses = np.array([O.frame_dose(proj[i], roi) for i in range(nproj)], np.float32)
+        dl = O.lognorm_doselog(doses, refs.darkdose)
+    else:
+        dl = np.zeros(1, np.float32)
+    out = O.lognorm_apply(proj, refs.dark, refs.logflat, dl, ndc=ndark > 0, nob=nflat > 0)
+    assert np.array_equal(out.view(np.uint32), out_r.view(np.uint32))
