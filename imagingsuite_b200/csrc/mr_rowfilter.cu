@@ -260,7 +260,9 @@ static __device__ __align__(256) float g_quant_scratch[2 * kQuantScratchMax];
 
 // Device address of g_quant_scratch per device ordinal, looked up on the first call made
 // with that device current. In host code the symbol itself is only a host-side stand-in,
-// never a device address, so kernels always receive the looked-up pointer.
+// never a device address, so kernels always receive the looked-up pointer. The cache lives
+// as long as the process; a cudaDeviceReset makes the cached address stale (documented in
+// the header).
 static float *quant_scratch_ptr(int device, mr_status *st)
 {
     constexpr int kMaxDevices = 64;
@@ -467,9 +469,15 @@ mr_status mr_quantize_noalloc(const float *in_d, size_t per, size_t nproj, int d
     cudaStream_t s = as_stream(stream);
     // the array keeps the previous call's values: the running maxima must start at zero
     MR_CUDA_TRY(cudaMemsetAsync(amax, 0, nproj * sizeof(float), s));
-    dim3 g(std::min<unsigned>(div_up(per, 256), 64u), static_cast<unsigned>(nproj));
-    k_absmax<<<g, 256, 0, s>>>(in_d, per, amax);
-    if ((st = check_launch("k_absmax")) != MR_OK) return st;
+    // one grid row per projection; gridDim.y stops at 65535, so the array's full 65536
+    // projections take two launches
+    constexpr size_t kGridYMax = 65535;
+    for (size_t p0 = 0; p0 < nproj; p0 += kGridYMax) {
+        const size_t np = std::min(kGridYMax, nproj - p0);
+        dim3 g(std::min<unsigned>(div_up(per, 256), 64u), static_cast<unsigned>(np));
+        k_absmax<<<g, 256, 0, s>>>(in_d + p0 * per, per, amax + p0);
+        if ((st = check_launch("k_absmax")) != MR_OK) return st;
+    }
     k_pow2_scales<<<div_up(nproj, 128), 128, 0, s>>>(amax, nproj, dtype, scale_d, inv);
     if ((st = check_launch("k_pow2_scales")) != MR_OK) return st;
     const size_t total = per * nproj;

@@ -233,8 +233,10 @@ mr_status mr_quantize(const float *in_d, size_t per, size_t nproj, int dtype, ui
  * library until the process exits); larger calls are rejected with MR_ERR_ARGUMENT. It
  * allocates nothing. The first call on a device looks up the array's device address
  * (cudaGetSymbolAddress) with that device current; make that first call before any stream
- * capture. All calls share the one array, and each call clears the part it uses first, so
- * calls that overlap on the GPU (on different streams without ordering) race. */
+ * capture. The address is kept for the life of the process: after cudaDeviceReset on a
+ * device, do not call this entry point on that device again. All calls share the one array,
+ * and each call clears the part it uses first, so calls that overlap on the GPU (on
+ * different streams without ordering) race. */
 mr_status mr_quantize_noalloc(const float *in_d, size_t per, size_t nproj, int dtype, uint16_t *out_d, float *scale_d,
                               void *stream);
 

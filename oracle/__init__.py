@@ -290,13 +290,51 @@ def fdk(proj, angles, weights, geom: FdkGeom, use_ref=False) -> np.ndarray:
     proj = _f32(proj)
     nproj, nv, nu = proj.shape
     angles, weights = _f32(angles), _f32(weights)
-    vol = np.zeros((nv, nu, nu), np.float32)
     if use_ref:
+        vol = np.empty((nv, nu, nu), np.float32)  # the harness copies the whole volume out
         _check_ref(ref().ref_fdk(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights),
                                  ctypes.byref(geom), _p(vol), None))
     else:
+        vol = np.zeros((nv, nu, nu), np.float32)
         orc().orc_fdk(_p(proj), _sz(nu), _sz(nv), _sz(nproj), _p(angles), _p(weights), ctypes.byref(geom), _p(vol))
     return vol
+
+
+class RefFdkSession:
+    """The reference FDKbp_single configured once (Configure + SetROI for the full detector)
+    and then given projections by repeated Process 3D calls, each adding into the same volume
+    (the way ReconEngine keeps one backprojector per slice block). Times the reference per
+    projection without its per-block set-up."""
+
+    def __init__(self, nu, nv, nproj_total, geom: FdkGeom):
+        lib = ref()
+        lib.ref_fdk_session_create.restype = ctypes.c_void_p
+        lib.ref_fdk_session_process.argtypes = [ctypes.c_void_p, _F, _sz, _F, _F]
+        lib.ref_fdk_session_volume.argtypes = [ctypes.c_void_p, _F]
+        lib.ref_fdk_session_destroy.argtypes = [ctypes.c_void_p]
+        self.nu, self.nv = nu, nv
+        self.h = lib.ref_fdk_session_create(_sz(nu), _sz(nv), _sz(nproj_total), ctypes.byref(geom))
+        if not self.h:
+            raise RuntimeError("reference module failed: " + lib.ref_last_error().decode(errors="replace"))
+
+    def process(self, proj, angles, weights) -> None:
+        proj = _f32(proj)
+        assert proj.shape[1:] == (self.nv, self.nu)
+        a, w = _f32(angles), _f32(weights)
+        _check_ref(ref().ref_fdk_session_process(self.h, _p(proj), _sz(proj.shape[0]), _p(a), _p(w)))
+
+    def volume(self) -> np.ndarray:
+        vol = np.empty((self.nv, self.nu, self.nu), np.float32)
+        _check_ref(ref().ref_fdk_session_volume(self.h, _p(vol)))
+        return vol
+
+    def close(self) -> None:
+        if self.h:
+            ref().ref_fdk_session_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def fdk_ramp(img) -> np.ndarray:

@@ -336,40 +336,108 @@ int ref_fdk_double(const float *proj, size_t nu, size_t nv, size_t nproj, const 
 }
 
 extern "C++" {
+static ReconConfig fdk_config(size_t nu, size_t nv, size_t nproj, const ref_fdk_geom *g)
+{
+    ReconConfig cfg;
+    cfg.ProjectionInfo.fSOD = g->sod;
+    cfg.ProjectionInfo.fSDD = g->sdd;
+    cfg.ProjectionInfo.fpPoint[0] = g->ppoint[0];
+    cfg.ProjectionInfo.fpPoint[1] = g->ppoint[1];
+    cfg.ProjectionInfo.fCenter = g->center;
+    cfg.ProjectionInfo.fResolution[0] = g->resolution[0];
+    cfg.ProjectionInfo.fResolution[1] = g->resolution[1];
+    cfg.MatrixInfo.fVoxelSize[0] = g->voxelsize[0];
+    cfg.MatrixInfo.fVoxelSize[1] = g->voxelsize[1];
+    cfg.MatrixInfo.fVoxelSize[2] = g->voxelsize[2];
+    cfg.ProjectionInfo.eDirection = static_cast<kipl::base::eRotationDirection>(g->direction);
+    cfg.ProjectionInfo.bCorrectTilt = g->correcttilt != 0;
+    cfg.ProjectionInfo.fTiltAngle = g->tiltangle;
+    cfg.ProjectionInfo.fTiltPivotPosition = g->tiltpivot;
+    cfg.ProjectionInfo.imagetype = ReconConfig::cProjections::ImageType_Projections;
+    cfg.ProjectionInfo.beamgeometry = ReconConfig::cProjections::BeamGeometry_Cone;
+    cfg.ProjectionInfo.nDims[0] = nu;
+    cfg.ProjectionInfo.nDims[1] = nv;
+    cfg.ProjectionInfo.nFirstIndex = 0;
+    cfg.ProjectionInfo.nLastIndex = nproj - 1;
+    cfg.ProjectionInfo.nProjectionStep = 1;
+    size_t roi[4] = {0, 0, nu, nv};
+    std::memcpy(cfg.ProjectionInfo.roi, roi, sizeof(roi));
+    std::memcpy(cfg.ProjectionInfo.projection_roi, roi, sizeof(roi));
+    cfg.MatrixInfo.nDims[0] = nu;
+    cfg.MatrixInfo.nDims[1] = nu;
+    cfg.MatrixInfo.nDims[2] = nv;
+    cfg.MatrixInfo.bUseROI = false;
+    return cfg;
+}
+} // extern "C++"
+
+// A configured FDKbp_single that keeps its volume between Process calls, as ReconEngine
+// keeps one backprojector per slice block and hands it projections (Configure and SetROI
+// once, then Process 3D; each Process adds into cbct_volume and redoes the final mirror).
+// Used to time the reference per projection without its per-block set-up.
+struct ref_fdk_session {
+    FDKbp_single *fdk;
+    size_t nu, nv;
+};
+
+void *ref_fdk_session_create(size_t nu, size_t nv, size_t nproj_total, const ref_fdk_geom *g)
+{
+    ref_fdk_session *s = nullptr;
+    int rc = guarded([&] {
+        std::unique_ptr<ref_fdk_session> hold(new ref_fdk_session{new FDKbp_single(nullptr), nu, nv});
+        std::map<std::string, std::string> par;
+        par["ProjectionBufferSize"] = "16";
+        par["SliceBlock"] = "32";
+        par["SubVolume"] = "1 1";
+        hold->fdk->Configure(fdk_config(nu, nv, nproj_total, g), par);
+        size_t roi[4] = {0, 0, nu, nv};
+        hold->fdk->SetROI(roi);
+        s = hold.release();
+    });
+    return rc == 0 ? s : nullptr;
+}
+
+int ref_fdk_session_process(void *session, const float *proj, size_t nproj, const float *angles,
+                            const float *weights)
+{
+    return guarded([&] {
+        ref_fdk_session *s = static_cast<ref_fdk_session *>(session);
+        size_t d3[3] = {s->nu, s->nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * s->nu * s->nv * nproj);
+        std::map<std::string, std::string> params;
+        params["angles"] = list_text(angles, nproj);
+        params["weights"] = list_text(weights, nproj);
+        s->fdk->Process(img, params);
+    });
+}
+
+// Copies the final volume (after the last Process call's mirror) to vol [nv][nu][nu].
+int ref_fdk_session_volume(void *session, float *vol)
+{
+    return guarded([&] {
+        ref_fdk_session *s = static_cast<ref_fdk_session *>(session);
+        std::memcpy(vol, s->fdk->volume.GetDataPtr(), sizeof(float) * s->fdk->volume.Size());
+    });
+}
+
+void ref_fdk_session_destroy(void *session)
+{
+    ref_fdk_session *s = static_cast<ref_fdk_session *>(session);
+    if (!s) return;
+    delete[] s->fdk->proj_matrices;
+    delete s->fdk;
+    delete s;
+}
+
+extern "C++" {
 template <typename Module>
 static void run_fdk(const float *proj, size_t nu, size_t nv, size_t nproj, const float *angles, const float *weights,
                     const ref_fdk_geom *g, float *vol, float *cbct_out)
 {
     {
-        ReconConfig cfg;
-        cfg.ProjectionInfo.fSOD = g->sod;
-        cfg.ProjectionInfo.fSDD = g->sdd;
-        cfg.ProjectionInfo.fpPoint[0] = g->ppoint[0];
-        cfg.ProjectionInfo.fpPoint[1] = g->ppoint[1];
-        cfg.ProjectionInfo.fCenter = g->center;
-        cfg.ProjectionInfo.fResolution[0] = g->resolution[0];
-        cfg.ProjectionInfo.fResolution[1] = g->resolution[1];
-        cfg.MatrixInfo.fVoxelSize[0] = g->voxelsize[0];
-        cfg.MatrixInfo.fVoxelSize[1] = g->voxelsize[1];
-        cfg.MatrixInfo.fVoxelSize[2] = g->voxelsize[2];
-        cfg.ProjectionInfo.eDirection = static_cast<kipl::base::eRotationDirection>(g->direction);
-        cfg.ProjectionInfo.bCorrectTilt = g->correcttilt != 0;
-        cfg.ProjectionInfo.fTiltAngle = g->tiltangle;
-        cfg.ProjectionInfo.fTiltPivotPosition = g->tiltpivot;
-        cfg.ProjectionInfo.imagetype = ReconConfig::cProjections::ImageType_Projections;
-        cfg.ProjectionInfo.beamgeometry = ReconConfig::cProjections::BeamGeometry_Cone;
-        cfg.ProjectionInfo.nDims[0] = nu;
-        cfg.ProjectionInfo.nDims[1] = nv;
-        cfg.ProjectionInfo.nFirstIndex = 0;
-        cfg.ProjectionInfo.nLastIndex = nproj - 1;
-        cfg.ProjectionInfo.nProjectionStep = 1;
+        ReconConfig cfg = fdk_config(nu, nv, nproj, g);
         size_t roi[4] = {0, 0, nu, nv};
-        std::memcpy(cfg.ProjectionInfo.roi, roi, sizeof(roi));
-        std::memcpy(cfg.ProjectionInfo.projection_roi, roi, sizeof(roi));
-        cfg.MatrixInfo.nDims[0] = nu;
-        cfg.MatrixInfo.nDims[1] = nu;
-        cfg.MatrixInfo.nDims[2] = nv;
-        cfg.MatrixInfo.bUseROI = false;
         std::map<std::string, std::string> par;
         par["ProjectionBufferSize"] = "16";
         par["SliceBlock"] = "32";

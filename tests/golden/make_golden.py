@@ -10,7 +10,8 @@ oracle/_ref/libmuhrec_ref.so (make -C oracle ref), on:
 * small seeded cases of FullLogNorm, ProjectionFilterSingle, MultiProjectionBPparallel, FDKbp_single
   and LinearForwardProjector (the Joseph projector).
 
-usage: python tests/golden/make_golden.py [reference root]
+usage: python tests/golden/make_golden.py <reference root>
+   (or set MUHREC_REFERENCE to the reference checkout)
 The fixtures are committed; the tests never read the reference tree.
 """
 import os
@@ -31,7 +32,10 @@ def tiff(path):
     return np.array(Image.open(path)).astype(np.float32)
 
 
-def main(ref_root="/root/reference"):
+def main(ref_root=None):
+    ref_root = ref_root or os.environ.get("MUHREC_REFERENCE")
+    if not ref_root or not os.path.isdir(ref_root):
+        sys.exit("make_golden.py: give the reference checkout as the argument or in MUHREC_REFERENCE")
     data = os.path.join(ref_root, "core", "algorithms", "UnitTests", "data")
     out = {}
 

@@ -45,6 +45,22 @@ def test_noalloc_matches_quantize_twice(cuda, dtype):
     assert status.value == 0
 
 
+def test_noalloc_at_its_maximum(cuda):
+    """Exactly 65536 projections (the array's size, one more than a grid's y extent) work and
+    equal mr_quantize run on the same projections in two calls (mr_quantize takes at most
+    65535 per call; every projection is scaled on its own)."""
+    lib = L.lib()
+    nproj, per = 65536, 4
+    rng = np.random.default_rng(7)
+    x = torch.from_numpy((rng.standard_normal((nproj, per)) * np.exp(rng.uniform(-20, 20, (nproj, 1))))
+                         .astype(np.float32)).to(cuda)
+    q_new, s_new = _run(lib.mr_quantize_noalloc, x, per, nproj, L.MR_F16)
+    q_a, s_a = _run(lib.mr_quantize, x[:65535].contiguous(), per, 65535, L.MR_F16)
+    q_b, s_b = _run(lib.mr_quantize, x[65535:].contiguous(), per, 1, L.MR_F16)
+    assert np.array_equal(s_new, np.concatenate([s_a, s_b]))
+    assert np.array_equal(q_new, np.concatenate([q_a, q_b]))
+
+
 def test_noalloc_rejects_oversize(cuda):
     lib = L.lib()
     x = torch.zeros(4, device=cuda)
