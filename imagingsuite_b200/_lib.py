@@ -24,6 +24,7 @@ P_double = ctypes.POINTER(ctypes.c_double)
 MR_OK, MR_ERR_ARGUMENT, MR_ERR_CUDA, MR_ERR_ALLOCATION, MR_ERR_UNSUPPORTED, MR_ERR_DEVICE = range(6)
 MR_F32, MR_BF16, MR_F16, MR_U16 = 0, 1, 2, 3
 MR_PLANE_XY, MR_PLANE_YZ = 1, 4
+MR_BP_MULTIPROJ_PARALLEL, MR_BP_MULTIPROJ_SERIAL, MR_BP_NEAREST = 0, 1, 2
 
 
 class FdkGeom(ctypes.Structure):
@@ -75,6 +76,9 @@ _PROTOS = {
                                       c_size, c_size, c_void, c_int, c_float, c_float, c_void, c_void]),
     "mr_bp_parallel_rows": (c_int, [c_void, c_size, c_int, c_void, c_void, c_void, c_void, c_void, c_void, c_size,
                                     c_size, c_size, c_void, c_int, c_float, c_float, c_size, c_size, c_void, c_void]),
+    "mr_bp_parallel_variant": (c_int, [c_int, c_void, c_size, c_int, c_void, c_void, c_void, c_void, c_void, c_void,
+                                       c_size, c_size, c_size, c_void, c_int, c_float, c_float, c_size, c_size, c_void,
+                                       c_void]),
     "mr_quantize": (c_int, [c_void, c_size, c_size, c_int, c_void, c_void, c_void]),
     "mr_quantize_noalloc": (c_int, [c_void, c_size, c_size, c_int, c_void, c_void, c_void]),
     "mr_fdk_partials": (c_int, [ctypes.POINTER(FdkGeom), c_size, c_size, P_float, c_size, P_float, P_float, P_float,

@@ -35,7 +35,13 @@ __device__ __forceinline__ float sample(const void *base, size_t idx)
 
 // MultiProjectionBPparallel::BackProject (MultiProjBPparallel.cpp:39-170). x1, y1 are the
 // reference's 1-based loop indices; the voxel is vol[y1-1][x1-1][z]; rows y1-1 in
-// [ybegin, yend) are processed.
+// [ybegin, yend) are processed. `variant` selects the factory's other two parallel-beam
+// backprojectors on the same loop structure:
+//   1 MultiProjectionBP (MultiProjBP.cpp:36-146): identical without tilt; with tilt the centre
+//     offset is subtracted after the x term and each 4-slice group g takes the weight
+//     |(u - n) - g * tinc| (one shift per group, :81-84);
+//   2 NearestNeighborBP (NNMultiProjBP.cpp:36-121): the sample at the truncated position only,
+//     no weights, the centre offset (tilt) subtracted after the x term, no per-slice shift.
 template <int DT, int CZ>
 __global__ void __launch_bounds__(128) k_bp_parallel(const void *__restrict__ proj, const float *__restrict__ scale,
                                                      const float *__restrict__ weight, const int32_t *__restrict__ index,
@@ -43,7 +49,7 @@ __global__ void __launch_bounds__(128) k_bp_parallel(const void *__restrict__ pr
                                                      const float *__restrict__ cosv, const float *__restrict__ startu,
                                                      int nproj, int nu, int nv, const uint32_t *__restrict__ mask,
                                                      int tilt, float toff, float tinc, int ybegin, int yend,
-                                                     float *__restrict__ vol)
+                                                     int variant, float *__restrict__ vol)
 {
     const int x1 = blockIdx.x * blockDim.x + threadIdx.x + 1;
     const int y1 = ybegin + blockIdx.y * blockDim.y + threadIdx.y + 1;
@@ -62,15 +68,61 @@ __global__ void __launch_bounds__(128) k_bp_parallel(const void *__restrict__ pr
 
     for (int i = 0; i < nproj; ++i) {
         float local = __fadd_rn(startu[i], __fmul_rn(cosv[i], fy));
-        if (tilt) local = __fsub_rn(local, toff);
+        if (tilt && variant == 0) local = __fsub_rn(local, toff);
         float posu = __fsub_rn(local, __fmul_rn(sinv[i], fx));
+        if (tilt && variant != 0) posu = __fsub_rn(posu, toff);
         const int n = __float2int_rz(posu);
         if (n < 0 || um2 < n) continue;
         const int slab = index ? index[i] : i;
         float w = weight ? weight[i] : 1.0f;
         if (DT != MR_F32) w = scale[slab] * w;
         const size_t base = static_cast<size_t>(slab) * pstride + n;
-        if (!tilt) {
+        if (variant == 2) {
+#pragma unroll
+            for (int c = 0; c < CZ; ++c) {
+                const int z = z0 + c;
+                if (z < nz4) {
+                    float pa = sample<DT>(proj, base + static_cast<size_t>(z) * nu);
+                    if (weight || DT != MR_F32) pa = __fmul_rn(pa, w);
+                    acc[c] = __fadd_rn(acc[c], pa);
+                }
+            }
+        } else if (variant == 1) {
+            // MultiProjBP.cpp:87-98 (tilt) and :128-143: column B is column A plus SizeV/4
+            // vectors, i.e. 4*(nv/4) slices further in the transposed, 4-padded projection
+            // buffer. With nv a multiple of 4 that is the next detector column; otherwise the
+            // sample of slice z is slice 4*(nv/4)+z of column n, the zero padding, or slice
+            // 4*(nv/4)+z-nvpad of column n+1.
+            const float d = __fsub_rn(posu, static_cast<float>(n));
+            const int nvpad = (nv & 3) ? nz4 + 4 : nv;
+#pragma unroll
+            for (int c = 0; c < CZ; c += 4) {
+                const int g = (z0 + c) / 4;
+                const float wb = tilt ? fabsf(__fsub_rn(d, __fmul_rn(static_cast<float>(g), tinc))) : fabsf(d);
+                const float wa = __fsub_rn(1.0f, wb);
+#pragma unroll
+                for (int q = 0; q < 4 && c + q < CZ; ++q) {
+                    const int z = z0 + c + q;
+                    if (z < nz4) {
+                        float pa = sample<DT>(proj, base + static_cast<size_t>(z) * nu);
+                        float pb;
+                        if (nvpad == nv) {
+                            pb = sample<DT>(proj, base + static_cast<size_t>(z) * nu + 1);
+                        } else {
+                            const int k = nz4 + z;
+                            pb = k < nv ? sample<DT>(proj, base + static_cast<size_t>(k) * nu)
+                                 : k < nvpad ? 0.0f
+                                             : sample<DT>(proj, base + static_cast<size_t>(k - nvpad) * nu + 1);
+                        }
+                        if (weight || DT != MR_F32) {
+                            pa = __fmul_rn(pa, w);
+                            pb = __fmul_rn(pb, w);
+                        }
+                        acc[c + q] = __fadd_rn(acc[c + q], __fadd_rn(__fmul_rn(pa, wa), __fmul_rn(pb, wb)));
+                    }
+                }
+            }
+        } else if (!tilt) {
             const float wb = fabsf(__fsub_rn(posu, static_cast<float>(n)));
             const float wa = __fsub_rn(1.0f, wb);
 #pragma unroll
@@ -268,10 +320,12 @@ namespace mr {
 mr_status bp_parallel_rows(const void *proj_d, int dtype, const float *scale_d, const float *weight_d,
                            const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
                            size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt,
-                           float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, float *vol_d, void *stream)
+                           float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, int variant, float *vol_d,
+                           void *stream)
 {
     if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
         return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: null pointer");
+    if (variant < 0 || variant > 2) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: unknown backprojector variant %d", variant);
     if (dtype != MR_F32 && dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: dtype");
     if (dtype != MR_F32 && !scale_d) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: 16-bit projections need scale_d");
     if (nu < 2 || nu > 65536 || nv > 65536) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel: unsupported size");
@@ -287,15 +341,15 @@ mr_status bp_parallel_rows(const void *proj_d, int dtype, const float *scale_d, 
     switch (dtype) {
     case MR_F32:
         k_bp_parallel<MR_F32, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, np, iu, iv,
-                                                         mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, vol_d);
+                                                         mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, variant, vol_d);
         break;
     case MR_BF16:
         k_bp_parallel<MR_BF16, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, np, iu, iv,
-                                                          mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, vol_d);
+                                                          mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, variant, vol_d);
         break;
     default:
         k_bp_parallel<MR_F16, CZ><<<grid, block, 0, s>>>(proj_d, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, np, iu, iv,
-                                                         mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, vol_d);
+                                                         mask_d, correcttilt, tiltoffset, tiltinc, yb, ye, variant, vol_d);
     }
     return check_launch("k_bp_parallel");
 }
@@ -309,7 +363,7 @@ mr_status mr_bp_parallel(const void *proj_d, int dtype, const float *scale_d, co
                          float tiltinc, float *vol_d, void *stream)
 {
     return bp_parallel_rows(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
-                            correcttilt, tiltoffset, tiltinc, 0, nu, vol_d, stream);
+                            correcttilt, tiltoffset, tiltinc, 0, nu, 0, vol_d, stream);
 }
 
 // FDKbp_single::getProjMatrix (fdkbp_single.cpp:83-255), float arithmetic as written there.

@@ -103,7 +103,22 @@ __device__ __forceinline__ void staged_column(float (&acc)[TZ], const float *p, 
     }
 }
 
-template <bool HASW>
+// NearestNeighborBP's column (NNMultiProjBP.cpp:84-90): the sample at the truncated position.
+template <bool HASW, bool FULL>
+__device__ __forceinline__ void staged_column_nn(float (&acc)[TZ], const float *p, float w, int zmax)
+{
+#pragma unroll
+    for (int q = 0; q < TZ; ++q) {
+        if (!FULL && q >= zmax) break;
+        float pa = p[q * BW];
+        if (HASW) pa = __fmul_rn(pa, w);
+        acc[q] = __fadd_rn(acc[q], pa);
+    }
+}
+
+// NN selects NearestNeighborBP (NNMultiProjBP.cpp:36-121, no tilt): same positions, the one
+// sample at n instead of the interpolation.
+template <bool HASW, bool NN>
 __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __grid_constant__ CUtensorMap tmap, const Params P)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
@@ -259,8 +274,14 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
                     for (int e = 0; e < G; ++e) {
                         if (q_mode[e] != 1) continue;
                         const float w = HASW ? S.geo[(gb * NB + b0 + e) * GEO + 3] : 1.0f;
-                        if (zmax == TZ) staged_column<HASW, true>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
-                        else staged_column<HASW, false>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
+                        if (NN) {
+                            if (zmax == TZ) staged_column_nn<HASW, true>(acc, S.box + q_off[e], w, zmax);
+                            else staged_column_nn<HASW, false>(acc, S.box + q_off[e], w, zmax);
+                        } else if (zmax == TZ) {
+                            staged_column<HASW, true>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
+                        } else {
+                            staged_column<HASW, false>(acc, S.box + q_off[e], q_wa[e], q_wb[e], w, zmax);
+                        }
                     }
                     continue;
                 }
@@ -273,7 +294,8 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
                     const int mode = setup(b, n, off, wa, wb); // formed again: no indexed arrays
                     const float w = HASW ? S.geo[(gb * NB + b) * GEO + 3] : 1.0f;
                     if (mode == 1) {
-                        staged_column<HASW, false>(acc, S.box + off, wa, wb, w, zmax);
+                        if (NN) staged_column_nn<HASW, false>(acc, S.box + off, w, zmax);
+                        else staged_column<HASW, false>(acc, S.box + off, wa, wb, w, zmax);
                     } else if (mode == 2) {
                         const int i = s * NB + b;
                         const int slab = P.index ? __float_as_int(S.geo[(gb * NB + b) * GEO + 4]) : i;
@@ -281,6 +303,12 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
 #pragma unroll
                         for (int q = 0; q < TZ; ++q) {
                             if (q >= zmax) break;
+                            if (NN) {
+                                float pa = __ldg(img + static_cast<size_t>(q) * P.nu);
+                                if (HASW) pa = __fmul_rn(pa, w);
+                                acc[q] = __fadd_rn(acc[q], pa);
+                                continue;
+                            }
                             float pa = __ldg(img + static_cast<size_t>(q) * P.nu), pb = __ldg(img + static_cast<size_t>(q) * P.nu + 1);
                             if (HASW) {
                                 pa = __fmul_rn(pa, w);
@@ -322,7 +350,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
 mr_status bp_parallel_staged_launch(const float *proj_d, size_t nslabs, const float *weight_d, const int32_t *index_d,
                                     const float *sin_d, const float *cos_d, const float *startu_d, size_t nproj,
                                     size_t nu, size_t nv, const uint32_t *mask_d, size_t y_begin, size_t y_end,
-                                    float *vol_d, cudaStream_t s)
+                                    bool nn, float *vol_d, cudaStream_t s)
 {
     using namespace bp2;
     if ((nu * 4) % 16 != 0 || (reinterpret_cast<uintptr_t>(proj_d) % 16) != 0 || nv < 4 || nslabs == 0 ||
@@ -356,25 +384,53 @@ mr_status bp_parallel_staged_launch(const float *proj_d, size_t nslabs, const fl
     P.yend = static_cast<int>(y_end);
     const size_t smem = Smem::bytes();
     dim3 grid(div_up(nu, TX), div_up(y_end - y_begin, TY), div_up(static_cast<size_t>(P.nz4), TZ));
-    if (weight_d) {
-        MR_CUDA_TRY(cudaFuncSetAttribute(k_bp_par_staged<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        k_bp_par_staged<true><<<grid, THREADS, smem, s>>>(map, P);
-    } else {
-        MR_CUDA_TRY(cudaFuncSetAttribute(k_bp_par_staged<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
-        k_bp_par_staged<false><<<grid, THREADS, smem, s>>>(map, P);
-    }
-    return check_launch("k_bp_par_staged");
+    auto launch = [&](auto kernel) -> mr_status {
+        MR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+        kernel<<<grid, THREADS, smem, s>>>(map, P);
+        return check_launch("k_bp_par_staged");
+    };
+    if (nn) return weight_d ? launch(k_bp_par_staged<true, true>) : launch(k_bp_par_staged<false, true>);
+    return weight_d ? launch(k_bp_par_staged<true, false>) : launch(k_bp_par_staged<false, false>);
 }
 
 // mr_backproject.cu: the direct-load kernel for a range of volume rows
 mr_status bp_parallel_rows(const void *proj_d, int dtype, const float *scale_d, const float *weight_d,
                            const int32_t *index_d, const float *sin_d, const float *cos_d, const float *startu_d,
                            size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt,
-                           float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, float *vol_d, void *stream);
+                           float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, int variant, float *vol_d,
+                           void *stream);
 
 } // namespace mr
 
 using namespace mr;
+
+extern "C" mr_status mr_bp_parallel_variant(int variant, const void *proj_d, size_t nslabs, int dtype,
+                                            const float *scale_d, const float *weight_d, const int32_t *index_d,
+                                            const float *sin_d, const float *cos_d, const float *startu_d, size_t nproj,
+                                            size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt,
+                                            float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, float *vol_d,
+                                            void *stream)
+{
+    if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
+        return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_variant: null pointer");
+    if (variant < MR_BP_MULTIPROJ_PARALLEL || variant > MR_BP_NEAREST)
+        return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_variant: unknown backprojector variant %d", variant);
+    if (y_begin > y_end || y_end > nu) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_variant: row range outside [0, nu]");
+    // the serial MultiProjectionBP computes exactly what MultiProjectionBPparallel computes
+    // unless the tilt is corrected or the slice count is not a multiple of 4 (its second
+    // interpolation sample is then read from another place of its projection buffer)
+    if (variant == MR_BP_MULTIPROJ_SERIAL && !correcttilt && (nv & 3) == 0) variant = MR_BP_MULTIPROJ_PARALLEL;
+    if (variant != MR_BP_MULTIPROJ_SERIAL && dtype == MR_F32 && !correcttilt && nproj > 0 && nproj <= 0x7fffffff &&
+        nu >= 2 && nu <= 65536 && nv <= 65536 && y_begin < y_end) {
+        if (!index_d && nslabs < nproj) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_variant: nslabs below nproj");
+        mr_status st = bp_parallel_staged_launch(static_cast<const float *>(proj_d), nslabs, weight_d, index_d, sin_d,
+                                                 cos_d, startu_d, nproj, nu, nv, mask_d, y_begin, y_end,
+                                                 variant == MR_BP_NEAREST, vol_d, as_stream(stream));
+        if (st != MR_ERR_UNSUPPORTED) return st;
+    }
+    return bp_parallel_rows(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
+                            correcttilt, tiltoffset, tiltinc, y_begin, y_end, variant, vol_d, stream);
+}
 
 extern "C" mr_status mr_bp_parallel_rows(const void *proj_d, size_t nslabs, int dtype, const float *scale_d,
                                          const float *weight_d, const int32_t *index_d, const float *sin_d,
@@ -382,19 +438,9 @@ extern "C" mr_status mr_bp_parallel_rows(const void *proj_d, size_t nslabs, int 
                                          const uint32_t *mask_d, int correcttilt, float tiltoffset, float tiltinc,
                                          size_t y_begin, size_t y_end, float *vol_d, void *stream)
 {
-    if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
-        return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: null pointer");
-    if (y_begin > y_end || y_end > nu) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: row range outside [0, nu]");
-    if (dtype == MR_F32 && !correcttilt && nproj > 0 && nproj <= 0x7fffffff && nu >= 2 && nu <= 65536 && nv <= 65536 &&
-        y_begin < y_end) {
-        if (!index_d && nslabs < nproj) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_staged: nslabs below nproj");
-        mr_status st = bp_parallel_staged_launch(static_cast<const float *>(proj_d), nslabs, weight_d, index_d, sin_d,
-                                                 cos_d, startu_d, nproj, nu, nv, mask_d, y_begin, y_end, vol_d,
-                                                 as_stream(stream));
-        if (st != MR_ERR_UNSUPPORTED) return st;
-    }
-    return bp_parallel_rows(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
-                            correcttilt, tiltoffset, tiltinc, y_begin, y_end, vol_d, stream);
+    return mr_bp_parallel_variant(MR_BP_MULTIPROJ_PARALLEL, proj_d, nslabs, dtype, scale_d, weight_d, index_d, sin_d,
+                                  cos_d, startu_d, nproj, nu, nv, mask_d, correcttilt, tiltoffset, tiltinc, y_begin,
+                                  y_end, vol_d, stream);
 }
 
 extern "C" mr_status mr_bp_parallel_staged(const void *proj_d, size_t nslabs, int dtype, const float *scale_d,

@@ -709,6 +709,8 @@ class MultiProjectionBPparallel(_BackProjectorBase):
     StdBackProjectorBase driver (StdBackProjectorBase.cpp). Volume is MatrixZXY:
     tensor (ny, nx, nz) = (nu, nu, nv), z fastest."""
 
+    _variant = L.MR_BP_MULTIPROJ_PARALLEL
+
     def __init__(self):
         super().__init__("Multi projection BP parallel")
         self.SizeU = self.SizeV = 0
@@ -790,7 +792,11 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         args = (dtype, _ptr(scale), None if prefiltered_weights else geo[3].data_ptr(), idx.data_ptr(),
                 geo[0].data_ptr(), geo[1].data_ptr(), geo[2].data_ptr(), sel.size, self.SizeU, self.SizeV,
                 self._mask.data_ptr(), int(pi.bCorrectTilt), toff.value, tinc.value, self.volume.data_ptr(), _stream())
-        if rows is not None:
+        if self._variant != L.MR_BP_MULTIPROJ_PARALLEL:
+            y0, y1 = (0, self.SizeU) if rows is None else (int(rows[0]), int(rows[1]))
+            check(L.lib().mr_bp_parallel_variant(self._variant, proj.data_ptr(), nproj, *args[:-2], y0, y1,
+                                                 *args[-2:]))
+        elif rows is not None:
             check(L.lib().mr_bp_parallel_rows(proj.data_ptr(), nproj, *args[:-2], int(rows[0]), int(rows[1]),
                                               *args[-2:]))
         elif self.staging:
@@ -813,21 +819,30 @@ class MultiProjectionBP(MultiProjectionBPparallel):
     """MultiProjectionBP, the reference's serial backprojector (factory name "MultiProjBP",
     StdBackProjectors/src/MultiProjBP.cpp:36-146). Without tilt correction it computes exactly
     what MultiProjectionBPparallel computes (the same positions, weights and accumulation order,
-    pinned against the compiled reference), so it runs the same kernels. With tilt correction the
-    serial version shifts the interpolation weight by one `4 tan(tilt)` per group of 4 slices
-    (MultiProjBP.cpp:83) where the parallel one shifts it twice (MultiProjBPparallel.cpp:88-99);
-    that variant is not built here, and Process raises for it."""
+    pinned against the compiled reference). With tilt correction it subtracts the centre offset
+    after the x term and shifts the interpolation weight by one `4 tan(tilt)` per group of 4
+    slices (MultiProjBP.cpp:61-84), where the parallel one shifts it twice
+    (MultiProjBPparallel.cpp:88-99): mr_bp_parallel_variant(MR_BP_MULTIPROJ_SERIAL)."""
+
+    _variant = L.MR_BP_MULTIPROJ_SERIAL
 
     def __init__(self):
         super().__init__()
         self.m_sModuleName = "Multi projection BP"
 
-    def Process(self, projections: torch.Tensor, parameters: dict, prefiltered_weights: bool = False,
-                rows: tuple | None = None) -> int:
-        if self.mConfig.ProjectionInfo.bCorrectTilt:
-            raise ReconException("MultiProjectionBP with tilt correction is not supported by this module "
-                                 "(MultiProjectionBPparallel is)")
-        return super().Process(projections, parameters, prefiltered_weights, rows)
+
+class NearestNeighborBP(MultiProjectionBPparallel):
+    """NearestNeighborBP (factory name "NNMultiProjBP", StdBackProjectors/src/NNMultiProjBP.cpp:
+    36-121): the same positions as MultiProjectionBP, each voxel adding the one sample at the
+    truncated detector position (no interpolation); with tilt correction the centre offset is
+    subtracted after the x term and there is no per-slice shift
+    (mr_bp_parallel_variant(MR_BP_NEAREST))."""
+
+    _variant = L.MR_BP_NEAREST
+
+    def __init__(self):
+        super().__init__()
+        self.m_sModuleName = "NearestNeighborBP"
 
 
 class FDKbp_single(_BackProjectorBase):

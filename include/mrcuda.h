@@ -291,6 +291,23 @@ mr_status mr_bp_parallel_rows(const void *proj_d, size_t nslabs, int dtype, cons
                               const float *startu_d, size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d,
                               int correcttilt, float tiltoffset, float tiltinc, size_t y_begin, size_t y_end,
                               float *vol_d, void *stream);
+/* The factory's three parallel-beam backprojectors on the same kernels
+ * (StdBackProjectors/src/StdBackProjectors.cpp:25-60), for the volume rows [y_begin, y_end):
+ *   MR_BP_MULTIPROJ_PARALLEL  "MultiProjBPparallel" (MultiProjBPparallel.cpp:39-170): as
+ *     mr_bp_parallel_rows;
+ *   MR_BP_MULTIPROJ_SERIAL    "MultiProjBP" (MultiProjBP.cpp:36-146): the same without tilt
+ *     correction; with it, u = ((startu_i + cos_i y) - sin_i x) - tiltoffset and the 4-slice
+ *     group g takes the weight |(u - n) - g*tiltinc|;
+ *   MR_BP_NEAREST             "NearestNeighborBP" (NNMultiProjBP.cpp:36-121): the same u (minus
+ *     tiltoffset after the x term with tilt correction), vol[z] += P_i[z][n] with n = (int)u in
+ *     [0, nu-2], no interpolation and no per-slice shift.
+ * Results equal each reference module's bit for bit (FP32). */
+enum { MR_BP_MULTIPROJ_PARALLEL = 0, MR_BP_MULTIPROJ_SERIAL = 1, MR_BP_NEAREST = 2 };
+mr_status mr_bp_parallel_variant(int variant, const void *proj_d, size_t nslabs, int dtype, const float *scale_d,
+                                 const float *weight_d, const int32_t *index_d, const float *sin_d, const float *cos_d,
+                                 const float *startu_d, size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d,
+                                 int correcttilt, float tiltoffset, float tiltinc, size_t y_begin, size_t y_end,
+                                 float *vol_d, void *stream);
 
 /* ---------------------------------------------------------------------------------
  * FDK cone-beam backprojection: FDKbp_single

@@ -381,7 +381,9 @@ static void bp_flush(const float *buf, size_t count, size_t nu, size_t nv, size_
                 int n = (int)posu;
                 if (n < 0 || sizeum2 < n) continue;
                 const float *a = buf + (i * nu + (size_t)n) * nvpad;
-                const float *b = a + nvpad;
+                /* MultiProjBP.cpp:92,147 steps to column B by SizeV/4 vectors, not the padded
+                 * column length: with nv not a multiple of 4 it reads inside the padded buffer */
+                const float *b = a + (variant == 1 ? 4 * (nv / 4) : nvpad);
                 if (variant == 2) {
                     for (size_t z = 0; z < 4 * sizez; ++z) col[z] = col[z] + a[z];
                 } else if (correcttilt && variant == 1) {

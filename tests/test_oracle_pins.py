@@ -62,12 +62,15 @@ def test_bp_serial_tilt_shifts_once(ref_lib):
 @pytest.mark.parametrize("tilt", [False, True])
 @pytest.mark.parametrize("direction", [0, 1])
 @pytest.mark.parametrize("buffersize", [16, 7])
-def test_bp_variants_bit_exact(ref_lib, variant, tilt, direction, buffersize):
+@pytest.mark.parametrize("nv", [12, 7, 10])
+def test_bp_variants_bit_exact(ref_lib, variant, tilt, direction, buffersize, nv):
     """The factory's other parallel-beam backprojectors restated (orc_bp_parallel_variant): the
-    serial MultiProjectionBP (one weight shift per slice group under tilt) and NearestNeighborBP
-    (truncated position, no interpolation, constant tilt offset), against the compiled modules."""
-    rng = _rng(30 + buffersize + 2 * direction)
-    nproj, nv, nu = 37, 12, 48
+    serial MultiProjectionBP (one weight shift per slice group under tilt; with a slice count
+    that is not a multiple of 4 its second sample comes from elsewhere in the padded buffer) and
+    NearestNeighborBP (truncated position, no interpolation, constant tilt offset), against the
+    compiled modules."""
+    rng = _rng(30 + buffersize + 2 * direction + nv)
+    nproj, nu = 37, 48
     proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
     ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
     w = rng.uniform(0.5, 1.5, nproj).astype(np.float32)
@@ -76,15 +79,18 @@ def test_bp_variants_bit_exact(ref_lib, variant, tilt, direction, buffersize):
     assert np.array_equal(O.bp_parallel(proj, ang, w, 23.5, **kw), O.bp_parallel(proj, ang, w, 23.5, use_ref=True, **kw))
 
 
-def test_bp_serial_module_rejects_tilt():
-    from imagingsuite_b200 import modules as M
-
-    cfg = M.ReconConfig()
-    cfg.ProjectionInfo.bCorrectTilt = True
-    mod = M.MultiProjectionBP()
-    mod.Configure(cfg, {"ProjectionBufferSize": "16", "SliceBlock": "32", "SubVolume": "1 1"})
-    with pytest.raises(M.ReconException, match="tilt"):
-        mod.Process(None, {})
+def test_bp_serial_ragged_differs_from_parallel(ref_lib):
+    """Without tilt and with a slice count that is not a multiple of 4 the serial
+    MultiProjectionBP no longer equals the parallel one (its column B stride), so the module
+    runs its own sampling there."""
+    rng = _rng(22)
+    nproj, nv, nu = 19, 7, 40
+    proj = rng.standard_normal((nproj, nv, nu)).astype(np.float32)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    w = np.ones(nproj, np.float32)
+    par = O.bp_parallel(proj, ang, w, 19.5, use_ref=True)
+    ser = O.bp_parallel(proj, ang, w, 19.5, use_ref=True, serial=True)
+    assert np.abs(par - ser).max() > 0.1
 
 
 def test_bp_parallel_ragged_sizes(ref_lib):
