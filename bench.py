@@ -648,7 +648,7 @@ def cpu_baseline(w, counts, pipe, angles, weights, cfg, device, budget_s=20.0):
     setup = _timed(lambda: sess_box.append(oracle.RefFdkSession(nu, nv, nproj, g)))
     sess = sess_box[0]
     pick = np.linspace(0, nproj, 17, endpoint=False).astype(np.int64)  # spread over the arc
-    sub = counts[torch.from_numpy(pick).to(device)]
+    sub = torch.stack([counts[int(i)] for i in pick])  # (uint16 tensors take no index lists)
     proj = pipe._lognorm_into(sub, out=torch.empty(sub.shape, dtype=torch.float32, device=device)).cpu().numpy()
     a, wt = angles[pick], weights[pick]
     t1 = _timed(lambda: sess.process(proj[:1], a[:1], wt[:1]))

@@ -60,6 +60,7 @@ class MatrixInfo:
     nDims: tuple = (0, 0, 0)
     fVoxelSize: tuple = (0.1, 0.1, 0.1)
     bUseROI: bool = False
+    roi: tuple = (0, 0, 0, 0)  # x0, y0, x1, y1 of the slices, inclusive (GetSlice crops to it)
 
 
 @dataclass
@@ -174,6 +175,7 @@ class FullLogNorm:
         self.nDCCount, self.nOBCount = nd, nf
         f32 = np.float32
         darkdose = f32(0.0)
+        self.mDark = self.mFlatField = None
         if nd:
             doses = self._frame_doses(darks) if self.bUseNormROI else np.zeros(nd, np.float32)
             acc = f32(0.0)
@@ -181,8 +183,6 @@ class FullLogNorm:
                 acc = doses[i] if i == 0 else f32(acc + doses[i])
             darkdose = f32(acc / f32(nd))
             self.mDark = self._average(darks)
-        else:
-            self.mDark = torch.zeros(flats.shape[1:], dtype=torch.float32, device=flats.device)
         flatdose = f32(1.0)
         if nf:
             doses = self._frame_doses(flats) if self.bUseNormROI else np.ones(nf, np.float32)
@@ -192,12 +192,20 @@ class FullLogNorm:
                 acc = t if i == 0 else f32(acc + t)
             flatdose = f32(acc / f32(nf))
             flat = self._average(flats)
-        else:
-            raise ReconException("FullLogNorm needs flat field images")
+            # FullLogNorm::SetReferenceImages (NormPlugins.cpp:300-311): the reference dose must be finite
+            dose = f32(1.0) / flatdose if flatdose != 0 else f32(np.inf)
+            if np.isnan(dose):
+                raise ReconException("The reference dose is a NaN")
+            if np.isinf(dose):
+                raise ReconException("The reference dose is Inf")
+            self.mFlatField = torch.empty_like(flat)
+            check(L.lib().mr_lognorm_logflat(self.mDark.data_ptr() if nd else flat.data_ptr(), flat.data_ptr(),
+                                             flat.numel(), int(nd > 0), float(flatdose), self.mFlatField.data_ptr(),
+                                             _stream()))
         self.fDarkDose, self.fFlatDose = float(darkdose), float(flatdose)
-        self.mFlatField = torch.empty_like(flat)
-        check(L.lib().mr_lognorm_logflat(self.mDark.data_ptr(), flat.data_ptr(), flat.numel(), int(nd > 0),
-                                         float(flatdose), self.mFlatField.data_ptr(), _stream()))
+        # without flats the module runs -log(I - D) + dose (NormPlugins.cpp:498-540); without
+        # darks I - D is I
+        self._refs_set = True
 
     def Process(self, img: torch.Tensor, coeff: dict | None = None) -> torch.Tensor:
         return self.ProcessCore(img, coeff if coeff is not None else {})
@@ -208,11 +216,14 @@ class FullLogNorm:
         Doses come from ``coeff['dose']`` (text, as the engine passes them) or, when absent,
         are computed on the device over the dose ROI (ProjectionReader::GetProjectionDose)."""
         _require_cuda(img, "projections")
-        if self.mFlatField is None:
+        if not getattr(self, "_refs_set", False):
             raise ReconException("FullLogNorm: reference images are not set")
         nproj, nv, nu = img.shape
-        if self.mFlatField.numel() != nv * nu:
+        if self.nOBCount and self.mFlatField.numel() != nv * nu:
             raise ReconException(f"Flat field ({self.mFlatField.shape[1]}, {self.mFlatField.shape[0]}), does not match "
+                                 f"projection ({nu}, {nv})")
+        if self.nDCCount and self.mDark.numel() != nv * nu:
+            raise ReconException(f"Dark field ({self.mDark.shape[1]}, {self.mDark.shape[0]}), does not match "
                                  f"projection ({nu}, {nv})")
         if self.bUseNormROI:
             doses = (_float_vector(coeff["dose"], nproj) if "dose" in coeff else self._frame_doses(img))
@@ -228,7 +239,7 @@ class FullLogNorm:
         elif out.shape != img.shape or out.dtype != torch.float32 or not out.is_contiguous():
             raise ReconException("FullLogNorm: out must be a contiguous float32 tensor of the projections' shape")
         apply = L.lib().mr_lognorm_apply_lut if self.bUseLUT else L.lib().mr_lognorm_apply
-        check(apply(img.data_ptr(), _DT[img.dtype], nv * nu, nproj, self.mDark.data_ptr(), self.mFlatField.data_ptr(),
+        check(apply(img.data_ptr(), _DT[img.dtype], nv * nu, nproj, _ptr(self.mDark), _ptr(self.mFlatField),
                     doselog.data_ptr(), doselog.numel(), int(self.nDCCount > 0), int(self.nOBCount > 0),
                     out.data_ptr(), _stream()))
         return out
@@ -703,6 +714,33 @@ class _BackProjectorBase:
     def GetVolume(self) -> torch.Tensor:
         return self.volume
 
+    def _slice_window(self, nx: int, ny: int):
+        """BackProjectorModuleBase::GetSlice's slice window (BackProjectorModuleBase.cpp:62-84):
+        the whole slice, or with MatrixInfo.bUseROI the inclusive crop roi[0]..roi[2] by
+        roi[1]..roi[3]. The reference copies the crop without checking it against the volume;
+        here a crop outside the slice raises."""
+        mi = self.mConfig.MatrixInfo
+        if not mi.bUseROI:
+            return 0, 0, nx, ny
+        x0, y0, x1, y1 = (int(v) for v in mi.roi)
+        w, h = x1 - x0 + 1, y1 - y0 + 1
+        if x0 < 0 or y0 < 0 or w <= 0 or h <= 0 or x0 + w > nx or y0 + h > ny:
+            raise ReconException(f"Matrix ROI {tuple(mi.roi)} is outside the {nx} x {ny} slice")
+        return x0, y0, w, h
+
+
+def TransferMatrix(backprojector, volume: torch.Tensor, dims, first_slice: int = 0) -> bool:
+    """ReconEngine::TransferMatrix (ReconEngine.cpp:531-574): the block's slices i = 0 ..
+    dims[3] - dims[1] - 1 of the backprojector (GetSlice, with the matrix ROI) are copied into
+    planes dims[1] - first_slice + i of the engine volume (planes, rows, columns). Errors of
+    GetSlice are re-raised with the reference's context."""
+    try:
+        for i in range(int(dims[3]) - int(dims[1])):
+            volume[int(dims[1]) - first_slice + i].copy_(backprojector.GetSlice(i))
+    except ReconException as e:
+        raise ReconException(f"Transfer matrix from backprojector failed with ReconException\n{e}") from e
+    return False
+
 
 class MultiProjectionBPparallel(_BackProjectorBase):
     """MultiProjectionBPparallel (StdBackProjectors/src/MultiProjBPparallel.cpp) with the
@@ -806,10 +844,14 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         return 0
 
     def GetSlice(self, idx: int) -> torch.Tensor:
-        """BackProjectorModuleBase::GetSlice for MatrixZXY: slice[y][x] = volume[y][x][idx]."""
+        """BackProjectorModuleBase::GetSlice for MatrixZXY (BackProjectorModuleBase.cpp:62-128):
+        slice[y][x] = volume[y0 + y][x0 + x][idx] over the slice window (the whole slice, or
+        the matrix ROI's inclusive crop)."""
         if idx >= self.volume.shape[2]:
-            raise ReconException("Slice index greater than matrix size (ZXY matrix)")
-        return self.volume[:, :, idx]
+            raise ReconException(f"Slice index greater than matrix size (ZXY matrix). Slice index is {idx} and "
+                                 f"Matrix Sixe is: {self.volume.shape[2]}")
+        x0, y0, w, h = self._slice_window(self.volume.shape[1], self.volume.shape[0])
+        return self.volume[y0:y0 + h, x0:x0 + w, idx].contiguous()
 
     def GetNSlices(self) -> int:
         return self.volume.shape[2]
@@ -992,9 +1034,13 @@ class FDKbp_single(_BackProjectorBase):
                                                   acc, kb, ke, self.volume.data_ptr(), st))
 
     def GetSlice(self, idx: int) -> torch.Tensor:
+        """BackProjectorModuleBase::GetSlice for MatrixXYZ (BackProjectorModuleBase.cpp:62-128):
+        slice[y][x] = volume[idx][y0 + y][x0 + x] over the slice window."""
         if idx >= self.volume.shape[0]:
-            raise ReconException("Slice index greater than matrix size (XYZ matrix)")
-        return self.volume[idx]
+            raise ReconException(f"Slice index greater than matrix size (XYZ matrix). Slice index is {idx} and "
+                                 f"Matrix Sixe is: {self.volume.shape[0]}")
+        x0, y0, w, h = self._slice_window(self.volume.shape[2], self.volume.shape[1])
+        return self.volume[idx, y0:y0 + h, x0:x0 + w].contiguous()
 
     def GetNSlices(self) -> int:
         return self.volume.shape[0]

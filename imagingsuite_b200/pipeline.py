@@ -56,8 +56,10 @@ class FdkPipeline:
         nproj, nv, nu = counts.shape
         out = self._norm_buf if out is None else out
         dl = torch.zeros(1, device=counts.device)
-        L.check(L.lib().mr_lognorm_apply(counts.data_ptr(), L.MR_U16, nv * nu, nproj, self.norm.mDark.data_ptr(),
-                                         self.norm.mFlatField.data_ptr(), dl.data_ptr(), 1,
+        dark, flat = self.norm.mDark, self.norm.mFlatField
+        L.check(L.lib().mr_lognorm_apply(counts.data_ptr(), L.MR_U16, nv * nu, nproj,
+                                         None if dark is None else dark.data_ptr(),
+                                         None if flat is None else flat.data_ptr(), dl.data_ptr(), 1,
                                          int(self.norm.nDCCount > 0), int(self.norm.nOBCount > 0),
                                          out.data_ptr(), torch.cuda.current_stream().cuda_stream))
         return out

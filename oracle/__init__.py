@@ -300,6 +300,19 @@ def fdk(proj, angles, weights, geom: FdkGeom, use_ref=False) -> np.ndarray:
     return vol
 
 
+def ref_getslice(vol, zxy: bool, idx: int, roi=None) -> np.ndarray:
+    """The reference BackProjectorModuleBase::GetSlice on `vol` (numpy, C order: (ny, nx, nz)
+    for MatrixZXY, (nz, ny, nx) for MatrixXYZ); roi = MatrixInfo.roi with bUseROI, or None."""
+    vol = _f32(vol)
+    d2, d1, d0 = vol.shape
+    out = np.empty(vol.size, np.float32)
+    dims = np.zeros(2, np.uintp)
+    r = np.asarray(roi if roi is not None else (0, 0, 0, 0), dtype=np.uintp)
+    _check_ref(ref().ref_getslice(_p(vol), _sz(d0), _sz(d1), _sz(d2), int(zxy), int(roi is not None), _p(r, _SZ),
+                                  _sz(idx), _p(out), _p(dims, _SZ)))
+    return out[: int(dims[0]) * int(dims[1])].reshape(int(dims[1]), int(dims[0]))
+
+
 class RefFdkSession:
     """The reference FDKbp_single configured once (Configure + SetROI for the full detector)
     and then given projections by repeated Process 3D calls, each adding into the same volume

@@ -371,6 +371,31 @@ static ReconConfig fdk_config(size_t nu, size_t nv, size_t nproj, const ref_fdk_
 }
 } // extern "C++"
 
+// BackProjectorModuleBase::GetSlice (BackProjectorModuleBase.cpp:62-128) of a volume given
+// with its kipl dims (d0 fastest): zxy = 1 on a MultiProjectionBPparallel (MatrixZXY), 0 on an
+// FDKbp_single (MatrixXYZ); use_roi/roi set MatrixInfo.bUseROI and MatrixInfo.roi. out gets the
+// slice, out_dims its two sizes.
+int ref_getslice(const float *vol, size_t d0, size_t d1, size_t d2, int zxy, int use_roi, const size_t *roi,
+                 size_t idx, float *out, size_t *out_dims)
+{
+    return guarded([&] {
+        std::unique_ptr<BackProjectorModuleBase> bp;
+        if (zxy)
+            bp.reset(new MultiProjectionBPparallel(nullptr));
+        else
+            bp.reset(new FDKbp_single(nullptr));
+        size_t d3[3] = {d0, d1, d2};
+        bp->volume.Resize(d3);
+        std::memcpy(bp->volume.GetDataPtr(), vol, sizeof(float) * d0 * d1 * d2);
+        bp->mConfig.MatrixInfo.bUseROI = use_roi != 0;
+        if (use_roi) std::memcpy(bp->mConfig.MatrixInfo.roi, roi, 4 * sizeof(size_t));
+        kipl::base::TImage<float, 2> s = bp->GetSlice(idx);
+        out_dims[0] = s.Size(0);
+        out_dims[1] = s.Size(1);
+        std::memcpy(out, s.GetDataPtr(), sizeof(float) * s.Size());
+    });
+}
+
 // A configured FDKbp_single that keeps its volume between Process calls, as ReconEngine
 // keeps one backprojector per slice block and hands it projections (Configure and SetROI
 // once, then Process 3D; each Process adds into cbct_volume and redoes the final mirror).

@@ -82,6 +82,41 @@ def test_fulllognorm_module(cuda, usenorm, method):
     assert np.array_equal(out == 0, exp == 0)  # the (I - D <= 0) mask is exact
 
 
+@pytest.mark.parametrize("ndark,nflat", [(5, 0), (0, 5), (0, 0)])
+@pytest.mark.parametrize("usenorm", [False, True])
+@pytest.mark.parametrize("uselut", [False, True])
+def test_fulllognorm_module_missing_references(cuda, ndark, nflat, usenorm, uselut):
+    """FullLogNorm without flat fields (-log(I - D) + dose, NormPlugins.cpp:498-540 and the LUT
+    path's dose shift), without darks (I alone), or with neither, through the module, against
+    the oracle (pinned to the compiled module on these branches)."""
+    proj, flats, darks = _counts(3, 11, 20, 36)
+    darks, flats = darks[:ndark], flats[:nflat]
+    roi = (3, 2, 30, 17)
+    cfg = M.ReconConfig()
+    cfg.ProjectionInfo.dose_roi = roi
+    cfg.ProjectionInfo.nOBCount, cfg.ProjectionInfo.nDCCount = nflat, ndark
+    mod = M.FullLogNorm()
+    mod.Configure(cfg, {"usenormregion": str(usenorm).lower(), "uselut": str(uselut).lower(),
+                        "referenceaverage": "ImageAverage"})
+    mod.SetReferenceImages(dev(darks.reshape(ndark, 20, 36), cuda), dev(flats.reshape(nflat, 20, 36), cuda))
+    out = mod.Process(dev(proj, cuda), {}).cpu().numpy()
+    refs = O.lognorm_refs(darks.reshape(ndark, 20, 36).astype(np.float32),
+                          flats.reshape(nflat, 20, 36).astype(np.float32), "ImageAverage", usenorm, roi)
+    if usenorm:
+        doses = np.array([O.frame_dose(proj[i].astype(np.float32), roi) for i in range(proj.shape[0])], np.float32)
+        dl = O.lognorm_doselog(doses, refs.darkdose)
+    else:
+        dl = np.zeros(1, np.float32)
+    exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, dl, ndc=ndark > 0, nob=nflat > 0,
+                          uselut=uselut)
+    if uselut:
+        assert np.array_equal(out, exp)  # the table is built with the reference's double log
+    else:
+        tol = 2 * np.spacing(np.float32(np.abs(refs.logflat).max() + np.abs(dl).max() + np.log(65536.0)))
+        assert np.abs(out.astype(np.float64) - exp).max() <= tol
+        assert np.array_equal(out == 0, exp == 0)
+
+
 def test_lognorm_f32_inplace_and_unaligned(cuda):
     proj, flats, darks = _counts(2, 3, 7, 13)  # npix = 91: scalar path
     refs = O.lognorm_refs(darks.astype(np.float32), flats.astype(np.float32))
