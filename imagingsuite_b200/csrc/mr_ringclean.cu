@@ -334,6 +334,10 @@ static mr_status wavelet_taps(const char *wname, int *begin, int *end, std::vect
     if (name.compare(0, 4, "daub") != 0) return fail(MR_ERR_UNSUPPORTED, "unsupported wavelet '%s' (daub1..daub30)", name.c_str());
     const int n = std::atoi(name.c_str() + 4);
     if (n < 1 || n > kDaubMax) return fail(MR_ERR_UNSUPPORTED, "Daubechies are only supported for N<=30");
+    // kipl's daub28 table has 48 entries for its 56 taps (wavelets.hpp, WaveletKernel case 28):
+    // the reference kernel copies 8 values from past the array, so its result is undefined
+    if (n == 28)
+        return fail(MR_ERR_UNSUPPORTED, "daub28 is not supported: the reference's table is shorter than the filter");
     const int K = 2 * n, e = K - 1;
     std::vector<double> k(kDaub[n - 1], kDaub[n - 1] + K);
     if (n == 3) k[4] = -k[4];

@@ -120,9 +120,11 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
  * mr_waveletringclean replaces WaveletRingClean::ProcessCore (frameworks/tomography/
  * Preprocessing/StdPreprocModules/src/WaveletRingClean.cpp:63-103): every detector row's
  * sinogram of projections [nproj][nv][nu], in place.
- * wname: "daub1".."daub30" (Daubechies filters computed from their definition; daub3 keeps the
- * reference's sign of its fifth coefficient); decnum: decomposition levels; sigma: damping
- * width. Scratch: up to about 1 GiB per call.
+ * wname: "daub1".."daub30" except daub28 (daub1..15 computed from their definition, equal to
+ * kipl's float kernels, daub3 with the reference's sign of its fifth coefficient; daub16..30
+ * kipl's own table values; kipl's daub28 table is shorter than its filter, so the reference's
+ * daub28 kernel is undefined and it returns MR_ERR_UNSUPPORTED); decnum: decomposition levels;
+ * sigma: damping width. Scratch: up to about 1 GiB per call.
  * mr_wavelet_kernel (host) returns begin/end and the four filters (analysis H, analysis G,
  * synthesis H, synthesis G; 4*(end-begin+1) floats) of WaveletKernel<float>. */
 mr_status mr_wavelet_kernel(const char *wname, int *begin, int *end, float *taps_h);

@@ -483,8 +483,8 @@ _DAUB = None
 
 
 def daubechies(n: int) -> np.ndarray:
-    """dbN scaling filter (float64) from the table generated from the spectral factorisation
-    (imagingsuite_b200/csrc/gen_daubechies.py)."""
+    """dbN scaling filter (float64) from the table of imagingsuite_b200/csrc/gen_daubechies.py
+    (N <= 15 from the spectral factorisation, N >= 16 kipl's table values as float)."""
     global _DAUB
     if _DAUB is None:
         import re
@@ -502,6 +502,8 @@ def wavelet_kernel(name: str):
     if not name.startswith("daub"):
         raise ValueError(f"unsupported wavelet {name}")
     n = int(name[4:])
+    if n == 28:
+        raise ValueError("daub28: the reference's table is shorter than the filter (undefined kernel)")
     k = daubechies(n).copy()
     if n == 3:
         k[4] = -k[4]

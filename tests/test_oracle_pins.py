@@ -275,11 +275,12 @@ def test_morphspotclean_module_defaults(ref_lib):
     assert np.array_equal(a, b)
 
 
-@pytest.mark.parametrize("n", list(range(1, 16)))
+@pytest.mark.parametrize("n", [n for n in range(1, 31) if n != 28])
 def test_wavelet_kernels_match_reference(ref_lib, n):
-    """dbN from the spectral factorisation equals the reference's float kernels for N <= 15
-    (daub3 with the reference's sign of h[4]); the reference's daub16..30 tables are less
-    accurate than float and are not reproduced."""
+    """The dbN table equals the reference's float kernels: N <= 15 from the spectral
+    factorisation (daub3 with the reference's sign of h[4]), N >= 16 kipl's own table values
+    (less accurate than float, and the results follow them). daub28 is refused: its reference
+    table is shorter than the filter."""
     import ctypes
 
     b, e, k = O.wavelet_kernel(f"daub{n}")
@@ -294,8 +295,21 @@ def test_wavelet_kernels_match_reference(ref_lib, n):
         assert np.array_equal(ours, theirs[:K])
 
 
+def test_daub28_refused():
+    import ctypes
+
+    from imagingsuite_b200 import _lib as L
+
+    taps = np.zeros(4 * 56, np.float32)
+    b, e = ctypes.c_int(), ctypes.c_int()
+    assert L.lib().mr_wavelet_kernel(b"daub28", ctypes.byref(b), ctypes.byref(e), O._p(taps)) == L.MR_ERR_UNSUPPORTED
+    with pytest.raises(ValueError):
+        O.wavelet_kernel("daub28")
+
+
 @pytest.mark.parametrize("name,levels,sigma", [("daub2", 1, 0.05), ("daub3", 3, 0.02), ("daub7", 2, 0.1),
-                                               ("daub15", 2, 0.05), ("daub5", 3, 0.2)])
+                                               ("daub15", 2, 0.05), ("daub5", 3, 0.2), ("daub20", 2, 0.05),
+                                               ("daub30", 2, 0.1)])
 def test_stripefilter_bit_exact(ref_lib, name, levels, sigma):
     rng = _rng(90)
     for _ in range(3):
