@@ -146,7 +146,7 @@ def test_fdk_partials_tilt_not_uniform():
     assert uni == 0
 
 
-@pytest.mark.parametrize("n", list(range(1, 31)))
+@pytest.mark.parametrize("n", [n for n in range(1, 31) if n != 28])
 def test_wavelet_kernel_abi(n):
     b, e = ctypes.c_int(), ctypes.c_int()
     taps = np.zeros(4 * 60, np.float32)
@@ -162,6 +162,7 @@ def test_wavelet_kernel_rejects_unknown():
     b, e = ctypes.c_int(), ctypes.c_int()
     assert L.lib().mr_wavelet_kernel(b"haar", ctypes.byref(b), ctypes.byref(e), None) == L.MR_ERR_UNSUPPORTED
     assert L.lib().mr_wavelet_kernel(b"daub31", ctypes.byref(b), ctypes.byref(e), None) == L.MR_ERR_UNSUPPORTED
+    assert L.lib().mr_wavelet_kernel(b"daub28", ctypes.byref(b), ctypes.byref(e), None) == L.MR_ERR_UNSUPPORTED
 
 
 @pytest.mark.parametrize("tilt", [0.0, 0.4])
