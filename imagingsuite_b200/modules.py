@@ -273,7 +273,8 @@ class MorphSpotCleanModule:
     the reference's single-threaded path (ProcessSingle :142-181) the cleaner runs with its
     own edge smoothing length (9; the `edgesmooth` parameter is read but not applied) and
     without inf/NaN removal (`removeinfnan` is read but not applied); clamping follows
-    `clampdata`."""
+    `clampdata` on that path and is off with `threading` (ProcessParallelStd never sets the
+    cleaner's limits)."""
 
     def __init__(self):
         self.m_eConnectivity = "conn4"
@@ -327,8 +328,11 @@ class MorphSpotCleanModule:
     def ProcessCore(self, img: torch.Tensor, coeff: dict) -> torch.Tensor:
         if self.m_eCleanMethod != "morphcleanreplace":
             raise ReconException("MorphSpotClean: only morphcleanreplace is supported by this module")
+        # threading=true takes the reference's ProcessParallelStd (MorphSpotCleanModule.cpp:
+        # 226-269), whose cleaners never get setLimits: no clamping there
+        clamp = self.m_bClampData and not self.m_bThreading
         return morph_spot_clean(img, _DETECT[self.m_eDetectionMethod], self.m_eConnectivity == "conn8",
-                                self.m_fThreshold[:2], self.m_fSigma[:2], edge=9, clamp=self.m_bClampData,
+                                self.m_fThreshold[:2], self.m_fSigma[:2], edge=9, clamp=clamp,
                                 minlevel=self.m_fMinLevel, maxlevel=self.m_fMaxLevel, removeinfnan=False)
 
 

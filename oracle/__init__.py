@@ -313,6 +313,94 @@ def ref_getslice(vol, zxy: bool, idx: int, roi=None) -> np.ndarray:
     return out[: int(dims[0]) * int(dims[1])].reshape(int(dims[1]), int(dims[0]))
 
 
+# ------------------------------------------------------ module libraries (plugin loading)
+
+
+def _lines(d: dict | None) -> bytes:
+    return "".join(f"{k}={v}\n" for k, v in (d or {}).items()).encode()
+
+
+def _parse_module_lines(text: str) -> dict:
+    out: dict = {}
+    for ln in text.splitlines():
+        if "|" in ln:
+            mod, kv = ln.split("|", 1)
+            k, v = kv.split("=", 1)
+            out.setdefault(mod, {})[k] = v
+    return out
+
+
+def ref_plugin_module_list(sofile: str, application: str) -> tuple[int, dict]:
+    """GetModuleList of a module library, called as ReconEngine's module configuration does."""
+    buf = ctypes.create_string_buffer(1 << 16)
+    _check_ref(ref().ref_plugin_module_list(sofile.encode(), application.encode(), buf, _sz(len(buf))))
+    text = buf.value.decode()
+    return int(text.splitlines()[0].split("=")[1]), _parse_module_lines(text)
+
+
+def ref_plugin_has_module(sofile: str, application: str, name: str) -> bool:
+    found = ctypes.c_int(-1)
+    _check_ref(ref().ref_plugin_has_module(sofile.encode(), application.encode(), name.encode(), ctypes.byref(found)))
+    return bool(found.value)
+
+
+def ref_module_parameters(name: str, backprojector: bool = False) -> dict:
+    """GetParameters of the reference's own module of that name (its defaults)."""
+    buf = ctypes.create_string_buffer(1 << 14)
+    _check_ref(ref().ref_module_parameters(name.encode(), int(backprojector), buf, _sz(len(buf))))
+    return _parse_module_lines(buf.value.decode()).get(name, {})
+
+
+def ref_write_mat(img, fname: str) -> None:
+    img = _f32(img)
+    _check_ref(ref().ref_write_mat(_p(img), _sz(img.shape[1]), _sz(img.shape[0]), fname.encode()))
+
+
+def ref_preproc_module(proj, name: str, params: dict, sofile: str | None = None, coeff: dict | None = None,
+                       refpath: str = "", obmask: str = "", nob: int = 0, obfirst: int = 1, dcmask: str = "",
+                       ndc: int = 0, dcfirst: int = 1, dose_roi=None, roi=None) -> np.ndarray:
+    """Configure (+ SetROI when roi is given) + Process 3D of a preprocessing module on a copy of
+    proj: the reference's own module (sofile None) or module `name` of the library `sofile`
+    loaded through the reference's ModuleItem."""
+    out = np.array(proj, dtype=np.float32, copy=True, order="C")
+    nproj, nv, nu = out.shape
+    dr = None if dose_roi is None else np.asarray(dose_roi, np.uintp)
+    r = None if roi is None else np.asarray(roi, np.uintp)
+    _check_ref(ref().ref_preproc_module(sofile.encode() if sofile else None, name.encode(), _lines(params),
+                                        _lines(coeff), refpath.encode(), obmask.encode(), _sz(nob), _sz(obfirst),
+                                        dcmask.encode(), _sz(ndc), _sz(dcfirst),
+                                        None if dr is None else _p(dr, _SZ), None if r is None else _p(r, _SZ),
+                                        _p(out), _sz(nu), _sz(nv), _sz(nproj)))
+    return out
+
+
+class RefBpConfig(ctypes.Structure):
+    _fields_ = [("center", ctypes.c_float), ("direction", ctypes.c_int), ("correcttilt", ctypes.c_int),
+                ("tiltangle", ctypes.c_float), ("tiltpivot", ctypes.c_float), ("cone", ctypes.c_int),
+                ("sod", ctypes.c_float), ("sdd", ctypes.c_float), ("ppoint", ctypes.c_float * 2),
+                ("resolution", ctypes.c_float * 2), ("voxelsize", ctypes.c_float * 3),
+                ("use_matrix_roi", ctypes.c_int), ("matrix_roi", ctypes.c_size_t * 4)]
+
+
+def ref_bp_module(proj, angles, weights, name: str, cfg: RefBpConfig, roi, params: dict,
+                  sofile: str | None = None):
+    """Configure + SetROI + Process 3D of a backprojector (the reference's own, or `name` of the
+    library `sofile` through BackProjItem); returns (volume in kipl order as a numpy array of
+    the module's matrix alignment, GetSlice of every slice as (nslices, h, w))."""
+    proj = _f32(proj)
+    nproj, nv, nu = proj.shape
+    a, w = _f32(angles), _f32(weights)
+    vol = np.empty(nu * nu * nv, np.float32)
+    slices = np.empty(nu * nu * nv, np.float32)
+    dims = np.zeros(3, np.uintp)
+    r = np.asarray(roi, np.uintp)
+    _check_ref(ref().ref_bp_module(sofile.encode() if sofile else None, name.encode(), _lines(params),
+                                   ctypes.byref(cfg), _p(r, _SZ), _p(proj), _sz(nproj), _p(a), _p(w), _p(vol),
+                                   _p(slices), _p(dims, _SZ)))
+    sw, sh, ns = (int(d) for d in dims)
+    return vol, slices[: ns * sw * sh].reshape(ns, sh, sw)
+
+
 class RefFdkSession:
     """The reference FDKbp_single configured once (Configure + SetROI for the full detector)
     and then given projections by repeated Process 3D calls, each adding into the same volume

@@ -62,8 +62,11 @@
 #include "fdkbp.h"
 #include "linearforwardprojector.h"
 #include <wavelets/wavelets.h>
+#include <ModuleItem.h>
+#include <io/io_matlab.h>
 #undef private
 #undef protected
+#include <dlfcn.h>
 #include <tiffio.h>
 
 namespace {
@@ -814,6 +817,268 @@ void ref_stream_float(float v, char *out, size_t len)
     std::ostringstream s;
     s << v;
     std::snprintf(out, len, "%s", s.str().c_str());
+}
+
+// ---------------------------------------------------------------------------------------
+// Module libraries loaded the way ReconEngine loads them: ModuleItem / BackProjItem
+// (frameworks/tomography/Framework/ReconFramework/src/ModuleItem.cpp, ModuleItemBase.cpp:
+// 97-131) open the library with dlopen and take GetModule / Destroy with dlsym; the module
+// then gets Configure, SetROI and Process from the reference's own framework code. A module
+// library resolves the framework's symbols from the process, so this library's symbols are
+// made global first (it was opened RTLD_LOCAL by the caller).
+
+static void make_self_global()
+{
+    static bool done = false;
+    if (done) return;
+    Dl_info info;
+    if (dladdr(reinterpret_cast<void *>(&make_self_global), &info) && info.dli_fname)
+        dlopen(info.dli_fname, RTLD_NOW | RTLD_NOLOAD | RTLD_GLOBAL);
+    done = true;
+}
+
+static std::map<std::string, std::string> parse_params(const char *text)
+{
+    std::map<std::string, std::string> m;
+    std::istringstream s(text ? text : "");
+    std::string line;
+    while (std::getline(s, line)) {
+        const size_t eq = line.find('=');
+        if (eq != std::string::npos) m[line.substr(0, eq)] = line.substr(eq + 1);
+    }
+    return m;
+}
+
+static std::string params_text(const std::map<std::string, std::string> &m)
+{
+    std::string t;
+    for (const auto &kv : m) t += kv.first + "=" + kv.second + "\n";
+    return t;
+}
+
+// The reference's own preprocessing module of that name (the module library's factory is not
+// part of this build, so the classes are constructed here).
+static PreprocModuleBase *reference_preproc(const std::string &name)
+{
+    if (name == "FullLogNorm") return new FullLogNorm;
+    if (name == "MorphSpotClean") return new MorphSpotCleanModule(nullptr);
+    if (name == "WaveletRingClean") return new WaveletRingClean(nullptr);
+    if (name == "ProjectionFilterSingle") return new ProjectionFilterSingle(nullptr);
+    throw std::runtime_error("no reference module " + name);
+}
+
+static BackProjectorModuleBase *reference_bp(const std::string &name)
+{
+    if (name == "MultiProjBPparallel") return new MultiProjectionBPparallel(nullptr);
+    if (name == "MultiProjBP") return new MultiProjectionBP(nullptr);
+    if (name == "NearestNeighborBP") return new NearestNeighborBP(nullptr);
+    if (name == "FDKbp_single") return new FDKbp_single(nullptr);
+    throw std::runtime_error("no reference backprojector " + name);
+}
+
+// GetModuleList of a module library (application tag `app`) as "module|key=value" lines.
+int ref_plugin_module_list(const char *sofile, const char *app, char *out, size_t len)
+{
+    return guarded([&] {
+        make_self_global();
+        void *h = dlopen(sofile, RTLD_NOW);
+        if (!h) throw std::runtime_error(std::string("dlopen: ") + dlerror());
+        typedef int (*list_fn)(const char *, void *);
+        list_fn f = reinterpret_cast<list_fn>(dlsym(h, "GetModuleList"));
+        if (!f) throw std::runtime_error("GetModuleList not exported");
+        std::map<std::string, std::map<std::string, std::string>> modules;
+        const int rc = f(app, &modules);
+        std::string t = "rc=" + std::to_string(rc) + "\n";
+        for (const auto &m : modules)
+            for (const auto &kv : m.second) t += m.first + "|" + kv.first + "=" + kv.second + "\n";
+        std::snprintf(out, len, "%s", t.c_str());
+    });
+}
+
+// GetModule of a module library for (app, name): 1 when it returns a module (destroyed again
+// through the library's Destroy), 0 for nullptr.
+int ref_plugin_has_module(const char *sofile, const char *app, const char *name, int *found)
+{
+    return guarded([&] {
+        make_self_global();
+        void *h = dlopen(sofile, RTLD_NOW);
+        if (!h) throw std::runtime_error(std::string("dlopen: ") + dlerror());
+        typedef void *(*get_fn)(const char *, const char *, void *);
+        typedef int (*destroy_fn)(const char *, void *);
+        get_fn g = reinterpret_cast<get_fn>(dlsym(h, "GetModule"));
+        destroy_fn d = reinterpret_cast<destroy_fn>(dlsym(h, "Destroy"));
+        if (!g || !d) throw std::runtime_error("GetModule / Destroy not exported");
+        void *m = g(app, name, nullptr);
+        *found = m != nullptr;
+        if (m && d(app, m) != 0) throw std::runtime_error("Destroy failed");
+    });
+}
+
+// GetParameters of the reference's own module of that name ("module|key=value" lines).
+int ref_module_parameters(const char *name, int backprojector, char *out, size_t len)
+{
+    return guarded([&] {
+        std::map<std::string, std::string> p;
+        if (backprojector) {
+            std::unique_ptr<BackProjectorModuleBase> m(reference_bp(name));
+            p = m->GetParameters();
+        } else {
+            std::unique_ptr<PreprocModuleBase> m(reference_preproc(name));
+            p = m->GetParameters();
+        }
+        std::string t;
+        for (const auto &kv : p) t += std::string(name) + "|" + kv.first + "=" + kv.second + "\n";
+        std::snprintf(out, len, "%s", t.c_str());
+    });
+}
+
+// Writes an image [nv][nu] as a MATLAB file through kipl (the format ProjectionReader reads
+// without the image libraries this build lacks).
+int ref_write_mat(const float *img, size_t nu, size_t nv, const char *fname)
+{
+    return guarded([&] {
+        size_t d2[2] = {nu, nv};
+        kipl::base::TImage<float, 2> im(d2);
+        std::memcpy(im.GetDataPtr(), img, sizeof(float) * nu * nv);
+        kipl::io::WriteMAT(im, fname, "img");
+    });
+}
+
+// Configure (+ SetROI when roi is given) + Process 3D of a preprocessing module on proj [nproj][nv][nu]
+// in place: the reference's own module (sofile NULL) or module `name` of library `sofile`
+// through ModuleItem. params/coeff: "key=value" lines. The ReconConfig fields FullLogNorm reads
+// for its reference images: reference path, open beam / dark masks, counts, first indices,
+// dose ROI.
+int ref_preproc_module(const char *sofile, const char *name, const char *params, const char *coeff,
+                       const char *refpath, const char *obmask, size_t nob, size_t obfirst, const char *dcmask,
+                       size_t ndc, size_t dcfirst, const size_t *dose_roi, const size_t *roi, float *proj, size_t nu,
+                       size_t nv, size_t nproj)
+{
+    return guarded([&] {
+        make_self_global();
+        ReconConfig cfg;
+        cfg.ProjectionInfo.sReferencePath = refpath ? refpath : "";
+        cfg.ProjectionInfo.sOBFileMask = obmask ? obmask : "";
+        cfg.ProjectionInfo.nOBCount = nob;
+        cfg.ProjectionInfo.nOBFirstIndex = obfirst;
+        cfg.ProjectionInfo.sDCFileMask = dcmask ? dcmask : "";
+        cfg.ProjectionInfo.nDCCount = ndc;
+        cfg.ProjectionInfo.nDCFirstIndex = dcfirst;
+        cfg.ProjectionInfo.imagetype = ReconConfig::cProjections::ImageType_Projections;
+        cfg.ProjectionInfo.nDims[0] = nu;
+        cfg.ProjectionInfo.nDims[1] = nv;
+        size_t full[4] = {0, 0, nu, nv};
+        std::memcpy(cfg.ProjectionInfo.dose_roi, dose_roi ? dose_roi : full, 4 * sizeof(size_t));
+        std::memcpy(cfg.ProjectionInfo.roi, roi ? roi : full, 4 * sizeof(size_t));
+        std::memcpy(cfg.ProjectionInfo.projection_roi, roi ? roi : full, 4 * sizeof(size_t));
+        std::unique_ptr<ModuleItem> item;
+        std::unique_ptr<PreprocModuleBase> own;
+        PreprocModuleBase *m = nullptr;
+        if (sofile && *sofile) {
+            item.reset(new ModuleItem("muhrec", sofile, name));
+            m = item->GetModule();
+        } else {
+            own.reset(reference_preproc(name));
+            m = own.get();
+        }
+        if (m->Configure(cfg, parse_params(params)) != 0) throw std::runtime_error("Configure failed");
+        if (roi) {
+            size_t r[4] = {roi[0], roi[1], roi[2], roi[3]};
+            m->SetROI(r);
+        }
+        size_t d3[3] = {nu, nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+        std::map<std::string, std::string> c = parse_params(coeff);
+        m->Process(img, c);
+        std::memcpy(proj, img.GetDataPtr(), sizeof(float) * nu * nv * nproj);
+    });
+}
+
+struct ref_bp_cfg {
+    float center;
+    int direction;
+    int correcttilt;
+    float tiltangle, tiltpivot;
+    int cone;
+    float sod, sdd, ppoint[2], resolution[2], voxelsize[3];
+    int use_matrix_roi;
+    size_t matrix_roi[4];
+};
+
+// Configure + SetROI(roi) + Process 3D of a backprojector (the reference's own, sofile NULL, or
+// module `name` of library `sofile` through BackProjItem), then the framework's GetVolume
+// (vol: the module's volume in kipl order) and GetSlice of every slice (slices: nslices
+// slices of w x h, the sizes written to slice_dims). proj [nproj][nv][nu], roi (x0, y0, x1, y1).
+int ref_bp_module(const char *sofile, const char *name, const char *params, const ref_bp_cfg *c, const size_t *roi,
+                  const float *proj, size_t nproj, const float *angles, const float *weights, float *vol,
+                  float *slices, size_t *slice_dims)
+{
+    return guarded([&] {
+        make_self_global();
+        const size_t nu = roi[2] - roi[0], nv = roi[3] - roi[1];
+        ReconConfig cfg;
+        cfg.ProjectionInfo.fCenter = c->center;
+        cfg.ProjectionInfo.eDirection = static_cast<kipl::base::eRotationDirection>(c->direction);
+        cfg.ProjectionInfo.bCorrectTilt = c->correcttilt != 0;
+        cfg.ProjectionInfo.fTiltAngle = c->tiltangle;
+        cfg.ProjectionInfo.fTiltPivotPosition = c->tiltpivot;
+        cfg.ProjectionInfo.imagetype = ReconConfig::cProjections::ImageType_Projections;
+        cfg.ProjectionInfo.beamgeometry = c->cone ? ReconConfig::cProjections::BeamGeometry_Cone
+                                                  : ReconConfig::cProjections::BeamGeometry_Parallel;
+        cfg.ProjectionInfo.nDims[0] = nu;
+        cfg.ProjectionInfo.nDims[1] = nv;
+        cfg.ProjectionInfo.fSOD = c->sod;
+        cfg.ProjectionInfo.fSDD = c->sdd;
+        cfg.ProjectionInfo.fpPoint[0] = c->ppoint[0];
+        cfg.ProjectionInfo.fpPoint[1] = c->ppoint[1];
+        cfg.ProjectionInfo.fResolution[0] = c->resolution[0];
+        cfg.ProjectionInfo.fResolution[1] = c->resolution[1];
+        cfg.ProjectionInfo.nFirstIndex = 0;
+        cfg.ProjectionInfo.nLastIndex = nproj - 1;
+        cfg.ProjectionInfo.nProjectionStep = 1;
+        std::memcpy(cfg.ProjectionInfo.roi, roi, 4 * sizeof(size_t));
+        std::memcpy(cfg.ProjectionInfo.projection_roi, roi, 4 * sizeof(size_t));
+        cfg.MatrixInfo.fVoxelSize[0] = c->voxelsize[0];
+        cfg.MatrixInfo.fVoxelSize[1] = c->voxelsize[1];
+        cfg.MatrixInfo.fVoxelSize[2] = c->voxelsize[2];
+        cfg.MatrixInfo.nDims[0] = nu;
+        cfg.MatrixInfo.nDims[1] = nu;
+        cfg.MatrixInfo.nDims[2] = nv;
+        cfg.MatrixInfo.bUseROI = c->use_matrix_roi != 0;
+        std::memcpy(cfg.MatrixInfo.roi, c->matrix_roi, 4 * sizeof(size_t));
+        std::unique_ptr<BackProjItem> item;
+        std::unique_ptr<BackProjectorModuleBase> own;
+        BackProjectorModuleBase *m = nullptr;
+        if (sofile && *sofile) {
+            item.reset(new BackProjItem("muhrecbp", sofile, name));
+            m = item->GetModule();
+        } else {
+            own.reset(reference_bp(name));
+            m = own.get();
+        }
+        m->Configure(cfg, parse_params(params));
+        size_t r[4] = {roi[0], roi[1], roi[2], roi[3]};
+        m->SetROI(r);
+        size_t d3[3] = {nu, nv, nproj};
+        kipl::base::TImage<float, 3> img(d3);
+        std::memcpy(img.GetDataPtr(), proj, sizeof(float) * nu * nv * nproj);
+        std::map<std::string, std::string> p;
+        p["angles"] = list_text(angles, nproj);
+        p["weights"] = list_text(weights, nproj);
+        m->Process(img, p);
+        kipl::base::TImage<float, 3> v = m->GetVolume();
+        std::memcpy(vol, v.GetDataPtr(), sizeof(float) * v.Size());
+        const size_t ns = m->GetNSlices();
+        for (size_t i = 0; i < ns; ++i) {
+            kipl::base::TImage<float, 2> s = m->GetSlice(i);
+            slice_dims[0] = s.Size(0);
+            slice_dims[1] = s.Size(1);
+            std::memcpy(slices + i * s.Size(), s.GetDataPtr(), sizeof(float) * s.Size());
+        }
+        slice_dims[2] = ns;
+        if (FDKbp_single *f = dynamic_cast<FDKbp_single *>(m)) delete[] f->proj_matrices;
+    });
 }
 
 // libtiff writers for the debug images BasicRingClean saves to the working directory

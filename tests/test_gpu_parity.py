@@ -109,12 +109,14 @@ def test_fulllognorm_module_missing_references(cuda, ndark, nflat, usenorm, usel
         dl = np.zeros(1, np.float32)
     exp = O.lognorm_apply(proj.astype(np.float32), refs.dark, refs.logflat, dl, ndc=ndark > 0, nob=nflat > 0,
                           uselut=uselut)
-    if uselut:
+    if uselut and nflat == 0:
         assert np.array_equal(out, exp)  # the table is built with the reference's double log
     else:
+        # log(flat) (and, on the exact path, log(I - D)) through CUDA's logf: within 1 ulp of glibc's
         tol = 2 * np.spacing(np.float32(np.abs(refs.logflat).max() + np.abs(dl).max() + np.log(65536.0)))
         assert np.abs(out.astype(np.float64) - exp).max() <= tol
-        assert np.array_equal(out == 0, exp == 0)
+        if not uselut:
+            assert np.array_equal(out == 0, exp == 0)
 
 
 def test_lognorm_f32_inplace_and_unaligned(cuda):
