@@ -733,6 +733,24 @@ class _BackProjectorBase:
         return x0, y0, w, h
 
 
+def _restrict_mask(mask: np.ndarray, nx: int, mi: MatrixInfo, cone: bool) -> None:
+    """The matrix-ROI part of BackProjectorModuleBase::BuildCircleMask
+    (BackProjectorModuleBase.cpp:196-214), in place on the (first, second) pairs per row: rows
+    inside roi[1]..roi[3] keep x in [roi[0], roi[2]] (parallel beam) or, mirrored,
+    [nx - roi[2], nx - roi[0]] (cone beam); rows outside get an empty range."""
+    if not mi.bUseROI:
+        return
+    r0, r1, r2, r3 = (int(v) for v in mi.roi)
+    m = mask.reshape(-1, 2)
+    for i in range(m.shape[0]):
+        if r1 <= i <= r3:
+            lo, hi = (r0, r2) if not cone else (nx - r2, nx - r0)
+            m[i, 0] = max(int(m[i, 0]), lo)
+            m[i, 1] = min(int(m[i, 1]), hi)
+        else:
+            m[i] = 0
+
+
 def TransferMatrix(backprojector, volume: torch.Tensor, dims, first_slice: int = 0) -> bool:
     """ReconEngine::TransferMatrix (ReconEngine.cpp:531-574): the block's slices i = 0 ..
     dims[3] - dims[1] - 1 of the backprojector (GetSlice, with the matrix ROI) are copied into
@@ -773,6 +791,7 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         nslices = int(pi.nDims[1]) if pi.nDims[1] else self.SizeV
         check(L.lib().mr_bp_circle_mask(self.SizeU, self.SizeU, int(pi.bCorrectTilt), float(pi.fTiltAngle), nslices,
                                         mask.ctypes.data_as(L.P_u32)))
+        _restrict_mask(mask, self.SizeU, self.mConfig.MatrixInfo, cone=False)
         self.mask_host = mask
         self._mask = torch.from_numpy(mask.view(np.int32)).to(dev)
 
@@ -913,6 +932,7 @@ class FDKbp_single(_BackProjectorBase):
         nslices = int(pi.nDims[1]) if pi.nDims[1] else self.SizeV
         check(L.lib().mr_bp_circle_mask(self.SizeU, self.SizeU, int(pi.bCorrectTilt), float(pi.fTiltAngle), nslices,
                                         mask.ctypes.data_as(L.P_u32)))
+        _restrict_mask(mask, self.SizeU, self.mConfig.MatrixInfo, cone=True)
         self._mask = torch.from_numpy(mask.view(np.int32)).to(dev)
         self._first = True
         self._geo_key = None
