@@ -20,6 +20,7 @@ host threads, on rank 0 only.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import math
 import os
@@ -291,8 +292,22 @@ def run_mr(args):
             pass
         hbm = float(peaks.get("hbm_gbs", 6650.0))
         peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-        bp_bytes = 4.0 * updates  # gathered FP32 samples, 4 B per voxel x projection update
-        ach = bp_bytes / tbp / 1e9
+        # HBM: the compulsory bytes of one backprojection launch, the filtered projections read
+        # once and the volume written once (4 B each)
+        hbm_bytes = 4.0 * nproj * nu * nv + 4.0 * nu * nu * nv
+        ach = hbm_bytes / tbp / 1e9
+        # on chip: one 32-bit gather per voxel x projection update from the TMA-staged box, one
+        # shared-memory wavefront per warp-update (32 updates) when conflict-free, against the
+        # measured shared-memory wavefront rate of this GPU (mr_measure_smem)
+        wf, smem_bytes = ctypes.c_double(), ctypes.c_double()
+        L.check(L.lib().mr_measure_smem(ctypes.byref(wf), ctypes.byref(smem_bytes)))
+        gather_wf = updates / 32.0 / tbp
+        sm_mhz = clocks.get("sm_mhz") or float(peaks.get("sm_max_mhz", 1965.0))
+        # issue: the reference-exact FP32 arithmetic takes 6 warp instructions per update (paired
+        # a1 + x1 and dw * (...), two +0.5, paired floor, two address IMADs, two loads, paired
+        # dw2 * v, two accumulating adds per two updates) plus the per-projection set-up (about
+        # one more per update); 4 warp instructions per clock per SM
+        issue_gups = 148 * 4 * sm_mhz * 1e6 * 32 / 7.0 / 1e9
         n = world
         res = {
             "metric": METRIC,
@@ -326,9 +341,20 @@ def run_mr(args):
             },
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                          "traffic": MEASURED_TRAFFIC.get(nu), "kernel": "k_fdk_staged<f32, exact>",
-                         "note": f"algorithmic bytes = 4 B/update gathered, served from shared memory and L2; "
-                                 f"peak {peak_src}; traffic = dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                 f"launch (ncu, profiles/k_fdk_staged_fdk256_fdk1024.md)"},
+                         "note": f"algorithmic bytes = the compulsory HBM bytes of one launch (filtered projections "
+                                 f"read once + volume written once, {hbm_bytes / 1e9:.2f} GB); peak {peak_src}; "
+                                 f"traffic = dram__bytes_read.sum + dram__bytes_write.sum of one launch (ncu, "
+                                 f"profiles/k_fdk_staged_fdk256_fdk1024.md). The samples are gathered from shared "
+                                 f"memory (TMA-staged), so HBM is not this kernel's bound: see onchip and issue"},
+            "onchip": {"bound": "shared-memory wavefronts", "achieved": gather_wf / 1e9, "peak": wf.value / 1e9,
+                       "unit": "G wavefronts/s", "frac": gather_wf / wf.value,
+                       "gathered_gbs": 4.0 * updates / tbp / 1e9, "peak_gbs": smem_bytes.value / 1e9,
+                       "note": "algorithmic: one 32-bit gather per update, one wavefront per 32 updates; peak "
+                               "measured on this GPU by mr_measure_smem (conflict-free loads)"},
+            "issue": {"bound": "warp-instruction issue", "achieved_gups": updates / tbp / 1e9,
+                      "roofline_gups": issue_gups, "frac": updates / tbp / 1e9 / issue_gups,
+                      "note": "7 warp instructions per update for the reference-exact FP32 arithmetic, 4 issued per "
+                              "clock per SM, 148 SMs at the SM clock sampled during the run"},
             "e2e": {"value": n * updates * e2e_steps / te2e / 1e9, "unit": "GUPS",
                     "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(nu * nu * nv * 4)},
             "gpu_launches": 3 * args.steps,
@@ -548,7 +574,11 @@ def run_parallel(args, production: bool):
             warps += (hi - 1) // 32 - (lo - 1) // 32 + 1
     wavefronts = 2.0 * warps * ((nrows // 4) * 4) * sel
     sm_mhz = clocks.get("sm_mhz") or float(peaks.get("sm_max_mhz", 1965.0))
-    wf_peak = 148 * sm_mhz * 1e6
+    from imagingsuite_b200 import _lib as L
+
+    wfm, _bytes = ctypes.c_double(), ctypes.c_double()
+    L.check(L.lib().mr_measure_smem(ctypes.byref(wfm), ctypes.byref(_bytes)))
+    wf_peak = wfm.value
     return {"metric": "parallel-beam chain GUPS (voxel x projection updates per second)",
             "value": updates * args.steps / t / 1e9, "unit": "GUPS", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -567,8 +597,7 @@ def run_parallel(args, production: bool):
                                  "so the binding roofline is the on-chip one below"},
             "onchip": {"bound": "shared-memory load wavefronts", "achieved": wavefronts / tbp / 1e9,
                        "peak": wf_peak / 1e9, "unit": "G wavefronts/s", "frac": wavefronts / tbp / wf_peak,
-                       "peak_source": "derived: one shared-memory wavefront per clock per SM x 148 SMs x the median "
-                                      "SM clock sampled during the run"},
+                       "peak_source": "measured on this GPU by mr_measure_smem (conflict-free 32-bit shared loads)"},
             "e2e": {"value": updates * e2e_steps / te / 1e9, "unit": "GUPS",
                     "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(bp.volume.numel() * 4)},
             "clocks": clocks}

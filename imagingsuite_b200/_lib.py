@@ -105,6 +105,7 @@ _PROTOS = {
                                   c_void, c_void]),
     "mr_slice_dot": (c_int, [c_void, c_void, c_size, c_size, c_size, c_void, c_void]),
     "mr_device_status": (c_int, [P_int]),
+    "mr_measure_smem": (c_int, [P_double, P_double]),
 }
 
 EXPORTED = tuple(_PROTOS)

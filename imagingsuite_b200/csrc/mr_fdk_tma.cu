@@ -170,24 +170,36 @@ __device__ __forceinline__ void fast_coord(const TG &t, float di, float dj, floa
 
 // Slices of one voxel column for one staged projection (exact arithmetic). a1: the 32
 // per-slice sums zip1 + yip1 of this warp. FULL: all TK slices exist.
+//
+// Two slices per step on the paired FP32 pipe: (a1 + x1) and dw * (...) as f32x2 add and mul,
+// + 0.5 as two scalar adds, the magic-number floor as one f32x2 add rounded down, and
+// dw2 * v as one f32x2 mul followed by two scalar adds into the accumulators. Every operation
+// is IEEE-rounded on its own, so each slice gets exactly the reference's float sequence; an
+// f32x2 mul is never followed directly by an f32x2 add, because ptxas contracts that pair into
+// an f32x2 fma even with explicit rounding.
 template <bool FULL>
 __device__ __forceinline__ void exact_column(float2 (&acc)[TK / 2], const unsigned char *smem, uint32_t base,
                                              uint32_t rowbytes, const float *a1, float x1f, float dw, float dw2,
                                              int kmax)
 {
+    const float2 x1 = make_float2(x1f, x1f), dwp = make_float2(dw, dw), dw2p = make_float2(dw2, dw2);
+    const float2 mg = make_float2(kMagic, kMagic);
 #pragma unroll
     for (int q4 = 0; q4 < TK / 4; ++q4) {
         const float4 a4 = reinterpret_cast<const float4 *>(a1)[q4];
-        const float av[4] = {a4.x, a4.y, a4.z, a4.w};
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int q = 4 * q4 + e;
+        for (int h = 0; h < 2; ++h) {
+            const int q = 4 * q4 + 2 * h; // slices q and q + 1 -> acc[q / 2]
             if (!FULL && q >= kmax) break;
-            const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(av[e], x1f)), 0.5f);
-            const uint32_t bits = __float_as_uint(__fadd_rd(r, kMagic));
-            const float v = *reinterpret_cast<const float *>(smem + (bits * rowbytes + base));
-            float &a = (q & 1) ? acc[q >> 1].y : acc[q >> 1].x;
-            a = __fadd_rn(a, __fmul_rn(dw2, v));
+            const bool two = FULL || q + 1 < kmax;
+            const float2 m = __fmul2_rn(dwp, __fadd2_rn(h ? make_float2(a4.z, a4.w) : make_float2(a4.x, a4.y), x1));
+            const float2 b = __fadd2_rd(make_float2(__fadd_rn(m.x, 0.5f), __fadd_rn(m.y, 0.5f)), mg);
+            const float v0 = *reinterpret_cast<const float *>(smem + (__float_as_uint(b.x) * rowbytes + base));
+            const float v1 =
+                two ? *reinterpret_cast<const float *>(smem + (__float_as_uint(b.y) * rowbytes + base)) : 0.0f;
+            const float2 p = __fmul2_rn(dw2p, make_float2(v0, v1));
+            acc[q >> 1].x = __fadd_rn(acc[q >> 1].x, p.x);
+            if (two) acc[q >> 1].y = __fadd_rn(acc[q >> 1].y, p.y);
         }
     }
 }

@@ -452,6 +452,14 @@ mr_status mr_slice_dot(const float *a_d, const float *b_d, size_t nproj, size_t 
  * synchronizes the device and clears the word. */
 mr_status mr_device_status(int *status);
 
+/* Diagnostics (no counterpart in the reference): the measured shared-memory load rate of the
+ * current device, the on-chip roofline of the staged backprojectors, which gather one 32-bit
+ * sample per lane from shared memory. A conflict-free kernel with many loads in flight,
+ * timed with CUDA events on the legacy default stream (synchronous; allocates a few bytes).
+ * wavefronts_per_s: shared-memory wavefronts served per second (a warp's conflict-free
+ * 32-bit load is one wavefront); bytes_per_s = 128 bytes per wavefront. */
+mr_status mr_measure_smem(double *wavefronts_per_s, double *bytes_per_s);
+
 #ifdef __cplusplus
 }
 #endif
