@@ -187,20 +187,26 @@ def run_mr(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     from imagingsuite_b200.distributed import DistContext
 
-    dctx = DistContext("nccl") if world > 1 else None
-    rank = dctx.rank if dctx else 0
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     device = torch.device("cuda", local)
+    # the timing collectives (barrier, MAX of the step time) go over NCCL; MR_DIST_BACKEND=gloo
+    # keeps them on the host (e.g. to exercise the slab path with several ranks per device)
+    backend = os.environ.get("MR_DIST_BACKEND", "nccl")
+    dctx = DistContext(backend, device=device if backend == "nccl" else None) if world > 1 else None
+    rank = dctx.rank if dctx else 0
     w = workload(args.small)
     nu, nv, nproj = w["nu"], w["nv"], w["nproj"]
     updates = float(nu) * nu * nv * nproj
 
-    counts, flats, darks = make_inputs(w, rank, device)
+    # every rank holds the same scan (one volume split across the ranks)
+    counts, flats, darks = make_inputs(w, 0, device)
     cfg = make_config(w)
     angles = np.arange(nproj, dtype=np.float32) * np.float32(360.0 / nproj)
     weights = np.full(nproj, np.float32(1.0 / nproj), np.float32)
     pipe32 = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="fp32")
+    if world > 1:
+        return run_mr_slabs(args, w, dctx, pipe32, counts, local, rank, world, updates)
     pipe16 = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="bf16")
     pipeh = pipeline.FdkPipeline(cfg, angles, weights, darks, flats, precision="fp16")
     stream = torch.cuda.current_stream()
@@ -365,6 +371,67 @@ def run_mr(args):
     if dctx:
         dctx.barrier()
         dctx.close()
+    return res
+
+
+def run_mr_slabs(args, w, dctx, pipe, counts, local, rank, world, updates):
+    """N > 1: one 1024^3 volume split into z-slabs (distributed.cone_slab_plan), each rank
+    normalising, filtering and backprojecting only its slab's detector-row window; no data-path
+    collective. `value` is the whole volume's updates over the slowest rank's time (strong
+    scaling); e2e copies each rank's row window in and its slab out."""
+    import torch
+
+    nu, nv, nproj = w["nu"], w["nv"], w["nproj"]
+    device = counts.device
+    plan = pipe.slab_plan(world)
+    s = plan[rank]
+    rows = counts[:, s.row_start:s.row_stop].contiguous()
+    stream = torch.cuda.current_stream()
+    sampler = ClockSampler(local)
+    sampler.start()
+    t = time_steps(lambda: pipe.run_slab(rows, s), args.steps, args.warmup, stream, dctx)
+    clocks = sampler.stop()
+    rows_h = rows.cpu().pin_memory()
+    out_h = torch.empty((s.size, nu, nu), dtype=torch.float32).pin_memory()
+
+    def e2e():
+        r = rows_h.to(device, non_blocking=True)
+        vol = pipe.run_slab(r, s)
+        out_h.copy_(vol[s.start:s.stop], non_blocking=True)
+
+    e2e_steps = max(1, min(args.steps, 3))
+    te = time_steps(e2e, e2e_steps, 1, stream, dctx)
+    h2d = dctx.max(float(rows.numel() * 2))
+    d2h = dctx.max(float(s.size * nu * nu * 4))
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_bytes = 2.0 * rows.numel() + 2 * 4.0 * rows.numel() + 4.0 * rows.numel() + 4.0 * s.size * nu * nu
+    res = None
+    if rank == 0:
+        res = {"metric": METRIC, "value": updates * args.steps / t / 1e9, "unit": "GUPS", "n_gpus": world,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3,
+               "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+               "data": "synthetic (seeded 10-ellipsoid phantom, analytic cone-beam line integrals, Poisson I0=5e4)",
+               "config": {"workload": w["name"], "volume": [nu, nu, nv], "projections": nproj,
+                          "chain": "FullLogNorm(u16) -> FDK ramp filter -> FDK NN backprojection, per z-slab",
+                          "parallelism": f"z-slab x{world}",
+                          "slabs": [[p.start, p.stop, p.row_start, p.row_stop] for p in plan],
+                          "l2": "inputs larger than L2"},
+               "e2e": {"value": updates * e2e_steps / te / 1e9, "unit": "GUPS",
+                       "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                       "note": "per rank (largest over ranks): its row window in, its slab out"},
+               "roofline": {"bound": "hbm", "achieved": hbm_bytes / (t / args.steps) / 1e9, "peak": hbm,
+                            "unit": "GB/s", "frac": hbm_bytes / (t / args.steps) / 1e9 / hbm, "traffic": None,
+                            "kernel": "slab step (FullLogNorm + FDK filter of the row window, k_fdk_staged)",
+                            "note": "rank 0's compulsory HBM bytes per step: counts window read, filtered window "
+                                    "written and read, slab written; the backprojection is bound by issue (N=1 line)"},
+               "gpu_launches": 4 * args.steps, "clocks": clocks}
+    dctx.barrier()
+    dctx.close()
     return res
 
 

@@ -85,6 +85,8 @@ _PROTOS = {
                                 P_float, P_float, P_int]),
     "mr_fdk_filter": (c_int, [c_void, c_size, c_size, c_size, c_void, c_float, c_float, c_int, c_void, c_void,
                               c_void]),
+    "mr_fdk_filter_rows": (c_int, [c_void, c_size, c_size, c_size, c_size, c_size, c_void, c_float, c_float, c_int,
+                                   c_void, c_void, c_void]),
     "mr_fdk_backproject": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_int,
                                    c_void, c_int, c_int, c_int, c_void, c_void]),
     "mr_fdk_backproject_slab": (c_int, [c_void, c_int, c_void, c_size, c_size, c_size, c_void, c_void, c_void, c_int,

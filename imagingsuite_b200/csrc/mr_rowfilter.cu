@@ -48,7 +48,9 @@ struct RowFilterArgs {
     size_t rows_per_weight;
     size_t nrows;
     int nu;          // row length (detector columns)
-    int nv;          // rows per projection (FDK edge-row replication)
+    int nv;          // rows per projection held (FDK edge-row replication)
+    int row0;        // FDK: absolute detector row of the first row held
+    int nvfull;      // FDK: detector rows of the whole projection
     int n;           // FFT length
     int logn;
     int ninsert;     // projection filter: data offset; FDK: pad_factor/2
@@ -86,19 +88,21 @@ __device__ __forceinline__ float padded_value(const RowFilterArgs &a, const floa
     }
 }
 
-// FDK edge-row replication (ramp_filter_tuned :874-880): rows 0..4 take row 5, rows
-// nv-5..nv-1 take row nv-6 (after the first copy).
-__device__ __forceinline__ size_t fdk_source_row(size_t r, int nv)
+// FDK edge-row replication (ramp_filter_tuned :874-880): detector rows 0..4 take row 5, rows
+// nvfull-5..nvfull-1 take row nvfull-6 (after the first copy). The rows held are the window
+// [row0, row0 + nv) of each projection (the whole detector: row0 = 0, nvfull = nv); the rule
+// applies to the absolute rows and the callers check that every source row is in the window.
+__device__ __forceinline__ size_t fdk_source_row(size_t r, int nv, int row0, int nvfull)
 {
     const size_t proj = r / nv;
-    int v = static_cast<int>(r - proj * nv);
-    if (v >= nv - 5) {
-        int q = nv - 6;
+    int v = static_cast<int>(r - proj * nv) + row0;
+    if (v >= nvfull - 5) {
+        int q = nvfull - 6;
         v = q < 5 ? 5 : q;
     } else if (v < 5) {
         v = 5;
     }
-    return proj * nv + v;
+    return proj * nv + (v - row0);
 }
 
 __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
@@ -108,8 +112,8 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
     const size_t r1 = r0 + 1;
     const bool has1 = r1 < a.nrows;
     const int n = a.n;
-    const size_t src0 = a.mode == kPadFdk ? fdk_source_row(r0, a.nv) : r0;
-    const size_t src1 = a.mode == kPadFdk ? fdk_source_row(r1, a.nv) : r1;
+    const size_t src0 = a.mode == kPadFdk ? fdk_source_row(r0, a.nv, a.row0, a.nvfull) : r0;
+    const size_t src1 = a.mode == kPadFdk ? fdk_source_row(r1, a.nv, a.row0, a.nvfull) : r1;
     const float *row0 = a.in + src0 * a.nu;
     const float *row1 = a.in + src1 * a.nu;
 
@@ -492,8 +496,23 @@ mr_status mr_quantize_noalloc(const float *in_d, size_t per, size_t nproj, int d
 mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, const float *weight_d, float sad_sid_2,
                         float scale, int out_dtype, void *out_d, float *scale_out_d, void *stream)
 {
+    return mr_fdk_filter_rows(in_d, nu, nv, 0, nv, nproj, weight_d, sad_sid_2, scale, out_dtype, out_d, scale_out_d,
+                              stream);
+}
+
+mr_status mr_fdk_filter_rows(const float *in_d, size_t nu, size_t nrows, size_t row0, size_t nv, size_t nproj,
+                             const float *weight_d, float sad_sid_2, float scale, int out_dtype, void *out_d,
+                             float *scale_out_d, void *stream)
+{
     if (!in_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: null pointer");
     if (nv < 11) return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: the edge-row replication needs at least 11 rows");
+    if (nrows == 0 || row0 + nrows > nv) return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: row window outside the detector");
+    // rows 0..4 are copies of row 5 and rows nv-5.. of row nv-6: those rows must be held too
+    if ((row0 < 5 && row0 + nrows <= 5) || (row0 + nrows > nv - 5 && row0 > nv - 6))
+        return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: the row window [%zu, %zu) misses the edge rows it copies", row0,
+                    row0 + nrows);
+    const size_t nvfull = nv;
+    nv = nrows; // rows held per projection from here on
     if (out_dtype != MR_F32 && out_dtype != MR_BF16 && out_dtype != MR_F16)
         return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: unknown output dtype");
     if (out_dtype != MR_F32 && !scale_out_d) return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: 16-bit output needs scale_out_d");
@@ -539,6 +558,8 @@ mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, c
         a.nrows = nv * nproj;
         a.nu = static_cast<int>(nu);
         a.nv = static_cast<int>(nv);
+        a.row0 = static_cast<int>(row0);
+        a.nvfull = static_cast<int>(nvfull);
         a.n = static_cast<int>(padwidth);
         a.logn = ilog2(padwidth);
         a.ninsert = static_cast<int>((padwidth - nu) / 2);

@@ -64,6 +64,50 @@ class FdkPipeline:
                                          out.data_ptr(), torch.cuda.current_stream().cuda_stream))
         return out
 
+    def slab_plan(self, world: int):
+        """The volume's z-slabs for `world` ranks with their detector-row windows
+        (distributed.cone_slab_plan on this geometry's partials)."""
+        from .distributed import cone_slab_plan
+
+        xip, yip, zip_, *_ = self.fdk.partials(self.angles)
+        return cone_slab_plan(self.nv, world, xip, yip, zip_, self.nu)
+
+    def run_slab(self, counts_rows: torch.Tensor, slab) -> torch.Tensor:
+        """One rank's share of the volume (FP32): counts_rows are the uint16 counts of the
+        slab's detector-row window (nproj, slab.rows, nu) on the device; FullLogNorm and the
+        ramp filter run on those rows only (mr_fdk_filter_rows), and the slab's slices are
+        backprojected (mr_fdk_backproject_slab). Returns the volume buffer (nv, nu, nu), of which
+        slices [slab.start, slab.stop) hold this slab; they equal the whole-volume call's."""
+        from . import _lib as L
+
+        if self.fdk.precision != "fp32":
+            raise M.ReconException("FdkPipeline.run_slab: FP32 only")
+        nproj, rows, nu = counts_rows.shape
+        if rows != slab.rows or nu != self.nu:
+            raise M.ReconException("FdkPipeline.run_slab: counts do not match the slab's row window")
+        dev = counts_rows.device
+        if getattr(self, "_slab_bufs", None) is None or self._slab_bufs[0].shape != counts_rows.shape:
+            self._slab_bufs = (torch.empty(counts_rows.shape, dtype=torch.float32, device=dev),
+                               torch.empty(counts_rows.shape, dtype=torch.float32, device=dev),
+                               torch.empty((nproj, self.nv, nu), dtype=torch.float32, device=dev))
+        norm, win, filt = self._slab_bufs
+        geo = self.fdk.prepare(self.angles, self.weights, dev)
+        w, *_, s2, sc, uni, box, maps = geo
+        st = torch.cuda.current_stream(dev).cuda_stream
+        off = slab.row_start * nu
+        dark, flat = self.norm.mDark, self.norm.mFlatField
+        dl = torch.zeros(1, device=dev)
+        L.check(L.lib().mr_lognorm_apply(counts_rows.data_ptr(), L.MR_U16, rows * nu, nproj,
+                                         None if dark is None else dark.data_ptr() + 4 * off,
+                                         None if flat is None else flat.data_ptr() + 4 * off, dl.data_ptr(), 1,
+                                         int(self.norm.nDCCount > 0), int(self.norm.nOBCount > 0), norm.data_ptr(),
+                                         st))
+        L.check(L.lib().mr_fdk_filter_rows(norm.data_ptr(), nu, rows, slab.row_start, self.nv, nproj, w.data_ptr(),
+                                           s2, sc, L.MR_F32, win.data_ptr(), None, st))
+        filt[:, slab.row_start:slab.row_stop].copy_(win)
+        self.fdk.backproject(filt, None, geo, k_range=slab.cbct_range(self.nv), accumulate=False)
+        return self.fdk.GetVolume()
+
     def run_host(self, counts_host: torch.Tensor, out_host: torch.Tensor, device, chunks: int = 8,
                  slabs: int = 8) -> torch.Tensor:
         """counts_host: pinned uint16 (nproj, nv, nu); out_host: pinned float32 (nv, nu, nu).

@@ -347,6 +347,18 @@ mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const floa
 mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, const float *weight_d,
                         float sad_sid_2, float scale, int out_dtype, void *out_d, float *scale_out_d,
                         void *stream);
+/* mr_fdk_filter on the detector rows [row0, row0 + nrows) of each projection only (in_d and
+ * out_d hold [nproj][nrows][nu]): the rows a slab of slices projects onto (the CBCT row
+ * window of ReconEngine's slice blocks, ReconEngine.cpp:954-1008). Each row equals the same
+ * row of the whole-detector call; the edge-row replication of the reference (rows 0..4 copy
+ * row 5, the last five copy row nv-6) refers to the absolute rows, so a window that reaches
+ * those rows must also hold row 5 (row nv-6), else MR_ERR_ARGUMENT. Rows are transformed two
+ * at a time (the real and imaginary parts of one complex FFT): with nv even, a window that
+ * starts on an even row and holds an even number of rows keeps the whole detector's pairs and
+ * its rows equal that call's bit for bit; other windows agree to FFT rounding. */
+mr_status mr_fdk_filter_rows(const float *in_d, size_t nu, size_t nrows, size_t row0, size_t nv, size_t nproj,
+                             const float *weight_d, float sad_sid_2, float scale, int out_dtype, void *out_d,
+                             float *scale_out_d, void *stream);
 /* Voxel-driven nearest-neighbour backprojection (:450-525) of nproj filtered
  * projections into the final volume (after FdkReconBase's per-slice mirror and z
  * reversal, fdkreconbase.cpp:259-270). vol_d [nv][nu][nu] is overwritten when

@@ -106,3 +106,57 @@ def test_parallel_chain_host_equals_device(cuda, nu, nv, nproj, chunks, blocks, 
     st = ctypes.c_int(-1)
     L.check(L.lib().mr_device_status(ctypes.byref(st)))
     assert st.value == 0
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_fdk_slabs_with_row_windows_equal_whole(cuda, world):
+    """Each rank's share (distributed.cone_slab_plan): FullLogNorm and the ramp filter on the
+    slab's detector-row window only, the slab's slices backprojected. The rows outside the
+    window are poisoned with NaN, so a voxel reading outside its window would show. Every slab
+    equals the same slices of the whole-volume reconstruction bit for bit."""
+    nu, nv, nproj = 64, 96, 20
+    rng = np.random.default_rng(7)
+    dev = torch.device("cuda", 0)
+    darks = torch.from_numpy(rng.normal(100, 3, (2, nv, nu)).astype(np.float32)).to(dev)
+    flats = torch.from_numpy(rng.normal(20000, 100, (3, nv, nu)).astype(np.float32)).to(dev)
+    counts = rng.integers(3000, 18000, (nproj, nv, nu)).astype(np.uint16)
+    angles = (np.arange(nproj) * 360.0 / nproj).astype(np.float32)
+    weights = np.full(nproj, np.float32(1.0 / nproj))
+    pipe = pipeline.FdkPipeline(_config(nu, nv, nproj), angles, weights, darks, flats)
+    whole = pipe.run_device(torch.from_numpy(counts.view(np.int16)).to(dev).view(torch.uint16)).cpu().numpy()
+    plan = pipe.slab_plan(world)
+    assert any(s.rows < nv for s in plan)
+    for s in plan:
+        rows = torch.from_numpy(np.ascontiguousarray(counts[:, s.row_start:s.row_stop]).view(np.int16)).to(dev)
+        pipe.run_slab(rows.view(torch.uint16), s)
+        pipe._slab_bufs[2].fill_(float("nan"))  # rows outside the next window stay NaN
+        vol = pipe.run_slab(rows.view(torch.uint16), s).cpu().numpy()
+        assert np.array_equal(vol[s.start:s.stop], whole[s.start:s.stop]), s
+    st = ctypes.c_int(-1)
+    L.check(L.lib().mr_device_status(ctypes.byref(st)))
+    assert st.value == 0
+
+
+def test_fdk_filter_rows_equals_whole_detector_rows(cuda):
+    """mr_fdk_filter_rows on windows inside, at the top and at the bottom of the detector gives
+    the whole-detector filter's rows; windows that miss the copied edge row are refused."""
+    nu, nv, nproj = 48, 40, 3
+    rng = np.random.default_rng(8)
+    x = torch.from_numpy(rng.standard_normal((nproj, nv, nu)).astype(np.float32)).to(cuda)
+    w = torch.from_numpy(rng.uniform(0.5, 1.5, nproj).astype(np.float32)).to(cuda)
+    st = torch.cuda.current_stream().cuda_stream
+    full = torch.empty_like(x)
+    L.check(L.lib().mr_fdk_filter(x.data_ptr(), nu, nv, nproj, w.data_ptr(), 0.25, 0.5, L.MR_F32, full.data_ptr(), None,
+                                  st))
+    # even windows: the filter transforms two rows at a time, so the whole detector's row pairs
+    # are kept (bit-identical rows)
+    for r0, r1 in ((0, 10), (8, 30), (30, 40), (12, 14), (0, 40)):
+        src = x[:, r0:r1].contiguous()
+        out = torch.empty_like(src)
+        L.check(L.lib().mr_fdk_filter_rows(src.data_ptr(), nu, r1 - r0, r0, nv, nproj, w.data_ptr(), 0.25, 0.5,
+                                           L.MR_F32, out.data_ptr(), None, st))
+        assert torch.equal(out, full[:, r0:r1]), (r0, r1)
+    bad = torch.empty((nproj, 3, nu), device=cuda)
+    for r0 in (1, 36):  # rows 1..3 need row 5; rows 36..38 need row 34
+        assert L.lib().mr_fdk_filter_rows(bad.data_ptr(), nu, 3, r0, nv, nproj, w.data_ptr(), 0.25, 0.5, L.MR_F32,
+                                          bad.data_ptr(), None, st) == L.MR_ERR_ARGUMENT
