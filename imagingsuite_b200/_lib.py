@@ -106,6 +106,9 @@ _PROTOS = {
     "mr_joseph_adjoint": (c_int, [c_void, c_size, c_size, c_void, c_size, c_size, c_float, c_float, c_float, c_int,
                                   c_void, c_void]),
     "mr_slice_dot": (c_int, [c_void, c_void, c_size, c_size, c_size, c_void, c_void]),
+    "mr_mbp_geometry": (c_int, [P_float, c_size, c_size, c_size, c_float, c_float, c_float, c_int, P_float, P_float]),
+    "mr_mbp_adjoint": (c_int, [c_void, c_size, c_size, c_void, c_void, c_size, c_void, c_int, c_void, c_void]),
+    "mr_mbp_forward": (c_int, [c_void, c_size, c_size, c_void, c_void, c_size, c_void, c_void, c_void, c_void]),
     "mr_device_status": (c_int, [P_int]),
     "mr_measure_smem": (c_int, [P_double, P_double]),
 }

@@ -1,0 +1,211 @@
+// Differentiation form matched to the parallel-beam backprojector: a forward projector that is
+// the exact transpose of MultiProjectionBPparallel's linear-interpolation backprojection
+// (MultiProjBPparallel.cpp:39-170), and that backprojection with a per-slice detector centre.
+//
+// Backprojection (the adjoint), voxel (x, y, z) with 1-based x, y inside the circle mask, every
+// projection i (no buffer-drop rule, weight 1):
+//     u = (startu[i][z] + cos_i * y) - sin_i * x,   n = (int)u in [0, nu - 2],
+//     wb = |u - n|, wa = 1 - wb,   vol[y-1][x-1][z] += P_i[z][n] * wa + P_i[z][n+1] * wb
+// with the reference's float operations in its order; startu[i][z] = (nu/2)(sin_i - cos_i) + c_z
+// and c_z = centre + tan(tilt) (z - pivot) (the detector centre of slice z). With tilt 0 this is
+// the production backprojector bit for bit (mr_bp_parallel with no weights).
+//
+// Forward projection (the exact transpose): detector bin m of slice z and projection i collects
+// wa * vol from every voxel whose n is m and wb * vol from every voxel whose n is m - 1, with the
+// same u, n, wa and wb evaluated by the same expressions, so <A x, p> = <x, A^T p> holds to float
+// summation. Ray-driven: a warp owns one (i, m) and 32 consecutive slices (lanes), walks the
+// volume rows when |sin_i| >= |cos_i| (else the columns) and, in each, only the candidate
+// voxels whose u can fall in [m - 1, m + 1): the interval of the affine u, widened by one voxel
+// on each side for the float evaluation (u is exact to ~1e-4 pixel, the walk's step is at least
+// 1/sqrt(2) pixel). Each candidate's contribution is decided by its own n, as in the adjoint.
+// The derivative d proj / d c_z (-vol for the wa term, +vol for the wb term: d wa / du = -1,
+// d wb / du = +1, du / dc_z = 1) comes out of the same walk.
+#include "mr_common.cuh"
+
+#include <cmath>
+#include <vector>
+
+namespace mr {
+
+static const float kFPi = 3.1415926535897932384626f;
+
+// One (x, y) voxel column, CZ slices from z0, per-slice start positions.
+template <int CZ>
+__global__ void __launch_bounds__(128) k_mbp_adjoint(const float *__restrict__ proj, const float2 *__restrict__ sc,
+                                                     const float *__restrict__ startu, int nproj, int n, int nz,
+                                                     const uint32_t *__restrict__ mask, int accumulate,
+                                                     float *__restrict__ vol)
+{
+    const int x1 = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int y1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int z0 = blockIdx.z * CZ;
+    if (x1 > n || y1 > n) return;
+    float *col = vol + (static_cast<size_t>(y1 - 1) * n + (x1 - 1)) * nz;
+    const uint32_t first = mask[2 * (y1 - 1)], second = mask[2 * (y1 - 1) + 1];
+    const bool inside = static_cast<uint32_t>(x1) > first && static_cast<uint32_t>(x1) <= second;
+    float acc[CZ];
+#pragma unroll
+    for (int c = 0; c < CZ; ++c) acc[c] = (accumulate && inside && z0 + c < nz) ? col[z0 + c] : 0.0f;
+    if (inside) {
+        const float fx = static_cast<float>(x1), fy = static_cast<float>(y1);
+        const size_t pstride = static_cast<size_t>(n) * nz;
+        for (int i = 0; i < nproj; ++i) {
+            const float2 s = sc[i];
+            const float cy = __fmul_rn(s.y, fy), sx = __fmul_rn(s.x, fx);
+            const float *su = startu + static_cast<size_t>(i) * nz;
+            const float *img = proj + static_cast<size_t>(i) * pstride;
+#pragma unroll
+            for (int c = 0; c < CZ; ++c) {
+                const int z = z0 + c;
+                if (z >= nz) break;
+                const float u = __fsub_rn(__fadd_rn(su[z], cy), sx);
+                const int m = __float2int_rz(u);
+                if (m < 0 || m > n - 2) continue;
+                const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
+                const float wa = __fsub_rn(1.0f, wb);
+                const float *row = img + static_cast<size_t>(z) * n + m;
+                acc[c] = __fadd_rn(acc[c], __fadd_rn(__fmul_rn(__ldg(row), wa), __fmul_rn(__ldg(row + 1), wb)));
+            }
+        }
+    }
+    // voxels outside the mask stay 0 (or keep what an accumulating call found there)
+    if (inside || !accumulate) {
+#pragma unroll
+        for (int c = 0; c < CZ; ++c)
+            if (z0 + c < nz) col[z0 + c] = acc[c];
+    }
+}
+
+// One warp per (projection i, bin m), lanes = 32 consecutive slices from z0.
+template <bool DERIV>
+__global__ void __launch_bounds__(128) k_mbp_forward(const float *__restrict__ vol, const float2 *__restrict__ sc,
+                                                     const float *__restrict__ startu, int nproj, int n, int nz,
+                                                     const uint32_t *__restrict__ mask, float *__restrict__ proj,
+                                                     float *__restrict__ dproj)
+{
+    const int lane = threadIdx.x & 31;
+    const int m = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int i = blockIdx.y;
+    const int z0 = blockIdx.z * 32, z = z0 + lane;
+    if (m >= n) return;
+    const bool zok = z < nz;
+    const float2 s = sc[i];
+    const float *su = startu + static_cast<size_t>(i) * nz;
+    const float suz = zok ? su[z] : 0.0f;
+    // the warp's extreme start positions (startu is affine in z), for the candidate interval
+    const int zl = min(z0 + 31, nz - 1);
+    const float sua = fminf(su[z0], su[zl]), sub = fmaxf(su[z0], su[zl]);
+    const float fm = static_cast<float>(m);
+    float acc = 0.0f, dacc = 0.0f;
+    auto visit = [&](int x1, int y1) {
+        const float u = __fsub_rn(__fadd_rn(suz, __fmul_rn(s.y, static_cast<float>(y1))), __fmul_rn(s.x, static_cast<float>(x1)));
+        const int k = __float2int_rz(u);
+        if (k < 0 || k > n - 2 || (k != m && k != m - 1)) return;
+        const float wb = fabsf(__fsub_rn(u, static_cast<float>(k)));
+        const float v = __ldg(vol + (static_cast<size_t>(y1 - 1) * n + (x1 - 1)) * nz + z);
+        if (k == m) {
+            acc = __fadd_rn(acc, __fmul_rn(v, __fsub_rn(1.0f, wb)));
+            if (DERIV) dacc = __fsub_rn(dacc, v);
+        } else {
+            acc = __fadd_rn(acc, __fmul_rn(v, wb));
+            if (DERIV) dacc = __fadd_rn(dacc, v);
+        }
+    };
+    if (fabsf(s.x) >= fabsf(s.y)) {
+        // walk the rows y; in row y, u = (su + cos y) - sin x lies in [m - 1, m + 1) for x in
+        // ((su + cos y - m - 1) / sin, (su + cos y - m + 1) / sin] (sin > 0; reversed for sin < 0)
+        const float inv = 1.0f / s.x;
+        for (int y1 = 1; y1 <= n; ++y1) {
+            const uint32_t first = mask[2 * (y1 - 1)], second = mask[2 * (y1 - 1) + 1];
+            if (second <= first) continue;
+            const float cy = s.y * static_cast<float>(y1);
+            const float e0 = (sua + cy - fm - 1.0f) * inv, e1 = (sub + cy - fm + 1.0f) * inv;
+            int xa = static_cast<int>(floorf(fminf(e0, e1))) - 1, xb = static_cast<int>(ceilf(fmaxf(e0, e1))) + 1;
+            xa = max(xa, static_cast<int>(first) + 1);
+            xb = min(xb, static_cast<int>(second));
+            if (zok)
+                for (int x1 = xa; x1 <= xb; ++x1) visit(x1, y1);
+        }
+    } else {
+        // walk the columns x; u lies in [m - 1, m + 1) for y in
+        // ((m - 1 - su + sin x) / cos, (m + 1 - su + sin x) / cos] (cos > 0; reversed otherwise)
+        const float inv = 1.0f / s.y;
+        for (int x1 = 1; x1 <= n; ++x1) {
+            const float sx = s.x * static_cast<float>(x1);
+            const float e0 = (fm - 1.0f - sub + sx) * inv, e1 = (fm + 1.0f - sua + sx) * inv;
+            int ya = max(static_cast<int>(floorf(fminf(e0, e1))) - 1, 1);
+            int yb = min(static_cast<int>(ceilf(fmaxf(e0, e1))) + 1, n);
+            if (zok)
+                for (int y1 = ya; y1 <= yb; ++y1) {
+                    const uint32_t first = mask[2 * (y1 - 1)], second = mask[2 * (y1 - 1) + 1];
+                    if (static_cast<uint32_t>(x1) > first && static_cast<uint32_t>(x1) <= second) visit(x1, y1);
+                }
+        }
+    }
+    if (zok) {
+        const size_t o = (static_cast<size_t>(i) * nz + z) * n + m;
+        proj[o] = acc;
+        if (DERIV) dproj[o] = dacc;
+    }
+}
+
+} // namespace mr
+
+using namespace mr;
+
+extern "C" {
+
+mr_status mr_mbp_geometry(const float *angles_h, size_t nproj, size_t n, size_t nz, float centre, float tan_tilt,
+                          float pivot, int direction, float *sincos_h, float *startu_h)
+{
+    if (nproj && (!angles_h || !sincos_h || !startu_h)) return fail(MR_ERR_ARGUMENT, "mr_mbp_geometry: null pointer");
+    if (n < 2) return fail(MR_ERR_ARGUMENT, "mr_mbp_geometry: n must be at least 2");
+    // StdBackProjectorBase::Process 2D (StdBackProjectorBase.cpp:72-79) with the centre of slice z
+    const float dirweight = 2.0f * (static_cast<float>(direction) - 0.5f);
+    const size_t mcx = n / 2;
+    for (size_t k = 0; k < nproj; ++k) {
+        const float s = std::sin(dirweight * angles_h[k] * kFPi / 180.0f);
+        const float c = std::cos(dirweight * angles_h[k] * kFPi / 180.0f);
+        sincos_h[2 * k] = s;
+        sincos_h[2 * k + 1] = c;
+        for (size_t z = 0; z < nz; ++z) {
+            const float cz = centre + tan_tilt * (static_cast<float>(z) - pivot);
+            startu_h[k * nz + z] = mcx * (s - c) + cz;
+        }
+    }
+    return MR_OK;
+}
+
+mr_status mr_mbp_adjoint(const float *proj_d, size_t n, size_t nz, const float *sincos_d, const float *startu_d,
+                         size_t nproj, const uint32_t *mask_d, int accumulate, float *vol_d, void *stream)
+{
+    if (!proj_d || !sincos_d || !startu_d || !mask_d || !vol_d) return fail(MR_ERR_ARGUMENT, "mr_mbp_adjoint: null pointer");
+    if (n < 2 || n > 65536 || nz == 0 || nz > 65536 || nproj > 0x7fffffff)
+        return fail(MR_ERR_ARGUMENT, "mr_mbp_adjoint: unsupported size");
+    constexpr int CZ = 8;
+    dim3 block(32, 4), grid(div_up(n, 32), div_up(n, 4), div_up(nz, CZ));
+    k_mbp_adjoint<CZ><<<grid, block, 0, as_stream(stream)>>>(proj_d, reinterpret_cast<const float2 *>(sincos_d), startu_d,
+                                                           static_cast<int>(nproj), static_cast<int>(n),
+                                                           static_cast<int>(nz), mask_d, accumulate, vol_d);
+    return check_launch("k_mbp_adjoint");
+}
+
+mr_status mr_mbp_forward(const float *vol_d, size_t n, size_t nz, const float *sincos_d, const float *startu_d,
+                         size_t nproj, const uint32_t *mask_d, float *proj_d, float *dproj_d, void *stream)
+{
+    if (!vol_d || !sincos_d || !startu_d || !mask_d || !proj_d) return fail(MR_ERR_ARGUMENT, "mr_mbp_forward: null pointer");
+    if (n < 2 || n > 65536 || nz == 0 || nz > 65536 || nproj == 0 || nproj > 65535)
+        return fail(MR_ERR_ARGUMENT, "mr_mbp_forward: unsupported size");
+    dim3 grid(div_up(n, 4), static_cast<unsigned>(nproj), div_up(nz, 32));
+    if (dproj_d)
+        k_mbp_forward<true><<<grid, 128, 0, as_stream(stream)>>>(vol_d, reinterpret_cast<const float2 *>(sincos_d),
+                                                               startu_d, static_cast<int>(nproj), static_cast<int>(n),
+                                                               static_cast<int>(nz), mask_d, proj_d, dproj_d);
+    else
+        k_mbp_forward<false><<<grid, 128, 0, as_stream(stream)>>>(vol_d, reinterpret_cast<const float2 *>(sincos_d),
+                                                                startu_d, static_cast<int>(nproj), static_cast<int>(n),
+                                                                static_cast<int>(nz), mask_d, proj_d, nullptr);
+    return check_launch("k_mbp_forward");
+}
+
+} // extern "C"

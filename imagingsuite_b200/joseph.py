@@ -1,7 +1,11 @@
-"""Differentiable parallel-beam projection: the Joseph projector pair of mrcuda
-(mr_joseph_forward / mr_joseph_adjoint, include/mrcuda.h) as a torch.autograd.Function,
-gradients with respect to the volume, the centre of rotation and the tilt, and CGLS with
-joint centre/tilt refinement.
+"""Differentiable parallel-beam projection: two projector pairs of mrcuda as a
+torch.autograd.Function, gradients with respect to the volume, the centre of rotation and the
+tilt, and CGLS with joint centre/tilt refinement.
+
+* MatchedOperator: the backprojector itself (MultiProjectionBPparallel's interpolation, the
+  production kernels) as A^T and its exact transpose as A (mr_mbp_*);
+* JosephOperator: the Joseph projector of the reference's LinearForwardProjector as A and its
+  exact transpose as A^T (mr_joseph_forward / mr_joseph_adjoint), the anchor to that module.
 
 Geometry. Volume (nz, n, n), x fastest; projections (nproj, nz, nu); angles in degrees. The
 detector centre of slice z is c_z = centre + tan(tilt) * (z - pivot) in detector bins
@@ -91,6 +95,92 @@ class JosephOperator:
                 tuple(p.shape) != (self.nproj, self.nz, self.nu):
             raise ValueError(f"projections must be a contiguous float32 CUDA tensor of shape "
                              f"{(self.nproj, self.nz, self.nu)}")
+
+
+class MatchedOperator:
+    """The pair matched to the parallel-beam backprojector (mr_mbp_*, include/mrcuda.h): A^T is
+    MultiProjectionBPparallel's linear-interpolation backprojection (MultiProjBPparallel.cpp:
+    39-170; every projection, weight 1) with the detector centre of slice z at
+    c_z = centre + tan(tilt) (z - pivot), and A is its exact transpose. With no tilt, A^T runs the
+    production backprojector itself (mr_bp_parallel_staged, TMA-staged); with tilt, the
+    per-slice form (mr_mbp_adjoint), which equals it bit for bit at tilt 0.
+
+    Layouts: volume (n, n, nz) = the backprojector's MatrixZXY [y][x][z]; projections
+    (nproj, nz, n): the detector is n bins wide, as the reference backprojector takes it; nz a
+    multiple of 4 (the backprojector updates slices in groups of 4). Angles in degrees, rotation
+    direction as ReconConfig's eDirection (0 = clockwise). Same interface as JosephOperator, so
+    project(), cgls(), fbp() and estimate_geometry() take either operator."""
+
+    def __init__(self, n: int, nz: int, angles_deg, pivot: float | None = None, direction: int = 0, device=None):
+        if nz % 4:
+            raise ValueError("MatchedOperator: nz must be a multiple of 4")
+        self.n, self.nz, self.nu = int(n), int(nz), int(n)
+        self.angles = np.ascontiguousarray(angles_deg, np.float32)
+        self.nproj = self.angles.size
+        self.pivot = float((nz - 1) / 2.0 if pivot is None else pivot)
+        self.direction = int(direction)
+        self.device = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        mask = np.zeros(2 * self.n, np.uint32)
+        check(L.lib().mr_bp_circle_mask(self.n, self.n, 0, 0.0, self.nz, mask.ctypes.data_as(L.P_u32)))
+        self._mask = torch.from_numpy(mask.view(np.int32)).to(self.device)
+        self._geo = {}
+
+    def geometry(self, centre: float, tilt_deg: float):
+        """(sincos (nproj, 2), startu (nproj, nz)) on the device for this centre and tilt."""
+        key = (float(centre), float(tilt_deg))
+        if key not in self._geo:
+            sc = np.empty((self.nproj, 2), np.float32)
+            su = np.empty((self.nproj, self.nz), np.float32)
+            check(L.lib().mr_mbp_geometry(self.angles.ctypes.data_as(L.P_float), self.nproj, self.n, self.nz,
+                                          float(centre), math.tan(math.radians(tilt_deg)), self.pivot,
+                                          self.direction, sc.ctypes.data_as(L.P_float), su.ctypes.data_as(L.P_float)))
+            if len(self._geo) >= 8:
+                self._geo.pop(next(iter(self._geo)))
+            self._geo[key] = tuple(torch.from_numpy(a).to(self.device) for a in (sc, su, np.ascontiguousarray(sc[:, 0]),
+                                                                              np.ascontiguousarray(sc[:, 1]),
+                                                                              np.ascontiguousarray(su[:, 0])))
+        return self._geo[key]
+
+    def forward(self, vol: torch.Tensor, centre: float, tilt_deg: float = 0.0, derivative: bool = False):
+        self._check_vol(vol)
+        sc, su, *_ = self.geometry(centre, tilt_deg)
+        proj = torch.empty((self.nproj, self.nz, self.n), dtype=torch.float32, device=vol.device)
+        dproj = torch.empty_like(proj) if derivative else None
+        check(L.lib().mr_mbp_forward(vol.data_ptr(), self.n, self.nz, sc.data_ptr(), su.data_ptr(), self.nproj,
+                                     self._mask.data_ptr(), proj.data_ptr(),
+                                     None if dproj is None else dproj.data_ptr(), _stream()))
+        return (proj, dproj) if derivative else proj
+
+    def adjoint(self, proj: torch.Tensor, centre: float, tilt_deg: float = 0.0, out: torch.Tensor | None = None,
+                accumulate: bool = False, staged: bool = True) -> torch.Tensor:
+        self._check_proj(proj)
+        sc, su, sn, cs, su0 = self.geometry(centre, tilt_deg)
+        if out is None:
+            out = torch.empty((self.n, self.n, self.nz), dtype=torch.float32, device=proj.device)
+        if tilt_deg == 0.0 and staged:
+            # the production backprojector: adds into the volume, so start from zero
+            if not accumulate:
+                out.zero_()
+            check(L.lib().mr_bp_parallel_staged(proj.data_ptr(), self.nproj, L.MR_F32, None, None, None, sn.data_ptr(),
+                                                cs.data_ptr(), su0.data_ptr(), self.nproj, self.n, self.nz,
+                                                self._mask.data_ptr(), 0, 0.0, 0.0, out.data_ptr(), _stream()))
+        else:
+            check(L.lib().mr_mbp_adjoint(proj.data_ptr(), self.n, self.nz, sc.data_ptr(), su.data_ptr(), self.nproj,
+                                         self._mask.data_ptr(), int(accumulate), out.data_ptr(), _stream()))
+        return out
+
+    slice_dot = JosephOperator.slice_dot
+    geometry_grad = JosephOperator.geometry_grad
+
+    def _check_vol(self, v):
+        if v.dtype != torch.float32 or not v.is_cuda or not v.is_contiguous() or tuple(v.shape) != (self.n, self.n, self.nz):
+            raise ValueError(f"volume must be a contiguous float32 CUDA tensor of shape {(self.n, self.n, self.nz)}")
+
+    def _check_proj(self, p):
+        if p.dtype != torch.float32 or not p.is_cuda or not p.is_contiguous() or \
+                tuple(p.shape) != (self.nproj, self.nz, self.n):
+            raise ValueError(f"projections must be a contiguous float32 CUDA tensor of shape "
+                             f"{(self.nproj, self.nz, self.n)}")
 
 
 class JosephProjection(torch.autograd.Function):

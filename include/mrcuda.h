@@ -460,6 +460,24 @@ mr_status mr_joseph_adjoint(const float *proj_d, size_t n, size_t nz, const floa
 mr_status mr_slice_dot(const float *a_d, const float *b_d, size_t nproj, size_t nz, size_t nu, double *out_d,
                        void *stream);
 
+/* ---- Differentiable pair matched to the parallel-beam backprojector (no counterpart in the
+ * reference's API): mr_mbp_adjoint is MultiProjectionBPparallel's linear-interpolation
+ * backprojection (MultiProjBPparallel.cpp:39-170, every projection, weight 1) with a detector
+ * centre per slice, c_z = centre + tan_tilt (z - pivot); with tan_tilt = 0 it equals
+ * mr_bp_parallel bit for bit. mr_mbp_forward is its exact transpose: each detector bin collects
+ * the same weights of the same voxels, so <A x, p> = <x, A^T p> up to float summation.
+ * Volume [n][n][nz] (MatrixZXY, z fastest; x, y in the circle mask of mr_bp_circle_mask(n, n, 0,
+ * 0, nz)), projections [nproj][nz][n] (the detector is n bins wide, as the reference's
+ * backprojector takes it). mr_mbp_geometry (host): sincos_h [nproj][2] = sin, cos of the
+ * direction-signed angle and startu_h [nproj][nz] = (n/2)(sin - cos) + c_z, the reference's float
+ * expressions. mr_mbp_forward also returns d proj / d c_z in dproj_d when it is not NULL. */
+mr_status mr_mbp_geometry(const float *angles_h, size_t nproj, size_t n, size_t nz, float centre, float tan_tilt,
+                          float pivot, int direction, float *sincos_h, float *startu_h);
+mr_status mr_mbp_adjoint(const float *proj_d, size_t n, size_t nz, const float *sincos_d, const float *startu_d,
+                         size_t nproj, const uint32_t *mask_d, int accumulate, float *vol_d, void *stream);
+mr_status mr_mbp_forward(const float *vol_d, size_t n, size_t nz, const float *sincos_d, const float *startu_d,
+                         size_t nproj, const uint32_t *mask_d, float *proj_d, float *dproj_d, void *stream);
+
 /* Device-side error word of bounded waits inside kernels (0 = none); reading it
  * synchronizes the device and clears the word. */
 mr_status mr_device_status(int *status);

@@ -654,6 +654,44 @@ def joseph_forward64(vol, angles, nu, centre, tan_tilt=0.0, pivot=0.0, derivativ
     return (proj, d) if derivative else proj
 
 
+def mbp_geometry(angles, n, nz, centre, tan_tilt=0.0, pivot=0.0, direction=0):
+    """sin/cos [nproj][2] and per-slice start positions [nproj][nz] of the pair matched to the
+    parallel-beam backprojector."""
+    a = _f32(angles)
+    sc = np.empty((a.size, 2), np.float32)
+    su = np.empty((a.size, nz), np.float32)
+    orc().orc_mbp_geometry(_p(a), _sz(a.size), _sz(n), _sz(nz), _f(centre), _f(tan_tilt), _f(pivot), int(direction),
+                           _p(sc), _p(su))
+    return sc, su
+
+
+def mbp_adjoint(proj, angles, centre, tan_tilt=0.0, pivot=0.0, direction=0) -> np.ndarray:
+    """The matched pair's backprojection (float, the reference's order). proj (nproj, nz, n);
+    returns the volume (n [y], n [x], nz)."""
+    proj = _f32(proj)
+    nproj, nz, n = proj.shape
+    sc, su = mbp_geometry(angles, n, nz, centre, tan_tilt, pivot, direction)
+    m = np.ascontiguousarray(circle_mask(n, n), np.uintp)
+    vol = np.empty((n, n, nz), np.float32)
+    orc().orc_mbp_adjoint(_p(proj), _sz(n), _sz(nz), _p(sc), _p(su), _sz(nproj), _p(m, _SZ), _p(vol))
+    return vol
+
+
+def mbp_forward64(vol, angles, centre, tan_tilt=0.0, pivot=0.0, direction=0, float_u=True, derivative=False):
+    """The matched pair's forward projection as the explicit transpose, FP64 accumulation.
+    vol (n, n, nz) z fastest; returns proj (nproj, nz, n) [and d proj / d c_z]."""
+    vol = _f32(vol)
+    n, _, nz = vol.shape
+    a = _f32(angles)
+    m = np.ascontiguousarray(circle_mask(n, n), np.uintp)
+    proj = np.empty((a.size, nz, n), np.float64)
+    d = np.empty_like(proj) if derivative else None
+    orc().orc_mbp_forward64(_p(vol), _sz(n), _sz(nz), _p(a), _sz(a.size), ctypes.c_double(centre),
+                            ctypes.c_double(tan_tilt), ctypes.c_double(pivot), int(direction), _p(m, _SZ),
+                            int(float_u), _p(proj, _D), None if d is None else _p(d, _D))
+    return (proj, d) if derivative else proj
+
+
 def joseph_adjoint64(proj, angles, n, centre, tan_tilt=0.0, pivot=0.0):
     """Exact transpose of joseph_forward64. proj (nproj, nz, nu) -> vol (nz, n, n) float64."""
     proj = np.ascontiguousarray(proj, np.float64)

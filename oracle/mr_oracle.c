@@ -852,6 +852,112 @@ void orc_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, siz
     circle_mask(nx, ny, correcttilt, tiltangle, nslices, mask);
 }
 
+/* ---------------------------------------- pair matched to MultiProjBPparallel */
+
+/* Per-projection sin/cos and per-slice start positions of the matched pair: the geometry of
+ * StdBackProjectorBase::Process 2D (StdBackProjectorBase.cpp:72-79) with the detector centre
+ * of slice z, c_z = centre + tan_tilt (z - pivot), in float. */
+void orc_mbp_geometry(const float *angles, size_t nproj, size_t n, size_t nz, float centre, float tan_tilt,
+                      float pivot, int direction, float *sc, float *su)
+{
+    const float dirweight = 2.0f * ((float)direction - 0.5f);
+    const size_t mcx = n / 2;
+    for (size_t k = 0; k < nproj; ++k) {
+        const float s = sinf(dirweight * angles[k] * kFPi / 180.0f);
+        const float c = cosf(dirweight * angles[k] * kFPi / 180.0f);
+        sc[2 * k] = s;
+        sc[2 * k + 1] = c;
+        for (size_t z = 0; z < nz; ++z) {
+            const float cz = centre + tan_tilt * ((float)z - pivot);
+            su[k * nz + z] = mcx * (s - c) + cz;
+        }
+    }
+}
+
+/* The backprojection of the pair (MultiProjBPparallel.cpp:39-170 without the buffer-drop rule
+ * and weights, start position per slice), float, in the reference's order. vol [n][n][nz]. */
+void orc_mbp_adjoint(const float *proj, size_t n, size_t nz, const float *sc, const float *su, size_t nproj,
+                     const size_t *mask, float *vol)
+{
+    memset(vol, 0, n * n * nz * sizeof(float));
+#pragma omp parallel for schedule(static)
+    for (long y = 1; y <= (long)n; ++y) {
+        const size_t x0 = mask[2 * (y - 1)], x1 = mask[2 * (y - 1) + 1];
+        for (size_t x = x0 + 1; x <= x1; ++x) {
+            float *col = vol + ((size_t)(y - 1) * n + (x - 1)) * nz;
+            for (size_t i = 0; i < nproj; ++i) {
+                const float s = sc[2 * i], c = sc[2 * i + 1];
+                for (size_t z = 0; z < nz; ++z) {
+                    const float u = (su[i * nz + z] + c * (float)y) - s * (float)x;
+                    const int m = (int)u;
+                    if (m < 0 || (int)n - 2 < m) continue;
+                    const float wb = fabsf(u - (float)m), wa = 1.0f - wb;
+                    const float *row = proj + (i * nz + z) * n + (size_t)m;
+                    col[z] = col[z] + (row[0] * wa + row[1] * wb);
+                }
+            }
+        }
+    }
+}
+
+/* The forward projection of the pair as the explicit transpose (scatter over voxels), FP64
+ * accumulation. float_u = 1: positions, bins and weights exactly as the kernels form them
+ * (the transpose of orc_mbp_adjoint); float_u = 0: everything in double from the geometry
+ * parameters (a smooth model in the centre and the tilt for finite differences). dproj (may be
+ * NULL) receives d proj / d c_z. */
+void orc_mbp_forward64(const float *vol, size_t n, size_t nz, const float *angles, size_t nproj, double centre,
+                       double tan_tilt, double pivot, int direction, const size_t *mask, int float_u, double *proj,
+                       double *dproj)
+{
+    memset(proj, 0, nproj * nz * n * sizeof(double));
+    if (dproj) memset(dproj, 0, nproj * nz * n * sizeof(double));
+    float *sc = (float *)malloc(2 * nproj * sizeof(float));
+    float *su = (float *)malloc(nproj * nz * sizeof(float));
+    orc_mbp_geometry(angles, nproj, n, nz, (float)centre, (float)tan_tilt, (float)pivot, direction, sc, su);
+    const double dirweight = 2.0 * ((double)direction - 0.5);
+    const double mcx = (double)(n / 2);
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < (long)nproj; ++i) {
+        const double ds = sin(dirweight * angles[i] * kDPi / 180.0), dc = cos(dirweight * angles[i] * kDPi / 180.0);
+        for (size_t y = 1; y <= n; ++y) {
+            const size_t x0 = mask[2 * (y - 1)], x1 = mask[2 * (y - 1) + 1];
+            for (size_t x = x0 + 1; x <= x1; ++x) {
+                const float *col = vol + ((y - 1) * n + (x - 1)) * nz;
+                for (size_t z = 0; z < nz; ++z) {
+                    double u, wa, wb;
+                    int m;
+                    if (float_u) {
+                        const float s = sc[2 * i], c = sc[2 * i + 1];
+                        const float uf = (su[i * nz + z] + c * (float)y) - s * (float)x;
+                        m = (int)uf;
+                        if (m < 0 || (int)n - 2 < m) continue;
+                        const float wbf = fabsf(uf - (float)m);
+                        wb = wbf;
+                        wa = 1.0f - wbf;
+                    } else {
+                        const double cz = centre + tan_tilt * ((double)z - pivot);
+                        u = (mcx * (ds - dc) + cz + dc * (double)y) - ds * (double)x;
+                        m = (int)u;
+                        if (m < 0 || (int)n - 2 < m) continue;
+                        wb = fabs(u - (double)m);
+                        wa = 1.0 - wb;
+                    }
+                    double *p = proj + ((size_t)i * nz + z) * n + (size_t)m;
+                    p[0] += wa * col[z];
+                    p[1] += wb * col[z];
+                    if (dproj) {
+                        double *d = dproj + ((size_t)i * nz + z) * n + (size_t)m;
+                        d[0] -= col[z];
+                        d[1] += col[z];
+                    }
+                }
+            }
+        }
+    }
+    free(sc);
+    free(su);
+}
+
 /* ------------------------------------------------------- morphology (kipl) */
 
 /* 2-D neighbourhoods of kipl::morphology::CNeighborhood (core/kipl/kipl/src/morphology/

@@ -60,6 +60,15 @@ void orc_bp_geometry(const float *angles, size_t n, size_t nu, float center, int
                      float *fstartu);
 void orc_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, size_t nslices, size_t *mask);
 
+/* The parallel-beam pair matched to MultiProjBPparallel (differentiation form). */
+void orc_mbp_geometry(const float *angles, size_t nproj, size_t n, size_t nz, float centre, float tan_tilt,
+                      float pivot, int direction, float *sc, float *su);
+void orc_mbp_adjoint(const float *proj, size_t n, size_t nz, const float *sc, const float *su, size_t nproj,
+                     const size_t *mask, float *vol);
+void orc_mbp_forward64(const float *vol, size_t n, size_t nz, const float *angles, size_t nproj, double centre,
+                       double tan_tilt, double pivot, int direction, const size_t *mask, int float_u, double *proj,
+                       double *dproj);
+
 /* FDKbp_single via FdkReconBase (FDKBackProjectors/src/fdkbp_single.cpp:83-994,
  * fdkreconbase.cpp:91-277). vol: XYZ [nv][nu][nu] after the final mirror. */
 typedef struct {
