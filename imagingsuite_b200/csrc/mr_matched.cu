@@ -13,7 +13,8 @@
 // Forward projection (the exact transpose): detector bin m of slice z and projection i collects
 // wa * vol from every voxel whose n is m and wb * vol from every voxel whose n is m - 1, with the
 // same u, n, wa and wb evaluated by the same expressions, so <A x, p> = <x, A^T p> holds to float
-// summation. Ray-driven: a warp owns one (i, m) and 32 consecutive slices (lanes), walks the
+// summation. Two kernels: a voxel-driven one (k_mbp_forward_smem, below) while a projection's
+// bins for 32 slices fit in shared memory, else a ray-driven one: a warp owns one (i, m) and 32 consecutive slices (lanes), walks the
 // volume rows when |sin_i| >= |cos_i| (else the columns) and, in each, only the candidate
 // voxels whose u can fall in [m - 1, m + 1): the interval of the affine u, widened by one voxel
 // on each side for the float evaluation (u is exact to ~1e-4 pixel, the walk's step is at least
@@ -149,6 +150,193 @@ __global__ void __launch_bounds__(128) k_mbp_forward(const float *__restrict__ v
     }
 }
 
+// The same forward projection, voxel-driven (used while the bins fit in shared memory): one CTA
+// per (projection i, 32 slices) holds that projection's bins of its slices in shared memory
+// (bin-major rows padded to 33 words, so the 32 lanes - one slice each - of a warp hit 32 banks
+// and the write-out reads 32 consecutive bins without conflicts). Its warps walk the masked
+// voxels line by line, along the axis on which u changes least (x when |sin| <= |cos|, else y;
+// |du| <= 1/sqrt(2) per step, so a lane's bin moves by at most one between steps), each voxel
+// once, with the adjoint's u, n, wa and wb. A lane keeps the running sums of its current pair of
+// bins (n, n + 1) in registers and adds a bin to shared memory (atomically) when its walk leaves
+// it, so most voxels cost no shared-memory access. The order of the additions into a bin depends
+// on the warps' timing: results agree with the ray-driven kernel to float summation, not bit for
+// bit.
+constexpr int kFwdPad = 33;
+constexpr int kFwdThreads = 1024;
+
+__host__ __device__ inline size_t fwd_smem_bytes(int n, bool deriv)
+{
+    return static_cast<size_t>(n) * kFwdPad * sizeof(float) * (deriv ? 2 : 1) + static_cast<size_t>(n) * sizeof(uint2) * 2;
+}
+
+template <bool DERIV>
+struct BinRun {
+    int mc = -2; // current bin (-2: none yet)
+    float a0 = 0.0f, a1 = 0.0f, d0 = 0.0f, d1 = 0.0f;
+    // one voxel: bin m (0 <= m <= n - 2), weights wa, wb, value v
+    __device__ __forceinline__ void add(float *bins, float *dbins, int lane, int m, float wa, float wb, float v)
+    {
+        const float pa = __fmul_rn(v, wa), pb = __fmul_rn(v, wb);
+        const int diff = m - mc;
+        if (diff == 0) {
+            a0 = __fadd_rn(a0, pa);
+            a1 = __fadd_rn(a1, pb);
+            if (DERIV) {
+                d0 = __fsub_rn(d0, v);
+                d1 = __fadd_rn(d1, v);
+            }
+        } else if (diff == -1) { // bin mc + 1 is left behind
+            atomicAdd(bins + (mc + 1) * kFwdPad + lane, a1);
+            a1 = __fadd_rn(a0, pb);
+            a0 = pa;
+            if (DERIV) {
+                atomicAdd(dbins + (mc + 1) * kFwdPad + lane, d1);
+                d1 = __fadd_rn(d0, v);
+                d0 = -v;
+            }
+            mc = m;
+        } else if (diff == 1) { // bin mc is left behind
+            atomicAdd(bins + mc * kFwdPad + lane, a0);
+            a0 = __fadd_rn(a1, pa);
+            a1 = pb;
+            if (DERIV) {
+                atomicAdd(dbins + mc * kFwdPad + lane, d0);
+                d0 = __fsub_rn(d1, v);
+                d1 = v;
+            }
+            mc = m;
+        } else {
+            done(bins, dbins, lane);
+            a0 = pa;
+            a1 = pb;
+            if (DERIV) {
+                d0 = -v;
+                d1 = v;
+            }
+            mc = m;
+        }
+    }
+    __device__ __forceinline__ void done(float *bins, float *dbins, int lane) const
+    {
+        if (mc < 0) return;
+        atomicAdd(bins + mc * kFwdPad + lane, a0);
+        atomicAdd(bins + (mc + 1) * kFwdPad + lane, a1);
+        if (DERIV) {
+            atomicAdd(dbins + mc * kFwdPad + lane, d0);
+            atomicAdd(dbins + (mc + 1) * kFwdPad + lane, d1);
+        }
+    }
+};
+
+template <bool DERIV>
+__global__ void __launch_bounds__(kFwdThreads, 1) k_mbp_forward_smem(const float *__restrict__ vol, const float2 *__restrict__ sc,
+                                                                  const float *__restrict__ startu, int nproj, int n,
+                                                                  int nz, const uint32_t *__restrict__ mask,
+                                                                  float *__restrict__ proj, float *__restrict__ dproj)
+{
+    extern __shared__ float bins[]; // [n][kFwdPad] (+ [n][kFwdPad] for the derivative), then the masks
+    float *dbins = bins + static_cast<size_t>(n) * kFwdPad;
+    uint2 *rowmask = reinterpret_cast<uint2 *>(bins + static_cast<size_t>(n) * kFwdPad * (DERIV ? 2 : 1));
+    uint2 *colspan = rowmask + n; // per column x: the rows [lo, hi] that hold voxels of it
+    const int i = blockIdx.x, z0 = blockIdx.y * 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const int z = z0 + lane;
+    const bool zok = z < nz;
+    for (int e = threadIdx.x; e < n * kFwdPad * (DERIV ? 2 : 1); e += blockDim.x) bins[e] = 0.0f;
+    for (int y = threadIdx.x; y < n; y += blockDim.x) rowmask[y] = make_uint2(mask[2 * y], mask[2 * y + 1]);
+    const float2 s = sc[i];
+    const bool by_rows = fabsf(s.x) <= fabsf(s.y);
+    __syncthreads();
+    if (!by_rows)
+        for (int x = threadIdx.x; x < n; x += blockDim.x) {
+            const uint32_t x1 = static_cast<uint32_t>(x) + 1;
+            int lo = 0, hi = -1;
+            for (int y = 0; y < n; ++y)
+                if (x1 > rowmask[y].x && x1 <= rowmask[y].y) {
+                    lo = y;
+                    break;
+                }
+            for (int y = n - 1; y >= lo; --y)
+                if (x1 > rowmask[y].x && x1 <= rowmask[y].y) {
+                    hi = y;
+                    break;
+                }
+            colspan[x] = make_uint2(static_cast<uint32_t>(lo), static_cast<uint32_t>(hi + 1));
+        }
+    __syncthreads();
+    BinRun<DERIV> run;
+    const float suz = zok ? startu[static_cast<size_t>(i) * nz + z] : 0.0f;
+    if (zok) {
+        if (by_rows) {
+            // line y: voxels x in (first, second], u = (su + cos y) - sin x
+            for (int y = warp; y < n; y += nwarps) {
+                const uint2 r = rowmask[y];
+                const float a = __fadd_rn(suz, __fmul_rn(s.y, static_cast<float>(y + 1)));
+                const float *p = vol + (static_cast<size_t>(y) * n + r.x) * nz + z;
+                constexpr int U = 4;
+                int x = static_cast<int>(r.x);
+                const int xe = min(static_cast<int>(r.y), n);
+                for (; x < xe; x += U) {
+                    float v[U];
+#pragma unroll
+                    for (int j = 0; j < U; ++j) v[j] = (x + j < xe) ? __ldg(p + static_cast<size_t>(j) * nz) : 0.0f;
+#pragma unroll
+                    for (int j = 0; j < U; ++j) {
+                        if (x + j >= xe) continue;
+                        const float u = __fsub_rn(a, __fmul_rn(s.x, static_cast<float>(x + j + 1)));
+                        const int m = __float2int_rz(u);
+                        if (m < 0 || m > n - 2) continue;
+                        const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
+                        run.add(bins, dbins, lane, m, __fsub_rn(1.0f, wb), wb, v[j]);
+                    }
+                    p += static_cast<size_t>(U) * nz;
+                }
+            }
+        } else {
+            // line x: voxels y in the column's span that the row masks hold
+            for (int x = warp; x < n; x += nwarps) {
+                const uint2 span = colspan[x];
+                const uint32_t x1 = static_cast<uint32_t>(x) + 1;
+                const float sx = __fmul_rn(s.x, static_cast<float>(x1));
+                const size_t ystride = static_cast<size_t>(n) * nz;
+                const float *p = vol + (static_cast<size_t>(span.x) * n + x) * nz + z;
+                constexpr int U = 4;
+                int y = static_cast<int>(span.x);
+                const int ye = static_cast<int>(span.y);
+                for (; y < ye; y += U) {
+                    float v[U];
+                    bool in[U];
+#pragma unroll
+                    for (int j = 0; j < U; ++j) {
+                        in[j] = y + j < ye && x1 > rowmask[y + j].x && x1 <= rowmask[y + j].y;
+                        v[j] = in[j] ? __ldg(p + static_cast<size_t>(j) * ystride) : 0.0f;
+                    }
+#pragma unroll
+                    for (int j = 0; j < U; ++j) {
+                        if (!in[j]) continue;
+                        const float u = __fsub_rn(__fadd_rn(suz, __fmul_rn(s.y, static_cast<float>(y + j + 1))), sx);
+                        const int m = __float2int_rz(u);
+                        if (m < 0 || m > n - 2) continue;
+                        const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
+                        run.add(bins, dbins, lane, m, __fsub_rn(1.0f, wb), wb, v[j]);
+                    }
+                    p += static_cast<size_t>(U) * ystride;
+                }
+            }
+        }
+        run.done(bins, dbins, lane);
+    }
+    __syncthreads();
+    // write-out: consecutive threads take consecutive bins of one slice (coalesced stores)
+    const int zs = min(32, nz - z0);
+    for (int e = threadIdx.x; e < zs * n; e += blockDim.x) {
+        const int zz = e / n, m = e - zz * n;
+        const size_t o = (static_cast<size_t>(i) * nz + z0 + zz) * n + m;
+        proj[o] = bins[m * kFwdPad + zz];
+        if (DERIV) dproj[o] = dbins[m * kFwdPad + zz];
+    }
+}
+
 } // namespace mr
 
 using namespace mr;
@@ -196,6 +384,23 @@ mr_status mr_mbp_forward(const float *vol_d, size_t n, size_t nz, const float *s
     if (!vol_d || !sincos_d || !startu_d || !mask_d || !proj_d) return fail(MR_ERR_ARGUMENT, "mr_mbp_forward: null pointer");
     if (n < 2 || n > 65536 || nz == 0 || nz > 65536 || nproj == 0 || nproj > 65535)
         return fail(MR_ERR_ARGUMENT, "mr_mbp_forward: unsupported size");
+    const float2 *sc = reinterpret_cast<const float2 *>(sincos_d);
+    int dev = 0, optin = 0;
+    MR_CUDA_TRY(cudaGetDevice(&dev));
+    MR_CUDA_TRY(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t smem = fwd_smem_bytes(static_cast<int>(n), dproj_d != nullptr);
+    if (smem <= static_cast<size_t>(optin)) {
+        dim3 sgrid(static_cast<unsigned>(nproj), div_up(nz, 32));
+        auto launch = [&](auto kernel, float *d) -> mr_status {
+            MR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem)));
+            kernel<<<sgrid, kFwdThreads, smem, as_stream(stream)>>>(vol_d, sc, startu_d, static_cast<int>(nproj),
+                                                                   static_cast<int>(n), static_cast<int>(nz), mask_d,
+                                                                   proj_d, d);
+            return check_launch("k_mbp_forward_smem");
+        };
+        return dproj_d ? launch(k_mbp_forward_smem<true>, dproj_d) : launch(k_mbp_forward_smem<false>, nullptr);
+    }
+    // bins beyond shared memory: the ray-driven kernel
     dim3 grid(div_up(n, 4), static_cast<unsigned>(nproj), div_up(nz, 32));
     if (dproj_d)
         k_mbp_forward<true><<<grid, 128, 0, as_stream(stream)>>>(vol_d, reinterpret_cast<const float2 *>(sincos_d),

@@ -55,6 +55,23 @@ def test_forward_matches_oracle_transpose(cuda, tilt):
     assert np.abs(d.cpu().numpy() - dexp).max() < 1e-3 * np.abs(dexp).max()
 
 
+def test_forward_both_kernels_at_1024(cuda):
+    """1024 bins: the value-only projection keeps its bins in shared memory (voxel-driven), the
+    one with the derivative needs twice that and takes the ray-driven kernel; both against the
+    oracle's transpose, and the two values against each other."""
+    rng = np.random.default_rng(5)
+    n, nz, nproj = 1024, 4, 5
+    ang = np.array([0.0, 17.3, 45.0, 101.9, 150.2], np.float32)
+    op = J.MatchedOperator(n, nz, ang, pivot=1.5)
+    x = torch.from_numpy(rng.standard_normal((n, n, nz)).astype(np.float32)).cuda()
+    v_only = op.forward(x, 511.3, 0.3).cpu().numpy()
+    v, d = op.forward(x, 511.3, 0.3, derivative=True)
+    exp, dexp = O.mbp_forward64(x.cpu().numpy(), ang, 511.3, math.tan(math.radians(0.3)), 1.5, derivative=True)
+    for got in (v_only, v.cpu().numpy()):
+        assert np.sqrt(np.sum((got - exp) ** 2) / np.sum(exp ** 2)) < 1e-6
+    assert np.abs(d.cpu().numpy() - dexp).max() < 1e-3 * np.abs(dexp).max()
+
+
 @pytest.mark.parametrize("n,nz,nproj,tilt", [(128, 32, 90, 0.0), (96, 16, 61, 0.7), (512, 8, 24, 0.4)])
 def test_dot_product(cuda, n, nz, nproj, tilt):
     g = torch.Generator(device="cuda").manual_seed(n + nz)
