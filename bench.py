@@ -155,6 +155,11 @@ def time_steps(fn, steps, warmup, stream, dist_ctx, events_kernel=None):
         fn()
     end.record(stream)
     torch.cuda.synchronize()
+    # a bounded wait that expired inside a kernel leaves the device error word set (the
+    # step's result would be incomplete): the run fails here instead of reporting it
+    from imagingsuite_b200 import _lib as L
+
+    L.check_device()
     if dist_ctx:
         dist_ctx.barrier()
     t = start.elapsed_time(end) / 1e3

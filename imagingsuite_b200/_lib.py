@@ -111,6 +111,11 @@ _PROTOS = {
     "mr_mbp_forward": (c_int, [c_void, c_size, c_size, c_void, c_void, c_size, c_void, c_void, c_void, c_void]),
     "mr_device_status": (c_int, [P_int]),
     "mr_measure_smem": (c_int, [P_double, P_double]),
+    "mr_data_validator": (c_int, [c_void, c_size, c_void, c_void]),
+    "mr_set_wait_limit": (c_int, [c_int]),
+    "mr_debug_fail_allocation": (c_int, [ctypes.c_longlong]),
+    "mr_trace_push": (c_int, [ctypes.c_char_p]),
+    "mr_trace_pop": (c_int, []),
 }
 
 EXPORTED = tuple(_PROTOS)
@@ -122,6 +127,7 @@ class MrError(RuntimeError):
     def __init__(self, status: int, message: str):
         super().__init__(f"{message} (status {status})")
         self.status = status
+        self.message = message
 
 
 def lib() -> ctypes.CDLL:
@@ -141,3 +147,12 @@ def lib() -> ctypes.CDLL:
 def check(status: int) -> None:
     if status != MR_OK:
         raise MrError(status, lib().mr_last_error().decode())
+
+
+def check_device() -> None:
+    """Reads (and clears) the device error word of the bounded waits; raises MrError with
+    MR_ERR_DEVICE when a kernel reported one. Synchronizes the device."""
+    word = ctypes.c_int(0)
+    check(lib().mr_device_status(ctypes.byref(word)))
+    if word.value:
+        raise MrError(MR_ERR_DEVICE, f"a kernel reported device error word {word.value} (bounded wait expired)")

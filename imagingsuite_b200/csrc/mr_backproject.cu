@@ -263,6 +263,7 @@ extern "C" {
 mr_status mr_bp_parallel_geometry(const float *angles_h, size_t nproj, size_t nu, float center, int direction,
                                   float *sin_h, float *cos_h, float *startu_h)
 {
+    MR_TRACE();
     if (nproj && (!angles_h || !sin_h || !cos_h || !startu_h))
         return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_geometry: null pointer");
     // StdBackProjectorBase::Process 2D (StdBackProjectorBase.cpp:72-79); eDirection 0 = CW
@@ -278,6 +279,7 @@ mr_status mr_bp_parallel_geometry(const float *angles_h, size_t nproj, size_t nu
 
 mr_status mr_bp_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltangle, size_t nslices, uint32_t *mask_h)
 {
+    MR_TRACE();
     if (!mask_h) return fail(MR_ERR_ARGUMENT, "mr_bp_circle_mask: null pointer");
     // BackProjectorModuleBase::BuildCircleMask (BackProjectorModuleBase.cpp:153-218), no matrix ROI
     const float cx = static_cast<float>(nx >> 1);
@@ -306,6 +308,7 @@ mr_status mr_bp_circle_mask(size_t nx, size_t ny, int correcttilt, float tiltang
 
 mr_status mr_bp_parallel_tilt(float tiltangle, float tiltpivot, size_t roi_y0, float *tiltoffset, float *tiltinc)
 {
+    MR_TRACE();
     if (!tiltoffset || !tiltinc) return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_tilt: null pointer");
     // MultiProjBPparallel.cpp:64-65,73
     *tiltoffset = (roi_y0 - tiltpivot) * std::tan(tiltangle * kFPi / 180);
@@ -362,6 +365,7 @@ mr_status mr_bp_parallel(const void *proj_d, int dtype, const float *scale_d, co
                          size_t nproj, size_t nu, size_t nv, const uint32_t *mask_d, int correcttilt, float tiltoffset,
                          float tiltinc, float *vol_d, void *stream)
 {
+    MR_TRACE();
     return bp_parallel_rows(proj_d, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv, mask_d,
                             correcttilt, tiltoffset, tiltinc, 0, nu, 0, vol_d, stream);
 }
@@ -473,6 +477,7 @@ static void fdk_frame(const mr_fdk_geom *g, size_t nu, size_t nv, float origin[3
 mr_status mr_fdk_partials(const mr_fdk_geom *g, size_t nu, size_t nv, const float *angles_h, size_t nproj,
                           float *xip_h, float *yip_h, float *zip_h, float *sad_sid_2, float *scale, int *uniform_z)
 {
+    MR_TRACE();
     if (!g || (nproj && (!angles_h || !xip_h || !yip_h || !zip_h)) || !sad_sid_2 || !scale || !uniform_z)
         return fail(MR_ERR_ARGUMENT, "mr_fdk_partials: null pointer");
     if (nu == 0 || nv == 0) return fail(MR_ERR_ARGUMENT, "mr_fdk_partials: empty detector");
@@ -564,6 +569,7 @@ static void fdk_projmatrix64(const mr_fdk_geom *g, double angle, double *pm)
 mr_status mr_fdk_maps64(const mr_fdk_geom *g, size_t nu, size_t nv, const float *angles_h, size_t nproj,
                         double *maps_h)
 {
+    MR_TRACE();
     if (!g || (nproj && (!angles_h || !maps_h))) return fail(MR_ERR_ARGUMENT, "mr_fdk_maps64: null pointer");
     if (nu == 0 || nv == 0) return fail(MR_ERR_ARGUMENT, "mr_fdk_maps64: empty detector");
     float originf[3];
@@ -607,6 +613,7 @@ mr_status mr_fdk_backproject_slab(const void *proj_d, int dtype, const float *sc
                                   const uint32_t *mask_d, int box_w, int box_h, int accumulate, size_t k_begin,
                                   size_t k_end, float *vol_d, void *stream)
 {
+    MR_TRACE();
     if (!proj_d || !xip_d || !yip_d || !zip_d || !mask_d || !vol_d)
         return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: null pointer");
     if (dtype != MR_F32 && dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject: dtype");
@@ -646,6 +653,7 @@ mr_status mr_fdk_backproject(const void *proj_d, int dtype, const float *scale_d
                              const float *xip_d, const float *yip_d, const float *zip_d, int uniform_z,
                              const uint32_t *mask_d, int box_w, int box_h, int accumulate, float *vol_d, void *stream)
 {
+    MR_TRACE();
     return mr_fdk_backproject_slab(proj_d, dtype, scale_d, nu, nv, nproj, xip_d, yip_d, zip_d, uniform_z, mask_d, box_w,
                                    box_h, accumulate, 0, nv, vol_d, stream);
 }

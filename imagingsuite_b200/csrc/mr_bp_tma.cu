@@ -56,6 +56,7 @@ struct Params {
     const uint32_t *mask;
     float *vol;
     int nproj, nu, nv, nz4;
+    int wait_limit; // tries of each per-batch wait
     int ybegin, yend; // volume rows y1 - 1 in [ybegin, yend)
 };
 
@@ -224,11 +225,12 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
     bool failed = false;
     const float fx = static_cast<float>(x1), fy = static_cast<float>(y1);
     const int um2 = P.nu - 2;
-    for (int s = 0, gb = 0; s < nbatch; ++s, gb = gb == 2 ? 0 : gb + 1) {
+    int s = 0;
+    for (int gb = 0; s < nbatch; ++s, gb = gb == 2 ? 0 : gb + 1) {
         const int st = s & 1; // stage buffer; geometry buffer gb = s % 3
         // a wait that timed out skips the batch in its whole warp; the block then leaves the
         // loop together at the barrier below
-        const bool got = __all_sync(0xffffffffu, tma::mbar_wait(&S.bars[st], st ? phase1 : phase0));
+        const bool got = __all_sync(0xffffffffu, tma::mbar_wait(&S.bars[st], st ? phase1 : phase0, P.wait_limit));
         if (got) {
             if (st) phase1 ^= 1; else phase0 ^= 1;
         } else {
@@ -327,8 +329,11 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
         if (s + 3 < nbatch) stage_geometry(s + 3, gb);
     }
     if (failed) {
-        tma::mbar_wait(&S.bars[0], phase0);
-        tma::mbar_wait(&S.bars[1], phase1);
+        // copies still in flight: batch s (its wait expired) and batch s+1 when it was issued;
+        // wait for them (bounded) before the block's shared memory is released
+        const int st = s & 1;
+        tma::mbar_wait(&S.bars[st], st ? phase1 : phase0);
+        if (s + 1 < nbatch) tma::mbar_wait(&S.bars[st ^ 1], st ? phase0 : phase1);
     }
     if (inside) {
 #pragma unroll
@@ -380,6 +385,7 @@ mr_status bp_parallel_staged_launch(const float *proj_d, size_t nslabs, const fl
     P.nu = static_cast<int>(nu);
     P.nv = static_cast<int>(nv);
     P.nz4 = static_cast<int>((nv / 4) * 4);
+    P.wait_limit = tma::g_batch_wait_limit.load();
     P.ybegin = static_cast<int>(y_begin);
     P.yend = static_cast<int>(y_end);
     const size_t smem = Smem::bytes();
@@ -411,6 +417,7 @@ extern "C" mr_status mr_bp_parallel_variant(int variant, const void *proj_d, siz
                                             float tiltoffset, float tiltinc, size_t y_begin, size_t y_end, float *vol_d,
                                             void *stream)
 {
+    MR_TRACE();
     if (!proj_d || !sin_d || !cos_d || !startu_d || !mask_d || !vol_d)
         return fail(MR_ERR_ARGUMENT, "mr_bp_parallel_variant: null pointer");
     if (variant < MR_BP_MULTIPROJ_PARALLEL || variant > MR_BP_NEAREST)
@@ -438,6 +445,7 @@ extern "C" mr_status mr_bp_parallel_rows(const void *proj_d, size_t nslabs, int 
                                          const uint32_t *mask_d, int correcttilt, float tiltoffset, float tiltinc,
                                          size_t y_begin, size_t y_end, float *vol_d, void *stream)
 {
+    MR_TRACE();
     return mr_bp_parallel_variant(MR_BP_MULTIPROJ_PARALLEL, proj_d, nslabs, dtype, scale_d, weight_d, index_d, sin_d,
                                   cos_d, startu_d, nproj, nu, nv, mask_d, correcttilt, tiltoffset, tiltinc, y_begin,
                                   y_end, vol_d, stream);
@@ -449,6 +457,7 @@ extern "C" mr_status mr_bp_parallel_staged(const void *proj_d, size_t nslabs, in
                                            const uint32_t *mask_d, int correcttilt, float tiltoffset, float tiltinc,
                                            float *vol_d, void *stream)
 {
+    MR_TRACE();
     return mr_bp_parallel_rows(proj_d, nslabs, dtype, scale_d, weight_d, index_d, sin_d, cos_d, startu_d, nproj, nu, nv,
                                mask_d, correcttilt, tiltoffset, tiltinc, 0, nu, vol_d, stream);
 }

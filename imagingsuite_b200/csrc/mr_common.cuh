@@ -13,6 +13,8 @@
 
 #include "mrcuda.h"
 
+#include <nvtx3/nvToolsExt.h>
+
 namespace mr {
 
 // Per-thread last error message (mr_last_error).
@@ -42,13 +44,45 @@ inline mr_status check_launch(const char *what)
         if (e_ != cudaSuccess) return ::mr::fail(MR_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_));   \
     } while (0)
 
+#define MR_TRY(expr)                                                                                       \
+    do {                                                                                                   \
+        const mr_status st_ = (expr);                                                                      \
+        if (st_ != MR_OK) return st_;                                                                      \
+    } while (0)
+
 inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
+
+// NVTX range over an entry point (a no-op unless a profiler is attached): every C-ABI call
+// shows up by name on the host timeline around the kernels it launches.
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange &) = delete;
+    TraceRange &operator=(const TraceRange &) = delete;
+};
+#define MR_TRACE() ::mr::TraceRange mr_trace_range_(__func__)
 
 // Keep memory freed by cudaFreeAsync cached in the current device's default pool (release
 // threshold = unlimited) instead of returning it to the driver at every synchronisation, so
 // that per-call scratch (up to tens of GB for a block of projections) is mapped once.
 // Applied once per device by the entry points that allocate scratch.
 void keep_pool_memory();
+
+// Scratch allocation of the entry points: stream-ordered from the device's default pool (kept
+// as above), or synchronous. MR_ERR_ALLOCATION when the device has no room, or when the
+// allocation-failure hook (mr_debug_fail_allocation) takes this allocation.
+mr_status device_alloc(void **p, size_t bytes, cudaStream_t s, const char *what);
+mr_status device_alloc_sync(void **p, size_t bytes, const char *what);
+template <class T>
+inline mr_status device_alloc(T **p, size_t bytes, cudaStream_t s, const char *what)
+{
+    return device_alloc(reinterpret_cast<void **>(p), bytes, s, what);
+}
+template <class T>
+inline mr_status device_alloc_sync(T **p, size_t bytes, const char *what)
+{
+    return device_alloc_sync(reinterpret_cast<void **>(p), bytes, what);
+}
 
 inline unsigned div_up(size_t a, size_t b) { return static_cast<unsigned>((a + b - 1) / b); }
 

@@ -12,6 +12,7 @@
 #include <vector>
 
 #include <cmath>
+#include <atomic>
 #include <cstring>
 
 namespace mr {
@@ -30,6 +31,47 @@ void keep_pool_memory()
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold);
     }
     done[dev] = true;
+}
+
+// Allocation-failure hook: the allocation that finds the countdown at 0 fails (the countdown
+// then stays disarmed at -1); each allocation that finds it above 0 counts it down.
+static std::atomic<long long> g_alloc_countdown{-1};
+
+static bool alloc_hook_takes()
+{
+    long long v = g_alloc_countdown.load();
+    while (v >= 0)
+        if (g_alloc_countdown.compare_exchange_weak(v, v - 1)) return v == 0;
+    return false;
+}
+
+mr_status device_alloc(void **p, size_t bytes, cudaStream_t s, const char *what)
+{
+    *p = nullptr;
+    if (alloc_hook_takes()) return fail(MR_ERR_ALLOCATION, "%s: %zu bytes (allocation-failure hook)", what, bytes);
+    keep_pool_memory();
+    const cudaError_t e = cudaMallocAsync(p, bytes, s);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? MR_ERR_ALLOCATION : MR_ERR_CUDA, "%s: %zu bytes: %s", what, bytes,
+                    cudaGetErrorString(e));
+    }
+    return MR_OK;
+}
+
+mr_status device_alloc_sync(void **p, size_t bytes, const char *what)
+{
+    *p = nullptr;
+    if (alloc_hook_takes()) return fail(MR_ERR_ALLOCATION, "%s: %zu bytes (allocation-failure hook)", what, bytes);
+    const cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(e == cudaErrorMemoryAllocation ? MR_ERR_ALLOCATION : MR_ERR_CUDA, "%s: %zu bytes: %s", what, bytes,
+                    cudaGetErrorString(e));
+    }
+    return MR_OK;
 }
 
 
@@ -351,6 +393,45 @@ static size_t compute_weights(const float *angles, size_t n, float arc0, float a
     return m;
 }
 
+// kipl::algorithms::dataValidator (core/kipl/kipl/include/algorithms/datavalidator.h:8-19) as
+// ReconEngine::validateImage uses it: NaNs (exponent all ones, mantissa not zero) and infinities
+// of either sign, counted by their bits. Grid-stride over float4 runs when the data are 16-byte
+// aligned; per-warp sums, one atomic per warp.
+__global__ void __launch_bounds__(256) k_nonfinite(const float *__restrict__ d, size_t n,
+                                                   unsigned long long *__restrict__ counts)
+{
+    unsigned cnan = 0, cinf = 0;
+    auto count = [&](float v) {
+        const uint32_t b = __float_as_uint(v) & 0x7fffffffu;
+        cnan += b > 0x7f800000u;
+        cinf += b == 0x7f800000u;
+    };
+    const size_t tid = static_cast<size_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
+    size_t head = 0;
+    if ((reinterpret_cast<uintptr_t>(d) & 15) == 0) {
+        const size_t n4 = n / 4;
+        const float4 *d4 = reinterpret_cast<const float4 *>(d);
+        for (size_t i = tid; i < n4; i += stride) {
+            const float4 v = __ldg(d4 + i);
+            count(v.x);
+            count(v.y);
+            count(v.z);
+            count(v.w);
+        }
+        head = n4 * 4;
+    }
+    for (size_t i = head + tid; i < n; i += stride) count(__ldg(d + i));
+    for (int o = 16; o > 0; o >>= 1) {
+        cnan += __shfl_down_sync(0xffffffffu, cnan, o);
+        cinf += __shfl_down_sync(0xffffffffu, cinf, o);
+    }
+    if ((threadIdx.x & 31) == 0 && (cnan | cinf)) {
+        atomicAdd(counts, static_cast<unsigned long long>(cnan));
+        atomicAdd(counts + 1, static_cast<unsigned long long>(cinf));
+    }
+}
+
 } // namespace mr
 
 using namespace mr;
@@ -374,9 +455,44 @@ const char *mr_status_string(mr_status s)
 
 const char *mr_last_error(void) { return g_last_error.c_str(); }
 
+mr_status mr_data_validator(const float *data_d, size_t n, unsigned long long *counts_d, void *stream)
+{
+    MR_TRACE();
+    if (!counts_d || (n && !data_d)) return fail(MR_ERR_ARGUMENT, "mr_data_validator: null pointer");
+    cudaStream_t s = as_stream(stream);
+    MR_CUDA_TRY(cudaMemsetAsync(counts_d, 0, 2 * sizeof(unsigned long long), s));
+    if (n == 0) return MR_OK;
+    int dev = 0, sms = 148;
+    MR_CUDA_TRY(cudaGetDevice(&dev));
+    MR_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const unsigned blocks = static_cast<unsigned>(std::min<size_t>(static_cast<size_t>(sms) * 8, div_up(n, 1024)));
+    k_nonfinite<<<blocks, 256, 0, s>>>(data_d, n, counts_d);
+    return check_launch("k_nonfinite");
+}
+
+mr_status mr_debug_fail_allocation(long long after)
+{
+    g_alloc_countdown.store(after < 0 ? -1 : after);
+    return MR_OK;
+}
+
+mr_status mr_trace_push(const char *name)
+{
+    if (!name) return fail(MR_ERR_ARGUMENT, "mr_trace_push: null name");
+    nvtxRangePushA(name);
+    return MR_OK;
+}
+
+mr_status mr_trace_pop(void)
+{
+    nvtxRangePop();
+    return MR_OK;
+}
+
 mr_status mr_reference_average(const float *frames_d, size_t nu, size_t nv, size_t n, int method, float *out_d,
                                void *stream)
 {
+    MR_TRACE();
     if (!frames_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_reference_average: null pointer");
     if (n == 0) return fail(MR_ERR_ARGUMENT, "mr_reference_average: no frames");
     if (method < 0 || method > 5)
@@ -390,8 +506,7 @@ mr_status mr_reference_average(const float *frames_d, size_t nu, size_t nv, size
                                          "(at least 5x5, at most 65535 frames)", n, nu, nv);
         cudaStream_t s = as_stream(stream);
         float *work = nullptr;
-        keep_pool_memory();
-        MR_CUDA_TRY(cudaMallocAsync(&work, 4 * n * npix * sizeof(float), s));
+        MR_TRY(device_alloc(&work, 4 * n * npix * sizeof(float), s, "mr_reference_average: scratch"));
         float *sigma = work, *sq = work + n * npix, *tmp = sq + n * npix, *s2 = tmp + n * npix;
         kf::stddev_filter<5>(frames_d, static_cast<int>(nu), static_cast<int>(nv), static_cast<unsigned>(n), sq, tmp,
                              s2, sigma, s);
@@ -408,6 +523,7 @@ mr_status mr_reference_average(const float *frames_d, size_t nu, size_t nv, size
 mr_status mr_projection_dose(const void *in_d, int dtype, size_t nu, size_t nv, size_t nframes, const size_t *roi_h,
                              float *dose_d, void *stream)
 {
+    MR_TRACE();
     if (!in_d || !dose_d || !roi_h) return fail(MR_ERR_ARGUMENT, "mr_projection_dose: null pointer");
     if (dtype != MR_F32 && dtype != MR_U16) return fail(MR_ERR_ARGUMENT, "mr_projection_dose: dtype must be f32 or u16");
     if (nframes == 0) return MR_OK;
@@ -421,8 +537,7 @@ mr_status mr_projection_dose(const void *in_d, int dtype, size_t nu, size_t nv, 
     const size_t w = roi_h[2] - roi_h[0], h = roi_h[3] - roi_h[1];
     if (h > 8192) return fail(MR_ERR_ARGUMENT, "mr_projection_dose: ROI taller than 8192 rows");
     float *means = nullptr;
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&means, nframes * h * sizeof(float), s));
+    MR_TRY(device_alloc(&means, nframes * h * sizeof(float), s, "mr_projection_dose: scratch"));
     dim3 g(div_up(h, 128), static_cast<unsigned>(nframes));
     if (dtype == MR_F32)
         k_row_means<float><<<g, 128, 0, s>>>(static_cast<const float *>(in_d), nu, nv, nframes, roi_h[0], roi_h[1], w, h,
@@ -444,6 +559,7 @@ mr_status mr_projection_dose(const void *in_d, int dtype, size_t nu, size_t nv, 
 mr_status mr_lognorm_logflat(const float *dark_d, const float *flat_d, size_t npix, int ndc, float flatdose,
                              float *logflat_d, void *stream)
 {
+    MR_TRACE();
     if (!flat_d || !logflat_d || (ndc && !dark_d)) return fail(MR_ERR_ARGUMENT, "mr_lognorm_logflat: null pointer");
     const float dose = 1.0f / flatdose; // host division, as the reference (NormPlugins.cpp:306)
     if (dose != dose) return fail(MR_ERR_ARGUMENT, "The reference dose is a NaN");
@@ -455,6 +571,7 @@ mr_status mr_lognorm_logflat(const float *dark_d, const float *flat_d, size_t np
 
 mr_status mr_lognorm_doselog(const float *dose_h, size_t n, float darkdose, float *doselog_h)
 {
+    MR_TRACE();
     if ((!dose_h || !doselog_h) && n) return fail(MR_ERR_ARGUMENT, "mr_lognorm_doselog: null pointer");
     for (size_t i = 0; i < n; ++i) {
         float d = dose_h[i] - darkdose;
@@ -467,6 +584,7 @@ mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t n
                            const float *logflat_d, const float *doselog_d, size_t ndose, int ndc, int nob,
                            float *out_d, void *stream)
 {
+    MR_TRACE();
     if (!in_d || !out_d || !doselog_d || (ndc && !dark_d) || (nob && !logflat_d))
         return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply: null pointer");
     if (in_dtype != MR_U16 && in_dtype != MR_F32) return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply: input must be u16 or f32");
@@ -491,6 +609,7 @@ mr_status mr_lognorm_apply(const void *in_d, int in_dtype, size_t npix, size_t n
 mr_status mr_compute_weights(const float *angles_h, size_t n, const float *scanarc_h, int golden_section,
                              float *angles_out_h, float *weights_out_h, size_t *nout_h)
 {
+    MR_TRACE();
     if ((n && (!angles_h || !angles_out_h || !weights_out_h)) || !scanarc_h || !nout_h)
         return fail(MR_ERR_ARGUMENT, "mr_compute_weights: null pointer");
     *nout_h = compute_weights(angles_h, n, scanarc_h[0], scanarc_h[1], golden_section != 0, angles_out_h,
@@ -502,6 +621,7 @@ mr_status mr_lognorm_apply_lut(const void *in_d, int in_dtype, size_t npix, size
                                const float *logflat_d, const float *doselog_d, size_t ndose, int ndc, int nob,
                                float *out_d, void *stream)
 {
+    MR_TRACE();
     if (!in_d || !out_d || !doselog_d || (ndc && !dark_d) || (nob && !logflat_d))
         return fail(MR_ERR_ARGUMENT, "mr_lognorm_apply_lut: null pointer");
     if (in_dtype != MR_U16 && in_dtype != MR_F32)
@@ -512,8 +632,7 @@ mr_status mr_lognorm_apply_lut(const void *in_d, int in_dtype, size_t npix, size
     const std::vector<float> &table = log_lut_table();
     cudaStream_t s = as_stream(stream);
     float *lut = nullptr;
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&lut, table.size() * sizeof(float), s));
+    MR_TRY(device_alloc(&lut, table.size() * sizeof(float), s, "mr_lognorm_apply_lut: scratch"));
     mr_status st = MR_OK;
     cudaError_t e = cudaMemcpyAsync(lut, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) st = fail(MR_ERR_CUDA, "mr_lognorm_apply_lut: table upload: %s", cudaGetErrorString(e));

@@ -78,6 +78,7 @@ struct Params {
     int accumulate;
     int kbegin, kend; // cbct slices backprojected: [kbegin, kend)
     int xalign;       // x coordinate alignment of a TMA load (elements)
+    int wait_limit;   // tries of each per-batch wait
 };
 
 using tma::mbar_expect_tx;
@@ -465,13 +466,14 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
     const float fdi = static_cast<float>(lane), fdj = static_cast<float>(warp); // voxel offset in the tile
     const uint32_t rowbytes = static_cast<uint32_t>(P.rowbytes);
     const bool warp_inside = __any_sync(0xffffffffu, inside);
-    for (int s = 0, gb = 0; s < nbatch; ++s, gb = gb == 2 ? 0 : gb + 1) {
+    int s = 0;
+    for (int gb = 0; s < nbatch; ++s, gb = gb == 2 ? 0 : gb + 1) {
         const int st = s & 1;  // stage buffer
         const float *geo = S.geo + gb * NB * GEO; // geometry buffer s % 3
         const uint32_t par = st ? phase1 : phase0;
         // a wait that timed out skips the batch in its whole warp; the block then leaves the
         // loop together at the barrier below
-        const bool got = __all_sync(0xffffffffu, mbar_wait(&S.bars[st], par));
+        const bool got = __all_sync(0xffffffffu, mbar_wait(&S.bars[st], par, P.wait_limit));
         if (got) {
             if (st) phase1 ^= 1; else phase0 ^= 1;
         } else {
@@ -638,9 +640,11 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
         if (s + 3 < nbatch) stage_geometry<EXACT, NB>(P, S.geo + gb * NB * GEO, s + 3, i0, j0, k0, kmax);
     }
     if (failed) {
-        // the other stage may still have a copy in flight: wait for it (bounded) before exit
-        mbar_wait(&S.bars[0], phase0);
-        mbar_wait(&S.bars[1], phase1);
+        // copies still in flight: batch s (its wait expired) and batch s+1 when it was issued;
+        // wait for them (bounded) before the block's shared memory is released
+        const int st = s & 1;
+        mbar_wait(&S.bars[st], st ? phase1 : phase0);
+        if (s + 1 < nbatch) mbar_wait(&S.bars[st ^ 1], st ? phase0 : phase1);
     }
     write_out();
 }
@@ -809,6 +813,7 @@ static mr_status staged_launch(bool exact, const void *proj_d, int dtype, const 
     P.kbegin = kbegin;
     P.kend = kend;
     P.xalign = xalign;
+    P.wait_limit = tma::g_batch_wait_limit.load();
     dim3 grid(div_up(nu, TI), div_up(nu, TJ), div_up(static_cast<size_t>(kend - kbegin), TK));
     auto go = [&](auto kernel, size_t smem) -> mr_status {
         MR_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(kMaxSmem)));
@@ -862,6 +867,7 @@ extern "C" {
 mr_status mr_fdk_box(const float *xip_h, const float *yip_h, const float *zip_h, size_t nu, size_t nv, size_t nproj,
                      int dtype, int *box_w, int *box_h)
 {
+    MR_TRACE();
     if (!xip_h || !yip_h || !zip_h || !box_w || !box_h) return fail(MR_ERR_ARGUMENT, "mr_fdk_box: null pointer");
     if (dtype != MR_F32 && dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_fdk_box: dtype");
     if (nu == 0 || nv == 0 || nproj == 0) {
@@ -873,6 +879,7 @@ mr_status mr_fdk_box(const float *xip_h, const float *yip_h, const float *zip_h,
 
 mr_status mr_fdk_box_maps(const double *maps_h, size_t nu, size_t nv, size_t nproj, int dtype, int *box_w, int *box_h)
 {
+    MR_TRACE();
     if (!maps_h || !box_w || !box_h) return fail(MR_ERR_ARGUMENT, "mr_fdk_box_maps: null pointer");
     if (dtype != MR_F32 && dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_fdk_box_maps: dtype");
     if (nu == 0 || nv == 0 || nproj == 0) {
@@ -891,6 +898,7 @@ mr_status mr_fdk_backproject_fast(const void *proj_d, int dtype, const float *sc
                                   size_t nproj, const double *maps_d, const uint32_t *mask_d, int box_w, int box_h,
                                   int accumulate, float *vol_d, void *stream)
 {
+    MR_TRACE();
     if (!proj_d || !scale_d || !maps_d || !mask_d || !vol_d)
         return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_fast: null pointer");
     if (dtype != MR_BF16 && dtype != MR_F16)
@@ -911,6 +919,7 @@ mr_status mr_fdk_backproject_f64(const float *proj_d, size_t nu, size_t nv, size
                                  const uint32_t *mask_d, const int *slices_d, size_t nslices, double *out_d,
                                  void *stream)
 {
+    MR_TRACE();
     if (!proj_d || !maps_d || !mask_d || !slices_d || !out_d)
         return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_f64: null pointer");
     if (nslices == 0 || nslices > 16) return fail(MR_ERR_ARGUMENT, "mr_fdk_backproject_f64: 1 to 16 slices");
@@ -923,8 +932,15 @@ mr_status mr_fdk_backproject_f64(const float *proj_d, size_t nu, size_t nv, size
     return check_launch("k_fdk_f64");
 }
 
+mr_status mr_set_wait_limit(int tries)
+{
+    tma::g_batch_wait_limit.store(tries < 0 ? tma::kWaitLimit : tries);
+    return MR_OK;
+}
+
 mr_status mr_device_status(int *status)
 {
+    MR_TRACE();
     if (!status) return fail(MR_ERR_ARGUMENT, "mr_device_status: null pointer");
     int v = 0, zero = 0;
     MR_CUDA_TRY(cudaMemcpyFromSymbol(&v, g_device_error, sizeof(int)));

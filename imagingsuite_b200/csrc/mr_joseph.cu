@@ -202,6 +202,7 @@ extern "C" {
 
 mr_status mr_joseph_geometry(const float *angles_h, size_t nproj, size_t n, float *params_h)
 {
+    MR_TRACE();
     if (nproj && (!angles_h || !params_h)) return fail(MR_ERR_ARGUMENT, "mr_joseph_geometry: null pointer");
     if (n < 2) return fail(MR_ERR_ARGUMENT, "mr_joseph_geometry: slice size below 2");
     const double kPi = 3.1415926535897932384626433832795028841971693993751;
@@ -233,6 +234,7 @@ mr_status mr_joseph_forward(const float *vol_d, float *volt_d, size_t n, size_t 
                             size_t nproj, size_t nu, float centre, float tan_tilt, float pivot, float *proj_d,
                             float *dproj_d, void *stream)
 {
+    MR_TRACE();
     if (!vol_d || !volt_d || !params_d || !proj_d) return fail(MR_ERR_ARGUMENT, "mr_joseph_forward: null pointer");
     if (n < 2 || n > 65536 || nz == 0 || nz > 65535 || nu == 0 || nproj == 0 || nproj > 65535)
         return fail(MR_ERR_ARGUMENT, "mr_joseph_forward: unsupported size");
@@ -251,6 +253,7 @@ mr_status mr_joseph_forward(const float *vol_d, float *volt_d, size_t n, size_t 
 mr_status mr_joseph_adjoint(const float *proj_d, size_t n, size_t nz, const float *params_d, size_t nproj, size_t nu,
                             float centre, float tan_tilt, float pivot, int accumulate, float *vol_d, void *stream)
 {
+    MR_TRACE();
     if (!proj_d || !params_d || !vol_d) return fail(MR_ERR_ARGUMENT, "mr_joseph_adjoint: null pointer");
     if (n < 2 || n > 65535 || nz == 0 || nz > 65535 || nu == 0 || nproj == 0 || nproj > 65535)
         return fail(MR_ERR_ARGUMENT, "mr_joseph_adjoint: unsupported size");
@@ -266,6 +269,7 @@ mr_status mr_joseph_adjoint(const float *proj_d, size_t n, size_t nz, const floa
 mr_status mr_slice_dot(const float *a_d, const float *b_d, size_t nproj, size_t nz, size_t nu, double *out_d,
                        void *stream)
 {
+    MR_TRACE();
     if (!a_d || !b_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_slice_dot: null pointer");
     if (nz == 0 || nz > 65535 || nproj * nu > 0x7fffffff) return fail(MR_ERR_ARGUMENT, "mr_slice_dot: unsupported size");
     k_slice_dot<<<static_cast<unsigned>(nz), 512, 0, as_stream(stream)>>>(a_d, b_d, static_cast<int>(nproj),

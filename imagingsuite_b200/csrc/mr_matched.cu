@@ -346,6 +346,7 @@ extern "C" {
 mr_status mr_mbp_geometry(const float *angles_h, size_t nproj, size_t n, size_t nz, float centre, float tan_tilt,
                           float pivot, int direction, float *sincos_h, float *startu_h)
 {
+    MR_TRACE();
     if (nproj && (!angles_h || !sincos_h || !startu_h)) return fail(MR_ERR_ARGUMENT, "mr_mbp_geometry: null pointer");
     if (n < 2) return fail(MR_ERR_ARGUMENT, "mr_mbp_geometry: n must be at least 2");
     // StdBackProjectorBase::Process 2D (StdBackProjectorBase.cpp:72-79) with the centre of slice z
@@ -367,6 +368,7 @@ mr_status mr_mbp_geometry(const float *angles_h, size_t nproj, size_t n, size_t 
 mr_status mr_mbp_adjoint(const float *proj_d, size_t n, size_t nz, const float *sincos_d, const float *startu_d,
                          size_t nproj, const uint32_t *mask_d, int accumulate, float *vol_d, void *stream)
 {
+    MR_TRACE();
     if (!proj_d || !sincos_d || !startu_d || !mask_d || !vol_d) return fail(MR_ERR_ARGUMENT, "mr_mbp_adjoint: null pointer");
     if (n < 2 || n > 65536 || nz == 0 || nz > 65536 || nproj > 0x7fffffff)
         return fail(MR_ERR_ARGUMENT, "mr_mbp_adjoint: unsupported size");
@@ -381,6 +383,7 @@ mr_status mr_mbp_adjoint(const float *proj_d, size_t n, size_t nz, const float *
 mr_status mr_mbp_forward(const float *vol_d, size_t n, size_t nz, const float *sincos_d, const float *startu_d,
                          size_t nproj, const uint32_t *mask_d, float *proj_d, float *dproj_d, void *stream)
 {
+    MR_TRACE();
     if (!vol_d || !sincos_d || !startu_d || !mask_d || !proj_d) return fail(MR_ERR_ARGUMENT, "mr_mbp_forward: null pointer");
     if (n < 2 || n > 65536 || nz == 0 || nz > 65536 || nproj == 0 || nproj > 65535)
         return fail(MR_ERR_ARGUMENT, "mr_mbp_forward: unsupported size");

@@ -45,6 +45,7 @@ using namespace mr;
 
 extern "C" mr_status mr_measure_smem(double *wavefronts_per_s, double *bytes_per_s)
 {
+    MR_TRACE();
     if (!wavefronts_per_s || !bytes_per_s) return fail(MR_ERR_ARGUMENT, "mr_measure_smem: null pointer");
     int dev = 0, sms = 0;
     MR_CUDA_TRY(cudaGetDevice(&dev));

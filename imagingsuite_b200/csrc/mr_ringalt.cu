@@ -453,6 +453,7 @@ extern "C" {
 mr_status mr_median_filter(const float *img_d, size_t nu, size_t nv, size_t nimg, int kx, int ky, float *out_d,
                            void *stream)
 {
+    MR_TRACE();
     if (!img_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_median_filter: null pointer");
     if (kx < 1 || ky < 1 || kx > 5 || ky > 5 || !(kx & 1) || !(ky & 1))
         return fail(MR_ERR_UNSUPPORTED, "mr_median_filter: kernel %dx%d (odd sizes up to 5)", kx, ky);
@@ -466,6 +467,7 @@ mr_status mr_median_filter(const float *img_d, size_t nu, size_t nv, size_t nimg
 
 mr_status mr_sigmoid_lut(size_t len, float lambda, float sigma, float *lut_h, float *param_h)
 {
+    MR_TRACE();
     if (!lut_h || !param_h) return fail(MR_ERR_ARGUMENT, "mr_sigmoid_lut: null pointer");
     if (len < 2) return fail(MR_ERR_ARGUMENT, "mr_sigmoid_lut: at least two entries");
     if (!(sigma > 0.0f) || !std::isfinite(sigma) || !std::isfinite(lambda))
@@ -476,6 +478,7 @@ mr_status mr_sigmoid_lut(size_t len, float lambda, float sigma, float *lut_h, fl
 
 mr_status mr_basicringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, void *stream)
 {
+    MR_TRACE();
     if (!proj_d) return fail(MR_ERR_ARGUMENT, "mr_basicringclean: null pointer");
     if (!median_size_ok(nu, nv, 3, 3))
         return fail(MR_ERR_ARGUMENT, "mr_basicringclean: projections of %zux%zu (at least 2x2)", nu, nv);
@@ -483,8 +486,7 @@ mr_status mr_basicringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, v
     cudaStream_t s = as_stream(stream);
     const size_t npix = nu * nv;
     float *work = nullptr;
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&work, 2 * npix * sizeof(float), s));
+    MR_TRY(device_alloc(&work, 2 * npix * sizeof(float), s, "mr_basicringclean: scratch"));
     float *mean = work, *diff = work + npix;
     mr_status st = mean_projection(proj_d, npix, nproj, 0, mean, s);
     if (st == MR_OK)
@@ -507,6 +509,7 @@ mr_status mr_basicringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, v
 mr_status mr_medianmixringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, float threshold, float width,
                                 void *stream)
 {
+    MR_TRACE();
     if (!proj_d) return fail(MR_ERR_ARGUMENT, "mr_medianmixringclean: null pointer");
     const int pky = nv < 3 ? 1 : 3, pkx = nv < 3 ? 5 : 3, mky = nv < 5 ? 1 : 5;
     if (!median_size_ok(nu, nv, pkx, pky) || !median_size_ok(nu, nv, 5, mky))
@@ -521,8 +524,7 @@ mr_status mr_medianmixringclean(float *proj_d, size_t nu, size_t nv, size_t npro
     // batch of projections filtered out of place: about 512 MiB
     const size_t batch = std::max<size_t>(1, std::min<size_t>(nproj, (size_t(1) << 27) / npix));
     float *work = nullptr;
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&work, (2 * npix + len + 4 + batch * npix) * sizeof(float), s));
+    MR_TRY(device_alloc(&work, (2 * npix + len + 4 + batch * npix) * sizeof(float), s, "mr_medianmixringclean: scratch"));
     float *mean = work, *wt = work + npix, *lut = work + 2 * npix, *out = lut + len + 4;
     mr_status st = MR_OK;
     cudaError_t e = cudaMemcpyAsync(lut, table.data(), table.size() * sizeof(float), cudaMemcpyHostToDevice, s);

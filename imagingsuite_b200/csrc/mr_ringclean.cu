@@ -489,8 +489,7 @@ static mr_status run_stripes(float *data_d, bool interleaved, size_t nu, size_t 
     size_t total = 4 * P.K;
     for (int l = 0; l < P.levels; ++l) total += P.nfft[l] * 2 + P.nfft[l];
     total += stripe_scratch(P, nb) + (interleaved ? static_cast<size_t>(nb) * nu * ntheta : 0);
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&work, total * sizeof(float), s));
+    MR_TRY(device_alloc(&work, total * sizeof(float), s, "stripe filter: scratch"));
     size_t off = 0;
     taps_d = work;
     off += 4 * P.K;
@@ -546,6 +545,7 @@ extern "C" {
 
 mr_status mr_wavelet_kernel(const char *wname, int *begin, int *end, float *taps_h)
 {
+    MR_TRACE();
     if (!begin || !end) return fail(MR_ERR_ARGUMENT, "mr_wavelet_kernel: null pointer");
     std::vector<float> t;
     mr_status st = wavelet_taps(wname, begin, end, t);
@@ -556,6 +556,7 @@ mr_status mr_wavelet_kernel(const char *wname, int *begin, int *end, float *taps
 mr_status mr_stripefilter(float *sino_d, size_t nu, size_t ntheta, size_t nsino, const char *wname, int decnum,
                           float sigma, void *stream)
 {
+    MR_TRACE();
     if (!sino_d) return fail(MR_ERR_ARGUMENT, "mr_stripefilter: null pointer");
     if (nsino == 0) return MR_OK;
     return run_stripes(sino_d, false, nu, nsino, ntheta, wname, decnum, sigma, stream);
@@ -564,6 +565,7 @@ mr_status mr_stripefilter(float *sino_d, size_t nu, size_t ntheta, size_t nsino,
 mr_status mr_waveletringclean(float *proj_d, size_t nu, size_t nv, size_t nproj, const char *wname, int decnum,
                               float sigma, void *stream)
 {
+    MR_TRACE();
     if (!proj_d) return fail(MR_ERR_ARGUMENT, "mr_waveletringclean: null pointer");
     if (nv == 0) return MR_OK;
     return run_stripes(proj_d, true, nu, nv, nproj, wname, decnum, sigma, stream);

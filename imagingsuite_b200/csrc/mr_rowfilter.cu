@@ -227,8 +227,7 @@ mr_status quantize_projections(const float *x_d, size_t per, size_t nproj, int k
                                cudaStream_t s)
 {
     float *amax = nullptr, *inv = nullptr;
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&amax, 2 * nproj * sizeof(float), s));
+    MR_TRY(device_alloc(&amax, 2 * nproj * sizeof(float), s, "16-bit quantisation: scratch"));
     inv = amax + nproj;
     mr_status st = MR_OK;
     if (cudaMemsetAsync(amax, 0, nproj * sizeof(float), s) != cudaSuccess) st = fail(MR_ERR_CUDA, "memset");
@@ -308,6 +307,7 @@ mr_status mr_projfilter_tables(size_t nu, const char *filtertype, float cutoff, 
                                float biasweight, int paddingdoubler, size_t *nfft_out, size_t *ninsert_out,
                                float *filter_h, float *pad_h)
 {
+    MR_TRACE();
     if (!filtertype) return fail(MR_ERR_ARGUMENT, "mr_projfilter_tables: null filter type");
     if (nu < 2) return fail(MR_ERR_ARGUMENT, "mr_projfilter_tables: row length must be at least 2");
     if (paddingdoubler < 0 || paddingdoubler > 4) return fail(MR_ERR_ARGUMENT, "mr_projfilter_tables: paddingdoubler out of range");
@@ -362,6 +362,7 @@ mr_status mr_projfilter_tables(size_t nu, const char *filtertype, float cutoff, 
 mr_status mr_projfilter_create(size_t nu, const char *filtertype, float cutoff, float order, int usebias,
                                float biasweight, int paddingdoubler, mr_filter_plan **plan)
 {
+    MR_TRACE();
     if (!plan) return fail(MR_ERR_ARGUMENT, "mr_projfilter_create: null pointer");
     *plan = nullptr;
     size_t nfft = 0, ins = 0;
@@ -385,10 +386,15 @@ mr_status mr_projfilter_create(size_t nu, const char *filtertype, float cutoff, 
     p->ninsert = ins;
     p->filter = filter;
     p->pad = pad;
-    cudaError_t err = cudaMalloc(&p->twiddle_d, tw.size() * sizeof(float2));
-    if (err == cudaSuccess) err = cudaMalloc(&p->response_d, nfft * sizeof(float));
-    if (err == cudaSuccess) err = cudaMalloc(&p->pad_d, std::max<size_t>(ins, 1) * sizeof(float));
-    if (err == cudaSuccess) err = cudaMemcpy(p->twiddle_d, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    mr_status ast = device_alloc_sync(&p->twiddle_d, tw.size() * sizeof(float2), "mr_projfilter_create: twiddles");
+    if (ast == MR_OK) ast = device_alloc_sync(&p->response_d, nfft * sizeof(float), "mr_projfilter_create: response");
+    if (ast == MR_OK)
+        ast = device_alloc_sync(&p->pad_d, std::max<size_t>(ins, 1) * sizeof(float), "mr_projfilter_create: pad");
+    if (ast != MR_OK) {
+        mr_projfilter_destroy(p);
+        return ast;
+    }
+    cudaError_t err = cudaMemcpy(p->twiddle_d, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
     if (err == cudaSuccess) err = cudaMemcpy(p->response_d, resp.data(), nfft * sizeof(float), cudaMemcpyHostToDevice);
     if (err == cudaSuccess && ins)
         err = cudaMemcpy(p->pad_d, pad.data(), ins * sizeof(float), cudaMemcpyHostToDevice);
@@ -402,6 +408,7 @@ mr_status mr_projfilter_create(size_t nu, const char *filtertype, float cutoff, 
 
 mr_status mr_projfilter_destroy(mr_filter_plan *plan)
 {
+    MR_TRACE();
     if (!plan) return MR_OK;
     cudaFree(plan->twiddle_d);
     cudaFree(plan->response_d);
@@ -412,6 +419,7 @@ mr_status mr_projfilter_destroy(mr_filter_plan *plan)
 
 mr_status mr_projfilter_info(const mr_filter_plan *plan, size_t *nfft, size_t *ninsert, float *filter_h, float *pad_h)
 {
+    MR_TRACE();
     if (!plan) return fail(MR_ERR_ARGUMENT, "mr_projfilter_info: null plan");
     if (nfft) *nfft = plan->nfft;
     if (ninsert) *ninsert = plan->ninsert;
@@ -423,6 +431,7 @@ mr_status mr_projfilter_info(const mr_filter_plan *plan, size_t *nfft, size_t *n
 mr_status mr_projfilter_apply(const mr_filter_plan *plan, const float *in_d, float *out_d, size_t nrows,
                               const float *row_weight_d, size_t rows_per_weight, void *stream)
 {
+    MR_TRACE();
     if (!plan || !in_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_projfilter_apply: null pointer");
     if (row_weight_d && rows_per_weight == 0) return fail(MR_ERR_ARGUMENT, "mr_projfilter_apply: rows_per_weight is 0");
     RowFilterArgs a{};
@@ -448,6 +457,7 @@ mr_status mr_projfilter_apply(const mr_filter_plan *plan, const float *in_d, flo
 mr_status mr_quantize(const float *in_d, size_t per, size_t nproj, int dtype, uint16_t *out_d, float *scale_d,
                       void *stream)
 {
+    MR_TRACE();
     if (!in_d || !out_d || !scale_d) return fail(MR_ERR_ARGUMENT, "mr_quantize: null pointer");
     if (dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_quantize: dtype must be bf16 or f16");
     if (nproj > 65535) return fail(MR_ERR_ARGUMENT, "mr_quantize: more than 65535 projections per call");
@@ -458,6 +468,7 @@ mr_status mr_quantize(const float *in_d, size_t per, size_t nproj, int dtype, ui
 mr_status mr_quantize_noalloc(const float *in_d, size_t per, size_t nproj, int dtype, uint16_t *out_d, float *scale_d,
                               void *stream)
 {
+    MR_TRACE();
     if (!in_d || !out_d || !scale_d) return fail(MR_ERR_ARGUMENT, "mr_quantize_noalloc: null pointer");
     if (dtype != MR_BF16 && dtype != MR_F16) return fail(MR_ERR_ARGUMENT, "mr_quantize_noalloc: dtype must be bf16 or f16");
     if (nproj > kQuantScratchMax)
@@ -496,6 +507,7 @@ mr_status mr_quantize_noalloc(const float *in_d, size_t per, size_t nproj, int d
 mr_status mr_fdk_filter(const float *in_d, size_t nu, size_t nv, size_t nproj, const float *weight_d, float sad_sid_2,
                         float scale, int out_dtype, void *out_d, float *scale_out_d, void *stream)
 {
+    MR_TRACE();
     return mr_fdk_filter_rows(in_d, nu, nv, 0, nv, nproj, weight_d, sad_sid_2, scale, out_dtype, out_d, scale_out_d,
                               stream);
 }
@@ -504,6 +516,7 @@ mr_status mr_fdk_filter_rows(const float *in_d, size_t nu, size_t nrows, size_t 
                              const float *weight_d, float sad_sid_2, float scale, int out_dtype, void *out_d,
                              float *scale_out_d, void *stream)
 {
+    MR_TRACE();
     if (!in_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: null pointer");
     if (nv < 11) return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: the edge-row replication needs at least 11 rows");
     if (nrows == 0 || row0 + nrows > nv) return fail(MR_ERR_ARGUMENT, "mr_fdk_filter: row window outside the detector");
@@ -536,12 +549,9 @@ mr_status mr_fdk_filter_rows(const float *in_d, size_t nu, size_t nrows, size_t 
     float *tmp = nullptr;
     mr_status st = MR_OK;
     const size_t total = nu * nv * nproj;
-    keep_pool_memory();
-    if (cudaMallocAsync(&tw_d, tw.size() * sizeof(float2), s) != cudaSuccess ||
-        cudaMallocAsync(&resp_d, padwidth * sizeof(float), s) != cudaSuccess)
-        st = fail(MR_ERR_ALLOCATION, "mr_fdk_filter: tables");
-    if (st == MR_OK && out_dtype != MR_F32 && cudaMallocAsync(&tmp, total * sizeof(float), s) != cudaSuccess)
-        st = fail(MR_ERR_ALLOCATION, "mr_fdk_filter: f32 staging buffer");
+    st = device_alloc(&tw_d, tw.size() * sizeof(float2), s, "mr_fdk_filter: twiddles");
+    if (st == MR_OK) st = device_alloc(&resp_d, padwidth * sizeof(float), s, "mr_fdk_filter: response");
+    if (st == MR_OK && out_dtype != MR_F32) st = device_alloc(&tmp, total * sizeof(float), s, "mr_fdk_filter: f32 staging buffer");
     if (st == MR_OK) {
         if (cudaMemcpyAsync(tw_d, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice, s) != cudaSuccess ||
             cudaMemcpyAsync(resp_d, ramp.data(), padwidth * sizeof(float), cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -573,8 +583,8 @@ mr_status mr_fdk_filter_rows(const float *in_d, size_t nu, size_t nrows, size_t 
         st = quantize_projections(tmp, nu * nv, nproj, out_dtype, static_cast<uint16_t *>(out_d), scale_out_d, s);
     // pageable-host uploads above are synchronous with respect to the host buffers, so the
     // vectors may go out of scope; device tables are released in stream order
-    cudaFreeAsync(tw_d, s);
-    cudaFreeAsync(resp_d, s);
+    if (tw_d) cudaFreeAsync(tw_d, s);
+    if (resp_d) cudaFreeAsync(resp_d, s);
     if (tmp) cudaFreeAsync(tmp, s);
     return st;
 }

@@ -91,6 +91,7 @@ extern "C" mr_status mr_slices_u16(const float *vol_d, int plane, size_t d0, siz
                                    size_t count, const size_t *roi_h, float lo, float hi, uint16_t *out_d,
                                    void *stream)
 {
+    MR_TRACE();
     if (!vol_d || !out_d) return fail(MR_ERR_ARGUMENT, "mr_slices_u16: null pointer");
     if (plane != MR_PLANE_XY && plane != MR_PLANE_YZ) return fail(MR_ERR_ARGUMENT, "mr_slices_u16: plane");
     if (d0 == 0 || d1 == 0 || d2 == 0 || d0 > 65535 || d1 > 65535 || d2 > 65535)

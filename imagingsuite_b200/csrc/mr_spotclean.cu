@@ -679,6 +679,7 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
                             const float *th_h, const float *sigma_h, int edge, int clamp, float minlevel,
                             float maxlevel, int removeinfnan, void *stream)
 {
+    MR_TRACE();
     if (!proj_d || !th_h || !sigma_h) return fail(MR_ERR_ARGUMENT, "mr_morphspotclean: null pointer");
     if (detect < 0 || detect > 2) return fail(MR_ERR_ARGUMENT, "Unkown detection method selected");
     if (nv < 5) return fail(MR_ERR_ARGUMENT, "mr_morphspotclean: images need at least 5 rows (the edge padding mirrors 5 rows)");
@@ -699,8 +700,7 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     const size_t budget = std::max<size_t>(size_t(1) << 30, free_b / 4);
     const size_t batch = std::max<size_t>(1, std::min<size_t>(nproj, budget / per_img));
     float *scratch = nullptr;
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&scratch, batch * per_img + 4 * batch * sizeof(float), s));
+    MR_TRY(device_alloc(&scratch, batch * per_img + 4 * batch * sizeof(float), s, "mr_morphspotclean: scratch"));
     float *P = scratch, *H = P + batch * n, *K = H + batch * n, *stats = K + batch * n;
     float *fmax = stats, *mn = stats + batch, *mx = stats + 2 * batch;
     int *lists = reinterpret_cast<int *>(stats + 4 * batch);

@@ -441,6 +441,7 @@ extern "C" mr_status mr_spotclean2(float *proj_d, size_t nu, size_t nv, size_t n
                                    float sigma, int iterations, float minlevel, float maxlevel, int maxarea,
                                    void *stream)
 {
+    MR_TRACE();
     using namespace spot2;
     if (!proj_d) return fail(MR_ERR_ARGUMENT, "mr_spotclean2: null pointer");
     if (nu < 16 || nv < 16 || nu * nv > (size_t(1) << 31) - 1)
@@ -464,8 +465,7 @@ extern "C" mr_status mr_spotclean2(float *proj_d, size_t nu, size_t nv, size_t n
                          static_cast<size_t>(batch) * (4 * sizeof(int) + sizeof(float)) +
                          static_cast<size_t>(batch) * (kStatBlocks + 1) * sizeof(double);
     char *work = nullptr;
-    keep_pool_memory();
-    MR_CUDA_TRY(cudaMallocAsync(&work, bytes, s));
+    MR_TRY(device_alloc(&work, bytes, s, "mr_spotclean2: scratch"));
     double *stats = reinterpret_cast<double *>(work);
     float *lut = reinterpret_cast<float *>(stats + static_cast<size_t>(batch) * (kStatBlocks + 1));
     float *X0 = lut + len + 4;

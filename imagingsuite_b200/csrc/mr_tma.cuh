@@ -7,6 +7,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <mutex>
 
@@ -14,6 +15,10 @@ namespace mr {
 namespace tma {
 
 constexpr int kWaitLimit = 1 << 22; // bounded mbarrier waits (iterations)
+
+// Iteration limit of the staged kernels' per-batch waits, read by each launch (mr_set_wait_limit
+// changes it; the waits that drain copies in flight after an expiry keep kWaitLimit).
+inline std::atomic<int> g_batch_wait_limit{kWaitLimit};
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
@@ -31,11 +36,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
                  : "memory");
 }
 
-// Bounded wait on an mbarrier phase; false when the limit expired.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+// Bounded wait on an mbarrier phase; false when `limit` tries expired.
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, int limit = kWaitLimit)
 {
     const uint32_t a = smem_addr(bar);
-    for (int it = 0; it < kWaitLimit; ++it) {
+    for (int it = 0; it < limit; ++it) {
         uint32_t ok;
         asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
                      "selp.u32 %0, 1, 0, p;\n\t}"

@@ -16,6 +16,8 @@ MultiProjectionBPparallel, which skips the last projection of every full buffer)
 from __future__ import annotations
 
 import ctypes
+import functools
+import logging
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -27,6 +29,46 @@ from ._lib import check
 
 class ReconException(RuntimeError):
     """Mirror of ReconException (frameworks/tomography/Framework/ReconFramework/include/ReconException.h)."""
+
+
+class LibraryFailure(ReconException, L.MrError):
+    """A failed library call inside a module: a ReconException to the engine (as the reference's
+    modules raise it, ReconEngine.cpp:810-833) that keeps the library's status code."""
+
+    def __init__(self, where: str, err: L.MrError):
+        L.MrError.__init__(self, err.status, f"{where}: {getattr(err, 'message', err)}")
+
+
+_MODULE_CALLS = ("Configure", "SetROI", "SetReferenceImages", "Process", "ProcessCore", "GetSlice")
+
+
+def _module(cls):
+    """Class decorator of the modules: each of their public calls runs inside an NVTX range
+    '<module>.<call>' (the reference times every Process, ProcessModuleBase.cpp:129-149) and
+    turns a library failure into LibraryFailure."""
+    for name in _MODULE_CALLS:
+        fn = cls.__dict__.get(name)
+        if fn is not None:
+            setattr(cls, name, _module_call(fn, name))
+    return cls
+
+
+def _module_call(fn, call: str):
+    @functools.wraps(fn)
+    def run(self, *args, **kwargs):
+        lib = L.lib()
+        where = f"{type(self).__name__}.{call}"
+        lib.mr_trace_push(where.encode())
+        try:
+            return fn(self, *args, **kwargs)
+        except LibraryFailure:
+            raise
+        except L.MrError as e:
+            raise LibraryFailure(where, e) from e
+        finally:
+            lib.mr_trace_pop()
+
+    return run
 
 
 # ---------------------------------------------------------------------------- config
@@ -64,9 +106,36 @@ class MatrixInfo:
 
 
 @dataclass
+class SystemInfo:
+    """Subset of ReconConfig::cSystem (ReconConfig.cpp:245-255,552): bValidateData turns on the
+    engine's NaN/infinity count after each module (ReconEngine::validateImage)."""
+
+    bValidateData: bool = False
+
+
+@dataclass
 class ReconConfig:
     ProjectionInfo: ProjectionInfo = field(default_factory=ProjectionInfo)
     MatrixInfo: MatrixInfo = field(default_factory=MatrixInfo)
+    System: SystemInfo = field(default_factory=SystemInfo)
+
+
+logger = logging.getLogger("imagingsuite_b200")
+
+
+def validate_image(data: torch.Tensor, description: str) -> int:
+    """ReconEngine::validateImage (ReconEngine.cpp:1724-1740): counts the NaNs and infinities of
+    a float tensor on the device (mr_data_validator) and logs the engine's warning when there
+    are any. Returns their number (reads it back, so the current stream is synchronised)."""
+    _require_cuda(data, "data")
+    if data.dtype != torch.float32:
+        raise ReconException("validate_image: float32 data expected")
+    counts = torch.empty(2, dtype=torch.int64, device=data.device)
+    check(L.lib().mr_data_validator(data.data_ptr(), data.numel(), counts.data_ptr(), _stream()))
+    nan, inf = (int(v) for v in counts.cpu())
+    if nan or inf:
+        logger.warning("Encountered %d infs and %d NaNs in %s", inf, nan, description)
+    return nan + inf
 
 
 def _string2bool(s: str) -> bool:
@@ -117,6 +186,7 @@ _AVERAGE = {"imagesum": 0, "imageaverage": 1, "imagemedian": 2, "imageweightedav
 # ------------------------------------------------------------------------ FullLogNorm
 
 
+@_module
 class FullLogNorm:
     """FullLogNorm (frameworks/tomography/Preprocessing/StdPreprocModules/src/NormPlugins.cpp:243-552).
 
@@ -268,6 +338,7 @@ def morph_spot_clean(img: torch.Tensor, detect: int = 0, conn8: bool = True, th=
     return img
 
 
+@_module
 class MorphSpotCleanModule:
     """MorphSpotCleanModule (StdPreprocModules/src/MorphSpotCleanModule.cpp:14-183). As in
     the reference's single-threaded path (ProcessSingle :142-181) the cleaner runs with its
@@ -350,6 +421,7 @@ def stripe_filter(sino: torch.Tensor, wname: str = "daub15", decnum: int = 2, si
     return sino
 
 
+@_module
 class WaveletRingClean:
     """WaveletRingClean (StdPreprocModules/src/WaveletRingClean.cpp:17-146). As in the
     reference, `method` is read but every sinogram is filtered with VerticalComponentFFT."""
@@ -388,8 +460,8 @@ class WaveletRingClean:
         st = L.lib().mr_waveletringclean(img.data_ptr(), nu, nv, nproj, self.m_sWName.encode(), self.m_nDecNum,
                                          self.m_fSigma, _stream())
         if st != L.MR_OK:
-            raise ReconException("Failed to process the projections using stripe filter: " +
-                                 L.lib().mr_last_error().decode())
+            raise LibraryFailure("Failed to process the projections using stripe filter",
+                                 L.MrError(st, L.lib().mr_last_error().decode()))
         return img
 
 
@@ -443,10 +515,11 @@ def median_filter(img: torch.Tensor, kx: int, ky: int) -> torch.Tensor:
     out = torch.empty_like(src)
     st = L.lib().mr_median_filter(src.data_ptr(), nu, nv, n, kx, ky, out.data_ptr(), _stream())
     if st != L.MR_OK:
-        raise ReconException("median filter failed: " + L.lib().mr_last_error().decode())
+        raise LibraryFailure("median filter failed", L.MrError(st, L.lib().mr_last_error().decode()))
     return out
 
 
+@_module
 class BasicRingClean:
     """BasicRingClean (StdPreprocModules/src/BasicRingClean.cpp:17-95): every projection minus
     (mean projection - its 3x3 median). No parameters. The reference also writes mean.tif,
@@ -472,10 +545,11 @@ class BasicRingClean:
         nproj, nv, nu = img.shape
         st = L.lib().mr_basicringclean(img.data_ptr(), nu, nv, nproj, _stream())
         if st != L.MR_OK:
-            raise ReconException("BasicRingClean failed: " + L.lib().mr_last_error().decode())
+            raise LibraryFailure("BasicRingClean failed", L.MrError(st, L.lib().mr_last_error().decode()))
         return img
 
 
+@_module
 class MedianMixRingClean:
     """MedianMixRingClean (StdPreprocModules/src/MedianMixRingClean.cpp:21-138): weights from
     a sigmoid of |mean projection - its 3x3 median| (threshold = sigmoid level, width = sigmoid
@@ -504,13 +578,14 @@ class MedianMixRingClean:
         nproj, nv, nu = img.shape
         st = L.lib().mr_medianmixringclean(img.data_ptr(), nu, nv, nproj, self.m_fLambda, self.m_fSigma, _stream())
         if st != L.MR_OK:
-            raise ReconException("MedianMixRingClean failed: " + L.lib().mr_last_error().decode())
+            raise LibraryFailure("MedianMixRingClean failed", L.MrError(st, L.lib().mr_last_error().decode()))
         return img
 
 
 _SPOT_METHODS = {"stddev": 0, "ring": 1, "median": 2, "minmax": 3, "trikernel": 4}
 
 
+@_module
 class SpotClean2:
     """SpotClean2 (StdPreprocModules/src/SpotClean2.cpp:42-130) over ImagingAlgorithms::SpotClean
     (core/algorithms/ImagingAlgorithms/src/SpotClean.cpp): detection image, sigmoid weights
@@ -559,10 +634,11 @@ class SpotClean2:
                                    self.m_fGamma, self.m_fSigma, iters, self.m_fMinLevel,
                                    self.m_fMaxLevel, self.m_nMaxArea, _stream())
         if st != L.MR_OK:
-            raise ReconException("SpotClean2 failed: " + L.lib().mr_last_error().decode())
+            raise LibraryFailure("SpotClean2 failed", L.MrError(st, L.lib().mr_last_error().decode()))
         return img
 
 
+@_module
 class GammaSpotClean:
     """GammaSpotCleanModule (StdPreprocModules/src/GammaSpotCleanModule.cpp:10-153). The
     reference keeps the parameters but its ProcessCore returns without touching the
@@ -603,6 +679,7 @@ class GammaSpotClean:
 # ------------------------------------------------------------ ProjectionFilterSingle
 
 
+@_module
 class ProjectionFilterSingle:
     """ProjectionFilterSingle (StdPreprocModules/src/ProjectionFilter.cpp:230-376)."""
 
@@ -643,7 +720,7 @@ class ProjectionFilterSingle:
                                           int(self.m_bUseBias), self.m_fBiasWeight, self.m_nPaddingDoubler,
                                           ctypes.byref(plan))
         if st != L.MR_OK:
-            raise ReconException(L.lib().mr_last_error().decode())
+            raise LibraryFailure(type(self).__name__, L.MrError(st, L.lib().mr_last_error().decode()))
         self._plan = plan
 
     def GetParameters(self) -> dict:
@@ -684,6 +761,7 @@ class ProjectionFilterSingle:
 # --------------------------------------------------------------- backprojector base
 
 
+@_module
 class _BackProjectorBase:
     def __init__(self, name: str):
         self.m_sModuleName = name
@@ -755,15 +833,23 @@ def TransferMatrix(backprojector, volume: torch.Tensor, dims, first_slice: int =
     """ReconEngine::TransferMatrix (ReconEngine.cpp:531-574): the block's slices i = 0 ..
     dims[3] - dims[1] - 1 of the backprojector (GetSlice, with the matrix ROI) are copied into
     planes dims[1] - first_slice + i of the engine volume (planes, rows, columns). Errors of
-    GetSlice are re-raised with the reference's context."""
+    GetSlice are re-raised with the reference's context; so is a device error word left by a
+    bounded wait that expired in the block's backprojection (the first point at which the
+    block's volume is read back)."""
     try:
+        vol = getattr(backprojector, "volume", None)
+        if isinstance(vol, torch.Tensor) and vol.is_cuda:
+            L.check_device()
         for i in range(int(dims[3]) - int(dims[1])):
             volume[int(dims[1]) - first_slice + i].copy_(backprojector.GetSlice(i))
+    except L.MrError as e:
+        raise LibraryFailure("Transfer matrix from backprojector failed with ReconException", e) from e
     except ReconException as e:
         raise ReconException(f"Transfer matrix from backprojector failed with ReconException\n{e}") from e
     return False
 
 
+@_module
 class MultiProjectionBPparallel(_BackProjectorBase):
     """MultiProjectionBPparallel (StdBackProjectors/src/MultiProjBPparallel.cpp) with the
     StdBackProjectorBase driver (StdBackProjectorBase.cpp). Volume is MatrixZXY:
@@ -880,6 +966,7 @@ class MultiProjectionBPparallel(_BackProjectorBase):
         return self.volume.shape[2]
 
 
+@_module
 class MultiProjectionBP(MultiProjectionBPparallel):
     """MultiProjectionBP, the reference's serial backprojector (factory name "MultiProjBP",
     StdBackProjectors/src/MultiProjBP.cpp:36-146). Without tilt correction it computes exactly
@@ -896,6 +983,7 @@ class MultiProjectionBP(MultiProjectionBPparallel):
         self.m_sModuleName = "Multi projection BP"
 
 
+@_module
 class NearestNeighborBP(MultiProjectionBPparallel):
     """NearestNeighborBP (factory name "NNMultiProjBP", StdBackProjectors/src/NNMultiProjBP.cpp:
     36-121): the same positions as MultiProjectionBP, each voxel adding the one sample at the
@@ -910,6 +998,7 @@ class NearestNeighborBP(MultiProjectionBPparallel):
         self.m_sModuleName = "NearestNeighborBP"
 
 
+@_module
 class FDKbp_single(_BackProjectorBase):
     """FDKbp_single (FDKBackProjectors/src/fdkbp_single.cpp) with the FdkReconBase driver
     (fdkreconbase.cpp). Volume is MatrixXYZ: tensor (nz, ny, nx) = (nv, nu, nu), x fastest."""

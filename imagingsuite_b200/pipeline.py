@@ -22,6 +22,15 @@ def _text(a) -> str:
     return " ".join("%.9g" % v for v in np.asarray(a, np.float32))
 
 
+def _check_device(where: str) -> None:
+    from . import _lib as L
+
+    try:
+        L.check_device()
+    except L.MrError as e:
+        raise M.LibraryFailure(where, e) from e
+
+
 class FdkPipeline:
     def __init__(self, config: M.ReconConfig, angles, weights, darks: torch.Tensor, flats: torch.Tensor,
                  precision: str = "fp32", norm_params: dict | None = None):
@@ -49,6 +58,12 @@ class FdkPipeline:
         proj = self.norm.ProcessCore(counts, {}) if counts.dtype == torch.float32 else self._lognorm_into(counts)
         self.fdk.Process(proj, self._params)
         return self.fdk.GetVolume()
+
+    @staticmethod
+    def check_device() -> None:
+        """Raises LibraryFailure (a ReconException) when a kernel of the finished work left the
+        device error word of an expired bounded wait; synchronises the device."""
+        _check_device("FdkPipeline")
 
     def _lognorm_into(self, counts, out=None):
         from . import _lib as L
@@ -207,8 +222,10 @@ class ParallelChain:
     fused) -> MultiProjectionBPparallel (weights not applied again)."""
 
     def __init__(self, norm: M.FullLogNorm, filt: M.ProjectionFilterSingle, bp: M.MultiProjectionBPparallel,
-                 angles, weights, spot: M.MorphSpotCleanModule | None = None, ring: M.WaveletRingClean | None = None):
+                 angles, weights, spot: M.MorphSpotCleanModule | None = None, ring: M.WaveletRingClean | None = None,
+                 validate: bool = False):
         self.norm, self.filt, self.bp, self.spot, self.ring = norm, filt, bp, spot, ring
+        self.validate = validate  # the engine's ReconConfig.System.bValidateData
         self.angles = np.asarray(angles, np.float32)
         self.weights = np.asarray(weights, np.float32)
         self._params = {"angles": _text(self.angles), "weights": _text(self.weights)}
@@ -220,17 +237,43 @@ class ParallelChain:
             self._w = torch.from_numpy(self.weights).to(device)
         return self._w
 
-    def run_device(self, counts: torch.Tensor) -> torch.Tensor:
-        """counts: uint16 (nproj, nv, nu) on the device. Returns the volume (ny, nx, nz)."""
+    def run_device(self, counts: torch.Tensor, progress=None) -> torch.Tensor | None:
+        """counts: uint16 (or float32) (nproj, nv, nu) on the device. Returns the volume
+        (ny, nx, nz).
+
+        progress(fraction, message) -> bool stands for InteractionBase::SetProgress: it is asked
+        before each module, as ReconEngine::Process3D does (ReconEngine.cpp:1283-1290), and a
+        True answer cancels the block between two modules (nothing of the block is left
+        running; returns None). With `validate` (System.bValidateData) the projections
+        are counted for NaNs and infinities after each preprocessing module and after the
+        backprojection (validate_image, which logs the engine's warning)."""
+        validate = self.validate
+        stages = ["FullLogNorm"] + (["MorphSpotClean"] if self.spot is not None else []) + \
+                 (["WaveletRingClean"] if self.ring is not None else []) + ["ProjectionFilterSingle", "BackProject"]
         self.bp.volume.zero_()
-        proj = self.norm.ProcessCore(counts, {})
-        if self.spot is not None:
-            self.spot.ProcessCore(proj, {})
-        if self.ring is not None:
-            self.ring.ProcessCore(proj, {})
-        self.filt.ProcessCore(proj, {}, weights=self._weights_on(counts.device))
-        self.bp.Process(proj, self._params, prefiltered_weights=True)
+        proj = None
+        for k, name in enumerate(stages):
+            if progress is not None and progress(k / len(stages), f"Processing: {name}"):
+                return None
+            if name == "FullLogNorm":
+                proj = self.norm.ProcessCore(counts, {})
+            elif name == "MorphSpotClean":
+                self.spot.ProcessCore(proj, {})
+            elif name == "WaveletRingClean":
+                self.ring.ProcessCore(proj, {})
+            elif name == "ProjectionFilterSingle":
+                self.filt.ProcessCore(proj, {}, weights=self._weights_on(counts.device))
+            else:
+                self.bp.Process(proj, self._params, prefiltered_weights=True)
+            if validate:
+                M.validate_image(proj, name if name != "BackProject" else "Projections post recon BackProject3D")
         return self.bp.GetVolume()
+
+    @staticmethod
+    def check_device() -> None:
+        """Raises LibraryFailure (a ReconException) when a kernel of the finished work left the
+        device error word of an expired bounded wait; synchronises the device."""
+        _check_device("ParallelChain")
 
     def run_host(self, counts_host: torch.Tensor, out_host: torch.Tensor, device, chunks: int = 2,
                  blocks: int = 8) -> torch.Tensor:

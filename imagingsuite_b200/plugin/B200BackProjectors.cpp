@@ -136,6 +136,7 @@ void MultiProjBPCUDA::backproject(const std::vector<Entry> &entries)
 // scan flushes what is buffered.
 size_t MultiProjBPCUDA::Process(kipl::base::TImage<float, 2> proj, float angle, float weight, bool bLastProjection)
 {
+    b200::Trace trace("MultiProjBPCUDA::Process");
     if (volume.Size() == 0) throw ReconException("The target matrix is not allocated.", __FILE__, __LINE__);
     const size_t per = SizeU * SizeV;
     if (proj.Size() != per) throw ReconException("The projection does not match the ROI", __FILE__, __LINE__);
@@ -160,6 +161,7 @@ size_t MultiProjBPCUDA::Process(kipl::base::TImage<float, 2> proj, float angle, 
 // through the 2D rule; the projections that rule backprojects go to the device in one call.
 size_t MultiProjBPCUDA::Process(kipl::base::TImage<float, 3> projections, std::map<std::string, std::string> parameters)
 {
+    b200::Trace trace("MultiProjBPCUDA::Process");
     if (volume.Size() == 0) throw ReconException("The target matrix is not allocated.", __FILE__, __LINE__);
     const size_t nProj = projections.Size(2), per = SizeU * SizeV;
     if (projections.Size(0) * projections.Size(1) != per)
@@ -286,6 +288,7 @@ void FDKbpCUDA::SetROI(size_t *roi)
 // projections weighted, ramp filtered and backprojected; every call adds into the volume.
 size_t FDKbpCUDA::Process(kipl::base::TImage<float, 3> projections, std::map<std::string, std::string> parameters)
 {
+    b200::Trace trace("FDKbpCUDA::Process");
     if (volume.Size() == 0) throw ReconException("The target matrix is not allocated.", __FILE__, __LINE__);
     const size_t nProj = projections.Size(2), nu = SizeU, nv = SizeV;
     if (projections.Size(0) != nu || projections.Size(1) != nv)

@@ -190,6 +190,7 @@ void FullLogNormCUDA::SetReferenceImages(kipl::base::TImage<float, 2> dark, kipl
 // FullLogNorm::ProcessCore 2D (NormPlugins.cpp:343-409): one projection, dose from coeff.
 int FullLogNormCUDA::ProcessCore(kipl::base::TImage<float, 2> &img, std::map<std::string, std::string> &coeff)
 {
+    b200::Trace trace("FullLogNormCUDA::ProcessCore");
     float dose = 1.0f;
     if (bUseNormROI) {
         dose = GetFloatParameter(coeff, "dose") - fDarkDose;
@@ -221,6 +222,7 @@ int FullLogNormCUDA::ProcessCore(kipl::base::TImage<float, 2> &img, std::map<std
 // FullLogNorm::ProcessCore 3D (NormPlugins.cpp:411-552)
 int FullLogNormCUDA::ProcessCore(kipl::base::TImage<float, 3> &img, std::map<std::string, std::string> &coeff)
 {
+    b200::Trace trace("FullLogNormCUDA::ProcessCore");
     int nDose = static_cast<int>(img.Size(2));
     std::vector<float> doselist(std::max(nDose, 1));
     if (bUseNormROI) {
@@ -367,6 +369,7 @@ void MorphSpotCleanCUDA::clean(float *img_h, size_t nu, size_t nv, size_t n, boo
 // (ProcessParallelStd, :226-269) sets neither.
 int MorphSpotCleanCUDA::ProcessCore(kipl::base::TImage<float, 3> &img, std::map<std::string, std::string> &coeff)
 {
+    b200::Trace trace("MorphSpotCleanCUDA::ProcessCore");
     (void)coeff;
     clean(img.GetDataPtr(), img.Size(0), img.Size(1), img.Size(2), m_bClampData && !m_bThreading, false);
     return 0;
@@ -375,6 +378,7 @@ int MorphSpotCleanCUDA::ProcessCore(kipl::base::TImage<float, 3> &img, std::map<
 // MorphSpotCleanModule::ProcessCore 2D (:112-148): limits and inf/NaN removal as configured
 int MorphSpotCleanCUDA::ProcessCore(kipl::base::TImage<float, 2> &img, std::map<std::string, std::string> &coeff)
 {
+    b200::Trace trace("MorphSpotCleanCUDA::ProcessCore");
     (void)coeff;
     clean(img.GetDataPtr(), img.Size(0), img.Size(1), 1, m_bClampData, m_bRemoveInfNaN);
     return 0;
@@ -423,6 +427,7 @@ bool WaveletRingCleanCUDA::SetROI(size_t *roi)
 // is always applied.
 int WaveletRingCleanCUDA::ProcessCore(kipl::base::TImage<float, 3> &img, std::map<std::string, std::string> &coeff)
 {
+    b200::Trace trace("WaveletRingCleanCUDA::ProcessCore");
     (void)coeff;
     const size_t total = img.Size();
     cudaStream_t s = stream.get();
@@ -515,6 +520,7 @@ void ProjectionFilterCUDA::filter(float *img_h, size_t nu, size_t rows)
 // ProjectionFilterBase::ProcessCore 2D/3D (ProjectionFilter.cpp:93-118)
 int ProjectionFilterCUDA::ProcessCore(kipl::base::TImage<float, 2> &img, std::map<std::string, std::string> &coeff)
 {
+    b200::Trace trace("ProjectionFilterCUDA::ProcessCore");
     (void)coeff;
     if (img.Size() == 0) throw ReconException("Empty projection image", __FILE__, __LINE__);
     filter(img.GetDataPtr(), img.Size(0), img.Size(1));
@@ -523,6 +529,7 @@ int ProjectionFilterCUDA::ProcessCore(kipl::base::TImage<float, 2> &img, std::ma
 
 int ProjectionFilterCUDA::ProcessCore(kipl::base::TImage<float, 3> &img, std::map<std::string, std::string> &coeff)
 {
+    b200::Trace trace("ProjectionFilterCUDA::ProcessCore");
     (void)coeff;
     if (img.Size() == 0) throw ReconException("Empty projection image", __FILE__, __LINE__);
     filter(img.GetDataPtr(), img.Size(0), img.Size(1) * img.Size(2));

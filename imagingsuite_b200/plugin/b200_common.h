@@ -111,6 +111,16 @@ inline void download(T *dst_h, const T *src_d, size_t count, cudaStream_t s)
     cuda_check(cudaMemcpyAsync(dst_h, src_d, count * sizeof(T), cudaMemcpyDeviceToHost, s), "device to host copy");
 }
 
+// NVTX range over a module call (mr_trace_push / mr_trace_pop of mrcuda): the engine's
+// per-module timer (ProcessModuleBase.cpp:129-149) as a range on the profiler's timeline.
+class Trace {
+public:
+    explicit Trace(const char *name) { mr_trace_push(name); }
+    ~Trace() { mr_trace_pop(); }
+    Trace(const Trace &) = delete;
+    Trace &operator=(const Trace &) = delete;
+};
+
 // Bounded device waits report through mrcuda's error word; a set word becomes an exception.
 inline void check_device(const char *what)
 {

@@ -482,6 +482,27 @@ mr_status mr_mbp_forward(const float *vol_d, size_t n, size_t nz, const float *s
  * synchronizes the device and clears the word. */
 mr_status mr_device_status(int *status);
 
+/* Failure detection and tracing (no counterpart in the reference, whose engine wraps module
+ * exceptions at each level, ReconEngine.cpp:810-833, and times modules with a CPU timer,
+ * ProcessModuleBase.cpp:129-149).
+ * mr_set_wait_limit: tries of each per-batch mbarrier wait in the TMA-staged backprojectors
+ *   (default 4194304; a negative value restores it), read at each launch. A wait that runs
+ *   out sets the device error word (mr_device_status returns 1), skips the rest of the block's
+ *   projections, waits for the block's copies still in flight (with the default limit) and
+ *   returns; the context stays usable. 0 makes every such wait expire at once.
+ * mr_debug_fail_allocation: the scratch allocation made after `after` further successful ones
+ *   fails with MR_ERR_ALLOCATION, once (a negative value disarms the hook). Process-wide.
+ * mr_trace_push / mr_trace_pop: an NVTX range on the calling thread (the host modules put one
+ *   around each Process; every entry point of this library opens one named after itself). */
+/* ReconEngine::validateImage (ReconEngine.cpp:1724-1740) over kipl::algorithms::dataValidator
+ * (datavalidator.h:8-19): counts_d[0] = NaNs and counts_d[1] = infinities (either sign) among
+ * the n floats at data_d. counts_d (device, two values) is zeroed first; asynchronous. */
+mr_status mr_data_validator(const float *data_d, size_t n, unsigned long long *counts_d, void *stream);
+mr_status mr_set_wait_limit(int tries);
+mr_status mr_debug_fail_allocation(long long after);
+mr_status mr_trace_push(const char *name);
+mr_status mr_trace_pop(void);
+
 /* Diagnostics (no counterpart in the reference): the measured shared-memory load rate of the
  * current device, the on-chip roofline of the staged backprojectors, which gather one 32-bit
  * sample per lane from shared memory. A conflict-free kernel with many loads in flight,
