@@ -40,7 +40,11 @@ METRIC = "backprojection GUPS + projections/s, FP32 vs BF16-proj at <=1e-3 rel R
 MEASURED_TRAFFIC = {1024: 553.50e9, 256: 111.7e6}
 
 
-def workload(small: bool):
+def workload(small: bool, c2: bool = False):
+    if c2:
+        # the plain FDK configuration: 720 projections over 360 deg on a 512 x 512 detector
+        return dict(name="FDK 512^3 from 720 projections of 512x512", nu=512, nv=512, nproj=720, sod=300.0,
+                    sdd=600.0, pitch=0.2, voxel=0.1, i0=50000.0)
     if small:
         return dict(name="FDK 256^3 from 256 projections of 256x256 (profiling case)", nu=256, nv=256, nproj=256,
                     sod=300.0, sdd=600.0, pitch=0.8, voxel=0.4, i0=50000.0)
@@ -200,7 +204,7 @@ def run_mr(args):
     backend = os.environ.get("MR_DIST_BACKEND", "nccl")
     dctx = DistContext(backend, device=device if backend == "nccl" else None) if world > 1 else None
     rank = dctx.rank if dctx else 0
-    w = workload(args.small)
+    w = workload(args.small, args.workload == "fdk-c2")
     nu, nv, nproj = w["nu"], w["nv"], w["nproj"]
     updates = float(nu) * nu * nv * nproj
 
@@ -511,29 +515,20 @@ def run_diff(args):
     return res
 
 
-def run_parallel(args, production: bool):
-    """Parallel-beam chains. C1 (production=False): 360 projections of 256 x 64 over 180 deg,
-    I0 3e4, 5 flats / 5 darks, FullLogNorm -> Hann ramp filter (cutoff 0.5) -> backprojection to
-    256 x 256 x 64, centre 127.5. C3 (production=True): 1125 projections of 2048 x 2048 over 180
-    deg, 20 flats / 10 darks, 0.05 % spot defects and 20 gain-error columns; one block of 512
-    detector rows (the slab the reference reconstructs per SliceBlock) through FullLogNorm ->
-    MorphSpotClean -> WaveletRingClean -> Hann filter -> backprojection to 2048 x 2048 x 512."""
-    import torch
-
+def parallel_inputs(production: bool, small: bool, dev):
+    """Seeded inputs of the parallel-beam workloads (C1, or the C3 block) and their
+    configuration: uint16 counts (nproj, nrows, nu), flats, darks on `dev`."""
     from imagingsuite_b200 import modules as M
-    from imagingsuite_b200 import phantom, pipeline
+    from imagingsuite_b200 import phantom
 
-    torch.cuda.set_device(0)
-    dev = torch.device("cuda", 0)
     if production:
         nu, nrows, nproj, nflat, ndark, i0 = 2048, 512, 1125, 20, 10, 3e4
-        if args.small:
+        if small:
             nu, nrows, nproj = 512, 128, 282
         name = f"C3 production block: {nproj} projections of {nu} x {nu} (block of {nrows} rows), spots + rings"
     else:
         nu, nrows, nproj, nflat, ndark, i0 = 256, 64, 360, 5, 5, 3e4
         name = f"C1 parallel FBP: {nproj} projections of {nu} x {nrows} -> {nu}x{nu}x{nrows}"
-    box = nu
     ells = phantom.ellipsoids(1000 + (3 if production else 1))
     v0 = (nu - nrows) // 2 if production else 0
     integ = phantom.parallel_integrals_torch(ells, nproj, nu, nrows, dev, box=float(nu) if production else None,
@@ -548,8 +543,104 @@ def run_parallel(args, production: bool):
     pi.roi = pi.projection_roi = (0, 0, nu, nrows)
     pi.nDims = (nu, nrows, nproj)
     pi.nOBCount, pi.nDCCount = nflat, ndark
-    angles = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
-    weights = np.full(nproj, np.float32(np.pi / nproj))
+    return {"nu": nu, "nrows": nrows, "nproj": nproj, "name": name, "counts": counts, "flats": flats, "darks": darks,
+            "cfg": cfg, "angles": (np.arange(nproj) * 180.0 / nproj).astype(np.float32),
+            "weights": np.full(nproj, np.float32(np.pi / nproj))}
+
+
+_SPOT_PARAMS = dict(connectivity="conn8", detectionmethod="morphdetectboth", threshold="0.1 0.1", sigma="0.01 0.01",
+                    edgesmooth=5, maxarea=30, removeinfnan=False, clampdata=False, minlevel=-0.1, maxlevel=12.0)
+
+
+def chain_cpu(P, production: bool, updates: float, sel: int):
+    """The reference's own modules (compiled from the reference sources, `oracle/_ref`) chained
+    on the host cores with all threads: FullLogNorm -> [MorphSpotCleanModule ->
+    WaveletRingClean] -> ProjectionFilterSingle -> MultiProjBPparallel.
+
+    C1: the whole workload. C3: the preprocessing modules on a sample of projections of the
+    block (per-projection cost), the backprojector into the full 2048 x 2048 x 512 volume with
+    2 and 6 projections (per-projection cost from the difference, fixed cost apart), scaled to
+    the block's projections. Returns the cpu_baseline object; value in the workload's GUPS."""
+    import oracle
+
+    cores = os.cpu_count() or 1
+    threads = os.environ.get("OMP_NUM_THREADS", str(cores))
+    if not oracle.ref_available():
+        return {"kind": "reference", "cores": 0, "value": None, "unit": "GUPS",
+                "sample": "reference library oracle/_ref/libmuhrec_ref.so not built"}
+    nu, nrows, nproj = P["nu"], P["nrows"], P["nproj"]
+    centre = P["cfg"].ProjectionInfo.fCenter
+    darks = P["darks"].cpu().numpy()
+    flats = P["flats"].cpu().numpy()
+    ang, wts = P["angles"], P["weights"]
+    if not production:
+        c = P["counts"].cpu().numpy().astype(np.float32)
+        t = {}
+        t0 = time.perf_counter()
+        p = oracle.ref_fulllognorm(c, darks, flats, "ImageAverage", False)[0]
+        t["FullLogNorm"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        p = oracle.ref_projfilter(p, "hanning", 0.5, 1.0, True, 0.1, 2)[0]
+        t["ProjectionFilterSingle"] = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        oracle.bp_parallel(p, ang, wts, centre, buffersize=16, use_ref=True)
+        t["MultiProjBPparallel"] = time.perf_counter() - t0
+        total = sum(t.values())
+        return {"kind": "reference", "cores": cores, "value": updates / total / 1e9, "unit": "GUPS",
+                "sample": f"the whole C1 workload through the reference modules (OMP_NUM_THREADS={threads})",
+                "module_s": t, "total_s": total}
+    k = 64  # projections through the preprocessing modules (the ring cleaner needs sinograms this tall)
+    c = P["counts"][:k].cpu().numpy().astype(np.float32)
+    per = {}
+    t0 = time.perf_counter()
+    p = oracle.ref_fulllognorm(c, darks, flats, "ImageAverage", False)[0]
+    per["FullLogNorm"] = (time.perf_counter() - t0) / k
+    t0 = time.perf_counter()
+    p = oracle.ref_morphspotclean_module(p, **_SPOT_PARAMS, threading=True)
+    per["MorphSpotCleanModule"] = (time.perf_counter() - t0) / k
+    t0 = time.perf_counter()
+    p = oracle.waveletringclean(p, "daub15", 2, 0.05, use_ref=True)
+    per["WaveletRingClean"] = (time.perf_counter() - t0) / k
+    t0 = time.perf_counter()
+    p = oracle.ref_projfilter(p, "hanning", 0.5, 1.0, True, 0.1, 2)[0]
+    per["ProjectionFilterSingle"] = (time.perf_counter() - t0) / k
+    n1, n2 = 2, 6
+    t0 = time.perf_counter()
+    oracle.bp_parallel(p[:n1], ang[:n1], wts[:n1], centre, buffersize=16, use_ref=True)
+    t1 = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    oracle.bp_parallel(p[:n2], ang[:n2], wts[:n2], centre, buffersize=16, use_ref=True)
+    t2 = time.perf_counter() - t0
+    per["MultiProjBPparallel"] = (t2 - t1) / (n2 - n1)
+    fixed = max(t1 - n1 * per["MultiProjBPparallel"], 0.0)
+    total = sum(v * nproj for k_, v in per.items() if k_ != "MultiProjBPparallel") + \
+        per["MultiProjBPparallel"] * sel + fixed
+    return {"kind": "reference", "cores": cores, "value": updates / total / 1e9, "unit": "GUPS",
+            "sample": f"preprocessing modules on {k} projections of the block, the backprojector into the full "
+                      f"{nu}x{nu}x{nrows} volume with {n1} and {n2} projections (per projection from the "
+                      f"difference), scaled to {nproj} projections ({sel} backprojected); "
+                      f"OMP_NUM_THREADS={threads}",
+            "s_per_projection": per, "bp_fixed_s": fixed, "estimated_block_s": total}
+
+
+def run_parallel(args, production: bool):
+    """Parallel-beam chains. C1 (production=False): 360 projections of 256 x 64 over 180 deg,
+    I0 3e4, 5 flats / 5 darks, FullLogNorm -> Hann ramp filter (cutoff 0.5) -> backprojection to
+    256 x 256 x 64, centre 127.5. C3 (production=True): 1125 projections of 2048 x 2048 over 180
+    deg, 20 flats / 10 darks, 0.05 % spot defects and 20 gain-error columns; one block of 512
+    detector rows (the slab the reference reconstructs per SliceBlock) through FullLogNorm ->
+    MorphSpotClean -> WaveletRingClean -> Hann filter -> backprojection to 2048 x 2048 x 512."""
+    import torch
+
+    from imagingsuite_b200 import modules as M
+    from imagingsuite_b200 import pipeline
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    P = parallel_inputs(production, args.small, dev)
+    nu, nrows, nproj, name = P["nu"], P["nrows"], P["nproj"], P["name"]
+    counts, flats, darks, cfg = P["counts"], P["flats"], P["darks"], P["cfg"]
+    angles, weights = P["angles"], P["weights"]
     norm = M.FullLogNorm()
     norm.Configure(cfg, {"usenormregion": "false", "uselut": "false", "referenceaverage": "ImageAverage"})
     norm.SetReferenceImages(darks, flats)
@@ -671,6 +762,7 @@ def run_parallel(args, production: bool):
     wfm, _bytes = ctypes.c_double(), ctypes.c_double()
     L.check(L.lib().mr_measure_smem(ctypes.byref(wfm), ctypes.byref(_bytes)))
     wf_peak = wfm.value
+    cpu = None if args.no_cpu_baseline else chain_cpu(P, production, updates, sel)
     return {"metric": "parallel-beam chain GUPS (voxel x projection updates per second)",
             "value": updates * args.steps / t / 1e9, "unit": "GUPS", "n_gpus": 1, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t / args.steps * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -692,6 +784,7 @@ def run_parallel(args, production: bool):
                        "peak_source": "measured on this GPU by mr_measure_smem (conflict-free 32-bit shared loads)"},
             "e2e": {"value": updates * e2e_steps / te / 1e9, "unit": "GUPS",
                     "h2d_bytes_per_step": int(counts.numel() * 2), "d2h_bytes_per_step": int(bp.volume.numel() * 4)},
+            **({"cpu_baseline": cpu} if cpu else {}),
             "clocks": clocks}
 
 
@@ -815,7 +908,7 @@ def run_reference(args):
         return None
     import oracle
 
-    w = workload(args.small)
+    w = workload(args.small, args.workload == "fdk-c2")
     if not oracle.ref_available():
         return {"impl": "reference", "unavailable": "reference library oracle/_ref/libmuhrec_ref.so not built"}
     nu, nv, nproj = w["nu"], w["nv"], w["nproj"]
@@ -855,6 +948,75 @@ def run_reference(args):
             "e2e": {"value": v, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def run_reference_chain(args, production: bool):
+    """Reference arm of the parallel-beam workloads: the reference's modules chained on the
+    host cores (chain_cpu) on this workload's inputs; rank 0 only under torchrun."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return None
+    import torch
+
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    P = parallel_inputs(production, args.small, dev)
+    nu, nrows, nproj = P["nu"], P["nrows"], P["nproj"]
+    k = np.arange(nproj)
+    sel = int(((k % 16) != 15).sum())  # StdBackProjectorBase drops the last entry of every full buffer of 16
+    updates = float(nu) * nu * (4 * (nrows // 4)) * sel
+    times = []
+    cpu = None
+    for _ in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        cpu = chain_cpu(P, production, updates, sel)
+        times.append(time.perf_counter() - t0)
+    if cpu.get("value") is None:
+        return {"impl": "reference", "unavailable": cpu["sample"]}
+    v = cpu["value"]
+    return {"impl": "reference", "metric": "parallel-beam chain GUPS (voxel x projection updates per second)",
+            "value": v, "unit": "GUPS", "n_gpus": world, "steps": len(times), "warmup": 0,
+            "ms_per_step": float(np.mean(times)) * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": {"workload": P["name"]},
+            "cpu_baseline": cpu, "e2e": {"value": v, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def run_reference_diff(args):
+    """Reference arm of the differentiation workload: the reference's own forward projector
+    (LinearForwardProjector, the Joseph anchor; the reference has no adjoint or gradient) on a
+    few slices of the 512 x 512 x 128 volume, 360 angles, one slice per call; GUPS of the forward
+    projection scaled from the slices timed."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and int(os.environ.get("RANK", "0")) != 0:
+        return None
+    import oracle
+
+    if not oracle.ref_available():
+        return {"impl": "reference", "unavailable": "reference library oracle/_ref/libmuhrec_ref.so not built"}
+    n, nproj, nslices = (128, 90, 32) if args.small else (512, 360, 128)
+    rng = np.random.default_rng(0)
+    ang = (np.arange(nproj) * 180.0 / nproj).astype(np.float32)
+    cores = os.cpu_count() or 1
+    k = min(64, 2 * cores)
+    sl = rng.random((k, n, n)).astype(np.float32)
+    from concurrent.futures import ThreadPoolExecutor
+
+    times = []
+    with ThreadPoolExecutor(max_workers=cores) as pool:  # one slice per call; ctypes releases the GIL
+        for _ in range(max(1, args.steps)):
+            t0 = time.perf_counter()
+            list(pool.map(lambda j: oracle.ref_joseph_project(sl[j], ang), range(k)))
+            times.append((time.perf_counter() - t0) / k)
+    per_slice = float(np.median(times))
+    v = float(n) * n * nproj / per_slice / 1e9
+    sample = (f"reference LinearForwardProjector (one slice per call) on {k} slices of {n} x {n}, {nproj} angles, "
+              f"{cores} slices at a time on {cores} host threads: {per_slice * 1e3:.2f} ms per slice (median of "
+              f"{len(times)} steps); the {nslices}-slice volume would take {per_slice * nslices:.2f} s")
+    return {"impl": "reference", "metric": "differentiable projector pair GUPS (voxel x projection, forward)",
+            "value": v, "unit": "GUPS", "n_gpus": world, "steps": len(times), "warmup": 0,
+            "ms_per_step": per_slice * k * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic", "config": {"workload": f"volume {n}x{n}x{nslices}, {nproj} projections"},
+            "cpu_baseline": {"value": v, "unit": "GUPS", "cores": cores, "kind": "reference", "sample": sample},
+            "e2e": {"value": v, "unit": "GUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -864,14 +1026,20 @@ def main():
     ap.add_argument("--small", action="store_true", help="256^3 profiling case")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
-    ap.add_argument("--workload", default="fdk", choices=["fdk", "diff", "parallel", "production"],
-                    help="fdk: FDK 1024^3 precision form (default); diff: Joseph pair + CGLS refinement; "
-                         "parallel: C1 parallel FBP; production: C3 preprocessing + parallel FBP block")
+    ap.add_argument("--workload", default="fdk", choices=["fdk", "fdk-c2", "diff", "parallel", "production"],
+                    help="fdk: FDK 1024^3 precision form (default); fdk-c2: FDK 512^3 from 720 projections; "
+                         "diff: projector pairs + CGLS refinement; parallel: C1 parallel FBP; production: C3 "
+                         "preprocessing + parallel FBP block")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
-        res = run_reference(args)
+        if args.workload in ("parallel", "production"):
+            res = run_reference_chain(args, args.workload == "production")
+        elif args.workload == "diff":
+            res = run_reference_diff(args)
+        else:
+            res = run_reference(args)
     elif args.workload == "diff":
         res = run_diff(args)
     elif args.workload in ("parallel", "production"):

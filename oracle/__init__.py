@@ -533,13 +533,15 @@ def morphspotclean(img, detect="holes", conn8=True, th=(0.1, 0.1), sigma=(0.01, 
 
 def ref_morphspotclean_module(proj, connectivity="conn4", detectionmethod="morphdetectpeaks", threshold="0.1 0.1",
                               sigma="0.01 0.01", edgesmooth=5, maxarea=30, removeinfnan=False, clampdata=False,
-                              minlevel=-0.1, maxlevel=7.0):
+                              minlevel=-0.1, maxlevel=7.0, threading=False):
+    """The reference MorphSpotCleanModule (morphcleanreplace) on a stack; threading selects its
+    ProcessParallelStd path (one thread per projection, no clamp or inf/NaN removal)."""
     out = np.array(proj, dtype=np.float32, copy=True, order="C")
     nproj, nv, nu = out.shape
     _check_ref(ref().ref_morphspotclean_module(_p(out), _sz(nu), _sz(nv), _sz(nproj), connectivity.encode(),
                                                b"morphcleanreplace", detectionmethod.encode(), threshold.encode(),
                                                sigma.encode(), int(edgesmooth), int(maxarea), int(removeinfnan),
-                                               int(clampdata), _f(minlevel), _f(maxlevel)))
+                                               int(clampdata), _f(minlevel), _f(maxlevel), int(threading)))
     return out
 
 

@@ -16,6 +16,8 @@
 #include <complex>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <utility>
 #include <vector>
 
 #include <fftw3.h>
@@ -38,6 +40,22 @@ struct PlanCommon {
 
 bool is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
 
+// exp(sign * 2 pi i m / n) for m < n/2, each evaluated directly (no recurrence), cached per
+// thread and size: the butterflies read the same values they would compute
+const std::vector<cd> &twiddles(int n, int sign)
+{
+    thread_local std::map<std::pair<int, int>, std::vector<cd>> cache;
+    std::vector<cd> &t = cache[{n, sign}];
+    if (t.empty()) {
+        t.resize(static_cast<size_t>(n / 2));
+        for (int m = 0; m < n / 2; ++m) {
+            const double ang = sign * 2.0 * M_PI * static_cast<double>(m) / n;
+            t[static_cast<size_t>(m)] = cd(std::cos(ang), std::sin(ang));
+        }
+    }
+    return t;
+}
+
 void fft1d(cd *a, int n, int sign)
 {
     if (n <= 1) return;
@@ -55,28 +73,37 @@ void fft1d(cd *a, int n, int sign)
         std::copy(r.begin(), r.end(), a);
         return;
     }
-    // bit reversal permutation
-    for (int i = 1, j = 0; i < n; ++i) {
+    // split real and imaginary parts (plain double loops; the butterflies are the same
+    // operations as with std::complex's finite-value product), bit-reversed order
+    thread_local std::vector<double> re, im;
+    re.resize(static_cast<size_t>(n));
+    im.resize(static_cast<size_t>(n));
+    for (int i = 0, j = 0; i < n; ++i) {
+        re[static_cast<size_t>(j)] = a[i].real();
+        im[static_cast<size_t>(j)] = a[i].imag();
         int bit = n >> 1;
         for (; j & bit; bit >>= 1) j ^= bit;
         j ^= bit;
-        if (i < j) std::swap(a[i], a[j]);
     }
+    const std::vector<cd> &tw = twiddles(n, sign);
     for (int len = 2; len <= n; len <<= 1) {
         const int half = len >> 1;
         const int stride = n / len;
         for (int i = 0; i < n; i += len) {
             for (int k = 0; k < half; ++k) {
-                // twiddle exp(sign * 2 pi i k / len), evaluated directly (no recurrence)
-                double ang = sign * 2.0 * M_PI * static_cast<double>(k * stride) / n;
-                cd w(std::cos(ang), std::sin(ang));
-                cd u = a[i + k];
-                cd v = a[i + k + half] * w;
-                a[i + k] = u + v;
-                a[i + k + half] = u - v;
+                const cd w = tw[static_cast<size_t>(k) * stride];
+                const size_t p = static_cast<size_t>(i + k), q = p + static_cast<size_t>(half);
+                const double vr = re[q] * w.real() - im[q] * w.imag();
+                const double vi = re[q] * w.imag() + im[q] * w.real();
+                const double ur = re[p], ui = im[p];
+                re[p] = ur + vr;
+                im[p] = ui + vi;
+                re[q] = ur - vr;
+                im[q] = ui - vi;
             }
         }
     }
+    for (int i = 0; i < n; ++i) a[i] = cd(re[static_cast<size_t>(i)], im[static_cast<size_t>(i)]);
 }
 
 // In-place multi-dimensional c2c over a row-major array of dims n[0..rank-1].

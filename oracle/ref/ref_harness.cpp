@@ -515,7 +515,7 @@ int ref_morphspotclean(float *img, size_t nu, size_t nv, int detect, int clean, 
 int ref_morphspotclean_module(float *proj, size_t nu, size_t nv, size_t nproj, const char *connectivity,
                               const char *cleanmethod, const char *detectionmethod, const char *threshold,
                               const char *sigma, int edgesmooth, int maxarea, int removeinfnan, int clampdata,
-                              float minlevel, float maxlevel)
+                              float minlevel, float maxlevel, int threading)
 {
     return guarded([&] {
         MorphSpotCleanModule mod(nullptr);
@@ -535,7 +535,7 @@ int ref_morphspotclean_module(float *proj, size_t nu, size_t nv, size_t nproj, c
         par["minlevel"] = b;
         std::snprintf(b, sizeof(b), "%.9g", maxlevel);
         par["maxlevel"] = b;
-        par["threading"] = "false";
+        par["threading"] = threading ? "true" : "false";
         if (mod.Configure(cfg, par) != 0) throw std::runtime_error("MorphSpotCleanModule::Configure failed");
         size_t d3[3] = {nu, nv, nproj};
         kipl::base::TImage<float, 3> img(d3);
