@@ -235,6 +235,16 @@ __global__ void k_peaks_forward_band(const float *__restrict__ pad, int pw, int 
     }
 }
 
+// One or two reconstructions of the same images in one launch (FillHole of the image and of its
+// negation in the 'both' mode): CTA b < nimg works on image b with sign[0] into vol[0], CTA
+// nimg + b on image b with sign[1] into vol[1]. Independent images share the SMs, so the long
+// completions of either set overlap.
+struct RecJobs {
+    float sign[2];
+    float *vol[2];
+    int nimg;
+};
+
 // Exact reconstruction by alternating row sweeps (see the file comment), one warp per image.
 // DILATE: v = min(g, max over neighbourhood); else v = max(g, min over neighbourhood); g is
 // `sign * pad`. Rows are staged in shared memory (coalesced global traffic); lane l owns the
@@ -283,9 +293,11 @@ __device__ __forceinline__ void clamp_then(float al, float ah, float &bl, float 
 // in registers across the vertical step and both scans. C odd: the lanes' chunk positions in
 // the shared row buffers fall in distinct banks.
 template <bool DILATE, int RW, int C>
-__global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict__ pad, float sign, int pw, int ph,
-                                                         int conn8, int rounds, float *__restrict__ vol)
+__global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict__ pad, RecJobs jobs, int pw, int ph,
+                                                         int conn8, int rounds)
 {
+    const int job = blockIdx.x >= jobs.nimg, img = blockIdx.x - job * jobs.nimg;
+    const float sign = jobs.sign[job];
     constexpr int T = 32 * RW, L = T * C + 2 + 1; // row buffer: a neutral element before and after
     extern __shared__ float rows_sm[];
     float(*Gb)[L] = reinterpret_cast<float(*)[L]>(rows_sm);         // [2][L] mask rows
@@ -294,8 +306,8 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
     __shared__ int any_changed[2];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const size_t n = static_cast<size_t>(pw) * ph;
-    const float *g = pad + blockIdx.x * n;
-    float *v = vol + blockIdx.x * n;
+    const float *g = pad + img * n;
+    float *v = jobs.vol[job] + img * n;
     const float neutral = DILATE ? -FLT_MAX : FLT_MAX;
     for (int c = t; c < L; c += T) {
         Gb[0][c] = Gb[1][c] = neutral * sign; // sign * stored = neutral
@@ -431,13 +443,13 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
 }
 
 template <bool DILATE, int RW, int C>
-static mr_status launch_rec(int nimg, const float *pad, float sign, int pw, int ph, int conn8, float *vol,
+static mr_status launch_rec(const RecJobs &jobs, int njobs, const float *pad, int pw, int ph, int conn8,
                             cudaStream_t s)
 {
     const size_t smem = 5 * static_cast<size_t>(32 * RW * C + 3) * sizeof(float);
     MR_CUDA_TRY(cudaFuncSetAttribute(k_reconstruct<DILATE, RW, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-    k_reconstruct<DILATE, RW, C><<<nimg, 32 * RW, smem, s>>>(pad, sign, pw, ph, conn8, kSweepRounds, vol);
+    k_reconstruct<DILATE, RW, C><<<jobs.nimg * njobs, 32 * RW, smem, s>>>(pad, jobs, pw, ph, conn8, kSweepRounds);
     return check_launch("k_reconstruct");
 }
 
@@ -472,13 +484,15 @@ __device__ __forceinline__ int fkey(float f)
 __device__ __forceinline__ float funkey(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
 
 template <bool DILATE, bool CONN8>
-__global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restrict__ pad, float sign, int pw, int ph,
-                                                            float *__restrict__ vol, int *__restrict__ lists, int cap)
+__global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restrict__ pad, RecJobs jobs, int pw,
+                                                            int ph, int *__restrict__ lists, int cap)
 {
     const int t = threadIdx.x;
     const int n = pw * ph;
-    const float *g = pad + blockIdx.x * static_cast<size_t>(n);
-    int *v = reinterpret_cast<int *>(vol + blockIdx.x * static_cast<size_t>(n));
+    const int job = blockIdx.x >= jobs.nimg, img = blockIdx.x - job * jobs.nimg;
+    const float sign = jobs.sign[job];
+    const float *g = pad + img * static_cast<size_t>(n);
+    int *v = reinterpret_cast<int *>(jobs.vol[job] + img * static_cast<size_t>(n));
     int *cur = lists + blockIdx.x * 2 * static_cast<size_t>(cap), *next = cur + cap;
     __shared__ int count[3];
     // floats -> keys, kUnroll pixels per thread at a time
@@ -612,22 +626,23 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
 inline int complete_cap(size_t n) { return static_cast<int>(std::min<size_t>(n, std::max<size_t>(256, n / 16))); }
 
 template <bool DILATE>
-static mr_status launch_reconstruct(int nimg, const float *pad, float sign, int pw, int ph, int conn8, float *vol,
+static mr_status launch_reconstruct(const RecJobs &jobs, int njobs, const float *pad, int pw, int ph, int conn8,
                                     int *lists, cudaStream_t s)
 {
     constexpr int RW = 4;
     const int per = (pw + 32 * RW - 1) / (32 * RW);
     mr_status st;
-    if (per <= 3) st = launch_rec<DILATE, RW, 3>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    else if (per <= 5) st = launch_rec<DILATE, RW, 5>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    else if (per <= 9) st = launch_rec<DILATE, RW, 9>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    else if (per <= 17) st = launch_rec<DILATE, RW, 17>(nimg, pad, sign, pw, ph, conn8, vol, s);
-    else if (per <= 33) st = launch_rec<DILATE, RW, 33>(nimg, pad, sign, pw, ph, conn8, vol, s);
+    if (per <= 3) st = launch_rec<DILATE, RW, 3>(jobs, njobs, pad, pw, ph, conn8, s);
+    else if (per <= 5) st = launch_rec<DILATE, RW, 5>(jobs, njobs, pad, pw, ph, conn8, s);
+    else if (per <= 9) st = launch_rec<DILATE, RW, 9>(jobs, njobs, pad, pw, ph, conn8, s);
+    else if (per <= 17) st = launch_rec<DILATE, RW, 17>(jobs, njobs, pad, pw, ph, conn8, s);
+    else if (per <= 33) st = launch_rec<DILATE, RW, 33>(jobs, njobs, pad, pw, ph, conn8, s);
     else return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 32 * RW * 33 - 2 * kMargin);
     if (st != MR_OK) return st;
     const int cap = complete_cap(static_cast<size_t>(pw) * ph);
-    if (conn8) k_complete<DILATE, true><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, lists, cap);
-    else k_complete<DILATE, false><<<nimg, kFrontThreads, 0, s>>>(pad, sign, pw, ph, vol, lists, cap);
+    const int nb = jobs.nimg * njobs;
+    if (conn8) k_complete<DILATE, true><<<nb, kFrontThreads, 0, s>>>(pad, jobs, pw, ph, lists, cap);
+    else k_complete<DILATE, false><<<nb, kFrontThreads, 0, s>>>(pad, jobs, pw, ph, lists, cap);
     return check_launch("k_complete");
 }
 
@@ -694,7 +709,7 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     // free device memory, so that a block of projections is cleaned concurrently (one CTA per
     // image)
     const size_t cap = static_cast<size_t>(complete_cap(n));
-    const size_t per_img = 3 * n * sizeof(float) + 2 * cap * sizeof(int);
+    const size_t per_img = 3 * n * sizeof(float) + 4 * cap * sizeof(int); // two worklists per reconstruction
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) free_b = size_t(1) << 30;
     const size_t budget = std::max<size_t>(size_t(1) << 30, free_b / 4);
@@ -713,18 +728,24 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
         k_pad<<<dim3(gx, nb), 256, 0, s>>>(img, w, h, removeinfnan ? fmax : nullptr, clamp, minlevel, maxlevel, P);
         k_edge_median<<<2 * nb, 32, pw * sizeof(float), s>>>(P, pw, ph, edge);
         k_minmax<<<nb, 1024, 0, s>>>(P, n, mn, mx);
-        if (detect == 0 || detect == 2) { // FillHole: erosion from a max marker
+        if (detect == 0) { // FillHole: erosion from a max marker
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
-            if ((st = launch_reconstruct<false>(nb, P, 1.0f, pw, ph, conn8, H, lists, s)) != MR_OK) break;
+            const RecJobs jobs{{1.0f, 1.0f}, {H, H}, nb};
+            if ((st = launch_reconstruct<false>(jobs, 1, P, pw, ph, conn8, lists, s)) != MR_OK) break;
         }
         if (detect == 1) { // FillPeaks: forward-scan band replay, then the exact dilation
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, 1.0f, K);
             k_peaks_forward_band<<<div_up(nb, 32), 32, 0, s>>>(P, pw, ph, nb, conn8, mn, K);
-            if ((st = launch_reconstruct<true>(nb, P, 1.0f, pw, ph, conn8, K, lists, s)) != MR_OK) break;
+            const RecJobs jobs{{1.0f, 1.0f}, {K, K}, nb};
+            if ((st = launch_reconstruct<true>(jobs, 1, P, pw, ph, conn8, lists, s)) != MR_OK) break;
         }
-        if (detect == 2) { // -FillHole(-padded): erosion of the negated image from marker max(-P) = -min(P)
+        if (detect == 2) {
+            // FillHole of the image, and -FillHole(-padded): erosion of the negated image from
+            // marker max(-P) = -min(P); both erosions in the same launches
+            k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, -1.0f, K);
-            if ((st = launch_reconstruct<false>(nb, P, -1.0f, pw, ph, conn8, K, lists, s)) != MR_OK) break;
+            const RecJobs jobs{{1.0f, -1.0f}, {H, K}, nb};
+            if ((st = launch_reconstruct<false>(jobs, 2, P, pw, ph, conn8, lists, s)) != MR_OK) break;
         }
         if ((st = check_launch("morphspotclean reconstruction")) != MR_OK) break;
         k_replace<<<dim3(gx, nb), 256, 0, s>>>(P, detect != 1 ? H : nullptr, detect != 0 ? K : nullptr, w, h, detect,
