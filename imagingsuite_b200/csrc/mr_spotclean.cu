@@ -52,7 +52,7 @@ int msc_device_status_take()
 namespace msc {
 
 constexpr int kMargin = 5;
-constexpr int kSweepRounds = 4; // dense sweep rounds before the worklist completion
+constexpr int kSweepRounds = 3; // dense sweep rounds before the worklist completion (2-6 measured: 3 is fastest)
 constexpr int kMaxEdge = 63;
 
 struct Clamp {
@@ -559,9 +559,13 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
                 // travels along a path without waiting for a barrier per pixel. Every moved
                 // pixel is relaxed afterwards, by this thread's chase or from the next list.
                 int p = cur[e];
+                // value of p: read for a listed pixel; for a chased one, the value this thread
+                // just gave it (a lower value someone else gave it meanwhile is propagated by that
+                // thread, and a candidate from a higher one is still an upper bound of the
+                // result), which saves a round trip to L2 per step
+                int kp = __ldcg(v + p);
                 for (int step = 0; p >= 0; ++step) {
                     const int y = p / pw, x = p % pw;
-                    const int kp = __ldcg(v + p);
                     int c[NN], kv[NN];
                     unsigned ok = 0;
 #pragma unroll
@@ -583,15 +587,20 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
                             old[k] = DILATE ? atomicMax(v + q, c[k]) : atomicMin(v + q, c[k]);
                         }
                     }
-                    int follow = -1;
+                    int follow = -1, kf = 0;
 #pragma unroll
                     for (int k = 0; k < NN; ++k) {
                         if (!(((ok >> k) & 1) && improves(c[k], old[k]))) continue;
                         const int q = p + ny[k] * pw + nx[k];
-                        if (follow < 0 && step + 1 < kChase) follow = q;
-                        else push(q, it);
+                        if (follow < 0 && step + 1 < kChase) {
+                            follow = q;
+                            kf = c[k];
+                        } else {
+                            push(q, it);
+                        }
                     }
                     p = follow;
+                    kp = kf;
                 }
             }
         }
