@@ -552,6 +552,23 @@ _SPOT_PARAMS = dict(connectivity="conn8", detectionmethod="morphdetectboth", thr
                     edgesmooth=5, maxarea=30, removeinfnan=False, clampdata=False, minlevel=-0.1, maxlevel=12.0)
 
 
+def module_hbm(times: dict, px: float, hbm_gbs: float, production: bool) -> dict:
+    """Each preprocessing module's compulsory HBM traffic over its measured time: the block read
+    and written once (FullLogNorm: 2 B of uint16 counts in, 4 B out per pixel; the in-place
+    cleaners and the filter: 4 B in, 4 B out), against the measured copy bandwidth."""
+    bpp = {"lognorm": 6.0, "filter": 8.0}
+    if production:
+        bpp.update({"spotclean": 8.0, "ringclean": 8.0})
+    out = {}
+    for name, b in bpp.items():
+        ms = times.get(name)
+        if not ms:
+            continue
+        gbs = b * px / (ms / 1e3) / 1e9
+        out[name] = {"ms": ms, "bytes_per_px": b, "achieved_gbs": gbs, "frac": gbs / hbm_gbs}
+    return out
+
+
 def chain_cpu(P, production: bool, updates: float, sel: int):
     """The reference's own modules (compiled from the reference sources, `oracle/_ref`) chained
     on the host cores with all threads: FullLogNorm -> [MorphSpotCleanModule ->
@@ -777,6 +794,7 @@ def run_parallel(args, production: bool):
                        "projections_backprojected": sel, "l2": "inputs larger than L2" if production else "inputs fit L2"},
             "projections_per_s": nproj * args.steps / t,
             "module_ms": times,
+            "module_hbm": module_hbm(times, float(nu) * nrows * nproj, hbm, production),
             **({"alt_ring_cleaners": alt} if alt else {}),
             "backprojection_gups": updates / tbp / 1e9,
             "roofline": {"bound": "hbm", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
