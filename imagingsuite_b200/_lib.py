@@ -10,6 +10,7 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libmrcuda.so")
+CHECKED_LIB_PATH = os.path.join(_HERE, "libmrcuda_checked.so")
 
 c_size = ctypes.c_size_t
 c_int = ctypes.c_int
@@ -113,6 +114,7 @@ _PROTOS = {
     "mr_measure_smem": (c_int, [P_double, P_double]),
     "mr_data_validator": (c_int, [c_void, c_size, c_void, c_void]),
     "mr_set_wait_limit": (c_int, [c_int]),
+    "mr_bounds_status": (c_int, [ctypes.POINTER(ctypes.c_ulonglong)]),
     "mr_debug_fail_allocation": (c_int, [ctypes.c_longlong]),
     "mr_trace_push": (c_int, [ctypes.c_char_p]),
     "mr_trace_pop": (c_int, []),
@@ -130,17 +132,23 @@ class MrError(RuntimeError):
         self.message = message
 
 
+def load(path: str) -> ctypes.CDLL:
+    """A build of the library at `path` with every prototype set (the bounds-checked build
+    libmrcuda_checked.so has the same entry points)."""
+    if not os.path.exists(path):
+        raise RuntimeError(f"mrcuda library not built: {path} (python -m imagingsuite_b200.build)")
+    l = ctypes.CDLL(path)
+    for name, (res, args) in _PROTOS.items():
+        f = getattr(l, name)
+        f.restype = res
+        f.argtypes = args
+    return l
+
+
 def lib() -> ctypes.CDLL:
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise RuntimeError(f"mrcuda library not built: {LIB_PATH} (python -m imagingsuite_b200.build)")
-        l = ctypes.CDLL(LIB_PATH)
-        for name, (res, args) in _PROTOS.items():
-            f = getattr(l, name)
-            f.restype = res
-            f.argtypes = args
-        _lib = l
+        _lib = load(LIB_PATH)
     return _lib
 
 

@@ -18,6 +18,8 @@
 
 namespace mr {
 
+MR_BOUNDS_TAKE(bounds_take_direct)
+
 mr_status fdk_tma_launch(const void *proj_d, int dtype, const float *scale_d, size_t nu, size_t nv, size_t nproj,
                          const float *xip_d, const float *yip_d, const float *zip_d, const uint32_t *mask_d,
                          int accumulate, int kbegin, int kend, float *vol_d, int bw, int bh, cudaStream_t s);
@@ -73,6 +75,7 @@ __global__ void __launch_bounds__(128) k_bp_parallel(const void *__restrict__ pr
         if (tilt && variant != 0) posu = __fsub_rn(posu, toff);
         const int n = __float2int_rz(posu);
         if (n < 0 || um2 < n) continue;
+        if (!MR_IN_BOUNDS(n + 1, nu, kSiteBpDirect)) continue;
         const int slab = index ? index[i] : i;
         float w = weight ? weight[i] : 1.0f;
         if (DT != MR_F32) w = scale[slab] * w;
@@ -223,6 +226,7 @@ __global__ void __launch_bounds__(128) k_fdk(const void *__restrict__ proj, cons
                     const float a1 = __fadd_rn(Z[3 * k + 1], y1);
                     const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, x1)), 0.5f);
                     if (r < 0.0f || r >= fh) continue; // value 0: acc + dw2*0 == acc
+                    if (!MR_IN_BOUNDS(__float2int_rz(r), nv, kSiteFdkDirect) || !MR_IN_BOUNDS(cc, nu, kSiteFdkDirect)) continue;
                     float v = sample<DT>(proj, base + static_cast<size_t>(__float2int_rz(r)) * nu);
                     if (DT != MR_F32) v = v * s;
                     acc[q] = __fadd_rn(acc[q], __fmul_rn(dw2, v));
@@ -239,6 +243,9 @@ __global__ void __launch_bounds__(128) k_fdk(const void *__restrict__ proj, cons
                     const float r = __fadd_rn(__fmul_rn(dw, __fadd_rn(a1, x1)), 0.5f);
                     const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(a0, x0)), 0.5f);
                     if (r < 0.0f || r >= fh || c < 0.0f || c >= fw) continue;
+                    if (!MR_IN_BOUNDS(__float2int_rz(r), nv, kSiteFdkDirect) ||
+                        !MR_IN_BOUNDS(__float2int_rz(c), nu, kSiteFdkDirect))
+                        continue;
                     float v = sample<DT>(proj, static_cast<size_t>(p) * pstride +
                                                    static_cast<size_t>(__float2int_rz(r)) * nu + __float2int_rz(c));
                     if (DT != MR_F32) v = v * s;

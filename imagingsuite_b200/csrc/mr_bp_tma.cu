@@ -33,6 +33,8 @@ namespace mr {
 // mr_device_status reads and clears it with the FDK kernels' word.
 __device__ int g_bp_error = 0;
 
+MR_BOUNDS_TAKE(bounds_take_bp)
+
 int bp_device_status_take()
 {
     int v = 0, zero = 0;
@@ -275,6 +277,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
 #pragma unroll
                     for (int e = 0; e < G; ++e) {
                         if (q_mode[e] != 1) continue;
+                        if (!MR_IN_BOUNDS(q_off[e] + (zmax - 1) * BW + 1, 2 * NB * BW * TZ, kSiteBpStaged)) continue;
                         const float w = HASW ? S.geo[(gb * NB + b0 + e) * GEO + 3] : 1.0f;
                         if (NN) {
                             if (zmax == TZ) staged_column_nn<HASW, true>(acc, S.box + q_off[e], w, zmax);
@@ -295,6 +298,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_bp_par_staged(const __
                     float wa, wb;
                     const int mode = setup(b, n, off, wa, wb); // formed again: no indexed arrays
                     const float w = HASW ? S.geo[(gb * NB + b) * GEO + 3] : 1.0f;
+                    if (mode == 1 && !MR_IN_BOUNDS(off + (zmax - 1) * BW + 1, 2 * NB * BW * TZ, kSiteBpStaged)) continue;
                     if (mode == 1) {
                         if (NN) staged_column_nn<HASW, false>(acc, S.box + off, w, zmax);
                         else staged_column<HASW, false>(acc, S.box + off, wa, wb, w, zmax);

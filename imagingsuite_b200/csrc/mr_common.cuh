@@ -52,6 +52,48 @@ inline mr_status check_launch(const char *what)
 
 inline cudaStream_t as_stream(void *s) { return static_cast<cudaStream_t>(s); }
 
+// Bounds-checked build (-DMR_BOUNDS_CHECK, libmrcuda_checked.so): the index checks at the gather
+// and scatter sites record the first failing site and index in their translation unit's word
+// and skip the access, instead of reading or writing out of bounds (no trap); the product build
+// compiles them to `true`. mr_bounds_status reads and clears every unit's word.
+#ifdef MR_BOUNDS_CHECK
+static __device__ unsigned long long g_bounds_word = 0; // site << 40 | index, first failure
+__device__ __forceinline__ bool bounds_ok(long long idx, long long size, int site)
+{
+    if (idx >= 0 && idx < size) return true;
+    atomicCAS(&g_bounds_word, 0ull,
+              (static_cast<unsigned long long>(site) << 40) | (static_cast<unsigned long long>(idx) & ((1ull << 40) - 1)));
+    return false;
+}
+#define MR_IN_BOUNDS(idx, size, site) ::mr::bounds_ok((idx), (size), (site))
+#define MR_BOUNDS_TAKE(fn)                                                                                  \
+    int fn(unsigned long long *w)                                                                          \
+    {                                                                                                      \
+        const unsigned long long zero = 0;                                                                 \
+        if (cudaMemcpyFromSymbol(w, g_bounds_word, sizeof(*w)) != cudaSuccess) return -1;                   \
+        return cudaMemcpyToSymbol(g_bounds_word, &zero, sizeof(zero)) == cudaSuccess ? 0 : -1;              \
+    }
+#else
+#define MR_IN_BOUNDS(idx, size, site) true
+#define MR_BOUNDS_TAKE(fn)                                                                                  \
+    int fn(unsigned long long *w)                                                                          \
+    {                                                                                                      \
+        *w = 0;                                                                                            \
+        return 0;                                                                                          \
+    }
+#endif
+// site codes of the checks
+enum BoundsSite {
+    kSiteBpDirect = 1,   // k_bp_parallel: detector column and slice of a sample
+    kSiteFdkDirect = 2,  // k_fdk: detector row and column of a sample
+    kSiteBpStaged = 3,   // k_bp_par_staged: staged box sample
+    kSiteFdkStaged = 4,  // k_fdk_staged: staged box sample (byte offset in the stage buffers)
+    kSiteMbpBins = 5,    // k_mbp_forward_smem: bin in shared memory
+    kSiteMbpAdjoint = 6, // k_mbp_adjoint: projection sample
+    kSiteRingRows = 7,   // k_dwt_rows_t / k_up_rows_t: staged row input
+    kSiteSpotNbr = 8     // k_complete: neighbour pixel
+};
+
 // NVTX range over an entry point (a no-op unless a profiler is attached): every C-ABI call
 // shows up by name on the host timeline around the kernels it launches.
 struct TraceRange {

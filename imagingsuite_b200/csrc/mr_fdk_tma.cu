@@ -49,6 +49,13 @@ namespace mr {
 
 __device__ int g_device_error = 0;
 int bp_device_status_take();  // mr_bp_tma.cu
+// bounds words of the bounds-checked build, one per translation unit with checks
+int bounds_take_bp(unsigned long long *w);      // mr_bp_tma.cu
+int bounds_take_direct(unsigned long long *w);  // mr_backproject.cu
+int bounds_take_matched(unsigned long long *w); // mr_matched.cu
+int bounds_take_ring(unsigned long long *w);    // mr_ringclean.cu
+int bounds_take_spot(unsigned long long *w);    // mr_spotclean.cu
+MR_BOUNDS_TAKE(bounds_take_fdk)
 int msc_device_status_take(); // mr_spotclean.cu
 
 namespace fdk2 {
@@ -181,8 +188,9 @@ __device__ __forceinline__ void fast_coord(const TG &t, float di, float dj, floa
 template <bool FULL>
 __device__ __forceinline__ void exact_column(float2 (&acc)[TK / 2], const unsigned char *smem, uint32_t base,
                                              uint32_t rowbytes, const float *a1, float x1f, float dw, float dw2,
-                                             int kmax)
+                                             int kmax, uint32_t stage_bytes)
 {
+    (void)stage_bytes; // the stage buffers' size, for the bounds-checked build
     const float2 x1 = make_float2(x1f, x1f), dwp = make_float2(dw, dw), dw2p = make_float2(dw2, dw2);
     const float2 mg = make_float2(kMagic, kMagic);
 #pragma unroll
@@ -195,9 +203,11 @@ __device__ __forceinline__ void exact_column(float2 (&acc)[TK / 2], const unsign
             const bool two = FULL || q + 1 < kmax;
             const float2 m = __fmul2_rn(dwp, __fadd2_rn(h ? make_float2(a4.z, a4.w) : make_float2(a4.x, a4.y), x1));
             const float2 b = __fadd2_rd(make_float2(__fadd_rn(m.x, 0.5f), __fadd_rn(m.y, 0.5f)), mg);
-            const float v0 = *reinterpret_cast<const float *>(smem + (__float_as_uint(b.x) * rowbytes + base));
-            const float v1 =
-                two ? *reinterpret_cast<const float *>(smem + (__float_as_uint(b.y) * rowbytes + base)) : 0.0f;
+            const uint32_t o0 = __float_as_uint(b.x) * rowbytes + base, o1 = __float_as_uint(b.y) * rowbytes + base;
+            const float v0 = MR_IN_BOUNDS(o0, stage_bytes, kSiteFdkStaged) ? *reinterpret_cast<const float *>(smem + o0) : 0.0f;
+            const float v1 = two && MR_IN_BOUNDS(o1, stage_bytes, kSiteFdkStaged)
+                                 ? *reinterpret_cast<const float *>(smem + o1)
+                                 : 0.0f;
             const float2 p = __fmul2_rn(dw2p, make_float2(v0, v1));
             acc[q >> 1].x = __fadd_rn(acc[q >> 1].x, p.x);
             if (two) acc[q >> 1].y = __fadd_rn(acc[q >> 1].y, p.y);
@@ -389,6 +399,8 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
     using T = typename Sample<DT>::T;
     extern __shared__ __align__(1024) unsigned char smem[];
     Smem<NB, GEO, EXACT> S(smem, P.boxbytes);
+    const uint32_t stage_bytes = static_cast<uint32_t>(2 * NB * P.boxbytes);
+    (void)stage_bytes;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int i0 = blockIdx.x * TI, j0 = blockIdx.y * TJ, k0 = P.kbegin + blockIdx.z * TK;
@@ -553,9 +565,11 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                         if constexpr (EXACT) {
                             const float *a1 = S.a1 + (warp * NB + b0 + e) * TK;
                             if (kmax == TK)
-                                exact_column<true>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
+                                exact_column<true>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax,
+                                                   stage_bytes);
                             else
-                                exact_column<false>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax);
+                                exact_column<false>(acc, smem, q_base[e], rowbytes, a1, q_c[e], q_a[e], q_b[e], kmax,
+                                                    stage_bytes);
                         } else {
                             const unsigned short wt = static_cast<unsigned short>(__float_as_uint(q_c[e]));
                             if (kmax == TK)
@@ -574,7 +588,8 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                     uint32_t qbase;
                     if (setup(b, qa, qb, qc, qbase)) { // set-up formed again: no indexed arrays
                         if constexpr (EXACT)
-                            exact_column<false>(acc, smem, qbase, rowbytes, S.a1 + (warp * NB + b) * TK, qc, qa, qb, kmax);
+                            exact_column<false>(acc, smem, qbase, rowbytes, S.a1 + (warp * NB + b) * TK, qc, qa, qb, kmax,
+                                                stage_bytes);
                         else
                             fast_column_staged<DT, false>(acc, smem, qbase, rowbytes, qa, qb,
                                                           static_cast<unsigned short>(__float_as_uint(qc)), kmax);
@@ -930,6 +945,28 @@ mr_status mr_fdk_backproject_f64(const float *proj_d, size_t nu, size_t nv, size
                                                          static_cast<int>(nproj), maps_d, mask_d, slices_d,
                                                          static_cast<int>(nslices), out_d);
     return check_launch("k_fdk_f64");
+}
+
+mr_status mr_bounds_status(unsigned long long *first)
+{
+    MR_TRACE();
+    if (!first) return fail(MR_ERR_ARGUMENT, "mr_bounds_status: null pointer");
+    unsigned long long w[6] = {};
+    int bad = 0;
+    bad |= bounds_take_fdk(&w[0]);
+    bad |= bounds_take_bp(&w[1]);
+    bad |= bounds_take_direct(&w[2]);
+    bad |= bounds_take_matched(&w[3]);
+    bad |= bounds_take_ring(&w[4]);
+    bad |= bounds_take_spot(&w[5]);
+    if (bad) return fail(MR_ERR_CUDA, "mr_bounds_status: reading a bounds word failed");
+    *first = 0;
+    for (unsigned long long v : w)
+        if (v) {
+            *first = v;
+            break;
+        }
+    return MR_OK;
 }
 
 mr_status mr_set_wait_limit(int tries)

@@ -30,6 +30,8 @@ namespace mr {
 
 static const float kFPi = 3.1415926535897932384626f;
 
+MR_BOUNDS_TAKE(bounds_take_matched)
+
 // One (x, y) voxel column, CZ slices from z0, per-slice start positions.
 template <int CZ>
 __global__ void __launch_bounds__(128) k_mbp_adjoint(const float *__restrict__ proj, const float2 *__restrict__ sc,
@@ -62,6 +64,7 @@ __global__ void __launch_bounds__(128) k_mbp_adjoint(const float *__restrict__ p
                 const float u = __fsub_rn(__fadd_rn(su[z], cy), sx);
                 const int m = __float2int_rz(u);
                 if (m < 0 || m > n - 2) continue;
+                if (!MR_IN_BOUNDS(m + 1, n, kSiteMbpAdjoint)) continue;
                 const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
                 const float wa = __fsub_rn(1.0f, wb);
                 const float *row = img + static_cast<size_t>(z) * n + m;
@@ -176,6 +179,7 @@ struct BinRun {
     // one voxel: bin m (0 <= m <= n - 2), weights wa, wb, value v
     __device__ __forceinline__ void add(float *bins, float *dbins, int lane, int m, float wa, float wb, float v)
     {
+        (void)dbins; // (the derivative bins follow the value bins)
         const float pa = __fmul_rn(v, wa), pb = __fmul_rn(v, wb);
         const int diff = m - mc;
         if (diff == 0) {
@@ -287,6 +291,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mbp_forward_smem(const float
                         const int m = __float2int_rz(u);
                         if (m < 0 || m > n - 2) continue;
                         const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
+                        if (!MR_IN_BOUNDS(m + 1, n, kSiteMbpBins)) continue;
                         run.add(bins, dbins, lane, m, __fsub_rn(1.0f, wb), wb, v[j]);
                     }
                     p += static_cast<size_t>(U) * nz;
@@ -318,6 +323,7 @@ __global__ void __launch_bounds__(kFwdThreads, 1) k_mbp_forward_smem(const float
                         const int m = __float2int_rz(u);
                         if (m < 0 || m > n - 2) continue;
                         const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
+                        if (!MR_IN_BOUNDS(m + 1, n, kSiteMbpBins)) continue;
                         run.add(bins, dbins, lane, m, __fsub_rn(1.0f, wb), wb, v[j]);
                     }
                     p += static_cast<size_t>(U) * ystride;

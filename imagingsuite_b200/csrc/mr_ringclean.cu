@@ -28,6 +28,9 @@
 #include <vector>
 
 namespace mr {
+
+MR_BOUNDS_TAKE(bounds_take_ring)
+
 namespace rc {
 
 constexpr int kMaxLevels = 16;
@@ -177,7 +180,9 @@ __global__ void __launch_bounds__(kConvThreads) k_dwt_rows_t(const float *__rest
 #pragma unroll
             for (int o = 0; o < kRowOut; ++o) {
                 const int i = t0 + o * kConvThreads;
-                const float x = (j & 1) ? ev[i - (j - 1) / 2] : od[i - j / 2];
+                const int ix = (j & 1) ? i - (j - 1) / 2 : i - j / 2;
+                if (!MR_IN_BOUNDS(ix, NE, kSiteRingRows)) continue;
+                const float x = (j & 1) ? ev[ix] : od[ix];
                 const float2 pr = __fmul2_rn(tt, make_float2(x, x));
                 aH[o] = __fadd_rn(aH[o], pr.x);
                 aG[o] = __fadd_rn(aG[o], pr.y);
@@ -285,6 +290,7 @@ __device__ __forceinline__ void up_rows_block(const float *tp, const float *xin,
         const float *s0 = xin + xoff; // src[(k0 + c) / 2]
 #pragma unroll
         for (int g = kRowBlk / 2 - 1; g >= 1 - KH; --g) {
+            if (!MR_IN_BOUNDS(xoff + g, kConvThreads * kRowBlk / 2 + KH + 2, kSiteRingRows)) continue;
             const float xv = s0[g];
 #pragma unroll
             for (int o = 0; o < kRowBlk; ++o) {

@@ -41,6 +41,8 @@ namespace mr {
 // relocatable device code); mr_device_status reads and clears it with the other kernels' words.
 __device__ int g_msc_error = 0;
 
+MR_BOUNDS_TAKE(bounds_take_spot)
+
 int msc_device_status_take()
 {
     int v = 0, zero = 0;
@@ -584,6 +586,7 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
                         old[k] = c[k];
                         if (((ok >> k) & 1) && improves(c[k], kv[k])) {
                             const int q = p + ny[k] * pw + nx[k];
+                            if (!MR_IN_BOUNDS(q, n, kSiteSpotNbr)) continue;
                             old[k] = DILATE ? atomicMax(v + q, c[k]) : atomicMin(v + q, c[k]);
                         }
                     }

@@ -498,6 +498,12 @@ mr_status mr_device_status(int *status);
  * (datavalidator.h:8-19): counts_d[0] = NaNs and counts_d[1] = infinities (either sign) among
  * the n floats at data_d. counts_d (device, two values) is zeroed first; asynchronous. */
 mr_status mr_data_validator(const float *data_d, size_t n, unsigned long long *counts_d, void *stream);
+/* Bounds-checked build (libmrcuda_checked.so, compiled with -DMR_BOUNDS_CHECK; no counterpart in
+ * the reference): the index checks at the gather sites of the backprojectors, the matched pair,
+ * the ring cleaner and the MorphSpotClean worklist record the first failing site and index and
+ * skip the access. *first = site << 40 | index of the first failure in any kernel since the last
+ * call (0: none), and the record is cleared; the product build always reports 0. Synchronizes. */
+mr_status mr_bounds_status(unsigned long long *first);
 mr_status mr_set_wait_limit(int tries);
 mr_status mr_debug_fail_allocation(long long after);
 mr_status mr_trace_push(const char *name);

@@ -29,6 +29,16 @@ def test_header_symbols_exported():
     assert set(names) == set(L.EXPORTED)
 
 
+def test_checked_build_exports_the_same_symbols():
+    """libmrcuda_checked.so (the bounds-checked build) has every entry point of the header and
+    answers mr_bounds_status without a device."""
+    if not os.path.exists(L.CHECKED_LIB_PATH):
+        pytest.skip("bounds-checked build not made (python -m imagingsuite_b200.build --bounds-check)")
+    lib = L.load(L.CHECKED_LIB_PATH)
+    for n in _declared():
+        assert hasattr(lib, n), n
+
+
 def test_version_and_status():
     lib = L.lib()
     assert lib.mr_version() >= 100
