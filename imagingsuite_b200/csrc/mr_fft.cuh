@@ -207,3 +207,33 @@ inline std::vector<float> fft_permute_response(const std::vector<float> &resp, i
 }
 
 } // namespace mr
+
+// In-place radix-2 DFT in double of a power-of-two length (re, im), sign -1 forward, +1
+// inverse (unnormalised); for the filter responses on the host.
+inline void host_dft(std::vector<double> &re, std::vector<double> &im, int sign)
+{
+    const size_t n = re.size();
+    for (size_t i = 1, j = 0; i < n; ++i) {
+        size_t bit = n >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            std::swap(re[i], re[j]);
+            std::swap(im[i], im[j]);
+        }
+    }
+    for (size_t len = 2; len <= n; len <<= 1) {
+        const size_t half = len / 2;
+        for (size_t k = 0; k < half; ++k) {
+            const double a = sign * 2.0 * M_PI * static_cast<double>(k) / static_cast<double>(len);
+            const double wr = std::cos(a), wi = std::sin(a);
+            for (size_t i = k; i < n; i += len) {
+                const double xr = re[i + half] * wr - im[i + half] * wi, xi = re[i + half] * wi + im[i + half] * wr;
+                re[i + half] = re[i] - xr;
+                im[i + half] = im[i] - xi;
+                re[i] += xr;
+                im[i] += xi;
+            }
+        }
+    }
+}

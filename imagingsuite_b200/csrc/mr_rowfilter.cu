@@ -34,7 +34,7 @@ namespace mr {
 static const double kDPi = 3.1415926535897932384626433832795028841971693993751;
 static const float kFPi = 3.1415926535897932384626f;
 
-enum PadMode { kPadProjFilter = 0, kPadFdk = 1 };
+enum PadMode { kPadProjFilter = 0, kPadFdk = 1, kPadProjCore = 2 };
 
 struct RowFilterArgs {
     const float *in;
@@ -44,6 +44,7 @@ struct RowFilterArgs {
     const float2 *twiddle;
     const float *response; // full-length real response H[k], k < n
     const float *pad;      // projection filter taper (ninsert values)
+    const float *tl, *tr;  // projection filter, short form: the tapers' responses per output column
     const float *row_weight;
     size_t rows_per_weight;
     size_t nrows;
@@ -63,6 +64,7 @@ struct RowFilterArgs {
 // Value of padded position p (0 <= p < n) of one row, reference padding rules.
 __device__ __forceinline__ float padded_value(const RowFilterArgs &a, const float *row, size_t rowidx, int p)
 {
+    if (a.mode == kPadProjCore) return p < a.nu ? row[p] : 0.0f; // the row alone, zero-padded
     if (a.mode == kPadProjFilter) {
         // ProjectionFilterSingle::Pad (:346-362): dest length n+16; data at ninsert;
         // left taper dest[i] = src[0]*pad[i]; right taper dest[n+15-i] = src[nu-1]*pad[i]
@@ -130,11 +132,20 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
     fft_inverse(buf, a.logn, a.twiddle);
 
     // crop and write
+    const float l0 = a.mode == kPadProjCore ? row0[0] : 0.0f, r0v = a.mode == kPadProjCore ? row0[a.nu - 1] : 0.0f;
+    const float l1 = a.mode == kPadProjCore && has1 ? row1[0] : 0.0f;
+    const float r1v = a.mode == kPadProjCore && has1 ? row1[a.nu - 1] : 0.0f;
     for (int i = threadIdx.x; i < a.nu; i += blockDim.x) {
-        const float2 v = buf[fft_slot(i + a.ninsert)];
+        float2 v = buf[fft_slot(i + (a.mode == kPadProjCore ? 0 : a.ninsert))];
+        if (a.mode == kPadProjCore) {
+            // the row's part plus the tapers' (scaled by the edge samples they repeat)
+            const float tl = a.tl[i], tr = a.tr[i];
+            v.x = __fadd_rn(__fadd_rn(v.x, __fmul_rn(l0, tl)), __fmul_rn(r0v, tr));
+            v.y = __fadd_rn(__fadd_rn(v.y, __fmul_rn(l1, tl)), __fmul_rn(r1v, tr));
+        }
         float y0 = __fmul_rn(v.x, a.scale);
         float y1 = __fmul_rn(v.y, a.scale);
-        if (a.mode == kPadProjFilter) {
+        if (a.mode != kPadFdk) {
             if (a.row_weight) {
                 y0 = __fmul_rn(y0, a.row_weight[r0 / a.rows_per_weight]);
                 if (has1) y1 = __fmul_rn(y1, a.row_weight[r1 / a.rows_per_weight]);
@@ -158,6 +169,13 @@ __global__ void __launch_bounds__(512) k_rowfilter(RowFilterArgs a)
             if (has1) a.out[r1 * a.nu + i] = y1;
         }
     }
+}
+
+static size_t next_pow2_size(size_t n)
+{
+    size_t p = 1;
+    while (p < n) p <<= 1;
+    return p;
 }
 
 static int ilog2(size_t n)
@@ -295,10 +313,12 @@ using namespace mr;
 
 struct mr_filter_plan {
     size_t nu = 0, nfft = 0, ninsert = 0;
+    size_t m = 0; // transform length on the device (m < nfft: the short form)
     std::vector<float> filter, pad;
     float2 *twiddle_d = nullptr;
     float *response_d = nullptr;
     float *pad_d = nullptr;
+    float *tl_d = nullptr, *tr_d = nullptr; // short form: taper responses per output column
 };
 
 extern "C" {
@@ -375,29 +395,77 @@ mr_status mr_projfilter_create(size_t nu, const char *filtertype, float cutoff, 
                               filter.data(), pad.data());
     if (st != MR_OK) return st;
     // full-length response: filter on 0..n2-1 and mirrored, Nyquist bin passes
-    std::vector<float> resp(nfft);
-    for (size_t k = 0; k < nfft; ++k) resp[k] = k == n2 ? 1.0f : filter[k < n2 ? k : nfft - k];
-    resp = fft_permute_response(resp, ilog2(nfft)); // in the order of the forward transform's output
-    std::vector<float2> tw = fft_twiddles(static_cast<int>(nfft));
+    std::vector<float> full(nfft);
+    for (size_t k = 0; k < nfft; ++k) full[k] = k == n2 ? 1.0f : filter[k < n2 ? k : nfft - k];
+    // Short form. The reference's output column i is sum_p h[(i + ins - p) mod N] d[p] over the
+    // padded row d (the row at ins, the left taper row[0] * pad[p] before it, the right taper
+    // row[nu-1] * pad[N + 15 - p] after it), h = IDFT_N(full) (unnormalised). Split by source:
+    // the row's part needs h only at lags |l| < nu, i.e. a circular convolution of length
+    // M >= 2 nu - 1 with h cut to those lags (response DFT_M(h cut) / M); the tapers' parts are
+    // row[0] * TL[i] + row[nu-1] * TR[i] with TL, TR fixed by the configuration. All computed
+    // in double. Used when M < N (the padding doubler makes N 2 to 4 times M).
+    const size_t m = next_pow2_size(2 * nu - 1);
+    std::vector<float> resp, tl, tr;
+    size_t tlen = nfft;
+    if (m < nfft) {
+        tlen = m;
+        std::vector<double> H(full.begin(), full.end());
+        std::vector<double> h(H), hi(nfft, 0.0);
+        host_dft(h, hi, +1); // h[l] = sum_k H[k] exp(+2 pi i k l / N)
+        std::vector<double> g(m, 0.0), gi(m, 0.0);
+        g[0] = h[0];
+        for (size_t j = 1; j < nu; ++j) g[j] = g[m - j] = h[j];
+        host_dft(g, gi, -1);
+        resp.resize(m);
+        for (size_t k = 0; k < m; ++k) resp[k] = static_cast<float>(g[k] / static_cast<double>(m));
+        // taper responses: IDFT(H * DFT(taper)) at column i + ins
+        auto taper_response = [&](bool left) {
+            std::vector<double> t(nfft, 0.0), ti(nfft, 0.0);
+            for (size_t i = 0; i < ins; ++i) {
+                if (left) t[i] = pad[i];
+                else if (nfft + 15 - i < nfft) t[nfft + 15 - i] = pad[i];
+            }
+            host_dft(t, ti, -1);
+            for (size_t k = 0; k < nfft; ++k) {
+                t[k] *= H[k];
+                ti[k] *= H[k];
+            }
+            host_dft(t, ti, +1);
+            std::vector<float> out(nu);
+            for (size_t i = 0; i < nu; ++i) out[i] = static_cast<float>(t[(i + ins) % nfft]);
+            return out;
+        };
+        tl = taper_response(true);
+        tr = taper_response(false);
+    } else {
+        resp = full;
+    }
+    resp = fft_permute_response(resp, ilog2(tlen)); // in the order of the forward transform's output
+    std::vector<float2> tw = fft_twiddles(static_cast<int>(tlen));
 
     mr_filter_plan *p = new mr_filter_plan;
     p->nu = nu;
     p->nfft = nfft;
+    p->m = tlen;
     p->ninsert = ins;
     p->filter = filter;
     p->pad = pad;
     mr_status ast = device_alloc_sync(&p->twiddle_d, tw.size() * sizeof(float2), "mr_projfilter_create: twiddles");
-    if (ast == MR_OK) ast = device_alloc_sync(&p->response_d, nfft * sizeof(float), "mr_projfilter_create: response");
+    if (ast == MR_OK) ast = device_alloc_sync(&p->response_d, tlen * sizeof(float), "mr_projfilter_create: response");
     if (ast == MR_OK)
         ast = device_alloc_sync(&p->pad_d, std::max<size_t>(ins, 1) * sizeof(float), "mr_projfilter_create: pad");
+    if (ast == MR_OK && !tl.empty()) ast = device_alloc_sync(&p->tl_d, nu * sizeof(float), "mr_projfilter_create: tapers");
+    if (ast == MR_OK && !tr.empty()) ast = device_alloc_sync(&p->tr_d, nu * sizeof(float), "mr_projfilter_create: tapers");
     if (ast != MR_OK) {
         mr_projfilter_destroy(p);
         return ast;
     }
     cudaError_t err = cudaMemcpy(p->twiddle_d, tw.data(), tw.size() * sizeof(float2), cudaMemcpyHostToDevice);
-    if (err == cudaSuccess) err = cudaMemcpy(p->response_d, resp.data(), nfft * sizeof(float), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess) err = cudaMemcpy(p->response_d, resp.data(), tlen * sizeof(float), cudaMemcpyHostToDevice);
     if (err == cudaSuccess && ins)
         err = cudaMemcpy(p->pad_d, pad.data(), ins * sizeof(float), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !tl.empty()) err = cudaMemcpy(p->tl_d, tl.data(), nu * sizeof(float), cudaMemcpyHostToDevice);
+    if (err == cudaSuccess && !tr.empty()) err = cudaMemcpy(p->tr_d, tr.data(), nu * sizeof(float), cudaMemcpyHostToDevice);
     if (err != cudaSuccess) {
         mr_projfilter_destroy(p);
         return fail(MR_ERR_CUDA, "mr_projfilter_create: %s", cudaGetErrorString(err));
@@ -413,6 +481,8 @@ mr_status mr_projfilter_destroy(mr_filter_plan *plan)
     cudaFree(plan->twiddle_d);
     cudaFree(plan->response_d);
     cudaFree(plan->pad_d);
+    if (plan->tl_d) cudaFree(plan->tl_d);
+    if (plan->tr_d) cudaFree(plan->tr_d);
     delete plan;
     return MR_OK;
 }
@@ -445,11 +515,13 @@ mr_status mr_projfilter_apply(const mr_filter_plan *plan, const float *in_d, flo
     a.nrows = nrows;
     a.nu = static_cast<int>(plan->nu);
     a.nv = 1;
-    a.n = static_cast<int>(plan->nfft);
-    a.logn = ilog2(plan->nfft);
+    a.n = static_cast<int>(plan->m);
+    a.logn = ilog2(plan->m);
     a.ninsert = static_cast<int>(plan->ninsert);
-    a.mode = kPadProjFilter;
-    a.scale = kFPi / (4.0f * static_cast<float>(plan->nfft / 2));
+    a.mode = plan->m < plan->nfft ? kPadProjCore : kPadProjFilter;
+    a.tl = plan->tl_d;
+    a.tr = plan->tr_d;
+    a.scale = kFPi / (4.0f * static_cast<float>(plan->nfft / 2)); // the reference's N
     a.post1 = a.post2 = 1.0f;
     return launch_rowfilter(a, as_stream(stream));
 }
