@@ -22,6 +22,7 @@
 // The derivative d proj / d c_z (-vol for the wa term, +vol for the wb term: d wa / du = -1,
 // d wb / du = +1, du / dc_z = 1) comes out of the same walk.
 #include "mr_common.cuh"
+#include "mr_tma.cuh"
 
 #include <cmath>
 #include <vector>
@@ -32,51 +33,144 @@ static const float kFPi = 3.1415926535897932384626f;
 
 MR_BOUNDS_TAKE(bounds_take_matched)
 
-// One (x, y) voxel column, CZ slices from z0, per-slice start positions.
-template <int CZ>
-__global__ void __launch_bounds__(128) k_mbp_adjoint(const float *__restrict__ proj, const float2 *__restrict__ sc,
-                                                     const float *__restrict__ startu, int nproj, int n, int nz,
-                                                     const uint32_t *__restrict__ mask, int accumulate,
-                                                     float *__restrict__ vol)
+// The adjoint with its projection rows staged in shared memory: a CTA owns 32 (x) x 8 (y) voxel
+// columns x 32 slices, a thread one column's 32 slices in registers over all projections. For a
+// batch of kAdjNB projections the CTA stages, per projection, the detector columns its tile can
+// reach in each of its slices: u is affine in x, y and (through the slice centre) z, so its
+// truncation is extreme at the tile's corners; the window starts one column before the smallest
+// and ends two after the largest (the sample pair n, n + 1 and a column of margin for the
+// float rounding), kAdjBW columns at most, else that projection is read from global memory for
+// this tile. Rows are copied with cp.async (zero outside the detector), the next batch while
+// the current one is summed. Every voxel adds its projections in order with the same float
+// operations as the plain kernel: the result is the same bit for bit.
+constexpr int kAdjTX = 32, kAdjTY = 8, kAdjTZ = 32, kAdjNB = 8, kAdjBW = 48;
+constexpr int kAdjThreads = kAdjTX * kAdjTY;
+constexpr int kAdjNoWindow = -0x40000000;
+
+__host__ __device__ constexpr size_t adj_smem_bytes()
 {
-    const int x1 = blockIdx.x * blockDim.x + threadIdx.x + 1;
-    const int y1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
-    const int z0 = blockIdx.z * CZ;
-    if (x1 > n || y1 > n) return;
-    float *col = vol + (static_cast<size_t>(y1 - 1) * n + (x1 - 1)) * nz;
-    const uint32_t first = mask[2 * (y1 - 1)], second = mask[2 * (y1 - 1) + 1];
-    const bool inside = static_cast<uint32_t>(x1) > first && static_cast<uint32_t>(x1) <= second;
-    float acc[CZ];
+    return sizeof(float) * (2ull * kAdjNB * kAdjTZ * kAdjBW + 2ull * kAdjNB * kAdjTZ) + sizeof(float2) * 2 * kAdjNB +
+           sizeof(int) * 2 * kAdjNB;
+}
+
+__global__ void __launch_bounds__(kAdjThreads) k_mbp_adjoint_staged(const float *__restrict__ proj,
+                                                                    const float2 *__restrict__ sc,
+                                                                    const float *__restrict__ startu, int nproj,
+                                                                    int n, int nz, const uint32_t *__restrict__ mask,
+                                                                    int accumulate, float *__restrict__ vol)
+{
+    extern __shared__ __align__(16) float adj_smem[];
+    float *box = adj_smem;                                   // [2][NB][TZ][BW]
+    float *sus = box + 2 * kAdjNB * kAdjTZ * kAdjBW;         // [2][NB][TZ] slice start positions
+    float2 *scs = reinterpret_cast<float2 *>(sus + 2 * kAdjNB * kAdjTZ); // [2][NB]
+    int *win = reinterpret_cast<int *>(scs + 2 * kAdjNB);    // [2][NB] first staged column
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int x0 = blockIdx.x * kAdjTX, y0 = blockIdx.y * kAdjTY, z0 = blockIdx.z * kAdjTZ;
+    const int x1 = x0 + lane + 1, y1 = y0 + warp + 1; // 1-based voxel
+    const bool valid = x1 <= n && y1 <= n;
+    const bool inside = valid && static_cast<uint32_t>(x1) > mask[2 * (y1 - 1)] &&
+                        static_cast<uint32_t>(x1) <= mask[2 * (y1 - 1) + 1];
+    const int zmax = min(kAdjTZ, nz - z0);
+    float *col = vol + (static_cast<size_t>(valid ? y1 - 1 : 0) * n + (valid ? x1 - 1 : 0)) * nz + z0;
+    float acc[kAdjTZ];
 #pragma unroll
-    for (int c = 0; c < CZ; ++c) acc[c] = (accumulate && inside && z0 + c < nz) ? col[z0 + c] : 0.0f;
-    if (inside) {
-        const float fx = static_cast<float>(x1), fy = static_cast<float>(y1);
-        const size_t pstride = static_cast<size_t>(n) * nz;
-        for (int i = 0; i < nproj; ++i) {
-            const float2 s = sc[i];
-            const float cy = __fmul_rn(s.y, fy), sx = __fmul_rn(s.x, fx);
-            const float *su = startu + static_cast<size_t>(i) * nz;
-            const float *img = proj + static_cast<size_t>(i) * pstride;
+    for (int c = 0; c < kAdjTZ; ++c) acc[c] = (accumulate && inside && c < zmax) ? col[c] : 0.0f;
+    const int nbatch = (nproj + kAdjNB - 1) / kAdjNB;
+    const size_t pstride = static_cast<size_t>(n) * nz;
+    const int xa = x0 + 1, xb = min(x0 + kAdjTX, n), ya = y0 + 1, yb = min(y0 + kAdjTY, n);
+    // geometry and window of batch b into stage st, then its rows by cp.async
+    auto stage = [&](int b, int st) {
+        for (int e = threadIdx.x; e < kAdjNB * kAdjTZ; e += kAdjThreads) {
+            const int i = b * kAdjNB + e / kAdjTZ, z = z0 + e % kAdjTZ;
+            sus[st * kAdjNB * kAdjTZ + e] = (i < nproj && z < nz) ? startu[static_cast<size_t>(i) * nz + z] : 0.0f;
+        }
+        if (threadIdx.x < kAdjNB) {
+            const int i = b * kAdjNB + threadIdx.x;
+            scs[st * kAdjNB + threadIdx.x] = i < nproj ? sc[i] : make_float2(0.0f, 0.0f);
+        }
+        __syncthreads();
+        if (warp < kAdjNB) { // warp w: the window of projection w of the batch, lanes 0-7 the corners
+            const int i = b * kAdjNB + warp;
+            int lo = INT_MAX, hi = INT_MIN;
+            if (lane < 8 && i < nproj) {
+                const float2 s = scs[st * kAdjNB + warp];
+                const float fx = static_cast<float>((lane & 1) ? xb : xa), fy = static_cast<float>((lane & 2) ? yb : ya);
+                const float su = sus[st * kAdjNB * kAdjTZ + warp * kAdjTZ + ((lane & 4) ? zmax - 1 : 0)];
+                const float u = __fsub_rn(__fadd_rn(su, __fmul_rn(s.y, fy)), __fmul_rn(s.x, fx));
+                lo = hi = __float2int_rz(u);
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+                hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+            }
+            if (lane == 0) win[st * kAdjNB + warp] = (i < nproj && hi + 2 - (lo - 1) < kAdjBW) ? lo - 1 : kAdjNoWindow;
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < kAdjNB * kAdjTZ * kAdjBW; e += kAdjThreads) {
+            const int bb = e / (kAdjTZ * kAdjBW), r = e - bb * kAdjTZ * kAdjBW;
+            const int z = r / kAdjBW, c = r - z * kAdjBW;
+            const int i = b * kAdjNB + bb, w0 = win[st * kAdjNB + bb];
+            const int m = w0 + c;
+            const bool ok = w0 != kAdjNoWindow && i < nproj && z < zmax && m >= 0 && m < n;
+            const float *src = ok ? proj + static_cast<size_t>(i) * pstride + static_cast<size_t>(z0 + z) * n + m : proj;
+            tma::copy4_zfill(box + st * kAdjNB * kAdjTZ * kAdjBW + e, src, ok);
+        }
+    };
+    if (nbatch > 0) stage(0, 0);
+    tma::copy_wait_all();
+    __syncthreads();
+    const float fx = static_cast<float>(x1), fy = static_cast<float>(y1);
+    for (int b = 0; b < nbatch; ++b) {
+        const int st = b & 1;
+        if (b + 1 < nbatch) stage(b + 1, st ^ 1); // its barriers only order the staging
+        if (inside) {
+            for (int e = 0; e < kAdjNB; ++e) {
+                const int i = b * kAdjNB + e;
+                if (i >= nproj) break;
+                const float2 s = scs[st * kAdjNB + e];
+                const float cy = __fmul_rn(s.y, fy), sx = __fmul_rn(s.x, fx);
+                const float *su = sus + (st * kAdjNB + e) * kAdjTZ;
+                const int w0 = win[st * kAdjNB + e];
+                if (w0 != kAdjNoWindow) {
+                    const float *bx = box + (st * kAdjNB + e) * kAdjTZ * kAdjBW - w0;
+                    // branch-free over the slices: a voxel whose column is off the detector reads
+                    // a staged column and keeps its sum (a select, not an added zero)
 #pragma unroll
-            for (int c = 0; c < CZ; ++c) {
-                const int z = z0 + c;
-                if (z >= nz) break;
-                const float u = __fsub_rn(__fadd_rn(su[z], cy), sx);
-                const int m = __float2int_rz(u);
-                if (m < 0 || m > n - 2) continue;
-                if (!MR_IN_BOUNDS(m + 1, n, kSiteMbpAdjoint)) continue;
-                const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
-                const float wa = __fsub_rn(1.0f, wb);
-                const float *row = img + static_cast<size_t>(z) * n + m;
-                acc[c] = __fadd_rn(acc[c], __fadd_rn(__fmul_rn(__ldg(row), wa), __fmul_rn(__ldg(row + 1), wb)));
+                    for (int c = 0; c < kAdjTZ; ++c) {
+                        if (c >= zmax) break;
+                        const float u = __fsub_rn(__fadd_rn(su[c], cy), sx);
+                        const int m = __float2int_rz(u);
+                        const bool ok = m >= 0 && m <= n - 2 && MR_IN_BOUNDS(m - w0 + 1, kAdjBW, kSiteMbpAdjoint);
+                        const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
+                        const float wa = __fsub_rn(1.0f, wb);
+                        const float *row = bx + c * kAdjBW + (ok ? m : w0);
+                        const float t = __fadd_rn(__fmul_rn(row[0], wa), __fmul_rn(row[1], wb));
+                        acc[c] = ok ? __fadd_rn(acc[c], t) : acc[c];
+                    }
+                } else {
+                    const float *img = proj + static_cast<size_t>(i) * pstride + static_cast<size_t>(z0) * n;
+#pragma unroll
+                    for (int c = 0; c < kAdjTZ; ++c) {
+                        if (c >= zmax) break;
+                        const float u = __fsub_rn(__fadd_rn(su[c], cy), sx);
+                        const int m = __float2int_rz(u);
+                        if (m < 0 || m > n - 2) continue;
+                        const float wb = fabsf(__fsub_rn(u, static_cast<float>(m)));
+                        const float wa = __fsub_rn(1.0f, wb);
+                        const float *row = img + static_cast<size_t>(c) * n + m;
+                        acc[c] = __fadd_rn(acc[c], __fadd_rn(__fmul_rn(__ldg(row), wa), __fmul_rn(__ldg(row + 1), wb)));
+                    }
+                }
             }
         }
+        // batch b+1's rows have landed; stage st is free for batch b+2
+        tma::copy_wait_all();
+        __syncthreads();
     }
-    // voxels outside the mask stay 0 (or keep what an accumulating call found there)
-    if (inside || !accumulate) {
+    if (valid && (inside || !accumulate)) {
 #pragma unroll
-        for (int c = 0; c < CZ; ++c)
-            if (z0 + c < nz) col[z0 + c] = acc[c];
+        for (int c = 0; c < kAdjTZ; ++c)
+            if (c < zmax) col[c] = acc[c];
     }
 }
 
@@ -378,12 +472,17 @@ mr_status mr_mbp_adjoint(const float *proj_d, size_t n, size_t nz, const float *
     if (!proj_d || !sincos_d || !startu_d || !mask_d || !vol_d) return fail(MR_ERR_ARGUMENT, "mr_mbp_adjoint: null pointer");
     if (n < 2 || n > 65536 || nz == 0 || nz > 65536 || nproj > 0x7fffffff)
         return fail(MR_ERR_ARGUMENT, "mr_mbp_adjoint: unsupported size");
-    constexpr int CZ = 8;
-    dim3 block(32, 4), grid(div_up(n, 32), div_up(n, 4), div_up(nz, CZ));
-    k_mbp_adjoint<CZ><<<grid, block, 0, as_stream(stream)>>>(proj_d, reinterpret_cast<const float2 *>(sincos_d), startu_d,
-                                                           static_cast<int>(nproj), static_cast<int>(n),
-                                                           static_cast<int>(nz), mask_d, accumulate, vol_d);
-    return check_launch("k_mbp_adjoint");
+    static bool attr = false;
+    if (!attr) {
+        MR_CUDA_TRY(cudaFuncSetAttribute(k_mbp_adjoint_staged, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         static_cast<int>(adj_smem_bytes())));
+        attr = true;
+    }
+    dim3 grid(div_up(n, kAdjTX), div_up(n, kAdjTY), div_up(nz, kAdjTZ));
+    k_mbp_adjoint_staged<<<grid, kAdjThreads, adj_smem_bytes(), as_stream(stream)>>>(
+        proj_d, reinterpret_cast<const float2 *>(sincos_d), startu_d, static_cast<int>(nproj), static_cast<int>(n),
+        static_cast<int>(nz), mask_d, accumulate, vol_d);
+    return check_launch("k_mbp_adjoint_staged");
 }
 
 mr_status mr_mbp_forward(const float *vol_d, size_t n, size_t nz, const float *sincos_d, const float *startu_d,
