@@ -34,6 +34,7 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 namespace mr {
 
@@ -291,13 +292,31 @@ __device__ __forceinline__ void clamp_then(float al, float ah, float &bl, float 
     bh = nh;
 }
 
+// Order-preserving integer keys of floats (the completion's atomics compare them as ints).
+__device__ __forceinline__ int fkey(float f)
+{
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7FFFFFFF;
+}
+
+__device__ __forceinline__ float funkey(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
+
 // One image per block of RW warps; lane t of the image owns the row chunk [t*C, t*C + C), held
 // in registers across the vertical step and both scans. C odd: the lanes' chunk positions in
 // the shared row buffers fall in distinct banks.
+//
+// The marker leaves this kernel as keys (fkey): the upward sweep of the last round stores them,
+// and an image that converged earlier is converted by one more pass. That sweep also lists the
+// pixels it changed (at most cap, then only counted) as the completion's first worklist: after
+// it every pixel has been relaxed from its neighbours' current values except from those in the
+// row above it that changed later in the sweep, and exactly those are listed. An image whose
+// round changed nothing is finished and lists nothing.
 template <bool DILATE, int RW, int C>
 __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict__ pad, RecJobs jobs, int pw, int ph,
-                                                         int conn8, int rounds)
+                                                         int conn8, int rounds, int *__restrict__ lists, int cap,
+                                                         int *__restrict__ counts)
 {
+    static_assert(C <= 64, "per-pixel change mask");
     const int job = blockIdx.x >= jobs.nimg, img = blockIdx.x - job * jobs.nimg;
     const float sign = jobs.sign[job];
     constexpr int T = 32 * RW, L = T * C + 2 + 1; // row buffer: a neutral element before and after
@@ -306,16 +325,19 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
     float(*Rb)[L] = reinterpret_cast<float(*)[L]>(rows_sm + 2 * L); // [3][L] marker rows
     __shared__ float wagg[2][RW][2];
     __shared__ int any_changed[2];
+    __shared__ int listed;
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const size_t n = static_cast<size_t>(pw) * ph;
     const float *g = pad + img * n;
     float *v = jobs.vol[job] + img * n;
+    int *list = lists + blockIdx.x * 2 * static_cast<size_t>(cap);
     const float neutral = DILATE ? -FLT_MAX : FLT_MAX;
     for (int c = t; c < L; c += T) {
         Gb[0][c] = Gb[1][c] = neutral * sign; // sign * stored = neutral
         Rb[0][c] = Rb[1][c] = Rb[2][c] = neutral;
     }
     if (t < 2) any_changed[t] = 0;
+    if (t == 0) listed = 0;
     __syncthreads();
     const int c0 = 1 + t * C; // buffer index of the chunk's first element (index 0 is the lead)
     auto fetch = [&](int y, float *G, float *V) {
@@ -360,79 +382,114 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
         return before_l; // the prefix applied to the neutral input
     };
 
-    for (int round = 0; round < rounds; ++round) {
+    // one sweep (pass 0 downward, 1 upward); LAST: the upward sweep of the last round, which lists
+    // the pixels it changes and stores keys. Returns whether this thread's chunks changed.
+    auto sweep = [&](int pass, auto last_tag) -> bool {
+        constexpr bool LAST = decltype(last_tag)::value;
         bool changed = false;
-        for (int pass = 0; pass < 2; ++pass) {
-            int gi = 0, vi = 0;
-            fetch(pass == 0 ? 0 : ph - 1, Gb[0], Rb[0]);
-            cp_async_wait_all();
-            image_sync<RW>();
-            for (int step = 0; step < ph; ++step) {
-                const int y = pass == 0 ? step : ph - 1 - step;
-                const float *G = Gb[gi];
-                float *V = Rb[vi];
-                const float *Pv = Rb[(vi + 2) % 3];
-                if (step + 1 < ph) fetch(pass == 0 ? y + 1 : y - 1, Gb[gi ^ 1], Rb[(vi + 1) % 3]);
-                float gv[C], cv[C];
+        int gi = 0, vi = 0;
+        fetch(pass == 0 ? 0 : ph - 1, Gb[0], Rb[0]);
+        cp_async_wait_all();
+        image_sync<RW>();
+        for (int step = 0; step < ph; ++step) {
+            const int y = pass == 0 ? step : ph - 1 - step;
+            const float *G = Gb[gi];
+            float *V = Rb[vi];
+            const float *Pv = Rb[(vi + 2) % 3];
+            if (step + 1 < ph) fetch(pass == 0 ? y + 1 : y - 1, Gb[gi ^ 1], Rb[(vi + 1) % 3]);
+            float gv[C], cv[C];
+            unsigned long long chg = 0; // LAST: bit j = element j of the chunk changed in this step
+            auto note = [&](int j, bool moved) {
+                if constexpr (LAST) chg |= static_cast<unsigned long long>(moved) << j;
+                else changed |= moved;
+            };
+#pragma unroll
+            for (int j = 0; j < C; ++j) {
+                gv[j] = sign * G[c0 + j];
+                cv[j] = V[c0 + j];
+            }
+            if (step > 0) {
 #pragma unroll
                 for (int j = 0; j < C; ++j) {
-                    gv[j] = sign * G[c0 + j];
-                    cv[j] = V[c0 + j];
+                    float nb = Pv[c0 + j];
+                    if (conn8)
+                        nb = DILATE ? fmaxf(nb, fmaxf(Pv[c0 + j - 1], Pv[c0 + j + 1]))
+                                    : fminf(nb, fminf(Pv[c0 + j - 1], Pv[c0 + j + 1]));
+                    const float nvl = rec_op<DILATE>(gv[j], cv[j], nb);
+                    note(j, nvl != cv[j]);
+                    cv[j] = nvl;
                 }
-                if (step > 0) {
-#pragma unroll
-                    for (int j = 0; j < C; ++j) {
-                        float nb = Pv[c0 + j];
-                        if (conn8)
-                            nb = DILATE ? fmaxf(nb, fmaxf(Pv[c0 + j - 1], Pv[c0 + j + 1]))
-                                        : fminf(nb, fminf(Pv[c0 + j - 1], Pv[c0 + j + 1]));
-                        const float nvl = rec_op<DILATE>(gv[j], cv[j], nb);
-                        changed |= nvl != cv[j];
-                        cv[j] = nvl;
-                    }
-                }
-                // forward along the row
-                {
-                    float lo = neutral, hi = -neutral;
-#pragma unroll
-                    for (int j = 0; j < C; ++j) {
-                        lo = rec_op<DILATE>(gv[j], cv[j], lo);
-                        hi = rec_op<DILATE>(gv[j], cv[j], hi);
-                    }
-                    float run = carry_in(lo, hi, true, 0);
-#pragma unroll
-                    for (int j = 0; j < C; ++j) {
-                        run = rec_op<DILATE>(gv[j], cv[j], run);
-                        changed |= run != cv[j];
-                        cv[j] = run;
-                    }
-                }
-                // backward
-                {
-                    float lo = neutral, hi = -neutral;
-#pragma unroll
-                    for (int j = C - 1; j >= 0; --j) {
-                        lo = rec_op<DILATE>(gv[j], cv[j], lo);
-                        hi = rec_op<DILATE>(gv[j], cv[j], hi);
-                    }
-                    float run = carry_in(lo, hi, false, 1);
-#pragma unroll
-                    for (int j = C - 1; j >= 0; --j) {
-                        run = rec_op<DILATE>(gv[j], cv[j], run);
-                        changed |= run != cv[j];
-                        cv[j] = run;
-                    }
-                }
-#pragma unroll
-                for (int j = 0; j < C; ++j) V[c0 + j] = cv[j];
-                image_sync<RW>();
-                const size_t ro = static_cast<size_t>(y) * pw;
-                for (int c = t; c < pw; c += T) v[ro + c] = V[1 + c];
-                cp_async_wait_all(); // the next row has landed
-                image_sync<RW>();
-                gi ^= 1;
-                vi = (vi + 1) % 3;
             }
+            // forward along the row
+            {
+                float lo = neutral, hi = -neutral;
+#pragma unroll
+                for (int j = 0; j < C; ++j) {
+                    lo = rec_op<DILATE>(gv[j], cv[j], lo);
+                    hi = rec_op<DILATE>(gv[j], cv[j], hi);
+                }
+                float run = carry_in(lo, hi, true, 0);
+#pragma unroll
+                for (int j = 0; j < C; ++j) {
+                    run = rec_op<DILATE>(gv[j], cv[j], run);
+                    note(j, run != cv[j]);
+                    cv[j] = run;
+                }
+            }
+            // backward
+            {
+                float lo = neutral, hi = -neutral;
+#pragma unroll
+                for (int j = C - 1; j >= 0; --j) {
+                    lo = rec_op<DILATE>(gv[j], cv[j], lo);
+                    hi = rec_op<DILATE>(gv[j], cv[j], hi);
+                }
+                float run = carry_in(lo, hi, false, 1);
+#pragma unroll
+                for (int j = C - 1; j >= 0; --j) {
+                    run = rec_op<DILATE>(gv[j], cv[j], run);
+                    note(j, run != cv[j]);
+                    cv[j] = run;
+                }
+            }
+            if constexpr (LAST) {
+                changed |= chg != 0;
+                // positions past the row never change (neutral), so every bit is a pixel
+                if (chg) {
+#pragma unroll
+                    for (int j = 0; j < C; ++j) {
+                        if (!((chg >> j) & 1)) continue;
+                        const int pos = atomicAdd(&listed, 1);
+                        if (pos < cap) list[pos] = y * pw + c0 + j - 1;
+                    }
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < C; ++j) V[c0 + j] = cv[j];
+            image_sync<RW>();
+            const size_t ro = static_cast<size_t>(y) * pw;
+            if constexpr (LAST) {
+                int *vk = reinterpret_cast<int *>(v);
+                for (int c = t; c < pw; c += T) vk[ro + c] = fkey(V[1 + c]);
+            } else {
+                for (int c = t; c < pw; c += T) v[ro + c] = V[1 + c];
+            }
+            cp_async_wait_all(); // the next row has landed
+            image_sync<RW>();
+            gi ^= 1;
+            vi = (vi + 1) % 3;
+        }
+        return changed;
+    };
+
+    bool keys = false; // the marker in global memory is stored as keys
+    for (int round = 0; round < rounds; ++round) {
+        bool changed = sweep(0, std::false_type{});
+        if (round == rounds - 1) {
+            changed |= sweep(1, std::true_type{});
+            keys = true;
+        } else {
+            changed |= sweep(1, std::false_type{});
         }
         // image-wide vote (alternating flags: the one read now is cleared for the round after)
         if (changed) any_changed[round & 1] = 1;
@@ -442,53 +499,65 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
         image_sync<RW>();
         if (!any) break;
     }
+    if (!keys) {
+        // converged before the last round: nothing to list; store the marker as keys
+        int *vk = reinterpret_cast<int *>(v);
+        for (size_t i = t; i < n; i += T) vk[i] = fkey(__int_as_float(vk[i]));
+    }
+    if (t == 0) counts[blockIdx.x] = listed; // the pushes precede the barriers of the last vote
 }
 
 template <bool DILATE, int RW, int C>
-static mr_status launch_rec(const RecJobs &jobs, int njobs, const float *pad, int pw, int ph, int conn8,
-                            cudaStream_t s)
+static mr_status launch_rec(const RecJobs &jobs, int njobs, const float *pad, int pw, int ph, int conn8, int *lists,
+                            int cap, int *counts, cudaStream_t s)
 {
     const size_t smem = 5 * static_cast<size_t>(32 * RW * C + 3) * sizeof(float);
     MR_CUDA_TRY(cudaFuncSetAttribute(k_reconstruct<DILATE, RW, C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      static_cast<int>(smem)));
-    k_reconstruct<DILATE, RW, C><<<jobs.nimg * njobs, 32 * RW, smem, s>>>(pad, jobs, pw, ph, conn8, kSweepRounds);
+    k_reconstruct<DILATE, RW, C><<<jobs.nimg * njobs, 32 * RW, smem, s>>>(pad, jobs, pw, ph, conn8, kSweepRounds,
+                                                                          lists, cap, counts);
     return check_launch("k_reconstruct");
 }
 
 // ---- completion: worklist relaxation
 //
 // After the sweeps the remaining changes are sparse (thin, winding paths through the noise),
-// so each image's CTA finishes the reconstruction with a worklist. Values are handled as
-// order-preserving integer keys so that the relaxation is one atomicMin (erosion:
+// so each image's CTA finishes the reconstruction with a worklist. Values are order-preserving
+// integer keys (the sweeps leave them so) so that the relaxation is one atomicMin (erosion:
 // v[q] = min(v[q], max(g[q], v[p]))) or atomicMax (dilation: v[q] = max(v[q], min(g[q], v[p])))
-// per neighbour. A pixel whose value moved is put on the next iteration's list (once per
-// move: a pixel moved twice in one iteration is listed twice, and its second visit finds its
-// neighbours already relaxed); it then relaxes its neighbours with its current value. When a
-// list overflows, the next iteration relaxes every pixel from its neighbours instead (the
-// first iteration always does). The reconstruction ends when an iteration moves nothing:
-// every pixel then satisfies the fixpoint equations with all its neighbours, and the fixpoint
-// is unique, so the result equals the reference's whatever the order of the updates.
-// Values are read through L2 (ld.cg), where the atomics resolve. Latency shapes the code: an
-// entry issues all its neighbour loads, then all its atomics, before it looks at any result,
-// and the dense passes handle kUnroll pixels per thread at a time.
+// per neighbour. The first list is the sweeps' (the pixels their last sweep changed); an image
+// whose sweeps converged lists nothing and is done. A relaxation is issued, without waiting for
+// its result, when its candidate improves the neighbour's value as loaded, and the neighbour is
+// then listed for the next iteration (or followed, below): every change of a value is made by
+// such an update, whose pixel is listed with the value written, so the last value of every
+// pixel is propagated; a listing whose update lost to a better concurrent one only repeats
+// work. It then relaxes its neighbours with its current value. When a list overflows, the next
+// iteration relaxes every pixel from its neighbours instead. The reconstruction ends when an
+// iteration lists nothing: every pixel then satisfies the fixpoint equations with all its
+// neighbours, and the fixpoint is unique, so the result equals the reference's whatever the
+// order of the updates. Values are read through L2 (ld.cg), where the atomics resolve. Latency
+// shapes the code: an entry issues all its neighbour loads, then all its updates, and the dense
+// passes handle kUnroll pixels per thread at a time.
 
-constexpr int kFrontThreads = 256;
+constexpr int kFrontThreads = 512;
 constexpr int kMaxIterations = 1 << 22;
 constexpr int kUnroll = 4;
 constexpr int kChase = 32; // pixels one thread follows within an iteration
 
-__device__ __forceinline__ int fkey(float f)
+template <bool DILATE>
+__device__ __forceinline__ void relax(int *addr, int c)
 {
-    const int i = __float_as_int(f);
-    return i >= 0 ? i : i ^ 0x7FFFFFFF;
+    if (DILATE) atomicMax(addr, c);
+    else atomicMin(addr, c);
 }
-
-__device__ __forceinline__ float funkey(int k) { return __int_as_float(k >= 0 ? k : k ^ 0x7FFFFFFF); }
 
 template <bool DILATE, bool CONN8>
 __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restrict__ pad, RecJobs jobs, int pw,
-                                                            int ph, int *__restrict__ lists, int cap)
+                                                            int ph, int *__restrict__ lists, int cap,
+                                                            const int *__restrict__ counts)
 {
+    const int first = counts[blockIdx.x]; // the sweeps' list (uniform over the CTA)
+    if (first == 0) return;
     const int t = threadIdx.x;
     const int n = pw * ph;
     const int job = blockIdx.x >= jobs.nimg, img = blockIdx.x - job * jobs.nimg;
@@ -497,18 +566,6 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
     int *v = reinterpret_cast<int *>(jobs.vol[job] + img * static_cast<size_t>(n));
     int *cur = lists + blockIdx.x * 2 * static_cast<size_t>(cap), *next = cur + cap;
     __shared__ int count[3];
-    // floats -> keys, kUnroll pixels per thread at a time
-    for (int i0 = t; i0 < n; i0 += kUnroll * kFrontThreads) {
-        int k[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-            const int i = i0 + u * kFrontThreads;
-            k[u] = i < n ? fkey(__int_as_float(__ldcg(v + i))) : 0;
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u)
-            if (i0 + u * kFrontThreads < n) __stcg(v + i0 + u * kFrontThreads, k[u]);
-    }
     if (t < 3) count[t] = 0;
     __syncthreads();
 
@@ -520,8 +577,8 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
         if (pos < cap) next[pos] = q;
     };
 
-    bool dense = true;
-    int nf = 0, it = 0;
+    bool dense = first > cap;
+    int nf = min(first, cap), it = 0;
     for (; it < kMaxIterations; ++it) {
         if (dense) {
             // every pixel from the extreme of its neighbours, kUnroll pixels at a time
@@ -543,16 +600,12 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
                     c[u] = DILATE ? min(kg, kn) : max(kg, kn);
                     kv[u] = i < n ? __ldcg(v + i) : c[u];
                 }
-                int old[kUnroll];
 #pragma unroll
                 for (int u = 0; u < kUnroll; ++u) {
-                    old[u] = c[u];
-                    if (improves(c[u], kv[u]))
-                        old[u] = DILATE ? atomicMax(v + i0 + u * kFrontThreads, c[u]) : atomicMin(v + i0 + u * kFrontThreads, c[u]);
+                    if (!improves(c[u], kv[u])) continue;
+                    relax<DILATE>(v + i0 + u * kFrontThreads, c[u]);
+                    push(i0 + u * kFrontThreads, it);
                 }
-#pragma unroll
-                for (int u = 0; u < kUnroll; ++u)
-                    if (improves(c[u], old[u])) push(i0 + u * kFrontThreads, it);
             }
         } else {
             for (int e = t; e < nf; e += kFrontThreads) {
@@ -578,23 +631,15 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
                         const int kg = in ? fkey(sign * __ldg(g + q)) : 0;
                         kv[k] = in ? __ldcg(v + q) : 0;
                         c[k] = DILATE ? min(kg, kp) : max(kg, kp);
-                        if (in) ok |= 1u << k;
-                    }
-                    int old[NN];
-#pragma unroll
-                    for (int k = 0; k < NN; ++k) {
-                        old[k] = c[k];
-                        if (((ok >> k) & 1) && improves(c[k], kv[k])) {
-                            const int q = p + ny[k] * pw + nx[k];
-                            if (!MR_IN_BOUNDS(q, n, kSiteSpotNbr)) continue;
-                            old[k] = DILATE ? atomicMax(v + q, c[k]) : atomicMin(v + q, c[k]);
-                        }
+                        if (in && improves(c[k], kv[k])) ok |= 1u << k;
                     }
                     int follow = -1, kf = 0;
 #pragma unroll
                     for (int k = 0; k < NN; ++k) {
-                        if (!(((ok >> k) & 1) && improves(c[k], old[k]))) continue;
+                        if (!((ok >> k) & 1)) continue;
                         const int q = p + ny[k] * pw + nx[k];
+                        if (!MR_IN_BOUNDS(q, n, kSiteSpotNbr)) continue;
+                        relax<DILATE>(v + q, c[k]);
                         if (follow < 0 && step + 1 < kChase) {
                             follow = q;
                             kf = c[k];
@@ -620,41 +665,31 @@ __global__ void __launch_bounds__(kFrontThreads) k_complete(const float *__restr
         nf = min(pushed, cap);
     }
     if (it == kMaxIterations && t == 0) atomicExch(&g_msc_error, 2);
-    __syncthreads();
-    for (int i0 = t; i0 < n; i0 += kUnroll * kFrontThreads) {
-        int k[kUnroll];
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
-            const int i = i0 + u * kFrontThreads;
-            k[u] = i < n ? __ldcg(v + i) : 0;
-        }
-#pragma unroll
-        for (int u = 0; u < kUnroll; ++u)
-            if (i0 + u * kFrontThreads < n) __stcg(v + i0 + u * kFrontThreads, __float_as_int(funkey(k[u])));
-    }
 }
 
 // Worklist capacity per image (entries); a larger frontier falls back to a dense iteration.
 inline int complete_cap(size_t n) { return static_cast<int>(std::min<size_t>(n, std::max<size_t>(256, n / 16))); }
 
+// Sweeps, then the completion, of jobs.nimg x njobs reconstructions (one CTA each). lists: two
+// worklists of complete_cap entries per CTA; counts: one word per CTA (the sweeps' list length).
 template <bool DILATE>
 static mr_status launch_reconstruct(const RecJobs &jobs, int njobs, const float *pad, int pw, int ph, int conn8,
-                                    int *lists, cudaStream_t s)
+                                    int *lists, int *counts, cudaStream_t s)
 {
     constexpr int RW = 4;
     const int per = (pw + 32 * RW - 1) / (32 * RW);
+    const int cap = complete_cap(static_cast<size_t>(pw) * ph);
     mr_status st;
-    if (per <= 3) st = launch_rec<DILATE, RW, 3>(jobs, njobs, pad, pw, ph, conn8, s);
-    else if (per <= 5) st = launch_rec<DILATE, RW, 5>(jobs, njobs, pad, pw, ph, conn8, s);
-    else if (per <= 9) st = launch_rec<DILATE, RW, 9>(jobs, njobs, pad, pw, ph, conn8, s);
-    else if (per <= 17) st = launch_rec<DILATE, RW, 17>(jobs, njobs, pad, pw, ph, conn8, s);
-    else if (per <= 33) st = launch_rec<DILATE, RW, 33>(jobs, njobs, pad, pw, ph, conn8, s);
+    if (per <= 3) st = launch_rec<DILATE, RW, 3>(jobs, njobs, pad, pw, ph, conn8, lists, cap, counts, s);
+    else if (per <= 5) st = launch_rec<DILATE, RW, 5>(jobs, njobs, pad, pw, ph, conn8, lists, cap, counts, s);
+    else if (per <= 9) st = launch_rec<DILATE, RW, 9>(jobs, njobs, pad, pw, ph, conn8, lists, cap, counts, s);
+    else if (per <= 17) st = launch_rec<DILATE, RW, 17>(jobs, njobs, pad, pw, ph, conn8, lists, cap, counts, s);
+    else if (per <= 33) st = launch_rec<DILATE, RW, 33>(jobs, njobs, pad, pw, ph, conn8, lists, cap, counts, s);
     else return fail(MR_ERR_UNSUPPORTED, "mr_morphspotclean: rows longer than %d pixels", 32 * RW * 33 - 2 * kMargin);
     if (st != MR_OK) return st;
-    const int cap = complete_cap(static_cast<size_t>(pw) * ph);
     const int nb = jobs.nimg * njobs;
-    if (conn8) k_complete<DILATE, true><<<nb, kFrontThreads, 0, s>>>(pad, jobs, pw, ph, lists, cap);
-    else k_complete<DILATE, false><<<nb, kFrontThreads, 0, s>>>(pad, jobs, pw, ph, lists, cap);
+    if (conn8) k_complete<DILATE, true><<<nb, kFrontThreads, 0, s>>>(pad, jobs, pw, ph, lists, cap, counts);
+    else k_complete<DILATE, false><<<nb, kFrontThreads, 0, s>>>(pad, jobs, pw, ph, lists, cap, counts);
     return check_launch("k_complete");
 }
 
@@ -673,8 +708,10 @@ __global__ void k_replace(const float *__restrict__ pad, const float *__restrict
         const size_t pi = b * n + static_cast<size_t>(y + kMargin) * pw + x + kMargin;
         const float val = pad[pi];
         float out = val;
-        const float hv = holes ? holes[pi] : 0.0f;
-        const float pv = peaks ? (detect == 2 ? -peaks[pi] : peaks[pi]) : 0.0f;
+        // the reconstructions are stored as keys
+        const float hv = holes ? funkey(__float_as_int(holes[pi])) : 0.0f;
+        const float pk = peaks ? funkey(__float_as_int(peaks[pi])) : 0.0f;
+        const float pv = detect == 2 ? -pk : pk;
         if (s0 == 0.0f && s1 == 0.0f) {
             if (detect != 1 && th0 < fabsf(__fsub_rn(val, hv))) out = hv;
             if (detect != 0 && th1 < fabsf(__fsub_rn(pv, val))) out = pv;
@@ -727,10 +764,11 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
     const size_t budget = std::max<size_t>(size_t(1) << 30, free_b / 4);
     const size_t batch = std::max<size_t>(1, std::min<size_t>(nproj, budget / per_img));
     float *scratch = nullptr;
-    MR_TRY(device_alloc(&scratch, batch * per_img + 4 * batch * sizeof(float), s, "mr_morphspotclean: scratch"));
+    MR_TRY(device_alloc(&scratch, batch * per_img + 5 * batch * sizeof(float), s, "mr_morphspotclean: scratch"));
     float *P = scratch, *H = P + batch * n, *K = H + batch * n, *stats = K + batch * n;
     float *fmax = stats, *mn = stats + batch, *mx = stats + 2 * batch;
-    int *lists = reinterpret_cast<int *>(stats + 4 * batch);
+    int *counts = reinterpret_cast<int *>(stats + 3 * batch); // two words per image (the sweeps' list lengths)
+    int *lists = reinterpret_cast<int *>(stats + 5 * batch);
     mr_status st = MR_OK;
     for (size_t b0 = 0; b0 < nproj && st == MR_OK; b0 += batch) {
         const int nb = static_cast<int>(std::min(batch, nproj - b0));
@@ -743,13 +781,13 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
         if (detect == 0) { // FillHole: erosion from a max marker
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
             const RecJobs jobs{{1.0f, 1.0f}, {H, H}, nb};
-            if ((st = launch_reconstruct<false>(jobs, 1, P, pw, ph, conn8, lists, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<false>(jobs, 1, P, pw, ph, conn8, lists, counts, s)) != MR_OK) break;
         }
         if (detect == 1) { // FillPeaks: forward-scan band replay, then the exact dilation
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, 1.0f, K);
             k_peaks_forward_band<<<div_up(nb, 32), 32, 0, s>>>(P, pw, ph, nb, conn8, mn, K);
             const RecJobs jobs{{1.0f, 1.0f}, {K, K}, nb};
-            if ((st = launch_reconstruct<true>(jobs, 1, P, pw, ph, conn8, lists, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<true>(jobs, 1, P, pw, ph, conn8, lists, counts, s)) != MR_OK) break;
         }
         if (detect == 2) {
             // FillHole of the image, and -FillHole(-padded): erosion of the negated image from
@@ -757,7 +795,7 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, -1.0f, K);
             const RecJobs jobs{{1.0f, -1.0f}, {H, K}, nb};
-            if ((st = launch_reconstruct<false>(jobs, 2, P, pw, ph, conn8, lists, s)) != MR_OK) break;
+            if ((st = launch_reconstruct<false>(jobs, 2, P, pw, ph, conn8, lists, counts, s)) != MR_OK) break;
         }
         if ((st = check_launch("morphspotclean reconstruction")) != MR_OK) break;
         k_replace<<<dim3(gx, nb), 256, 0, s>>>(P, detect != 1 ? H : nullptr, detect != 0 ? K : nullptr, w, h, detect,
