@@ -97,34 +97,83 @@ __global__ void k_pad(const float *__restrict__ img, int w, int h, const float *
     const int b = blockIdx.y;
     const float *src = img + static_cast<size_t>(b) * w * h;
     float *dst = pad + b * n;
-    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < n;
-         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int y = static_cast<int>(idx / pw), x = static_cast<int>(idx % pw) - kMargin;
-        float v = 0.0f;
-        if (x >= 0 && x < w) {
-            int sy = y - kMargin;
-            if (sy < 0) sy = -1 - sy;                 // padded row m-1-i <- image row i
-            else if (sy >= h) sy = 2 * h - 1 - sy;    // padded row ph-m+i <- image row h-1-i
-            v = src[static_cast<size_t>(sy) * w + x];
-            if (finite_max && !isfinite(v)) v = finite_max[b];
-            if (clamp) v = v < lo ? lo : (v > hi ? hi : v);
+    (void)n;
+    for (int y = blockIdx.x; y < ph; y += gridDim.x) {
+        int sy = y - kMargin;
+        if (sy < 0) sy = -1 - sy;              // padded row m-1-i <- image row i
+        else if (sy >= h) sy = 2 * h - 1 - sy; // padded row ph-m+i <- image row h-1-i
+        const float *srow = src + static_cast<size_t>(sy) * w;
+        float *drow = dst + static_cast<size_t>(y) * pw;
+        for (int xp = threadIdx.x; xp < pw; xp += blockDim.x) {
+            const int x = xp - kMargin;
+            float v = 0.0f;
+            if (x >= 0 && x < w) {
+                v = srow[x];
+                if (finite_max && !isfinite(v)) v = finite_max[b];
+                if (clamp) v = v < lo ? lo : (v > hi ? hi : v);
+            }
+            drow[xp] = v;
         }
-        dst[idx] = v;
+    }
+}
+
+// Sliding in-place median of E samples in registers: the window holds the E samples of the
+// current position, the median just written enters it at its place, the next sample at its
+// end. The samples are ordered by an odd-even transposition sort, which swaps only adjacent
+// samples in strictly decreasing order and so ends in the same (stable) order as the
+// reference's insertion sort for any input without NaN.
+template <int E>
+__device__ void edge_median_reg(float *srow, int pw)
+{
+    constexpr int l2 = E / 2;
+    float win[E];
+#pragma unroll
+    for (int q = 0; q < E; ++q) win[q] = q < pw ? srow[q] : 0.0f;
+    for (int i = l2; i < pw - l2; ++i) {
+        float b[E];
+#pragma unroll
+        for (int q = 0; q < E; ++q) b[q] = win[q];
+#pragma unroll
+        for (int pass = 0; pass < E; ++pass) {
+#pragma unroll
+            for (int k = pass & 1; k + 1 < E; k += 2) {
+                const float a = b[k], c = b[k + 1];
+                const bool sw = a > c;
+                b[k] = sw ? c : a;
+                b[k + 1] = sw ? a : c;
+            }
+        }
+        const float m = (E & 1) ? b[E / 2] : static_cast<float>(0.5 * (static_cast<double>(b[E / 2 - 1]) + b[E / 2]));
+        srow[i] = m;
+#pragma unroll
+        for (int q = 0; q + 1 < E; ++q) win[q] = win[q + 1];
+        win[l2 - 1 >= 0 ? l2 - 1 : 0] = l2 >= 1 ? m : win[0];
+        win[E - 1] = i + 1 + l2 < pw ? srow[i + 1 + l2] : 0.0f;
     }
 }
 
 // In-place sliding median of `edge` samples along padded rows 0 and ph-1 (:283-299). One warp
 // per edge row: the row is staged in shared memory, lane 0 runs the sequential in-place loop
 // there (each median sees the medians already written to its left, as in the reference), and
-// the warp writes the row back.
+// the warp writes the row back. Edges 3, 5, 7 and 9 of a row without NaN run in registers.
 __global__ void k_edge_median(float *__restrict__ pad, int pw, int ph, int edge)
 {
     extern __shared__ float srow[];
     const int lane = threadIdx.x;
     float *row = pad + static_cast<size_t>(blockIdx.x >> 1) * pw * ph + ((blockIdx.x & 1) ? static_cast<size_t>(ph - 1) * pw : 0);
-    for (int i = lane; i < pw; i += 32) srow[i] = row[i];
+    bool nan = false;
+    for (int i = lane; i < pw; i += 32) {
+        srow[i] = row[i];
+        nan |= isnan(srow[i]);
+    }
+    nan = __any_sync(0xffffffffu, nan);
     __syncwarp();
-    if (lane == 0) {
+    if (lane == 0 && !nan && (edge == 3 || edge == 5 || edge == 7 || edge == 9)) {
+        if (edge == 3) edge_median_reg<3>(srow, pw);
+        else if (edge == 5) edge_median_reg<5>(srow, pw);
+        else if (edge == 7) edge_median_reg<7>(srow, pw);
+        else edge_median_reg<9>(srow, pw);
+    } else if (lane == 0) {
         const int l2 = edge / 2;
         float buf[kMaxEdge];
         for (int i = l2; i < pw - l2; ++i) {
@@ -188,11 +237,12 @@ __global__ void k_marker(const float *__restrict__ pad, int pw, int ph, const fl
     const size_t n = static_cast<size_t>(pw) * ph;
     const int b = blockIdx.y;
     const float in = sign * interior[b]; // max(-P) = -min(P) for the negated image
-    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < n;
-         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int y = static_cast<int>(idx / pw), x = static_cast<int>(idx % pw);
-        const bool border = y == 0 || y == ph - 1 || x == 0 || x == pw - 1;
-        v[b * n + idx] = border ? sign * pad[b * n + idx] : in;
+    for (int y = blockIdx.x; y < ph; y += gridDim.x) {
+        const size_t ro = b * n + static_cast<size_t>(y) * pw;
+        for (int x = threadIdx.x; x < pw; x += blockDim.x) {
+            const bool border = y == 0 || y == ph - 1 || x == 0 || x == pw - 1;
+            v[ro + x] = border ? sign * pad[ro + x] : in;
+        }
     }
 }
 
@@ -246,6 +296,8 @@ struct RecJobs {
     float sign[2];
     float *vol[2];
     int nimg;
+    const float *interior[2]; // per-image interior value of the marker, formed by the sweeps; null:
+                              // the marker is in vol already
 };
 
 // Exact reconstruction by alternating row sweeps (see the file comment), one warp per image.
@@ -340,11 +392,17 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
     if (t == 0) listed = 0;
     __syncthreads();
     const int c0 = 1 + t * C; // buffer index of the chunk's first element (index 0 is the lead)
-    auto fetch = [&](int y, float *G, float *V) {
+    // row y of the mask into G and of the marker into V; from_marker: the initial marker row,
+    // formed here (the image on the border, the interior value inside; morphextrema.h:268-283)
+    const float *inter = jobs.interior[job];
+    const float in_val = inter ? sign * inter[img] : 0.0f;
+    auto fetch = [&](int y, float *G, float *V, bool from_marker) {
         const size_t ro = static_cast<size_t>(y) * pw;
+        const bool brow = y == 0 || y == ph - 1;
         for (int c = t; c < pw; c += T) {
             cp_async4(G + 1 + c, g + ro + c);
-            cp_async4(V + 1 + c, v + ro + c);
+            if (!from_marker) cp_async4(V + 1 + c, v + ro + c);
+            else V[1 + c] = brow || c == 0 || c == pw - 1 ? sign * g[ro + c] : in_val;
         }
     };
     // exclusive scan over the image's lanes of clamp pairs; returns the carry into this lane
@@ -384,11 +442,11 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
 
     // one sweep (pass 0 downward, 1 upward); LAST: the upward sweep of the last round, which lists
     // the pixels it changes and stores keys. Returns whether this thread's chunks changed.
-    auto sweep = [&](int pass, auto last_tag) -> bool {
+    auto sweep = [&](int pass, bool from_marker, auto last_tag) -> bool {
         constexpr bool LAST = decltype(last_tag)::value;
         bool changed = false;
         int gi = 0, vi = 0;
-        fetch(pass == 0 ? 0 : ph - 1, Gb[0], Rb[0]);
+        fetch(pass == 0 ? 0 : ph - 1, Gb[0], Rb[0], from_marker);
         cp_async_wait_all();
         image_sync<RW>();
         for (int step = 0; step < ph; ++step) {
@@ -396,7 +454,7 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
             const float *G = Gb[gi];
             float *V = Rb[vi];
             const float *Pv = Rb[(vi + 2) % 3];
-            if (step + 1 < ph) fetch(pass == 0 ? y + 1 : y - 1, Gb[gi ^ 1], Rb[(vi + 1) % 3]);
+            if (step + 1 < ph) fetch(pass == 0 ? y + 1 : y - 1, Gb[gi ^ 1], Rb[(vi + 1) % 3], from_marker);
             float gv[C], cv[C];
             unsigned long long chg = 0; // LAST: bit j = element j of the chunk changed in this step
             auto note = [&](int j, bool moved) {
@@ -484,12 +542,12 @@ __global__ void __launch_bounds__(32 * RW) k_reconstruct(const float *__restrict
 
     bool keys = false; // the marker in global memory is stored as keys
     for (int round = 0; round < rounds; ++round) {
-        bool changed = sweep(0, std::false_type{});
+        bool changed = sweep(0, round == 0 && inter, std::false_type{});
         if (round == rounds - 1) {
-            changed |= sweep(1, std::true_type{});
+            changed |= sweep(1, false, std::true_type{});
             keys = true;
         } else {
-            changed |= sweep(1, std::false_type{});
+            changed |= sweep(1, false, std::false_type{});
         }
         // image-wide vote (alternating flags: the one read now is cleared for the round after)
         if (changed) any_changed[round & 1] = 1;
@@ -702,9 +760,9 @@ __global__ void k_replace(const float *__restrict__ pad, const float *__restrict
     const size_t n = static_cast<size_t>(pw) * ph;
     const int b = blockIdx.y;
     const size_t per = static_cast<size_t>(w) * h;
-    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < per;
-         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
-        const int y = static_cast<int>(idx / w), x = static_cast<int>(idx % w);
+    for (int y = blockIdx.x; y < h; y += gridDim.x)
+    for (int x = threadIdx.x; x < w; x += blockDim.x) {
+        const size_t idx = static_cast<size_t>(y) * w + x;
         const size_t pi = b * n + static_cast<size_t>(y + kMargin) * pw + x + kMargin;
         const float val = pad[pi];
         float out = val;
@@ -778,23 +836,20 @@ mr_status mr_morphspotclean(float *proj_d, size_t nu, size_t nv, size_t nproj, i
         k_pad<<<dim3(gx, nb), 256, 0, s>>>(img, w, h, removeinfnan ? fmax : nullptr, clamp, minlevel, maxlevel, P);
         k_edge_median<<<2 * nb, 32, pw * sizeof(float), s>>>(P, pw, ph, edge);
         k_minmax<<<nb, 1024, 0, s>>>(P, n, mn, mx);
-        if (detect == 0) { // FillHole: erosion from a max marker
-            k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
-            const RecJobs jobs{{1.0f, 1.0f}, {H, H}, nb};
+        if (detect == 0) { // FillHole: erosion from a max marker (formed by the first sweep)
+            const RecJobs jobs{{1.0f, 1.0f}, {H, H}, nb, {mx, mx}};
             if ((st = launch_reconstruct<false>(jobs, 1, P, pw, ph, conn8, lists, counts, s)) != MR_OK) break;
         }
         if (detect == 1) { // FillPeaks: forward-scan band replay, then the exact dilation
             k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, 1.0f, K);
             k_peaks_forward_band<<<div_up(nb, 32), 32, 0, s>>>(P, pw, ph, nb, conn8, mn, K);
-            const RecJobs jobs{{1.0f, 1.0f}, {K, K}, nb};
+            const RecJobs jobs{{1.0f, 1.0f}, {K, K}, nb, {nullptr, nullptr}};
             if ((st = launch_reconstruct<true>(jobs, 1, P, pw, ph, conn8, lists, counts, s)) != MR_OK) break;
         }
         if (detect == 2) {
             // FillHole of the image, and -FillHole(-padded): erosion of the negated image from
             // marker max(-P) = -min(P); both erosions in the same launches
-            k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mx, 1.0f, H);
-            k_marker<<<dim3(gx, nb), 256, 0, s>>>(P, pw, ph, mn, -1.0f, K);
-            const RecJobs jobs{{1.0f, -1.0f}, {H, K}, nb};
+            const RecJobs jobs{{1.0f, -1.0f}, {H, K}, nb, {mx, mn}};
             if ((st = launch_reconstruct<false>(jobs, 2, P, pw, ph, conn8, lists, counts, s)) != MR_OK) break;
         }
         if ((st = check_launch("morphspotclean reconstruction")) != MR_OK) break;

@@ -97,6 +97,19 @@ def test_noisy_profile_worklist_completion(cuda, conn8):
         assert np.array_equal(got, O.morphspotclean(img, d, conn8, (0.1, 0.1), (0.0, 0.0), edge=5)), d
 
 
+@pytest.mark.parametrize("edge", [1, 2, 3, 4, 5, 6, 7, 8, 9, 11])
+def test_edge_smoothing_lengths(cuda, edge):
+    """The sliding in-place median along the first and last padded rows at every length (3, 5, 7
+    and 9 run in registers with a sorting network, the others the reference's insertion sort),
+    on values with many ties and zeros of both signs."""
+    rng = np.random.default_rng(85 + edge)
+    img = (np.round(rng.standard_normal((2, 24, 90)) * 2) / 2).astype(np.float32)
+    img[img == 0] = np.where(rng.random(int((img == 0).sum())) < 0.5, -0.0, 0.0).astype(np.float32)
+    for d in ("holes", "both"):
+        got = gpu_clean(img, d, True, (0.3, 0.3), (0.0, 0.0), edge=edge)
+        assert np.array_equal(got, O.morphspotclean(img, d, True, (0.3, 0.3), (0.0, 0.0), edge=edge)), d
+
+
 def test_clamp_and_infnan(cuda):
     rng = np.random.default_rng(82)
     img = (rng.standard_normal((2, 12, 20)) * 5).astype(np.float32)
