@@ -244,56 +244,72 @@ struct Smem {
     unsigned char *stage; // [2][NB] boxes
     float *geo;           // [3][NB][GEO]
     float *a1;            // [NWARPS][NB][TK] (exact kernel)
+    float2 *zy;           // [NWARPS][NB]: Z0 + y0, Z2 + y2 of the warp's voxel row (exact kernel)
     float *tg;            // [2][NB][TGEO] (fast kernel)
-    int4 *meta;           // [2][NB]: x0, y0, mode
+    int4 *meta;           // [2][NB]: x0, y0, mode; .w of a group's first entry: a footprint of the group
+                          // did not fit its box
     uint64_t *bars;       // [2]
+    uint32_t *gdesc;      // [NB][GEO]: source of each geometry element (exact kernel)
     __device__ Smem(unsigned char *base, int boxbytes)
     {
         stage = base;
         geo = reinterpret_cast<float *>(base + 2 * NB * boxbytes);
         a1 = geo + 3 * NB * GEO;
-        tg = a1 + (A1 ? NWARPS * NB * TK : 0);
+        zy = reinterpret_cast<float2 *>(a1 + (A1 ? NWARPS * NB * TK : 0));
+        tg = reinterpret_cast<float *>(zy + (A1 ? NWARPS * NB : 0));
         meta = reinterpret_cast<int4 *>(tg + (A1 ? 0 : 2 * NB * TGEO));
         bars = reinterpret_cast<uint64_t *>(meta + 2 * NB);
+        gdesc = reinterpret_cast<uint32_t *>(bars + 2);
     }
     static size_t bytes(int boxbytes)
     {
         return 2 * NB * static_cast<size_t>(boxbytes) +
-               (3 * NB * GEO + (A1 ? NWARPS * NB * TK : 2 * NB * TGEO)) * sizeof(float) + 2 * NB * sizeof(int4) +
-               2 * sizeof(uint64_t);
+               (3 * NB * GEO + (A1 ? NWARPS * NB * (TK + 2) : 2 * NB * TGEO)) * sizeof(float) +
+               2 * NB * sizeof(int4) + 2 * sizeof(uint64_t) + (A1 ? NB * GEO * sizeof(uint32_t) : 0);
     }
 };
+
+// Sources of the exact kernel's geometry elements of a batch, fixed for the tile: element idx
+// (projection b = idx / GEO_EXACT of the batch) is array[offset + p * stride], p the projection;
+// bits 0-25 the offset, 26-27 the array (0 zip, 1 xip, 2 yip, 3 none: zero), 28-31 b.
+template <int NB>
+__device__ __forceinline__ void geometry_sources(const Params &P, uint32_t *gdesc, int i0, int j0, int k0, int kmax)
+{
+    for (int idx = threadIdx.x; idx < NB * GEO_EXACT; idx += THREADS) {
+        const int b = idx / GEO_EXACT, e = idx % GEO_EXACT;
+        uint32_t arr = 3, off = 0;
+        if (e < TK) {
+            if (e < kmax) arr = 0, off = static_cast<uint32_t>((k0 + e) * 3 + 1);
+        } else if (e < TK + 3 * TI) {
+            const int ii = i0 + (e - TK) / 3;
+            if (ii < P.nu) arr = 1, off = static_cast<uint32_t>(ii * 3 + (e - TK) % 3);
+        } else if (e < TK + 3 * TI + 3 * TJ) {
+            const int jj = j0 + (e - TK - 3 * TI) / 3;
+            if (jj < P.nu) arr = 2, off = static_cast<uint32_t>(jj * 3 + (e - TK - 3 * TI) % 3);
+        } else if (e == TK + 3 * TI + 3 * TJ) {
+            arr = 0, off = 0;
+        } else if (e == TK + 3 * TI + 3 * TJ + 1) {
+            arr = 0, off = 2;
+        }
+        gdesc[idx] = off | arr << 26 | static_cast<uint32_t>(b) << 28;
+    }
+}
 
 // Starts the asynchronous copy of batch s's per-projection geometry into geometry buffer gb
 // (all threads; zero where a projection, column, row or slice does not exist).
 template <bool EXACT, int NB>
-__device__ __forceinline__ void stage_geometry(const Params &P, float *geo, int s, int i0, int j0, int k0, int kmax)
+__device__ __forceinline__ void stage_geometry(const Params &P, float *geo, int s, int i0, int j0, int k0, int kmax,
+                                               const uint32_t *gdesc)
 {
     if constexpr (EXACT) {
+        const size_t zstride = static_cast<size_t>(P.nv) * 3, xstride = static_cast<size_t>(P.nu) * 3;
         for (int idx = threadIdx.x; idx < NB * GEO_EXACT; idx += THREADS) {
-            const int b = idx / GEO_EXACT, e = idx % GEO_EXACT, p = s * NB + b;
-            const float *src = P.zip;
-            bool ok = false;
-            if (p < P.nproj) {
-                if (e < TK) {
-                    ok = e < kmax;
-                    src = P.zip + (static_cast<size_t>(p) * P.nv + k0 + e) * 3 + 1;
-                } else if (e < TK + 3 * TI) {
-                    const int ii = i0 + (e - TK) / 3;
-                    ok = ii < P.nu;
-                    src = P.xip + (static_cast<size_t>(p) * P.nu + ii) * 3 + (e - TK) % 3;
-                } else if (e < TK + 3 * TI + 3 * TJ) {
-                    const int jj = j0 + (e - TK - 3 * TI) / 3;
-                    ok = jj < P.nu;
-                    src = P.yip + (static_cast<size_t>(p) * P.nu + jj) * 3 + (e - TK - 3 * TI) % 3;
-                } else if (e == TK + 3 * TI + 3 * TJ) {
-                    ok = true;
-                    src = P.zip + static_cast<size_t>(p) * P.nv * 3;
-                } else if (e == TK + 3 * TI + 3 * TJ + 1) {
-                    ok = true;
-                    src = P.zip + static_cast<size_t>(p) * P.nv * 3 + 2;
-                }
-            }
+            const uint32_t d = gdesc[idx];
+            const uint32_t arr = (d >> 26) & 3;
+            const int p = s * NB + static_cast<int>(d >> 28);
+            const bool ok = arr != 3 && p < P.nproj;
+            const float *base = arr == 0 ? P.zip : arr == 1 ? P.xip : P.yip;
+            const float *src = base + (d & 0x3FFFFFFu) + static_cast<size_t>(p) * (arr == 0 ? zstride : xstride);
             copy4_zfill(geo + idx, ok ? src : P.zip, ok);
         }
     } else {
@@ -381,10 +397,11 @@ __device__ __forceinline__ void issue_batch(const Params &P, const CUtensorMap *
         }
     }
     const unsigned staged = __ballot_sync(0xffffffffu, corner == 0 && mode == 1);
+    const bool unfit = __ballot_sync(0xffffffffu, corner == 0 && p < P.nproj && mode == 0) != 0; // this warp's group
     if (lane == 0) mbar_expect_tx(&S.bars[st], static_cast<uint32_t>(__popc(staged)) * P.bw * P.bh * sizeof(T));
     __syncwarp();
     if (corner == 0 && p < P.nproj) {
-        S.meta[st * NB + b] = make_int4(x0, y0, mode, 0);
+        S.meta[st * NB + b] = make_int4(x0, y0, mode, (b & 3) == 0 && unfit);
         if (mode == 1) {
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             tma_load_3d(S.stage + (st * NB + b) * P.boxbytes, tmap, x0, y0, p, &S.bars[st]);
@@ -465,7 +482,12 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
     const int nbatch = (P.nproj + NB - 1) / NB;
 
     // geometry of batches 0-2, footprints and copies of batches 0-1
-    for (int s = 0; s < 3 && s < nbatch; ++s) stage_geometry<EXACT, NB>(P, S.geo + s * NB * GEO, s, i0, j0, k0, kmax);
+    if constexpr (EXACT) {
+        geometry_sources<NB>(P, S.gdesc, i0, j0, k0, kmax);
+        __syncthreads();
+    }
+    for (int s = 0; s < 3 && s < nbatch; ++s)
+        stage_geometry<EXACT, NB>(P, S.geo + s * NB * GEO, s, i0, j0, k0, kmax, S.gdesc);
     copy_wait_all();
     __syncthreads();
     for (int s = 0; s < 2 && s < nbatch; ++s)
@@ -500,6 +522,11 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                     const float *g = geo + (idx / TK) * GEO_EXACT;
                     S.a1[warp * NB * TK + idx] = __fadd_rn(g[idx % TK], g[TK + 3 * TI + 3 * warp + 1]);
                 }
+                if (lane < NB) { // the warp-uniform first sums of the set-up: (Z0 + y0), (Z2 + y2)
+                    const float *g = geo + lane * GEO_EXACT;
+                    S.zy[warp * NB + lane] = make_float2(__fadd_rn(g[TK + 3 * TI + 3 * TJ], g[TK + 3 * TI + 3 * warp]),
+                                                         __fadd_rn(g[TK + 3 * TI + 3 * TJ + 1], g[TK + 3 * TI + 3 * warp + 2]));
+                }
                 __syncwarp();
             }
         }
@@ -519,10 +546,9 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                 if constexpr (EXACT) {
                     const float *g = geo + b * GEO;
                     const float x0f = g[TK + 3 * lane], x1f = g[TK + 3 * lane + 1], x2f = g[TK + 3 * lane + 2];
-                    const float y0f = g[TK + 3 * TI + 3 * warp], y2f = g[TK + 3 * TI + 3 * warp + 2];
-                    const float Z0 = g[TK + 3 * TI + 3 * TJ], Z2 = g[TK + 3 * TI + 3 * TJ + 1];
-                    const float dw = __frcp_rn(__fadd_rn(__fadd_rn(Z2, y2f), x2f));
-                    const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(__fadd_rn(Z0, y0f), x0f)), 0.5f);
+                    const float2 zy = S.zy[warp * NB + b];
+                    const float dw = __frcp_rn(__fadd_rn(zy.y, x2f));
+                    const float c = __fadd_rn(__fmul_rn(dw, __fadd_rn(zy.x, x0f)), 0.5f);
                     const int cc = static_cast<int>(c);
                     qa = dw;
                     qb = __fmul_rn(dw, dw);
@@ -555,9 +581,8 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                 // a footprint that did not fit its box (rare; uniform over the CTA) sends the
                 // whole group through the in-order path below, so that every voxel still sums
                 // its projections in the reference's order
-                bool fallback = false;
-#pragma unroll
-                for (int e = 0; e < G; ++e) fallback |= s * NB + b0 + e < P.nproj && S.meta[st * NB + b0 + e].z == 0;
+                static_assert(G == 4, "groups of four projections are the producer warps' groups");
+                const bool fallback = S.meta[st * NB + b0].w != 0;
                 if (!fallback) {
 #pragma unroll
                     for (int e = 0; e < G; ++e) {
@@ -652,7 +677,7 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
             const int g2 = gb == 0 ? 2 : gb - 1;
             issue_batch<DT, EXACT, NB>(P, &tmap, S, S.geo + g2 * NB * GEO, s + 2, st, i0, j0, k0, i_hi, j_hi, kmax);
         }
-        if (s + 3 < nbatch) stage_geometry<EXACT, NB>(P, S.geo + gb * NB * GEO, s + 3, i0, j0, k0, kmax);
+        if (s + 3 < nbatch) stage_geometry<EXACT, NB>(P, S.geo + gb * NB * GEO, s + 3, i0, j0, k0, kmax, S.gdesc);
     }
     if (failed) {
         // copies still in flight: batch s (its wait expired) and batch s+1 when it was issued;
