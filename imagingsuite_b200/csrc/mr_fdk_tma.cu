@@ -165,12 +165,14 @@ __device__ __forceinline__ bool tile_geometry(const double *m, int i0, int j0, i
 
 // Voxel (i0 + di, j0 + dj) relative to the tile origin: inverse depth dw, column
 // c0 + tc, row of slice k0 + q: r0 + tr0 + q dr (tc, tr0 fractions relative to the integer
-// parts TG_C0, TG_R0). The footprints and the voxels use this same function.
+// parts TG_C0, TG_R0). The footprints and the voxels use this same function. The inverse
+// depth is the hardware's approximate reciprocal (relative error ~1e-7, far below the 16-bit
+// samples' 4e-3 and 5e-4 steps).
 template <typename TG>
 __device__ __forceinline__ void fast_coord(const TG &t, float di, float dj, float &dw, float &tc, float &tr0, float &dr)
 {
     const float w = fmaf(t[TG_M8], di, fmaf(t[TG_M9], dj, t[TG_W0]));
-    dw = __frcp_rn(w);
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(dw) : "f"(w));
     tc = fmaf(fmaf(t[TG_AU], di, t[TG_BU] * dj), dw, t[TG_FC]);
     tr0 = fmaf(fmaf(t[TG_AV], di, t[TG_BV] * dj), dw, t[TG_FR]);
     dr = t[TG_M6] * dw;
@@ -557,7 +559,15 @@ __global__ void __launch_bounds__(THREADS, CTAS_PER_SM) k_fdk_staged(const __gri
                     qbase = boxoff + static_cast<uint32_t>(cc - m.x) * 4u - static_cast<uint32_t>(kMagicBits + m.y) * rowbytes;
                     return c >= 0.0f && c < fw;
                 } else {
-                    const float *t = S.tg + (st * NB + b) * TGEO;
+                    float t[TGEO]; // the tile geometry, four vector loads
+#pragma unroll
+                    for (int e = 0; e < TGEO / 4; ++e) {
+                        const float4 t4 = reinterpret_cast<const float4 *>(S.tg + (st * NB + b) * TGEO)[e];
+                        t[4 * e] = t4.x;
+                        t[4 * e + 1] = t4.y;
+                        t[4 * e + 2] = t4.z;
+                        t[4 * e + 3] = t4.w;
+                    }
                     float dw, tc, tr0, dr;
                     fast_coord(t, fdi, fdj, dw, tc, tr0, dr);
                     const int cc = __float_as_int(__fadd_rd(tc, kMagic)) - kMagicBits + __float_as_int(t[TG_C0]);
