@@ -187,6 +187,28 @@ def kernel_time(fn, stream, reps=2):
     return s.elapsed_time(e) / 1e3 / reps
 
 
+def per_kernel_ms(fn, top=20):
+    """Device time per kernel name over one call of fn: the CUDA activity records of the torch
+    profiler (not the timed numbers; the profiler adds overhead around launches)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    out = {}
+    for e in prof.key_averages():
+        us = getattr(e, "self_device_time_total", None)
+        if us is None:
+            us = getattr(e, "self_cuda_time_total", 0.0)
+        if us <= 0:
+            continue
+        name = e.key.split("(")[0].replace("void ", "").strip()
+        out[name] = out.get(name, 0.0) + us / 1e3
+    return dict(sorted(out.items(), key=lambda kv: -kv[1])[:top])
+
+
 def run_mr(args):
     import torch
 
@@ -718,6 +740,7 @@ def run_parallel(args, production: bool):
     t = time_steps(step, args.steps, args.warmup, stream, None)
     clocks = sampler.stop()
     step(record=True)
+    kernels = per_kernel_ms(lambda: step()) if args.kernel_times else None
     alt = None
     if production:
         # the alternative cleaners a configuration can name instead of MorphSpotClean or
@@ -794,6 +817,7 @@ def run_parallel(args, production: bool):
                        "projections_backprojected": sel, "l2": "inputs larger than L2" if production else "inputs fit L2"},
             "projections_per_s": nproj * args.steps / t,
             "module_ms": times,
+            **({"kernel_ms": kernels} if kernels else {}),
             "module_hbm": module_hbm(times, float(nu) * nrows * nproj, hbm, production),
             **({"alt_ring_cleaners": alt} if alt else {}),
             "backprojection_gups": updates / tbp / 1e9,
@@ -1048,6 +1072,8 @@ def main():
     ap.add_argument("--impl", default="mr", choices=["mr", "reference"])
     ap.add_argument("--small", action="store_true", help="256^3 profiling case")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--kernel-times", action="store_true",
+                    help="parallel/production: per-kernel device times of one extra step (torch profiler)")
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--workload", default="fdk", choices=["fdk", "fdk-c2", "diff", "parallel", "production"],
                     help="fdk: FDK 1024^3 precision form (default); fdk-c2: FDK 512^3 from 720 projections; "
