@@ -1075,10 +1075,23 @@ class FDKbp_single(_BackProjectorBase):
         weights = _float_vector(_get(parameters, "weights"), nproj)
         angles = _float_vector(_get(parameters, "angles"), nproj)
         geo = self.prepare(angles, weights, projections.device)
-        filt, scale = self.ramp_filter(projections, geo)
+        filt, scale = self.ramp_filter(projections, geo, *self._filter_out(projections))
         self.backproject(filt, scale, geo)
         self._first = False
         return 0
+
+    def _filter_out(self, projections: torch.Tensor):
+        """(first, out, scale) for ramp_filter: the filtered projections' buffer and the 16-bit
+        path's per-projection scales, kept between calls of the same shape and precision (a
+        block of projections is several GB: no allocation per call)."""
+        dtype = torch.float32 if _PRECISION[self.precision] == L.MR_F32 else torch.uint16
+        buf = getattr(self, "_filt_buf", None)
+        if buf is None or buf.shape != projections.shape or buf.dtype != dtype or buf.device != projections.device:
+            self._filt_buf = self._filt_scale = None  # release the old buffers first
+            self._filt_buf = torch.empty(projections.shape, dtype=dtype, device=projections.device)
+            self._filt_scale = None if dtype == torch.float32 else \
+                torch.empty(projections.shape[0], dtype=torch.float32, device=projections.device)
+        return 0, self._filt_buf, self._filt_scale
 
     def prepare(self, angles: np.ndarray, weights: np.ndarray, dev):
         """Per-projection geometry (partials or FP64 maps, staging box, filter weights) on the
